@@ -1,0 +1,175 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import
+this module.  It runs the C++ restatement in ``pamtra_oracle.cpp`` column by
+column, mirroring ``PamtraFortranWrapper`` (python/pyPamtra/libWrapper.py:24)
+of the reference.
+"""
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+MAXNLEG = 200
+
+_lib = None
+
+
+class OrcSettings(ctypes.Structure):
+    _fields_ = [
+        ("emissivity", ctypes.c_double),
+        ("hydro_threshold", ctypes.c_double),
+        ("hydro_softsphere_min_density", ctypes.c_double),
+        ("lgas_extinction", ctypes.c_int32),
+        ("lhyd_absorption", ctypes.c_int32),
+        ("lhyd_scattering", ctypes.c_int32),
+        ("lhyd_emission", ctypes.c_int32),
+        ("hydro_includehydroinrhoair", ctypes.c_int32),
+        ("hydro_adaptive_grid", ctypes.c_int32),
+        ("conserve_mass_rescale_dsd", ctypes.c_int32),
+        ("hydro_limit_density_area", ctypes.c_int32),
+        ("outpol_vh", ctypes.c_int32),
+        ("nummu", ctypes.c_int32),
+    ]
+
+
+class OrcDebug(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in
+                ("kextatmo", "kexttot", "salbedo", "nlegen", "legen", "present", "scatter_matrix", "ext",
+                 "emis", "num_doubles")]
+
+
+def build():
+    """Compile the oracle with its Makefile (g++ only)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        l = ctypes.CDLL(LIB)
+        dp = ctypes.POINTER(ctypes.c_double)
+        l.orc_run_column.restype = ctypes.c_int
+        l.orc_run_column.argtypes = [ctypes.POINTER(OrcSettings), ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                     dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, ctypes.c_double, ctypes.c_int,
+                                     dp, ctypes.c_char, ctypes.c_int, dp, dp, dp, dp,
+                                     ctypes.POINTER(OrcDebug)]
+        l.orc_gas_r98.restype = ctypes.c_int
+        l.orc_gas_r98.argtypes = [ctypes.c_double] * 4 + [dp]
+        l.orc_eps_water_tkc.restype = None
+        l.orc_eps_water_tkc.argtypes = [ctypes.c_double, ctypes.c_double, dp, dp]
+        l.orc_lobatto.argtypes = [ctypes.c_int, dp, dp]
+        l.orc_minvert.restype = ctypes.c_int
+        l.orc_minvert.argtypes = [ctypes.c_int, dp, dp]
+        l.orc_e_sat.argtypes = [ctypes.c_double, dp]
+        _lib = l
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def settings(pk_settings):
+    """Copy a pamtra_b200.packing.Settings into the oracle's struct."""
+    s = OrcSettings()
+    for name, _ in OrcSettings._fields_:
+        setattr(s, name, getattr(pk_settings, name))
+    return s
+
+
+def run_column(st, species, cols, c, freqs, debug=False):
+    """Run column ``c`` of packed ``cols`` (pamtra_b200.packing.profile_columns)."""
+    l = lib()
+    L = int(cols["nlyrs"][c])
+    Lmax = int(cols["max_nlyrs"])
+    H = len(species)
+    N = st.nummu
+    nf = len(freqs)
+    nout = int(cols["noutlevels"])
+    f64 = lambda a: np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    hl = {k: f64(cols[k][c, :L + 1]) for k in ("hgt_lev", "temp_lev", "press_lev", "relhum_lev")}
+    ly = {k: f64(cols[k][c, :L]) for k in ("hgt", "temp", "press", "relhum")}
+    hq = {k: f64(cols[k][c, :L, :]) if H else np.zeros(1) for k in ("hydro_q", "hydro_n", "hydro_reff")}
+    obs = f64(cols["obs_height"][c])
+    fr = f64(freqs)
+    tb = np.zeros((nout, 2 * N, nf, 2))
+    em = np.zeros((2, nf, N))
+    ang = np.zeros(2 * N)
+    dbg = None
+    out_dbg = None
+    if debug:
+        n = 2 * N
+        out_dbg = dict(kextatmo=np.zeros((nf, L)), kexttot=np.zeros((nf, L)), salbedo=np.zeros((nf, L)),
+                       nlegen=np.zeros((nf, L), np.int32), legen=np.zeros((nf, L, 3, MAXNLEG)),
+                       present=np.zeros(L, np.int32), scatter_matrix=np.zeros((nf, L, 4, n, n)),
+                       ext=np.zeros((nf, L)), emis=np.zeros((nf, L)), num_doubles=np.zeros((nf, L), np.int32))
+        dbg = OrcDebug(**{k: v.ctypes.data for k, v in out_dbg.items()})
+    sp = np.ascontiguousarray(species)
+    refl = bytes([int(cols["sfc_refl"][c]) & 0xFF])
+    err = l.orc_run_column(ctypes.byref(st), sp.ctypes.data if H else None, H, L,
+                           _p(hl["hgt_lev"]), _p(hl["temp_lev"]), _p(hl["press_lev"]), _p(hl["relhum_lev"]),
+                           _p(ly["hgt"]), _p(ly["temp"]), _p(ly["press"]), _p(ly["relhum"]),
+                           _p(hq["hydro_q"]), _p(hq["hydro_n"]), _p(hq["hydro_reff"]),
+                           float(cols["groundtemp"][c]), nout, _p(obs), refl, nf, _p(fr), _p(tb), _p(em),
+                           _p(ang), ctypes.byref(dbg) if dbg is not None else None)
+    return err, tb, em, ang, out_dbg
+
+
+def run_pamtra(pam, freqs, nummu=16, debug=False):
+    """Oracle counterpart of ``pyPamtra.runPamtra``: returns a results dict with
+    ``tb`` (ngridx, ngridy, noutlevels, 2N, nfreq, 2), ``emissivity``,
+    ``angles_deg`` and the error code."""
+    from pamtra_b200 import packing
+    st = settings(packing.settings_from_nml(pam.nmlSet, nummu))
+    sp = packing.species_from_df(pam.df.data)
+    cols = packing.profile_columns(pam.p, pam.df.nhydro)
+    nx, ny = int(pam.p["ngridx"]), int(pam.p["ngridy"])
+    nout = int(cols["noutlevels"])
+    N = nummu
+    tb = np.full((nx * ny, nout, 2 * N, len(freqs), 2), -9999.0)
+    em = np.full((nx * ny, 2, len(freqs), N), -9999.0)
+    err_all = 0
+    ang = None
+    dbgs = []
+    for c in range(nx * ny):
+        err, t, e, a, d = run_column(st, sp, cols, c, freqs, debug)
+        err_all = max(err_all, err)
+        tb[c], em[c], ang = t, e, a
+        dbgs.append(d)
+    r = dict(tb=tb.reshape(nx, ny, nout, 2 * N, len(freqs), 2),
+             emissivity=em.reshape(nx, ny, 2, len(freqs), N), angles_deg=ang)
+    if debug:
+        r["debug"] = dbgs
+    return r, err_all
+
+
+def gas_r98(f, T, rhowv, p):
+    k = ctypes.c_double()
+    err = lib().orc_gas_r98(f, T, rhowv, p, ctypes.byref(k))
+    return err, k.value
+
+
+def eps_water_tkc(T_c, f):
+    re, im = ctypes.c_double(), ctypes.c_double()
+    lib().orc_eps_water_tkc(T_c, f, ctypes.byref(re), ctypes.byref(im))
+    return complex(re.value, im.value)
+
+
+def lobatto(n):
+    mu, w = np.zeros(n), np.zeros(n)
+    lib().orc_lobatto(n, _p(mu), _p(w))
+    return mu, w
+
+
+def minvert(A):
+    A = np.asfortranarray(np.asarray(A, dtype=np.float64))
+    out = np.zeros_like(A, order="F")
+    err = lib().orc_minvert(A.shape[0], _p(A), _p(out))
+    return err, out

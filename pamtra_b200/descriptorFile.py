@@ -1,0 +1,102 @@
+"""Hydrometeor descriptor file, same columns and semantics as the reference's
+``pamDescriptorFile`` (python/pyPamtra/descriptorFile.py:12-240).
+
+A descriptor row has 20 fields:
+hydro_name, as_ratio, liq_ice, rho_ms, a_ms, b_ms, alpha_as, beta_as,
+moment_in, nbin, dist_name, p_1, p_2, p_3, p_4, d_1, d_2, scat_name,
+vel_size_mod, canting.
+"""
+
+import csv
+
+import numpy as np
+
+missingNumber = -9999.0
+
+NAMES = ["hydro_name", "as_ratio", "liq_ice", "rho_ms", "a_ms", "b_ms", "alpha_as", "beta_as",
+         "moment_in", "nbin", "dist_name", "p_1", "p_2", "p_3", "p_4", "d_1", "d_2", "scat_name",
+         "vel_size_mod", "canting"]
+TYPES = ["U15", float, int, float, float, float, float, float, int, int, "U15", float, float, float,
+         float, float, float, "U60", "U30", float]
+
+
+class pamDescriptorFile(object):
+    """Descriptor table of the hydrometeor species of a :class:`pyPamtra` run.
+
+    Mirrors python/pyPamtra/descriptorFile.py:12 (``data`` recarray, ``data4D``
+    and ``dataFullSpec`` dicts, ``nhydro``).
+    """
+
+    def __init__(self, parent):
+        self.names = np.array(NAMES)
+        self.types = TYPES
+        self.data = np.recarray((0,), dtype=list(zip(self.names, self.types)))
+        self.data4D = dict()
+        self.nhydro = 0
+        self.parent = parent
+        self.dataFullSpec = dict()
+        self.fs_nbin = 0
+
+    def readFile(self, fname):
+        """Read an ASCII descriptor file (descriptorFile.py:30-56): space separated,
+        lines starting with ``!`` are comments."""
+        with open(fname, "r") as f:
+            for row in csv.reader(f, delimiter=" ", skipinitialspace=True):
+                if not row or row[0][0] == "!":
+                    continue
+                assert len(row) == len(self.names)
+                for ii, item in enumerate(row):
+                    if self.types[ii] == float:
+                        row[ii] = item.replace("d", "e")
+                    if self.types[ii] in ("S15", "U15"):
+                        row[ii] = item.replace("'", "").replace('"', "")
+                self.addHydrometeor(row)
+
+    def writeFile(self, fname):
+        """Write the table as an ASCII descriptor file (descriptorFile.py:58-70)."""
+        assert len(self.names) == len(self.data.dtype.names)
+        with open(fname, "w") as f:
+            writer = csv.writer(f, delimiter=" ")
+            for row in self.data:
+                writer.writerow(list(row))
+
+    def addHydrometeor(self, hydroTuple):
+        """Append one species (descriptorFile.py:72-97).  Extends the parent's
+        ``hydro_q``/``hydro_reff``/``hydro_n`` profile arrays with a missing-value
+        slice, as the reference does."""
+        assert hydroTuple[0] not in self.data["hydro_name"]
+        assert len(list(self.dataFullSpec.keys())) == 0
+        row = np.array(tuple(hydroTuple), dtype=list(zip(self.names, self.types)))
+        self.data = np.append(self.data, row).view(np.recarray)
+        self.nhydro += 1
+        par = self.parent
+        par._shape4D = (par.p["ngridx"], par.p["ngridy"], par.p["max_nlyrs"], self.nhydro)
+        for key in ["hydro_q", "hydro_reff", "hydro_n"]:
+            if key in par.p:
+                par.p[key] = np.concatenate(
+                    [par.p[key], np.ones(par._shape3D + (1,)) * missingNumber], axis=-1)
+
+    def removeHydrometeor(self, hydroName):
+        """Remove a species by name, or all with ``"all"`` (descriptorFile.py:99-133)."""
+        assert len(list(self.dataFullSpec.keys())) == 0
+        if hydroName == "all":
+            self.__init__(self.parent)
+            return
+        matches = np.where(self.data["hydro_name"] == hydroName)[0]
+        if len(matches) == 0:
+            raise ValueError("Did not find " + hydroName)
+        idx = matches[0]
+        self.data = np.delete(self.data, idx).view(np.recarray)
+        self.nhydro -= 1
+        par = self.parent
+        for key in ["hydro_q", "hydro_reff", "hydro_n"]:
+            if key in par.p:
+                par.p[key] = np.delete(par.p[key], idx, axis=-1)
+        for key in list(self.data4D.keys()):
+            self.data4D[key] = np.delete(self.data4D[key], idx, axis=-1)
+
+    def add4D(self, key, arr):
+        """Per-(x,y,layer,species) override of a numeric descriptor column
+        (the reference's ``data4D``, libWrapper.py:117-121)."""
+        assert key in self.names
+        self.data4D[key] = np.asarray(arr, dtype=float)

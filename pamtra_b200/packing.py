@@ -1,0 +1,151 @@
+"""Host-side packer: turns the pyPamtra session state (``nmlSet``, descriptor
+table, profile dict ``p``) into the flat column-major-by-column arrays the
+C-ABI takes.  This replaces the module-global copies that the reference's
+``PamtraFortranWrapper`` performs (python/pyPamtra/libWrapper.py:24-207).
+
+Columns are the flattened (ngridx, ngridy) grid in C order.
+"""
+
+import ctypes
+
+import numpy as np
+
+# dist_name codes shared with the native library (include/pamtra_b200.h)
+DIST_CODES = {"exp": 0, "exp_field_t": 1, "mgamma": 2, "mono": 3, "exp_cosmo_snow": 4,
+              "exp_ryan": 5, "logn": 6, "disabled": 7}
+# scat_name codes: only Mie spheres are on this path
+SCAT_CODES = {"mie-sphere": 0, "disabled": 1}
+
+MAXNLEG = 200
+
+
+class Settings(ctypes.Structure):
+    """Mirror of ``pamtra_b200_settings`` (include/pamtra_b200.h)."""
+    _fields_ = [
+        ("emissivity", ctypes.c_double),
+        ("hydro_threshold", ctypes.c_double),
+        ("hydro_softsphere_min_density", ctypes.c_double),
+        ("lgas_extinction", ctypes.c_int32),
+        ("lhyd_absorption", ctypes.c_int32),
+        ("lhyd_scattering", ctypes.c_int32),
+        ("lhyd_emission", ctypes.c_int32),
+        ("hydro_includehydroinrhoair", ctypes.c_int32),
+        ("hydro_adaptive_grid", ctypes.c_int32),
+        ("conserve_mass_rescale_dsd", ctypes.c_int32),
+        ("hydro_limit_density_area", ctypes.c_int32),
+        ("outpol_vh", ctypes.c_int32),
+        ("nummu", ctypes.c_int32),
+    ]
+
+
+class Species(ctypes.Structure):
+    """Mirror of ``pamtra_b200_species``: one descriptor-file row."""
+    _fields_ = [
+        ("liq_ice", ctypes.c_int32),
+        ("moment_in", ctypes.c_int32),
+        ("nbin", ctypes.c_int32),
+        ("dist", ctypes.c_int32),
+        ("as_ratio", ctypes.c_double),
+        ("rho_ms", ctypes.c_double),
+        ("a_ms", ctypes.c_double),
+        ("b_ms", ctypes.c_double),
+        ("alpha_as", ctypes.c_double),
+        ("beta_as", ctypes.c_double),
+        ("p_1", ctypes.c_double),
+        ("p_2", ctypes.c_double),
+        ("p_3", ctypes.c_double),
+        ("p_4", ctypes.c_double),
+        ("d_1", ctypes.c_double),
+        ("d_2", ctypes.c_double),
+    ]
+
+
+SPECIES_DTYPE = np.dtype([(name, np.int32 if ct is ctypes.c_int32 else np.float64)
+                          for name, ct in Species._fields_])
+assert SPECIES_DTYPE.itemsize == ctypes.sizeof(Species)
+
+
+def settings_from_nml(nmlSet, nummu=16):
+    """Validate the namelist keys this path honours and build the settings
+    struct.  Options whose reference branch is not on the passive Mie path
+    raise NotImplementedError instead of silently changing behaviour."""
+    if str(nmlSet.get("gas_mod", "R98")).strip() != "R98":
+        raise NotImplementedError("gas_mod %r: only R98 is on this path" % nmlSet["gas_mod"])
+    if str(nmlSet.get("liq_mod", "TKC")).strip() != "TKC":
+        raise NotImplementedError("liq_mod %r: only TKC is on this path" % nmlSet["liq_mod"])
+    if nmlSet.get("hydro_fullspec", False):
+        raise NotImplementedError("hydro_fullspec input is not on this path")
+    outpol = str(nmlSet.get("outpol", "VH")).strip()
+    if outpol not in ("VH", "IQ"):
+        raise ValueError("outpol must be VH or IQ")
+    s = Settings()
+    s.emissivity = float(nmlSet["emissivity"])
+    s.hydro_threshold = float(nmlSet["hydro_threshold"])
+    s.hydro_softsphere_min_density = float(nmlSet["hydro_softsphere_min_density"])
+    s.lgas_extinction = int(bool(nmlSet["lgas_extinction"]))
+    s.lhyd_absorption = int(bool(nmlSet["lhyd_absorption"]))
+    s.lhyd_scattering = int(bool(nmlSet["lhyd_scattering"]))
+    s.lhyd_emission = int(bool(nmlSet["lhyd_emission"]))
+    s.hydro_includehydroinrhoair = int(bool(nmlSet["hydro_includehydroinrhoair"]))
+    s.hydro_adaptive_grid = int(bool(nmlSet["hydro_adaptive_grid"]))
+    s.conserve_mass_rescale_dsd = int(bool(nmlSet["conserve_mass_rescale_dsd"]))
+    s.hydro_limit_density_area = int(bool(nmlSet["hydro_limit_density_area"]))
+    s.outpol_vh = int(outpol == "VH")
+    s.nummu = int(nummu)
+    return s
+
+
+def species_from_df(data):
+    """Descriptor recarray -> structured array of ``pamtra_b200_species``."""
+    out = np.zeros(len(data), dtype=SPECIES_DTYPE)
+    for i, row in enumerate(data):
+        dist = str(row["dist_name"]).strip()
+        scat = str(row["scat_name"]).strip()
+        if dist not in DIST_CODES or dist == "exp_cosmo_snow":
+            raise NotImplementedError("dist_name %r is not on this path" % dist)
+        if scat not in SCAT_CODES:
+            raise NotImplementedError("scat_name %r is not on this path (mie-sphere only)" % scat)
+        out[i]["liq_ice"] = int(row["liq_ice"])
+        out[i]["moment_in"] = int(row["moment_in"])
+        out[i]["nbin"] = int(row["nbin"])
+        out[i]["dist"] = DIST_CODES["disabled"] if scat == "disabled" else DIST_CODES[dist]
+        for k in ("as_ratio", "rho_ms", "a_ms", "b_ms", "alpha_as", "beta_as", "p_1", "p_2", "p_3", "p_4",
+                  "d_1", "d_2"):
+            out[i][k] = float(row[k])
+    return out
+
+
+def profile_columns(p, nhydro):
+    """Profile dict -> dict of C-contiguous float64/int arrays, one row per
+    column (flattened x, y)."""
+    nx, ny, L = int(p["ngridx"]), int(p["ngridy"]), int(p["max_nlyrs"])
+    ncol = nx * ny
+
+    def col(key, tail, fill=np.nan):
+        if key in p and isinstance(p[key], np.ndarray) and p[key].size > 0:
+            a = np.asarray(p[key], dtype=np.float64).reshape((ncol,) + tail)
+        else:
+            a = np.full((ncol,) + tail, fill)
+        return np.ascontiguousarray(a)
+
+    cols = dict()
+    cols["nlyrs"] = np.ascontiguousarray(np.asarray(p["nlyrs"]).reshape(ncol).astype(np.int32))
+    for k in ("hgt_lev", "temp_lev", "press_lev", "relhum_lev"):
+        cols[k] = col(k, (L + 1,))
+    for k in ("hgt", "temp", "press", "relhum"):
+        cols[k] = col(k, (L,))
+    for k in ("hydro_q", "hydro_n", "hydro_reff"):
+        cols[k] = col(k, (L, nhydro), fill=0.0) if nhydro > 0 else np.zeros((ncol, L, 0))
+    cols["groundtemp"] = col("groundtemp", ())
+    nout = int(p["noutlevels"])
+    cols["obs_height"] = col("obs_height", (nout,))
+    refl = np.asarray(p["sfc_refl"]).reshape(ncol)
+    refl = np.array([(r.decode() if isinstance(r, bytes) else str(r))[:1] or 'S' for r in refl])
+    cols["sfc_refl"] = np.ascontiguousarray(np.frombuffer("".join(refl).encode(), dtype=np.int8).copy())
+    sfc_type = np.asarray(p.get("sfc_type", np.full(ncol, -9999))).reshape(ncol)
+    if np.any((sfc_type == 0) | (sfc_type == 1)):
+        raise NotImplementedError("sfc_type 0/1 (ocean/land emissivity models) is not on this path")
+    cols["ncol"] = ncol
+    cols["max_nlyrs"] = L
+    cols["noutlevels"] = nout
+    return cols
