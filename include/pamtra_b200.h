@@ -1,0 +1,176 @@
+/*
+ * pamtra_b200.h -- C ABI of the B200-native PAMTRA passive forward path.
+ *
+ * Boundary being replaced.  The reference crosses from Python into native
+ * code through f2py: python/pyPamtra/libWrapper.py:24-235
+ * (PamtraFortranWrapper) copies the namelist settings, the descriptor file
+ * and the profile into Fortran module globals and calls
+ * pypamtralib.run_pamtra() (src/pyPamtraLib.f90:18), which loops
+ * frequency x grid and calls run_rt (src/run_rt.f90:1) per column.  Results
+ * come back as vars_output.out_* arrays.  Error codes are 0 (success),
+ * 1 (warning), 2 (fatal) (src/report_module.f90:11-14).
+ *
+ * Here the same seam is one re-entrant call per batch of columns on a
+ * caller-provided CUDA stream, with plain pointers and sizes.  All array
+ * pointers in pamtra_b200_columns / pamtra_b200_outputs are DEVICE pointers
+ * (caller-owned), except in pamtra_b200_run_host, which takes HOST pointers
+ * and performs the copies itself.  The library owns only its scratch arena,
+ * held by the context.
+ *
+ * Layouts (row-major, C order):
+ *   level arrays  [ncol][max_nlyrs+1]   bottom-up, NaN = missing
+ *   layer arrays  [ncol][max_nlyrs]     bottom-up, NaN = missing
+ *   hydro arrays  [ncol][max_nlyrs][nhydro]
+ *   tb            [ncol][noutlevels][2*max_nummu][max_nfreq][2]   (V,H or I,Q)
+ *   emissivity    [ncol][2][max_nfreq][max_nummu]
+ *   status        [ncol][max_nfreq]   0 ok, 2 fatal, see PAMTRA_B200_ST_*
+ */
+#ifndef PAMTRA_B200_H
+#define PAMTRA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PAMTRA_B200_MAXNLEG 200   /* src/settings.f90:13 maxleg */
+#define PAMTRA_B200_MAXBIN 256    /* bins per species slot */
+
+/* error / status codes (src/report_module.f90:11-14, plus per-column detail) */
+#define PAMTRA_B200_OK 0
+#define PAMTRA_B200_WARNING 1
+#define PAMTRA_B200_FATAL 2
+#define PAMTRA_B200_ST_NORM 0x100      /* check_norm4 failed (src/radscat4.f90:125) */
+#define PAMTRA_B200_ST_PSD 0x200       /* run_drop_size_dist fatal */
+#define PAMTRA_B200_ST_MIE 0x400       /* calc_mie_spheres assertion failed */
+#define PAMTRA_B200_ST_GAS 0x800       /* rosen98 input range (src/rosen98_gasabs.f90:103-125) */
+#define PAMTRA_B200_ST_PIVOT 0x1000    /* singular matrix in an inverse */
+#define PAMTRA_B200_ST_NAN 0x2000      /* NaN in extinction / coefficients */
+#define PAMTRA_B200_ST_SIZE 0x4000     /* a size limit of this library was exceeded */
+
+/* dist_name codes (src/make_dist_param.f90) */
+#define PAMTRA_B200_DIST_EXP 0
+#define PAMTRA_B200_DIST_EXP_FIELD_T 1
+#define PAMTRA_B200_DIST_MGAMMA 2
+#define PAMTRA_B200_DIST_MONO 3
+#define PAMTRA_B200_DIST_EXP_RYAN 5
+#define PAMTRA_B200_DIST_LOGN 6
+#define PAMTRA_B200_DIST_DISABLED 7
+
+/* precision of the doubling / adding matrix products */
+#define PAMTRA_B200_PREC_FP64 0      /* plain and batched FP64 */
+#define PAMTRA_B200_PREC_3XTF32 1    /* 3xTF32 tensor-core products, FP64 inverses */
+
+/* Settings: the nmlSet keys on the passive Mie path
+ * (src/settings.f90:454-573; python/pyPamtra/core.py:89-157). */
+typedef struct pamtra_b200_settings {
+  double emissivity;                 /* nmlSet['emissivity'] (sfc_optics.f90:79-81) */
+  double hydro_threshold;            /* nmlSet['hydro_threshold'] */
+  double hydro_softsphere_min_density;
+  int32_t lgas_extinction;
+  int32_t lhyd_absorption;
+  int32_t lhyd_scattering;
+  int32_t lhyd_emission;
+  int32_t hydro_includehydroinrhoair;
+  int32_t hydro_adaptive_grid;
+  int32_t conserve_mass_rescale_dsd;
+  int32_t hydro_limit_density_area;
+  int32_t outpol_vh;                 /* nmlSet['outpol'] == 'VH' */
+  int32_t nummu;                     /* default quadrature angles per hemisphere */
+} pamtra_b200_settings;
+
+/* One descriptor-file row (python/pyPamtra/descriptorFile.py:19-20);
+ * string fields are encoded: dist (PAMTRA_B200_DIST_*), scat = mie-sphere. */
+typedef struct pamtra_b200_species {
+  int32_t liq_ice, moment_in, nbin, dist;
+  double as_ratio, rho_ms, a_ms, b_ms, alpha_as, beta_as;
+  double p_1, p_2, p_3, p_4, d_1, d_2;
+} pamtra_b200_species;
+
+/* A batch of columns.  The plain form passes ncol = 1. */
+typedef struct pamtra_b200_columns {
+  int32_t ncol, max_nlyrs, nhydro, max_nfreq, noutlevels, max_nummu;
+  int32_t species_stride;     /* 0: one species table for all columns; nhydro: per column */
+  int32_t max_present;        /* upper bound on hydrometeor-bearing layers in the batch, 0 = ncol*max_nlyrs */
+  int32_t nummu_mask;         /* bit 0: N=8, bit 1: N=16, bit 2: N=32 present; 0 = settings.nummu only */
+  const pamtra_b200_species* species;  /* HOST pointer, [ncol or 1][nhydro] (copied by the library) */
+  const int32_t* nlyrs;       /* [ncol] */
+  const int32_t* nummu;       /* [ncol] in {8,16,32}; NULL = settings.nummu */
+  const int32_t* nfreq;       /* [ncol]; NULL = max_nfreq for all */
+  const double* freqs;        /* [ncol][max_nfreq] GHz, or [max_nfreq] if nfreq == NULL */
+  const double *hgt_lev, *temp_lev, *press_lev, *relhum_lev;   /* [ncol][max_nlyrs+1] */
+  const double *hgt, *temp, *press, *relhum;                   /* [ncol][max_nlyrs]   */
+  const double *hydro_q, *hydro_n, *hydro_reff;                /* [ncol][max_nlyrs][nhydro] */
+  const double* groundtemp;   /* [ncol], NaN = lowest level temperature */
+  const double* obs_height;   /* [ncol][noutlevels] m */
+  const int8_t* sfc_refl;     /* [ncol] 'S', 'L' or 'F' */
+} pamtra_b200_columns;
+
+typedef struct pamtra_b200_outputs {
+  double* tb;            /* [ncol][noutlevels][2*max_nummu][max_nfreq][2] */
+  double* emissivity;    /* [ncol][2][max_nfreq][max_nummu] or NULL */
+  double* angles_deg;    /* [2*max_nummu] or NULL (angles of max_nummu) */
+  int32_t* status;       /* [ncol][max_nfreq] or NULL */
+  /* optional single-scattering output of save_ssp (run_rt.f90:140-146),
+   * for all columns/frequencies; NULL to skip */
+  double* kextatmo;      /* [ncol][max_nfreq][max_nlyrs] Np/m */
+  double* kexttot;       /* [ncol][max_nfreq][max_nlyrs] */
+  double* salbedo;       /* [ncol][max_nfreq][max_nlyrs] */
+  double* scatter_matrix;/* [ncol][max_nfreq][max_nlyrs][4][n][n], n = 2*max_nummu, row=(i2,j2) */
+  int32_t* num_doubles;  /* [ncol][max_nfreq][max_nlyrs] bottom-up, -1 = non-scattering */
+} pamtra_b200_outputs;
+
+typedef struct pamtra_b200_ctx pamtra_b200_ctx;
+
+/* Create / destroy a context bound to a CUDA device.  The context owns a
+ * scratch arena that grows to the largest batch seen (cudaMalloc outside
+ * any run) and the quadrature tables.  One context may be used from one
+ * host thread at a time; use one context per concurrent stream. */
+int32_t pamtra_b200_create(int32_t device, pamtra_b200_ctx** out);
+int32_t pamtra_b200_destroy(pamtra_b200_ctx* ctx);
+
+/* Scratch bytes a batch needs (so callers can pack batches by free HBM). */
+size_t pamtra_b200_workspace_bytes(const pamtra_b200_columns* cols, int32_t precision);
+
+/* Reserve the arena for batches up to this size before capture/serving. */
+int32_t pamtra_b200_reserve(pamtra_b200_ctx* ctx, size_t bytes);
+
+/* Run the passive forward model on a batch (replaces run_pamtra,
+ * src/pyPamtraLib.f90:18, for the columns given).  Asynchronous on `stream`
+ * (a cudaStream_t; NULL = legacy default stream).  Returns 0, or 2 on an
+ * argument/launch error; per-column failures are in outputs->status. */
+int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* settings,
+                        const pamtra_b200_columns* cols, const pamtra_b200_outputs* out,
+                        int32_t precision, void* stream);
+
+/* Same with HOST pointers in cols/out: copies inputs to the device, runs,
+ * copies outputs back and synchronises the stream. */
+int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* settings,
+                             const pamtra_b200_columns* cols, const pamtra_b200_outputs* out,
+                             int32_t precision, void* stream);
+
+/* Number of kernel launches the last pamtra_b200_run issued on ctx. */
+int32_t pamtra_b200_last_launch_count(const pamtra_b200_ctx* ctx);
+
+/* ---- single-stage entry points (parity tests of individual routines) ---- */
+
+/* Rosenkranz-98 absorption (src/rosen98_gasabs.f90:2 + get_gasabs.f90:95),
+ * element-wise over device arrays; kext in Np/m. */
+int32_t pamtra_b200_gas_r98(const double* freq, const double* temp, const double* rho_vap,
+                            const double* press, double* kext, int32_t* status, int32_t n, void* stream);
+
+/* TKC water permittivity (src/eps_water.f90:653), element-wise; T in degC. */
+int32_t pamtra_b200_eps_water_tkc(const double* t_c, const double* freq, double* eps_re, double* eps_im,
+                                  int32_t n, void* stream);
+
+/* Matrix inverse with partial pivoting of `count` column-major n x n matrices
+ * (replaces MINVERT, src/radmat.f90:155), n in {16,32,64}. */
+int32_t pamtra_b200_minvert_batched(const double* a, double* ainv, int32_t* status, int32_t n, int32_t count,
+                                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PAMTRA_B200_H */

@@ -1,0 +1,181 @@
+"""ctypes binding of the C ABI in include/pamtra_b200.h.
+
+The shared library is built in-tree (pamtra_b200/_lib/libpamtra_b200.so) by
+:func:`pamtra_b200.build.build`.  There is no fallback: if the library or a
+CUDA device is missing, loading raises.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+from .packing import Settings, Species, SPECIES_DTYPE
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libpamtra_b200.so")
+
+PREC_FP64 = 0
+PREC_3XTF32 = 1
+
+ST_NORM = 0x100
+ST_PSD = 0x200
+ST_MIE = 0x400
+ST_GAS = 0x800
+ST_PIVOT = 0x1000
+ST_NAN = 0x2000
+ST_SIZE = 0x4000
+
+_vp = ctypes.c_void_p
+_i32 = ctypes.c_int32
+
+
+class Columns(ctypes.Structure):
+    """Mirror of ``pamtra_b200_columns``."""
+    _fields_ = [("ncol", _i32), ("max_nlyrs", _i32), ("nhydro", _i32), ("max_nfreq", _i32),
+                ("noutlevels", _i32), ("max_nummu", _i32), ("species_stride", _i32), ("max_present", _i32),
+                ("nummu_mask", _i32), ("species", _vp), ("nlyrs", _vp), ("nummu", _vp), ("nfreq", _vp),
+                ("freqs", _vp), ("hgt_lev", _vp), ("temp_lev", _vp), ("press_lev", _vp), ("relhum_lev", _vp),
+                ("hgt", _vp), ("temp", _vp), ("press", _vp), ("relhum", _vp), ("hydro_q", _vp),
+                ("hydro_n", _vp), ("hydro_reff", _vp), ("groundtemp", _vp), ("obs_height", _vp),
+                ("sfc_refl", _vp)]
+
+
+class Outputs(ctypes.Structure):
+    """Mirror of ``pamtra_b200_outputs``."""
+    _fields_ = [("tb", _vp), ("emissivity", _vp), ("angles_deg", _vp), ("status", _vp), ("kextatmo", _vp),
+                ("kexttot", _vp), ("salbedo", _vp), ("scatter_matrix", _vp), ("num_doubles", _vp)]
+
+
+EXPORTS = ["pamtra_b200_create", "pamtra_b200_destroy", "pamtra_b200_workspace_bytes", "pamtra_b200_reserve",
+           "pamtra_b200_run", "pamtra_b200_run_host", "pamtra_b200_last_launch_count", "pamtra_b200_gas_r98",
+           "pamtra_b200_eps_water_tkc", "pamtra_b200_minvert_batched"]
+
+_lib = None
+
+
+def load():
+    """Load the shared library (raises OSError if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError("pamtra_b200 native library not built: %s (run pamtra_b200.build.build())" % LIB_PATH)
+        l = ctypes.CDLL(LIB_PATH)
+        l.pamtra_b200_create.restype = _i32
+        l.pamtra_b200_create.argtypes = [_i32, ctypes.POINTER(_vp)]
+        l.pamtra_b200_destroy.restype = _i32
+        l.pamtra_b200_destroy.argtypes = [_vp]
+        l.pamtra_b200_workspace_bytes.restype = ctypes.c_size_t
+        l.pamtra_b200_workspace_bytes.argtypes = [ctypes.POINTER(Columns), _i32]
+        l.pamtra_b200_reserve.restype = _i32
+        l.pamtra_b200_reserve.argtypes = [_vp, ctypes.c_size_t]
+        for fn in (l.pamtra_b200_run, l.pamtra_b200_run_host):
+            fn.restype = _i32
+            fn.argtypes = [_vp, ctypes.POINTER(Settings), ctypes.POINTER(Columns), ctypes.POINTER(Outputs), _i32, _vp]
+        l.pamtra_b200_last_launch_count.restype = _i32
+        l.pamtra_b200_last_launch_count.argtypes = [_vp]
+        l.pamtra_b200_gas_r98.restype = _i32
+        l.pamtra_b200_gas_r98.argtypes = [_vp] * 6 + [_i32, _vp]
+        l.pamtra_b200_eps_water_tkc.restype = _i32
+        l.pamtra_b200_eps_water_tkc.argtypes = [_vp] * 4 + [_i32, _vp]
+        l.pamtra_b200_minvert_batched.restype = _i32
+        l.pamtra_b200_minvert_batched.argtypes = [_vp, _vp, _vp, _i32, _i32, _vp]
+        _lib = l
+    return _lib
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+class Engine(object):
+    """A native context on one CUDA device."""
+
+    def __init__(self, device=0):
+        self.lib = load()
+        h = _vp()
+        err = self.lib.pamtra_b200_create(int(device), ctypes.byref(h))
+        if err != 0:
+            raise RuntimeError("pamtra_b200_create failed (%d): no usable CUDA device?" % err)
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.pamtra_b200_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @staticmethod
+    def make_columns(arrs, species, nmu_mask=0, max_present=0, species_stride=0, max_nummu=16):
+        """Columns struct from a dict of arrays (numpy for host runs, torch CUDA
+        tensors for device runs).  ``species`` is always a host structured array."""
+        c = Columns()
+        c.ncol = int(arrs["ncol"])
+        c.max_nlyrs = int(arrs["max_nlyrs"])
+        c.nhydro = int(arrs["nhydro"])
+        c.max_nfreq = int(arrs["max_nfreq"])
+        c.noutlevels = int(arrs["noutlevels"])
+        c.max_nummu = int(max_nummu)
+        c.species_stride = int(species_stride)
+        c.max_present = int(max_present)
+        c.nummu_mask = int(nmu_mask)
+        c.species = species.ctypes.data if len(species) else None
+        for k in ("nlyrs", "nummu", "nfreq", "freqs", "hgt_lev", "temp_lev", "press_lev", "relhum_lev", "hgt",
+                  "temp", "press", "relhum", "hydro_q", "hydro_n", "hydro_reff", "groundtemp", "obs_height",
+                  "sfc_refl"):
+            setattr(c, k, _ptr(arrs.get(k)))
+        return c
+
+    @staticmethod
+    def make_outputs(outs):
+        o = Outputs()
+        for k in ("tb", "emissivity", "angles_deg", "status", "kextatmo", "kexttot", "salbedo", "scatter_matrix",
+                  "num_doubles"):
+            setattr(o, k, _ptr(outs.get(k)))
+        return o
+
+    def run(self, settings, columns, outputs, precision=PREC_FP64, stream=None):
+        """Device-pointer run on ``stream`` (a torch.cuda.Stream or None)."""
+        s = None if stream is None else stream.cuda_stream
+        err = self.lib.pamtra_b200_run(self.handle, ctypes.byref(settings), ctypes.byref(columns),
+                                       ctypes.byref(outputs), int(precision), s)
+        if err != 0:
+            raise RuntimeError("pamtra_b200_run failed with code %d" % err)
+
+    def run_host(self, settings, columns, outputs, precision=PREC_FP64, stream=None):
+        """Host-pointer run: copies in, computes, copies out, synchronises."""
+        s = None if stream is None else stream.cuda_stream
+        err = self.lib.pamtra_b200_run_host(self.handle, ctypes.byref(settings), ctypes.byref(columns),
+                                            ctypes.byref(outputs), int(precision), s)
+        if err != 0:
+            raise RuntimeError("pamtra_b200_run_host failed with code %d" % err)
+
+    def reserve(self, nbytes):
+        if self.lib.pamtra_b200_reserve(self.handle, int(nbytes)) != 0:
+            raise MemoryError("cannot reserve %d bytes of device scratch" % nbytes)
+
+    def workspace_bytes(self, columns, precision=PREC_FP64):
+        return int(self.lib.pamtra_b200_workspace_bytes(ctypes.byref(columns), int(precision)))
+
+    def last_launch_count(self):
+        return int(self.lib.pamtra_b200_last_launch_count(self.handle))
+
+
+_engines = {}
+
+
+def engine(device=0):
+    """Process-wide engine per device."""
+    if device not in _engines:
+        _engines[device] = Engine(device)
+    return _engines[device]

@@ -1,0 +1,630 @@
+// C-ABI implementation: context, scratch arena, launch sequence.
+//
+// One batch = columns x frequencies.  Launch sequence on the caller's stream:
+//   k_atmo      column pre-processing + output levels        (thread/column)
+//   k_gas       Rosenkranz-98 gas absorption                 (thread/layer-frequency)
+//   k_psd       size distributions                           (thread/layer-species)
+//   k_compact   list of hydrometeor-bearing layers           (one block)
+//   k_mie       Mie + species sums -> Legendre coefficients  (warp/layer-frequency, persistent)
+//   k_layer<N>  scatcnv + doubling -> layer R, T, S          (CTA/layer-frequency, persistent)
+//   k_adding<N> adding + radiance + TB                       (CTA/column-frequency, persistent)
+// All work lists live on the device, so the sequence has no host
+// synchronisation and can be captured in a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+#include "mie.cuh"
+#include "prep.cuh"
+#include "rt.cuh"
+#include "work.cuh"
+
+using namespace pb;
+
+namespace {
+
+// Rosenkranz-98 line tables (src/gasabs_module.f90:106-211, 214-333); the
+// reference declares them as default REAL literals.
+const float H_O2_W300[40] = {1.63f, 1.646f, 1.468f, 1.449f, 1.382f, 1.360f, 1.319f, 1.297f, 1.266f, 1.248f,
+                             1.221f, 1.207f, 1.181f, 1.171f, 1.144f, 1.139f, 1.110f, 1.108f, 1.079f, 1.078f,
+                             1.05f,  1.05f,  1.02f,  1.02f,  1.0f,   1.0f,   0.97f,  0.97f,  0.94f,  0.94f,
+                             0.92f,  0.92f,  0.89f,  0.89f,  1.92f,  1.92f,  1.92f,  1.81f,  1.81f,  1.81f};
+const float H_O2_Y300[40] = {-0.0233f, 0.2408f,  -0.3486f, 0.5227f,  -0.5430f, 0.5877f,  -0.3970f, 0.3237f,
+                             -0.1348f, 0.0311f,  0.0725f,  -0.1663f, 0.2832f,  -0.3629f, 0.3970f,  -0.4599f,
+                             0.4695f,  -0.5199f, 0.5187f,  -0.5597f, 0.5903f,  -0.6246f, 0.6656f,  -0.6942f,
+                             0.7086f,  -0.7325f, 0.7348f,  -0.7546f, 0.7702f,  -0.7864f, 0.8083f,  -0.8210f,
+                             0.8439f,  -0.8529f, 0.f,      0.f,      0.f,      0.f,      0.f,      0.f};
+const float H_O2_V[40] = {0.0079f,  -0.0978f, 0.0844f,  -0.1273f, 0.0699f,  -0.0776f, 0.2309f,  -0.2825f,
+                          0.0436f,  -0.0584f, 0.6056f,  -0.6619f, 0.6451f,  -0.6759f, 0.6547f,  -0.6675f,
+                          0.6135f,  -0.6139f, 0.2952f,  -0.2895f, 0.2654f,  -0.2590f, 0.3750f,  -0.3680f,
+                          0.5085f,  -0.5002f, 0.6206f,  -0.6091f, 0.6526f,  -0.6393f, 0.6640f,  -0.6475f,
+                          0.6729f,  -0.6545f, 0.f,      0.f,      0.f,      0.f,      0.f,      0.f};
+const float H_O2_F[40] = {118.7503f, 56.2648f, 62.4863f, 58.4466f, 60.3061f, 59.5910f, 59.1642f, 60.4348f,
+                          58.3239f,  61.1506f, 57.6125f, 61.8002f, 56.9682f, 62.4112f, 56.3634f, 62.9980f,
+                          55.7838f,  63.5685f, 55.2214f, 64.1278f, 54.6712f, 64.6789f, 54.1300f, 65.2241f,
+                          53.5957f,  65.7648f, 53.0669f, 66.3021f, 52.5424f, 66.8368f, 52.0214f, 67.3696f,
+                          51.5034f,  67.9009f, 368.4984f, 424.7631f, 487.2494f, 715.3932f, 773.8397f, 834.1453f};
+const float H_O2_S300[40] = {0.2936E-14f, 0.8079E-15f, 0.2480E-14f, 0.2228E-14f, 0.3351E-14f, 0.3292E-14f,
+                             0.3721E-14f, 0.3891E-14f, 0.3640E-14f, 0.4005E-14f, 0.3227E-14f, 0.3715E-14f,
+                             0.2627E-14f, 0.3156E-14f, 0.1982E-14f, 0.2477E-14f, 0.1391E-14f, 0.1808E-14f,
+                             0.9124E-15f, 0.1230E-14f, 0.5603E-15f, 0.7842E-15f, 0.3228E-15f, 0.4689E-15f,
+                             0.1748E-15f, 0.2632E-15f, 0.8898E-16f, 0.1389E-15f, 0.4264E-16f, 0.6899E-16f,
+                             0.1924E-16f, 0.3229E-16f, 0.8191E-17f, 0.1423E-16f, 0.6460E-15f, 0.7047E-14f,
+                             0.3011E-14f, 0.1826E-14f, 0.1152E-13f, 0.3971E-14f};
+const float H_O2_BE[40] = {0.009f, 0.015f, 0.083f, 0.084f, 0.212f, 0.212f, 0.391f, 0.391f, 0.626f, 0.626f,
+                           0.915f, 0.915f, 1.26f,  1.26f,  1.66f,  1.665f, 2.119f, 2.115f, 2.624f, 2.625f,
+                           3.194f, 3.194f, 3.814f, 3.814f, 4.484f, 4.484f, 5.224f, 5.224f, 6.004f, 6.004f,
+                           6.844f, 6.844f, 7.744f, 7.744f, 0.048f, 0.044f, 0.049f, 0.145f, 0.141f, 0.145f};
+const float H_H2O_FL[15] = {22.2351f, 183.3101f, 321.2256f, 325.1529f, 380.1974f, 439.1508f, 443.0183f, 448.0011f,
+                            470.8890f, 474.6891f, 488.4911f, 556.9360f, 620.7008f, 752.0332f, 916.1712f};
+const float H_H2O_S1[15] = {0.1310E-13f, 0.2273E-11f, 0.8036E-13f, 0.2694E-11f, 0.2438E-10f,
+                            0.2179E-11f, 0.4624E-12f, 0.2562E-10f, 0.8369E-12f, 0.3263E-11f,
+                            0.6659E-12f, 0.1531E-08f, 0.1707E-10f, 0.1011E-08f, 0.4227E-10f};
+const float H_H2O_B2[15] = {2.144f, .668f, 6.179f, 1.541f, 1.048f, 3.595f, 5.048f, 1.405f,
+                            3.597f, 2.379f, 2.852f, .159f,  2.391f, .396f,  1.441f};
+const float H_H2O_W3[15] = {0.002656f, 0.00281f, 0.0023f,  0.00278f, 0.00287f, 0.0021f,  0.00186f, 0.00263f,
+                            0.00215f,  0.00236f, 0.0026f,  0.00321f, 0.00244f, 0.00306f, 0.00267f};
+const float H_H2O_X[15] = {0.69f, 0.64f, 0.67f, 0.68f, 0.54f, 0.63f, 0.60f, 0.66f,
+                           0.66f, 0.65f, 0.69f, 0.69f, 0.71f, 0.68f, 0.70f};
+const float H_H2O_WS[15] = {0.0127488f, 0.01491f, 0.0108f,  0.0135f,  0.01541f, 0.0090f,  0.00788f, 0.01275f,
+                            0.00983f,   0.01095f, 0.01313f, 0.01320f, 0.01140f, 0.01253f, 0.01275f};
+const float H_H2O_XS[15] = {0.61f, 0.85f, 0.54f, 0.74f, 0.89f, 0.52f, 0.50f, 0.67f,
+                            0.65f, 0.64f, 0.72f, 1.0f,  0.68f, 0.84f, 0.78f};
+
+constexpr int GQ_MAX = 256;
+
+// Gauss-Legendre nodes/weights for every n = 1..GQ_MAX (src/scat_utilities.f90:1-44),
+// packed at offset n*(n-1)/2.  Block per n, thread per node pair.
+__global__ void k_gauss_table(double* gx, double* gw) {
+  const int n = blockIdx.x + 1;
+  const int jj = threadIdx.x + 1;
+  if (jj > (n + 1) / 2) return;
+  double* xa = gx + (size_t)n * (n - 1) / 2;
+  double* wt = gw + (size_t)n * (n - 1) / 2;
+  double x = cos(PI * (jj - 0.25) / (n + 0.5));
+  int i = 0;
+  double pl, pl1, pl2, dpl, xp;
+  do {
+    pl1 = 1;
+    pl = x;
+    for (int l = 2; l <= n; l++) {
+      pl2 = pl1;
+      pl1 = pl;
+      pl = ((2 * l - 1) * x * pl1 - (l - 1) * pl2) / l;
+    }
+    dpl = n * (x * pl - pl1) / (x * x - 1);
+    xp = x;
+    x = xp - pl / dpl;
+    i = i + 1;
+  } while (fabs(x - xp) > 3.0e-13 && i < 10);
+  xa[jj - 1] = -x;
+  xa[n - jj] = x;
+  double ww = 2.0 / ((1.0 - x * x) * dpl * dpl);
+  wt[jj - 1] = ww;
+  wt[n - jj] = ww;
+}
+
+// Lobatto nodes/weights for N = 8, 16, 32 (src/rt_utilities.f90:165-203).
+__global__ void k_lobatto_table(double* mu, double* w) {
+  const int which = blockIdx.x;  // 0: 8, 1: 16, 2: 32
+  const int num = 8 << which;
+  const int off = lob_off(num);
+  const int jj = threadIdx.x + 1;
+  if (jj > num) return;
+  if (jj == num) {
+    mu[off + num - 1] = 1.0;
+    w[off + num - 1] = 2.0 / ((2 * num) * (2 * num - 1));
+    return;
+  }
+  const int n = 2 * num, n1 = n - 1;
+  const double ci = 0.50;
+  double x = sin(F(3.141592654f) * (jj - ci) / (n - .5));
+  int i = 0;
+  double pl, pl1, pl2, dpl, d2pl, xp;
+  do {
+    pl1 = 1;
+    pl = x;
+    for (int l = 2; l <= n1; l++) {
+      pl2 = pl1;
+      pl1 = pl;
+      pl = ((2 * l - 1) * x * pl1 - (l - 1) * pl2) / l;
+    }
+    dpl = n1 * (x * pl - pl1) / (x * x - 1);
+    d2pl = (2.0 * x * dpl - n1 * (n1 + 1) * pl) / (1.0 - x * x);
+    xp = x;
+    x = xp - dpl / d2pl;
+    i = i + 1;
+  } while (fabs(x - xp) > 3.0e-14 && i < 10);
+  mu[off + jj - 1] = x;
+  w[off + jj - 1] = 2.0 / (n * n1 * pl * pl);
+}
+
+__global__ void k_fill_d(double* p, double v, size_t n) {
+  size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+// angles in degrees (src/run_rt.f90:196-197) for N = max_nummu
+__global__ void k_angles(double* out, const double* lob_mu, int N) {
+  int jj = threadIdx.x;
+  if (jj >= N) return;
+  const double* mu = lob_mu + lob_off(N);
+  out[jj] = 180 - (180. * acos(mu[N - 1 - jj]) / PI);
+  out[N + jj] = (180. * acos(mu[jj]) / PI);
+}
+
+// save_ssp-style per-(column, frequency, layer) outputs
+__global__ void k_ssp_out(Batch b, Work w, pamtra_b200_outputs out) {
+  const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
+  if (idx >= (size_t)b.ncol * Fm * Lm) return;
+  const int z = idx % Lm, f = (idx / Lm) % Fm, c = idx / ((size_t)Lm * Fm);
+  const int p = (z < b.nlyrs[c]) ? w.pres_idx[(size_t)c * Lm + z] : -1;
+  const size_t item = (size_t)p * Fm + f;
+  if (out.kexttot) out.kexttot[idx] = (p >= 0) ? w.m_kext[item] : 0.0;
+  if (out.salbedo) out.salbedo[idx] = (p >= 0) ? w.m_salb[item] : 0.0;
+  if (out.num_doubles) out.num_doubles[idx] = (p >= 0) ? w.lay_nd[item] : -1;
+}
+
+__global__ void k_status_out(Work w, int32_t* out, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = w.status[i];
+}
+
+struct Plan {
+  size_t total;
+  size_t o_hgt_lev, o_temp_lev, o_temp, o_press, o_rho_vap, o_q_hum, o_gtemp, o_outlev, o_kgas;
+  size_t o_slot_st, o_slot_nb, o_bd, o_bdd, o_bnd, o_brho, o_bmass;
+  size_t o_pres_idx, o_plist, o_counters, o_mkext, o_msalb, o_mnleg, o_mlegen, o_lay, o_laynd, o_status, o_colst;
+  size_t o_species;
+  int pmax;
+  int max_nbin;
+  int maxN;
+  size_t lay_stride;
+};
+
+size_t lay_stride_for(int N) {
+  int n = 2 * N;
+  size_t s = 2 * (size_t)n * (n + 2) + 2 * n;
+  return (s + 1) & ~(size_t)1;  // keep 16-byte alignment of each item
+}
+
+Plan make_plan(const pamtra_b200_columns* c, int default_nummu) {
+  Plan p{};
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = (off + 255) & ~(size_t)255;
+    off = o + bytes;
+    return o;
+  };
+  const size_t C = c->ncol, Lm = c->max_nlyrs, H = c->nhydro, Fm = c->max_nfreq;
+  int mb = 1;
+  const size_t nsp = c->species_stride ? C * H : H;
+  for (size_t i = 0; i < nsp; i++) mb = std::max(mb, c->species[i].dist == PAMTRA_B200_DIST_MONO ? 2 : c->species[i].nbin);
+  p.max_nbin = mb;
+  int mask = c->nummu_mask ? c->nummu_mask : (default_nummu == 8 ? 1 : default_nummu == 16 ? 2 : 4);
+  p.maxN = (mask & 4) ? 32 : (mask & 2) ? 16 : 8;
+  p.pmax = c->max_present > 0 ? c->max_present : (int)(C * Lm);
+  p.lay_stride = lay_stride_for(p.maxN);
+  const size_t S = C * Lm * H;
+  p.o_hgt_lev = take(C * (Lm + 1) * 8);
+  p.o_temp_lev = take(C * (Lm + 1) * 8);
+  p.o_temp = take(C * Lm * 8);
+  p.o_press = take(C * Lm * 8);
+  p.o_rho_vap = take(C * Lm * 8);
+  p.o_q_hum = take(C * Lm * 8);
+  p.o_gtemp = take(C * 8);
+  p.o_outlev = take(C * std::max(1, c->noutlevels) * 4);
+  p.o_kgas = take(C * Fm * Lm * 8);
+  p.o_slot_st = take(std::max<size_t>(S, 1));
+  p.o_slot_nb = take(std::max<size_t>(S, 1) * 4);
+  p.o_bd = take(std::max<size_t>(S, 1) * mb * 8);
+  p.o_bdd = take(std::max<size_t>(S, 1) * mb * 8);
+  p.o_bnd = take(std::max<size_t>(S, 1) * mb * 8);
+  p.o_brho = take(std::max<size_t>(S, 1) * mb * 8);
+  p.o_bmass = take(std::max<size_t>(S, 1) * mb * 8);
+  p.o_pres_idx = take(C * Lm * 4);
+  p.o_plist = take((size_t)std::max(1, p.pmax) * 4);
+  p.o_counters = take(16 * 4);
+  const size_t items = (size_t)std::max(1, p.pmax) * Fm;
+  p.o_mkext = take(items * 8);
+  p.o_msalb = take(items * 8);
+  p.o_mnleg = take(items * 4);
+  p.o_mlegen = take(items * 3 * MAXNLEG * 8);
+  p.o_lay = take(items * p.lay_stride * 8);
+  p.o_laynd = take(items * 4);
+  p.o_status = take(C * Fm * 4);
+  p.o_colst = take(C * 4);
+  p.o_species = take(std::max<size_t>(nsp, 1) * sizeof(pamtra_b200_species));
+  p.total = take(0) + 256;
+  return p;
+}
+
+int occupancy_blocks(const void* func, int threads, size_t smem, int sms) {
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, func, threads, smem) != cudaSuccess || nb < 1) nb = 1;
+  return nb * sms;
+}
+
+}  // namespace
+
+namespace {
+// ---------------------------------------------------------------- single stages
+__global__ void k_gas_elem(const double* f, const double* T, const double* rv, const double* p, double* k,
+                                  int32_t* st, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int s = gas_r98(f[i], T[i], rv[i], p[i], &k[i]);
+  if (st) st[i] = s;
+}
+
+template <int n>
+__global__ void k_minvert(const double* a, double* ainv, int32_t* status, int count) {
+  constexpr int RS = (n >= 64) ? 2 : 1;
+  constexpr int LD = TeamCfg<n, RS>::LD, R = TeamCfg<n, RS>::R;
+  __shared__ double M[n * LD];
+  __shared__ double f[n], redv[8];
+  __shared__ int piv[n], redi[8 + n];
+  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R;
+  for (int m = blockIdx.x; m < count; m += gridDim.x) {
+    const double* src = a + (size_t)m * n * n;
+    for (int ii = 0; ii < R; ii++) M[j * LD + r0 + ii] = src[(size_t)j * n + r0 + ii];
+    __syncthreads();
+    int s = ginv<n, RS>(M, f, piv, redv, redi);
+    double* dst = ainv + (size_t)m * n * n;
+    for (int ii = 0; ii < R; ii++) dst[(size_t)j * n + r0 + ii] = M[j * LD + r0 + ii];
+    if (status && t == 0) status[m] = s ? (PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT) : 0;
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+struct pamtra_b200_ctx {
+  int device = 0;
+  int sm_count = 0;
+  char* arena = nullptr;
+  size_t arena_bytes = 0;
+  double* gq_x = nullptr;
+  double* gq_w = nullptr;
+  double* lob_mu = nullptr;
+  double* lob_w = nullptr;
+  pamtra_b200_species* h_species = nullptr;  // pinned staging
+  size_t h_species_cap = 0;
+  int last_launches = 0;
+  char* stage = nullptr;  // device staging for run_host
+  size_t stage_bytes = 0;
+};
+
+static int set_smem_attrs() {
+  static std::once_flag once;
+  static int rc = 0;
+  std::call_once(once, [] {
+    auto set = [](const void* f, size_t bytes) {
+      if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) rc = 1;
+    };
+    set((const void*)k_mie, MIE_WARPS * sizeof(MieSmem));
+    set((const void*)k_layer<8>, sizeof(LayerSmem<8>));
+    set((const void*)k_layer<16>, sizeof(LayerSmem<16>));
+    set((const void*)k_layer<32>, sizeof(LayerSmem<32>));
+    set((const void*)k_adding<8>, sizeof(AddSmem<8>));
+    set((const void*)k_adding<16>, sizeof(AddSmem<16>));
+  });
+  return rc;
+}
+
+extern "C" {
+
+int32_t pamtra_b200_create(int32_t device, pamtra_b200_ctx** out) {
+  if (!out) return PAMTRA_B200_FATAL;
+  if (cudaSetDevice(device) != cudaSuccess) return PAMTRA_B200_FATAL;
+  pamtra_b200_ctx* ctx = new pamtra_b200_ctx();
+  ctx->device = device;
+  cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+  if (set_smem_attrs()) { delete ctx; return PAMTRA_B200_FATAL; }
+  const size_t gq_n = (size_t)GQ_MAX * (GQ_MAX + 1) / 2;
+  if (cudaMalloc(&ctx->gq_x, gq_n * 8) || cudaMalloc(&ctx->gq_w, gq_n * 8) || cudaMalloc(&ctx->lob_mu, 56 * 8) ||
+      cudaMalloc(&ctx->lob_w, 56 * 8)) {
+    delete ctx;
+    return PAMTRA_B200_FATAL;
+  }
+  k_gauss_table<<<GQ_MAX, 128>>>(ctx->gq_x, ctx->gq_w);
+  k_lobatto_table<<<3, 32>>>(ctx->lob_mu, ctx->lob_w);
+  cudaMemcpyToSymbol(c_o2_w300, H_O2_W300, sizeof(H_O2_W300));
+  cudaMemcpyToSymbol(c_o2_y300, H_O2_Y300, sizeof(H_O2_Y300));
+  cudaMemcpyToSymbol(c_o2_v, H_O2_V, sizeof(H_O2_V));
+  cudaMemcpyToSymbol(c_o2_f, H_O2_F, sizeof(H_O2_F));
+  cudaMemcpyToSymbol(c_o2_s300, H_O2_S300, sizeof(H_O2_S300));
+  cudaMemcpyToSymbol(c_o2_be, H_O2_BE, sizeof(H_O2_BE));
+  cudaMemcpyToSymbol(c_h2o_fl, H_H2O_FL, sizeof(H_H2O_FL));
+  cudaMemcpyToSymbol(c_h2o_s1, H_H2O_S1, sizeof(H_H2O_S1));
+  cudaMemcpyToSymbol(c_h2o_b2, H_H2O_B2, sizeof(H_H2O_B2));
+  cudaMemcpyToSymbol(c_h2o_w3, H_H2O_W3, sizeof(H_H2O_W3));
+  cudaMemcpyToSymbol(c_h2o_x, H_H2O_X, sizeof(H_H2O_X));
+  cudaMemcpyToSymbol(c_h2o_ws, H_H2O_WS, sizeof(H_H2O_WS));
+  cudaMemcpyToSymbol(c_h2o_xs, H_H2O_XS, sizeof(H_H2O_XS));
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    delete ctx;
+    return PAMTRA_B200_FATAL;
+  }
+  *out = ctx;
+  return PAMTRA_B200_OK;
+}
+
+int32_t pamtra_b200_destroy(pamtra_b200_ctx* ctx) {
+  if (!ctx) return PAMTRA_B200_OK;
+  cudaSetDevice(ctx->device);
+  cudaFree(ctx->arena);
+  cudaFree(ctx->gq_x);
+  cudaFree(ctx->gq_w);
+  cudaFree(ctx->lob_mu);
+  cudaFree(ctx->lob_w);
+  cudaFree(ctx->stage);
+  if (ctx->h_species) cudaFreeHost(ctx->h_species);
+  delete ctx;
+  return PAMTRA_B200_OK;
+}
+
+size_t pamtra_b200_workspace_bytes(const pamtra_b200_columns* cols, int32_t precision) {
+  (void)precision;
+  if (!cols || !cols->species) return 0;
+  return make_plan(cols, 16).total;
+}
+
+int32_t pamtra_b200_reserve(pamtra_b200_ctx* ctx, size_t bytes) {
+  if (!ctx) return PAMTRA_B200_FATAL;
+  if (bytes <= ctx->arena_bytes) return PAMTRA_B200_OK;
+  cudaSetDevice(ctx->device);
+  cudaFree(ctx->arena);
+  ctx->arena = nullptr;
+  ctx->arena_bytes = 0;
+  if (cudaMalloc(&ctx->arena, bytes) != cudaSuccess) return PAMTRA_B200_FATAL;
+  ctx->arena_bytes = bytes;
+  return PAMTRA_B200_OK;
+}
+
+int32_t pamtra_b200_last_launch_count(const pamtra_b200_ctx* ctx) { return ctx ? ctx->last_launches : 0; }
+
+int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, const pamtra_b200_columns* cols,
+                        const pamtra_b200_outputs* out, int32_t precision, void* stream_) {
+  if (!ctx || !st || !cols || !out || !out->tb) return PAMTRA_B200_FATAL;
+  if (precision != PAMTRA_B200_PREC_FP64) return PAMTRA_B200_FATAL;
+  if (cols->ncol < 1 || cols->max_nlyrs < 2 || cols->max_nfreq < 1 || cols->noutlevels < 1 || cols->nhydro < 0)
+    return PAMTRA_B200_FATAL;
+  if (cols->nhydro > 0 && !cols->species) return PAMTRA_B200_FATAL;
+  if (!(st->nummu == 8 || st->nummu == 16 || st->nummu == 32)) return PAMTRA_B200_FATAL;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  cudaSetDevice(ctx->device);
+  pamtra_b200_species dummy{};
+  pamtra_b200_columns cc = *cols;
+  if (cc.nhydro == 0) { cc.species = &dummy; cc.species_stride = 0; }
+  Plan pl = make_plan(&cc, st->nummu);
+  if (pl.max_nbin > MAXBIN) return PAMTRA_B200_FATAL;
+  if (pl.total > ctx->arena_bytes) {
+    cudaStreamSynchronize(stream);
+    if (pamtra_b200_reserve(ctx, pl.total + pl.total / 8)) return PAMTRA_B200_FATAL;
+  }
+  const int mask = cc.nummu_mask ? cc.nummu_mask : (st->nummu == 8 ? 1 : st->nummu == 16 ? 2 : 4);
+  if (pl.maxN > cc.max_nummu) return PAMTRA_B200_FATAL;
+  if (mask & 4) return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;  // N=32 adding not available in this build
+  char* A = ctx->arena;
+  // species table -> device (pinned staging so the copy is stream ordered)
+  const size_t nsp = cc.species_stride ? (size_t)cc.ncol * cc.nhydro : (size_t)std::max(cc.nhydro, 1);
+  if (nsp > ctx->h_species_cap) {
+    cudaStreamSynchronize(stream);
+    if (ctx->h_species) cudaFreeHost(ctx->h_species);
+    if (cudaMallocHost(&ctx->h_species, nsp * sizeof(pamtra_b200_species)) != cudaSuccess) return PAMTRA_B200_FATAL;
+    ctx->h_species_cap = nsp;
+  } else {
+    cudaStreamSynchronize(stream);  // staging buffer may still be read by a previous copy
+  }
+  std::memcpy(ctx->h_species, cc.species, nsp * sizeof(pamtra_b200_species));
+  pamtra_b200_species* d_species = (pamtra_b200_species*)(A + pl.o_species);
+  cudaMemcpyAsync(d_species, ctx->h_species, nsp * sizeof(pamtra_b200_species), cudaMemcpyHostToDevice, stream);
+
+  Batch b{};
+  b.ncol = cc.ncol; b.max_nlyrs = cc.max_nlyrs; b.nhydro = cc.nhydro; b.max_nfreq = cc.max_nfreq;
+  b.noutlevels = cc.noutlevels; b.max_nummu = cc.max_nummu; b.max_nbin = pl.max_nbin;
+  b.species_stride = cc.species_stride; b.default_nummu = st->nummu; b.species = d_species;
+  b.nlyrs = cc.nlyrs; b.nummu = cc.nummu; b.nfreq = cc.nfreq; b.freqs = cc.freqs; b.freq_per_col = cc.nfreq != nullptr;
+  b.hgt_lev = cc.hgt_lev; b.temp_lev = cc.temp_lev; b.press_lev = cc.press_lev; b.relhum_lev = cc.relhum_lev;
+  b.hgt = cc.hgt; b.temp = cc.temp; b.press = cc.press; b.relhum = cc.relhum;
+  b.hydro_q = cc.hydro_q; b.hydro_n = cc.hydro_n; b.hydro_reff = cc.hydro_reff;
+  b.groundtemp = cc.groundtemp; b.obs_height = cc.obs_height; b.sfc_refl = cc.sfc_refl;
+
+  Work w{};
+  w.hgt_lev = (double*)(A + pl.o_hgt_lev); w.temp_lev = (double*)(A + pl.o_temp_lev);
+  w.temp = (double*)(A + pl.o_temp); w.press = (double*)(A + pl.o_press);
+  w.rho_vap = (double*)(A + pl.o_rho_vap); w.q_hum = (double*)(A + pl.o_q_hum);
+  w.gtemp = (double*)(A + pl.o_gtemp); w.outlev = (int*)(A + pl.o_outlev); w.kgas = (double*)(A + pl.o_kgas);
+  w.slot_st = (int8_t*)(A + pl.o_slot_st); w.slot_nb = (int*)(A + pl.o_slot_nb);
+  w.b_d = (double*)(A + pl.o_bd); w.b_dd = (double*)(A + pl.o_bdd); w.b_nd = (double*)(A + pl.o_bnd);
+  w.b_rho = (double*)(A + pl.o_brho); w.b_mass = (double*)(A + pl.o_bmass);
+  w.pres_idx = (int*)(A + pl.o_pres_idx); w.plist = (int*)(A + pl.o_plist); w.pmax = pl.pmax;
+  w.counters = (int*)(A + pl.o_counters);
+  w.m_kext = (double*)(A + pl.o_mkext); w.m_salb = (double*)(A + pl.o_msalb); w.m_nleg = (int*)(A + pl.o_mnleg);
+  w.m_legen = (double*)(A + pl.o_mlegen);
+  w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
+  w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
+  w.gq_x = ctx->gq_x; w.gq_w = ctx->gq_w; w.gq_max = GQ_MAX; w.lob_mu = ctx->lob_mu; w.lob_w = ctx->lob_w;
+
+  int launches = 0;
+  const size_t C = cc.ncol, Lm = cc.max_nlyrs, Fm = cc.max_nfreq, H = cc.nhydro;
+  cudaMemsetAsync(w.counters, 0, 16 * 4, stream);
+  cudaMemsetAsync(w.status, 0, C * Fm * 4, stream);
+  cudaMemsetAsync(w.col_status, 0, C * 4, stream);
+  const size_t ntb = C * cc.noutlevels * 2 * cc.max_nummu * Fm * 2;
+  k_fill_d<<<(unsigned)((ntb + 255) / 256), 256, 0, stream>>>(out->tb, -9999.0, ntb); launches++;
+  k_atmo<<<(unsigned)((C + 127) / 128), 128, 0, stream>>>(b, w); launches++;
+  const size_t ngas = C * Fm * Lm;
+  k_gas<<<(unsigned)((ngas + 255) / 256), 256, 0, stream>>>(b, w, st->lgas_extinction); launches++;
+  if (H > 0) {
+    const size_t ns = C * Lm * H;
+    k_psd<<<(unsigned)((ns + 127) / 128), 128, 0, stream>>>(b, w, *st); launches++;
+  } else {
+    cudaMemsetAsync(w.slot_st, 0, 1, stream);
+  }
+  k_compact<<<1, 1024, 0, stream>>>(b, w); launches++;
+  const int sms = ctx->sm_count;
+  if (H > 0) {
+    const size_t sm_mie = MIE_WARPS * sizeof(MieSmem);
+    int g = occupancy_blocks((const void*)k_mie, 32 * MIE_WARPS, sm_mie, sms);
+    k_mie<<<g, 32 * MIE_WARPS, sm_mie, stream>>>(b, w, *st); launches++;
+  }
+  double* ssp = out->scatter_matrix;
+  if (mask & 1) {
+    int g = occupancy_blocks((const void*)k_layer<8>, RTCfg<8>::T, sizeof(LayerSmem<8>), sms);
+    if (H > 0) { k_layer<8><<<g, RTCfg<8>::T, sizeof(LayerSmem<8>), stream>>>(b, w, *st, ssp); launches++; }
+    g = occupancy_blocks((const void*)k_adding<8>, RTCfg<8>::T, sizeof(AddSmem<8>), sms);
+    k_adding<8><<<g, RTCfg<8>::T, sizeof(AddSmem<8>), stream>>>(b, w, *st, *out); launches++;
+  }
+  if (mask & 2) {
+    int g = occupancy_blocks((const void*)k_layer<16>, RTCfg<16>::T, sizeof(LayerSmem<16>), sms);
+    if (H > 0) { k_layer<16><<<g, RTCfg<16>::T, sizeof(LayerSmem<16>), stream>>>(b, w, *st, ssp); launches++; }
+    g = occupancy_blocks((const void*)k_adding<16>, RTCfg<16>::T, sizeof(AddSmem<16>), sms);
+    k_adding<16><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out); launches++;
+  }
+  if (out->angles_deg) { k_angles<<<1, 32, 0, stream>>>(out->angles_deg, ctx->lob_mu, cc.max_nummu); launches++; }
+  if (out->kexttot || out->salbedo || out->num_doubles) {
+    k_ssp_out<<<(unsigned)((ngas + 255) / 256), 256, 0, stream>>>(b, w, *out); launches++;
+  }
+  if (out->kextatmo) cudaMemcpyAsync(out->kextatmo, w.kgas, ngas * 8, cudaMemcpyDeviceToDevice, stream);
+  if (out->status) {
+    k_status_out<<<(unsigned)((C * Fm + 255) / 256), 256, 0, stream>>>(w, out->status, (int)(C * Fm)); launches++;
+  }
+  ctx->last_launches = launches;
+  return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
+}
+
+int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, const pamtra_b200_columns* hc,
+                             const pamtra_b200_outputs* ho, int32_t precision, void* stream_) {
+  if (!ctx || !st || !hc || !ho || !ho->tb) return PAMTRA_B200_FATAL;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  cudaSetDevice(ctx->device);
+  const size_t C = hc->ncol, Lm = hc->max_nlyrs, Fm = hc->max_nfreq, H = hc->nhydro, NO = hc->noutlevels;
+  const size_t NA = 2 * (size_t)hc->max_nummu;
+  struct Seg { const void* h; size_t bytes; size_t off; };
+  std::vector<Seg> in;
+  size_t off = 0;
+  auto add = [&](const void* h, size_t bytes) -> size_t {
+    size_t o = (off + 255) & ~(size_t)255;
+    off = o + bytes;
+    if (h) in.push_back({h, bytes, o});
+    return o;
+  };
+  const size_t nfq = hc->nfreq ? C * Fm : Fm;
+  size_t o_nly = add(hc->nlyrs, C * 4), o_nmu = add(hc->nummu, hc->nummu ? C * 4 : 0);
+  size_t o_nfr = add(hc->nfreq, hc->nfreq ? C * 4 : 0), o_frq = add(hc->freqs, nfq * 8);
+  size_t o_hl = add(hc->hgt_lev, C * (Lm + 1) * 8), o_tl = add(hc->temp_lev, C * (Lm + 1) * 8);
+  size_t o_pl = add(hc->press_lev, C * (Lm + 1) * 8), o_rl = add(hc->relhum_lev, C * (Lm + 1) * 8);
+  size_t o_h = add(hc->hgt, C * Lm * 8), o_t = add(hc->temp, C * Lm * 8), o_p = add(hc->press, C * Lm * 8);
+  size_t o_r = add(hc->relhum, C * Lm * 8);
+  size_t o_q = add(hc->hydro_q, C * Lm * H * 8), o_n = add(hc->hydro_n, C * Lm * H * 8);
+  size_t o_re = add(hc->hydro_reff, C * Lm * H * 8);
+  size_t o_g = add(hc->groundtemp, C * 8), o_ob = add(hc->obs_height, C * NO * 8), o_sr = add(hc->sfc_refl, C);
+  size_t o_tb = add(nullptr, C * NO * NA * Fm * 2 * 8);
+  size_t o_em = add(nullptr, ho->emissivity ? C * 2 * Fm * hc->max_nummu * 8 : 0);
+  size_t o_an = add(nullptr, ho->angles_deg ? NA * 8 : 0);
+  size_t o_st = add(nullptr, ho->status ? C * Fm * 4 : 0);
+  size_t o_ka = add(nullptr, ho->kextatmo ? C * Fm * Lm * 8 : 0);
+  size_t o_kt = add(nullptr, ho->kexttot ? C * Fm * Lm * 8 : 0);
+  size_t o_sa = add(nullptr, ho->salbedo ? C * Fm * Lm * 8 : 0);
+  size_t o_sc = add(nullptr, ho->scatter_matrix ? C * Fm * Lm * 4 * NA * NA * 8 : 0);
+  size_t o_nd = add(nullptr, ho->num_doubles ? C * Fm * Lm * 4 : 0);
+  if (off > ctx->stage_bytes) {
+    cudaStreamSynchronize(stream);
+    cudaFree(ctx->stage);
+    ctx->stage = nullptr;
+    ctx->stage_bytes = 0;
+    if (cudaMalloc(&ctx->stage, off + off / 8) != cudaSuccess) return PAMTRA_B200_FATAL;
+    ctx->stage_bytes = off + off / 8;
+  }
+  char* D = ctx->stage;
+  for (auto& s : in) cudaMemcpyAsync(D + s.off, s.h, s.bytes, cudaMemcpyHostToDevice, stream);
+  pamtra_b200_columns dc = *hc;
+  auto dp = [&](const void* h, size_t o) -> const void* { return h ? (const void*)(D + o) : nullptr; };
+  dc.nlyrs = (const int32_t*)dp(hc->nlyrs, o_nly);
+  dc.nummu = (const int32_t*)dp(hc->nummu, o_nmu);
+  dc.nfreq = (const int32_t*)dp(hc->nfreq, o_nfr);
+  dc.freqs = (const double*)dp(hc->freqs, o_frq);
+  dc.hgt_lev = (const double*)dp(hc->hgt_lev, o_hl);
+  dc.temp_lev = (const double*)dp(hc->temp_lev, o_tl);
+  dc.press_lev = (const double*)dp(hc->press_lev, o_pl);
+  dc.relhum_lev = (const double*)dp(hc->relhum_lev, o_rl);
+  dc.hgt = (const double*)dp(hc->hgt, o_h);
+  dc.temp = (const double*)dp(hc->temp, o_t);
+  dc.press = (const double*)dp(hc->press, o_p);
+  dc.relhum = (const double*)dp(hc->relhum, o_r);
+  dc.hydro_q = (const double*)dp(hc->hydro_q, o_q);
+  dc.hydro_n = (const double*)dp(hc->hydro_n, o_n);
+  dc.hydro_reff = (const double*)dp(hc->hydro_reff, o_re);
+  dc.groundtemp = (const double*)dp(hc->groundtemp, o_g);
+  dc.obs_height = (const double*)dp(hc->obs_height, o_ob);
+  dc.sfc_refl = (const int8_t*)dp(hc->sfc_refl, o_sr);
+  pamtra_b200_outputs dout{};
+  dout.tb = (double*)(D + o_tb);
+  dout.emissivity = ho->emissivity ? (double*)(D + o_em) : nullptr;
+  dout.angles_deg = ho->angles_deg ? (double*)(D + o_an) : nullptr;
+  dout.status = ho->status ? (int32_t*)(D + o_st) : nullptr;
+  dout.kextatmo = ho->kextatmo ? (double*)(D + o_ka) : nullptr;
+  dout.kexttot = ho->kexttot ? (double*)(D + o_kt) : nullptr;
+  dout.salbedo = ho->salbedo ? (double*)(D + o_sa) : nullptr;
+  dout.scatter_matrix = ho->scatter_matrix ? (double*)(D + o_sc) : nullptr;
+  dout.num_doubles = ho->num_doubles ? (int32_t*)(D + o_nd) : nullptr;
+  if (dout.scatter_matrix) cudaMemsetAsync(dout.scatter_matrix, 0, C * Fm * Lm * 4 * NA * NA * 8, stream);
+  int32_t rc = pamtra_b200_run(ctx, st, &dc, &dout, precision, stream);
+  if (rc != PAMTRA_B200_OK) return rc;
+  cudaMemcpyAsync(ho->tb, dout.tb, C * NO * NA * Fm * 2 * 8, cudaMemcpyDeviceToHost, stream);
+  if (ho->emissivity) cudaMemcpyAsync(ho->emissivity, dout.emissivity, C * 2 * Fm * hc->max_nummu * 8, cudaMemcpyDeviceToHost, stream);
+  if (ho->angles_deg) cudaMemcpyAsync(ho->angles_deg, dout.angles_deg, NA * 8, cudaMemcpyDeviceToHost, stream);
+  if (ho->status) cudaMemcpyAsync(ho->status, dout.status, C * Fm * 4, cudaMemcpyDeviceToHost, stream);
+  if (ho->kextatmo) cudaMemcpyAsync(ho->kextatmo, dout.kextatmo, C * Fm * Lm * 8, cudaMemcpyDeviceToHost, stream);
+  if (ho->kexttot) cudaMemcpyAsync(ho->kexttot, dout.kexttot, C * Fm * Lm * 8, cudaMemcpyDeviceToHost, stream);
+  if (ho->salbedo) cudaMemcpyAsync(ho->salbedo, dout.salbedo, C * Fm * Lm * 8, cudaMemcpyDeviceToHost, stream);
+  if (ho->scatter_matrix)
+    cudaMemcpyAsync(ho->scatter_matrix, dout.scatter_matrix, C * Fm * Lm * 4 * NA * NA * 8, cudaMemcpyDeviceToHost, stream);
+  if (ho->num_doubles) cudaMemcpyAsync(ho->num_doubles, dout.num_doubles, C * Fm * Lm * 4, cudaMemcpyDeviceToHost, stream);
+  if (cudaStreamSynchronize(stream) != cudaSuccess) return PAMTRA_B200_FATAL;
+  return PAMTRA_B200_OK;
+}
+
+int32_t pamtra_b200_gas_r98(const double* freq, const double* temp, const double* rho_vap, const double* press,
+                            double* kext, int32_t* status, int32_t n, void* stream) {
+  if (n <= 0) return PAMTRA_B200_OK;
+  k_gas_elem<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(freq, temp, rho_vap, press, kext, status, n);
+  return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
+}
+
+__global__ void k_tkc_elem(const double* tc, const double* f, double* re, double* im, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  cplx e = eps_water_tkc(tc[i], f[i]);
+  re[i] = e.re;
+  im[i] = e.im;
+}
+
+int32_t pamtra_b200_eps_water_tkc(const double* t_c, const double* freq, double* eps_re, double* eps_im, int32_t n,
+                                  void* stream) {
+  if (n <= 0) return PAMTRA_B200_OK;
+  k_tkc_elem<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(t_c, freq, eps_re, eps_im, n);
+  return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
+}
+
+int32_t pamtra_b200_minvert_batched(const double* a, double* ainv, int32_t* status, int32_t n, int32_t count,
+                                    void* stream) {
+  if (count <= 0) return PAMTRA_B200_OK;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int g = std::min(count, 65535);
+  if (n == 16) k_minvert<16><<<g, 16, 0, s>>>(a, ainv, status, count);
+  else if (n == 32) k_minvert<32><<<g, 32, 0, s>>>(a, ainv, status, count);
+  else if (n == 64) k_minvert<64><<<g, 128, 0, s>>>(a, ainv, status, count);
+  else return PAMTRA_B200_FATAL;
+  return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
+}
+
+}  // extern "C"

@@ -1,0 +1,345 @@
+// Single scattering of Mie spheres, integrated over the size distribution,
+// summed over species into normalised Legendre coefficients per
+// (column, layer, frequency).
+#pragma once
+#include "common.cuh"
+#include "work.cuh"
+
+namespace pb {
+
+constexpr int MIE_WARPS = 4;
+constexpr int NQ_MAX = 256;   // Gauss points per series (nquad)
+constexpr int NT_MAX = 128;   // Mie terms per bin
+
+struct MieSmem {
+  double sump[4][NQ_MAX];
+  double legh[3][MAXNLEG];
+  double legc[3][MAXNLEG];
+};
+
+// src/eps_water.f90:653-757 eps_water_tkc (T in degC, f in GHz)
+__device__ cplx eps_water_tkc(double T, double f) {
+  const double a_1 = 8.169396e+01, b_1 = 4.410555e-03, c_1 = 1.208992e-13, d_1 = 6.768869e+02;
+  const double a_2 = 1.597733e+00, b_2 = 1.060228e-02, c_2 = 9.982113e-15, d_2 = 5.720517e+02;
+  const double t_c = 1.351758e+02;
+  const double frq = f * 1e9;
+  double eps_s = 87.9144 - 0.404399 * T + 9.58726e-4 * (T * T) - 1.32802e-6 * pow(T, 3.0);
+  double delta_1 = a_1 * exp(-b_1 * T), tau_1 = c_1 * exp(d_1 / (T + t_c));
+  double delta_2 = a_2 * exp(-b_2 * T), tau_2 = c_2 * exp(d_2 / (T + t_c));
+  double wv = 2.0 * PI * frq;
+  double x1 = wv * tau_1, x2 = wv * tau_2;
+  double t1 = ((tau_1 * tau_1) * delta_1) / (1.0 + x1 * x1);
+  double t2 = ((tau_2 * tau_2) * delta_2) / (1.0 + x2 * x2);
+  double eps1 = eps_s - (wv * wv) * (t1 + t2);
+  t1 = (tau_1 * delta_1) / (1.0 + x1 * x1);
+  t2 = (tau_2 * delta_2) / (1.0 + x2 * x2);
+  double eps2 = wv * (t1 + t2);
+  return cmplx4(eps1, eps2);  // CMPLX without KIND (eps_water.f90:749)
+}
+
+// src/ref_water.f90 (liq_mod TKC): m = sqrt(eps), (refre, refim) with refim > 0
+__device__ cplx ref_water(double T_c, double f) { return csqrt_(eps_water_tkc(T_c, f)); }
+
+// src/eps_ice.f90 + src/ref_ice.f90 (Maetzler ice)
+__device__ cplx ref_ice(double T, double f) {
+  double eps_real = (T >= 240.0) ? 3.1884 + 9.1e-4 * (T - 273.0) : 3.1884 + 9.1e-4 * (240.0 - 273.0);
+  double mit = (300.0 / T) - 1.0;
+  double alpha = (0.00504 + 0.0062 * mit) * exp(-22.1 * mit);
+  double e = exp(335.0 / T);
+  double beta_m = (0.0207 / T) * e / ((e - 1.0) * (e - 1.0));
+  beta_m = beta_m + 1.16e-11 * (f * f);
+  double delta_beta = exp(-9.963 + 0.0372 * (T - 273.16));
+  double beta = beta_m + delta_beta;
+  double eps_imag = (alpha / f) + beta * f;
+  return csqrt_(cmk(eps_real, eps_imag));
+}
+
+// src/eps_mix.f90 with eps0 = 1: Sihvola mixing applied to the refractive
+// index m of ice for a particle of density mix_de (mie_spheres.f90:139-144)
+__device__ cplx eps_mix_m(cplx eps1, double mix_de) {
+  const double v = 0.85, f = mix_de / 917.0, re1 = eps1.re, e0 = 1.0;
+  double bb = re1 + 2.0 * e0 - 2.0 * v * e0 - f * (re1 - e0) * (1 + v);
+  double aa = e0 * (re1 + (2.0 - v) * e0 + f * (2.0 - v) * (re1 - e0));
+  double em_real = (sqrt(bb * bb + 4.0 * v * aa) - bb) / (2.0 * v);
+  double em_imag = eps1.im * (-1.0 * (em_real - e0) + f * (em_real + 2.0 * e0 + v * (em_real - e0))) /
+                   ((re1 + 2.0 * e0 + 2.0 * v * (em_real - e0)) - f * (1.0 + v) * (re1 - e0));
+  return cmplx4(em_real, em_imag);  // CMPLX without KIND (eps_mix.f90:44)
+}
+
+__device__ __forceinline__ int mie_nstop(double x) { return (int)(x + 4.0 * pow(x, F(0.3334f)) + 2); }
+
+// src/mie_scat_utilities.f90:8-116 miecalc + miecross for one particle: Mie
+// coefficients a_n (into ab[0..]) and b_n (into bb[0..]), 1-based n stored at n-1.
+__device__ void miecalc_cross(int nterms, double x, cplx mn, cplx* ab, cplx* bb, double& qext, double& qscat,
+                              double& qback) {
+  const cplx m = cconj(mn);
+  const cplx y = cscale(m, x);
+  const int nn = nterms + 15;
+  // downward recurrence d(n-1) = n/y - 1/(d(n) + n/y), d(nn) = 0; keep d(1..nterms)
+  cplx d = cmk(0.0, 0.0);
+  for (int n = nn; n >= 2; n--) {
+    cplx ny = cdiv(cmk((double)n, 0.0), y);
+    d = csub(ny, cdiv(cmk(1.0, 0.0), cadd(d, ny)));
+    if (n - 1 <= nterms) ab[n - 2] = d;  // d(n-1) stored at index n-2
+  }
+  double psim = cos(x), psin = sin(x), chim = -sin(x), chin = cos(x);
+  double sum1 = 0.0, sum2 = 0.0;
+  cplx sum3 = cmk(0.0, 0.0);
+  for (int n = 1; n <= nterms; n++) {
+    double tmp = psin;
+    psin = (2 * n - 1) / x * psin - psim;
+    psim = tmp;
+    tmp = chin;
+    chin = (2 * n - 1) / x * chin - chim;
+    chim = tmp;
+    const cplx xin = cmplx4(psin, -chin), xim = cmplx4(psim, -chim);
+    const cplx dn = ab[n - 1];
+    cplx ctmp = cdiv(dn, m);
+    ctmp.re = ctmp.re + n / x;
+    cplx an = cdiv(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
+    ctmp = cmul(m, dn);
+    ctmp.re = ctmp.re + n / x;
+    cplx bn = cdiv(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
+    ab[n - 1] = an;
+    bb[n - 1] = bn;
+    sum1 = sum1 + (2 * n + 1) * (an.re + bn.re);
+    sum2 = sum2 + (2 * n + 1) * ((an.re * an.re - an.im * (-an.im)) + (bn.re * bn.re - bn.im * (-bn.im)));
+    double fac = (double)((float)(2 * n + 1) * ((n & 1) ? -1.0f : 1.0f));
+    sum3 = cadd(sum3, cscale(csub(an, bn), fac));
+  }
+  qext = 2.0 / (x * x) * sum1;
+  qscat = 2.0 / (x * x) * sum2;
+  cplx t = cscale(sum3, 1.0 / (x * x));
+  qback = t.re * sum3.re - t.im * (-sum3.im);
+}
+
+// src/mie_scat_utilities.f90:119-160 mieangle
+__device__ __forceinline__ void mieangle(int nterms, const cplx* ab, const cplx* bb, double mu, double p[4]) {
+  cplx s1 = cmk(0.0, 0.0), s2 = cmk(0.0, 0.0);
+  double pin = 1.0, pim = 0.0;
+  for (int n = 1; n <= nterms; n++) {
+    double taun = n * mu * pin - (n + 1) * pim;
+    double c = (double)((float)(2 * n + 1) / (float)(n * (n + 1)));  // REAL(4) division
+    const cplx a = ab[n - 1], b = bb[n - 1];
+    s1.re = fma(c, fma(a.re, pin, b.re * taun), s1.re);
+    s1.im = fma(c, fma(a.im, pin, b.im * taun), s1.im);
+    s2.re = fma(c, fma(b.re, pin, a.re * taun), s2.re);
+    s2.im = fma(c, fma(b.im, pin, a.im * taun), s2.im);
+    double tmp = pin;
+    pin = ((2 * n + 1) * mu * pin - (n + 1) * pim) / n;
+    pim = tmp;
+  }
+  double as1 = hypot(s1.re, s1.im), as2 = hypot(s2.re, s2.im);
+  p[0] = 0.5 * (as2 * as2 + as1 * as1);
+  p[1] = 0.5 * (as2 * as2 - as1 * as1);
+  p[2] = s2.re * s1.re - (-s2.im) * s1.im;
+  p[3] = s1.re * s2.im + (-s1.im) * s2.re;
+}
+
+// One warp per (present layer, frequency) item; species loop in descriptor
+// order.  src/scatProperties.f90:62-1002 (mie-sphere branch and the species
+// sums :920-949, finalize :993) with src/mie_spheres.f90:14-345 per species.
+// Bins are spread over lanes; per-angle phase functions and the efficiencies
+// are summed over bins with warp shuffles; the Legendre projection is a
+// lane-per-quadrature-point series reduced with shuffles.
+__global__ void __launch_bounds__(32 * MIE_WARPS) k_mie(Batch b, Work w, pamtra_b200_settings st) {
+  extern __shared__ double smem_raw[];
+  MieSmem& S = reinterpret_cast<MieSmem*>(smem_raw)[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const int Lm = b.max_nlyrs, Fm = b.max_nfreq, H = b.nhydro;
+  const int P = min(w.counters[0], w.pmax);
+  const int nitems = P * Fm;
+  cplx ab[NT_MAX], bb[NT_MAX];
+  for (;;) {
+    int item = 0;
+    if (lane == 0) item = atomicAdd(&w.counters[1], 1);
+    item = __shfl_sync(0xffffffffu, item, 0);
+    if (item >= nitems) break;
+    const int p = item / Fm, f = item % Fm;
+    const int cz = w.plist[p];
+    const int c = cz / Lm, z = cz % Lm;
+    if (f >= b.col_nfreq(c)) continue;
+    const double freq = b.freq(c, f);
+    const double wl = C_LIGHT / (freq * 1e9);
+    const double T = w.temp[(size_t)c * Lm + z];
+    for (int jj = lane; jj < MAXNLEG; jj += 32) { S.legc[0][jj] = 0.0; S.legc[1][jj] = 0.0; S.legc[2][jj] = 0.0; }
+    double kexttot = 0.0, salbedo = 0.0;
+    int nlegen_coef = 0;
+    int status = 0;
+    for (int h = 0; h < H; h++) {
+      const size_t s_idx = ((size_t)c * Lm + z) * H + h;
+      if (w.slot_st[s_idx] != 2) continue;
+      const pamtra_b200_species sp = b.species_of(c, h);
+      const int nb = w.slot_nb[s_idx];
+      const size_t base = s_idx * (size_t)b.max_nbin;
+      const double* bd = w.b_d + base;
+      const double* bdd = w.b_dd + base;
+      const double* bnd = w.b_nd + base;
+      const double* brho = w.b_rho + base;
+      const double* bmass = w.b_mass + base;
+      cplx mref = (sp.liq_ice == 1) ? ref_water(T - F(273.15f), freq) : ref_ice(T, freq);
+      const cplx m_ice = cmk(mref.re, -mref.im);
+      // density / diameter of bin i (frequency-dependent soft spheroids of
+      // make_soft_spheroid.f90:109-114 resolved here)
+      auto dens_diam = [&](int i, double& rho, double& dia) {
+        rho = brho[i];
+        dia = bd[i];
+        if (rho == -1.0) {
+          const double mind = st.hydro_softsphere_min_density;
+          rho = (sp.as_ratio == -20.) ? 0.863 * freq + 115.0 : 0.815 * freq + 11.2;
+          if (rho < mind) rho = mind;
+          dia = pow((6.0 * bmass[i]) / (PI * rho), 1.0 / 3.0);
+          if (st.hydro_limit_density_area) {
+            if (rho > RHO_ICE) rho = RHO_ICE;
+            else if (rho < mind) rho = mind;
+          }
+        }
+      };
+      double rho0, dia0, rhoN, diaN;
+      dens_diam(0, rho0, dia0);
+      dens_diam(nb - 1, rhoN, diaN);
+      const bool use_mix = (sp.liq_ice == -1) && (rho0 != 917.0);
+      const double xmax = PI * diaN / wl;
+      const int nterms = mie_nstop(xmax);
+      int nlegen = min(MAXNLEG - 1, 2 * nterms);
+      const int nquad = (nlegen + 2 * nterms + 2) / 2;
+      if (nquad > NQ_MAX || nquad > w.gq_max || nterms + 1 > NT_MAX) {
+        status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
+        break;
+      }
+      const double* gx = w.gq_x + (size_t)nquad * (nquad - 1) / 2;
+      const double* gw = w.gq_w + (size_t)nquad * (nquad - 1) / 2;
+      for (int i = lane; i < nquad; i += 32) { S.sump[0][i] = 0; S.sump[1][i] = 0; S.sump[2][i] = 0; S.sump[3][i] = 0; }
+      __syncwarp();
+      double sqe = 0.0, sqs = 0.0, sqb = 0.0;
+      for (int c0 = 0; c0 < nb; c0 += 32) {
+        const int ir = c0 + lane;
+        bool act = false;
+        double wgt = 0.0, ndens = 0.0, deld = 0.0;
+        int nm = 0;
+        if (ir < nb) {
+          deld = bdd[ir];
+          ndens = bnd[ir] / deld;
+          act = ndens > 0;
+        }
+        if (act) {
+          double rho, dia;
+          dens_diam(ir, rho, dia);
+          const cplx ms = (sp.liq_ice == -1 && rho != 917.0) ? eps_mix_m(m_ice, rho) : m_ice;
+          const double x = PI * dia / wl;
+          int nmie = mie_nstop(x);
+          if (nmie + 1 > NT_MAX) { nmie = NT_MAX - 1; status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE; }
+          double qe, qs, qb;
+          miecalc_cross(nmie, x, ms, ab, bb, qe, qs, qb);
+          const double r2 = (dia / 2.0) * (dia / 2.0);
+          qe = qe * r2 * PI;
+          qs = qs * r2 * PI;
+          qb = qb * r2 * PI;
+          qe = qe * ndens;
+          qs = qs * ndens;
+          qb = qb * ndens;
+          sqe = sqe + qe * deld;
+          sqs = sqs + qs * deld;
+          sqb = sqb + qb * deld;
+          nm = min(nmie, nterms);
+          wgt = ndens;
+        }
+        for (int i = 0; i < nquad; i++) {
+          double pp[4] = {0.0, 0.0, 0.0, 0.0};
+          if (act) {
+            mieangle(nm, ab, bb, gx[i], pp);
+#pragma unroll
+            for (int k = 0; k < 4; k++) pp[k] = pp[k] * wgt * deld;
+          }
+#pragma unroll
+          for (int k = 0; k < 4; k++) pp[k] = warp_sum(pp[k]);
+          if (lane == (i & 31)) {
+#pragma unroll
+            for (int k = 0; k < 4; k++) S.sump[k][i] += pp[k];
+          }
+        }
+      }
+      __syncwarp();
+      sqe = warp_sum(sqe);
+      sqs = warp_sum(sqs);
+      sqb = warp_sum(sqb);
+      const double extinction = st.lhyd_absorption ? sqe : sqe - sqs;
+      const double scatter = sqs;
+      const double salb_h = scatter / extinction;
+      const double tmp = (wl * wl / (PI * scatter));
+      for (int i = lane; i < nquad; i += 32) {
+        const double wt = gw[i];
+#pragma unroll
+        for (int k = 0; k < 4; k++) S.sump[k][i] = tmp * S.sump[k][i] * wt;
+      }
+      __syncwarp();
+      // Legendre projection: coef_l = sum_i sump(i) P_l(mu_i), l = 0..nlegen
+      constexpr int NQL = NQ_MAX / 32;
+      double pl[NQL], pl1[NQL], pl2[NQL];
+#pragma unroll
+      for (int q = 0; q < NQL; q++) { pl[q] = 1.0; pl1[q] = 1.0; pl2[q] = 0.0; }
+      const double thr = F(1.0e-7f);
+      int last = -1;
+      for (int l = 0; l <= nlegen; l++) {
+        double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int q = 0; q < NQL; q++) {
+          const int i = lane + 32 * q;
+          if (i < nquad) {
+            const double mu = gx[i];
+            if (l > 0) pl[q] = (2 * l - 1) * mu * pl1[q] / l - (l - 1) * pl2[q] / l;
+#pragma unroll
+            for (int k = 0; k < 3; k++) acc[k] = fma(S.sump[k][i], pl[q], acc[k]);
+            pl2[q] = pl1[q];
+            pl1[q] = pl[q];
+          }
+        }
+        const double fac = (double)((float)(2 * l + 1) / 2.0f);  // REAL(4) division, exact
+#pragma unroll
+        for (int k = 0; k < 3; k++) acc[k] = fac * warp_sum(acc[k]);
+        if (lane == 0) { S.legh[0][l] = acc[0]; S.legh[1][l] = acc[1]; S.legh[2][l] = acc[2]; }
+        if (acc[0] > thr) last = l;
+      }
+      for (int l = nlegen + 1 + lane; l < MAXNLEG; l += 32) { S.legh[0][l] = 0; S.legh[1][l] = 0; S.legh[2][l] = 0; }
+      __syncwarp();
+      const int nlegen_h = (last >= 0) ? last : nlegen;  // mie_spheres.f90:307-314
+      if (!(extinction > 0) || !(scatter > 0) || !(sqb > 0) || isnan(extinction)) {
+        status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_MIE;
+        break;
+      }
+      // species sums (scatProperties.f90:920-949)
+      nlegen_coef = max(nlegen_coef, nlegen_h);
+      kexttot = kexttot + extinction;
+      if (kexttot == 0.0) salbedo = 0.0;
+      else salbedo = salbedo + (salb_h * extinction);
+      for (int jj = lane; jj < nlegen_coef; jj += 32) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) S.legc[k][jj] = S.legc[k][jj] + (S.legh[k][jj] * salb_h * extinction);
+      }
+      __syncwarp();
+      if (nlegen_coef > MAXNLEG - 1) { status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE; break; }
+    }
+    // finalize_rt3_scatProperties (scatProperties.f90:993-1002)
+    salbedo = salbedo / kexttot;
+    const double den = salbedo * kexttot;
+    double* out = w.m_legen + (size_t)item * 3 * MAXNLEG;
+    for (int jj = lane; jj <= nlegen_coef && jj < MAXNLEG; jj += 32) {
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        double v = S.legc[k][jj] / den;
+        if (isnan(v) && nlegen_coef > 0) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_NAN;
+        out[k * MAXNLEG + jj] = v;
+      }
+    }
+    status = __reduce_or_sync(0xffffffffu, status);
+    if (lane == 0) {
+      w.m_kext[item] = kexttot;
+      w.m_salb[item] = salbedo;
+      w.m_nleg[item] = nlegen_coef;
+      if (status) atomicOr(&w.status[(size_t)c * Fm + f], status);
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace pb

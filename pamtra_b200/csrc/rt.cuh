@@ -1,0 +1,699 @@
+// RT4 on the GPU.
+//   k_layer<N>: per (present layer, frequency) item -- scatcnv (Legendre
+//     series -> quadrature phase matrices), check_norm4, INITIALIZE4 /
+//     INITIAL_SOURCE4 and DOUBLING_INTEGRATION4; writes the layer's R, T and
+//     S+/S- to the scratch arena.
+//   k_adding<N>: per (column, frequency) unit -- adding of all layers top
+//     down (COMBINE_LAYERS4 specialised by structure), surface, internal
+//     radiance at the output levels and conversion to brightness temperature.
+#pragma once
+#include "common.cuh"
+#include "work.cuh"
+
+namespace pb {
+
+constexpr double TWO_PI = 2.0 * 3.1415926535897932384;
+constexpr double LN2_F32 = 0.693147182464599609375;  // log(2.) in REAL(4) (radtran4.f90:325)
+
+// src/rt_utilities.f90:69-90 PLANCK_FUNCTION, UNITS='r'
+__device__ __forceinline__ double planck(double T, double wl) {
+  return (T > 0.0) ? 1.1911e8 / p5(wl) / (exp(1.4388e4 / (wl * T)) - 1) : 0.0;
+}
+
+// src/rt_utilities.f90:687-735 CONVERT_OUTPUT (UNITS='T', FLUXCODE=0)
+__device__ __forceinline__ double rad_to_tb(double rad, double wl) {
+  if (rad > 0.0) return 1.4388e4 / (wl * log(1.0 + 1.1911e8 / (rad * p5(wl))));
+  if (rad == 0.0) return 0.0;
+  return -1.4388e4 / (wl * log(1.0 + 1.1911e8 / (-rad * p5(wl))));
+}
+
+template <int N>
+struct RTCfg {
+  static constexpr int n = 2 * N;
+  static constexpr int RS = (N >= 32) ? 2 : 1;
+  static constexpr int T = n * RS;
+  static constexpr int LD = n + 2;
+  static constexpr int MAT = n * LD;
+  static constexpr size_t LAY_STRIDE = 2 * (size_t)MAT + 2 * n;  // R, T, S+, S-
+};
+
+// ============================================================== layer kernel
+template <int N>
+struct LayerSmem {
+  static constexpr int n = RTCfg<N>::n, MAT = RTCfg<N>::MAT;
+  double m[5][MAT];
+  double coef[3][MAXNLEG];
+  double lin[2 * n], cst[2 * n];
+  double v[4][n], u[4][n];
+  double f[n];
+  double mu[N], wq[N];
+  double redv[8];
+  int piv[n];
+  int redi[8 + n];
+};
+
+template <int N>
+__global__ void __launch_bounds__(RTCfg<N>::T) k_layer(Batch b, Work w, pamtra_b200_settings st,
+                                                       double* __restrict__ ssp_scat) {
+  constexpr int n = RTCfg<N>::n, RS = RTCfg<N>::RS, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT;
+  constexpr int R_ = n / RS;
+  extern __shared__ double smem_raw[];
+  LayerSmem<N>& S = *reinterpret_cast<LayerSmem<N>*>(smem_raw);
+  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R_;
+  const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
+  const int P = min(w.counters[0], w.pmax);
+  const int nitems = P * Fm;
+  if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
+  __shared__ int s_item;
+  for (;;) {
+    team_sync();
+    if (t == 0) s_item = atomicAdd(&w.counters[2 + (N == 8 ? 0 : (N == 16 ? 1 : 2))], 1);
+    team_sync();
+    const int item = s_item;
+    if (item >= nitems) break;
+    const int p = item / Fm, fi = item % Fm;
+    const int cz = w.plist[p];
+    const int c = cz / Lm, z = cz % Lm;
+    if (fi >= b.col_nfreq(c) || b.col_nummu(c) != N) continue;
+    const double freq = b.freq(c, fi);
+    const double wl = C_LIGHT / (freq * 1.e3);
+    const double* hl = w.hgt_lev + (size_t)c * (Lm + 1);
+    const double* tl = w.temp_lev + (size_t)c * (Lm + 1);
+    const double zdiff = fabs(hl[z + 1] - hl[z]);
+    const double gas = fmax(w.kgas[((size_t)c * Fm + fi) * Lm + z], 0.0);
+    const double planck0 = planck(tl[z + 1], wl), planck1 = planck(tl[z], wl);
+    const int nleg = w.m_nleg[item];
+    const double kext = w.m_kext[item], salb = w.m_salb[item];
+    double* Rb = S.m[0];
+    double* Tb = S.m[1];
+    double* Gb = S.m[2];
+    double* Ab = S.m[3];
+    double* Bb = S.m[4];
+    double ext = 0.0, emis = 0.0;
+    int status = 0;
+    // ---------------- scatcnv (src/scatcnv.f90) into P1 (Tb) and P2 (Rb)
+    if (nleg > 0) {
+      ext = kext;
+      emis = (1.0 - salb) * kext;
+      const double cst = kext * salb / (4.0 * 3.1415926535897932384);
+      const double* lg = w.m_legen + (size_t)item * 3 * MAXNLEG;
+      for (int l = t; l <= nleg; l += RTCfg<N>::T) {
+        S.coef[0][l] = cst * lg[l];
+        S.coef[1][l] = cst * lg[MAXNLEG + l];
+        S.coef[2][l] = cst * lg[2 * MAXNLEG + l];
+      }
+      team_sync();
+      const int numpts = 2 * ((nleg + 1) / 2) + 4;
+      const int K = numpts / 2 + 1;
+      for (int it = t; it < 2 * N * N; it += RTCfg<N>::T) {
+        const int q = it / (N * N), j1 = (it / N) % N, j2 = it % N;
+        const double mu1 = (q == 0) ? S.mu[j1] : -S.mu[j1];
+        const double mu2 = S.mu[j2];
+        const double st1 = sqrt(1. - mu1 * mu1), st2 = sqrt(1. - mu2 * mu2);
+        const double sqm = sqrt((1. - mu1 * mu1) * (1. - mu2 * mu2));
+        double a11 = 0, a12 = 0, a21 = 0, a22 = 0, m11 = 0, m12 = 0, m21 = 0, m22 = 0;
+        for (int k = 1; k <= K; k++) {
+          const double delphi = (TWO_PI * (k - 1)) / numpts;
+          const double cosphi = cos(delphi), sinphi = sin(delphi);
+          const double cs = mu1 * mu2 + sqm * cosphi;
+          // SUM_LEGENDRE, DOSUM = (1,1,1,0,0,0)
+          double s0 = S.coef[0][0], s1 = S.coef[1][0], s2 = S.coef[2][0];
+          double pl1 = 1.0, pl2 = 0.0, pl = 1.0;
+          for (int L = 1; L <= nleg; L++) {
+            pl = (2 * L - 1) * cs * pl1 / L - (L - 1) * pl2 / L;
+            s0 = fma(S.coef[0][L], pl, s0);
+            s1 = fma(S.coef[1][L], pl, s1);
+            s2 = fma(S.coef[2][L], pl, s2);
+            pl2 = pl1;
+            pl1 = pl;
+          }
+          // ROTATE_PHASE_MATRIX (NSTOKES=2)
+          const double ss = sqrt(fmax(0.0, 1. - cs * cs));
+          double sin1, sin2, cos1, cos2;
+          if (ss == 0.0) {
+            sin1 = 0; sin2 = 0; cos1 = 1; cos2 = -1;
+          } else {
+            sin1 = st2 * sinphi / ss;
+            sin2 = st1 * sinphi / ss;
+            cos1 = (st1 * mu2 - st2 * mu1 * cosphi) / ss;
+            cos2 = (st2 * mu1 - st1 * mu2 * cosphi) / ss;
+          }
+          const double sin21 = 2.0 * sin1 * cos1, cos21 = 1.0 - 2.0 * (sin1 * sin1);
+          const double sin22 = 2.0 * sin2 * cos2, cos22 = 1.0 - 2.0 * (sin2 * sin2);
+          const double e11 = s0, e12 = s1 * cos21, e21 = s1 * cos22, e22 = s0 * cos21 * cos22 - s2 * sin21 * sin22;
+          // FOURIER_BASIS order 0: points k and numpts-k+2 coincide (MATRIX_SYMMETRY)
+          a11 += e11; a12 += e12; a21 += e21; a22 += e22;
+          if (k > 1 && k < K) { m11 += e11; m12 += e12; m21 += e21; m22 += e22; }
+        }
+        double* Q = (q == 0) ? Tb : Rb;
+        const int row0 = 2 * j2, col0 = 2 * j1;
+        Q[(col0 + 0) * LD + row0 + 0] = (a11 + m11) / numpts;
+        Q[(col0 + 1) * LD + row0 + 0] = (a12 + m12) / numpts;
+        Q[(col0 + 0) * LD + row0 + 1] = (a21 + m21) / numpts;
+        Q[(col0 + 1) * LD + row0 + 1] = (a22 + m22) / numpts;
+      }
+      team_sync();
+      if (!st.lhyd_scattering) {
+        for (int e = t; e < MAT; e += RTCfg<N>::T) { Tb[e] = 0.0; Rb[e] = 0.0; }
+        team_sync();
+      }
+      if (!st.lhyd_emission) emis = 0.0;
+    } else {
+      for (int e = t; e < MAT; e += RTCfg<N>::T) { Tb[e] = 0.0; Rb[e] = 0.0; }
+      team_sync();
+    }
+    // optional save_ssp output of the 4 quadrants (l=1,4 equal; l=2,3 equal)
+    if (ssp_scat) {
+      const size_t o = (((size_t)c * Fm + fi) * Lm + z) * 4 * (size_t)(2 * b.max_nummu) * (2 * b.max_nummu);
+      const int nn = 2 * b.max_nummu;
+      for (int e = t; e < n * n; e += RTCfg<N>::T) {
+        const int row = e / n, col = e % n;
+        const double p1 = Tb[col * LD + row], p2 = Rb[col * LD + row];
+        ssp_scat[o + 0 * (size_t)nn * nn + (size_t)row * nn + col] = p1;
+        ssp_scat[o + 1 * (size_t)nn * nn + (size_t)row * nn + col] = p2;
+        ssp_scat[o + 2 * (size_t)nn * nn + (size_t)row * nn + col] = p2;
+        ssp_scat[o + 3 * (size_t)nn * nn + (size_t)row * nn + col] = p1;
+      }
+    }
+    // ---------------- CHECK_NORM4 (src/radscat4.f90:87-136)
+    if (t < N) {
+      double sum = emis - ext;
+      for (int j2 = 0; j2 < N; j2++)
+        sum = sum + 2.0 * 3.1415926535897932384 * S.wq[j2] * (Tb[(2 * t) * LD + 2 * j2] + Rb[(2 * t) * LD + 2 * j2]);
+      S.f[t] = fabs(sum);
+    }
+    team_sync();
+    if (t == 0) {
+      double mx = 0.0;
+      for (int i = 0; i < N; i++) mx = fmax(mx, S.f[i]);
+      if (mx > 5.0e-4) S.redi[0] = PAMTRA_B200_FATAL | PAMTRA_B200_ST_NORM;
+      else S.redi[0] = 0;
+    }
+    team_sync();
+    status |= S.redi[0];
+    // ---------------- number of doublings (src/radtran4.f90:319-329)
+    const double extinct = ext + gas;
+    const double fl = log(fmax(extinct * zdiff, 1.0e-7) / 1.0e-6) / LN2_F32;
+    int nd = 0;
+    if (fl > 0.0) nd = (int)fl + 1;
+    const double num_sub = ldexp(1.0, nd);
+    const double delta_z = zdiff / num_sub;
+    // ---------------- INITIALIZE4 (src/radintg4.f90:1-45), in place over P1/P2
+    {
+      const double C = 2.0 * 3.1415926535897932384;
+      const int col = j, i1 = col & 1, j1 = col >> 1;
+      const double wj1 = S.wq[j1];
+      for (int ii = 0; ii < R_; ii++) {
+        const int row = r0 + ii, i2 = row & 1, j2 = row >> 1;
+        const double tmp = delta_z / S.mu[j2];
+        const double gext = (i1 == i2) ? gas : 0.0;
+        const double diag = (row == col) ? 1.0 : 0.0;
+        double ex = 0.0;
+        if (j1 == j2) ex = ((i1 == i2) ? ext : 0.0) + gext;
+        Rb[col * LD + row] = C * tmp * wj1 * Rb[col * LD + row];
+        Tb[col * LD + row] = diag - tmp * (ex - C * wj1 * Tb[col * LD + row]);
+      }
+    }
+    // INITIAL_SOURCE4 (src/radintg4.f90:51-73)
+    if (t < n) {
+      const int i = t & 1, jj = t >> 1;
+      const double tmp = planck0 * delta_z / S.mu[jj];
+      const double v = (i == 0) ? tmp * (emis + gas) : tmp * (0.0 + 0.0);
+      S.lin[t] = v;
+      S.lin[n + t] = v;
+      S.cst[t] = v;
+      S.cst[n + t] = v;
+    }
+    double linfac = (planck0 == 0.0) ? 0.0 : (planck1 / planck0 - 1.0) / num_sub;
+    team_sync();
+    // ---------------- DOUBLING_INTEGRATION4, SYMMETRIC (src/radintg4.f90:174-309)
+    for (int itd = 0; itd < nd; itd++) {
+      mm<n, RS>(Rb, Rb, Ab);
+      team_sync();
+      for (int ii = 0; ii < R_; ii++) {
+        const int row = r0 + ii;
+        Ab[j * LD + row] = ((row == j) ? 1.0 : 0.0) - Ab[j * LD + row];
+      }
+      team_sync();
+      if (ginv<n, RS>(Ab, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      { double* tmp = Gb; Gb = Ab; Ab = tmp; }
+      // source chains: v = [S- + f C-, C-, S+, C+] -> R v -> add -> G -> T
+      if (t < n) {
+        S.v[0][t] = S.lin[n + t] + linfac * S.cst[n + t];
+        S.v[1][t] = S.cst[n + t];
+        S.v[2][t] = S.lin[t];
+        S.v[3][t] = S.cst[t];
+      }
+      team_sync();
+      if (t < n) {
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        for (int k = 0; k < n; k++) {
+          const double r = Rb[k * LD + t];
+          a0 = fma(r, S.v[0][k], a0); a1 = fma(r, S.v[1][k], a1); a2 = fma(r, S.v[2][k], a2); a3 = fma(r, S.v[3][k], a3);
+        }
+        S.u[0][t] = S.lin[t] + a0;
+        S.u[1][t] = S.cst[t] + a1;
+        S.u[2][t] = S.v[0][t] + a2;
+        S.u[3][t] = S.cst[n + t] + a3;
+      }
+      team_sync();
+      if (t < n) {
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        for (int k = 0; k < n; k++) {
+          const double g = Gb[k * LD + t];
+          a0 = fma(g, S.u[0][k], a0); a1 = fma(g, S.u[1][k], a1); a2 = fma(g, S.u[2][k], a2); a3 = fma(g, S.u[3][k], a3);
+        }
+        S.v[0][t] = a0; S.v[1][t] = a1; S.v[2][t] = a2; S.v[3][t] = a3;
+      }
+      team_sync();
+      double o0 = 0, o1 = 0, o2 = 0, o3 = 0;
+      if (t < n) {
+        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+        for (int k = 0; k < n; k++) {
+          const double tt = Tb[k * LD + t];
+          a0 = fma(tt, S.v[0][k], a0); a1 = fma(tt, S.v[1][k], a1); a2 = fma(tt, S.v[2][k], a2); a3 = fma(tt, S.v[3][k], a3);
+        }
+        o0 = (S.lin[t] + a0) + linfac * S.cst[t];
+        o1 = S.cst[t] + a1;
+        o2 = S.lin[n + t] + a2;
+        o3 = S.cst[n + t] + a3;
+      }
+      // matrices: R' = R + T G R T ; T' = T G T
+      mm<n, RS>(Rb, Tb, Ab);
+      team_sync();
+      mm<n, RS>(Gb, Ab, Bb);
+      team_sync();
+      mm<n, RS>(Tb, Bb, Ab);
+      team_sync();
+      for (int ii = 0; ii < R_; ii++) Rb[j * LD + r0 + ii] = Rb[j * LD + r0 + ii] + Ab[j * LD + r0 + ii];
+      mm<n, RS>(Gb, Tb, Bb);
+      team_sync();
+      mm<n, RS>(Tb, Bb, Ab);
+      team_sync();
+      { double* tmp = Tb; Tb = Ab; Ab = tmp; }
+      if (t < n) {
+        S.lin[t] = o0; S.cst[t] = o1; S.lin[n + t] = o2; S.cst[n + t] = o3;
+      }
+      linfac = 2.0 * linfac;
+      team_sync();
+    }
+    // ---------------- write layer R, T, S+, S-
+    double* out = w.lay + (size_t)item * w.lay_stride;
+    for (int e = t; e < MAT; e += RTCfg<N>::T) { out[e] = Rb[e]; out[MAT + e] = Tb[e]; }
+    if (t < 2 * n) out[2 * MAT + t] = S.lin[t];
+    if (RTCfg<N>::T < 2 * n)
+      for (int e = t + RTCfg<N>::T; e < 2 * n; e += RTCfg<N>::T) out[2 * MAT + e] = S.lin[e];
+    if (t == 0) {
+      w.lay_nd[item] = nd;
+      if (status) atomicOr(&w.status[(size_t)c * Fm + fi], status);
+    }
+  }
+}
+
+// ============================================================== adding kernel
+// Shared memory: stack (R+, R-, T+, T-), layer (R2, T2), G and three temps,
+// vectors.
+template <int N>
+struct AddSmem {
+  static constexpr int n = RTCfg<N>::n, MAT = RTCfg<N>::MAT;
+  double m[10][MAT];
+  double sp[n], sm[n], s2p[n], s2m[n], t1[n], t2[n], nsp[n], nsm[n];
+  double wv[n], wv2[n];
+  double sky[n], gnd[n], uprad[n], dnrad[n];
+  double f[n];
+  double mu[N], wq[N];
+  double redv[8];
+  int piv[n];
+  int redi[8 + n];
+};
+
+// team helpers on AddSmem
+template <int n, int RS>
+__device__ __forceinline__ void mat_ident_minus(double* A) {  // A = I - A
+  constexpr int LD = TeamCfg<n, RS>::LD, R = TeamCfg<n, RS>::R;
+  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R;
+  for (int ii = 0; ii < R; ii++) {
+    const int row = r0 + ii;
+    A[j * LD + row] = ((row == j) ? 1.0 : 0.0) - A[j * LD + row];
+  }
+}
+template <int n, int RS>
+__device__ __forceinline__ void mat_fill_diag(double* A, const double* d) {  // A = diag(d)
+  constexpr int LD = TeamCfg<n, RS>::LD, R = TeamCfg<n, RS>::R;
+  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R;
+  for (int ii = 0; ii < R; ii++) {
+    const int row = r0 + ii;
+    A[j * LD + row] = (row == j) ? d[j] : 0.0;
+  }
+}
+template <int n, int RS>
+__device__ __forceinline__ double mvr(const double* M, const double* x, int row) {
+  return mv_row<n, RS>(M, x, row);
+}
+
+template <int N>
+__global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_b200_settings st,
+                                                        pamtra_b200_outputs out) {
+  constexpr int n = RTCfg<N>::n, RS = RTCfg<N>::RS, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT;
+  constexpr int R_ = n / RS, T = RTCfg<N>::T;
+  extern __shared__ double smem_raw[];
+  AddSmem<N>& S = *reinterpret_cast<AddSmem<N>*>(smem_raw);
+  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R_;
+  const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
+  const int nunits = b.ncol * Fm;
+  if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
+  __shared__ int s_unit;
+  for (;;) {
+    team_sync();
+    if (t == 0) s_unit = atomicAdd(&w.counters[5 + (N == 8 ? 0 : (N == 16 ? 1 : 2))], 1);
+    team_sync();
+    const int unit = s_unit;
+    if (unit >= nunits) break;
+    const int c = unit / Fm, fi = unit % Fm;
+    if (fi >= b.col_nfreq(c) || b.col_nummu(c) != N) continue;
+    const int L = b.nlyrs[c];
+    const double freq = b.freq(c, fi);
+    const double wl = C_LIGHT / (freq * 1.e3);
+    const double* hl = w.hgt_lev + (size_t)c * (Lm + 1);
+    const double* tl = w.temp_lev + (size_t)c * (Lm + 1);
+    int status = 0;
+    if (w.col_status[c]) status |= w.col_status[c];
+    // stack buffers (roles swap by pointer)
+    double *Rp = S.m[0], *Rm = S.m[1], *Tp = S.m[2], *Tm = S.m[3];
+    double *R2 = S.m[4], *T2 = S.m[5];
+    double *G = S.m[6], *X = S.m[7], *Y = S.m[8], *Z = S.m[9];
+    // stack state: 0 empty, 1 clear (R = 0, T = diag t1, same both sides), 2 general
+    int sstate = 0;
+    for (int k = 0; k < L; k++) {  // top-down layer index
+      const int z = L - 1 - k;
+      const int pidx = w.pres_idx[(size_t)c * Lm + z];
+      const bool scat = pidx >= 0;
+      if (!scat) {
+        // NONSCATTER_LAYER4 (src/radintg4.f90:79-117)
+        if (t < n) {
+          const int jj = t >> 1, i = t & 1;
+          const double zdiff = fabs(hl[z + 1] - hl[z]);
+          const double gas = fmax(w.kgas[((size_t)c * Fm + fi) * Lm + z], 0.0);
+          const double dtau = zdiff * gas;
+          const double p0 = planck(tl[z + 1], wl), p1 = planck(tl[z], wl);
+          S.t2[t] = exp(-dtau / S.mu[jj]);
+          double a = 0.0, bq = 0.0;
+          if (dtau > 0.0 && i == 0) {
+            const double path = dtau / S.mu[jj];
+            const double slope = (p1 - p0) / path;
+            a = p1 - slope - (p1 - slope * (1.0 + path)) * exp(-path);
+            bq = p0 + slope - (p0 + slope * (1.0 + path)) * exp(-path);
+          }
+          S.s2p[t] = a;
+          S.s2m[t] = bq;
+        }
+        team_sync();
+        if (sstate == 0) {
+          if (t < n) { S.t1[t] = S.t2[t]; S.sp[t] = S.s2p[t]; S.sm[t] = S.s2m[t]; }
+          sstate = 1;
+        } else if (sstate == 1) {
+          if (t < n) {
+            const double sp = S.s2p[t] + S.t2[t] * S.sp[t];
+            const double sm = S.sm[t] + S.t1[t] * S.s2m[t];
+            S.t1[t] = S.t2[t] * S.t1[t];
+            S.sp[t] = sp;
+            S.sm[t] = sm;
+          }
+        } else {
+          // general stack + clear layer
+          double nsp = 0.0, nsm = 0.0;
+          if (t < n) {
+            nsp = S.s2p[t] + S.t2[t] * (S.sp[t] + mvr<n, RS>(Rp, S.s2m, t));
+            nsm = S.sm[t] + mvr<n, RS>(Tm, S.s2m, t);
+          }
+          team_sync();  // all reads of the old R+, T- done before the in-place updates
+          const double t2j = S.t2[j];
+          for (int ii = 0; ii < R_; ii++) {
+            const int row = r0 + ii;
+            const double t2i = S.t2[row];
+            Rp[j * LD + row] = t2i * (Rp[j * LD + row] * t2j);
+            Tp[j * LD + row] = t2i * Tp[j * LD + row];
+            Tm[j * LD + row] = Tm[j * LD + row] * t2j;
+          }
+          team_sync();
+          if (t < n) { S.sp[t] = nsp; S.sm[t] = nsm; }
+        }
+        team_sync();
+        continue;
+      }
+      // scattering layer: fetch R2, T2, S2 from the arena
+      {
+        const double* src = w.lay + ((size_t)pidx * Fm + fi) * w.lay_stride;
+        for (int e = t; e < MAT; e += T) { R2[e] = src[e]; T2[e] = src[MAT + e]; }
+        for (int e = t; e < n; e += T) { S.s2p[e] = src[2 * MAT + e]; S.s2m[e] = src[2 * MAT + n + e]; }
+      }
+      team_sync();
+      if (sstate == 0) {
+        // stack := layer
+        for (int e = t; e < MAT; e += T) { Rp[e] = R2[e]; Rm[e] = R2[e]; Tp[e] = T2[e]; Tm[e] = T2[e]; }
+        if (t < n) { S.sp[t] = S.s2p[t]; S.sm[t] = S.s2m[t]; }
+        sstate = 2;
+        team_sync();
+        continue;
+      }
+      if (sstate == 1) {
+        // clear stack (t1, sp, sm) + scattering layer
+        double nsp = 0.0, nsm = 0.0;
+        if (t < n) {
+          nsp = S.s2p[t] + mvr<n, RS>(T2, S.sp, t);
+          nsm = S.sm[t] + S.t1[t] * (S.s2m[t] + mvr<n, RS>(R2, S.sp, t));
+        }
+        const double t1j = S.t1[j];
+        for (int ii = 0; ii < R_; ii++) {
+          const int row = r0 + ii;
+          const double t1i = S.t1[row];
+          const double r2 = R2[j * LD + row], tt = T2[j * LD + row];
+          Rp[j * LD + row] = r2;
+          Rm[j * LD + row] = t1i * (r2 * t1j);
+          Tp[j * LD + row] = tt * t1j;
+          Tm[j * LD + row] = t1i * tt;
+        }
+        team_sync();
+        if (t < n) { S.sp[t] = nsp; S.sm[t] = nsm; }
+        sstate = 2;
+        team_sync();
+        continue;
+      }
+      // ---- general COMBINE_LAYERS4 (src/radintg4.f90:447-513), R2p = R2m, T2p = T2m
+      mm<n, RS>(Rp, R2, X);  // GAMMAp = inv(I - R1p R2m)
+      team_sync();
+      mat_ident_minus<n, RS>(X);
+      team_sync();
+      if (ginv<n, RS>(X, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      { double* tp = G; G = X; X = tp; }
+      mm<n, RS>(Rp, T2, X);  // RTp = R2p + T2p G R1p T2m
+      team_sync();
+      mm<n, RS>(G, X, Y);
+      team_sync();
+      mm<n, RS>(T2, Y, X);
+      team_sync();
+      for (int ii = 0; ii < R_; ii++) Y[j * LD + r0 + ii] = R2[j * LD + r0 + ii] + X[j * LD + r0 + ii];  // new R+ in Y
+      mm<n, RS>(G, Tp, X);  // TTp = T2p G T1p
+      team_sync();
+      mm<n, RS>(T2, X, Z);  // new T+ in Z
+      // STp = S2p + T2p G (S1p + R1p S2m)
+      if (t < n) S.wv[t] = S.sp[t] + mvr<n, RS>(Rp, S.s2m, t);
+      team_sync();
+      if (t < n) S.wv2[t] = mvr<n, RS>(G, S.wv, t);
+      team_sync();
+      if (t < n) S.nsp[t] = S.s2p[t] + mvr<n, RS>(T2, S.wv2, t);
+      mm<n, RS>(R2, Rp, X);  // GAMMAm = inv(I - R2m R1p)
+      team_sync();
+      mat_ident_minus<n, RS>(X);
+      team_sync();
+      if (ginv<n, RS>(X, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      { double* tp = G; G = X; X = tp; }
+      mm<n, RS>(R2, Tp, X);  // RTm = R1m + T1m G R2m T1p
+      team_sync();
+      mm<n, RS>(G, X, Rp);  // old R+ is dead
+      team_sync();
+      mm<n, RS>(Tm, Rp, X);
+      team_sync();
+      for (int ii = 0; ii < R_; ii++) Rm[j * LD + r0 + ii] = Rm[j * LD + r0 + ii] + X[j * LD + r0 + ii];
+      mm<n, RS>(G, T2, X);  // TTm = T1m G T2m
+      team_sync();
+      mm<n, RS>(Tm, X, Tp);  // old T+ is dead; new T- in Tp buffer
+      // STm = S1m + T1m G (S2m + R2m S1p)
+      if (t < n) S.wv[t] = S.s2m[t] + mvr<n, RS>(R2, S.sp, t);
+      team_sync();
+      if (t < n) S.wv2[t] = mvr<n, RS>(G, S.wv, t);
+      team_sync();
+      if (t < n) S.nsm[t] = S.sm[t] + mvr<n, RS>(Tm, S.wv2, t);
+      team_sync();
+      {
+        // roles: new R+ = Y, new R- = Rm, new T+ = Z, new T- = Tp
+        double *oRp = Rp, *oTm = Tm;
+        Rp = Y;
+        Tm = Tp;
+        Tp = Z;
+        Y = oRp;
+        Z = oTm;
+      }
+      if (t < n) { S.sp[t] = S.nsp[t]; S.sm[t] = S.nsm[t]; }
+      team_sync();
+    }
+    // materialise a clear stack
+    if (sstate == 1) {
+      mat_fill_diag<n, RS>(Tp, S.t1);
+      mat_fill_diag<n, RS>(Tm, S.t1);
+      for (int e = t; e < MAT; e += T) { Rp[e] = 0.0; Rm[e] = 0.0; }
+      team_sync();
+    }
+    // surface (src/sfc_matrices.f90; default emissivity sfc_optics.f90:79-81)
+    // and sky (src/surface.f90:169-195)
+    const char refl = (char)b.sfc_refl[c];
+    const double e = st.emissivity, rr = 1.0 - e;
+    const double pg = planck(w.gtemp[c], wl), psky = planck(SKY_TEMP, wl);
+    // R2 := surface R- (R+ = 0), T2 := I
+    for (int ii = 0; ii < R_; ii++) {
+      const int row = r0 + ii;
+      double v = 0.0;
+      if (refl == 'S' || refl == 'F') {
+        const double r1 = (rr + rr) / 2.0, r2 = (rr - rr) / 2.0;
+        if ((row >> 1) == (j >> 1)) v = ((row & 1) == (j & 1)) ? r1 : r2;
+      } else if (refl == 'L') {
+        if ((row & 1) == 0 && (j & 1) == 0) v = 2.0 * rr * S.mu[j >> 1] * S.wq[j >> 1];
+      }
+      R2[j * LD + row] = v;
+      T2[j * LD + row] = (row == j) ? 1.0 : 0.0;
+    }
+    if (refl != 'S' && refl != 'F' && refl != 'L') status |= PAMTRA_B200_WARNING;
+    if (t < n) {
+      const int i = t & 1;
+      double gv = 0.0;
+      if (refl == 'S' || refl == 'F') {
+        const double r1 = (rr + rr) / 2.0, r2 = (rr - rr) / 2.0;
+        gv = (i == 0) ? (1.0 - r1) * pg : -r2 * pg;
+      } else if (refl == 'L') {
+        gv = (i == 0) ? e * pg : 0.0;
+      }
+      S.gnd[t] = gv;
+      S.sky[t] = (i == 0) ? (1.0 - 0.0) * psky : 0.0;
+    }
+    team_sync();
+    // output levels: level L+1 uses (stack, surface); level 1 uses (empty, stack+surface)
+    int lev_order[2] = {-1, -1};
+    int nlev = 0;
+    for (int io = 0; io < b.noutlevels; io++) {
+      const int lev = w.outlev[(size_t)c * b.noutlevels + io];
+      if (lev == L + 1) lev_order[0] = io;
+      else if (lev == 1) lev_order[1] = io;
+      else status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;  // intermediate levels not supported
+      nlev++;
+    }
+    (void)nlev;
+    for (int pass = 0; pass < 2; pass++) {
+      const int io = lev_order[pass];
+      if (pass == 1 && io >= 0) {
+        // down stack for level 1: (stack) on top of (surface), minus side only
+        mm<n, RS>(R2, Rp, X);  // GAMMAm = inv(I - Rsfc R1p)
+        team_sync();
+        mat_ident_minus<n, RS>(X);
+        team_sync();
+        if (ginv<n, RS>(X, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+        { double* tp = G; G = X; X = tp; }
+        mm<n, RS>(R2, Tp, X);
+        team_sync();
+        mm<n, RS>(G, X, Y);
+        team_sync();
+        mm<n, RS>(Tm, Y, X);
+        team_sync();
+        for (int ii = 0; ii < R_; ii++) Rm[j * LD + r0 + ii] = Rm[j * LD + r0 + ii] + X[j * LD + r0 + ii];
+        mm<n, RS>(G, T2, X);
+        team_sync();
+        mm<n, RS>(Tm, X, Y);  // new T- in Y
+        if (t < n) S.wv[t] = 0.0 + mvr<n, RS>(R2, S.sp, t);
+        team_sync();
+        if (t < n) S.wv2[t] = mvr<n, RS>(G, S.wv, t);
+        team_sync();
+        if (t < n) S.nsm[t] = S.sm[t] + mvr<n, RS>(Tm, S.wv2, t);
+        team_sync();
+        { double* tp = Tm; Tm = Y; Y = tp; }
+        if (t < n) S.sm[t] = S.nsm[t];
+        // up side: empty stack -> R+ = 0, T+ = I, S+ = 0; reuse Rp/Tp/sp
+        for (int ii = 0; ii < R_; ii++) {
+          const int row = r0 + ii;
+          Rp[j * LD + row] = 0.0;
+          Tp[j * LD + row] = (row == j) ? 1.0 : 0.0;
+        }
+        if (t < n) S.sp[t] = 0.0;
+        // down side: R2 := new R-, T2 := new T-, s2m := sm
+        for (int e2 = t; e2 < MAT; e2 += T) { R2[e2] = Rm[e2]; T2[e2] = Tm[e2]; }
+        if (t < n) S.s2m[t] = S.sm[t];
+        team_sync();
+      } else if (pass == 0) {
+        if (t < n) S.s2m[t] = 0.0;  // surface source is zero
+        team_sync();
+      }
+      if (io < 0) continue;
+      // INTERNAL_RADIANCE4 (src/radintg4.f90:119-172): up = (Rp, Tp, sp), down = (R2, T2, s2m)
+      mm<n, RS>(Rp, R2, X);
+      team_sync();
+      mat_ident_minus<n, RS>(X);
+      team_sync();
+      if (ginv<n, RS>(X, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      if (t < n) S.wv[t] = mvr<n, RS>(T2, S.gnd, t);
+      team_sync();
+      if (t < n) {
+        double s = mvr<n, RS>(Rp, S.wv, t);
+        s = mvr<n, RS>(Tp, S.sky, t) + s;
+        s = mvr<n, RS>(Rp, S.s2m, t) + s;
+        s = S.sp[t] + s;
+        S.wv2[t] = s;
+      }
+      team_sync();
+      if (t < n) S.dnrad[t] = mvr<n, RS>(X, S.wv2, t);
+      team_sync();
+      mm<n, RS>(R2, Rp, X);
+      team_sync();
+      mat_ident_minus<n, RS>(X);
+      team_sync();
+      if (ginv<n, RS>(X, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      if (t < n) S.wv[t] = mvr<n, RS>(Tp, S.sky, t);
+      team_sync();
+      if (t < n) {
+        double s = mvr<n, RS>(R2, S.wv, t);
+        s = mvr<n, RS>(T2, S.gnd, t) + s;
+        s = mvr<n, RS>(R2, S.sp, t) + s;
+        s = S.s2m[t] + s;
+        S.wv2[t] = s;
+      }
+      team_sync();
+      if (t < n) S.uprad[t] = mvr<n, RS>(X, S.wv2, t);
+      team_sync();
+      // collect_output + CONVERT_OUTPUT
+      if (t < N) {
+        const int jj = t;
+        double u0 = S.uprad[2 * jj], u1 = S.uprad[2 * jj + 1], d0 = S.dnrad[2 * jj], d1 = S.dnrad[2 * jj + 1];
+        if (st.outpol_vh) {
+          double iv = 0.5 * (u0 + u1), ih = 0.5 * (u0 - u1);
+          u0 = iv; u1 = ih;
+          iv = 0.5 * (d0 + d1); ih = 0.5 * (d0 - d1);
+          d0 = iv; d1 = ih;
+          u0 = 2.0 * u0; u1 = 2.0 * u1; d0 = 2.0 * d0; d1 = 2.0 * d1;
+        }
+        const int NA = 2 * b.max_nummu;
+        double* tbo = out.tb + ((size_t)c * b.noutlevels + io) * NA * Fm * 2;
+        const size_t up_i = ((size_t)(N - 1 - jj) * Fm + fi) * 2, dn_i = ((size_t)(N + jj) * Fm + fi) * 2;
+        tbo[up_i + 0] = rad_to_tb(u0, wl);
+        tbo[up_i + 1] = rad_to_tb(u1, wl);
+        tbo[dn_i + 0] = rad_to_tb(d0, wl);
+        tbo[dn_i + 1] = rad_to_tb(d1, wl);
+      }
+      team_sync();
+    }
+    if (t == 0) {
+      if (out.emissivity)
+        for (int i = 0; i < 2; i++)
+          for (int jj = 0; jj < N; jj++) out.emissivity[(((size_t)c * 2 + i) * Fm + fi) * b.max_nummu + jj] = e;
+      if (status) atomicOr(&w.status[(size_t)c * Fm + fi], status);
+    }
+  }
+}
+
+}  // namespace pb

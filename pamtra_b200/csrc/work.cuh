@@ -1,0 +1,76 @@
+// Device-side views of a batch (inputs) and of the scratch arena.
+#pragma once
+#include "common.cuh"
+
+namespace pb {
+
+// Inputs of one batch; copies of the pamtra_b200_columns pointers plus the
+// padded sizes.  Passed by value to kernels.
+struct Batch {
+  int ncol, max_nlyrs, nhydro, max_nfreq, noutlevels, max_nummu, max_nbin, species_stride;
+  int default_nummu;
+  const pamtra_b200_species* species;
+  const int* nlyrs;
+  const int* nummu;
+  const int* nfreq;
+  const double* freqs;
+  int freq_per_col;
+  const double *hgt_lev, *temp_lev, *press_lev, *relhum_lev;
+  const double *hgt, *temp, *press, *relhum;
+  const double *hydro_q, *hydro_n, *hydro_reff;
+  const double* groundtemp;
+  const double* obs_height;
+  const int8_t* sfc_refl;
+
+  __device__ __forceinline__ int col_nfreq(int c) const { return nfreq ? nfreq[c] : max_nfreq; }
+  __device__ __forceinline__ double freq(int c, int f) const {
+    return freq_per_col ? freqs[(size_t)c * max_nfreq + f] : freqs[f];
+  }
+  __device__ __forceinline__ int col_nummu(int c) const { return nummu ? nummu[c] : default_nummu; }
+  __device__ __forceinline__ pamtra_b200_species species_of(int c, int h) const {
+    return species[(size_t)c * species_stride + h];
+  }
+};
+
+// Scratch arena views.  Index conventions:
+//   column-level  [c][...]
+//   slot          s = (c*Lm + z)*H + h
+//   present layer p (compact), unit-layer item i = p*Fm + f
+struct Work {
+  // atmosphere
+  double *hgt_lev, *temp_lev;          // [C][Lm+1]
+  double *temp, *press, *rho_vap, *q_hum;  // [C][Lm]
+  double* gtemp;                       // [C]
+  int* outlev;                         // [C][nout]
+  double* kgas;                        // [C][Fm][Lm]
+  // size distributions
+  int8_t* slot_st;                     // [S] 0 absent, 1 present w/o bins, 2 bins, 3 fatal
+  int* slot_nb;                        // [S]
+  double *b_d, *b_dd, *b_nd, *b_rho, *b_mass;  // [S][max_nbin]
+  // compaction
+  int* pres_idx;                       // [C][Lm]
+  int* plist;                          // [pmax]
+  int pmax;
+  int* counters;                       // [16] 0: P, 1: mie work, 2: rt work, 3: adding work
+  // single-scattering per item
+  double *m_kext, *m_salb;             // [pmax*Fm]
+  int* m_nleg;                         // [pmax*Fm]
+  double* m_legen;                     // [pmax*Fm][3][MAXNLEG]
+  // layer R, T, S per item (R,T padded n x (n+2), symmetric +/-)
+  double* lay;                         // [pmax*Fm][lay_stride]
+  size_t lay_stride;
+  int* lay_nd;                         // [pmax*Fm]
+  // status
+  int* status;                         // [C][Fm]
+  int* col_status;                     // [C]
+  // quadrature tables
+  const double* gq_x;                  // Gauss-Legendre nodes, packed: nquad=q at offset q*(q-1)/2
+  const double* gq_w;
+  int gq_max;
+  const double* lob_mu;                // Lobatto nodes for N = 8,16,32 at offsets 0, 8, 24
+  const double* lob_w;
+};
+
+__host__ __device__ __forceinline__ int lob_off(int N) { return N == 8 ? 0 : (N == 16 ? 8 : 24); }
+
+}  // namespace pb
