@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 passive forward path.
+
+Metric: column x frequency solves per second (one solve = gas + PSD + Mie +
+scatcnv + RT4 + TB for one column at one frequency).
+
+Default workload (the batched FP64 configuration): 4096 seeded columns of 50
+layers over 0-12 km, cloud liquid (exp, 40 bins) and rain (Marshall-Palmer,
+50 bins) in layers 5-25 with mixing ratios log-uniform over 0.01-2 g/kg,
+frequencies 23.8, 31.4, 89 and 150 GHz, NUMMU = 16, FP64.
+
+  value  : batched solves/s with inputs resident in HBM (device-timed,
+           CUDA events on the launching stream, L2 flushed between steps)
+  e2e    : same metric through the C ABI with host buffers (pinned), the
+           host<->device copies inside the timed region
+  plain  : the plain form (one column per call) on a sample of columns
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Under torchrun each rank runs its own columns (weak scaling, no collective on
+the data path); rank 0 prints one JSON line.
+"""
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FREQS = [23.8, 31.4, 89.0, 150.0]
+METRIC = "column*freq solves/s"
+
+
+def _args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--ncol", type=int, default=4096)
+    ap.add_argument("--cpu-sample", type=int, default=0, help="columns for the CPU baseline (0 = 2 per core)")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def _config(ncol):
+    return {"workload": "batched FP64: %d columns x 50 layers (0-12 km), 2 Mie species (cloud exp 40 bins, "
+                        "rain Marshall-Palmer 50 bins) in layers 5-25, q log-uniform 0.01-2 g/kg, "
+                        "f = 23.8/31.4/89/150 GHz, NUMMU=16" % ncol,
+            "columns_per_gpu": ncol, "layers": 50, "frequencies": FREQS, "nummu": 16,
+            "l2": "flushed between timed steps (256 MiB write)"}
+
+
+# ---------------------------------------------------------------- CPU baseline
+def _oracle_chunk(task):
+    st_fields, species, cols, idxs, freqs = task
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    st = oracle.OrcSettings(**st_fields)
+    out = []
+    t0 = time.perf_counter()
+    for c in idxs:
+        err, tb, _, _, _ = oracle.run_column(st, species, cols, c, freqs)
+        out.append((c, err, tb))
+    return out, time.perf_counter() - t0
+
+
+def make_pool(cores):
+    """Worker processes (spawned, so no CUDA state is inherited), warmed up
+    outside any timed region."""
+    import multiprocessing as mp
+    pool = mp.get_context("spawn").Pool(cores)
+    pool.map(_warm, range(cores))
+    return pool
+
+
+def _warm(_):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    oracle.lib()
+    return 0
+
+
+def cpu_baseline(batch, idxs, freqs, cores, pool):
+    """Time the oracle (C++ restatement of the reference) on host cores,
+    one single-threaded worker per core (the reference's runParallelPamtra
+    process model)."""
+    st_fields = {k: getattr(batch.settings, k) for k, _ in batch.settings._fields_}
+    cols = {k: (v[idxs] if isinstance(v, np.ndarray) and v.ndim >= 1 and v.shape[0] == batch.ncol else v)
+            for k, v in batch.host.items()}
+    local = list(range(len(idxs)))
+    chunks = [local[i::cores] for i in range(cores)]
+    tasks = [(st_fields, batch.species, cols, ch, freqs) for ch in chunks if ch]
+    t0 = time.perf_counter()
+    res = pool.map(_oracle_chunk, tasks)
+    wall = time.perf_counter() - t0
+    tbs = {}
+    for out, _ in res:
+        for c, err, tb in out:
+            tbs[idxs[c]] = tb
+    return len(idxs) * len(freqs) / wall, wall, tbs
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler(object):
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def fp64_peak_tflops(dev):
+    """Measured FP64 throughput of cuBLAS DGEMM on this GPU (the roofline
+    denominator for FP64 kernels; the driver's peak file carries bf16 only)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    for _ in range(2):
+        torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 0.0
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2.0 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def layer_flops(nd, N):
+    """Algorithmic FLOPs of the doubling stage: per scattering layer and
+    frequency, each doubling is 6 n x n products and one inverse (2 n^3
+    each), n = 2N."""
+    n = 2 * N
+    d = nd[nd > 0].astype(np.float64)
+    return float(np.sum(d) * 7 * 2 * n ** 3)
+
+
+# ---------------------------------------------------------------- reference arm
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import warnings
+    warnings.simplefilter("ignore")
+    from pamtra_b200 import batch as pbatch
+    from pamtra_b200.workloads import c2_pam
+    cores = os.cpu_count() or 1
+    ncol = min(args.ncol, 512)
+    b = pbatch.pack_pam(c2_pam(ncol), FREQS)
+    per_step = max(1, 4 * cores) if not args.cpu_sample else args.cpu_sample
+    rng = np.random.default_rng(0)
+    vals = []
+    pool = make_pool(cores)
+    for step in range(args.warmup + args.steps):
+        idxs = sorted(rng.choice(ncol, size=min(per_step, ncol), replace=False).tolist())
+        v, wall, _ = cpu_baseline(b, idxs, FREQS, cores, pool)
+        if step >= args.warmup:
+            vals.append((len(idxs) * len(FREQS), wall))
+    pool.close()
+    solves = sum(s for s, _ in vals)
+    wall = sum(w for _, w in vals)
+    value = solves / wall
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / len(vals),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded)", "config": _config(args.ncol),
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": "%d random columns x %d frequencies per step of the same workload; "
+                                       "C++ FP64 restatement of the reference Fortran (no Fortran compiler "
+                                       "on this image)" % (per_step, len(FREQS))},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- our arm
+def main():
+    args = _args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import warnings
+    warnings.simplefilter("ignore")
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    from pamtra_b200 import batch as pbatch
+    from pamtra_b200 import build as pbuild
+    from pamtra_b200._native import Engine
+    from pamtra_b200.workloads import c2_pam
+    pbuild.build()
+    eng = Engine(local)
+    b = pbatch.pack_pam(c2_pam(args.ncol, seed=2 + rank), FREQS)
+    stream = torch.cuda.Stream(dev)
+    out = b.alloc_outputs(dev, ssp=True)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            pbatch.run(b, local, out, stream=stream, eng=eng)
+    stream.synchronize()
+    status = out["status"].cpu().numpy()
+    nd = out["num_doubles"].cpu().numpy()
+    nlaunch = eng.last_launch_count()
+    # ---- device-timed batched steps
+    eng.set_timing(True)
+    stage_tot = {}
+    times = []
+    sampler = ClockSampler(local)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            pbatch.run(b, local, out, stream=stream, eng=eng)
+            e.record(stream)
+        e.synchronize()
+        times.append(s.elapsed_time(e))
+        for k, v in eng.stage_ms().items():
+            stage_tot[k] = stage_tot.get(k, 0.0) + v
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    eng.set_timing(False)
+    t_total = sum(times) * 1e-3
+    if dist is not None:
+        tt = torch.tensor([t_total], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_total = float(tt.item())
+    solves_step = b.n_solves()
+    value = world * solves_step * args.steps / t_total
+    # ---- end-to-end through the C ABI with host buffers
+    hout = b.alloc_outputs(None, pinned=True)
+    pbatch.run_host(b, local, hout, eng=eng)
+    e2e_t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        pbatch.run_host(b, local, hout, eng=eng)
+        e2e_t.append(time.perf_counter() - t0)
+    e2e_total = sum(e2e_t)
+    if dist is not None:
+        tt = torch.tensor([e2e_total], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_total = float(tt.item())
+    h2d = sum(v.nbytes for v in b.host.values() if isinstance(v, np.ndarray))
+    d2h = sum(v.nbytes for v in hout.values())
+    # ---- plain form: one column per call
+    nplain = 32
+    plain_batches = [pbatch.pack_pam(c2_pam(1, seed=1000 + i), FREQS) for i in range(nplain)]
+    pouts = [pb_.alloc_outputs(dev) for pb_ in plain_batches]
+    with torch.cuda.stream(stream):
+        for pb_, po in zip(plain_batches, pouts):
+            pbatch.run(pb_, local, po, stream=stream, eng=eng)
+    stream.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        s.record(stream)
+        for pb_, po in zip(plain_batches, pouts):
+            pbatch.run(pb_, local, po, stream=stream, eng=eng)
+        e.record(stream)
+    e.synchronize()
+    plain_value = nplain * len(FREQS) / (s.elapsed_time(e) * 1e-3)
+
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+    # ---- roofline of the dominant kernel (doubling stage)
+    peak = fp64_peak_tflops(dev)
+    t_layer = stage_tot.get("layer", 0.0) / args.steps * 1e-3
+    flops = layer_flops(nd, 16)
+    achieved = flops / t_layer / 1e12 if t_layer > 0 else 0.0
+    roofline = {"bound": "fp64", "kernel": "k_layer<16> (scatcnv + init + doubling)", "achieved": achieved,
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 pipe)",
+                "flops_per_launch": flops, "kernel_ms": t_layer * 1e3}
+    # ---- CPU baseline + TB error vs the oracle on the same columns
+    cpu = None
+    tb_err = None
+    if not args.no_cpu:
+        cores = os.cpu_count() or 1
+        nsamp = args.cpu_sample or min(b.ncol, 8 * cores)
+        idxs = sorted(np.random.default_rng(7).choice(b.ncol, size=nsamp, replace=False).tolist())
+        pool = make_pool(cores)
+        cval, wall, tbs = cpu_baseline(b, idxs, FREQS, cores, pool)
+        pool.close()
+        tb_gpu = out["tb"].cpu().numpy()
+        tb_err = max(float(np.max(np.abs(tb_gpu[c] - tbs[c]))) for c in idxs)
+        cpu = {"value": cval, "unit": "solves/s", "cores": cores, "kind": "port",
+               "sample": "%d random columns x %d frequencies of the same workload, one worker process per core; "
+                         "C++ FP64 restatement of the reference Fortran (no Fortran compiler on this image)"
+                         % (nsamp, len(FREQS))}
+    line = {
+        "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
+        "config": _config(args.ncol),
+        "e2e": {"value": world * solves_step * args.steps / e2e_total, "unit": "solves/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(nlaunch * args.steps),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "plain_fp64": {"value": plain_value, "unit": "solves/s", "form": "one column per call, FP64"},
+        "batched_over_plain": value / world / plain_value,
+        "tb_err_vs_oracle_K": tb_err,
+        "stage_ms": {k: v / args.steps for k, v in stage_tot.items()},
+        "status_nonzero": int(np.count_nonzero(status)),
+    }
+    print(json.dumps(line))
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

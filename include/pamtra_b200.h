@@ -154,6 +154,19 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
 /* Number of kernel launches the last pamtra_b200_run issued on ctx. */
 int32_t pamtra_b200_last_launch_count(const pamtra_b200_ctx* ctx);
 
+/* Per-stage timing (the reference only prints total runtime, core.py:1567).
+ * When enabled, pamtra_b200_run records CUDA events between its stages on
+ * its stream; pamtra_b200_stage_ms waits for the last run and returns
+ * milliseconds per stage: [0] pre-processing + gas + outputs, [1] size
+ * distributions, [2] Mie, [3] layer doubling, [4] adding + radiance. */
+#define PAMTRA_B200_NSTAGES 5
+int32_t pamtra_b200_set_timing(pamtra_b200_ctx* ctx, int32_t enable);
+int32_t pamtra_b200_stage_ms(pamtra_b200_ctx* ctx, float* ms, int32_t n);
+
+/* sizeof of the ABI structs, in order settings, species, columns, outputs
+ * (for bindings to check their struct layouts). */
+int32_t pamtra_b200_abi_sizes(size_t* out, int32_t n);
+
 /* ---- single-stage entry points (parity tests of individual routines) ---- */
 
 /* Rosenkranz-98 absorption (src/rosen98_gasabs.f90:2 + get_gasabs.f90:95),

@@ -49,7 +49,9 @@ class Outputs(ctypes.Structure):
 
 EXPORTS = ["pamtra_b200_create", "pamtra_b200_destroy", "pamtra_b200_workspace_bytes", "pamtra_b200_reserve",
            "pamtra_b200_run", "pamtra_b200_run_host", "pamtra_b200_last_launch_count", "pamtra_b200_gas_r98",
-           "pamtra_b200_eps_water_tkc", "pamtra_b200_minvert_batched"]
+           "pamtra_b200_eps_water_tkc", "pamtra_b200_minvert_batched", "pamtra_b200_set_timing",
+           "pamtra_b200_stage_ms", "pamtra_b200_abi_sizes"]
+STAGES = ["prep", "psd", "mie", "layer", "adding"]
 
 _lib = None
 
@@ -80,6 +82,12 @@ def load():
         l.pamtra_b200_eps_water_tkc.argtypes = [_vp] * 4 + [_i32, _vp]
         l.pamtra_b200_minvert_batched.restype = _i32
         l.pamtra_b200_minvert_batched.argtypes = [_vp, _vp, _vp, _i32, _i32, _vp]
+        l.pamtra_b200_set_timing.restype = _i32
+        l.pamtra_b200_set_timing.argtypes = [_vp, _i32]
+        l.pamtra_b200_stage_ms.restype = _i32
+        l.pamtra_b200_stage_ms.argtypes = [_vp, ctypes.POINTER(ctypes.c_float), _i32]
+        l.pamtra_b200_abi_sizes.restype = _i32
+        l.pamtra_b200_abi_sizes.argtypes = [ctypes.POINTER(ctypes.c_size_t), _i32]
         _lib = l
     return _lib
 
@@ -169,6 +177,22 @@ class Engine(object):
 
     def last_launch_count(self):
         return int(self.lib.pamtra_b200_last_launch_count(self.handle))
+
+    def set_timing(self, on):
+        self.lib.pamtra_b200_set_timing(self.handle, int(bool(on)))
+
+    def stage_ms(self):
+        """Milliseconds per stage of the last run (needs set_timing(True))."""
+        buf = (ctypes.c_float * len(STAGES))()
+        self.lib.pamtra_b200_stage_ms(self.handle, buf, len(STAGES))
+        return dict(zip(STAGES, [float(v) for v in buf]))
+
+
+def abi_sizes():
+    """(settings, species, columns, outputs) struct sizes as compiled."""
+    buf = (ctypes.c_size_t * 4)()
+    load().pamtra_b200_abi_sizes(buf, 4)
+    return tuple(int(v) for v in buf)
 
 
 _engines = {}

@@ -189,9 +189,7 @@ struct Plan {
 };
 
 size_t lay_stride_for(int N) {
-  int n = 2 * N;
-  size_t s = 2 * (size_t)n * (n + 2) + 2 * n;
-  return (s + 1) & ~(size_t)1;  // keep 16-byte alignment of each item
+  return (lay_stride_n(N) + 1) & ~(size_t)1;  // keep 16-byte alignment of each item
 }
 
 Plan make_plan(const pamtra_b200_columns* c, int default_nummu) {
@@ -265,19 +263,18 @@ __global__ void k_gas_elem(const double* f, const double* T, const double* rv, c
 
 template <int n>
 __global__ void k_minvert(const double* a, double* ainv, int32_t* status, int count) {
-  constexpr int RS = (n >= 64) ? 2 : 1;
-  constexpr int LD = TeamCfg<n, RS>::LD, R = TeamCfg<n, RS>::R;
-  __shared__ double M[n * LD];
-  __shared__ double f[n], redv[8];
-  __shared__ int piv[n], redi[8 + n];
-  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R;
+  constexpr int LD = Team<n>::LD, T = Team<n>::T;
+  extern __shared__ double smem_raw[];
+  double* M = smem_raw;
+  InvScratch<n>& S = *reinterpret_cast<InvScratch<n>*>(smem_raw + n * LD);
+  const int t = threadIdx.x;
   for (int m = blockIdx.x; m < count; m += gridDim.x) {
     const double* src = a + (size_t)m * n * n;
-    for (int ii = 0; ii < R; ii++) M[j * LD + r0 + ii] = src[(size_t)j * n + r0 + ii];
+    for (int e = t; e < n * n; e += T) M[(e / n) * LD + e % n] = src[e];
     __syncthreads();
-    int s = ginv<n, RS>(M, f, piv, redv, redi);
+    int s = ginv<n>(M, S);
     double* dst = ainv + (size_t)m * n * n;
-    for (int ii = 0; ii < R; ii++) dst[(size_t)j * n + r0 + ii] = M[j * LD + r0 + ii];
+    for (int e = t; e < n * n; e += T) dst[e] = M[(e / n) * LD + e % n];
     if (status && t == 0) status[m] = s ? (PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT) : 0;
     __syncthreads();
   }
@@ -299,7 +296,22 @@ struct pamtra_b200_ctx {
   int last_launches = 0;
   char* stage = nullptr;  // device staging for run_host
   size_t stage_bytes = 0;
+  // optional per-stage timing (events recorded on the run's stream)
+  int timing = 0;
+  cudaEvent_t ev[16] = {};
+  int nev = 0;
+  int ev_stage[16] = {};
 };
+
+enum Stage { STG_PREP = 0, STG_PSD, STG_MIE, STG_LAYER, STG_ADDING, STG_COUNT };
+
+static void mark(pamtra_b200_ctx* ctx, cudaStream_t s, int stage) {
+  if (!ctx->timing || ctx->nev >= 16) return;
+  if (!ctx->ev[ctx->nev]) cudaEventCreate(&ctx->ev[ctx->nev]);
+  cudaEventRecord(ctx->ev[ctx->nev], s);
+  ctx->ev_stage[ctx->nev] = stage;
+  ctx->nev++;
+}
 
 static int set_smem_attrs() {
   static std::once_flag once;
@@ -314,6 +326,7 @@ static int set_smem_attrs() {
     set((const void*)k_layer<32>, sizeof(LayerSmem<32>));
     set((const void*)k_adding<8>, sizeof(AddSmem<8>));
     set((const void*)k_adding<16>, sizeof(AddSmem<16>));
+    set((const void*)k_minvert<64>, Team<64>::MAT * 8 + sizeof(InvScratch<64>));
   });
   return rc;
 }
@@ -334,6 +347,17 @@ int32_t pamtra_b200_create(int32_t device, pamtra_b200_ctx** out) {
     return PAMTRA_B200_FATAL;
   }
   k_gauss_table<<<GQ_MAX, 128>>>(ctx->gq_x, ctx->gq_w);
+  {
+    double la[MAXNLEG], lb[MAXNLEG];
+    la[0] = 0.0;
+    lb[0] = 0.0;
+    for (int l = 1; l < MAXNLEG; l++) {
+      la[l] = (2.0 * l - 1.0) / l;
+      lb[l] = (l - 1.0) / l;
+    }
+    cudaMemcpyToSymbol(c_leg_a, la, sizeof(la));
+    cudaMemcpyToSymbol(c_leg_b, lb, sizeof(lb));
+  }
   k_lobatto_table<<<3, 32>>>(ctx->lob_mu, ctx->lob_w);
   cudaMemcpyToSymbol(c_o2_w300, H_O2_W300, sizeof(H_O2_W300));
   cudaMemcpyToSymbol(c_o2_y300, H_O2_Y300, sizeof(H_O2_Y300));
@@ -366,6 +390,8 @@ int32_t pamtra_b200_destroy(pamtra_b200_ctx* ctx) {
   cudaFree(ctx->lob_w);
   cudaFree(ctx->stage);
   if (ctx->h_species) cudaFreeHost(ctx->h_species);
+  for (int i = 0; i < 16; i++)
+    if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
   delete ctx;
   return PAMTRA_B200_OK;
 }
@@ -389,6 +415,33 @@ int32_t pamtra_b200_reserve(pamtra_b200_ctx* ctx, size_t bytes) {
 }
 
 int32_t pamtra_b200_last_launch_count(const pamtra_b200_ctx* ctx) { return ctx ? ctx->last_launches : 0; }
+
+int32_t pamtra_b200_abi_sizes(size_t* out, int32_t n) {
+  const size_t sz[4] = {sizeof(pamtra_b200_settings), sizeof(pamtra_b200_species), sizeof(pamtra_b200_columns),
+                        sizeof(pamtra_b200_outputs)};
+  for (int i = 0; i < n && i < 4; i++) out[i] = sz[i];
+  return PAMTRA_B200_OK;
+}
+
+int32_t pamtra_b200_set_timing(pamtra_b200_ctx* ctx, int32_t enable) {
+  if (!ctx) return PAMTRA_B200_FATAL;
+  ctx->timing = enable ? 1 : 0;
+  return PAMTRA_B200_OK;
+}
+
+int32_t pamtra_b200_stage_ms(pamtra_b200_ctx* ctx, float* ms, int32_t n) {
+  if (!ctx || !ms) return PAMTRA_B200_FATAL;
+  for (int i = 0; i < n; i++) ms[i] = 0.f;
+  if (ctx->nev < 2) return PAMTRA_B200_OK;
+  if (cudaEventSynchronize(ctx->ev[ctx->nev - 1]) != cudaSuccess) return PAMTRA_B200_FATAL;
+  for (int i = 1; i < ctx->nev; i++) {
+    float t = 0.f;
+    cudaEventElapsedTime(&t, ctx->ev[i - 1], ctx->ev[i]);
+    int st = ctx->ev_stage[i];
+    if (st >= 0 && st < n) ms[st] += t;
+  }
+  return PAMTRA_B200_OK;
+}
 
 int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, const pamtra_b200_columns* cols,
                         const pamtra_b200_outputs* out, int32_t precision, void* stream_) {
@@ -454,7 +507,9 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   w.gq_x = ctx->gq_x; w.gq_w = ctx->gq_w; w.gq_max = GQ_MAX; w.lob_mu = ctx->lob_mu; w.lob_w = ctx->lob_w;
 
   int launches = 0;
+  ctx->nev = 0;
   const size_t C = cc.ncol, Lm = cc.max_nlyrs, Fm = cc.max_nfreq, H = cc.nhydro;
+  mark(ctx, stream, -1);
   cudaMemsetAsync(w.counters, 0, 16 * 4, stream);
   cudaMemsetAsync(w.status, 0, C * Fm * 4, stream);
   cudaMemsetAsync(w.col_status, 0, C * 4, stream);
@@ -463,6 +518,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   k_atmo<<<(unsigned)((C + 127) / 128), 128, 0, stream>>>(b, w); launches++;
   const size_t ngas = C * Fm * Lm;
   k_gas<<<(unsigned)((ngas + 255) / 256), 256, 0, stream>>>(b, w, st->lgas_extinction); launches++;
+  mark(ctx, stream, STG_PREP);
   if (H > 0) {
     const size_t ns = C * Lm * H;
     k_psd<<<(unsigned)((ns + 127) / 128), 128, 0, stream>>>(b, w, *st); launches++;
@@ -470,24 +526,30 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     cudaMemsetAsync(w.slot_st, 0, 1, stream);
   }
   k_compact<<<1, 1024, 0, stream>>>(b, w); launches++;
+  mark(ctx, stream, STG_PSD);
   const int sms = ctx->sm_count;
   if (H > 0) {
     const size_t sm_mie = MIE_WARPS * sizeof(MieSmem);
     int g = occupancy_blocks((const void*)k_mie, 32 * MIE_WARPS, sm_mie, sms);
     k_mie<<<g, 32 * MIE_WARPS, sm_mie, stream>>>(b, w, *st); launches++;
   }
+  mark(ctx, stream, STG_MIE);
   double* ssp = out->scatter_matrix;
   if (mask & 1) {
     int g = occupancy_blocks((const void*)k_layer<8>, RTCfg<8>::T, sizeof(LayerSmem<8>), sms);
     if (H > 0) { k_layer<8><<<g, RTCfg<8>::T, sizeof(LayerSmem<8>), stream>>>(b, w, *st, ssp); launches++; }
+    mark(ctx, stream, STG_LAYER);
     g = occupancy_blocks((const void*)k_adding<8>, RTCfg<8>::T, sizeof(AddSmem<8>), sms);
     k_adding<8><<<g, RTCfg<8>::T, sizeof(AddSmem<8>), stream>>>(b, w, *st, *out); launches++;
+    mark(ctx, stream, STG_ADDING);
   }
   if (mask & 2) {
     int g = occupancy_blocks((const void*)k_layer<16>, RTCfg<16>::T, sizeof(LayerSmem<16>), sms);
     if (H > 0) { k_layer<16><<<g, RTCfg<16>::T, sizeof(LayerSmem<16>), stream>>>(b, w, *st, ssp); launches++; }
+    mark(ctx, stream, STG_LAYER);
     g = occupancy_blocks((const void*)k_adding<16>, RTCfg<16>::T, sizeof(AddSmem<16>), sms);
     k_adding<16><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out); launches++;
+    mark(ctx, stream, STG_ADDING);
   }
   if (out->angles_deg) { k_angles<<<1, 32, 0, stream>>>(out->angles_deg, ctx->lob_mu, cc.max_nummu); launches++; }
   if (out->kexttot || out->salbedo || out->num_doubles) {
@@ -497,6 +559,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   if (out->status) {
     k_status_out<<<(unsigned)((C * Fm + 255) / 256), 256, 0, stream>>>(w, out->status, (int)(C * Fm)); launches++;
   }
+  mark(ctx, stream, STG_PREP);
   ctx->last_launches = launches;
   return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
 }
@@ -620,9 +683,12 @@ int32_t pamtra_b200_minvert_batched(const double* a, double* ainv, int32_t* stat
   if (count <= 0) return PAMTRA_B200_OK;
   cudaStream_t s = (cudaStream_t)stream;
   const int g = std::min(count, 65535);
-  if (n == 16) k_minvert<16><<<g, 16, 0, s>>>(a, ainv, status, count);
-  else if (n == 32) k_minvert<32><<<g, 32, 0, s>>>(a, ainv, status, count);
-  else if (n == 64) k_minvert<64><<<g, 128, 0, s>>>(a, ainv, status, count);
+  if (n == 16)
+    k_minvert<16><<<g, Team<16>::T, Team<16>::MAT * 8 + sizeof(InvScratch<16>), s>>>(a, ainv, status, count);
+  else if (n == 32)
+    k_minvert<32><<<g, Team<32>::T, Team<32>::MAT * 8 + sizeof(InvScratch<32>), s>>>(a, ainv, status, count);
+  else if (n == 64)
+    k_minvert<64><<<g, Team<64>::T, Team<64>::MAT * 8 + sizeof(InvScratch<64>), s>>>(a, ainv, status, count);
   else return PAMTRA_B200_FATAL;
   return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
 }

@@ -83,133 +83,176 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 // ------------------------------------------------------------------ team linear algebra
-// A "team" is one CTA of T = n*RS threads working on n x n FP64 matrices held
-// in shared memory, column-major with leading dimension LD = n + 2 (even, so a
-// column is 16-byte aligned for vector loads; two-way bank conflicts at most
-// on strided column reads).  Thread t owns column t % n and the row block
-// [(t/n)*R, (t/n)*R + R), R = n/RS.
-template <int n, int RS>
-struct TeamCfg {
-  static constexpr int T = n * RS;
-  static constexpr int LD = n + 2;
-  static constexpr int R = n / RS;
+// A "team" is one CTA working on n x n FP64 matrices (n = 16, 32, 64) held in
+// shared memory, column-major with leading dimension LD = n + 4 (LD = 4 mod
+// 16 doubles makes the DMMA fragment loads below bank-conflict free).  The
+// team has one warp per 16 x 16 output tile: T = 32 (n/16)^2 threads.
+template <int n>
+struct Team {
+  static constexpr int T = 32 * (n / 16) * (n / 16);
+  static constexpr int LD = n + 4;
   static constexpr int MAT = n * LD;  // doubles per matrix
+  static constexpr int RG = T / n;    // threads per column in element-wise phases
 };
 
 __device__ __forceinline__ void team_sync() { __syncthreads(); }
 
-// C = A * B (C must not alias A or B).  k-ascending accumulation with FMA.
-template <int n, int RS>
-__device__ __forceinline__ void mm(const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C) {
-  constexpr int LD = TeamCfg<n, RS>::LD, R = TeamCfg<n, RS>::R;
-  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R;
-  double acc[R];
-#pragma unroll
-  for (int i = 0; i < R; i++) acc[i] = 0.0;
-#pragma unroll 4
-  for (int k = 0; k < n; k++) {
-    const double b = B[j * LD + k];
-    const double2* a2 = reinterpret_cast<const double2*>(A + k * LD + r0);
-#pragma unroll
-    for (int i = 0; i < R / 2; i++) {
-      const double2 a = a2[i];
-      acc[2 * i] = fma(a.x, b, acc[2 * i]);
-      acc[2 * i + 1] = fma(a.y, b, acc[2 * i + 1]);
-    }
-  }
-#pragma unroll
-  for (int i = 0; i < R; i++) C[j * LD + r0 + i] = acc[i];
+// FP64 tensor-core MMA, D(8x8) += A(8x4) * B(4x8); fragments: a = A[g][q],
+// b = B[q][g], d = D[g][2q], D[g][2q+1] with g = lane/4, q = lane%4.
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
 }
 
-// y = M * x for vectors in shared memory (threads t < n compute row t).
-template <int n, int RS>
+enum MMMode { MM_SET = 0, MM_ACC = 1, MM_IMINUS = 2 };
+
+// C = A*B (MM_SET), C = D + A*B (MM_ACC; D may be C itself) or C = I - A*B
+// (MM_IMINUS).  C must not alias A or B.  Each warp computes one 16 x 16 tile
+// with 2 x 2 DMMA fragments per k-step of 4.
+template <int n, int MODE>
+__device__ __forceinline__ void mm(const double* __restrict__ A, const double* __restrict__ B, double* C,
+                                   const double* D = nullptr) {
+  constexpr int LD = Team<n>::LD, WT = n / 16;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int row0 = (warp / WT) * 16, col0 = (warp % WT) * 16;
+  const int g = lane >> 2, q = lane & 3;
+  double c[2][2][2];
+#pragma unroll
+  for (int rt = 0; rt < 2; rt++)
+#pragma unroll
+    for (int ct = 0; ct < 2; ct++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int row = row0 + rt * 8 + g, col = col0 + ct * 8 + 2 * q + i;
+        c[rt][ct][i] = (MODE == MM_ACC) ? D[col * LD + row] : ((MODE == MM_IMINUS) ? (row == col ? 1.0 : 0.0) : 0.0);
+      }
+  const double sgn = (MODE == MM_IMINUS) ? -1.0 : 1.0;
+#pragma unroll 4
+  for (int kk = 0; kk < n; kk += 4) {
+    const double a0 = sgn * A[(kk + q) * LD + row0 + g];
+    const double a1 = sgn * A[(kk + q) * LD + row0 + 8 + g];
+    const double b0 = B[(col0 + g) * LD + kk + q];
+    const double b1 = B[(col0 + 8 + g) * LD + kk + q];
+    dmma(c[0][0], a0, b0);
+    dmma(c[0][1], a0, b1);
+    dmma(c[1][0], a1, b0);
+    dmma(c[1][1], a1, b1);
+  }
+#pragma unroll
+  for (int rt = 0; rt < 2; rt++)
+#pragma unroll
+    for (int ct = 0; ct < 2; ct++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int row = row0 + rt * 8 + g, col = col0 + ct * 8 + 2 * q + i;
+        C[col * LD + row] = c[rt][ct][i];
+      }
+}
+
+// row `row` of M * x (k-ascending FMA chain)
+template <int n>
 __device__ __forceinline__ double mv_row(const double* __restrict__ M, const double* __restrict__ x, int row) {
-  constexpr int LD = TeamCfg<n, RS>::LD;
+  constexpr int LD = Team<n>::LD;
   double s = 0.0;
 #pragma unroll 8
   for (int k = 0; k < n; k++) s = fma(M[k * LD + row], x[k], s);
   return s;
 }
 
-// In-place Gauss-Jordan inverse with partial (row) pivoting of A (n x n).
-// scratch: f[n] doubles, piv[n] ints, redv[8] doubles, redi[8] ints.
-// Returns nonzero (to every thread) if a pivot was exactly zero.
-template <int n, int RS>
-__device__ int ginv(double* A, double* f, int* piv, double* redv, int* redi) {
-  constexpr int LD = TeamCfg<n, RS>::LD, R = TeamCfg<n, RS>::R, T = TeamCfg<n, RS>::T;
-  constexpr int NW = (n + 31) / 32;  // warps that hold one row each for the pivot search
-  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R;
-  const int lane = t & 31, warp = t >> 5;
-  int singular = 0;
+// Scratch for ginv: f[n], fpre[n], prow[n] doubles; piv[n] + perm[n] + 2 ints.
+template <int n>
+struct InvScratch {
+  double f[n], fpre[n], prow[n];
+  int piv[n], perm[n];
+  int p, sing;
+};
+
+// In-place Gauss-Jordan inverse with partial (row) pivoting of A (n x n),
+// three team barriers per elimination step.  Returns nonzero to every
+// thread if a pivot was exactly zero.
+template <int n>
+__device__ int ginv(double* A, InvScratch<n>& S) {
+  constexpr int LD = Team<n>::LD, T = Team<n>::T, RG = Team<n>::RG, NR = n / RG;
+  const int t = threadIdx.x, j = t % n, rg = t / n;
+  if (t == 0) S.sing = 0;
   for (int k = 0; k < n; k++) {
-    // pivot search: thread t < n examines row t of column k
-    if (t < n) {
-      double v = (t >= k) ? fabs(A[k * LD + t]) : -1.0;
-      int idx = t;
-      const unsigned mask = (n >= 32) ? 0xffffffffu : ((1u << n) - 1u);
+    // (a) warp 0: pivot search on column k, keep the column
+    if (t < 32) {
+      double best = -1.0;
+      int bi = t;
 #pragma unroll
-      for (int o = (n >= 32 ? 16 : n / 2); o > 0; o >>= 1) {
-        double ov = __shfl_xor_sync(mask, v, o);
-        int oi = __shfl_xor_sync(mask, idx, o);
-        if (ov > v || (ov == v && oi < idx)) { v = ov; idx = oi; }
+      for (int h = 0; h < (n + 31) / 32; h++) {
+        const int i = t + 32 * h;
+        if (i < n) {
+          const double v = A[k * LD + i];
+          S.fpre[i] = v;
+          const double av = (i >= k) ? fabs(v) : -1.0;
+          if (av > best) { best = av; bi = i; }
+        }
       }
-      if (lane == 0) { redv[warp] = v; redi[warp] = idx; }
-    }
-    team_sync();
-    int p = redi[0];
-    if (NW > 1) {
-      double bv = redv[0];
 #pragma unroll
-      for (int w = 1; w < NW; w++)
-        if (redv[w] > bv) { bv = redv[w]; p = redi[w]; }
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+      }
+      __syncwarp();
+      if (t == 0) {
+        S.p = bi;
+        S.piv[k] = bi;
+        if (S.fpre[bi] == 0.0) S.sing = 1;
+      }
     }
-    // row interchange k <-> p (threads of row block 0 own the whole column)
-    if (t < n && p != k) {
-      double tmp = A[j * LD + k];
-      A[j * LD + k] = A[j * LD + p];
-      A[j * LD + p] = tmp;
+    team_sync();
+    // (b) row interchange k <-> p, pivot column after interchange, scaled pivot row
+    const int p = S.p;
+    const double rp = 1.0 / S.fpre[p];
+    if (t < n) {
+      const double fk = (t == k) ? S.fpre[p] : ((t == p) ? S.fpre[k] : S.fpre[t]);
+      S.f[t] = fk;
+      double akj = A[j * LD + p];  // row k after the interchange
+      if (p != k) {
+        A[j * LD + p] = A[j * LD + k];
+        A[j * LD + k] = akj;
+      }
+      S.prow[j] = (j == k) ? rp : akj * rp;
     }
-    if (t == 0) piv[k] = p;
     team_sync();
-    if (t < n) f[t] = A[k * LD + t];
-    team_sync();
-    const double pv = f[k];
-    if (pv == 0.0) singular = 1;
-    const double rp = 1.0 / pv;
-    const double akj = (j == k) ? rp : A[j * LD + k] * rp;
-    if (RS > 1) team_sync();
+    // (c) eliminate column k from every other row
+    const double pj = S.prow[j];
 #pragma unroll 4
-    for (int ii = 0; ii < R; ii++) {
-      const int i = r0 + ii;
+    for (int ii = 0; ii < NR; ii++) {
+      const int i = rg + RG * ii;
       double v;
-      if (i == k) v = akj;
-      else if (j == k) v = -f[i] * rp;
-      else v = A[j * LD + i] - f[i] * akj;
+      if (i == k) v = pj;
+      else if (j == k) v = -S.f[i] * rp;
+      else v = fma(-S.f[i], pj, A[j * LD + i]);
       A[j * LD + i] = v;
     }
     team_sync();
   }
-  // undo the row interchanges as column interchanges, applied in reverse
+  // undo the row interchanges as column interchanges in reverse order
   if (t == 0) {
-    for (int q = 0; q < n; q++) redi[8 + q] = q;  // caller provides redi[8 + n]
+    for (int q = 0; q < n; q++) S.perm[q] = q;
     for (int k = n - 1; k >= 0; k--) {
-      int p = piv[k];
-      int tmp = redi[8 + k];
-      redi[8 + k] = redi[8 + p];
-      redi[8 + p] = tmp;
+      const int p = S.piv[k];
+      const int tmp = S.perm[k];
+      S.perm[k] = S.perm[p];
+      S.perm[p] = tmp;
     }
   }
   team_sync();
-  double col[R];
-  const int src = redi[8 + j];
+  double col[NR];
+  const int src = S.perm[j];
 #pragma unroll
-  for (int ii = 0; ii < R; ii++) col[ii] = A[src * LD + r0 + ii];
+  for (int ii = 0; ii < NR; ii++) col[ii] = A[src * LD + rg + RG * ii];
   team_sync();
 #pragma unroll
-  for (int ii = 0; ii < R; ii++) A[j * LD + r0 + ii] = col[ii];
+  for (int ii = 0; ii < NR; ii++) A[j * LD + rg + RG * ii] = col[ii];
   team_sync();
   (void)T;
-  return singular;
+  return S.sing;
 }
 
 }  // namespace pb

@@ -6,6 +6,8 @@
 //   k_adding<N>: per (column, frequency) unit -- adding of all layers top
 //     down (COMBINE_LAYERS4 specialised by structure), surface, internal
 //     radiance at the output levels and conversion to brightness temperature.
+// Both are persistent kernels: one CTA ("team", see common.cuh) per item,
+// items taken from a device-side counter.
 #pragma once
 #include "common.cuh"
 #include "work.cuh"
@@ -14,6 +16,11 @@ namespace pb {
 
 constexpr double TWO_PI = 2.0 * 3.1415926535897932384;
 constexpr double LN2_F32 = 0.693147182464599609375;  // log(2.) in REAL(4) (radtran4.f90:325)
+constexpr int KMAX = 104;                             // azimuth points: numpts/2+1 for nlegen <= 199
+
+// Legendre upward-recurrence coefficients P_l = a_l x P_{l-1} - b_l P_{l-2},
+// a_l = (2l-1)/l, b_l = (l-1)/l (filled at context creation).
+__constant__ double c_leg_a[MAXNLEG], c_leg_b[MAXNLEG];
 
 // src/rt_utilities.f90:69-90 PLANCK_FUNCTION, UNITS='r'
 __device__ __forceinline__ double planck(double T, double wl) {
@@ -30,46 +37,44 @@ __device__ __forceinline__ double rad_to_tb(double rad, double wl) {
 template <int N>
 struct RTCfg {
   static constexpr int n = 2 * N;
-  static constexpr int RS = (N >= 32) ? 2 : 1;
-  static constexpr int T = n * RS;
-  static constexpr int LD = n + 2;
-  static constexpr int MAT = n * LD;
-  static constexpr size_t LAY_STRIDE = 2 * (size_t)MAT + 2 * n;  // R, T, S+, S-
+  static constexpr int T = Team<n>::T;
+  static constexpr int LD = Team<n>::LD;
+  static constexpr int MAT = Team<n>::MAT;
 };
+
+__host__ __device__ __forceinline__ size_t lay_stride_n(int N) {
+  const int n = 2 * N;
+  return 2 * (size_t)n * (n + 4) + 2 * n;
+}
 
 // ============================================================== layer kernel
 template <int N>
 struct LayerSmem {
   static constexpr int n = RTCfg<N>::n, MAT = RTCfg<N>::MAT;
-  double m[5][MAT];
-  double coef[3][MAXNLEG];
+  double m[5][MAT];  // R, T, G, W, Y; during scatcnv G (and W) hold the coefficients, Y the azimuth table
   double lin[2 * n], cst[2 * n];
   double v[4][n], u[4][n];
-  double f[n];
-  double mu[N], wq[N];
-  double redv[8];
-  int piv[n];
-  int redi[8 + n];
+  double mu[N], wq[N], nrm[N];
+  InvScratch<n> inv;
+  int item, stat;
 };
 
 template <int N>
-__global__ void __launch_bounds__(RTCfg<N>::T) k_layer(Batch b, Work w, pamtra_b200_settings st,
+__global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch b, Work w, pamtra_b200_settings st,
                                                        double* __restrict__ ssp_scat) {
-  constexpr int n = RTCfg<N>::n, RS = RTCfg<N>::RS, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT;
-  constexpr int R_ = n / RS;
+  constexpr int n = RTCfg<N>::n, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT, T = RTCfg<N>::T;
   extern __shared__ double smem_raw[];
   LayerSmem<N>& S = *reinterpret_cast<LayerSmem<N>*>(smem_raw);
-  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R_;
+  const int t = threadIdx.x;
   const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
   const int P = min(w.counters[0], w.pmax);
   const int nitems = P * Fm;
   if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
-  __shared__ int s_item;
   for (;;) {
     team_sync();
-    if (t == 0) s_item = atomicAdd(&w.counters[2 + (N == 8 ? 0 : (N == 16 ? 1 : 2))], 1);
+    if (t == 0) S.item = atomicAdd(&w.counters[2 + (N == 8 ? 0 : (N == 16 ? 1 : 2))], 1);
     team_sync();
-    const int item = s_item;
+    const int item = S.item;
     if (item >= nitems) break;
     const int p = item / Fm, fi = item % Fm;
     const int cz = w.plist[p];
@@ -87,8 +92,8 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_layer(Batch b, Work w, pamtra_b
     double* Rb = S.m[0];
     double* Tb = S.m[1];
     double* Gb = S.m[2];
-    double* Ab = S.m[3];
-    double* Bb = S.m[4];
+    double* Wb = S.m[3];
+    double* Yb = S.m[4];
     double ext = 0.0, emis = 0.0;
     int status = 0;
     // ---------------- scatcnv (src/scatcnv.f90) into P1 (Tb) and P2 (Rb)
@@ -97,33 +102,40 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_layer(Batch b, Work w, pamtra_b
       emis = (1.0 - salb) * kext;
       const double cst = kext * salb / (4.0 * 3.1415926535897932384);
       const double* lg = w.m_legen + (size_t)item * 3 * MAXNLEG;
-      for (int l = t; l <= nleg; l += RTCfg<N>::T) {
-        S.coef[0][l] = cst * lg[l];
-        S.coef[1][l] = cst * lg[MAXNLEG + l];
-        S.coef[2][l] = cst * lg[2 * MAXNLEG + l];
-      }
-      team_sync();
+      double* coef = Gb;          // [3][MAXNLEG], may run on into Wb (n = 16)
+      double* cphi = Yb;          // [KMAX]
+      double* sphi = Yb + KMAX;   // [KMAX]
       const int numpts = 2 * ((nleg + 1) / 2) + 4;
       const int K = numpts / 2 + 1;
-      for (int it = t; it < 2 * N * N; it += RTCfg<N>::T) {
+      for (int l = t; l <= nleg; l += T) {
+        coef[l] = cst * lg[l];
+        coef[MAXNLEG + l] = cst * lg[MAXNLEG + l];
+        coef[2 * MAXNLEG + l] = cst * lg[2 * MAXNLEG + l];
+      }
+      for (int k = t; k < K; k += T) {
+        const double delphi = (TWO_PI * k) / numpts;
+        cphi[k] = cos(delphi);
+        sphi[k] = sin(delphi);
+      }
+      team_sync();
+      for (int it = t; it < 2 * N * N; it += T) {
         const int q = it / (N * N), j1 = (it / N) % N, j2 = it % N;
         const double mu1 = (q == 0) ? S.mu[j1] : -S.mu[j1];
         const double mu2 = S.mu[j2];
         const double st1 = sqrt(1. - mu1 * mu1), st2 = sqrt(1. - mu2 * mu2);
         const double sqm = sqrt((1. - mu1 * mu1) * (1. - mu2 * mu2));
         double a11 = 0, a12 = 0, a21 = 0, a22 = 0, m11 = 0, m12 = 0, m21 = 0, m22 = 0;
-        for (int k = 1; k <= K; k++) {
-          const double delphi = (TWO_PI * (k - 1)) / numpts;
-          const double cosphi = cos(delphi), sinphi = sin(delphi);
+        for (int k = 0; k < K; k++) {
+          const double cosphi = cphi[k], sinphi = sphi[k];
           const double cs = mu1 * mu2 + sqm * cosphi;
           // SUM_LEGENDRE, DOSUM = (1,1,1,0,0,0)
-          double s0 = S.coef[0][0], s1 = S.coef[1][0], s2 = S.coef[2][0];
-          double pl1 = 1.0, pl2 = 0.0, pl = 1.0;
+          double s0 = coef[0], s1 = coef[MAXNLEG], s2 = coef[2 * MAXNLEG];
+          double pl1 = 1.0, pl2 = 0.0;
           for (int L = 1; L <= nleg; L++) {
-            pl = (2 * L - 1) * cs * pl1 / L - (L - 1) * pl2 / L;
-            s0 = fma(S.coef[0][L], pl, s0);
-            s1 = fma(S.coef[1][L], pl, s1);
-            s2 = fma(S.coef[2][L], pl, s2);
+            const double pl = fma(c_leg_a[L] * cs, pl1, -c_leg_b[L] * pl2);
+            s0 = fma(coef[L], pl, s0);
+            s1 = fma(coef[MAXNLEG + L], pl, s1);
+            s2 = fma(coef[2 * MAXNLEG + L], pl, s2);
             pl2 = pl1;
             pl1 = pl;
           }
@@ -133,17 +145,18 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_layer(Batch b, Work w, pamtra_b
           if (ss == 0.0) {
             sin1 = 0; sin2 = 0; cos1 = 1; cos2 = -1;
           } else {
-            sin1 = st2 * sinphi / ss;
-            sin2 = st1 * sinphi / ss;
-            cos1 = (st1 * mu2 - st2 * mu1 * cosphi) / ss;
-            cos2 = (st2 * mu1 - st1 * mu2 * cosphi) / ss;
+            const double r = 1.0 / ss;
+            sin1 = st2 * sinphi * r;
+            sin2 = st1 * sinphi * r;
+            cos1 = (st1 * mu2 - st2 * mu1 * cosphi) * r;
+            cos2 = (st2 * mu1 - st1 * mu2 * cosphi) * r;
           }
           const double sin21 = 2.0 * sin1 * cos1, cos21 = 1.0 - 2.0 * (sin1 * sin1);
           const double sin22 = 2.0 * sin2 * cos2, cos22 = 1.0 - 2.0 * (sin2 * sin2);
           const double e11 = s0, e12 = s1 * cos21, e21 = s1 * cos22, e22 = s0 * cos21 * cos22 - s2 * sin21 * sin22;
-          // FOURIER_BASIS order 0: points k and numpts-k+2 coincide (MATRIX_SYMMETRY)
+          // FOURIER_BASIS order 0: points k and numpts-k coincide (MATRIX_SYMMETRY)
           a11 += e11; a12 += e12; a21 += e21; a22 += e22;
-          if (k > 1 && k < K) { m11 += e11; m12 += e12; m21 += e21; m22 += e22; }
+          if (k > 0 && k < K - 1) { m11 += e11; m12 += e12; m21 += e21; m22 += e22; }
         }
         double* Q = (q == 0) ? Tb : Rb;
         const int row0 = 2 * j2, col0 = 2 * j1;
@@ -154,19 +167,19 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_layer(Batch b, Work w, pamtra_b
       }
       team_sync();
       if (!st.lhyd_scattering) {
-        for (int e = t; e < MAT; e += RTCfg<N>::T) { Tb[e] = 0.0; Rb[e] = 0.0; }
+        for (int e = t; e < MAT; e += T) { Tb[e] = 0.0; Rb[e] = 0.0; }
         team_sync();
       }
       if (!st.lhyd_emission) emis = 0.0;
     } else {
-      for (int e = t; e < MAT; e += RTCfg<N>::T) { Tb[e] = 0.0; Rb[e] = 0.0; }
+      for (int e = t; e < MAT; e += T) { Tb[e] = 0.0; Rb[e] = 0.0; }
       team_sync();
     }
     // optional save_ssp output of the 4 quadrants (l=1,4 equal; l=2,3 equal)
     if (ssp_scat) {
-      const size_t o = (((size_t)c * Fm + fi) * Lm + z) * 4 * (size_t)(2 * b.max_nummu) * (2 * b.max_nummu);
       const int nn = 2 * b.max_nummu;
-      for (int e = t; e < n * n; e += RTCfg<N>::T) {
+      const size_t o = (((size_t)c * Fm + fi) * Lm + z) * 4 * (size_t)nn * nn;
+      for (int e = t; e < n * n; e += T) {
         const int row = e / n, col = e % n;
         const double p1 = Tb[col * LD + row], p2 = Rb[col * LD + row];
         ssp_scat[o + 0 * (size_t)nn * nn + (size_t)row * nn + col] = p1;
@@ -180,17 +193,14 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_layer(Batch b, Work w, pamtra_b
       double sum = emis - ext;
       for (int j2 = 0; j2 < N; j2++)
         sum = sum + 2.0 * 3.1415926535897932384 * S.wq[j2] * (Tb[(2 * t) * LD + 2 * j2] + Rb[(2 * t) * LD + 2 * j2]);
-      S.f[t] = fabs(sum);
+      S.nrm[t] = fabs(sum);
     }
     team_sync();
     if (t == 0) {
       double mx = 0.0;
-      for (int i = 0; i < N; i++) mx = fmax(mx, S.f[i]);
-      if (mx > 5.0e-4) S.redi[0] = PAMTRA_B200_FATAL | PAMTRA_B200_ST_NORM;
-      else S.redi[0] = 0;
+      for (int i = 0; i < N; i++) mx = fmax(mx, S.nrm[i]);
+      S.stat = (mx > 5.0e-4) ? (PAMTRA_B200_FATAL | PAMTRA_B200_ST_NORM) : 0;
     }
-    team_sync();
-    status |= S.redi[0];
     // ---------------- number of doublings (src/radtran4.f90:319-329)
     const double extinct = ext + gas;
     const double fl = log(fmax(extinct * zdiff, 1.0e-7) / 1.0e-6) / LN2_F32;
@@ -201,10 +211,10 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_layer(Batch b, Work w, pamtra_b
     // ---------------- INITIALIZE4 (src/radintg4.f90:1-45), in place over P1/P2
     {
       const double C = 2.0 * 3.1415926535897932384;
-      const int col = j, i1 = col & 1, j1 = col >> 1;
-      const double wj1 = S.wq[j1];
-      for (int ii = 0; ii < R_; ii++) {
-        const int row = r0 + ii, i2 = row & 1, j2 = row >> 1;
+      for (int e = t; e < n * n; e += T) {
+        const int col = e / n, row = e % n;
+        const int i1 = col & 1, j1 = col >> 1, i2 = row & 1, j2 = row >> 1;
+        const double wj1 = S.wq[j1];
         const double tmp = delta_z / S.mu[j2];
         const double gext = (i1 == i2) ? gas : 0.0;
         const double diag = (row == col) ? 1.0 : 0.0;
@@ -226,83 +236,81 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_layer(Batch b, Work w, pamtra_b
     }
     double linfac = (planck0 == 0.0) ? 0.0 : (planck1 / planck0 - 1.0) / num_sub;
     team_sync();
+    status |= S.stat;
     // ---------------- DOUBLING_INTEGRATION4, SYMMETRIC (src/radintg4.f90:174-309)
     for (int itd = 0; itd < nd; itd++) {
-      mm<n, RS>(Rb, Rb, Ab);
+      mm<n, MM_IMINUS>(Rb, Rb, Gb);  // I - R+ R-
       team_sync();
-      for (int ii = 0; ii < R_; ii++) {
-        const int row = r0 + ii;
-        Ab[j * LD + row] = ((row == j) ? 1.0 : 0.0) - Ab[j * LD + row];
-      }
-      team_sync();
-      if (ginv<n, RS>(Ab, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-      { double* tmp = Gb; Gb = Ab; Ab = tmp; }
+      if (ginv<n>(Gb, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
       // source chains: v = [S- + f C-, C-, S+, C+] -> R v -> add -> G -> T
-      if (t < n) {
-        S.v[0][t] = S.lin[n + t] + linfac * S.cst[n + t];
-        S.v[1][t] = S.cst[n + t];
-        S.v[2][t] = S.lin[t];
-        S.v[3][t] = S.cst[t];
+      for (int o = t; o < 4 * n; o += T) {
+        const int r = o % n, k = o / n;
+        double v;
+        if (k == 0) v = S.lin[n + r] + linfac * S.cst[n + r];
+        else if (k == 1) v = S.cst[n + r];
+        else if (k == 2) v = S.lin[r];
+        else v = S.cst[r];
+        S.v[k][r] = v;
       }
       team_sync();
-      if (t < n) {
-        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-        for (int k = 0; k < n; k++) {
-          const double r = Rb[k * LD + t];
-          a0 = fma(r, S.v[0][k], a0); a1 = fma(r, S.v[1][k], a1); a2 = fma(r, S.v[2][k], a2); a3 = fma(r, S.v[3][k], a3);
-        }
-        S.u[0][t] = S.lin[t] + a0;
-        S.u[1][t] = S.cst[t] + a1;
-        S.u[2][t] = S.v[0][t] + a2;
-        S.u[3][t] = S.cst[n + t] + a3;
+      for (int o = t; o < 4 * n; o += T) {
+        const int r = o % n, k = o / n;
+        const double a = mv_row<n>(Rb, S.v[k], r);
+        double u;
+        if (k == 0) u = S.lin[r] + a;
+        else if (k == 1) u = S.cst[r] + a;
+        else if (k == 2) u = S.v[0][r] + a;
+        else u = S.cst[n + r] + a;
+        S.u[k][r] = u;
       }
       team_sync();
-      if (t < n) {
-        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-        for (int k = 0; k < n; k++) {
-          const double g = Gb[k * LD + t];
-          a0 = fma(g, S.u[0][k], a0); a1 = fma(g, S.u[1][k], a1); a2 = fma(g, S.u[2][k], a2); a3 = fma(g, S.u[3][k], a3);
-        }
-        S.v[0][t] = a0; S.v[1][t] = a1; S.v[2][t] = a2; S.v[3][t] = a3;
+      for (int o = t; o < 4 * n; o += T) {
+        const int r = o % n, k = o / n;
+        S.v[k][r] = mv_row<n>(Gb, S.u[k], r);
       }
       team_sync();
-      double o0 = 0, o1 = 0, o2 = 0, o3 = 0;
-      if (t < n) {
-        double a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-        for (int k = 0; k < n; k++) {
-          const double tt = Tb[k * LD + t];
-          a0 = fma(tt, S.v[0][k], a0); a1 = fma(tt, S.v[1][k], a1); a2 = fma(tt, S.v[2][k], a2); a3 = fma(tt, S.v[3][k], a3);
+      double onew[(4 * n + T - 1) / T];
+#pragma unroll
+      for (int s = 0; s < (4 * n + T - 1) / T; s++) {
+        const int o = t + s * T;
+        if (o < 4 * n) {
+          const int r = o % n, k = o / n;
+          const double a = mv_row<n>(Tb, S.v[k], r);
+          if (k == 0) onew[s] = (S.lin[r] + a) + linfac * S.cst[r];
+          else if (k == 1) onew[s] = S.cst[r] + a;
+          else if (k == 2) onew[s] = S.lin[n + r] + a;
+          else onew[s] = S.cst[n + r] + a;
         }
-        o0 = (S.lin[t] + a0) + linfac * S.cst[t];
-        o1 = S.cst[t] + a1;
-        o2 = S.lin[n + t] + a2;
-        o3 = S.cst[n + t] + a3;
       }
       // matrices: R' = R + T G R T ; T' = T G T
-      mm<n, RS>(Rb, Tb, Ab);
+      mm<n, MM_SET>(Rb, Tb, Wb);
       team_sync();
-      mm<n, RS>(Gb, Ab, Bb);
+      mm<n, MM_SET>(Gb, Wb, Yb);
       team_sync();
-      mm<n, RS>(Tb, Bb, Ab);
+      mm<n, MM_ACC>(Tb, Yb, Rb, Rb);
+      mm<n, MM_SET>(Gb, Tb, Wb);
       team_sync();
-      for (int ii = 0; ii < R_; ii++) Rb[j * LD + r0 + ii] = Rb[j * LD + r0 + ii] + Ab[j * LD + r0 + ii];
-      mm<n, RS>(Gb, Tb, Bb);
+      mm<n, MM_SET>(Tb, Wb, Yb);
       team_sync();
-      mm<n, RS>(Tb, Bb, Ab);
-      team_sync();
-      { double* tmp = Tb; Tb = Ab; Ab = tmp; }
-      if (t < n) {
-        S.lin[t] = o0; S.cst[t] = o1; S.lin[n + t] = o2; S.cst[n + t] = o3;
+      { double* tmp = Tb; Tb = Yb; Yb = tmp; }
+#pragma unroll
+      for (int s = 0; s < (4 * n + T - 1) / T; s++) {
+        const int o = t + s * T;
+        if (o < 4 * n) {
+          const int r = o % n, k = o / n;
+          if (k == 0) S.lin[r] = onew[s];
+          else if (k == 1) S.cst[r] = onew[s];
+          else if (k == 2) S.lin[n + r] = onew[s];
+          else S.cst[n + r] = onew[s];
+        }
       }
       linfac = 2.0 * linfac;
       team_sync();
     }
     // ---------------- write layer R, T, S+, S-
     double* out = w.lay + (size_t)item * w.lay_stride;
-    for (int e = t; e < MAT; e += RTCfg<N>::T) { out[e] = Rb[e]; out[MAT + e] = Tb[e]; }
-    if (t < 2 * n) out[2 * MAT + t] = S.lin[t];
-    if (RTCfg<N>::T < 2 * n)
-      for (int e = t + RTCfg<N>::T; e < 2 * n; e += RTCfg<N>::T) out[2 * MAT + e] = S.lin[e];
+    for (int e = t; e < MAT; e += T) { out[e] = Rb[e]; out[MAT + e] = Tb[e]; }
+    for (int e = t; e < 2 * n; e += T) out[2 * MAT + e] = S.lin[e];
     if (t == 0) {
       w.lay_nd[item] = nd;
       if (status) atomicOr(&w.status[(size_t)c * Fm + fi], status);
@@ -311,8 +319,6 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_layer(Batch b, Work w, pamtra_b
 }
 
 // ============================================================== adding kernel
-// Shared memory: stack (R+, R-, T+, T-), layer (R2, T2), G and three temps,
-// vectors.
 template <int N>
 struct AddSmem {
   static constexpr int n = RTCfg<N>::n, MAT = RTCfg<N>::MAT;
@@ -320,54 +326,48 @@ struct AddSmem {
   double sp[n], sm[n], s2p[n], s2m[n], t1[n], t2[n], nsp[n], nsm[n];
   double wv[n], wv2[n];
   double sky[n], gnd[n], uprad[n], dnrad[n];
-  double f[n];
   double mu[N], wq[N];
-  double redv[8];
-  int piv[n];
-  int redi[8 + n];
+  InvScratch<n> inv;
+  int unit;
 };
 
-// team helpers on AddSmem
-template <int n, int RS>
-__device__ __forceinline__ void mat_ident_minus(double* A) {  // A = I - A
-  constexpr int LD = TeamCfg<n, RS>::LD, R = TeamCfg<n, RS>::R;
-  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R;
-  for (int ii = 0; ii < R; ii++) {
-    const int row = r0 + ii;
-    A[j * LD + row] = ((row == j) ? 1.0 : 0.0) - A[j * LD + row];
+template <int n>
+__device__ __forceinline__ void ew_ident(double* A) {  // A = I
+  constexpr int LD = Team<n>::LD, T = Team<n>::T;
+  for (int e = threadIdx.x; e < n * n; e += T) {
+    const int col = e / n, row = e % n;
+    A[col * LD + row] = (row == col) ? 1.0 : 0.0;
   }
 }
-template <int n, int RS>
-__device__ __forceinline__ void mat_fill_diag(double* A, const double* d) {  // A = diag(d)
-  constexpr int LD = TeamCfg<n, RS>::LD, R = TeamCfg<n, RS>::R;
-  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R;
-  for (int ii = 0; ii < R; ii++) {
-    const int row = r0 + ii;
-    A[j * LD + row] = (row == j) ? d[j] : 0.0;
-  }
+template <int n>
+__device__ __forceinline__ void ew_zero(double* A) {
+  constexpr int LD = Team<n>::LD, T = Team<n>::T;
+  for (int e = threadIdx.x; e < n * n; e += T) A[(e / n) * LD + e % n] = 0.0;
 }
-template <int n, int RS>
-__device__ __forceinline__ double mvr(const double* M, const double* x, int row) {
-  return mv_row<n, RS>(M, x, row);
+template <int n>
+__device__ __forceinline__ void ew_diag(double* A, const double* d) {
+  constexpr int LD = Team<n>::LD, T = Team<n>::T;
+  for (int e = threadIdx.x; e < n * n; e += T) {
+    const int col = e / n, row = e % n;
+    A[col * LD + row] = (row == col) ? d[col] : 0.0;
+  }
 }
 
 template <int N>
 __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_b200_settings st,
                                                         pamtra_b200_outputs out) {
-  constexpr int n = RTCfg<N>::n, RS = RTCfg<N>::RS, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT;
-  constexpr int R_ = n / RS, T = RTCfg<N>::T;
+  constexpr int n = RTCfg<N>::n, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT, T = RTCfg<N>::T;
   extern __shared__ double smem_raw[];
   AddSmem<N>& S = *reinterpret_cast<AddSmem<N>*>(smem_raw);
-  const int t = threadIdx.x, j = t % n, r0 = (t / n) * R_;
+  const int t = threadIdx.x;
   const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
   const int nunits = b.ncol * Fm;
   if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
-  __shared__ int s_unit;
   for (;;) {
     team_sync();
-    if (t == 0) s_unit = atomicAdd(&w.counters[5 + (N == 8 ? 0 : (N == 16 ? 1 : 2))], 1);
+    if (t == 0) S.unit = atomicAdd(&w.counters[5 + (N == 8 ? 0 : (N == 16 ? 1 : 2))], 1);
     team_sync();
-    const int unit = s_unit;
+    const int unit = S.unit;
     if (unit >= nunits) break;
     const int c = unit / Fm, fi = unit % Fm;
     if (fi >= b.col_nfreq(c) || b.col_nummu(c) != N) continue;
@@ -376,19 +376,16 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
     const double wl = C_LIGHT / (freq * 1.e3);
     const double* hl = w.hgt_lev + (size_t)c * (Lm + 1);
     const double* tl = w.temp_lev + (size_t)c * (Lm + 1);
-    int status = 0;
-    if (w.col_status[c]) status |= w.col_status[c];
-    // stack buffers (roles swap by pointer)
+    int status = w.col_status[c];
     double *Rp = S.m[0], *Rm = S.m[1], *Tp = S.m[2], *Tm = S.m[3];
     double *R2 = S.m[4], *T2 = S.m[5];
     double *G = S.m[6], *X = S.m[7], *Y = S.m[8], *Z = S.m[9];
-    // stack state: 0 empty, 1 clear (R = 0, T = diag t1, same both sides), 2 general
+    // stack state: 0 empty, 1 clear (R = 0, T = diag t1 on both sides), 2 general
     int sstate = 0;
     for (int k = 0; k < L; k++) {  // top-down layer index
       const int z = L - 1 - k;
       const int pidx = w.pres_idx[(size_t)c * Lm + z];
-      const bool scat = pidx >= 0;
-      if (!scat) {
+      if (pidx < 0) {
         // NONSCATTER_LAYER4 (src/radintg4.f90:79-117)
         if (t < n) {
           const int jj = t >> 1, i = t & 1;
@@ -412,6 +409,7 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
           if (t < n) { S.t1[t] = S.t2[t]; S.sp[t] = S.s2p[t]; S.sm[t] = S.s2m[t]; }
           sstate = 1;
         } else if (sstate == 1) {
+          // clear + clear
           if (t < n) {
             const double sp = S.s2p[t] + S.t2[t] * S.sp[t];
             const double sm = S.sm[t] + S.t1[t] * S.s2m[t];
@@ -421,22 +419,19 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
           }
         } else {
           // general stack + clear layer
-          double nsp = 0.0, nsm = 0.0;
           if (t < n) {
-            nsp = S.s2p[t] + S.t2[t] * (S.sp[t] + mvr<n, RS>(Rp, S.s2m, t));
-            nsm = S.sm[t] + mvr<n, RS>(Tm, S.s2m, t);
-          }
-          team_sync();  // all reads of the old R+, T- done before the in-place updates
-          const double t2j = S.t2[j];
-          for (int ii = 0; ii < R_; ii++) {
-            const int row = r0 + ii;
-            const double t2i = S.t2[row];
-            Rp[j * LD + row] = t2i * (Rp[j * LD + row] * t2j);
-            Tp[j * LD + row] = t2i * Tp[j * LD + row];
-            Tm[j * LD + row] = Tm[j * LD + row] * t2j;
+            S.nsp[t] = S.s2p[t] + S.t2[t] * (S.sp[t] + mv_row<n>(Rp, S.s2m, t));
+            S.nsm[t] = S.sm[t] + mv_row<n>(Tm, S.s2m, t);
           }
           team_sync();
-          if (t < n) { S.sp[t] = nsp; S.sm[t] = nsm; }
+          for (int e = t; e < n * n; e += T) {
+            const int col = e / n, row = e % n, a = col * LD + row;
+            const double t2i = S.t2[row], t2j = S.t2[col];
+            Rp[a] = t2i * (Rp[a] * t2j);
+            Tp[a] = t2i * Tp[a];
+            Tm[a] = Tm[a] * t2j;
+          }
+          if (t < n) { S.sp[t] = S.nsp[t]; S.sm[t] = S.nsm[t]; }
         }
         team_sync();
         continue;
@@ -449,7 +444,6 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
       }
       team_sync();
       if (sstate == 0) {
-        // stack := layer
         for (int e = t; e < MAT; e += T) { Rp[e] = R2[e]; Rm[e] = R2[e]; Tp[e] = T2[e]; Tm[e] = T2[e]; }
         if (t < n) { S.sp[t] = S.s2p[t]; S.sm[t] = S.s2m[t]; }
         sstate = 2;
@@ -458,90 +452,75 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
       }
       if (sstate == 1) {
         // clear stack (t1, sp, sm) + scattering layer
-        double nsp = 0.0, nsm = 0.0;
         if (t < n) {
-          nsp = S.s2p[t] + mvr<n, RS>(T2, S.sp, t);
-          nsm = S.sm[t] + S.t1[t] * (S.s2m[t] + mvr<n, RS>(R2, S.sp, t));
+          S.nsp[t] = S.s2p[t] + mv_row<n>(T2, S.sp, t);
+          S.nsm[t] = S.sm[t] + S.t1[t] * (S.s2m[t] + mv_row<n>(R2, S.sp, t));
         }
-        const double t1j = S.t1[j];
-        for (int ii = 0; ii < R_; ii++) {
-          const int row = r0 + ii;
-          const double t1i = S.t1[row];
-          const double r2 = R2[j * LD + row], tt = T2[j * LD + row];
-          Rp[j * LD + row] = r2;
-          Rm[j * LD + row] = t1i * (r2 * t1j);
-          Tp[j * LD + row] = tt * t1j;
-          Tm[j * LD + row] = t1i * tt;
+        for (int e = t; e < n * n; e += T) {
+          const int col = e / n, row = e % n, a = col * LD + row;
+          const double t1i = S.t1[row], t1j = S.t1[col];
+          const double r2 = R2[a], tt = T2[a];
+          Rp[a] = r2;
+          Rm[a] = t1i * (r2 * t1j);
+          Tp[a] = tt * t1j;
+          Tm[a] = t1i * tt;
         }
         team_sync();
-        if (t < n) { S.sp[t] = nsp; S.sm[t] = nsm; }
+        if (t < n) { S.sp[t] = S.nsp[t]; S.sm[t] = S.nsm[t]; }
         sstate = 2;
         team_sync();
         continue;
       }
       // ---- general COMBINE_LAYERS4 (src/radintg4.f90:447-513), R2p = R2m, T2p = T2m
-      mm<n, RS>(Rp, R2, X);  // GAMMAp = inv(I - R1p R2m)
+      mm<n, MM_IMINUS>(Rp, R2, G);  // GAMMAp = inv(I - R1p R2m)
       team_sync();
-      mat_ident_minus<n, RS>(X);
+      if (ginv<n>(G, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      mm<n, MM_SET>(Rp, T2, X);  // RTp = R2p + T2p G R1p T2m
+      if (t < n) S.wv[t] = S.sp[t] + mv_row<n>(Rp, S.s2m, t);  // STp chain
       team_sync();
-      if (ginv<n, RS>(X, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-      { double* tp = G; G = X; X = tp; }
-      mm<n, RS>(Rp, T2, X);  // RTp = R2p + T2p G R1p T2m
+      mm<n, MM_SET>(G, X, Y);
+      if (t < n) S.wv2[t] = mv_row<n>(G, S.wv, t);
       team_sync();
-      mm<n, RS>(G, X, Y);
+      mm<n, MM_ACC>(T2, Y, Z, R2);  // new R+ in Z
+      mm<n, MM_SET>(G, Tp, X);      // TTp = T2p G T1p
+      if (t < n) S.nsp[t] = S.s2p[t] + mv_row<n>(T2, S.wv2, t);
       team_sync();
-      mm<n, RS>(T2, Y, X);
+      mm<n, MM_SET>(T2, X, Y);              // new T+ in Y
+      mm<n, MM_IMINUS>(R2, Rp, G);          // GAMMAm = inv(I - R2m R1p); Gp is dead
       team_sync();
-      for (int ii = 0; ii < R_; ii++) Y[j * LD + r0 + ii] = R2[j * LD + r0 + ii] + X[j * LD + r0 + ii];  // new R+ in Y
-      mm<n, RS>(G, Tp, X);  // TTp = T2p G T1p
+      if (ginv<n>(G, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      mm<n, MM_SET>(R2, Tp, X);  // RTm = R1m + T1m G R2m T1p
+      if (t < n) S.wv[t] = S.s2m[t] + mv_row<n>(R2, S.sp, t);  // STm chain
       team_sync();
-      mm<n, RS>(T2, X, Z);  // new T+ in Z
-      // STp = S2p + T2p G (S1p + R1p S2m)
-      if (t < n) S.wv[t] = S.sp[t] + mvr<n, RS>(Rp, S.s2m, t);
+      mm<n, MM_SET>(G, X, Rp);  // old R+ is dead
+      if (t < n) S.wv2[t] = mv_row<n>(G, S.wv, t);
       team_sync();
-      if (t < n) S.wv2[t] = mvr<n, RS>(G, S.wv, t);
+      mm<n, MM_ACC>(Tm, Rp, Rm, Rm);  // new R- in place
+      mm<n, MM_SET>(G, T2, X);        // TTm = T1m G T2m
+      if (t < n) S.nsm[t] = S.sm[t] + mv_row<n>(Tm, S.wv2, t);
       team_sync();
-      if (t < n) S.nsp[t] = S.s2p[t] + mvr<n, RS>(T2, S.wv2, t);
-      mm<n, RS>(R2, Rp, X);  // GAMMAm = inv(I - R2m R1p)
-      team_sync();
-      mat_ident_minus<n, RS>(X);
-      team_sync();
-      if (ginv<n, RS>(X, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-      { double* tp = G; G = X; X = tp; }
-      mm<n, RS>(R2, Tp, X);  // RTm = R1m + T1m G R2m T1p
-      team_sync();
-      mm<n, RS>(G, X, Rp);  // old R+ is dead
-      team_sync();
-      mm<n, RS>(Tm, Rp, X);
-      team_sync();
-      for (int ii = 0; ii < R_; ii++) Rm[j * LD + r0 + ii] = Rm[j * LD + r0 + ii] + X[j * LD + r0 + ii];
-      mm<n, RS>(G, T2, X);  // TTm = T1m G T2m
-      team_sync();
-      mm<n, RS>(Tm, X, Tp);  // old T+ is dead; new T- in Tp buffer
-      // STm = S1m + T1m G (S2m + R2m S1p)
-      if (t < n) S.wv[t] = S.s2m[t] + mvr<n, RS>(R2, S.sp, t);
-      team_sync();
-      if (t < n) S.wv2[t] = mvr<n, RS>(G, S.wv, t);
-      team_sync();
-      if (t < n) S.nsm[t] = S.sm[t] + mvr<n, RS>(Tm, S.wv2, t);
+      mm<n, MM_SET>(Tm, X, Tp);  // old T+ is dead: new T- in Tp buffer
       team_sync();
       {
-        // roles: new R+ = Y, new R- = Rm, new T+ = Z, new T- = Tp
+        // roles: new R+ = Z, new R- = Rm, new T+ = Y, new T- = Tp
         double *oRp = Rp, *oTm = Tm;
-        Rp = Y;
+        Rp = Z;
         Tm = Tp;
-        Tp = Z;
-        Y = oRp;
-        Z = oTm;
+        Tp = Y;
+        Z = oRp;
+        Y = oTm;
       }
       if (t < n) { S.sp[t] = S.nsp[t]; S.sm[t] = S.nsm[t]; }
       team_sync();
     }
-    // materialise a clear stack
-    if (sstate == 1) {
-      mat_fill_diag<n, RS>(Tp, S.t1);
-      mat_fill_diag<n, RS>(Tm, S.t1);
-      for (int e = t; e < MAT; e += T) { Rp[e] = 0.0; Rm[e] = 0.0; }
+    // materialise a clear (or empty) stack
+    if (sstate <= 1) {
+      if (sstate == 0 && t < n) { S.t1[t] = 1.0; S.sp[t] = 0.0; S.sm[t] = 0.0; }
+      team_sync();
+      ew_diag<n>(Tp, S.t1);
+      ew_diag<n>(Tm, S.t1);
+      ew_zero<n>(Rp);
+      ew_zero<n>(Rm);
       team_sync();
     }
     // surface (src/sfc_matrices.f90; default emissivity sfc_optics.f90:79-81)
@@ -549,18 +528,17 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
     const char refl = (char)b.sfc_refl[c];
     const double e = st.emissivity, rr = 1.0 - e;
     const double pg = planck(w.gtemp[c], wl), psky = planck(SKY_TEMP, wl);
-    // R2 := surface R- (R+ = 0), T2 := I
-    for (int ii = 0; ii < R_; ii++) {
-      const int row = r0 + ii;
+    for (int ee = t; ee < n * n; ee += T) {  // R2 := surface R- (R+ = 0), T2 := I
+      const int col = ee / n, row = ee % n;
       double v = 0.0;
       if (refl == 'S' || refl == 'F') {
         const double r1 = (rr + rr) / 2.0, r2 = (rr - rr) / 2.0;
-        if ((row >> 1) == (j >> 1)) v = ((row & 1) == (j & 1)) ? r1 : r2;
+        if ((row >> 1) == (col >> 1)) v = ((row & 1) == (col & 1)) ? r1 : r2;
       } else if (refl == 'L') {
-        if ((row & 1) == 0 && (j & 1) == 0) v = 2.0 * rr * S.mu[j >> 1] * S.wq[j >> 1];
+        if ((row & 1) == 0 && (col & 1) == 0) v = 2.0 * rr * S.mu[col >> 1] * S.wq[col >> 1];
       }
-      R2[j * LD + row] = v;
-      T2[j * LD + row] = (row == j) ? 1.0 : 0.0;
+      R2[col * LD + row] = v;
+      T2[col * LD + row] = (row == col) ? 1.0 : 0.0;
     }
     if (refl != 'S' && refl != 'F' && refl != 'L') status |= PAMTRA_B200_WARNING;
     if (t < n) {
@@ -574,97 +552,72 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
       }
       S.gnd[t] = gv;
       S.sky[t] = (i == 0) ? (1.0 - 0.0) * psky : 0.0;
+      S.s2m[t] = 0.0;  // the surface carries no source in the adding
     }
     team_sync();
-    // output levels: level L+1 uses (stack, surface); level 1 uses (empty, stack+surface)
+    // output levels: L+1 -> (stack, surface); 1 -> (empty, stack on surface)
     int lev_order[2] = {-1, -1};
-    int nlev = 0;
     for (int io = 0; io < b.noutlevels; io++) {
       const int lev = w.outlev[(size_t)c * b.noutlevels + io];
       if (lev == L + 1) lev_order[0] = io;
       else if (lev == 1) lev_order[1] = io;
       else status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;  // intermediate levels not supported
-      nlev++;
     }
-    (void)nlev;
     for (int pass = 0; pass < 2; pass++) {
       const int io = lev_order[pass];
-      if (pass == 1 && io >= 0) {
+      if (io < 0) continue;
+      if (pass == 1) {
         // down stack for level 1: (stack) on top of (surface), minus side only
-        mm<n, RS>(R2, Rp, X);  // GAMMAm = inv(I - Rsfc R1p)
+        mm<n, MM_IMINUS>(R2, Rp, G);  // GAMMAm = inv(I - Rsfc R1p)
         team_sync();
-        mat_ident_minus<n, RS>(X);
+        if (ginv<n>(G, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+        mm<n, MM_SET>(R2, Tp, X);
+        if (t < n) S.wv[t] = 0.0 + mv_row<n>(R2, S.sp, t);
         team_sync();
-        if (ginv<n, RS>(X, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-        { double* tp = G; G = X; X = tp; }
-        mm<n, RS>(R2, Tp, X);
+        mm<n, MM_SET>(G, X, Y);
+        if (t < n) S.wv2[t] = mv_row<n>(G, S.wv, t);
         team_sync();
-        mm<n, RS>(G, X, Y);
+        mm<n, MM_ACC>(Tm, Y, Rm, Rm);
+        mm<n, MM_SET>(G, T2, X);
+        if (t < n) S.nsm[t] = S.sm[t] + mv_row<n>(Tm, S.wv2, t);
         team_sync();
-        mm<n, RS>(Tm, Y, X);
+        mm<n, MM_SET>(Tm, X, Y);  // new T- in Y
         team_sync();
-        for (int ii = 0; ii < R_; ii++) Rm[j * LD + r0 + ii] = Rm[j * LD + r0 + ii] + X[j * LD + r0 + ii];
-        mm<n, RS>(G, T2, X);
-        team_sync();
-        mm<n, RS>(Tm, X, Y);  // new T- in Y
-        if (t < n) S.wv[t] = 0.0 + mvr<n, RS>(R2, S.sp, t);
-        team_sync();
-        if (t < n) S.wv2[t] = mvr<n, RS>(G, S.wv, t);
-        team_sync();
-        if (t < n) S.nsm[t] = S.sm[t] + mvr<n, RS>(Tm, S.wv2, t);
-        team_sync();
-        { double* tp = Tm; Tm = Y; Y = tp; }
-        if (t < n) S.sm[t] = S.nsm[t];
-        // up side: empty stack -> R+ = 0, T+ = I, S+ = 0; reuse Rp/Tp/sp
-        for (int ii = 0; ii < R_; ii++) {
-          const int row = r0 + ii;
-          Rp[j * LD + row] = 0.0;
-          Tp[j * LD + row] = (row == j) ? 1.0 : 0.0;
-        }
-        if (t < n) S.sp[t] = 0.0;
-        // down side: R2 := new R-, T2 := new T-, s2m := sm
-        for (int e2 = t; e2 < MAT; e2 += T) { R2[e2] = Rm[e2]; T2[e2] = Tm[e2]; }
-        if (t < n) S.s2m[t] = S.sm[t];
-        team_sync();
-      } else if (pass == 0) {
-        if (t < n) S.s2m[t] = 0.0;  // surface source is zero
+        // up side: empty (R+ = 0, T+ = I, S+ = 0); down side: (new R-, new T-, new S-)
+        ew_zero<n>(Rp);
+        ew_ident<n>(Tp);
+        for (int ee = t; ee < MAT; ee += T) { R2[ee] = Rm[ee]; T2[ee] = Y[ee]; }
+        if (t < n) { S.sp[t] = 0.0; S.s2m[t] = S.nsm[t]; }
         team_sync();
       }
-      if (io < 0) continue;
       // INTERNAL_RADIANCE4 (src/radintg4.f90:119-172): up = (Rp, Tp, sp), down = (R2, T2, s2m)
-      mm<n, RS>(Rp, R2, X);
+      mm<n, MM_IMINUS>(Rp, R2, X);
+      if (t < n) S.wv[t] = mv_row<n>(T2, S.gnd, t);
       team_sync();
-      mat_ident_minus<n, RS>(X);
-      team_sync();
-      if (ginv<n, RS>(X, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-      if (t < n) S.wv[t] = mvr<n, RS>(T2, S.gnd, t);
-      team_sync();
+      if (ginv<n>(X, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
       if (t < n) {
-        double s = mvr<n, RS>(Rp, S.wv, t);
-        s = mvr<n, RS>(Tp, S.sky, t) + s;
-        s = mvr<n, RS>(Rp, S.s2m, t) + s;
+        double s = mv_row<n>(Rp, S.wv, t);
+        s = mv_row<n>(Tp, S.sky, t) + s;
+        s = mv_row<n>(Rp, S.s2m, t) + s;
         s = S.sp[t] + s;
         S.wv2[t] = s;
       }
       team_sync();
-      if (t < n) S.dnrad[t] = mvr<n, RS>(X, S.wv2, t);
+      if (t < n) S.dnrad[t] = mv_row<n>(X, S.wv2, t);
       team_sync();
-      mm<n, RS>(R2, Rp, X);
+      mm<n, MM_IMINUS>(R2, Rp, X);
+      if (t < n) S.wv[t] = mv_row<n>(Tp, S.sky, t);
       team_sync();
-      mat_ident_minus<n, RS>(X);
-      team_sync();
-      if (ginv<n, RS>(X, S.f, S.piv, S.redv, S.redi)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-      if (t < n) S.wv[t] = mvr<n, RS>(Tp, S.sky, t);
-      team_sync();
+      if (ginv<n>(X, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
       if (t < n) {
-        double s = mvr<n, RS>(R2, S.wv, t);
-        s = mvr<n, RS>(T2, S.gnd, t) + s;
-        s = mvr<n, RS>(R2, S.sp, t) + s;
+        double s = mv_row<n>(R2, S.wv, t);
+        s = mv_row<n>(T2, S.gnd, t) + s;
+        s = mv_row<n>(R2, S.sp, t) + s;
         s = S.s2m[t] + s;
         S.wv2[t] = s;
       }
       team_sync();
-      if (t < n) S.uprad[t] = mvr<n, RS>(X, S.wv2, t);
+      if (t < n) S.uprad[t] = mv_row<n>(X, S.wv2, t);
       team_sync();
       // collect_output + CONVERT_OUTPUT
       if (t < N) {

@@ -42,10 +42,10 @@ def host_inputs(cols, freqs):
     arrs = dict(cols)
     arrs["freqs"] = np.ascontiguousarray(np.asarray(freqs, dtype=np.float64))
     arrs["max_nfreq"] = len(freqs)
-    arrs["nhydro"] = cols["hydro_q"].shape[-1]
-    arrs["hydro_q"] = np.ascontiguousarray(cols["hydro_q"].reshape(cols["ncol"], cols["max_nlyrs"], -1))
-    arrs["hydro_n"] = np.ascontiguousarray(cols["hydro_n"].reshape(cols["ncol"], cols["max_nlyrs"], -1))
-    arrs["hydro_reff"] = np.ascontiguousarray(cols["hydro_reff"].reshape(cols["ncol"], cols["max_nlyrs"], -1))
+    nh = cols["hydro_q"].shape[-1]
+    arrs["nhydro"] = nh
+    for k in ("hydro_q", "hydro_n", "hydro_reff"):
+        arrs[k] = np.ascontiguousarray(cols[k].reshape(cols["ncol"], cols["max_nlyrs"], nh))
     return arrs
 
 

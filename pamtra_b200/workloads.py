@@ -1,4 +1,5 @@
-"""Seeded scenarios shared by tests, smoke and bench.
+"""Seeded synthetic workloads of the named shapes (shared by tests, smoke and
+bench).  No dataset is involved: the reference publishes none for this path.
 
 ``golden_pam`` rebuilds the reference's golden regression column
 (tests/_scenario.py:14-38 of the reference): rain (exp, N0 = 8e6, 30 bins)
@@ -18,8 +19,7 @@ import warnings
 
 import numpy as np
 
-import pamtra_b200 as pb
-from pamtra_b200 import meteoSI
+from . import core, importer, meteoSI
 
 GOLDEN_FREQS = [10.65, 35.5]
 C1_FREQS = [23.8, 31.4, 89.0]
@@ -39,10 +39,10 @@ RAIN_C1 = ("rwc_q", -99.0, 1, -99.0, -99.0, -99.0, -99.0, -99.0, 3, 50, "exp", -
 
 def golden_pam():
     warnings.simplefilter("ignore")
-    pam = pb.pyPamtra()
+    pam = core.pyPamtra()
     pam.df.addHydrometeor(RAIN_GOLDEN)
     pam.df.addHydrometeor(SNOW_GOLDEN)
-    pam = pb.importer.createUsStandardProfile(pam, hgt_lev=[0.0, 1000.0, 2000.0, 3000.0])
+    pam = importer.createUsStandardProfile(pam, hgt_lev=[0.0, 1000.0, 2000.0, 3000.0])
     pam.nmlSet["randomseed"] = 10
     pam.p["hydro_q"][0, 0, 1, 0] = 1e-3
     pam.p["hydro_q"][0, 0, 2, 1] = 5e-4
@@ -70,7 +70,7 @@ def _columns(ncol, nlay, seed, q_cloud=None, q_rain=None):
 
 def _pam_from(cols, ncol, nlay):
     warnings.simplefilter("ignore")
-    pam = pb.pyPamtra()
+    pam = core.pyPamtra()
     pam.df.addHydrometeor(CLOUD_C1)
     pam.df.addHydrometeor(RAIN_C1)
     pam.nmlSet["hydro_adaptive_grid"] = False
