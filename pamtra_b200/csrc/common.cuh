@@ -107,12 +107,13 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
 
 enum MMMode { MM_SET = 0, MM_ACC = 1, MM_IMINUS = 2 };
 
-// C = A*B (MM_SET), C = D + A*B (MM_ACC; D may be C itself) or C = I - A*B
-// (MM_IMINUS).  C must not alias A or B.  Each warp computes one 16 x 16 tile
-// with 2 x 2 DMMA fragments per k-step of 4.
-template <int n, int MODE>
-__device__ __forceinline__ void mm(const double* __restrict__ A, const double* __restrict__ B, double* C,
-                                   const double* D = nullptr) {
+// C = A*B (MM_SET), C = D + A*B (MM_ACC) or C = I - A*B (MM_IMINUS).
+// Each warp computes one 16 x 16 tile with 2 x 2 DMMA fragments per k-step
+// of 4.  Without INPLACE, C must not alias A or B; with INPLACE the team
+// synchronises between reading the operands and writing C, so C may be A,
+// B or D.
+template <int n, int MODE, bool INPLACE = false>
+__device__ __forceinline__ void mm(const double* A, const double* B, double* C, const double* D = nullptr) {
   constexpr int LD = Team<n>::LD, WT = n / 16;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int row0 = (warp / WT) * 16, col0 = (warp % WT) * 16;
@@ -139,6 +140,7 @@ __device__ __forceinline__ void mm(const double* __restrict__ A, const double* _
     dmma(c[1][0], a1, b0);
     dmma(c[1][1], a1, b1);
   }
+  if (INPLACE) team_sync();
 #pragma unroll
   for (int rt = 0; rt < 2; rt++)
 #pragma unroll
@@ -160,76 +162,93 @@ __device__ __forceinline__ double mv_row(const double* __restrict__ M, const dou
   return s;
 }
 
-// Scratch for ginv: f[n], fpre[n], prow[n] doubles; piv[n] + perm[n] + 2 ints.
+// Scratch of the inverse routines.
 template <int n>
 struct InvScratch {
   double f[n], fpre[n], prow[n];
+  double cand_v[4];
+  int cand_i[4];
   int piv[n], perm[n];
-  int p, sing;
+  double nrm;
+  int sing;
 };
 
-// In-place Gauss-Jordan inverse with partial (row) pivoting of A (n x n),
-// three team barriers per elimination step.  Returns nonzero to every
-// thread if a pivot was exactly zero.
+// Pivot candidate of rows i >= k among the n/32 (or one) warps of a column
+// group: the lanes hold rows i (value v of column k).
+template <int n>
+__device__ __forceinline__ void pivot_candidates(int i, int k, double v, InvScratch<n>& S) {
+  constexpr int W = (n >= 32) ? 32 : n;
+  S.fpre[i] = v;
+  double best = (i >= k) ? fabs(v) : -1.0;
+  int bi = i;
+  const unsigned mask = (n >= 32) ? 0xffffffffu : (((1u << n) - 1u) << (threadIdx.x & 31 & ~(n - 1)));
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(mask, best, o);
+    const int oi = __shfl_xor_sync(mask, bi, o);
+    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+  }
+  if ((i & (W - 1)) == 0) {
+    S.cand_v[i / W] = best;
+    S.cand_i[i / W] = bi;
+  }
+}
+
+// In-place Gauss-Jordan inverse with partial (row) pivoting of A (n x n).
+// Thread t owns row t % n of the columns cg, cg + CG, ... (cg = t / n,
+// CG = T / n), so every shared-memory sweep is bank-conflict free; the
+// pivot search of the next column is fused into the elimination, leaving
+// two team barriers per step.  Returns nonzero to every thread if a pivot
+// was exactly zero.
 template <int n>
 __device__ int ginv(double* A, InvScratch<n>& S) {
-  constexpr int LD = Team<n>::LD, T = Team<n>::T, RG = Team<n>::RG, NR = n / RG;
-  const int t = threadIdx.x, j = t % n, rg = t / n;
+  constexpr int LD = Team<n>::LD, T = Team<n>::T, CG = T / n, NC = n / CG, NGW = (n + 31) / 32;
+  const int t = threadIdx.x, i = t % n, cg = t / n;
+  if (cg == 0) pivot_candidates<n>(i, 0, A[i], S);
   if (t == 0) S.sing = 0;
+  team_sync();
   for (int k = 0; k < n; k++) {
-    // (a) warp 0: pivot search on column k, keep the column
-    if (t < 32) {
-      double best = -1.0;
-      int bi = t;
+    // (b) resolve the pivot, interchange rows k and p, scaled pivot row
+    int p = S.cand_i[0];
+    {
+      double bv = S.cand_v[0];
 #pragma unroll
-      for (int h = 0; h < (n + 31) / 32; h++) {
-        const int i = t + 32 * h;
-        if (i < n) {
-          const double v = A[k * LD + i];
-          S.fpre[i] = v;
-          const double av = (i >= k) ? fabs(v) : -1.0;
-          if (av > best) { best = av; bi = i; }
-        }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-      }
-      __syncwarp();
-      if (t == 0) {
-        S.p = bi;
-        S.piv[k] = bi;
-        if (S.fpre[bi] == 0.0) S.sing = 1;
-      }
+      for (int w = 1; w < NGW; w++)
+        if (S.cand_v[w] > bv) { bv = S.cand_v[w]; p = S.cand_i[w]; }
     }
-    team_sync();
-    // (b) row interchange k <-> p, pivot column after interchange, scaled pivot row
-    const int p = S.p;
-    const double rp = 1.0 / S.fpre[p];
+    const double pv = S.fpre[p];
+    const double rp = 1.0 / pv;
     if (t < n) {
-      const double fk = (t == k) ? S.fpre[p] : ((t == p) ? S.fpre[k] : S.fpre[t]);
-      S.f[t] = fk;
-      double akj = A[j * LD + p];  // row k after the interchange
+      const int j = t;
+      const double akj = A[j * LD + p];
       if (p != k) {
         A[j * LD + p] = A[j * LD + k];
         A[j * LD + k] = akj;
       }
       S.prow[j] = (j == k) ? rp : akj * rp;
+      S.f[t] = (t == k) ? pv : ((t == p) ? S.fpre[k] : S.fpre[t]);
+      if (t == 0) {
+        S.piv[k] = p;
+        if (pv == 0.0) S.sing = 1;
+      }
     }
     team_sync();
-    // (c) eliminate column k from every other row
-    const double pj = S.prow[j];
-#pragma unroll 4
-    for (int ii = 0; ii < NR; ii++) {
-      const int i = rg + RG * ii;
+    // (c) eliminate column k from every other row; the group that owns
+    // column k+1 also finds the next pivot
+    const double fi = S.f[i];
+    double vnext = 0.0;
+#pragma unroll
+    for (int jj = 0; jj < NC; jj++) {
+      const int j = cg + CG * jj;
+      const double pj = S.prow[j];
       double v;
       if (i == k) v = pj;
-      else if (j == k) v = -S.f[i] * rp;
-      else v = fma(-S.f[i], pj, A[j * LD + i]);
+      else if (j == k) v = -fi * rp;
+      else v = fma(-fi, pj, A[j * LD + i]);
       A[j * LD + i] = v;
+      if (j == k + 1) vnext = v;
     }
+    if (k + 1 < n && cg == (k + 1) % CG) pivot_candidates<n>(i, k + 1, vnext, S);
     team_sync();
   }
   // undo the row interchanges as column interchanges in reverse order
@@ -243,16 +262,68 @@ __device__ int ginv(double* A, InvScratch<n>& S) {
     }
   }
   team_sync();
-  double col[NR];
-  const int src = S.perm[j];
+  double col[NC];
 #pragma unroll
-  for (int ii = 0; ii < NR; ii++) col[ii] = A[src * LD + rg + RG * ii];
+  for (int jj = 0; jj < NC; jj++) col[jj] = A[S.perm[cg + CG * jj] * LD + i];
   team_sync();
 #pragma unroll
-  for (int ii = 0; ii < NR; ii++) A[j * LD + rg + RG * ii] = col[ii];
+  for (int jj = 0; jj < NC; jj++) A[(cg + CG * jj) * LD + i] = col[jj];
   team_sync();
-  (void)T;
   return S.sing;
+}
+
+// G = (I - X)^-1 in FP64.  X (in buffer P) is overwritten.  When the row-sum
+// norm of X is below 0.74 the inverse is the product (I + X)(I + X^2)(I + X^4)...
+// truncated where ||X||^(2^m) < 2^-54 (relative truncation error below the
+// FP64 rounding unit); otherwise Gauss-Jordan with partial pivoting is used.
+// Returns the buffer holding the inverse (P or G); *sing set on a zero pivot.
+template <int n>
+__device__ double* inv_iminus(double* P, double* G, InvScratch<n>& S, int* sing) {
+  constexpr int LD = Team<n>::LD, T = Team<n>::T;
+  const int t = threadIdx.x;
+  // infinity norm of X
+  if (t < n) {
+    double r = 0.0;
+#pragma unroll 8
+    for (int j = 0; j < n; j++) r += fabs(P[j * LD + t]);
+    const unsigned mask = (n >= 32) ? 0xffffffffu : ((1u << n) - 1u);
+#pragma unroll
+    for (int o = ((n >= 32) ? 16 : n / 2); o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(mask, r, o));
+    if ((t & 31) == 0) S.cand_v[t >> 5] = r;
+  }
+  team_sync();
+  double nrm = S.cand_v[0];
+#pragma unroll
+  for (int w = 1; w < (n + 31) / 32; w++) nrm = fmax(nrm, S.cand_v[w]);
+  int m = 1;
+  double pw = nrm;
+  while (pw > 5.0e-17 && m < 8) {
+    pw = pw * pw;
+    m++;
+  }
+  if (m >= 8) {
+    // Gauss-Jordan on I - X
+    for (int e = t; e < n * n; e += T) {
+      const int col = e / n, row = e % n;
+      P[col * LD + row] = ((row == col) ? 1.0 : 0.0) - P[col * LD + row];
+    }
+    team_sync();
+    if (ginv<n>(P, S)) *sing = 1;
+    return P;
+  }
+  // G = I + X
+  for (int e = t; e < n * n; e += T) {
+    const int col = e / n, row = e % n;
+    G[col * LD + row] = ((row == col) ? 1.0 : 0.0) + P[col * LD + row];
+  }
+  team_sync();
+  for (int k = 1; k < m; k++) {
+    mm<n, MM_SET, true>(P, P, P);     // P = P^2
+    team_sync();
+    mm<n, MM_ACC, true>(G, P, G, G);  // G = G + G P
+    team_sync();
+  }
+  return G;
 }
 
 }  // namespace pb

@@ -239,9 +239,14 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
     status |= S.stat;
     // ---------------- DOUBLING_INTEGRATION4, SYMMETRIC (src/radintg4.f90:174-309)
     for (int itd = 0; itd < nd; itd++) {
-      mm<n, MM_IMINUS>(Rb, Rb, Gb);  // I - R+ R-
+      mm<n, MM_SET>(Rb, Rb, Gb);  // R+ R-
       team_sync();
-      if (ginv<n>(Gb, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      {
+        int sg = 0;
+        double* gi = inv_iminus<n>(Gb, Wb, S.inv, &sg);  // GAMMA = inv(I - R+ R-)
+        if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+        if (gi != Gb) { Wb = Gb; Gb = gi; }
+      }
       // source chains: v = [S- + f C-, C-, S+, C+] -> R v -> add -> G -> T
       for (int o = t; o < 4 * n; o += T) {
         const int r = o % n, k = o / n;
@@ -472,9 +477,14 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
         continue;
       }
       // ---- general COMBINE_LAYERS4 (src/radintg4.f90:447-513), R2p = R2m, T2p = T2m
-      mm<n, MM_IMINUS>(Rp, R2, G);  // GAMMAp = inv(I - R1p R2m)
+      mm<n, MM_SET>(Rp, R2, G);  // GAMMAp = inv(I - R1p R2m)
       team_sync();
-      if (ginv<n>(G, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      {
+        int sg = 0;
+        double* gi = inv_iminus<n>(G, X, S.inv, &sg);
+        if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+        if (gi != G) { X = G; G = gi; }
+      }
       mm<n, MM_SET>(Rp, T2, X);  // RTp = R2p + T2p G R1p T2m
       if (t < n) S.wv[t] = S.sp[t] + mv_row<n>(Rp, S.s2m, t);  // STp chain
       team_sync();
@@ -485,10 +495,16 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
       mm<n, MM_SET>(G, Tp, X);      // TTp = T2p G T1p
       if (t < n) S.nsp[t] = S.s2p[t] + mv_row<n>(T2, S.wv2, t);
       team_sync();
-      mm<n, MM_SET>(T2, X, Y);              // new T+ in Y
-      mm<n, MM_IMINUS>(R2, Rp, G);          // GAMMAm = inv(I - R2m R1p); Gp is dead
+      mm<n, MM_SET>(T2, X, Y);  // new T+ in Y
       team_sync();
-      if (ginv<n>(G, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      mm<n, MM_SET>(R2, Rp, G);  // GAMMAm = inv(I - R2m R1p); Gp is dead
+      team_sync();
+      {
+        int sg = 0;
+        double* gi = inv_iminus<n>(G, X, S.inv, &sg);
+        if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+        if (gi != G) { X = G; G = gi; }
+      }
       mm<n, MM_SET>(R2, Tp, X);  // RTm = R1m + T1m G R2m T1p
       if (t < n) S.wv[t] = S.s2m[t] + mv_row<n>(R2, S.sp, t);  // STm chain
       team_sync();
@@ -568,9 +584,14 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
       if (io < 0) continue;
       if (pass == 1) {
         // down stack for level 1: (stack) on top of (surface), minus side only
-        mm<n, MM_IMINUS>(R2, Rp, G);  // GAMMAm = inv(I - Rsfc R1p)
+        mm<n, MM_SET>(R2, Rp, G);  // GAMMAm = inv(I - Rsfc R1p)
         team_sync();
-        if (ginv<n>(G, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+        {
+          int sg = 0;
+          double* gi = inv_iminus<n>(G, X, S.inv, &sg);
+          if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+          if (gi != G) { X = G; G = gi; }
+        }
         mm<n, MM_SET>(R2, Tp, X);
         if (t < n) S.wv[t] = 0.0 + mv_row<n>(R2, S.sp, t);
         team_sync();
@@ -591,10 +612,15 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
         team_sync();
       }
       // INTERNAL_RADIANCE4 (src/radintg4.f90:119-172): up = (Rp, Tp, sp), down = (R2, T2, s2m)
-      mm<n, MM_IMINUS>(Rp, R2, X);
+      mm<n, MM_SET>(Rp, R2, X);
       if (t < n) S.wv[t] = mv_row<n>(T2, S.gnd, t);
       team_sync();
-      if (ginv<n>(X, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      double* Ginv;
+      {
+        int sg = 0;
+        Ginv = inv_iminus<n>(X, G, S.inv, &sg);
+        if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      }
       if (t < n) {
         double s = mv_row<n>(Rp, S.wv, t);
         s = mv_row<n>(Tp, S.sky, t) + s;
@@ -603,12 +629,16 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
         S.wv2[t] = s;
       }
       team_sync();
-      if (t < n) S.dnrad[t] = mv_row<n>(X, S.wv2, t);
+      if (t < n) S.dnrad[t] = mv_row<n>(Ginv, S.wv2, t);
       team_sync();
-      mm<n, MM_IMINUS>(R2, Rp, X);
+      mm<n, MM_SET>(R2, Rp, X);
       if (t < n) S.wv[t] = mv_row<n>(Tp, S.sky, t);
       team_sync();
-      if (ginv<n>(X, S.inv)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      {
+        int sg = 0;
+        Ginv = inv_iminus<n>(X, G, S.inv, &sg);
+        if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+      }
       if (t < n) {
         double s = mv_row<n>(R2, S.wv, t);
         s = mv_row<n>(T2, S.gnd, t) + s;
@@ -617,7 +647,7 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
         S.wv2[t] = s;
       }
       team_sync();
-      if (t < n) S.uprad[t] = mv_row<n>(X, S.wv2, t);
+      if (t < n) S.uprad[t] = mv_row<n>(Ginv, S.wv2, t);
       team_sync();
       // collect_output + CONVERT_OUTPUT
       if (t < N) {
