@@ -183,6 +183,34 @@ int32_t pamtra_b200_eps_water_tkc(const double* t_c, const double* freq, double*
 int32_t pamtra_b200_minvert_batched(const double* a, double* ainv, int32_t* status, int32_t n, int32_t count,
                                     void* stream);
 
+/* ---- allocation-free single column ----
+ * No counterpart in the reference (its Fortran owns module-global arrays).
+ * For callers that cannot call cudaMalloc: hosts whose own device memory
+ * manager owns all allocations and forbids outside ones, and latency-critical
+ * callers that cannot accept the device-wide synchronisation an allocation
+ * implies.  Runs the plain form (one column, same kernels as
+ * pamtra_b200_run) with all scratch in a fixed static device array of
+ * PAMTRA_B200_NOALLOC_SCRATCH_MIB MiB that every GPU loading this library
+ * keeps until the process exits.  No context is needed and nothing is
+ * allocated: no cudaMalloc, cudaFree, pinned host memory or library
+ * allocator.  All pointers in `cols` and `out` are DEVICE pointers,
+ * `cols->species` included.  Limits: ncol = 1, max_nlyrs <= 64,
+ * max_nfreq <= 4, nhydro <= 4, nbin <= 64 per species, nummu 8 or 16,
+ * noutlevels <= 2; larger requests return PAMTRA_B200_FATAL |
+ * PAMTRA_B200_ST_SIZE without running.  The first call on a device (with
+ * that device current) resolves the array's device address with
+ * cudaGetSymbolAddress and fills the quadrature and line tables; make that
+ * first call before any stream capture.  Every call shares the one array and
+ * clears what must start at zero, so calls that overlap on the GPU (other
+ * streams, other host threads) race: serialise them. */
+#define PAMTRA_B200_NOALLOC_SCRATCH_MIB 8
+#define PAMTRA_B200_NOALLOC_MAX_NLYRS 64
+#define PAMTRA_B200_NOALLOC_MAX_NFREQ 4
+#define PAMTRA_B200_NOALLOC_MAX_NHYDRO 4
+#define PAMTRA_B200_NOALLOC_MAX_NBIN 64
+int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* settings, const pamtra_b200_columns* cols,
+                                const pamtra_b200_outputs* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -694,3 +694,152 @@ int32_t pamtra_b200_minvert_batched(const double* a, double* ainv, int32_t* stat
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- allocation-free single column
+// Scratch of pamtra_b200_run_noalloc: a fixed, file-scope device array, so the
+// entry point never calls an allocator.  Every GPU that loads this library
+// holds it until the process exits.  Its capacity bounds the column sizes the
+// entry point accepts (see PAMTRA_B200_NOALLOC_* in the header).
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)PAMTRA_B200_NOALLOC_SCRATCH_MIB << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+// quadrature tables of the allocation-free path (filled at per-device set-up)
+constexpr int NOALLOC_GQ = 256;
+static __device__ __align__(256) double g_noalloc_tables[2 * (NOALLOC_GQ * (NOALLOC_GQ + 1) / 2) + 2 * 56];
+
+namespace {
+struct NoallocDevice {
+  int ready = 0;
+  char* scratch = nullptr;  // device address of g_noalloc_scratch
+  double* tables = nullptr; // device address of g_noalloc_tables
+};
+NoallocDevice g_noalloc_dev[64];
+std::mutex g_noalloc_mu;
+}  // namespace
+
+extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const pamtra_b200_columns* cols,
+                                           const pamtra_b200_outputs* out, void* stream_) {
+  if (!st || !cols || !out || !out->tb) return PAMTRA_B200_FATAL;
+  cudaStream_t stream = (cudaStream_t)stream_;
+  // size limits of the static scratch
+  if (cols->ncol != 1 || cols->max_nlyrs < 2 || cols->max_nlyrs > PAMTRA_B200_NOALLOC_MAX_NLYRS ||
+      cols->max_nfreq < 1 || cols->max_nfreq > PAMTRA_B200_NOALLOC_MAX_NFREQ || cols->nhydro < 0 ||
+      cols->nhydro > PAMTRA_B200_NOALLOC_MAX_NHYDRO || cols->noutlevels < 1 || cols->noutlevels > 2 ||
+      !(cols->max_nummu == 8 || cols->max_nummu == 16) || !(st->nummu == 8 || st->nummu == 16) ||
+      (cols->nhydro > 0 && !cols->species))
+    return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PAMTRA_B200_FATAL;
+  NoallocDevice& D = g_noalloc_dev[dev];
+  {
+    // once per device, with that device current: resolve the device addresses
+    // of the static arrays and fill the tables
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!D.ready) {
+      void* sp = nullptr;
+      void* tp = nullptr;
+      if (cudaGetSymbolAddress(&sp, g_noalloc_scratch) != cudaSuccess) return PAMTRA_B200_FATAL;
+      if (cudaGetSymbolAddress(&tp, g_noalloc_tables) != cudaSuccess) return PAMTRA_B200_FATAL;
+      if (set_smem_attrs()) return PAMTRA_B200_FATAL;
+      double* tab = (double*)tp;
+      const size_t gqn = (size_t)NOALLOC_GQ * (NOALLOC_GQ + 1) / 2;
+      k_gauss_table<<<NOALLOC_GQ, 128, 0, stream>>>(tab, tab + gqn);
+      k_lobatto_table<<<3, 32, 0, stream>>>(tab + 2 * gqn, tab + 2 * gqn + 56);
+      double la[MAXNLEG], lb[MAXNLEG];
+      la[0] = 0.0;
+      lb[0] = 0.0;
+      for (int l = 1; l < MAXNLEG; l++) {
+        la[l] = (2.0 * l - 1.0) / l;
+        lb[l] = (l - 1.0) / l;
+      }
+      if (cudaMemcpyToSymbol(c_leg_a, la, sizeof(la)) || cudaMemcpyToSymbol(c_leg_b, lb, sizeof(lb)) ||
+          cudaMemcpyToSymbol(c_o2_w300, H_O2_W300, sizeof(H_O2_W300)) ||
+          cudaMemcpyToSymbol(c_o2_y300, H_O2_Y300, sizeof(H_O2_Y300)) ||
+          cudaMemcpyToSymbol(c_o2_v, H_O2_V, sizeof(H_O2_V)) || cudaMemcpyToSymbol(c_o2_f, H_O2_F, sizeof(H_O2_F)) ||
+          cudaMemcpyToSymbol(c_o2_s300, H_O2_S300, sizeof(H_O2_S300)) ||
+          cudaMemcpyToSymbol(c_o2_be, H_O2_BE, sizeof(H_O2_BE)) ||
+          cudaMemcpyToSymbol(c_h2o_fl, H_H2O_FL, sizeof(H_H2O_FL)) ||
+          cudaMemcpyToSymbol(c_h2o_s1, H_H2O_S1, sizeof(H_H2O_S1)) ||
+          cudaMemcpyToSymbol(c_h2o_b2, H_H2O_B2, sizeof(H_H2O_B2)) ||
+          cudaMemcpyToSymbol(c_h2o_w3, H_H2O_W3, sizeof(H_H2O_W3)) ||
+          cudaMemcpyToSymbol(c_h2o_x, H_H2O_X, sizeof(H_H2O_X)) ||
+          cudaMemcpyToSymbol(c_h2o_ws, H_H2O_WS, sizeof(H_H2O_WS)) ||
+          cudaMemcpyToSymbol(c_h2o_xs, H_H2O_XS, sizeof(H_H2O_XS)))
+        return PAMTRA_B200_FATAL;
+      if (cudaStreamSynchronize(stream) != cudaSuccess) return PAMTRA_B200_FATAL;
+      D.scratch = (char*)sp;
+      D.tables = tab;
+      D.ready = 1;
+    }
+  }
+  // scratch layout (same plan as the arena of pamtra_b200_run); bins are
+  // sized for PAMTRA_B200_NOALLOC_MAX_NBIN
+  pamtra_b200_columns cc = *cols;
+  pamtra_b200_species plan_sp{};
+  plan_sp.nbin = PAMTRA_B200_NOALLOC_MAX_NBIN;
+  cc.species = &plan_sp;
+  cc.species_stride = 0;
+  const int nh = cc.nhydro;
+  cc.nhydro = nh > 0 ? nh : 0;
+  Plan pl = make_plan(&cc, st->nummu);
+  if (pl.total > NOALLOC_SCRATCH_BYTES || pl.maxN > 16) return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
+  const int mask = cc.nummu_mask ? cc.nummu_mask : (st->nummu == 8 ? 1 : 2);
+  if (mask & 4) return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
+  char* A = D.scratch;
+  const size_t gqn = (size_t)NOALLOC_GQ * (NOALLOC_GQ + 1) / 2;
+  Batch b{};
+  b.ncol = 1; b.max_nlyrs = cc.max_nlyrs; b.nhydro = nh; b.max_nfreq = cc.max_nfreq;
+  b.noutlevels = cc.noutlevels; b.max_nummu = cc.max_nummu; b.max_nbin = pl.max_nbin;
+  b.species_stride = 0; b.default_nummu = st->nummu; b.species = cols->species;  // device pointer here
+  b.nlyrs = cc.nlyrs; b.nummu = cc.nummu; b.nfreq = cc.nfreq; b.freqs = cc.freqs; b.freq_per_col = cc.nfreq != nullptr;
+  b.hgt_lev = cc.hgt_lev; b.temp_lev = cc.temp_lev; b.press_lev = cc.press_lev; b.relhum_lev = cc.relhum_lev;
+  b.hgt = cc.hgt; b.temp = cc.temp; b.press = cc.press; b.relhum = cc.relhum;
+  b.hydro_q = cc.hydro_q; b.hydro_n = cc.hydro_n; b.hydro_reff = cc.hydro_reff;
+  b.groundtemp = cc.groundtemp; b.obs_height = cc.obs_height; b.sfc_refl = cc.sfc_refl;
+  Work w{};
+  w.hgt_lev = (double*)(A + pl.o_hgt_lev); w.temp_lev = (double*)(A + pl.o_temp_lev);
+  w.temp = (double*)(A + pl.o_temp); w.press = (double*)(A + pl.o_press);
+  w.rho_vap = (double*)(A + pl.o_rho_vap); w.q_hum = (double*)(A + pl.o_q_hum);
+  w.gtemp = (double*)(A + pl.o_gtemp); w.outlev = (int*)(A + pl.o_outlev); w.kgas = (double*)(A + pl.o_kgas);
+  w.slot_st = (int8_t*)(A + pl.o_slot_st); w.slot_nb = (int*)(A + pl.o_slot_nb);
+  w.b_d = (double*)(A + pl.o_bd); w.b_dd = (double*)(A + pl.o_bdd); w.b_nd = (double*)(A + pl.o_bnd);
+  w.b_rho = (double*)(A + pl.o_brho); w.b_mass = (double*)(A + pl.o_bmass);
+  w.pres_idx = (int*)(A + pl.o_pres_idx); w.plist = (int*)(A + pl.o_plist); w.pmax = pl.pmax;
+  w.counters = (int*)(A + pl.o_counters);
+  w.m_kext = (double*)(A + pl.o_mkext); w.m_salb = (double*)(A + pl.o_msalb); w.m_nleg = (int*)(A + pl.o_mnleg);
+  w.m_legen = (double*)(A + pl.o_mlegen);
+  w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
+  w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
+  w.gq_x = D.tables; w.gq_w = D.tables + gqn; w.gq_max = NOALLOC_GQ;
+  w.lob_mu = D.tables + 2 * gqn; w.lob_w = D.tables + 2 * gqn + 56;
+  const size_t Lm = cc.max_nlyrs, Fm = cc.max_nfreq;
+  // the scratch keeps the previous call's contents: clear what must start at zero
+  cudaMemsetAsync(w.counters, 0, 16 * 4, stream);
+  cudaMemsetAsync(w.status, 0, Fm * 4, stream);
+  cudaMemsetAsync(w.col_status, 0, 4, stream);
+  const size_t ntb = (size_t)cc.noutlevels * 2 * cc.max_nummu * Fm * 2;
+  k_fill_d<<<(unsigned)((ntb + 255) / 256), 256, 0, stream>>>(out->tb, -9999.0, ntb);
+  k_atmo<<<1, 128, 0, stream>>>(b, w);
+  k_gas<<<(unsigned)((Fm * Lm + 255) / 256), 256, 0, stream>>>(b, w, st->lgas_extinction);
+  if (nh > 0) k_psd<<<(unsigned)((Lm * nh + 127) / 128), 128, 0, stream>>>(b, w, *st);
+  k_compact<<<1, 1024, 0, stream>>>(b, w);
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (nh > 0) {
+    const size_t sm_mie = MIE_WARPS * sizeof(MieSmem);
+    k_mie<<<sms, 32 * MIE_WARPS, sm_mie, stream>>>(b, w, *st);
+  }
+  if (mask & 1) {
+    if (nh > 0) k_layer<8><<<sms, RTCfg<8>::T, sizeof(LayerSmem<8>), stream>>>(b, w, *st, out->scatter_matrix);
+    k_adding<8><<<sms, RTCfg<8>::T, sizeof(AddSmem<8>), stream>>>(b, w, *st, *out);
+  }
+  if (mask & 2) {
+    if (nh > 0) k_layer<16><<<sms, RTCfg<16>::T, sizeof(LayerSmem<16>), stream>>>(b, w, *st, out->scatter_matrix);
+    k_adding<16><<<sms, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out);
+  }
+  if (out->angles_deg) k_angles<<<1, 32, 0, stream>>>(out->angles_deg, w.lob_mu, cc.max_nummu);
+  if (out->kexttot || out->salbedo || out->num_doubles)
+    k_ssp_out<<<(unsigned)((Fm * Lm + 255) / 256), 256, 0, stream>>>(b, w, *out);
+  if (out->kextatmo) cudaMemcpyAsync(out->kextatmo, w.kgas, Fm * Lm * 8, cudaMemcpyDeviceToDevice, stream);
+  if (out->status) k_status_out<<<1, 256, 0, stream>>>(w, out->status, (int)Fm);
+  return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
+}
