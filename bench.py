@@ -47,6 +47,8 @@ def _args():
     ap.add_argument("--ncol", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=0, help="columns for the CPU baseline (0 = 2 per core)")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=24, help="requests in the serving replay (0 = skip)")
+    ap.add_argument("--target-cols", type=int, default=1024, help="columns of the 150-layer target batch (0 = skip)")
     return ap.parse_args()
 
 
@@ -179,6 +181,11 @@ def fp64_peak_tflops(dev):
     return best
 
 
+# k_layer<16> DRAM traffic per (layer, frequency) item: ncu capture of the
+# 256-column run (21,504 items): 13.1 MB read + 349.2 MB written per launch
+LAYER_TRAFFIC_PER_ITEM = (13.093632e6 + 349.194752e6) / 21504
+
+
 def layer_flops(nd, N):
     """Algorithmic FLOPs of the doubling stage: per scattering layer and
     frequency, each doubling is 6 n x n products and one inverse (2 n^3
@@ -186,6 +193,88 @@ def layer_flops(nd, N):
     n = 2 * N
     d = nd[nd > 0].astype(np.float64)
     return float(np.sum(d) * 7 * 2 * n ** 3)
+
+
+def _target_shape(args, local, eng, stream):
+    """The 150-layer, 16-angle, 4-species shape: batched FP64 over
+    ``--target-cols`` columns (device-timed, L2 flushed) against the plain
+    form (one column per call) on 16 of them."""
+    import torch
+    from pamtra_b200 import batch as pbatch
+    from pamtra_b200.workloads import target_batch
+    dev = torch.device("cuda", local)
+    b = target_batch(args.target_cols, seed=4)
+    out = b.alloc_outputs(dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            pbatch.run(b, local, out, stream=stream, eng=eng)
+    stream.synchronize()
+    ms = []
+    for _ in range(3):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            pbatch.run(b, local, out, stream=stream, eng=eng)
+            e.record(stream)
+        e.synchronize()
+        ms.append(s.elapsed_time(e))
+    batched = b.n_solves() / (np.mean(ms) * 1e-3)
+    st_bad = int((out["status"] != 0).sum())
+    singles = [pbatch.subset(b, [c]) for c in range(16)]
+    souts = [sb.alloc_outputs(dev) for sb in singles]
+    with torch.cuda.stream(stream):
+        for sb, so in zip(singles, souts):
+            pbatch.run(sb, local, so, stream=stream, eng=eng)
+    stream.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        s.record(stream)
+        for sb, so in zip(singles, souts):
+            pbatch.run(sb, local, so, stream=stream, eng=eng)
+        e.record(stream)
+    e.synchronize()
+    plain = sum(sb.n_solves() for sb in singles) / (s.elapsed_time(e) * 1e-3)
+    tb = out["tb"].cpu().numpy()
+    same = all(np.array_equal(so["tb"].cpu().numpy()[0], tb[c]) for c, so in enumerate(souts))
+    del flush
+    return {"workload": "%d columns x 150 layers (0-15 km), NUMMU=16, 4 Mie species (cloud water, cloud ice, "
+                        "snow, rain; 40 bins each), f = 23.8/31.4/89/150 GHz" % args.target_cols,
+            "batched_fp64": batched, "plain_fp64": plain, "batched_over_plain": batched / plain,
+            "unit": "solves/s", "batched_ms_per_step": float(np.mean(ms)), "status_nonzero": st_bad,
+            "plain_sample_columns": 16, "plain_equals_batched_bitwise": bool(same)}
+
+
+def _serving(args, local):
+    """Replay a seeded Poisson stream (200 requests/s) of uneven requests
+    through the continuous-batching server; the plain form (one column per
+    call, one slot) serves the first three requests of the same stream."""
+    from pamtra_b200 import serve
+    reqs = serve.request_stream(args.serve_requests, seed=5, max_cols=512, nfreq_range=(1, 32))
+    arr = serve.poisson_arrivals(len(reqs), 200.0, seed=6)
+    warm = serve.request_stream(3, seed=7, max_cols=16, nfreq_range=(1, 4))
+    srv = serve.Server(local, slots=3, hbm_fraction=0.5, max_cols=2048)
+    for b in warm:
+        srv.submit(b)
+    srv.drain()
+    done, wall = serve.replay(srv, reqs, arr)
+    nb = srv.batches_launched
+    srv.close()
+    solves = sum(r.n_solves() for r in done)
+    errs = sum(1 for r in done if r.error)
+    res = {"stream": "%d requests, Poisson 200/s (seed 6); each 1-512 columns of 40-150 layers, 1-5 species, "
+                     "1-32 frequencies in 10-183 GHz, NUMMU in {8,16,32}" % len(reqs),
+           "batched_fp64": dict(serve.latency_stats(done), solves_per_s=solves / wall, solves=solves,
+                                wall_s=wall, batches=nb - len(warm), requests_with_error=errs, slots=3)}
+    k = min(3, len(reqs))
+    psrv = serve.Server(local, slots=1, hbm_fraction=0.2, max_cols=1)
+    pdone, pwall = serve.replay(psrv, reqs[:k], arr[:k])
+    psrv.close()
+    psolves = sum(r.n_solves() for r in pdone)
+    res["plain_fp64"] = dict(serve.latency_stats(pdone), solves_per_s=psolves / pwall, solves=psolves,
+                             wall_s=pwall, requests=k)
+    return res
 
 
 # ---------------------------------------------------------------- reference arm
@@ -329,14 +418,21 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
+    target = _target_shape(args, local, eng, stream) if args.target_cols > 0 else None
+    serving = _serving(args, local) if args.serve_requests > 0 else None
     # ---- roofline of the dominant kernel (doubling stage)
     peak = fp64_peak_tflops(dev)
     t_layer = stage_tot.get("layer", 0.0) / args.steps * 1e-3
     flops = layer_flops(nd, 16)
     achieved = flops / t_layer / 1e12 if t_layer > 0 else 0.0
-    roofline = {"bound": "fp64", "kernel": "k_layer<16> (scatcnv + init + doubling)", "achieved": achieved,
-                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None, "traffic": None,
-                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 pipe)",
+    items = int(np.count_nonzero(nd >= 0))
+    roofline = {"bound": "tensor", "pipe": "FP64 tensor (DMMA)", "kernel": "k_layer<16> (scatcnv + init + doubling)",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                "traffic": LAYER_TRAFFIC_PER_ITEM * items,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at 256 columns "
+                                  "(21,504 items), scaled by the %d items of this launch" % items,
+                "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe); "
+                               "MEASURED_PEAKS.json carries bf16 and HBM only",
                 "flops_per_launch": flops, "kernel_ms": t_layer * 1e3}
     # ---- CPU baseline + TB error vs the oracle on the same columns
     cpu = None
@@ -369,6 +465,8 @@ def main():
         "batched_over_plain": value / world / plain_value,
         "tb_err_vs_oracle_K": tb_err,
         "stage_ms": {k: v / args.steps for k, v in stage_tot.items()},
+        "target_shape": target,
+        "serving": serving,
         "status_nonzero": int(np.count_nonzero(status)),
     }
     print(json.dumps(line))

@@ -176,7 +176,7 @@ class Engine(object):
             raise MemoryError("cannot reserve %d bytes of device scratch" % nbytes)
 
     def workspace_bytes(self, columns, precision=PREC_FP64):
-        return int(self.lib.pamtra_b200_workspace_bytes(ctypes.byref(columns), int(precision)))
+        return workspace_bytes(columns, precision=precision)
 
     def last_launch_count(self):
         return int(self.lib.pamtra_b200_last_launch_count(self.handle))
@@ -189,6 +189,13 @@ class Engine(object):
         buf = (ctypes.c_float * len(STAGES))()
         self.lib.pamtra_b200_stage_ms(self.handle, buf, len(STAGES))
         return dict(zip(STAGES, [float(v) for v in buf]))
+
+
+def workspace_bytes(columns, species=None, precision=PREC_FP64):
+    """Scratch bytes a batch needs (pamtra_b200_workspace_bytes; no device
+    work).  ``species`` only keeps the array behind columns.species alive."""
+    del species
+    return int(load().pamtra_b200_workspace_bytes(ctypes.byref(columns), int(precision)))
 
 
 def abi_sizes():

@@ -181,7 +181,8 @@ struct Plan {
   size_t o_hgt_lev, o_temp_lev, o_temp, o_press, o_rho_vap, o_q_hum, o_gtemp, o_outlev, o_kgas;
   size_t o_slot_st, o_slot_nb, o_bd, o_bdd, o_bnd, o_brho, o_bmass;
   size_t o_pres_idx, o_plist, o_counters, o_mkext, o_msalb, o_mnleg, o_mlegen, o_lay, o_laynd, o_status, o_colst;
-  size_t o_species;
+  size_t o_species, o_addscr;
+  int add_grid;  // CTAs of k_adding<32> the scratch is sized for
   int pmax;
   int max_nbin;
   int maxN;
@@ -192,7 +193,7 @@ size_t lay_stride_for(int N) {
   return (lay_stride_n(N) + 1) & ~(size_t)1;  // keep 16-byte alignment of each item
 }
 
-Plan make_plan(const pamtra_b200_columns* c, int default_nummu) {
+Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms) {
   Plan p{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -239,6 +240,8 @@ Plan make_plan(const pamtra_b200_columns* c, int default_nummu) {
   p.o_status = take(C * Fm * 4);
   p.o_colst = take(C * 4);
   p.o_species = take(std::max<size_t>(nsp, 1) * sizeof(pamtra_b200_species));
+  p.add_grid = (mask & 4) ? std::max(1, sms) : 0;
+  p.o_addscr = take((size_t)p.add_grid * (10 - AddSmem<32>::NS) * RTCfg<32>::MAT * 8);
   p.total = take(0) + 256;
   return p;
 }
@@ -291,8 +294,18 @@ struct pamtra_b200_ctx {
   double* gq_w = nullptr;
   double* lob_mu = nullptr;
   double* lob_w = nullptr;
-  pamtra_b200_species* h_species = nullptr;  // pinned staging
-  size_t h_species_cap = 0;
+  // species tables: pinned staging ring and the table last left in the arena
+  static constexpr int NSP_RING = 3;
+  struct SpStage {
+    pamtra_b200_species* h = nullptr;
+    size_t cap = 0;
+    cudaEvent_t ev = nullptr;
+    int used = 0;
+  } sp_ring[NSP_RING];
+  int sp_next = 0;
+  std::vector<unsigned char> sp_last;
+  const char* sp_last_arena = nullptr;
+  size_t sp_last_off = 0;
   int last_launches = 0;
   char* stage = nullptr;  // device staging for run_host
   size_t stage_bytes = 0;
@@ -326,6 +339,7 @@ static int set_smem_attrs() {
     set((const void*)k_layer<32>, sizeof(LayerSmem<32>));
     set((const void*)k_adding<8>, sizeof(AddSmem<8>));
     set((const void*)k_adding<16>, sizeof(AddSmem<16>));
+    set((const void*)k_adding<32>, sizeof(AddSmem<32>));
     set((const void*)k_minvert<64>, Team<64>::MAT * 8 + sizeof(InvScratch<64>));
   });
   return rc;
@@ -389,7 +403,10 @@ int32_t pamtra_b200_destroy(pamtra_b200_ctx* ctx) {
   cudaFree(ctx->lob_mu);
   cudaFree(ctx->lob_w);
   cudaFree(ctx->stage);
-  if (ctx->h_species) cudaFreeHost(ctx->h_species);
+  for (auto& sg : ctx->sp_ring) {
+    if (sg.ev) cudaEventSynchronize(sg.ev), cudaEventDestroy(sg.ev);
+    if (sg.h) cudaFreeHost(sg.h);
+  }
   for (int i = 0; i < 16; i++)
     if (ctx->ev[i]) cudaEventDestroy(ctx->ev[i]);
   delete ctx;
@@ -399,7 +416,9 @@ int32_t pamtra_b200_destroy(pamtra_b200_ctx* ctx) {
 size_t pamtra_b200_workspace_bytes(const pamtra_b200_columns* cols, int32_t precision) {
   (void)precision;
   if (!cols || !cols->species) return 0;
-  return make_plan(cols, 16).total;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return make_plan(cols, 16, sms).total;
 }
 
 int32_t pamtra_b200_reserve(pamtra_b200_ctx* ctx, size_t bytes) {
@@ -409,6 +428,7 @@ int32_t pamtra_b200_reserve(pamtra_b200_ctx* ctx, size_t bytes) {
   cudaFree(ctx->arena);
   ctx->arena = nullptr;
   ctx->arena_bytes = 0;
+  ctx->sp_last_arena = nullptr;  // the arena contents are gone
   if (cudaMalloc(&ctx->arena, bytes) != cudaSuccess) return PAMTRA_B200_FATAL;
   ctx->arena_bytes = bytes;
   return PAMTRA_B200_OK;
@@ -456,7 +476,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   pamtra_b200_species dummy{};
   pamtra_b200_columns cc = *cols;
   if (cc.nhydro == 0) { cc.species = &dummy; cc.species_stride = 0; }
-  Plan pl = make_plan(&cc, st->nummu);
+  Plan pl = make_plan(&cc, st->nummu, ctx->sm_count);
   if (pl.max_nbin > MAXBIN) return PAMTRA_B200_FATAL;
   if (pl.total > ctx->arena_bytes) {
     cudaStreamSynchronize(stream);
@@ -464,21 +484,37 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   }
   const int mask = cc.nummu_mask ? cc.nummu_mask : (st->nummu == 8 ? 1 : st->nummu == 16 ? 2 : 4);
   if (pl.maxN > cc.max_nummu) return PAMTRA_B200_FATAL;
-  if (mask & 4) return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;  // N=32 adding not available in this build
   char* A = ctx->arena;
-  // species table -> device (pinned staging so the copy is stream ordered)
+  // species table -> device.  The table the previous run left in the arena is
+  // reused when it is byte-identical and at the same place (no host wait, so
+  // steady-state runs can be captured in a CUDA graph); otherwise it goes
+  // through a ring of pinned staging buffers, waiting only for a buffer whose
+  // previous copy is still queued.
   const size_t nsp = cc.species_stride ? (size_t)cc.ncol * cc.nhydro : (size_t)std::max(cc.nhydro, 1);
-  if (nsp > ctx->h_species_cap) {
-    cudaStreamSynchronize(stream);
-    if (ctx->h_species) cudaFreeHost(ctx->h_species);
-    if (cudaMallocHost(&ctx->h_species, nsp * sizeof(pamtra_b200_species)) != cudaSuccess) return PAMTRA_B200_FATAL;
-    ctx->h_species_cap = nsp;
-  } else {
-    cudaStreamSynchronize(stream);  // staging buffer may still be read by a previous copy
-  }
-  std::memcpy(ctx->h_species, cc.species, nsp * sizeof(pamtra_b200_species));
+  const size_t spb = nsp * sizeof(pamtra_b200_species);
   pamtra_b200_species* d_species = (pamtra_b200_species*)(A + pl.o_species);
-  cudaMemcpyAsync(d_species, ctx->h_species, nsp * sizeof(pamtra_b200_species), cudaMemcpyHostToDevice, stream);
+  const bool cached = ctx->sp_last_arena == A && ctx->sp_last_off == pl.o_species && ctx->sp_last.size() == spb &&
+                      std::memcmp(ctx->sp_last.data(), cc.species, spb) == 0;
+  if (!cached) {
+    pamtra_b200_ctx::SpStage& sg = ctx->sp_ring[ctx->sp_next];
+    ctx->sp_next = (ctx->sp_next + 1) % pamtra_b200_ctx::NSP_RING;
+    if (sg.used && cudaEventSynchronize(sg.ev) != cudaSuccess) return PAMTRA_B200_FATAL;
+    if (spb > sg.cap) {
+      if (sg.h) cudaFreeHost(sg.h);
+      sg.h = nullptr;
+      sg.cap = 0;
+      if (cudaMallocHost(&sg.h, spb) != cudaSuccess) return PAMTRA_B200_FATAL;
+      sg.cap = spb;
+    }
+    if (!sg.ev && cudaEventCreateWithFlags(&sg.ev, cudaEventDisableTiming) != cudaSuccess) return PAMTRA_B200_FATAL;
+    std::memcpy(sg.h, cc.species, spb);
+    cudaMemcpyAsync(d_species, sg.h, spb, cudaMemcpyHostToDevice, stream);
+    cudaEventRecord(sg.ev, stream);
+    sg.used = 1;
+    ctx->sp_last.assign((const unsigned char*)cc.species, (const unsigned char*)cc.species + spb);
+    ctx->sp_last_arena = A;
+    ctx->sp_last_off = pl.o_species;
+  }
 
   Batch b{};
   b.ncol = cc.ncol; b.max_nlyrs = cc.max_nlyrs; b.nhydro = cc.nhydro; b.max_nfreq = cc.max_nfreq;
@@ -504,6 +540,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   w.m_legen = (double*)(A + pl.o_mlegen);
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
+  w.add_scr = (double*)(A + pl.o_addscr);
   w.gq_x = ctx->gq_x; w.gq_w = ctx->gq_w; w.gq_max = GQ_MAX; w.lob_mu = ctx->lob_mu; w.lob_w = ctx->lob_w;
 
   int launches = 0;
@@ -549,6 +586,14 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     mark(ctx, stream, STG_LAYER);
     g = occupancy_blocks((const void*)k_adding<16>, RTCfg<16>::T, sizeof(AddSmem<16>), sms);
     k_adding<16><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out); launches++;
+    mark(ctx, stream, STG_ADDING);
+  }
+  if (mask & 4) {
+    int g = occupancy_blocks((const void*)k_layer<32>, RTCfg<32>::T, sizeof(LayerSmem<32>), sms);
+    if (H > 0) { k_layer<32><<<g, RTCfg<32>::T, sizeof(LayerSmem<32>), stream>>>(b, w, *st, ssp); launches++; }
+    mark(ctx, stream, STG_LAYER);
+    g = std::min(occupancy_blocks((const void*)k_adding<32>, RTCfg<32>::T, sizeof(AddSmem<32>), sms), pl.add_grid);
+    k_adding<32><<<g, RTCfg<32>::T, sizeof(AddSmem<32>), stream>>>(b, w, *st, *out); launches++;
     mark(ctx, stream, STG_ADDING);
   }
   if (out->angles_deg) { k_angles<<<1, 32, 0, stream>>>(out->angles_deg, ctx->lob_mu, cc.max_nummu); launches++; }
@@ -780,7 +825,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   cc.species_stride = 0;
   const int nh = cc.nhydro;
   cc.nhydro = nh > 0 ? nh : 0;
-  Plan pl = make_plan(&cc, st->nummu);
+  Plan pl = make_plan(&cc, st->nummu, 0);
   if (pl.total > NOALLOC_SCRATCH_BYTES || pl.maxN > 16) return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
   const int mask = cc.nummu_mask ? cc.nummu_mask : (st->nummu == 8 ? 1 : 2);
   if (mask & 4) return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;

@@ -195,10 +195,8 @@ __global__ void __launch_bounds__(32 * MIE_WARPS) k_mie(Batch b, Work w, pamtra_
           }
         }
       };
-      double rho0, dia0, rhoN, diaN;
-      dens_diam(0, rho0, dia0);
+      double rhoN, diaN;
       dens_diam(nb - 1, rhoN, diaN);
-      const bool use_mix = (sp.liq_ice == -1) && (rho0 != 917.0);
       const double xmax = PI * diaN / wl;
       const int nterms = mie_nstop(xmax);
       int nlegen = min(MAXNLEG - 1, 2 * nterms);

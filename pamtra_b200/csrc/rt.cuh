@@ -324,10 +324,15 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
 }
 
 // ============================================================== adding kernel
+// Ten n x n matrices per column-frequency unit.  For N <= 16 all of them live
+// in shared memory; for N = 32 (n = 64, 34 KB per matrix) the first six do and
+// the last four (G, X, Y, Z) live in a per-CTA slice of global scratch
+// (Work::add_scr), which stays L2-resident.
 template <int N>
 struct AddSmem {
   static constexpr int n = RTCfg<N>::n, MAT = RTCfg<N>::MAT;
-  double m[10][MAT];
+  static constexpr int NS = (N == 32) ? 6 : 10;  // matrices in shared memory
+  double m[NS][MAT];
   double sp[n], sm[n], s2p[n], s2m[n], t1[n], t2[n], nsp[n], nsm[n];
   double wv[n], wv2[n];
   double sky[n], gnd[n], uprad[n], dnrad[n];
@@ -382,9 +387,14 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
     const double* hl = w.hgt_lev + (size_t)c * (Lm + 1);
     const double* tl = w.temp_lev + (size_t)c * (Lm + 1);
     int status = w.col_status[c];
-    double *Rp = S.m[0], *Rm = S.m[1], *Tp = S.m[2], *Tm = S.m[3];
-    double *R2 = S.m[4], *T2 = S.m[5];
-    double *G = S.m[6], *X = S.m[7], *Y = S.m[8], *Z = S.m[9];
+    double* mats[10];
+#pragma unroll
+    for (int q = 0; q < 10; q++)
+      mats[q] = (q < AddSmem<N>::NS) ? S.m[q < AddSmem<N>::NS ? q : 0]
+                                     : w.add_scr + ((size_t)blockIdx.x * (10 - AddSmem<N>::NS) + (q - AddSmem<N>::NS)) * MAT;
+    double *Rp = mats[0], *Rm = mats[1], *Tp = mats[2], *Tm = mats[3];
+    double *R2 = mats[4], *T2 = mats[5];
+    double *G = mats[6], *X = mats[7], *Y = mats[8], *Z = mats[9];
     // stack state: 0 empty, 1 clear (R = 0, T = diag t1 on both sides), 2 general
     int sstate = 0;
     for (int k = 0; k < L; k++) {  // top-down layer index

@@ -60,6 +60,8 @@ struct Work {
   double* lay;                         // [pmax*Fm][lay_stride]
   size_t lay_stride;
   int* lay_nd;                         // [pmax*Fm]
+  // adding matrices that do not fit in shared memory (N = 32 only)
+  double* add_scr;                     // [adding CTAs][4][MAT]
   // status
   int* status;                         // [C][Fm]
   int* col_status;                     // [C]

@@ -95,6 +95,17 @@ def settings_from_nml(nmlSet, nummu=16):
     return s
 
 
+def disabled_species():
+    """A species slot that takes no part (dist ``disabled``), used to pad
+    columns with fewer species in a batch with per-column species tables."""
+    r = np.zeros((), dtype=SPECIES_DTYPE)
+    for k in ("as_ratio", "rho_ms", "a_ms", "b_ms", "alpha_as", "beta_as", "p_1", "p_2", "p_3", "p_4", "d_1", "d_2"):
+        r[k] = -99.0
+    r["liq_ice"], r["moment_in"], r["nbin"] = 1, 3, 2
+    r["dist"] = DIST_CODES["disabled"]
+    return r
+
+
 def species_from_df(data):
     """Descriptor recarray -> structured array of ``pamtra_b200_species``."""
     out = np.zeros(len(data), dtype=SPECIES_DTYPE)

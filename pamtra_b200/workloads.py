@@ -13,13 +13,24 @@ standard-atmosphere T/p jitter, RH 40-95 %, cloud liquid (exp, 40 bins over
 
 ``c2_pam`` is the batched workload: ``ncol`` seeded columns of 50 layers with
 the same two species and mixing ratios log-uniform over 0.01-2 g/kg.
+
+``uneven_batch`` is the uneven workload: layer counts uniform over 40-150,
+1-5 species per column drawn from cloud water, cloud ice, snow, graupel and
+rain with exponential or modified-gamma size distributions (mu uniform over
+0-4), 20-80 bins each, ice densities 100-900 kg/m3 (soft spheres, Sihvola
+mixing), 8-32 frequencies per column from 10-183 GHz and NUMMU from
+{8, 16, 32}, all per column.
+
+``target_batch`` is the 150-layer, 16-angle, 4-species shape: 150 layers
+over 0-15 km with cloud water, cloud ice, snow and rain in overlapping bands.
 """
 
 import warnings
 
 import numpy as np
 
-from . import core, importer, meteoSI
+from . import batch as _batch
+from . import core, importer, meteoSI, packing
 
 GOLDEN_FREQS = [10.65, 35.5]
 C1_FREQS = [23.8, 31.4, 89.0]
@@ -91,3 +102,149 @@ def c1_pam(seed=1):
 
 def c2_pam(ncol=4096, seed=2):
     return _pam_from(_columns(ncol, 50, seed), ncol, 50)
+
+
+# ------------------------------------------------------------------ packed (per-column) workloads
+# species kinds: (liq_ice, d_1, d_2, effective radius p_2 of the gamma forms, band bottom/top in m)
+_KINDS = {
+    "cwc": (1, 2.0e-6, 1.0e-4, 1.0e-5, 500.0, 6000.0),
+    "iwc": (-1, 1.0e-5, 2.0e-3, 5.0e-5, 6000.0, 12000.0),
+    "swc": (-1, 1.0e-4, 1.0e-2, 5.0e-4, 3000.0, 10000.0),
+    "gwc": (-1, 1.0e-4, 8.0e-3, 4.0e-4, 2000.0, 8000.0),
+    "rwc": (1, 1.0e-4, 6.0e-3, 3.0e-4, 0.0, 4000.0),
+}
+_KIND_ORDER = ("cwc", "iwc", "swc", "gwc", "rwc")
+
+
+def _species_row(kind, rng, nbin=None, gamma=None, rho=None):
+    li, d1, d2, reff, _, _ = _KINDS[kind]
+    r = np.zeros((), dtype=packing.SPECIES_DTYPE)
+    for k in ("as_ratio", "rho_ms", "a_ms", "b_ms", "alpha_as", "beta_as", "p_1", "p_2", "p_3", "p_4"):
+        r[k] = -99.0
+    r["liq_ice"] = li
+    r["moment_in"] = 3
+    r["nbin"] = int(rng.integers(20, 81)) if nbin is None else nbin
+    use_gamma = (rng.random() < 0.5) if gamma is None else gamma
+    if li == -1:
+        r["rho_ms"] = float(rng.uniform(100.0, 900.0)) if rho is None else rho
+    if use_gamma:
+        r["dist"] = packing.DIST_CODES["mgamma"]
+        r["p_2"] = reff
+        r["p_3"] = float(rng.uniform(0.0, 4.0))
+        r["p_4"] = 1.0
+    else:
+        r["dist"] = packing.DIST_CODES["exp"]
+        if kind == "rwc":
+            r["p_3"] = 8.0e6  # Marshall-Palmer intercept
+        else:
+            r["p_2"] = reff
+    r["d_1"], r["d_2"] = d1, d2
+    return r
+
+
+def _settings(nummu=16):
+    warnings.simplefilter("ignore")
+    nml = dict(core.pyPamtra().nmlSet)
+    nml["hydro_adaptive_grid"] = False
+    nml["emissivity"] = 0.5
+    return packing.settings_from_nml(nml, nummu)
+
+
+def _atmosphere(rng, nl, top):
+    h = np.linspace(0.0, top, nl + 1)
+    _, p0, t0 = meteoSI.usStandard(h)
+    t = t0 + rng.uniform(-1.0, 1.0, nl + 1)
+    p = p0 * (1.0 + rng.uniform(-0.005, 0.005, nl + 1))
+    rh = rng.uniform(40.0, 95.0, nl + 1)
+    return h, t, p, rh
+
+
+def _packed(st, species, stride, nly, freqs_list, nummu, kinds_list, qs, top, rng, Lm, H, per_freq):
+    C = len(nly)
+    F = max(len(f) for f in freqs_list)
+    host = dict()
+    for k in ("hgt_lev", "temp_lev", "press_lev", "relhum_lev"):
+        host[k] = np.full((C, Lm + 1), np.nan)
+    for k in ("hgt", "temp", "press", "relhum"):
+        host[k] = np.full((C, Lm), np.nan)
+    hq = np.zeros((C, Lm, H))
+    for c in range(C):
+        nl = int(nly[c])
+        h, t, p, rh = _atmosphere(rng, nl, top[c])
+        host["hgt_lev"][c, :nl + 1], host["temp_lev"][c, :nl + 1] = h, t
+        host["press_lev"][c, :nl + 1], host["relhum_lev"][c, :nl + 1] = p, rh
+        host["hgt"][c, :nl] = 0.5 * (h[1:] + h[:-1])
+        mid = host["hgt"][c, :nl]
+        for j, kind in enumerate(kinds_list[c]):
+            if kind is None:
+                continue
+            lo, hi = _KINDS[kind][4], _KINDS[kind][5]
+            band = (mid >= lo) & (mid <= hi)
+            hq[c, :nl, j] = np.where(band, qs[c][j] * 10 ** rng.uniform(-0.5, 0.5, nl), 0.0)
+    host["hydro_q"] = hq
+    host["hydro_n"] = np.zeros_like(hq)
+    host["hydro_reff"] = np.zeros_like(hq)
+    host["nlyrs"] = np.ascontiguousarray(np.asarray(nly, dtype=np.int32))
+    host["groundtemp"] = np.full(C, 290.0)
+    host["obs_height"] = np.tile([833000.0, 0.0], (C, 1))
+    host["sfc_refl"] = np.full(C, ord("S"), dtype=np.int8)
+    host["ncol"], host["max_nlyrs"], host["noutlevels"], host["nhydro"] = C, Lm, 2, H
+    host["max_nfreq"] = F
+    if per_freq:
+        fr = np.zeros((C, F))
+        for c, f in enumerate(freqs_list):
+            fr[c, :len(f)] = f
+        host["freqs"] = fr
+        host["nfreq"] = np.asarray([len(f) for f in freqs_list], dtype=np.int32)
+    else:
+        host["freqs"] = np.asarray(freqs_list[0], dtype=np.float64)
+    if nummu is not None:
+        host["nummu"] = np.asarray(nummu, dtype=np.int32)
+    return _batch.pack_columns(st, species, host, stride)
+
+
+def uneven_batch(ncol=16384, seed=3, nummu_choices=(8, 16, 32), nfreq_range=(8, 32)):
+    """Seeded uneven batch (per-column layers, species, frequencies, NUMMU)."""
+    rng = np.random.default_rng(seed)
+    H = 5
+    st = _settings(16)
+    nly = rng.integers(40, 151, ncol)
+    top = nly * 100.0  # 100 m layers
+    nummu = rng.choice(np.asarray(nummu_choices), ncol)
+    sp = np.empty(ncol * H, dtype=packing.SPECIES_DTYPE)
+    kinds_list, qs, freqs_list = [], [], []
+    for c in range(ncol):
+        nk = int(rng.integers(1, 6))
+        chosen = sorted(rng.choice(H, nk, replace=False).tolist())
+        kl = [None] * H
+        qq = [0.0] * H
+        for j in range(H):
+            if j in chosen:
+                kl[j] = _KIND_ORDER[j]
+                sp[c * H + j] = _species_row(_KIND_ORDER[j], rng)
+                qq[j] = 10 ** rng.uniform(-5.0, np.log10(2e-3))
+            else:
+                sp[c * H + j] = packing.disabled_species()
+        kinds_list.append(kl)
+        qs.append(qq)
+        nf = int(rng.integers(nfreq_range[0], nfreq_range[1] + 1))
+        freqs_list.append(np.sort(rng.uniform(10.0, 183.0, nf)))
+    return _packed(st, sp, H, nly, freqs_list, nummu, kinds_list, qs, top, rng, int(nly.max()), H, True)
+
+
+TARGET_FREQS = [23.8, 31.4, 89.0, 150.0]
+
+
+def target_batch(ncol=1024, seed=4):
+    """150-layer, NUMMU = 16 columns with four species (cloud water, cloud
+    ice, snow, rain), shared species table and frequencies."""
+    rng = np.random.default_rng(seed)
+    st = _settings(16)
+    kinds = ["cwc", "iwc", "swc", "rwc"]
+    sp = np.empty(4, dtype=packing.SPECIES_DTYPE)
+    for j, k in enumerate(kinds):
+        sp[j] = _species_row(k, np.random.default_rng(100 + j), nbin=40, gamma=(k != "rwc"), rho=300.0)
+    nly = np.full(ncol, 150)
+    top = np.full(ncol, 15000.0)
+    qs = [[10 ** rng.uniform(-5.0, np.log10(2e-3)) for _ in kinds] for _ in range(ncol)]
+    return _packed(st, sp, 0, nly, [TARGET_FREQS], None, [kinds] * ncol, qs, top, rng, 150, 4, False)

@@ -204,6 +204,61 @@ def test_nummu_8(oracle_mod, native):
     assert np.max(np.abs(res["tb"] - ref["tb"])) < TB_TOL
 
 
+def test_nummu_32(oracle_mod, native):
+    from pamtra_b200.libWrapper import PamtraFortranWrapper
+    pam = _custom_pam(q={(5, 1): 1e-3, (6, 0): 2e-4, (7, 1): 3e-3})
+    ref, _ = oracle_mod.run_pamtra(copy.deepcopy(pam), [31.4, 150.0], nummu=32)
+    pam._prepare_freqs([31.4, 150.0])
+    res, err, _ = PamtraFortranWrapper(pam.set, pam.nmlSet, pam.df.data, {}, {}, pam.p, nummu=32)
+    assert err == 0
+    assert np.max(np.abs(res["tb"] - ref["tb"])) < TB_TOL
+
+
+def _oracle_packed_column(oracle_mod, b, c):
+    """Oracle TB of column c of a packed batch with per-column settings."""
+    h = b.host
+    st = copy.copy(b.settings)
+    if h.get("nummu") is not None:
+        st.nummu = int(h["nummu"][c])
+    H = int(h["nhydro"])
+    sp = b.species[c * H:(c + 1) * H] if b.species_stride else b.species
+    freqs = h["freqs"][c, :int(h["nfreq"][c])] if h.get("nfreq") is not None else h["freqs"]
+    err, tb, _, _, _ = oracle_mod.run_column(oracle_mod.settings(st), sp, h, c, list(freqs))
+    return err, tb, int(st.nummu), len(freqs)
+
+
+def test_uneven_batch_against_oracle(oracle_mod, native):
+    # per-column layer counts, species sets, PSD forms, ice densities,
+    # frequency lists and NUMMU in one launch sequence
+    import torch
+    b = wl.uneven_batch(9, seed=11, nfreq_range=(2, 4))
+    assert b.nummu_mask == 7
+    out = pbatch.run(b, 0)
+    torch.cuda.synchronize()
+    tb = out["tb"].cpu().numpy()
+    status = out["status"].cpu().numpy()
+    for c in range(b.ncol):
+        err, t, N, nf = _oracle_packed_column(oracle_mod, b, c)
+        assert err == 0 and not np.any(status[c, :nf])
+        d = np.max(np.abs(tb[c][:, :2 * N, :nf, :] - t))
+        assert d < TB_TOL, (c, N, d)
+        assert np.all(tb[c][:, 2 * N:, :, :] == -9999.0)
+
+
+def test_chunked_run_equals_single_run(native):
+    # chunks grouped by NUMMU and trimmed to their own sizes give the same
+    # bits as one launch over the whole batch
+    import torch
+    b = wl.uneven_batch(24, seed=12, nfreq_range=(2, 6))
+    one = pbatch.run(b, 0)
+    torch.cuda.synchronize()
+    ch = pbatch.chunk_columns(b, 96 << 20)
+    assert len(ch) > 2
+    got = pbatch.run_chunked(b, 96 << 20)
+    assert np.array_equal(got["tb"], one["tb"].cpu().numpy())
+    assert np.array_equal(got["status"], one["status"].cpu().numpy())
+
+
 def test_ragged_columns(oracle_mod, native):
     # three columns with 30, 24 and 18 layers, padded with -9999 (pyPamtra convention)
     warnings.simplefilter("ignore")

@@ -1,0 +1,51 @@
+"""Serving loop on the GPU: every request's result is the same served alone
+and served in a mix of concurrent requests (merged batches, chunked
+requests, overlapping slots).  Tolerance: 0 K (bit-identical), since a
+(column, frequency) solve never reads another column's data."""
+import numpy as np
+import pytest
+
+from pamtra_b200 import batch as pbatch
+from pamtra_b200 import serve
+
+pytestmark = pytest.mark.gpu
+
+
+def _alone(b):
+    import torch
+    out = pbatch.run(b, 0)
+    torch.cuda.synchronize()
+    return {k: v.cpu().numpy() for k, v in out.items()}
+
+
+def test_results_same_alone_and_in_mix(native):
+    reqs = serve.request_stream(7, seed=50, max_cols=24, nfreq_range=(1, 6))
+    alone = [_alone(b) for b in reqs]
+    # small arenas force chunking of the larger requests and merging of the small ones
+    srv = serve.Server(0, slots=3, arena_bytes=192 << 20, max_cols=48)
+    try:
+        served = [srv.submit(b) for b in reqs]
+        assert srv.drain(timeout=300)
+    finally:
+        srv.close()
+    chunked = sum(1 for r in served if r._parts is not None)
+    assert chunked >= 1
+    for r, a in zip(served, alone):
+        assert r.error is None, r.error
+        assert np.array_equal(r.result["tb"], a["tb"])
+        assert np.array_equal(r.result["status"], a["status"])
+        assert r.latency > 0
+
+
+def test_plain_server_matches(native):
+    reqs = serve.request_stream(2, seed=51, max_cols=4, nfreq_range=(1, 3))
+    alone = [_alone(b) for b in reqs]
+    srv = serve.Server(0, slots=1, arena_bytes=256 << 20, max_cols=1)
+    try:
+        served = [srv.submit(b) for b in reqs]
+        assert srv.drain(timeout=300)
+    finally:
+        srv.close()
+    assert srv.batches_launched == sum(b.ncol for b in reqs)
+    for r, a in zip(served, alone):
+        assert np.array_equal(r.result["tb"], a["tb"])
