@@ -183,6 +183,13 @@ int32_t pamtra_b200_eps_water_tkc(const double* t_c, const double* freq, double*
 int32_t pamtra_b200_minvert_batched(const double* a, double* ainv, int32_t* status, int32_t n, int32_t count,
                                     void* stream);
 
+/* C = A * B for `count` column-major n x n matrices (replaces MMULT,
+ * src/radmat.f90:137, for batches) computed as 3xTF32 split-precision
+ * tcgen05 tensor-core products with FP32 accumulation; n = 32.  *err is
+ * OR-ed with 1 if a wait on the tensor core timed out. */
+int32_t pamtra_b200_mmult_3xtf32_batched(const double* a, const double* b, double* c, int32_t n, int32_t count,
+                                         int32_t* err, void* stream);
+
 /* ---- allocation-free single column ----
  * No counterpart in the reference (its Fortran owns module-global arrays).
  * For callers that cannot call cudaMalloc: hosts whose own device memory

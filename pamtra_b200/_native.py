@@ -50,7 +50,8 @@ class Outputs(ctypes.Structure):
 EXPORTS = ["pamtra_b200_create", "pamtra_b200_destroy", "pamtra_b200_workspace_bytes", "pamtra_b200_reserve",
            "pamtra_b200_run", "pamtra_b200_run_host", "pamtra_b200_last_launch_count", "pamtra_b200_gas_r98",
            "pamtra_b200_eps_water_tkc", "pamtra_b200_minvert_batched", "pamtra_b200_set_timing",
-           "pamtra_b200_stage_ms", "pamtra_b200_abi_sizes", "pamtra_b200_run_noalloc"]
+           "pamtra_b200_stage_ms", "pamtra_b200_abi_sizes", "pamtra_b200_run_noalloc",
+           "pamtra_b200_mmult_3xtf32_batched"]
 STAGES = ["prep", "psd", "mie", "layer", "adding"]
 
 _lib = None
@@ -89,6 +90,8 @@ def load():
         l.pamtra_b200_run_noalloc.restype = _i32
         l.pamtra_b200_run_noalloc.argtypes = [ctypes.POINTER(Settings), ctypes.POINTER(Columns),
                                               ctypes.POINTER(Outputs), _vp]
+        l.pamtra_b200_mmult_3xtf32_batched.restype = _i32
+        l.pamtra_b200_mmult_3xtf32_batched.argtypes = [_vp, _vp, _vp, _i32, _i32, _vp, _vp]
         l.pamtra_b200_abi_sizes.restype = _i32
         l.pamtra_b200_abi_sizes.argtypes = [ctypes.POINTER(ctypes.c_size_t), _i32]
         _lib = l

@@ -22,6 +22,7 @@
 #include "mie.cuh"
 #include "prep.cuh"
 #include "rt.cuh"
+#include "tc.cuh"
 #include "work.cuh"
 
 using namespace pb;
@@ -281,6 +282,69 @@ __global__ void k_minvert(const double* a, double* ainv, int32_t* status, int co
     if (status && t == 0) status[m] = s ? (PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT) : 0;
     __syncthreads();
   }
+}
+
+// C = A * B for `count` column-major 32 x 32 matrices as 3xTF32 tcgen05
+// products (FP32 accumulation in tensor memory).  One CTA of 128 threads per
+// matrix pair; rows 32..127 of the A tile stay zero.
+__global__ void __launch_bounds__(128) k_mmult_3xtf32(const double* a, const double* b, double* c, int count,
+                                                      int* err) {
+  extern __shared__ __align__(128) float tsm[];
+  float* a_hi = tsm;
+  float* a_lo = tsm + 128 * 32;
+  float* b_hi = tsm + 2 * 128 * 32;
+  float* b_lo = b_hi + 32 * 32;
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tslot;
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  if (warp == 0) tc::tmem_alloc(&tslot, 32);
+  if (t == 0) tc::mbar_init(&mbar, 1);
+  for (int i = t; i < 2 * 128 * 32; i += 128) tsm[i] = 0.f;
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = tslot;
+  uint32_t parity = 0;
+  bool ok = true;
+  for (int m = blockIdx.x; m < count && ok; m += gridDim.x) {
+    const double* am = a + (size_t)m * 1024;
+    const double* bm = b + (size_t)m * 1024;
+    if (t < 32) {
+      float v[32];
+#pragma unroll
+      for (int k = 0; k < 32; k++) v[k] = (float)am[k * 32 + t];  // row t of A
+      tc::put_row(a_hi, a_lo, t, v);
+    } else if (t < 64) {
+      float v[32];
+#pragma unroll
+      for (int k = 0; k < 32; k++) v[k] = (float)bm[(t - 32) * 32 + k];  // column t-32 of B
+      tc::put_row(b_hi, b_lo, t - 32, v);
+    }
+    tc::fence_async_smem();
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+    if (t == 0) tc::mma3(tbase, a_hi, a_lo, b_hi, b_lo, &mbar);
+    ok = tc::mbar_wait(&mbar, parity);
+    parity ^= 1;
+    tc::fence_after_sync();
+    if (ok && warp == 0) {
+      float d[32];
+      tc::tmem_ld32(tbase, d);
+      double* cm = c + (size_t)m * 1024;
+#pragma unroll
+      for (int n = 0; n < 32; n++) cm[n * 32 + lane] = d[n];
+    }
+    tc::fence_before_sync();
+    __syncthreads();
+    tc::fence_after_sync();
+  }
+  if (!ok) {
+    if (t == 0) atomicOr(err, 1);
+    tc::mbar_wait(&mbar, parity ^ 1);  // let a late MMA finish before the memory is released
+  }
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tbase, 32);
 }
 
 }  // namespace
@@ -735,6 +799,15 @@ int32_t pamtra_b200_minvert_batched(const double* a, double* ainv, int32_t* stat
   else if (n == 64)
     k_minvert<64><<<g, Team<64>::T, Team<64>::MAT * 8 + sizeof(InvScratch<64>), s>>>(a, ainv, status, count);
   else return PAMTRA_B200_FATAL;
+  return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
+}
+
+int32_t pamtra_b200_mmult_3xtf32_batched(const double* a, const double* b, double* c, int32_t n, int32_t count,
+                                         int32_t* err, void* stream) {
+  if (count <= 0) return PAMTRA_B200_OK;
+  if (n != 32 || !a || !b || !c || !err) return PAMTRA_B200_FATAL;
+  const int g = std::min(count, 65535);
+  k_mmult_3xtf32<<<g, 128, (2 * 128 * 32 + 2 * 32 * 32) * sizeof(float), (cudaStream_t)stream>>>(a, b, c, count, err);
   return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
 }
 

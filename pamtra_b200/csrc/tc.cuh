@@ -1,0 +1,186 @@
+// Blackwell tensor-core primitives (tcgen05 + TMEM) for split-precision
+// (3xTF32) products of small matrices.
+//
+// Operand tiles live in shared memory in the K-major, non-swizzled
+// ("interleaved") canonical layout of the tcgen05 matrix descriptors: core
+// matrices of 8 rows x 16 bytes (4 TF32 values), the K-chunks of a row group
+// stored one after another.  For a tile with K = 32 (8 chunks) element
+// (row r, k) is at float offset
+//     (r / 8) * 256 + (k / 4) * 32 + (r % 8) * 4 + (k % 4)
+// so a row group spans 1024 bytes (SBO) and neighbouring K-chunks are 128
+// bytes apart (LBO).  One MMA consumes K = 8 (two chunks): the descriptor of
+// k-step s starts 256 * s bytes into the tile.
+//
+// A product X * Y with FP32 operands is formed as
+//     X_hi Y_hi + X_hi Y_lo + X_lo Y_hi,   X_hi = rna_tf32(X), X_lo = rna_tf32(X - X_hi)
+// with FP32 accumulation in tensor memory (the dropped X_lo Y_lo term is
+// below 2^-22 relative).
+#pragma once
+#include <cstdint>
+
+namespace pb {
+namespace tc {
+
+constexpr int TILE_K = 32;               // K extent of every operand tile
+constexpr int RG_FLOATS = 256;           // floats per 8-row group (8 chunks x 32)
+constexpr uint32_t SBO_BYTES = 1024;     // row group to row group
+constexpr uint32_t LBO_BYTES = 128;      // K-chunk to K-chunk
+// instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 32
+constexpr uint32_t IDESC_M128_N32 = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 24;  // bounded waits on MMA completion
+
+__device__ __forceinline__ int tile_off(int r, int k) {
+  return (r >> 3) * RG_FLOATS + (k >> 2) * 32 + (r & 7) * 4 + (k & 3);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// shared-memory matrix descriptor (K-major, no swizzle, sm_100 version 1)
+__device__ __forceinline__ uint64_t desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFFu);
+  d |= (uint64_t)((LBO_BYTES >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((SBO_BYTES >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)1u << 46;
+  return d;
+}
+
+__device__ __forceinline__ float rna_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void split(float x, float& hi, float& lo) {
+  hi = rna_tf32(x);
+  lo = rna_tf32(x - hi);
+}
+
+// D[tmem] (+)= A * B^T over K = 8 from the given descriptors (one thread)
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t"
+      ".reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+      "}\n"
+      :
+      : "r"(d_tmem), "l"(a), "l"(b), "r"(IDESC_M128_N32), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+// 3xTF32 product of a 128 x 32 A tile pair and a 32 x 32 B tile pair into
+// D (128 lanes x 32 columns, FP32).  Issued by one thread; completion is
+// signalled on `mbar` through tcgen05.commit.
+__device__ __forceinline__ void mma3(uint32_t d_tmem, const float* a_hi, const float* a_lo, const float* b_hi,
+                                     const float* b_lo, uint64_t* mbar) {
+  const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo), bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+  uint32_t acc = 0;
+#pragma unroll
+  for (int s = 0; s < TILE_K / 8; s++) {
+    mma(d_tmem, desc(al + 256 * s), desc(bh + 256 * s), acc);
+    acc = 1;
+  }
+#pragma unroll
+  for (int s = 0; s < TILE_K / 8; s++) mma(d_tmem, desc(ah + 256 * s), desc(bl + 256 * s), 1);
+#pragma unroll
+  for (int s = 0; s < TILE_K / 8; s++) mma(d_tmem, desc(ah + 256 * s), desc(bh + 256 * s), 1);
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :
+               : "r"(smem_u32(mbar))
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(smem_u32(mbar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Wait for phase `parity` of `mbar` to complete; false after the spin limit.
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
+  const uint32_t a = smem_u32(mbar);
+  for (uint32_t i = 0; i < MBAR_SPIN_LIMIT; i++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t"
+        "}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// generic-proxy shared-memory writes -> visible to the tensor core
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Allocate / free tensor-memory columns (whole warp).  The base address is
+// written to *slot (shared memory).
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+               :
+               : "r"(smem_u32(slot)), "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" : : "r"(taddr), "r"(ncols) : "memory");
+}
+
+// 32 consecutive FP32 columns of this thread's lane (warp w reads lanes
+// 32w..32w+31; taddr carries the lane base in bits 16..31).
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// Write one 32-value row of a tile pair (hi, lo) from FP32 values.
+__device__ __forceinline__ void put_row(float* hi, float* lo, int r, const float (&v)[32]) {
+#pragma unroll
+  for (int c = 0; c < 8; c++) {
+    float4 h, l;
+    split(v[4 * c + 0], h.x, l.x);
+    split(v[4 * c + 1], h.y, l.y);
+    split(v[4 * c + 2], h.z, l.z);
+    split(v[4 * c + 3], h.w, l.w);
+    const int o = (r >> 3) * RG_FLOATS + c * 32 + (r & 7) * 4;
+    *reinterpret_cast<float4*>(hi + o) = h;
+    *reinterpret_cast<float4*>(lo + o) = l;
+  }
+}
+
+// Write one 32-value column (k fixed, rows 0..31) of a tile pair: the
+// transposed store of a thread's lane.  Rows are visited in a rotated order
+// so that a warp's stores hit 32 distinct banks.
+__device__ __forceinline__ void put_col(float* hi, float* lo, int k, const float (&v)[32]) {
+#pragma unroll
+  for (int j = 0; j < 32; j++) {
+    const int r = ((k >> 2) + j) & 31;
+    float h, l;
+    split(v[r], h, l);
+    const int o = tile_off(r, k);
+    hi[o] = h;
+    lo[o] = l;
+  }
+}
+
+}  // namespace tc
+}  // namespace pb

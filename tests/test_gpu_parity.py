@@ -345,3 +345,28 @@ def test_c2_full_size_properties(oracle_mod, native):
     out2 = pbatch.run(b, 0)
     torch.cuda.synchronize()
     assert np.array_equal(out2["tb"].cpu().numpy(), tb)
+
+
+# ----------------------------------------------------------------- tensor-core products
+def test_mmult_3xtf32_kernel(native):
+    # 3xTF32 tcgen05 products: FP32-level accuracy (a single TF32 product
+    # would be off by ~1e-3 relative)
+    import torch
+    rng = np.random.default_rng(17)
+    cnt = 300
+    a = rng.normal(size=(cnt, 32, 32))
+    b = rng.normal(size=(cnt, 32, 32))
+    dev = torch.device("cuda", 0)
+    at = torch.from_numpy(np.ascontiguousarray(a.transpose(0, 2, 1))).to(dev)
+    bt = torch.from_numpy(np.ascontiguousarray(b.transpose(0, 2, 1))).to(dev)
+    ct = torch.zeros_like(at)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    rc = native.load().pamtra_b200_mmult_3xtf32_batched(at.data_ptr(), bt.data_ptr(), ct.data_ptr(), 32, cnt,
+                                                        err.data_ptr(), None)
+    assert rc == 0
+    torch.cuda.synchronize()
+    assert int(err.item()) == 0
+    c = ct.cpu().numpy().transpose(0, 2, 1)
+    ref = a @ b
+    rel = np.max(np.abs(c - ref)) / np.max(np.abs(ref))
+    assert rel < 2e-6, rel
