@@ -195,6 +195,32 @@ def layer_flops(nd, N):
     return float(np.sum(d) * 7 * 2 * n ** 3)
 
 
+def _timed_steps(b, local, eng, stream, out, prec, steps, warmup, flush):
+    """Device-timed batched steps (CUDA events on the launching stream, L2
+    flushed before each); returns per-step ms and mean stage ms."""
+    import torch
+    from pamtra_b200 import batch as pbatch
+    with torch.cuda.stream(stream):
+        for _ in range(warmup):
+            pbatch.run(b, local, out, precision=prec, stream=stream, eng=eng)
+    stream.synchronize()
+    eng.set_timing(True)
+    ms, stages = [], {}
+    for _ in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            pbatch.run(b, local, out, precision=prec, stream=stream, eng=eng)
+            e.record(stream)
+        e.synchronize()
+        ms.append(s.elapsed_time(e))
+        for k, v in eng.stage_ms().items():
+            stages[k] = stages.get(k, 0.0) + v / steps
+    eng.set_timing(False)
+    return ms, stages
+
+
 def _target_shape(args, local, eng, stream):
     """The 150-layer, 16-angle, 4-species shape: batched FP64 over
     ``--target-cols`` columns (device-timed, L2 flushed) against the plain
@@ -222,6 +248,11 @@ def _target_shape(args, local, eng, stream):
         ms.append(s.elapsed_time(e))
     batched = b.n_solves() / (np.mean(ms) * 1e-3)
     st_bad = int((out["status"] != 0).sum())
+    from pamtra_b200._native import PREC_3XTF32
+    sout = b.alloc_outputs(dev)
+    sms_, sstages = _timed_steps(b, local, eng, stream, sout, PREC_3XTF32, 3, 2, flush)
+    split = b.n_solves() / (np.mean(sms_) * 1e-3)
+    split_err = float((sout["tb"] - out["tb"]).abs().max().item())
     singles = [pbatch.subset(b, [c]) for c in range(16)]
     souts = [sb.alloc_outputs(dev) for sb in singles]
     with torch.cuda.stream(stream):
@@ -242,6 +273,8 @@ def _target_shape(args, local, eng, stream):
     return {"workload": "%d columns x 150 layers (0-15 km), NUMMU=16, 4 Mie species (cloud water, cloud ice, "
                         "snow, rain; 40 bins each), f = 23.8/31.4/89/150 GHz" % args.target_cols,
             "batched_fp64": batched, "plain_fp64": plain, "batched_over_plain": batched / plain,
+            "batched_3xtf32": split, "batched_3xtf32_over_plain": split / plain,
+            "tb_err_3xtf32_vs_fp64_K": split_err, "stage_ms_3xtf32": sstages,
             "unit": "solves/s", "batched_ms_per_step": float(np.mean(ms)), "status_nonzero": st_bad,
             "plain_sample_columns": 16, "plain_equals_batched_bitwise": bool(same)}
 
@@ -396,6 +429,13 @@ def main():
         e2e_total = float(tt.item())
     h2d = sum(v.nbytes for v in b.host.values() if isinstance(v, np.ndarray))
     d2h = sum(v.nbytes for v in hout.values())
+    # ---- split-precision batched form (3xTF32 tcgen05 doubling) on the same columns
+    from pamtra_b200._native import PREC_3XTF32
+    sout = b.alloc_outputs(dev)
+    sms_, sstages = _timed_steps(b, local, eng, stream, sout, PREC_3XTF32, args.steps, args.warmup, flush)
+    split_value = world * solves_step / (np.mean(sms_) * 1e-3)
+    tb_split = sout["tb"].cpu().numpy()
+    split_err_f64 = float(np.max(np.abs(tb_split - out["tb"].cpu().numpy())))
     # ---- plain form: one column per call
     nplain = 32
     plain_batches = [pbatch.pack_pam(c2_pam(1, seed=1000 + i), FREQS) for i in range(nplain)]
@@ -437,6 +477,7 @@ def main():
     # ---- CPU baseline + TB error vs the oracle on the same columns
     cpu = None
     tb_err = None
+    split_err_oracle = None
     if not args.no_cpu:
         cores = os.cpu_count() or 1
         nsamp = args.cpu_sample or min(b.ncol, 8 * cores)
@@ -446,6 +487,7 @@ def main():
         pool.close()
         tb_gpu = out["tb"].cpu().numpy()
         tb_err = max(float(np.max(np.abs(tb_gpu[c] - tbs[c]))) for c in idxs)
+        split_err_oracle = max(float(np.max(np.abs(tb_split[c] - tbs[c]))) for c in idxs)
         cpu = {"value": cval, "unit": "solves/s", "cores": cores, "kind": "port",
                "sample": "%d random columns x %d frequencies of the same workload, one worker process per core; "
                          "C++ FP64 restatement of the reference Fortran (no Fortran compiler on this image)"
@@ -464,6 +506,12 @@ def main():
         "plain_fp64": {"value": plain_value, "unit": "solves/s", "form": "one column per call, FP64"},
         "batched_over_plain": value / world / plain_value,
         "tb_err_vs_oracle_K": tb_err,
+        "split_3xtf32": {"value": split_value, "unit": "solves/s", "ms_per_step": float(np.mean(sms_)),
+                         "over_plain": split_value / world / plain_value,
+                         "tb_err_vs_fp64_batched_K": split_err_f64,
+                         "tb_err_vs_oracle_K": split_err_oracle, "stage_ms": sstages,
+                         "form": "doubling products as 3xTF32 tcgen05 MMAs (FP32 accumulation in TMEM); "
+                                 "thin-layer init, adding and surface in FP64"},
         "stage_ms": {k: v / args.steps for k, v in stage_tot.items()},
         "target_shape": target,
         "serving": serving,

@@ -49,6 +49,7 @@ extern "C" {
 #define PAMTRA_B200_ST_PIVOT 0x1000    /* singular matrix in an inverse */
 #define PAMTRA_B200_ST_NAN 0x2000      /* NaN in extinction / coefficients */
 #define PAMTRA_B200_ST_SIZE 0x4000     /* a size limit of this library was exceeded */
+#define PAMTRA_B200_ST_TIMEOUT 0x8000  /* a bounded wait on the tensor core gave up */
 
 /* dist_name codes (src/make_dist_param.f90) */
 #define PAMTRA_B200_DIST_EXP 0
@@ -61,7 +62,8 @@ extern "C" {
 
 /* precision of the doubling / adding matrix products */
 #define PAMTRA_B200_PREC_FP64 0      /* plain and batched FP64 */
-#define PAMTRA_B200_PREC_3XTF32 1    /* 3xTF32 tensor-core products, FP64 inverses */
+#define PAMTRA_B200_PREC_3XTF32 1    /* batched form: layer doubling products as 3xTF32 tcgen05 MMAs
+                                       (NUMMU = 16; NUMMU 8 / 32 and the adding stay FP64) */
 
 /* Settings: the nmlSet keys on the passive Mie path
  * (src/settings.f90:454-573; python/pyPamtra/core.py:89-157). */

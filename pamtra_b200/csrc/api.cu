@@ -23,6 +23,7 @@
 #include "prep.cuh"
 #include "rt.cuh"
 #include "tc.cuh"
+#include "layer_tc.cuh"
 #include "work.cuh"
 
 using namespace pb;
@@ -286,7 +287,10 @@ __global__ void k_minvert(const double* a, double* ainv, int32_t* status, int co
 
 // C = A * B for `count` column-major 32 x 32 matrices as 3xTF32 tcgen05
 // products (FP32 accumulation in tensor memory).  One CTA of 128 threads per
-// matrix pair; rows 32..127 of the A tile stay zero.
+// matrix pair: thread m writes row m of A into the A tile, warp 1 transposes
+// the rows of B it loaded so that tile row n is column n of B, and TMEM lane
+// m holds row m of C.
+// Rows 32..127 of the A tile stay zero.
 __global__ void __launch_bounds__(128) k_mmult_3xtf32(const double* a, const double* b, double* c, int count,
                                                       int* err) {
   extern __shared__ __align__(128) float tsm[];
@@ -317,8 +321,8 @@ __global__ void __launch_bounds__(128) k_mmult_3xtf32(const double* a, const dou
     } else if (t < 64) {
       float v[32];
 #pragma unroll
-      for (int k = 0; k < 32; k++) v[k] = (float)bm[(t - 32) * 32 + k];  // column t-32 of B
-      tc::put_row(b_hi, b_lo, t - 32, v);
+      for (int k = 0; k < 32; k++) v[k] = (float)bm[k * 32 + (t - 32)];  // row t-32 of B, transposed below
+      tc::put_rows_from_cols(b_hi, b_lo, v);  // tile row n = column n of B
     }
     tc::fence_async_smem();
     tc::fence_before_sync();
@@ -401,6 +405,7 @@ static int set_smem_attrs() {
     set((const void*)k_layer<8>, sizeof(LayerSmem<8>));
     set((const void*)k_layer<16>, sizeof(LayerSmem<16>));
     set((const void*)k_layer<32>, sizeof(LayerSmem<32>));
+    set((const void*)k_layer_tc<16>, layer_tc_smem<16>());
     set((const void*)k_adding<8>, sizeof(AddSmem<8>));
     set((const void*)k_adding<16>, sizeof(AddSmem<16>));
     set((const void*)k_adding<32>, sizeof(AddSmem<32>));
@@ -530,7 +535,7 @@ int32_t pamtra_b200_stage_ms(pamtra_b200_ctx* ctx, float* ms, int32_t n) {
 int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, const pamtra_b200_columns* cols,
                         const pamtra_b200_outputs* out, int32_t precision, void* stream_) {
   if (!ctx || !st || !cols || !out || !out->tb) return PAMTRA_B200_FATAL;
-  if (precision != PAMTRA_B200_PREC_FP64) return PAMTRA_B200_FATAL;
+  if (precision != PAMTRA_B200_PREC_FP64 && precision != PAMTRA_B200_PREC_3XTF32) return PAMTRA_B200_FATAL;
   if (cols->ncol < 1 || cols->max_nlyrs < 2 || cols->max_nfreq < 1 || cols->noutlevels < 1 || cols->nhydro < 0)
     return PAMTRA_B200_FATAL;
   if (cols->nhydro > 0 && !cols->species) return PAMTRA_B200_FATAL;
@@ -645,10 +650,18 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     mark(ctx, stream, STG_ADDING);
   }
   if (mask & 2) {
-    int g = occupancy_blocks((const void*)k_layer<16>, RTCfg<16>::T, sizeof(LayerSmem<16>), sms);
-    if (H > 0) { k_layer<16><<<g, RTCfg<16>::T, sizeof(LayerSmem<16>), stream>>>(b, w, *st, ssp); launches++; }
+    if (H > 0 && precision == PAMTRA_B200_PREC_3XTF32) {
+      // three CTAs per SM by shared memory and registers (the occupancy query
+      // under-reports this kernel); the persistent CTAs take work from a counter
+      const size_t smb = layer_tc_smem<16>();
+      const int g = 3 * sms;
+      k_layer_tc<16><<<g, 128, smb, stream>>>(b, w, *st, ssp); launches++;
+    } else if (H > 0) {
+      int g = occupancy_blocks((const void*)k_layer<16>, RTCfg<16>::T, sizeof(LayerSmem<16>), sms);
+      k_layer<16><<<g, RTCfg<16>::T, sizeof(LayerSmem<16>), stream>>>(b, w, *st, ssp); launches++;
+    }
     mark(ctx, stream, STG_LAYER);
-    g = occupancy_blocks((const void*)k_adding<16>, RTCfg<16>::T, sizeof(AddSmem<16>), sms);
+    const int g = occupancy_blocks((const void*)k_adding<16>, RTCfg<16>::T, sizeof(AddSmem<16>), sms);
     k_adding<16><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out); launches++;
     mark(ctx, stream, STG_ADDING);
   }

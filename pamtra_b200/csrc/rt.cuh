@@ -59,27 +59,27 @@ struct LayerSmem {
   int item, stat;
 };
 
+// Per-item state of the layer stage after the thin-layer initialisation.
+struct LayerItem {
+  int c, z, fi, nd, status;
+  double linfac;
+};
+
+// scatcnv, CHECK_NORM4, number of doublings, INITIALIZE4 and
+// INITIAL_SOURCE4 of one (present layer, frequency) item: leaves the
+// thin-layer R (S.m[0]) and T (S.m[1]) and the sources S.lin / S.cst in
+// shared memory.  Returns false when the item is not for this N.
 template <int N>
-__global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch b, Work w, pamtra_b200_settings st,
-                                                       double* __restrict__ ssp_scat) {
+__device__ __forceinline__ bool layer_setup(const Batch& b, const Work& w, const pamtra_b200_settings& st,
+                                            double* __restrict__ ssp_scat, LayerSmem<N>& S, int item,
+                                            LayerItem& it) {
   constexpr int n = RTCfg<N>::n, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT, T = RTCfg<N>::T;
-  extern __shared__ double smem_raw[];
-  LayerSmem<N>& S = *reinterpret_cast<LayerSmem<N>*>(smem_raw);
   const int t = threadIdx.x;
   const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
-  const int P = min(w.counters[0], w.pmax);
-  const int nitems = P * Fm;
-  if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
-  for (;;) {
-    team_sync();
-    if (t == 0) S.item = atomicAdd(&w.counters[2 + (N == 8 ? 0 : (N == 16 ? 1 : 2))], 1);
-    team_sync();
-    const int item = S.item;
-    if (item >= nitems) break;
     const int p = item / Fm, fi = item % Fm;
     const int cz = w.plist[p];
     const int c = cz / Lm, z = cz % Lm;
-    if (fi >= b.col_nfreq(c) || b.col_nummu(c) != N) continue;
+    if (fi >= b.col_nfreq(c) || b.col_nummu(c) != N) return false;
     const double freq = b.freq(c, fi);
     const double wl = C_LIGHT / (freq * 1.e3);
     const double* hl = w.hgt_lev + (size_t)c * (Lm + 1);
@@ -93,6 +93,7 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
     double* Tb = S.m[1];
     double* Gb = S.m[2];
     double* Wb = S.m[3];
+    (void)Wb;
     double* Yb = S.m[4];
     double ext = 0.0, emis = 0.0;
     int status = 0;
@@ -237,6 +238,55 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
     double linfac = (planck0 == 0.0) ? 0.0 : (planck1 / planck0 - 1.0) / num_sub;
     team_sync();
     status |= S.stat;
+  it.c = c;
+  it.z = z;
+  it.fi = fi;
+  it.nd = nd;
+  it.status = status;
+  it.linfac = linfac;
+  return true;
+}
+
+// Write the layer R, T and S+/S- of an item (FP64, the layout k_adding reads).
+template <int N>
+__device__ __forceinline__ void layer_store(const Work& w, int item, const double* Rb, const double* Tb,
+                                            const double* lin) {
+  constexpr int n = RTCfg<N>::n, MAT = RTCfg<N>::MAT, T = RTCfg<N>::T;
+  const int t = threadIdx.x;
+  double* out = w.lay + (size_t)item * w.lay_stride;
+  for (int e = t; e < MAT; e += T) { out[e] = Rb[e]; out[MAT + e] = Tb[e]; }
+  for (int e = t; e < 2 * n; e += T) out[2 * MAT + e] = lin[e];
+}
+
+template <int N>
+__global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch b, Work w, pamtra_b200_settings st,
+                                                       double* __restrict__ ssp_scat) {
+  constexpr int n = RTCfg<N>::n, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT, T = RTCfg<N>::T;
+  (void)LD;
+  (void)MAT;
+  extern __shared__ double smem_raw[];
+  LayerSmem<N>& S = *reinterpret_cast<LayerSmem<N>*>(smem_raw);
+  const int t = threadIdx.x;
+  const int Fm = b.max_nfreq;
+  const int P = min(w.counters[0], w.pmax);
+  const int nitems = P * Fm;
+  if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
+  for (;;) {
+    team_sync();
+    if (t == 0) S.item = atomicAdd(&w.counters[2 + (N == 8 ? 0 : (N == 16 ? 1 : 2))], 1);
+    team_sync();
+    const int item = S.item;
+    if (item >= nitems) break;
+    LayerItem it;
+    if (!layer_setup<N>(b, w, st, ssp_scat, S, item, it)) continue;
+    const int nd = it.nd, c = it.c, fi = it.fi;
+    int status = it.status;
+    double linfac = it.linfac;
+    double* Rb = S.m[0];
+    double* Tb = S.m[1];
+    double* Gb = S.m[2];
+    double* Wb = S.m[3];
+    double* Yb = S.m[4];
     // ---------------- DOUBLING_INTEGRATION4, SYMMETRIC (src/radintg4.f90:174-309)
     for (int itd = 0; itd < nd; itd++) {
       mm<n, MM_SET>(Rb, Rb, Gb);  // R+ R-
@@ -312,10 +362,7 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
       linfac = 2.0 * linfac;
       team_sync();
     }
-    // ---------------- write layer R, T, S+, S-
-    double* out = w.lay + (size_t)item * w.lay_stride;
-    for (int e = t; e < MAT; e += T) { out[e] = Rb[e]; out[MAT + e] = Tb[e]; }
-    for (int e = t; e < 2 * n; e += T) out[2 * MAT + e] = S.lin[e];
+    layer_store<N>(w, item, Rb, Tb, S.lin);
     if (t == 0) {
       w.lay_nd[item] = nd;
       if (status) atomicOr(&w.status[(size_t)c * Fm + fi], status);

@@ -9,8 +9,12 @@
 //     (r / 8) * 256 + (k / 4) * 32 + (r % 8) * 4 + (k % 4)
 // so a row group spans 1024 bytes (SBO) and neighbouring K-chunks are 128
 // bytes apart (LBO).  One MMA consumes K = 8 (two chunks): the descriptor of
-// k-step s starts 256 * s bytes into the tile.
-//
+// k-step s starts 256 * s bytes into the tile.  Both operands use it: the MMA
+// forms D = A * B^T with A (M x K) and B (N x K) stored row by row.  A thread
+// writing one row stores 8 float4 and a quarter warp covers 128 contiguous
+// bytes, so row writes are free of bank conflicts; a warp whose lanes hold
+// columns transposes them in registers first (warp_transpose32).
+
 // A product X * Y with FP32 operands is formed as
 //     X_hi Y_hi + X_hi Y_lo + X_lo Y_hi,   X_hi = rna_tf32(X), X_lo = rna_tf32(X - X_hi)
 // with FP32 accumulation in tensor memory (the dropped X_lo Y_lo term is
@@ -22,30 +26,25 @@ namespace pb {
 namespace tc {
 
 constexpr int TILE_K = 32;               // K extent of every operand tile
-constexpr int RG_FLOATS = 256;           // floats per 8-row group (8 chunks x 32)
-constexpr uint32_t SBO_BYTES = 1024;     // row group to row group
-constexpr uint32_t LBO_BYTES = 128;      // K-chunk to K-chunk
+constexpr int RG_FLOATS = 256;           // floats per 8-row group of an A tile (8 chunks x 32)
 // instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 32
 constexpr uint32_t IDESC_M128_N32 = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
 constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 24;  // bounded waits on MMA completion
-
-__device__ __forceinline__ int tile_off(int r, int k) {
-  return (r >> 3) * RG_FLOATS + (k >> 2) * 32 + (r & 7) * 4 + (k & 3);
-}
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// shared-memory matrix descriptor (K-major, no swizzle, sm_100 version 1)
-__device__ __forceinline__ uint64_t desc(uint32_t addr) {
+// shared-memory matrix descriptor (no swizzle, sm_100 version 1)
+__device__ __forceinline__ uint64_t desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
   uint64_t d = 0;
   d |= (uint64_t)((addr >> 4) & 0x3FFFu);
-  d |= (uint64_t)((LBO_BYTES >> 4) & 0x3FFFu) << 16;
-  d |= (uint64_t)((SBO_BYTES >> 4) & 0x3FFFu) << 32;
+  d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
   d |= (uint64_t)1u << 46;
   return d;
 }
+__device__ __forceinline__ uint64_t desc_k(uint32_t addr) { return desc(addr, 128, 1024); }
 
 __device__ __forceinline__ float rna_tf32(float x) {
   uint32_t r;
@@ -71,7 +70,7 @@ __device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uin
 }
 
 // 3xTF32 product of a 128 x 32 A tile pair and a 32 x 32 B tile pair into
-// D (128 lanes x 32 columns, FP32).  Issued by one thread; completion is
+// D = A * B^T (128 lanes x 32 columns, FP32).  Issued by one thread; completion is
 // signalled on `mbar` through tcgen05.commit.
 __device__ __forceinline__ void mma3(uint32_t d_tmem, const float* a_hi, const float* a_lo, const float* b_hi,
                                      const float* b_lo, uint64_t* mbar) {
@@ -79,13 +78,13 @@ __device__ __forceinline__ void mma3(uint32_t d_tmem, const float* a_hi, const f
   uint32_t acc = 0;
 #pragma unroll
   for (int s = 0; s < TILE_K / 8; s++) {
-    mma(d_tmem, desc(al + 256 * s), desc(bh + 256 * s), acc);
+    mma(d_tmem, desc_k(al + 256 * s), desc_k(bh + 256 * s), acc);
     acc = 1;
   }
 #pragma unroll
-  for (int s = 0; s < TILE_K / 8; s++) mma(d_tmem, desc(ah + 256 * s), desc(bl + 256 * s), 1);
+  for (int s = 0; s < TILE_K / 8; s++) mma(d_tmem, desc_k(ah + 256 * s), desc_k(bl + 256 * s), 1);
 #pragma unroll
-  for (int s = 0; s < TILE_K / 8; s++) mma(d_tmem, desc(ah + 256 * s), desc(bh + 256 * s), 1);
+  for (int s = 0; s < TILE_K / 8; s++) mma(d_tmem, desc_k(ah + 256 * s), desc_k(bh + 256 * s), 1);
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                :
                : "r"(smem_u32(mbar))
@@ -167,19 +166,32 @@ __device__ __forceinline__ void put_row(float* hi, float* lo, int r, const float
   }
 }
 
-// Write one 32-value column (k fixed, rows 0..31) of a tile pair: the
-// transposed store of a thread's lane.  Rows are visited in a rotated order
-// so that a warp's stores hit 32 distinct banks.
-__device__ __forceinline__ void put_col(float* hi, float* lo, int k, const float (&v)[32]) {
+// In-register transpose across a warp: lane L holding v[i] = M[i][L] ends
+// holding v[i] = M[L][i].  Five butterfly stages exchange the bit b of the
+// lane index with the bit b of the register index (16 shuffles each).
+__device__ __forceinline__ void warp_transpose32(float (&v)[32]) {
+  const int lane = threadIdx.x & 31;
 #pragma unroll
-  for (int j = 0; j < 32; j++) {
-    const int r = ((k >> 2) + j) & 31;
-    float h, l;
-    split(v[r], h, l);
-    const int o = tile_off(r, k);
-    hi[o] = h;
-    lo[o] = l;
+  for (int b = 16; b >= 1; b >>= 1) {
+    const bool upper = (lane & b) != 0;
+#pragma unroll
+    for (int i = 0; i < 32; i++) {
+      if ((i & b) == 0) {
+        const int j = i | b;
+        const float send = upper ? v[i] : v[j];
+        const float recv = __shfl_xor_sync(0xffffffffu, send, b);
+        if (upper) v[i] = recv;
+        else v[j] = recv;
+      }
+    }
   }
+}
+
+// Whole warp: lane L holds column L of a 32 x 32 matrix X; write X row by
+// row into a tile pair (row n = X[n][:]).  `v` is transposed in place.
+__device__ __forceinline__ void put_rows_from_cols(float* hi, float* lo, float (&v)[32]) {
+  warp_transpose32(v);
+  put_row(hi, lo, threadIdx.x & 31, v);
 }
 
 }  // namespace tc

@@ -370,3 +370,51 @@ def test_mmult_3xtf32_kernel(native):
     ref = a @ b
     rel = np.max(np.abs(c - ref)) / np.max(np.abs(ref))
     assert rel < 2e-6, rel
+
+
+# ----------------------------------------------------------------- split-precision batched form
+SPLIT_TB_TOL = 0.05  # K: every TB of the 3xTF32 batched form against FP64
+
+
+def _run_prec(b, prec):
+    import torch
+    out = pbatch.run(b, 0, precision=prec)
+    torch.cuda.synchronize()
+    return {k: v.cpu().numpy() for k, v in out.items()}
+
+
+def test_split_precision_c2(oracle_mod, native):
+    from pamtra_b200._native import PREC_3XTF32, PREC_FP64
+    b = pbatch.pack_pam(wl.c2_pam(96, seed=8), wl.C2_FREQS)
+    f64 = _run_prec(b, PREC_FP64)
+    s = _run_prec(b, PREC_3XTF32)
+    assert int(np.count_nonzero(s["status"])) == 0
+    d = np.abs(s["tb"] - f64["tb"])
+    assert np.max(d) <= SPLIT_TB_TOL, np.max(d)
+    assert np.max(d) > 0.0  # the products really ran in split precision
+    for c in (0, 47, 95):
+        err, t, _, _, _ = oracle_mod.run_column(oracle_mod.settings(b.settings), b.species, b.host, c, wl.C2_FREQS)
+        assert err == 0
+        assert np.max(np.abs(s["tb"][c] - t)) <= SPLIT_TB_TOL
+
+
+def test_split_precision_target_shape(native):
+    from pamtra_b200._native import PREC_3XTF32, PREC_FP64
+    b = wl.target_batch(48, seed=9)
+    f64 = _run_prec(b, PREC_FP64)
+    s = _run_prec(b, PREC_3XTF32)
+    assert int(np.count_nonzero(s["status"])) == 0
+    assert np.max(np.abs(s["tb"] - f64["tb"])) <= SPLIT_TB_TOL
+
+
+def test_split_precision_uneven(native):
+    # NUMMU 16 columns take the tensor-core doubling, NUMMU 8 / 32 the FP64 one
+    from pamtra_b200._native import PREC_3XTF32, PREC_FP64
+    b = wl.uneven_batch(24, seed=13, nfreq_range=(2, 5))
+    f64 = _run_prec(b, PREC_FP64)
+    s = _run_prec(b, PREC_3XTF32)
+    assert np.array_equal(s["status"], f64["status"])
+    nmu = b.host["nummu"]
+    d = np.abs(s["tb"] - f64["tb"])
+    assert np.max(d) <= SPLIT_TB_TOL
+    assert np.all(d[nmu != 16] == 0.0)
