@@ -374,6 +374,10 @@ struct pamtra_b200_ctx {
   std::vector<unsigned char> sp_last;
   const char* sp_last_arena = nullptr;
   size_t sp_last_off = 0;
+  // scatcnv weight tables per NUMMU (allocated when first needed) and their
+  // need / ready flags [2][3][SCAT_NPI]
+  double* wtab[3] = {nullptr, nullptr, nullptr};
+  int* wt_flags = nullptr;
   int last_launches = 0;
   char* stage = nullptr;  // device staging for run_host
   size_t stage_bytes = 0;
@@ -472,6 +476,8 @@ int32_t pamtra_b200_destroy(pamtra_b200_ctx* ctx) {
   cudaFree(ctx->lob_mu);
   cudaFree(ctx->lob_w);
   cudaFree(ctx->stage);
+  for (double* p : ctx->wtab) cudaFree(p);
+  cudaFree(ctx->wt_flags);
   for (auto& sg : ctx->sp_ring) {
     if (sg.ev) cudaEventSynchronize(sg.ev), cudaEventDestroy(sg.ev);
     if (sg.h) cudaFreeHost(sg.h);
@@ -610,6 +616,22 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
   w.add_scr = (double*)(A + pl.o_addscr);
+  // scatcnv weight tables (context-resident; a table that cannot be allocated
+  // leaves the direct azimuth sums in place)
+  if (cc.nhydro > 0) {
+    if (!ctx->wt_flags && cudaMalloc(&ctx->wt_flags, 2 * 3 * SCAT_NPI * sizeof(int)) == cudaSuccess)
+      cudaMemsetAsync(ctx->wt_flags, 0, 2 * 3 * SCAT_NPI * sizeof(int), stream);
+    const int Ns[3] = {8, 16, 32};
+    for (int i = 0; i < 3; i++)
+      if (ctx->wt_flags && (mask & (1 << i)) && !ctx->wtab[i] &&
+          cudaMalloc(&ctx->wtab[i], scat_weight_doubles(Ns[i]) * sizeof(double)) != cudaSuccess) {
+        ctx->wtab[i] = nullptr;
+        cudaGetLastError();
+      }
+  }
+  for (int i = 0; i < 3; i++) w.wtab[i] = ctx->wt_flags ? ctx->wtab[i] : nullptr;
+  w.wt_need = ctx->wt_flags;
+  w.wt_ready = ctx->wt_flags ? ctx->wt_flags + 3 * SCAT_NPI : nullptr;
   w.gq_x = ctx->gq_x; w.gq_w = ctx->gq_w; w.gq_max = GQ_MAX; w.lob_mu = ctx->lob_mu; w.lob_w = ctx->lob_w;
 
   int launches = 0;
@@ -638,6 +660,18 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     const size_t sm_mie = MIE_WARPS * sizeof(MieSmem);
     int g = occupancy_blocks((const void*)k_mie, 32 * MIE_WARPS, sm_mie, sms);
     k_mie<<<g, 32 * MIE_WARPS, sm_mie, stream>>>(b, w, *st); launches++;
+    if (w.wtab[0] && (mask & 1)) {
+      k_scat_weights<8><<<SCAT_NPI * ((2 * 8 * 8 + 127) / 128), 128, 0, stream>>>(ctx->wtab[0], w.wt_need, w.wt_ready, ctx->lob_mu);
+      launches++;
+    }
+    if (w.wtab[1] && (mask & 2)) {
+      k_scat_weights<16><<<SCAT_NPI * ((2 * 16 * 16 + 127) / 128), 128, 0, stream>>>(ctx->wtab[1], w.wt_need, w.wt_ready, ctx->lob_mu);
+      launches++;
+    }
+    if (w.wtab[2] && (mask & 4)) {
+      k_scat_weights<32><<<SCAT_NPI * ((2 * 32 * 32 + 127) / 128), 128, 0, stream>>>(ctx->wtab[2], w.wt_need, w.wt_ready, ctx->lob_mu);
+      launches++;
+    }
   }
   mark(ctx, stream, STG_MIE);
   double* ssp = out->scatter_matrix;

@@ -104,6 +104,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
   const int Fm = b.max_nfreq;
   const int P = min(w.counters[0], w.pmax);
   const int nitems = P * Fm;
+  scat_weights_mark_ready<N>(w);
   if (warp == 0) tc::tmem_alloc(&tslot, 64);
   if (t == 0) {
     tc::mbar_init(&mbar, 1);

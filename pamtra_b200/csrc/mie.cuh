@@ -334,6 +334,10 @@ __global__ void __launch_bounds__(32 * MIE_WARPS) k_mie(Batch b, Work w, pamtra_
       w.m_kext[item] = kexttot;
       w.m_salb[item] = salbedo;
       w.m_nleg[item] = nlegen_coef;
+      if (w.wt_need && nlegen_coef > 0) {
+        const int numpts = 2 * ((nlegen_coef + 1) / 2) + 4;
+        w.wt_need[nmu_index(b.col_nummu(c)) * SCAT_NPI + (numpts - 4) / 2] = 1;
+      }
       if (status) atomicOr(&w.status[(size_t)c * Fm + f], status);
     }
     __syncwarp();

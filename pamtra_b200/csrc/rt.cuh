@@ -59,6 +59,81 @@ struct LayerSmem {
   int item, stat;
 };
 
+// Azimuth weights of scatcnv (src/scatcnv.f90:103-192 with SUM_LEGENDRE,
+// ROTATE_PHASE_MATRIX, MATRIX_SYMMETRY and FOURIER_BASIS order 0 of
+// src/rt_utilities.f90:242-493).  For NSTOKES = 2 the m = 0 phase-matrix
+// entries of one (mu1, mu2) pair are linear in the Legendre coefficients
+// c0, c1, c2 of an item:
+//   P11 = sum_l c0_l A_l,  P12 = sum_l c1_l B_l,  P21 = sum_l c1_l C_l,
+//   P22 = sum_l (c0_l D_l + c2_l E_l),
+// where A..E are the azimuth sums over k = 0..numpts/2 (weight 1 at the two
+// ends, 2 inside, / numpts) of P_l(cos Theta_k) times 1, cos 2i1, cos 2i2,
+// cos 2i1 cos 2i2 and -sin 2i1 sin 2i2.  The tables depend only on NUMMU and
+// numpts, so one kernel fills every numpts a batch has met (wt_need) that is
+// not filled yet (wt_ready); one thread per (numpts, mu1, mu2).
+template <int N>
+__global__ void __launch_bounds__(128) k_scat_weights(double* __restrict__ tab, const int* __restrict__ need,
+                                                      const int* __restrict__ ready, const double* lob_mu) {
+  constexpr int C2 = 2 * N * N;
+  constexpr int NB = (C2 + 127) / 128;
+  const int pi = blockIdx.x / NB;
+  const int combo = (blockIdx.x % NB) * 128 + threadIdx.x;
+  const int ni = nmu_index(N);
+  if (pi >= SCAT_NPI || combo >= C2 || !need[ni * SCAT_NPI + pi] || ready[ni * SCAT_NPI + pi]) return;
+  const int numpts = 2 * pi + 4, K = numpts / 2 + 1, nl = numpts - 3;
+  const int q = combo / (N * N), j1 = (combo / N) % N, j2 = combo % N;
+  const double mu1 = (q == 0) ? lob_mu[lob_off(N) + j1] : -lob_mu[lob_off(N) + j1];
+  const double mu2 = lob_mu[lob_off(N) + j2];
+  const double st1 = sqrt(1. - mu1 * mu1), st2 = sqrt(1. - mu2 * mu2);
+  const double sqm = sqrt((1. - mu1 * mu1) * (1. - mu2 * mu2));
+  double* T = tab + scat_weight_offset(N, pi) + combo;
+  for (int e = 0; e < nl * 5; e++) T[(size_t)e * C2] = 0.0;
+  for (int k = 0; k < K; k++) {
+    const double delphi = (TWO_PI * k) / numpts;
+    const double cosphi = cos(delphi), sinphi = sin(delphi);
+    const double cs = mu1 * mu2 + sqm * cosphi;
+    const double ss = sqrt(fmax(0.0, 1. - cs * cs));
+    double sin1, sin2, cos1, cos2;
+    if (ss == 0.0) {
+      sin1 = 0; sin2 = 0; cos1 = 1; cos2 = -1;
+    } else {
+      const double r = 1.0 / ss;
+      sin1 = st2 * sinphi * r;
+      sin2 = st1 * sinphi * r;
+      cos1 = (st1 * mu2 - st2 * mu1 * cosphi) * r;
+      cos2 = (st2 * mu1 - st1 * mu2 * cosphi) * r;
+    }
+    const double sin21 = 2.0 * sin1 * cos1, cos21 = 1.0 - 2.0 * (sin1 * sin1);
+    const double sin22 = 2.0 * sin2 * cos2, cos22 = 1.0 - 2.0 * (sin2 * sin2);
+    const double wk = (k > 0 && k < K - 1) ? 2.0 : 1.0;
+    const double f[5] = {wk, wk * cos21, wk * cos22, wk * (cos21 * cos22), -wk * (sin21 * sin22)};
+    double pl1 = 1.0, pl2 = 0.0;
+    for (int l = 0; l < nl; l++) {
+      double pl = 1.0;
+      if (l > 0) {
+        pl = fma(c_leg_a[l] * cs, pl1, -c_leg_b[l] * pl2);
+        pl2 = pl1;
+        pl1 = pl;
+      }
+      double* Tl = T + (size_t)l * 5 * C2;
+#pragma unroll
+      for (int e = 0; e < 5; e++) Tl[(size_t)e * C2] = fma(pl, f[e], Tl[(size_t)e * C2]);
+    }
+  }
+  const double inv = 1.0 / numpts;
+  for (int e = 0; e < nl * 5; e++) T[(size_t)e * C2] *= inv;
+}
+
+// Mark the numpts tables of N filled by k_scat_weights (run by one block of
+// the kernel that follows it on the stream).
+template <int N>
+__device__ __forceinline__ void scat_weights_mark_ready(const Work& w) {
+  const int ni = nmu_index(N);
+  if (blockIdx.x == 0 && w.wt_need)
+    for (int i = threadIdx.x; i < SCAT_NPI; i += blockDim.x)
+      if (w.wt_need[ni * SCAT_NPI + i]) w.wt_ready[ni * SCAT_NPI + i] = 1;
+}
+
 // Per-item state of the layer stage after the thin-layer initialisation.
 struct LayerItem {
   int c, z, fi, nd, status;
@@ -113,58 +188,94 @@ __device__ __forceinline__ bool layer_setup(const Batch& b, const Work& w, const
         coef[MAXNLEG + l] = cst * lg[MAXNLEG + l];
         coef[2 * MAXNLEG + l] = cst * lg[2 * MAXNLEG + l];
       }
-      for (int k = t; k < K; k += T) {
-        const double delphi = (TWO_PI * k) / numpts;
-        cphi[k] = cos(delphi);
-        sphi[k] = sin(delphi);
-      }
-      team_sync();
-      for (int it = t; it < 2 * N * N; it += T) {
-        const int q = it / (N * N), j1 = (it / N) % N, j2 = it % N;
-        const double mu1 = (q == 0) ? S.mu[j1] : -S.mu[j1];
-        const double mu2 = S.mu[j2];
-        const double st1 = sqrt(1. - mu1 * mu1), st2 = sqrt(1. - mu2 * mu2);
-        const double sqm = sqrt((1. - mu1 * mu1) * (1. - mu2 * mu2));
-        double a11 = 0, a12 = 0, a21 = 0, a22 = 0, m11 = 0, m12 = 0, m21 = 0, m22 = 0;
-        for (int k = 0; k < K; k++) {
-          const double cosphi = cphi[k], sinphi = sphi[k];
-          const double cs = mu1 * mu2 + sqm * cosphi;
-          // SUM_LEGENDRE, DOSUM = (1,1,1,0,0,0)
-          double s0 = coef[0], s1 = coef[MAXNLEG], s2 = coef[2 * MAXNLEG];
-          double pl1 = 1.0, pl2 = 0.0;
-          for (int L = 1; L <= nleg; L++) {
-            const double pl = fma(c_leg_a[L] * cs, pl1, -c_leg_b[L] * pl2);
-            s0 = fma(coef[L], pl, s0);
-            s1 = fma(coef[MAXNLEG + L], pl, s1);
-            s2 = fma(coef[2 * MAXNLEG + L], pl, s2);
-            pl2 = pl1;
-            pl1 = pl;
+      const double* W = w.wtab[nmu_index(N)];
+      if (W) {
+        // phase matrices from the azimuth weight tables (k_scat_weights)
+        team_sync();
+        constexpr int C2 = 2 * N * N, CPT = C2 / T;
+        static_assert(C2 % T == 0, "combos per thread");
+        const double* Wp = W + scat_weight_offset(N, (numpts - 4) / 2);
+        double acc[CPT][4];
+#pragma unroll
+        for (int u = 0; u < CPT; u++) acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0;
+        for (int l = 0; l <= nleg; l++) {
+          const double c0 = coef[l], c1 = coef[MAXNLEG + l], c2 = coef[2 * MAXNLEG + l];
+          const double* Wl = Wp + (size_t)l * 5 * C2 + t;
+#pragma unroll
+          for (int u = 0; u < CPT; u++) {
+            const double* Wc = Wl + u * T;
+            acc[u][0] = fma(c0, Wc[0], acc[u][0]);
+            acc[u][1] = fma(c1, Wc[C2], acc[u][1]);
+            acc[u][2] = fma(c1, Wc[2 * C2], acc[u][2]);
+            acc[u][3] = fma(c0, Wc[3 * C2], acc[u][3]);
+            acc[u][3] = fma(c2, Wc[4 * C2], acc[u][3]);
           }
-          // ROTATE_PHASE_MATRIX (NSTOKES=2)
-          const double ss = sqrt(fmax(0.0, 1. - cs * cs));
-          double sin1, sin2, cos1, cos2;
-          if (ss == 0.0) {
-            sin1 = 0; sin2 = 0; cos1 = 1; cos2 = -1;
-          } else {
-            const double r = 1.0 / ss;
-            sin1 = st2 * sinphi * r;
-            sin2 = st1 * sinphi * r;
-            cos1 = (st1 * mu2 - st2 * mu1 * cosphi) * r;
-            cos2 = (st2 * mu1 - st1 * mu2 * cosphi) * r;
-          }
-          const double sin21 = 2.0 * sin1 * cos1, cos21 = 1.0 - 2.0 * (sin1 * sin1);
-          const double sin22 = 2.0 * sin2 * cos2, cos22 = 1.0 - 2.0 * (sin2 * sin2);
-          const double e11 = s0, e12 = s1 * cos21, e21 = s1 * cos22, e22 = s0 * cos21 * cos22 - s2 * sin21 * sin22;
-          // FOURIER_BASIS order 0: points k and numpts-k coincide (MATRIX_SYMMETRY)
-          a11 += e11; a12 += e12; a21 += e21; a22 += e22;
-          if (k > 0 && k < K - 1) { m11 += e11; m12 += e12; m21 += e21; m22 += e22; }
         }
-        double* Q = (q == 0) ? Tb : Rb;
-        const int row0 = 2 * j2, col0 = 2 * j1;
-        Q[(col0 + 0) * LD + row0 + 0] = (a11 + m11) / numpts;
-        Q[(col0 + 1) * LD + row0 + 0] = (a12 + m12) / numpts;
-        Q[(col0 + 0) * LD + row0 + 1] = (a21 + m21) / numpts;
-        Q[(col0 + 1) * LD + row0 + 1] = (a22 + m22) / numpts;
+#pragma unroll
+        for (int u = 0; u < CPT; u++) {
+          const int it = t + u * T;
+          const int q = it / (N * N), j1 = (it / N) % N, j2 = it % N;
+          double* Qm = (q == 0) ? Tb : Rb;
+          const int row0 = 2 * j2, col0 = 2 * j1;
+          Qm[(col0 + 0) * LD + row0 + 0] = acc[u][0];
+          Qm[(col0 + 1) * LD + row0 + 0] = acc[u][1];
+          Qm[(col0 + 0) * LD + row0 + 1] = acc[u][2];
+          Qm[(col0 + 1) * LD + row0 + 1] = acc[u][3];
+        }
+      } else {
+        for (int k = t; k < K; k += T) {
+          const double delphi = (TWO_PI * k) / numpts;
+          cphi[k] = cos(delphi);
+          sphi[k] = sin(delphi);
+        }
+        team_sync();
+        for (int it = t; it < 2 * N * N; it += T) {
+          const int q = it / (N * N), j1 = (it / N) % N, j2 = it % N;
+          const double mu1 = (q == 0) ? S.mu[j1] : -S.mu[j1];
+          const double mu2 = S.mu[j2];
+          const double st1 = sqrt(1. - mu1 * mu1), st2 = sqrt(1. - mu2 * mu2);
+          const double sqm = sqrt((1. - mu1 * mu1) * (1. - mu2 * mu2));
+          double a11 = 0, a12 = 0, a21 = 0, a22 = 0, m11 = 0, m12 = 0, m21 = 0, m22 = 0;
+          for (int k = 0; k < K; k++) {
+            const double cosphi = cphi[k], sinphi = sphi[k];
+            const double cs = mu1 * mu2 + sqm * cosphi;
+            // SUM_LEGENDRE, DOSUM = (1,1,1,0,0,0)
+            double s0 = coef[0], s1 = coef[MAXNLEG], s2 = coef[2 * MAXNLEG];
+            double pl1 = 1.0, pl2 = 0.0;
+            for (int L = 1; L <= nleg; L++) {
+              const double pl = fma(c_leg_a[L] * cs, pl1, -c_leg_b[L] * pl2);
+              s0 = fma(coef[L], pl, s0);
+              s1 = fma(coef[MAXNLEG + L], pl, s1);
+              s2 = fma(coef[2 * MAXNLEG + L], pl, s2);
+              pl2 = pl1;
+              pl1 = pl;
+            }
+            // ROTATE_PHASE_MATRIX (NSTOKES=2)
+            const double ss = sqrt(fmax(0.0, 1. - cs * cs));
+            double sin1, sin2, cos1, cos2;
+            if (ss == 0.0) {
+              sin1 = 0; sin2 = 0; cos1 = 1; cos2 = -1;
+            } else {
+              const double r = 1.0 / ss;
+              sin1 = st2 * sinphi * r;
+              sin2 = st1 * sinphi * r;
+              cos1 = (st1 * mu2 - st2 * mu1 * cosphi) * r;
+              cos2 = (st2 * mu1 - st1 * mu2 * cosphi) * r;
+            }
+            const double sin21 = 2.0 * sin1 * cos1, cos21 = 1.0 - 2.0 * (sin1 * sin1);
+            const double sin22 = 2.0 * sin2 * cos2, cos22 = 1.0 - 2.0 * (sin2 * sin2);
+            const double e11 = s0, e12 = s1 * cos21, e21 = s1 * cos22, e22 = s0 * cos21 * cos22 - s2 * sin21 * sin22;
+            // FOURIER_BASIS order 0: points k and numpts-k coincide (MATRIX_SYMMETRY)
+            a11 += e11; a12 += e12; a21 += e21; a22 += e22;
+            if (k > 0 && k < K - 1) { m11 += e11; m12 += e12; m21 += e21; m22 += e22; }
+          }
+          double* Q = (q == 0) ? Tb : Rb;
+          const int row0 = 2 * j2, col0 = 2 * j1;
+          Q[(col0 + 0) * LD + row0 + 0] = (a11 + m11) / numpts;
+          Q[(col0 + 1) * LD + row0 + 0] = (a12 + m12) / numpts;
+          Q[(col0 + 0) * LD + row0 + 1] = (a21 + m21) / numpts;
+          Q[(col0 + 1) * LD + row0 + 1] = (a22 + m22) / numpts;
+        }
       }
       team_sync();
       if (!st.lhyd_scattering) {
@@ -270,6 +381,7 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
   const int Fm = b.max_nfreq;
   const int P = min(w.counters[0], w.pmax);
   const int nitems = P * Fm;
+  scat_weights_mark_ready<N>(w);
   if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
   for (;;) {
     team_sync();

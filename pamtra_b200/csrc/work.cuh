@@ -62,6 +62,10 @@ struct Work {
   int* lay_nd;                         // [pmax*Fm]
   // adding matrices that do not fit in shared memory (N = 32 only)
   double* add_scr;                     // [adding CTAs][4][MAT]
+  // scatcnv weight tables per NUMMU index (0: N = 8, 1: 16, 2: 32); null = direct sums
+  const double* wtab[3];               // [numpts index][l][5][2 N^2], see scat_weight_offset
+  int* wt_need;                        // [3][SCAT_NPI] numpts values seen (set by k_mie)
+  int* wt_ready;                       // [3][SCAT_NPI] tables already computed
   // status
   int* status;                         // [C][Fm]
   int* col_status;                     // [C]
@@ -74,5 +78,16 @@ struct Work {
 };
 
 __host__ __device__ __forceinline__ int lob_off(int N) { return N == 8 ? 0 : (N == 16 ? 8 : 24); }
+__host__ __device__ __forceinline__ int nmu_index(int N) { return N == 8 ? 0 : (N == 16 ? 1 : 2); }
+
+// scatcnv weight tables: numpts = 2 * ((nlegen + 1) / 2) + 4 takes SCAT_NPI
+// values 4, 6, ..., 204 (index pi = (numpts - 4) / 2); the table of pi holds
+// numpts - 3 = 2 pi + 1 Legendre orders x 5 weights x 2 N^2 (mu1, mu2) pairs,
+// so it starts 10 N^2 pi^2 doubles into the tables of N.
+constexpr int SCAT_NPI = 101;
+__host__ __device__ __forceinline__ size_t scat_weight_offset(int N, int pi) {
+  return (size_t)10 * N * N * pi * pi;
+}
+__host__ __device__ __forceinline__ size_t scat_weight_doubles(int N) { return scat_weight_offset(N, SCAT_NPI); }
 
 }  // namespace pb
