@@ -398,6 +398,20 @@ static void mark(pamtra_b200_ctx* ctx, cudaStream_t s, int stage) {
   ctx->nev++;
 }
 
+// c_n of mieangle in REAL(4) arithmetic (host float division is IEEE, as on
+// the device) and 1/n
+static int upload_mie_constants() {
+  double c[NT_MAX + 1], r[NT_MAX + 1];
+  c[0] = 0.0;
+  r[0] = 0.0;
+  for (int n = 1; n <= NT_MAX; n++) {
+    c[n] = (double)((float)(2 * n + 1) / (float)(n * (n + 1)));
+    r[n] = 1.0 / n;
+  }
+  return (cudaMemcpyToSymbol(c_mie_c, c, sizeof(c)) != cudaSuccess ||
+          cudaMemcpyToSymbol(c_mie_inv, r, sizeof(r)) != cudaSuccess) ? 1 : 0;
+}
+
 static int set_smem_attrs() {
   static std::once_flag once;
   static int rc = 0;
@@ -445,6 +459,7 @@ int32_t pamtra_b200_create(int32_t device, pamtra_b200_ctx** out) {
     cudaMemcpyToSymbol(c_leg_a, la, sizeof(la));
     cudaMemcpyToSymbol(c_leg_b, lb, sizeof(lb));
   }
+  upload_mie_constants();
   k_lobatto_table<<<3, 32>>>(ctx->lob_mu, ctx->lob_w);
   cudaMemcpyToSymbol(c_o2_w300, H_O2_W300, sizeof(H_O2_W300));
   cudaMemcpyToSymbol(c_o2_y300, H_O2_Y300, sizeof(H_O2_Y300));
@@ -916,7 +931,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
         la[l] = (2.0 * l - 1.0) / l;
         lb[l] = (l - 1.0) / l;
       }
-      if (cudaMemcpyToSymbol(c_leg_a, la, sizeof(la)) || cudaMemcpyToSymbol(c_leg_b, lb, sizeof(lb)) ||
+      if (upload_mie_constants() || cudaMemcpyToSymbol(c_leg_a, la, sizeof(la)) || cudaMemcpyToSymbol(c_leg_b, lb, sizeof(lb)) ||
           cudaMemcpyToSymbol(c_o2_w300, H_O2_W300, sizeof(H_O2_W300)) ||
           cudaMemcpyToSymbol(c_o2_y300, H_O2_Y300, sizeof(H_O2_Y300)) ||
           cudaMemcpyToSymbol(c_o2_v, H_O2_V, sizeof(H_O2_V)) || cudaMemcpyToSymbol(c_o2_f, H_O2_F, sizeof(H_O2_F)) ||

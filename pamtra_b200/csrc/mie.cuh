@@ -10,12 +10,19 @@ namespace pb {
 constexpr int MIE_WARPS = 4;
 constexpr int NQ_MAX = 256;   // Gauss points per series (nquad)
 constexpr int NT_MAX = 128;   // Mie terms per bin
+constexpr int ANG_G = 2;      // angles per pass over a bin's Mie coefficients
 
 struct MieSmem {
   double sump[4][NQ_MAX];
   double legh[3][MAXNLEG];
   double legc[3][MAXNLEG];
 };
+
+// Per-term constants: c_n = (2n+1) / (n(n+1)) of mieangle evaluated in REAL(4)
+// as the reference does (mie_scat_utilities.f90:139), and 1/n, which replaces
+// the divisions by n in the pi_n and Legendre recurrences (the reference
+// divides; the products differ from the quotients in the last bit only).
+__constant__ double c_mie_c[NT_MAX + 1], c_mie_inv[NT_MAX + 1];
 
 // src/eps_water.f90:653-757 eps_water_tkc (T in degC, f in GHz)
 __device__ cplx eps_water_tkc(double T, double f) {
@@ -75,10 +82,12 @@ __device__ void miecalc_cross(int nterms, double x, cplx mn, cplx* ab, cplx* bb,
   const cplx m = cconj(mn);
   const cplx y = cscale(m, x);
   const int nn = nterms + 15;
+  // n / y and d / m through the reciprocals of y and m (one complex division each per particle)
+  const cplx yinv = cdiv(cmk(1.0, 0.0), y), minv = cdiv(cmk(1.0, 0.0), m);
   // downward recurrence d(n-1) = n/y - 1/(d(n) + n/y), d(nn) = 0; keep d(1..nterms)
   cplx d = cmk(0.0, 0.0);
   for (int n = nn; n >= 2; n--) {
-    cplx ny = cdiv(cmk((double)n, 0.0), y);
+    cplx ny = cscale(yinv, (double)n);
     d = csub(ny, cdiv(cmk(1.0, 0.0), cadd(d, ny)));
     if (n - 1 <= nterms) ab[n - 2] = d;  // d(n-1) stored at index n-2
   }
@@ -94,7 +103,7 @@ __device__ void miecalc_cross(int nterms, double x, cplx mn, cplx* ab, cplx* bb,
     chim = tmp;
     const cplx xin = cmplx4(psin, -chin), xim = cmplx4(psim, -chim);
     const cplx dn = ab[n - 1];
-    cplx ctmp = cdiv(dn, m);
+    cplx ctmp = cmul(dn, minv);
     ctmp.re = ctmp.re + n / x;
     cplx an = cdiv(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
     ctmp = cmul(m, dn);
@@ -134,6 +143,43 @@ __device__ __forceinline__ void mieangle(int nterms, const cplx* ab, const cplx*
   p[1] = 0.5 * (as2 * as2 - as1 * as1);
   p[2] = s2.re * s1.re - (-s2.im) * s1.im;
   p[3] = s1.re * s2.im + (-s1.im) * s2.re;
+}
+
+// mieangle for ANG_G angles of one particle at once: the coefficients a_n,
+// b_n are read once per n for all angles, and the pi_n recurrence multiplies
+// by the tabulated 1/n.
+__device__ __forceinline__ void mieangle_group(int nterms, const cplx* ab, const cplx* bb, const double (&mu)[ANG_G],
+                                               double (&p)[ANG_G][4]) {
+  double pin[ANG_G], pim[ANG_G], s1r[ANG_G], s1i[ANG_G], s2r[ANG_G], s2i[ANG_G];
+#pragma unroll
+  for (int g = 0; g < ANG_G; g++) {
+    pin[g] = 1.0; pim[g] = 0.0;
+    s1r[g] = 0.0; s1i[g] = 0.0; s2r[g] = 0.0; s2i[g] = 0.0;
+  }
+  for (int n = 1; n <= nterms; n++) {
+    const cplx a = ab[n - 1], b = bb[n - 1];
+    const double c = c_mie_c[n], rn = c_mie_inv[n];
+    const double dn = (double)n, dn1 = (double)(n + 1), d2n1 = (double)(2 * n + 1);
+#pragma unroll
+    for (int g = 0; g < ANG_G; g++) {
+      const double taun = dn * mu[g] * pin[g] - dn1 * pim[g];
+      s1r[g] = fma(c, fma(a.re, pin[g], b.re * taun), s1r[g]);
+      s1i[g] = fma(c, fma(a.im, pin[g], b.im * taun), s1i[g]);
+      s2r[g] = fma(c, fma(b.re, pin[g], a.re * taun), s2r[g]);
+      s2i[g] = fma(c, fma(b.im, pin[g], a.im * taun), s2i[g]);
+      const double tmp = pin[g];
+      pin[g] = (d2n1 * mu[g] * pin[g] - dn1 * pim[g]) * rn;
+      pim[g] = tmp;
+    }
+  }
+#pragma unroll
+  for (int g = 0; g < ANG_G; g++) {
+    const double as1 = hypot(s1r[g], s1i[g]), as2 = hypot(s2r[g], s2i[g]);
+    p[g][0] = 0.5 * (as2 * as2 + as1 * as1);
+    p[g][1] = 0.5 * (as2 * as2 - as1 * as1);
+    p[g][2] = s2r[g] * s1r[g] - (-s2i[g]) * s1i[g];
+    p[g][3] = s1r[g] * s2i[g] + (-s1i[g]) * s2r[g];
+  }
 }
 
 // One warp per (present layer, frequency) item; species loop in descriptor
@@ -242,18 +288,32 @@ __global__ void __launch_bounds__(32 * MIE_WARPS) k_mie(Batch b, Work w, pamtra_
           nm = min(nmie, nterms);
           wgt = ndens;
         }
-        for (int i = 0; i < nquad; i++) {
-          double pp[4] = {0.0, 0.0, 0.0, 0.0};
+        for (int i0 = 0; i0 < nquad; i0 += ANG_G) {
+          double pp[ANG_G][4];
           if (act) {
-            mieangle(nm, ab, bb, gx[i], pp);
+            double mu[ANG_G];
 #pragma unroll
-            for (int k = 0; k < 4; k++) pp[k] = pp[k] * wgt * deld;
+            for (int g = 0; g < ANG_G; g++) mu[g] = (i0 + g < nquad) ? gx[i0 + g] : 0.0;
+            mieangle_group(nm, ab, bb, mu, pp);
+#pragma unroll
+            for (int g = 0; g < ANG_G; g++)
+#pragma unroll
+              for (int k = 0; k < 4; k++) pp[g][k] = pp[g][k] * wgt * deld;
+          } else {
+#pragma unroll
+            for (int g = 0; g < ANG_G; g++)
+#pragma unroll
+              for (int k = 0; k < 4; k++) pp[g][k] = 0.0;
           }
 #pragma unroll
-          for (int k = 0; k < 4; k++) pp[k] = warp_sum(pp[k]);
-          if (lane == (i & 31)) {
+          for (int g = 0; g < ANG_G; g++) {
+            const int i = i0 + g;
 #pragma unroll
-            for (int k = 0; k < 4; k++) S.sump[k][i] += pp[k];
+            for (int k = 0; k < 4; k++) pp[g][k] = warp_sum(pp[g][k]);
+            if (i < nquad && lane == (i & 31)) {
+#pragma unroll
+              for (int k = 0; k < 4; k++) S.sump[k][i] += pp[g][k];
+            }
           }
         }
       }
@@ -285,7 +345,7 @@ __global__ void __launch_bounds__(32 * MIE_WARPS) k_mie(Batch b, Work w, pamtra_
           const int i = lane + 32 * q;
           if (i < nquad) {
             const double mu = gx[i];
-            if (l > 0) pl[q] = (2 * l - 1) * mu * pl1[q] / l - (l - 1) * pl2[q] / l;
+            if (l > 0) pl[q] = ((2 * l - 1) * mu * pl1[q] - (l - 1) * pl2[q]) * c_mie_inv[l];
 #pragma unroll
             for (int k = 0; k < 3; k++) acc[k] = fma(S.sump[k][i], pl[q], acc[k]);
             pl2[q] = pl1[q];
