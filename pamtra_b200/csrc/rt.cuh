@@ -400,16 +400,13 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
     double* Wb = S.m[3];
     double* Yb = S.m[4];
     // ---------------- DOUBLING_INTEGRATION4, SYMMETRIC (src/radintg4.f90:174-309)
+    // R' = R + T G R T and T' = T G T with G = (I - R R)^-1, as five products
+    // per step: W = T G, then R' = R + W (R T) and T' = W T; the source
+    // chains use W u for T G u.
+    constexpr int NV = (4 * n + T - 1) / T;
     for (int itd = 0; itd < nd; itd++) {
       mm<n, MM_SET>(Rb, Rb, Gb);  // R+ R-
-      team_sync();
-      {
-        int sg = 0;
-        double* gi = inv_iminus<n>(Gb, Wb, S.inv, &sg);  // GAMMA = inv(I - R+ R-)
-        if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-        if (gi != Gb) { Wb = Gb; Gb = gi; }
-      }
-      // source chains: v = [S- + f C-, C-, S+, C+] -> R v -> add -> G -> T
+      // v = [S- + f C-, C-, S+, C+]
       for (int o = t; o < 4 * n; o += T) {
         const int r = o % n, k = o / n;
         double v;
@@ -420,6 +417,14 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
         S.v[k][r] = v;
       }
       team_sync();
+      {
+        int sg = 0;
+        double* gi = inv_iminus<n>(Gb, Wb, S.inv, &sg);  // GAMMA = inv(I - R+ R-)
+        if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+        if (gi != Gb) { Wb = Gb; Gb = gi; }
+      }
+      // W = T G;  u = [S+ + R v0, C+ + R v1, v0 + R v2, C- + R v3]
+      mm<n, MM_SET>(Tb, Gb, Wb);
       for (int o = t; o < 4 * n; o += T) {
         const int r = o % n, k = o / n;
         const double a = mv_row<n>(Rb, S.v[k], r);
@@ -431,37 +436,27 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
         S.u[k][r] = u;
       }
       team_sync();
-      for (int o = t; o < 4 * n; o += T) {
-        const int r = o % n, k = o / n;
-        S.v[k][r] = mv_row<n>(Gb, S.u[k], r);
-      }
-      team_sync();
-      double onew[(4 * n + T - 1) / T];
+      // Y = R T;  new sources from W u
+      mm<n, MM_SET>(Rb, Tb, Yb);
+      double onew[NV];
 #pragma unroll
-      for (int s = 0; s < (4 * n + T - 1) / T; s++) {
+      for (int s = 0; s < NV; s++) {
         const int o = t + s * T;
         if (o < 4 * n) {
           const int r = o % n, k = o / n;
-          const double a = mv_row<n>(Tb, S.v[k], r);
+          const double a = mv_row<n>(Wb, S.u[k], r);
           if (k == 0) onew[s] = (S.lin[r] + a) + linfac * S.cst[r];
           else if (k == 1) onew[s] = S.cst[r] + a;
           else if (k == 2) onew[s] = S.lin[n + r] + a;
           else onew[s] = S.cst[n + r] + a;
         }
       }
-      // matrices: R' = R + T G R T ; T' = T G T
-      mm<n, MM_SET>(Rb, Tb, Wb);
       team_sync();
-      mm<n, MM_SET>(Gb, Wb, Yb);
-      team_sync();
-      mm<n, MM_ACC>(Tb, Yb, Rb, Rb);
-      mm<n, MM_SET>(Gb, Tb, Wb);
-      team_sync();
-      mm<n, MM_SET>(Tb, Wb, Yb);
-      team_sync();
-      { double* tmp = Tb; Tb = Yb; Yb = tmp; }
+      // R' = R + W Y;  T' = W T (into the G buffer)
+      mm<n, MM_ACC>(Wb, Yb, Rb, Rb);
+      mm<n, MM_SET>(Wb, Tb, Gb);
 #pragma unroll
-      for (int s = 0; s < (4 * n + T - 1) / T; s++) {
+      for (int s = 0; s < NV; s++) {
         const int o = t + s * T;
         if (o < 4 * n) {
           const int r = o % n, k = o / n;
@@ -471,6 +466,7 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
           else S.cst[n + r] = onew[s];
         }
       }
+      { double* tmp = Tb; Tb = Gb; Gb = tmp; }
       linfac = 2.0 * linfac;
       team_sync();
     }
