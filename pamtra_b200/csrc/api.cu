@@ -700,10 +700,10 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   }
   if (mask & 2) {
     if (H > 0 && precision == PAMTRA_B200_PREC_3XTF32) {
-      // three CTAs per SM by shared memory and registers (the occupancy query
-      // under-reports this kernel); the persistent CTAs take work from a counter
+      // two CTAs (two item pairs) per SM by shared memory; the persistent CTAs
+      // take pairs of items from a counter
       const size_t smb = layer_tc_smem<16>();
-      const int g = 3 * sms;
+      const int g = 2 * sms;
       k_layer_tc<16><<<g, 128, smb, stream>>>(b, w, *st, ssp); launches++;
     } else if (H > 0) {
       int g = occupancy_blocks((const void*)k_layer<16>, RTCfg<16>::T, sizeof(LayerSmem<16>), sms);

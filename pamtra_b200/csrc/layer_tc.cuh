@@ -8,25 +8,26 @@
 // useful relative accuracy, so the loop carries the deviations
 //     T~ = I - T,   G~ = G - I,   G = (I - R R)^-1
 // and adds identity parts exactly in the epilogues:
-//     P  = R R                     V  = R - R T~
-//     G~ = P + P^2 + ... (repeated squaring from G~ = 0, X = P:
-//                         G~' = G~ + X + X G~, X' = X X)
-//     Y  = V + G~ V                Z~ = T~ - G~ + G~ T~
+//     P  = R R                     V  = R - R T~          (= R T)
+//     G~ = P + P^2 + ...   repeated squaring from G~ = 0, X = P:
+//                          G~' = G~ + X + X G~,  X' = X X
+//     Y  = V + G~ V                Z~ = T~ - G~ + G~ T~   (G T = I - Z~)
 //     R' = R + Y - T~ Y            T~' = T~ + Z~ - T~ Z~
-// Sources follow the FP64 kernel (R v, G u = u + G~ u, T w = w - T~ w).
+// Sources follow the FP64 kernel (R v, G u = u + G~ u, T w = w - T~ w) as
+// FP32 matrix-vector products on the CUDA cores, overlapped with the MMAs.
 //
-// Products are arranged so that each MMA computes two n x n products that
-// share their left factor X:  D = [A1^T; A2^T; v^T] * X^T.  Row m of the A
-// tile is column m of a right factor, row n of the B tile is row n of X, and
-// TMEM lane m of D is column m of X A1 (lanes 32+m: X A2; lanes 64..67: X v
-// for the four source vectors).  Threads hold columns, so A rows are written
-// directly and B tiles after an in-register warp transpose.  M = 128 (rows
-// 68..127 of the A tile are never used), N = 32, K = 32.
-//
-// Thread roles (128 threads): warp 0 owns lanes 0..31 (first product), warp 1
-// lanes 32..63 (second product), lanes 0..3 of warp 2 the source vectors,
-// thread 96 issues the MMAs.  One (layer, frequency) item per CTA at a time;
-// 3 CTAs per SM (the launch asks for that many) overlap their MMA chains.
+// Pairing.  One CTA (4 warps) carries two (layer, frequency) items through
+// their doublings in lockstep, and every MMA serves both: with D = A B^T,
+//     A = [Y1a^T; Y1b^T; Y2a^T; Y2b^T]   (128 rows: columns of the right factors)
+//     B = [X1; X2]                        (64 rows: rows of each item's left factor)
+// lane 64i + 32p + m of D, columns 32i..32i+31, is column m of X_i Y_ip.  The
+// off-diagonal blocks (X1 Y2a, ...) are computed and ignored, so each item's
+// results depend on its own operands only: the pairing does not change any
+// value.  Warp 2i + p owns the lanes of product p of item i, so every warp
+// does the same kind of work (no idle warps, no divergent roles inside a warp).
+// An item that has finished its doublings (or its series steps) while its
+// partner goes on keeps its state and skips its epilogues.  M = 128, N = 64,
+// K = 32: no row of the MMA is padding.
 #pragma once
 #include "rt.cuh"
 #include "tc.cuh"
@@ -35,24 +36,37 @@ namespace pb {
 
 constexpr int MS = 36;  // column stride of the FP32 masters: quarter-warp float4 accesses are conflict-free
 
-struct TcSmem {
-  float a_hi[9 * 256], a_lo[9 * 256];  // A tile pair, rows 0..71 (the MMA also reads rows 72..127)
-  float br_hi[1024], br_lo[1024];      // B tile of the left factor R
-  float bt_hi[1024], bt_lo[1024];      // B tile of T~
-  float bx_hi[1024], bx_lo[1024];      // B tile of X, then of G~
-  float rm[32 * 36], tm[32 * 36], gm[32 * 36], xm[32 * 36];  // FP32 masters, column c at [c * MS]
-  float lp[32], cp[32], lmn[32], cmn[32];        // S+ linear, S+ constant, S- linear, S- constant
-  float vv[4][32], uv[4][32];
-  float nrm, pad_[3];
+// FP32 state of one item of the pair (column-major masters, column c at [c * MS]).
+struct TcItemState {
+  float rm[32 * MS], tm[32 * MS], gm[32 * MS], xm[32 * MS];  // R, T~, G~, X
+  float src[4][32];                                          // S+ linear, S+ constant, S- linear, S- constant
+  float vv[4][32], uv[4][32], wv[4][32];                     // right-hand vectors of the three groups
+  float nrm;
+  int pad_[3];
 };
-static_assert(sizeof(TcSmem) % 16 == 0, "tile alignment");
+
+struct TcTiles {
+  float a_hi[128 * 32], a_lo[128 * 32];  // A tile pair (128 rows)
+  float b_hi[64 * 32], b_lo[64 * 32];    // B tile pair (64 rows: 32 per item)
+};
+
+union __align__(128) TcScratch {
+  TcTiles tl;
+  LayerSmem<16> setup;  // the FP64 set-up of one item at a time
+};
+
+struct TcPairSmem {
+  TcItemState st[2];
+  TcScratch u;
+};
+static_assert(sizeof(TcItemState) % 16 == 0, "tile alignment");
 
 constexpr float NEUMANN_TOL = 1.0e-8f;  // truncation of G~ relative to its size
 constexpr float NEUMANN_MAX_NORM = 0.75f;
 
 template <int N>
 constexpr size_t layer_tc_smem() {
-  return (sizeof(LayerSmem<N>) > sizeof(TcSmem) ? sizeof(LayerSmem<N>) : sizeof(TcSmem));
+  return sizeof(TcPairSmem);
 }
 
 // thread-owned column helpers (column-major masters, column stride S)
@@ -69,38 +83,62 @@ __device__ __forceinline__ void st_col(float* m, int col, const float (&v)[32]) 
 #pragma unroll
   for (int r = 0; r < 32; r += 4) *reinterpret_cast<float4*>(m + col * S + r) = make_float4(v[r], v[r + 1], v[r + 2], v[r + 3]);
 }
+// row `row` of a master (lanes read consecutive words: conflict-free)
+__device__ __forceinline__ void ld_row(const float* m, int row, float (&v)[32]) {
+#pragma unroll
+  for (int k = 0; k < 32; k++) v[k] = m[k * MS + row];
+}
 
-// Whole warp, lane L holding column L of a 32 x 32 matrix (v[i] = M[i][L]):
-// returns in lane L the sum of row L, sum_m M[L][m] (reduce-scatter in five
-// butterfly stages, 31 shuffles; v is consumed).
-__device__ __forceinline__ float row_sum_scatter(float (&v)[32]) {
-  const int lane = threadIdx.x & 31;
+// (M x0)[r] and (M x1)[r] for a master M (k-ascending FMA chains)
+__device__ __forceinline__ void matvec2(const float* __restrict__ M, const float* __restrict__ x0,
+                                        const float* __restrict__ x1, int r, float& y0, float& y1) {
+  float a0 = 0.f, a1 = 0.f;
 #pragma unroll
-  for (int h = 16; h >= 1; h >>= 1) {
-    const bool upper = (lane & h) != 0;
-#pragma unroll
-    for (int k = 0; k < h; k++) {
-      const float lo = v[k], hi = v[k + h];
-      const float send = upper ? lo : hi;
-      const float keep = upper ? hi : lo;
-      v[k] = keep + __shfl_xor_sync(0xffffffffu, send, h);
-    }
+  for (int k = 0; k < 32; k += 4) {
+    const float4 p = *reinterpret_cast<const float4*>(x0 + k);
+    const float4 q = *reinterpret_cast<const float4*>(x1 + k);
+    const float m0 = M[k * MS + r], m1 = M[(k + 1) * MS + r], m2 = M[(k + 2) * MS + r], m3 = M[(k + 3) * MS + r];
+    a0 = fmaf(m0, p.x, a0); a1 = fmaf(m0, q.x, a1);
+    a0 = fmaf(m1, p.y, a0); a1 = fmaf(m1, q.y, a1);
+    a0 = fmaf(m2, p.z, a0); a1 = fmaf(m2, q.z, a1);
+    a0 = fmaf(m3, p.w, a0); a1 = fmaf(m3, q.w, a1);
   }
-  return v[0];
+  y0 = a0;
+  y1 = a1;
+}
+
+// Number of squarings of the series for ||X|| = nrm (any sub-multiplicative
+// norm): s >= 1 means s + 1 MMAs, 0 means G~ = X, -1 the FP64 fallback.
+__device__ __forceinline__ int series_steps(float nrm) {
+  if (!(nrm < NEUMANN_MAX_NORM)) return -1;
+  float pw = nrm;  // nrm^(2^(s+1) - 1)
+  float pk = nrm;  // nrm^(2^s)
+  int s = 0;
+  while (pw > NEUMANN_TOL && s < 6) {
+    pk = pk * pk;
+    pw = pw * pk;
+    s++;
+  }
+  return s;
 }
 
 template <int N>
-__global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b200_settings st,
+__global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b200_settings st,
                                                      double* __restrict__ ssp_scat) {
   static_assert(N == 16, "the split-precision layer kernel is built for NUMMU = 16");
   constexpr int n = 32, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT;
   extern __shared__ __align__(1024) double smem_raw[];
-  LayerSmem<N>& S = *reinterpret_cast<LayerSmem<N>*>(smem_raw);
-  TcSmem& Q = *reinterpret_cast<TcSmem*>(smem_raw);  // aliases S after the FP64 setup
+  TcPairSmem& Q = *reinterpret_cast<TcPairSmem*>(smem_raw);
+  LayerSmem<N>& S = Q.u.setup;
+  TcTiles& TL = Q.u.tl;
   __shared__ uint64_t mbar;
   __shared__ uint32_t tslot;
-  __shared__ int s_item, s_dead;
+  __shared__ int s_base, s_dead;
+  __shared__ int s_valid[2], s_nd[2], s_status[2], s_c[2], s_fi[2];
+  __shared__ float s_linfac[2];
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int mi = warp >> 1, slot = warp & 1;  // my item of the pair, my product
+  TcItemState& my = Q.st[mi];
   const int Fm = b.max_nfreq;
   const int P = min(w.counters[0], w.pmax);
   const int nitems = P * Fm;
@@ -113,18 +151,20 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  const uint32_t tm0 = tslot;       // D region 1 (columns 0..31)
-  const uint32_t tm1 = tslot + 32;  // D region 2 (columns 32..63)
-  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  const uint32_t dmine = tslot + ((uint32_t)(warp * 32) << 16) + 32u * mi;  // my lanes, my item's columns
+  const int arow0 = 64 * mi + lane;       // A row of slot 0 for my lane
+  const int arow1 = 64 * mi + 32 + lane;  // A row of slot 1
+  const int brow = 32 * mi + lane;        // B row of my item for my lane
   uint32_t parity = 0;
 
-  // one 3xTF32 group: operands are in place; MMA into `dt`, wait, fence
-  auto group = [&](uint32_t dt, const float* bhi, const float* blo) -> bool {
+  auto issue = [&]() {
     tc::fence_async_smem();
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    if (t == 96) tc::mma3(dt, Q.a_hi, Q.a_lo, bhi, blo, &mbar);
+    if (t == 0) tc::mma3(tslot, TL.a_hi, TL.a_lo, TL.b_hi, TL.b_lo, &mbar, tc::IDESC_M128_N64);
+  };
+  auto wait = [&]() -> bool {
     const bool mine = tc::mbar_wait(&mbar, parity);
     parity ^= 1;
     const bool ok = __syncthreads_and(mine) != 0;  // one verdict for the whole CTA
@@ -134,259 +174,276 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
 
   for (;;) {
     __syncthreads();
-    if (t == 0) s_item = atomicAdd(&w.counters[3], 1);
-    if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
+    if (t == 0) s_base = atomicAdd(&w.counters[3], 2);
     __syncthreads();
-    const int item = s_item;
-    if (item >= nitems || s_dead) break;
-    LayerItem it;
-    if (!layer_setup<N>(b, w, st, ssp_scat, S, item, it)) continue;
-    __syncthreads();
-    const int nd = it.nd;
-    int status = it.status;
-    if (nd == 0) {
-      layer_store<N>(w, item, S.m[0], S.m[1], S.lin);
-    } else {
-      // ---- FP64 thin layer -> FP32 masters and tiles (read all, then write: Q aliases S)
-      float col[32];
-      float linfac = (float)it.linfac;
-      if (warp == 0) {
-#pragma unroll
-        for (int r = 0; r < 32; r++) col[r] = (float)S.m[0][lane * LD + r];
-      } else if (warp == 1) {
-#pragma unroll
-        for (int r = 0; r < 32; r++) col[r] = (float)((r == lane ? 1.0 : 0.0) - S.m[1][lane * LD + r]);
-      } else if (warp == 2 && lane < 4) {
-        const double* src = (lane == 0) ? S.lin : (lane == 1) ? S.cst : (lane == 2) ? S.lin + n : S.cst + n;
-#pragma unroll
-        for (int r = 0; r < 32; r++) col[r] = (float)src[r];
-      }
+    const int base = s_base;
+    if (base >= nitems || s_dead) break;
+    // ---- FP64 set-up of both items (one at a time through the shared scratch)
+    for (int i = 0; i < 2; i++) {
+      const int item = base + i;
+      if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
       __syncthreads();
-      if (warp == 0) {
-        st_col(Q.rm, lane, col);
-        tc::put_row(Q.a_hi, Q.a_lo, lane, col);
-        tc::put_rows_from_cols(Q.br_hi, Q.br_lo, col);
-      } else if (warp == 1) {
-        st_col(Q.tm, lane, col);
-        tc::put_row(Q.a_hi, Q.a_lo, 32 + lane, col);
-        tc::put_rows_from_cols(Q.bt_hi, Q.bt_lo, col);
-      } else if (warp == 2 && lane < 4) {
-        float* dst = (lane == 0) ? Q.lp : (lane == 1) ? Q.cp : (lane == 2) ? Q.lmn : Q.cmn;
-#pragma unroll
-        for (int r = 0; r < 32; r++) dst[r] = col[r];
+      LayerItem it;
+      const bool valid = item < nitems && layer_setup<N>(b, w, st, ssp_scat, S, item, it);
+      if (valid && it.nd == 0) {
+        layer_store<N>(w, item, S.m[0], S.m[1], S.lin);
+      } else if (valid) {
+        TcItemState& D = Q.st[i];
+        for (int e = t; e < n * n; e += 128) {
+          const int cc = e >> 5, r = e & 31;
+          D.rm[cc * MS + r] = (float)S.m[0][cc * LD + r];
+          D.tm[cc * MS + r] = (float)((r == cc ? 1.0 : 0.0) - S.m[1][cc * LD + r]);
+        }
+        if (t < n) {
+          D.src[0][t] = (float)S.lin[t];
+          D.src[1][t] = (float)S.cst[t];
+          D.src[2][t] = (float)S.lin[n + t];
+          D.src[3][t] = (float)S.cst[n + t];
+        }
       }
-      __syncwarp();
-      if (warp == 2 && lane < 4) {  // v = [S- + f C-, C-, S+, C+]
-        float v[32];
-#pragma unroll
-        for (int r = 0; r < 32; r++)
-          v[r] = (lane == 0) ? Q.lmn[r] + linfac * Q.cmn[r] : (lane == 1) ? Q.cmn[r] : (lane == 2) ? Q.lp[r] : Q.cp[r];
-        st_col<32>(&Q.vv[0][0], lane, v);
-        tc::put_row(Q.a_hi, Q.a_lo, 64 + lane, v);
+      if (t == 0) {
+        s_valid[i] = valid;
+        s_nd[i] = valid ? it.nd : 0;
+        s_status[i] = valid ? it.status : 0;
+        s_linfac[i] = valid ? (float)it.linfac : 0.f;
+        s_c[i] = valid ? it.c : 0;
+        s_fi[i] = valid ? it.fi : 0;
       }
-      bool ok = true;
-      for (int itd = 0; itd < nd && ok; itd++) {
-        // ---- group 1: [R; T~; v] x R  ->  P = R R, R T~, R v
-        ok = group(tm0, Q.br_hi, Q.br_lo);
+      __syncthreads();  // the scratch is reused by the next set-up / the tiles
+    }
+    const int ndmax = max(s_nd[0], s_nd[1]);
+    const int my_nd = s_nd[mi];
+    float linfac = s_linfac[mi];
+    bool ok = true;
+    if (ndmax > 0) {
+      // operands of the first group: A slot 0 = R, slot 1 = T~, B = R; v
+      if (my_nd > 0) {
+        float c[32];
+        if (slot == 0) {
+          ld_col(my.rm, lane, c);
+          tc::put_row(TL.a_hi, TL.a_lo, arow0, c);
+          ld_row(my.rm, lane, c);
+          tc::put_row(TL.b_hi, TL.b_lo, brow, c);
+          my.vv[2][lane] = my.src[0][lane];
+          my.vv[3][lane] = my.src[1][lane];
+        } else {
+          ld_col(my.tm, lane, c);
+          tc::put_row(TL.a_hi, TL.a_lo, arow1, c);
+          my.vv[0][lane] = my.src[2][lane] + linfac * my.src[3][lane];
+          my.vv[1][lane] = my.src[3][lane];
+        }
+      }
+      for (int d = 0; d < ndmax; d++) {
+        const bool act = d < my_nd;
+        float dv[32], keep[32];
+        float m0 = 0.f, m1 = 0.f;
+        // ---- group 1: [R; T~] x R  ->  P = R R (slot 0), R T~ (slot 1); R v
+        issue();
+        if (act) matvec2(my.rm, my.vv[2 * slot], my.vv[2 * slot + 1], lane, m0, m1);
+        ok = wait();
         if (!ok) break;
-        float d[32];
-        if (warp == 0 || warp == 2) tc::tmem_ld32(tm0 + lane_base, d);
-        if (warp == 0) {
-          // X = P, G~ = X; row-sum norm of P (the lanes hold its columns)
-          float a[32];
+        if (act) {
+          tc::tmem_ld32(dmine, dv);
+          if (slot == 0) {
+            // u0 = S+ + R v0, u1 = C+ + R v1;  X = P and its column-sum norm
+            my.uv[0][lane] = my.src[0][lane] + m0;
+            my.uv[1][lane] = my.src[1][lane] + m1;
+            st_col(my.xm, lane, dv);
+            float s = 0.f;
 #pragma unroll
-          for (int r = 0; r < 32; r++) a[r] = fabsf(d[r]);
-          float rs = row_sum_scatter(a);
+            for (int r = 0; r < 32; r++) s += fabsf(dv[r]);
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) rs = fmaxf(rs, __shfl_xor_sync(0xffffffffu, rs, o));
-          if (lane == 0) Q.nrm = rs;
-          st_col(Q.xm, lane, d);
-          st_col(Q.gm, lane, d);
-          tc::put_rows_from_cols(Q.bx_hi, Q.bx_lo, d);
-        } else if (warp == 2 && lane < 4) {
-          // u = [S+ + Rv0, C+ + Rv1, v0 + Rv2, C- + Rv3]
-          float u[32];
+            for (int o = 16; o > 0; o >>= 1) s = fmaxf(s, __shfl_xor_sync(0xffffffffu, s, o));
+            if (lane == 0) my.nrm = s;
+          } else {
+            // u2 = v0 + R v2, u3 = C- + R v3;  V = R - R T~ (kept in registers)
+            my.uv[2][lane] = my.vv[0][lane] + m0;
+            my.uv[3][lane] = my.src[3][lane] + m1;
+            float rc[32];
+            ld_col(my.rm, lane, rc);
 #pragma unroll
-          for (int r = 0; r < 32; r++) {
-            const float base = (lane == 0) ? Q.lp[r] : (lane == 1) ? Q.cp[r] : (lane == 2) ? Q.vv[0][r] : Q.cmn[r];
-            u[r] = base + d[r];
+            for (int r = 0; r < 32; r++) keep[r] = rc[r] - dv[r];
           }
-          st_col<32>(&Q.uv[0][0], lane, u);
         }
         __syncthreads();
-        const float nrm = Q.nrm;
-        int steps = 0;  // 0: G~ = X; s > 0: s + 1 factors of the product, one MMA each
-        if (nrm < NEUMANN_MAX_NORM) {
-          float pw = nrm;  // nrm^(2^(steps+1) - 1)
-          float pk = nrm;  // nrm^(2^steps)
-          while (pw > NEUMANN_TOL && steps < 6) {
-            pk = pk * pk;
-            pw = pw * pk;
-            steps++;
+        // ---- G~ = (I - P)^-1 - I
+        const int stp0 = (d < s_nd[0]) ? series_steps(Q.st[0].nrm) : -2;
+        const int stp1 = (d < s_nd[1]) ? series_steps(Q.st[1].nrm) : -2;
+        for (int i = 0; i < 2; i++) {
+          if ((i == 0 ? stp0 : stp1) != -1) continue;
+          // ||P|| too large for the series: FP64 Gauss-Jordan on I - X (the tiles are free here)
+          double* M = reinterpret_cast<double*>(&TL);
+          InvScratch<32>& IS = *reinterpret_cast<InvScratch<32>*>(M + Team<32>::MAT);
+          TcItemState& D = Q.st[i];
+          for (int e = t; e < n * n; e += 128) {
+            const int cc = e >> 5, r = e & 31;
+            M[cc * Team<32>::LD + r] = (r == cc ? 1.0 : 0.0) - (double)D.xm[cc * MS + r];
           }
-        } else {
-          steps = -1;
+          __syncthreads();
+          if (ginv<32>(M, IS) && t == 0) s_status[i] |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+          for (int e = t; e < n * n; e += 128) {
+            const int cc = e >> 5, r = e & 31;
+            D.gm[cc * MS + r] = (float)(M[cc * Team<32>::LD + r] - (r == cc ? 1.0 : 0.0));
+          }
+          __syncthreads();
         }
-        if (steps > 0) {
-          // steps + 1 factors (I + X)(I + X^2)...: start from G~ = 0 with A = [X; 0]
-          if (warp == 0) {
-            ld_col(Q.xm, lane, d);
-            tc::put_row(Q.a_hi, Q.a_lo, lane, d);
-          } else if (warp == 1) {
-            float z[32];
+        const int mys = mi ? stp1 : stp0;
+        const int smax = max(stp0, stp1);
+        if (act && mys == 0 && slot == 1) {  // G~ = X
+          float x[32];
+          ld_col(my.xm, lane, x);
+          st_col(my.gm, lane, x);
+        }
+        if (smax > 0) {
+          // series operands: A slot 0 = X, slot 1 = G~ = 0, B = X
+          if (mys > 0) {
+            float c[32];
+            if (slot == 0) {
+              ld_col(my.xm, lane, c);
+              tc::put_row(TL.a_hi, TL.a_lo, arow0, c);
+              ld_row(my.xm, lane, c);
+              tc::put_row(TL.b_hi, TL.b_lo, brow, c);
+            } else {
 #pragma unroll
-            for (int r = 0; r < 32; r++) z[r] = 0.f;
-            st_col(Q.gm, lane, z);
-            tc::put_row(Q.a_hi, Q.a_lo, 32 + lane, z);
-          }
-          for (int k = 0; k <= steps && ok; k++) {
-            const bool last = (k == steps);
-            ok = group(tm1, Q.bx_hi, Q.bx_lo);  // [X; G~] x X -> X X, X G~
-            if (!ok) break;
-            float e[32];
-            if (warp < 2) tc::tmem_ld32(tm1 + lane_base, e);
-            if (warp == 1) {
-              float x[32], g[32];
-              ld_col(Q.xm, lane, x);
-              ld_col(Q.gm, lane, g);
-#pragma unroll
-              for (int r = 0; r < 32; r++) g[r] = g[r] + (x[r] + e[r]);
-              st_col(Q.gm, lane, g);
-              if (!last) tc::put_row(Q.a_hi, Q.a_lo, 32 + lane, g);
-              else tc::put_rows_from_cols(Q.bx_hi, Q.bx_lo, g);
+              for (int r = 0; r < 32; r++) c[r] = 0.f;
+              st_col(my.gm, lane, c);
+              tc::put_row(TL.a_hi, TL.a_lo, arow1, c);
             }
-            __syncthreads();  // X_k read before it is replaced
-            if (warp == 0 && !last) {
-              st_col(Q.xm, lane, e);
-              tc::put_row(Q.a_hi, Q.a_lo, lane, e);
-              tc::put_rows_from_cols(Q.bx_hi, Q.bx_lo, e);
+          }
+          for (int k = 0; k <= smax; k++) {
+            issue();
+            ok = wait();
+            if (!ok) break;
+            const bool on = mys > 0 && k <= mys;
+            const bool last = k == mys;
+            if (on) {
+              tc::tmem_ld32(dmine, dv);
+              if (slot == 1) {  // G~ += X + X G~
+                float x[32], g[32];
+                ld_col(my.xm, lane, x);
+                ld_col(my.gm, lane, g);
+#pragma unroll
+                for (int r = 0; r < 32; r++) g[r] = g[r] + (x[r] + dv[r]);
+                st_col(my.gm, lane, g);
+                if (!last) tc::put_row(TL.a_hi, TL.a_lo, arow1, g);
+              }
+            }
+            __syncthreads();  // X read before it is replaced
+            if (on && slot == 0 && !last) {  // X = X X
+              st_col(my.xm, lane, dv);
+              tc::put_row(TL.a_hi, TL.a_lo, arow0, dv);
+              __syncwarp();
+              ld_row(my.xm, lane, dv);
+              tc::put_row(TL.b_hi, TL.b_lo, brow, dv);
             }
           }
           if (!ok) break;
-        } else if (steps < 0) {
-          // ||R R|| too large for the series: FP64 Gauss-Jordan on I - X
-          double* M = reinterpret_cast<double*>(Q.a_hi);  // the A tiles are free here
-          InvScratch<32>& IS = *reinterpret_cast<InvScratch<32>*>(M + Team<32>::MAT);
-          for (int e2 = t; e2 < 1024; e2 += 128) {
-            const int cc = e2 >> 5, r = e2 & 31;
-            M[cc * Team<32>::LD + r] = (r == cc ? 1.0 : 0.0) - (double)Q.xm[cc * MS + r];
-          }
-          __syncthreads();
-          if (ginv<32>(M, IS)) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-          if (warp == 1) {
-            float g[32];
-#pragma unroll
-            for (int r = 0; r < 32; r++) g[r] = (float)(M[lane * Team<32>::LD + r] - (r == lane ? 1.0 : 0.0));
-            st_col(Q.gm, lane, g);
-            tc::put_rows_from_cols(Q.bx_hi, Q.bx_lo, g);
-          }
-          __syncthreads();  // M (in the A tiles) is read before group 2 operands go there
         }
-        // ---- group 2: [V; T~; u] x G~  ->  G~V, G~T~, G~u
-        if (warp == 1) {
-          float rt[32], r0[32];
-          tc::tmem_ld32(tm0 + lane_base, rt);  // R T~ (region 1 kept its group-1 result)
-          ld_col(Q.rm, lane, r0);
-#pragma unroll
-          for (int r = 0; r < 32; r++) r0[r] = r0[r] - rt[r];  // V = R - R T~
-          st_col(Q.xm, lane, r0);
-          tc::put_row(Q.a_hi, Q.a_lo, lane, r0);
-          ld_col(Q.tm, lane, rt);
-          tc::put_row(Q.a_hi, Q.a_lo, 32 + lane, rt);
-        } else if (warp == 2) {
-          float u[32];
-          if (lane < 4) {
-            ld_col<32>(&Q.uv[0][0], lane, u);
-            tc::put_row(Q.a_hi, Q.a_lo, 64 + lane, u);
+        __syncthreads();  // G~ complete
+        // ---- group 2: [T~; V] x G~  ->  G~ T~ (slot 0), G~ V (slot 1); G~ u
+        if (act) {
+          float c[32];
+          if (slot == 0) {
+            ld_col(my.tm, lane, c);
+            tc::put_row(TL.a_hi, TL.a_lo, arow0, c);
+          } else {
+            tc::put_row(TL.a_hi, TL.a_lo, arow1, keep);
+            ld_row(my.gm, lane, c);
+            tc::put_row(TL.b_hi, TL.b_lo, brow, c);
           }
         }
-        ok = group(tm0, Q.bx_hi, Q.bx_lo);
+        issue();
+        if (act) matvec2(my.gm, my.uv[2 * slot], my.uv[2 * slot + 1], lane, m0, m1);
+        ok = wait();
         if (!ok) break;
-        float keep[32];  // Y (warp 0), Z~ (warp 1), w (warp 2 lanes 0..3)
-        if (warp < 3) tc::tmem_ld32(tm0 + lane_base, d);
-        if (warp == 0) {
-          float v[32];
-          ld_col(Q.xm, lane, v);
+        if (act) {
+          // w = u + G~ u
+          my.wv[2 * slot][lane] = my.uv[2 * slot][lane] + m0;
+          my.wv[2 * slot + 1][lane] = my.uv[2 * slot + 1][lane] + m1;
+          tc::tmem_ld32(dmine, dv);
+          if (slot == 0) {  // Z~ = (T~ - G~) + G~ T~;  B = T~
+            float tt[32], g[32];
+            ld_col(my.tm, lane, tt);
+            ld_col(my.gm, lane, g);
 #pragma unroll
-          for (int r = 0; r < 32; r++) keep[r] = v[r] + d[r];  // Y = V + G~V
-          tc::put_row(Q.a_hi, Q.a_lo, lane, keep);
-        } else if (warp == 1) {
-          float tt[32], g[32];
-          ld_col(Q.tm, lane, tt);
-          ld_col(Q.gm, lane, g);
+            for (int r = 0; r < 32; r++) keep[r] = (tt[r] - g[r]) + dv[r];
+            tc::put_row(TL.a_hi, TL.a_lo, arow0, keep);
+            ld_row(my.tm, lane, tt);
+            tc::put_row(TL.b_hi, TL.b_lo, brow, tt);
+          } else {  // Y = V + G~ V
 #pragma unroll
-          for (int r = 0; r < 32; r++) keep[r] = (tt[r] - g[r]) + d[r];  // Z~ = T~ - G~ + G~T~
-          tc::put_row(Q.a_hi, Q.a_lo, 32 + lane, keep);
-        } else if (warp == 2 && lane < 4) {
-          float u[32];
-          ld_col<32>(&Q.uv[0][0], lane, u);
-#pragma unroll
-          for (int r = 0; r < 32; r++) keep[r] = u[r] + d[r];  // w = G u
-          tc::put_row(Q.a_hi, Q.a_lo, 64 + lane, keep);
-        }
-        // ---- group 3: [Y; Z~; w] x T~  ->  T~Y, T~Z~, T~w
-        ok = group(tm1, Q.bt_hi, Q.bt_lo);
-        if (!ok) break;
-        if (warp < 3) tc::tmem_ld32(tm1 + lane_base, d);
-        if (warp == 0) {
-          float r0[32];
-          ld_col(Q.rm, lane, r0);
-#pragma unroll
-          for (int r = 0; r < 32; r++) r0[r] = r0[r] + (keep[r] - d[r]);  // R' = R + Y - T~Y
-          st_col(Q.rm, lane, r0);
-          tc::put_row(Q.a_hi, Q.a_lo, lane, r0);
-          tc::put_rows_from_cols(Q.br_hi, Q.br_lo, r0);
-        } else if (warp == 1) {
-          float tt[32];
-          ld_col(Q.tm, lane, tt);
-#pragma unroll
-          for (int r = 0; r < 32; r++) tt[r] = tt[r] + (keep[r] - d[r]);  // T~' = T~ + Z~ - T~Z~
-          st_col(Q.tm, lane, tt);
-          tc::put_row(Q.a_hi, Q.a_lo, 32 + lane, tt);
-          tc::put_rows_from_cols(Q.bt_hi, Q.bt_lo, tt);
-        } else if (warp == 2 && lane < 4) {
-          // a = T w;  S+ = (S+ + a0) + f C+,  C+ += a1,  S- += a2,  C- += a3
-          float nv[32];
-#pragma unroll
-          for (int r = 0; r < 32; r++) {
-            const float a = keep[r] - d[r];
-            nv[r] = (lane == 0) ? (Q.lp[r] + a) + linfac * Q.cp[r]
-                  : (lane == 1) ? Q.cp[r] + a : (lane == 2) ? Q.lmn[r] + a : Q.cmn[r] + a;
+            for (int r = 0; r < 32; r++) keep[r] = keep[r] + dv[r];
+            tc::put_row(TL.a_hi, TL.a_lo, arow1, keep);
           }
-          __syncwarp(0xFu);
-          float* dst = (lane == 0) ? Q.lp : (lane == 1) ? Q.cp : (lane == 2) ? Q.lmn : Q.cmn;
+        }
+        // ---- group 3: [Z~; Y] x T~  ->  T~ Z~ (slot 0), T~ Y (slot 1); T~ w
+        issue();
+        if (act) matvec2(my.tm, my.wv[2 * slot], my.wv[2 * slot + 1], lane, m0, m1);
+        ok = wait();
+        if (!ok) break;
+        if (act) {
+          tc::tmem_ld32(dmine, dv);
+          // T w = w - T~ w for my two vectors
+          const float a0 = my.wv[2 * slot][lane] - m0, a1 = my.wv[2 * slot + 1][lane] - m1;
+          float c[32];
+          if (slot == 0) {
+            // T~' = T~ + (Z~ - T~ Z~) -> next A slot 1;  S+' = (S+ + a0) + f C+,  C+' = C+ + a1
+            ld_col(my.tm, lane, c);
 #pragma unroll
-          for (int r = 0; r < 32; r++) dst[r] = nv[r];
-          __syncwarp(0xFu);
-          const float f2 = 2.0f * linfac;
+            for (int r = 0; r < 32; r++) c[r] = c[r] + (keep[r] - dv[r]);
+            st_col(my.tm, lane, c);
+            tc::put_row(TL.a_hi, TL.a_lo, arow1, c);
+            const float sp = (my.src[0][lane] + a0) + linfac * my.src[1][lane];
+            const float cp = my.src[1][lane] + a1;
+            my.src[0][lane] = sp;
+            my.src[1][lane] = cp;
+            my.vv[2][lane] = sp;
+            my.vv[3][lane] = cp;
+          } else {
+            // R' = R + (Y - T~ Y) -> next A slot 0 and B;  S-' = S- + a2,  C-' = C- + a3
+            ld_col(my.rm, lane, c);
 #pragma unroll
-          for (int r = 0; r < 32; r++)
-            nv[r] = (lane == 0) ? Q.lmn[r] + f2 * Q.cmn[r] : (lane == 1) ? Q.cmn[r] : (lane == 2) ? Q.lp[r] : Q.cp[r];
-          st_col<32>(&Q.vv[0][0], lane, nv);
-          tc::put_row(Q.a_hi, Q.a_lo, 64 + lane, nv);
+            for (int r = 0; r < 32; r++) c[r] = c[r] + (keep[r] - dv[r]);
+            st_col(my.rm, lane, c);
+            tc::put_row(TL.a_hi, TL.a_lo, arow0, c);
+            __syncwarp();
+            ld_row(my.rm, lane, c);
+            tc::put_row(TL.b_hi, TL.b_lo, brow, c);
+            const float sm = my.src[2][lane] + a0;
+            const float cm = my.src[3][lane] + a1;
+            my.src[2][lane] = sm;
+            my.src[3][lane] = cm;
+            my.vv[0][lane] = sm + (2.0f * linfac) * cm;
+            my.vv[1][lane] = cm;
+          }
         }
         linfac = 2.0f * linfac;
       }
-      if (!ok) {
-        status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_TIMEOUT;
-        if (t == 0) s_dead = 1;
+      if (!ok && t == 0) {
+        s_dead = 1;
+        s_status[0] |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_TIMEOUT;
+        s_status[1] |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_TIMEOUT;
       }
       __syncthreads();
       // ---- layer R, T = I - T~, S+/S- in FP64
-      double* out = w.lay + (size_t)item * w.lay_stride;
-      for (int e2 = t; e2 < n * n; e2 += 128) {
-        const int cc = e2 >> 5, r = e2 & 31;
-        out[cc * LD + r] = (double)Q.rm[cc * MS + r];
-        out[MAT + cc * LD + r] = (r == cc ? 1.0 : 0.0) - (double)Q.tm[cc * MS + r];
-      }
-      if (t < 32) {
-        out[2 * MAT + t] = (double)Q.lp[t];
-        out[2 * MAT + n + t] = (double)Q.lmn[t];
+      for (int i = 0; i < 2; i++) {
+        if (s_nd[i] == 0) continue;
+        const TcItemState& D = Q.st[i];
+        double* out = w.lay + (size_t)(base + i) * w.lay_stride;
+        for (int e = t; e < n * n; e += 128) {
+          const int cc = e >> 5, r = e & 31;
+          out[cc * LD + r] = (double)D.rm[cc * MS + r];
+          out[MAT + cc * LD + r] = (r == cc ? 1.0 : 0.0) - (double)D.tm[cc * MS + r];
+        }
+        if (t < n) {
+          out[2 * MAT + t] = (double)D.src[0][t];
+          out[2 * MAT + n + t] = (double)D.src[2][t];
+        }
       }
     }
-    if (t == 0) {
-      w.lay_nd[item] = nd;
-      if (status) atomicOr(&w.status[(size_t)it.c * Fm + it.fi], status);
+    if (t < 2 && s_valid[t]) {
+      w.lay_nd[base + t] = s_nd[t];
+      if (s_status[t]) atomicOr(&w.status[(size_t)s_c[t] * Fm + s_fi[t]], s_status[t]);
     }
   }
   // a timed-out CTA lets its last MMA finish before the memory is released

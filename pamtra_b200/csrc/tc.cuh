@@ -27,8 +27,12 @@ namespace tc {
 
 constexpr int TILE_K = 32;               // K extent of every operand tile
 constexpr int RG_FLOATS = 256;           // floats per 8-row group of an A tile (8 chunks x 32)
-// instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = 32
-constexpr uint32_t IDESC_M128_N32 = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+// instruction descriptors: D = F32, A = B = TF32, both K-major, M = 128, N = 32 or 64
+constexpr uint32_t idesc_tf32(uint32_t m, uint32_t n) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+constexpr uint32_t IDESC_M128_N32 = idesc_tf32(128, 32);
+constexpr uint32_t IDESC_M128_N64 = idesc_tf32(128, 64);
 constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 24;  // bounded waits on MMA completion
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -58,7 +62,8 @@ __device__ __forceinline__ void split(float x, float& hi, float& lo) {
 }
 
 // D[tmem] (+)= A * B^T over K = 8 from the given descriptors (one thread)
-__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate,
+                                    uint32_t idesc = IDESC_M128_N32) {
   asm volatile(
       "{\n\t"
       ".reg .pred p;\n\t"
@@ -66,25 +71,25 @@ __device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uin
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
       "}\n"
       :
-      : "r"(d_tmem), "l"(a), "l"(b), "r"(IDESC_M128_N32), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      : "r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 
-// 3xTF32 product of a 128 x 32 A tile pair and a 32 x 32 B tile pair into
-// D = A * B^T (128 lanes x 32 columns, FP32).  Issued by one thread; completion is
-// signalled on `mbar` through tcgen05.commit.
+// 3xTF32 product of a 128 x 32 A tile pair and an N x 32 B tile pair into
+// D = A * B^T (128 lanes x N columns, FP32; N = 32 or 64 by `idesc`).  Issued
+// by one thread; completion is signalled on `mbar` through tcgen05.commit.
 __device__ __forceinline__ void mma3(uint32_t d_tmem, const float* a_hi, const float* a_lo, const float* b_hi,
-                                     const float* b_lo, uint64_t* mbar) {
+                                     const float* b_lo, uint64_t* mbar, uint32_t idesc = IDESC_M128_N32) {
   const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo), bh = smem_u32(b_hi), bl = smem_u32(b_lo);
   uint32_t acc = 0;
 #pragma unroll
   for (int s = 0; s < TILE_K / 8; s++) {
-    mma(d_tmem, desc_k(al + 256 * s), desc_k(bh + 256 * s), acc);
+    mma(d_tmem, desc_k(al + 256 * s), desc_k(bh + 256 * s), acc, idesc);
     acc = 1;
   }
 #pragma unroll
-  for (int s = 0; s < TILE_K / 8; s++) mma(d_tmem, desc_k(ah + 256 * s), desc_k(bl + 256 * s), 1);
+  for (int s = 0; s < TILE_K / 8; s++) mma(d_tmem, desc_k(ah + 256 * s), desc_k(bl + 256 * s), 1, idesc);
 #pragma unroll
-  for (int s = 0; s < TILE_K / 8; s++) mma(d_tmem, desc_k(ah + 256 * s), desc_k(bh + 256 * s), 1);
+  for (int s = 0; s < TILE_K / 8; s++) mma(d_tmem, desc_k(ah + 256 * s), desc_k(bh + 256 * s), 1, idesc);
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                :
                : "r"(smem_u32(mbar))

@@ -418,3 +418,20 @@ def test_split_precision_uneven(native):
     d = np.abs(s["tb"] - f64["tb"])
     assert np.max(d) <= SPLIT_TB_TOL
     assert np.all(d[nmu != 16] == 0.0)
+
+
+def test_split_precision_pairing_independent(native):
+    # The split-precision layer kernel carries two items per tensor-core MMA;
+    # each item's result depends on its own operands only, so a column gives
+    # bit-identical TBs when the items around it (and hence the pairs) change.
+    # Three frequencies make the per-column item count odd, so dropping the
+    # first column re-pairs every later item.
+    from pamtra_b200._native import PREC_3XTF32
+    freqs = [23.8, 31.4, 89.0]
+    b = pbatch.pack_pam(wl.c2_pam(9, seed=21), freqs)
+    full = _run_prec(b, PREC_3XTF32)
+    assert int(np.count_nonzero(full["status"])) == 0
+    sub = _run_prec(pbatch.subset(b, list(range(1, 9))), PREC_3XTF32)
+    assert np.array_equal(sub["tb"], full["tb"][1:])
+    again = _run_prec(b, PREC_3XTF32)
+    assert np.array_equal(again["tb"], full["tb"])
