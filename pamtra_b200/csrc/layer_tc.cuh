@@ -38,9 +38,11 @@ constexpr int MS = 36;  // column stride of the FP32 masters: quarter-warp float
 
 // FP32 state of one item of the pair (column-major masters, column c at [c * MS]).
 struct TcItemState {
-  float rm[32 * MS], tm[32 * MS], gm[32 * MS], xm[32 * MS];  // R, T~, G~, X
-  float src[4][32];                                          // S+ linear, S+ constant, S- linear, S- constant
-  float vv[4][32], uv[4][32], wv[4][32];                     // right-hand vectors of the three groups
+  float rm[32 * MS], tm[32 * MS], gm[32 * MS];  // R, T~, G~
+  float vm[32 * MS];                            // V = R T, then Y = G R T
+  float xa[32 * MS], xb[32 * MS];               // series powers X (ping-pong); Z~ in xa
+  float src[4][32];                             // S+ linear, S+ constant, S- linear, S- constant
+  float vv[4][32], uv[4][32], wv[4][32];        // right-hand vectors of the three groups
   float nrm;
   int pad_[3];
 };
@@ -83,10 +85,28 @@ __device__ __forceinline__ void st_col(float* m, int col, const float (&v)[32]) 
 #pragma unroll
   for (int r = 0; r < 32; r += 4) *reinterpret_cast<float4*>(m + col * S + r) = make_float4(v[r], v[r + 1], v[r + 2], v[r + 3]);
 }
-// row `row` of a master (lanes read consecutive words: conflict-free)
-__device__ __forceinline__ void ld_row(const float* m, int row, float (&v)[32]) {
+
+// Operands of one group for the calling thread: A row `arow` from column
+// `lane` of master `asrc`, and K-chunks 4h..4h+3 of B row `brow` (row `lane`
+// of master `bsrc`, read down its columns: conflict-free), split into TF32
+// hi / lo pairs.  The two warps of an item cover the B row's two halves.
+__device__ __forceinline__ void build_operands(TcTiles& TL, const float* asrc, const float* bsrc, int arow,
+                                               int brow, int h, int lane) {
+  float c[32];
+  ld_col(asrc, lane, c);
+  tc::put_row(TL.a_hi, TL.a_lo, arow, c);
 #pragma unroll
-  for (int k = 0; k < 32; k++) v[k] = m[k * MS + row];
+  for (int q = 0; q < 4; q++) {
+    const int k0 = 16 * h + 4 * q;
+    float4 hi, lo;
+    tc::split(bsrc[(k0 + 0) * MS + lane], hi.x, lo.x);
+    tc::split(bsrc[(k0 + 1) * MS + lane], hi.y, lo.y);
+    tc::split(bsrc[(k0 + 2) * MS + lane], hi.z, lo.z);
+    tc::split(bsrc[(k0 + 3) * MS + lane], hi.w, lo.w);
+    const int o = (brow >> 3) * tc::RG_FLOATS + (k0 >> 2) * 32 + (brow & 7) * 4;
+    *reinterpret_cast<float4*>(TL.b_hi + o) = hi;
+    *reinterpret_cast<float4*>(TL.b_lo + o) = lo;
+  }
 }
 
 // (M x0)[r] and (M x1)[r] for a master M (k-ascending FMA chains)
@@ -127,6 +147,7 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
                                                      double* __restrict__ ssp_scat) {
   static_assert(N == 16, "the split-precision layer kernel is built for NUMMU = 16");
   constexpr int n = 32, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT;
+  enum { G1 = 0, SER = 1, G2 = 2, G3 = 3 };
   extern __shared__ __align__(1024) double smem_raw[];
   TcPairSmem& Q = *reinterpret_cast<TcPairSmem*>(smem_raw);
   LayerSmem<N>& S = Q.u.setup;
@@ -152,25 +173,9 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t dmine = tslot + ((uint32_t)(warp * 32) << 16) + 32u * mi;  // my lanes, my item's columns
-  const int arow0 = 64 * mi + lane;       // A row of slot 0 for my lane
-  const int arow1 = 64 * mi + 32 + lane;  // A row of slot 1
-  const int brow = 32 * mi + lane;        // B row of my item for my lane
+  const int arow = 32 * warp + lane;  // A row = D lane of this thread
+  const int brow = 32 * mi + lane;    // B row of my item for my lane
   uint32_t parity = 0;
-
-  auto issue = [&]() {
-    tc::fence_async_smem();
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    if (t == 0) tc::mma3(tslot, TL.a_hi, TL.a_lo, TL.b_hi, TL.b_lo, &mbar, tc::IDESC_M128_N64);
-  };
-  auto wait = [&]() -> bool {
-    const bool mine = tc::mbar_wait(&mbar, parity);
-    parity ^= 1;
-    const bool ok = __syncthreads_and(mine) != 0;  // one verdict for the whole CTA
-    tc::fence_after_sync();
-    return ok;
-  };
 
   for (;;) {
     __syncthreads();
@@ -216,208 +221,181 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
     float linfac = s_linfac[mi];
     bool ok = true;
     if (ndmax > 0) {
-      // operands of the first group: A slot 0 = R, slot 1 = T~, B = R; v
-      if (my_nd > 0) {
-        float c[32];
+      if (my_nd > 0) {  // v = [S- + f C-, C-, S+, C+]
         if (slot == 0) {
-          ld_col(my.rm, lane, c);
-          tc::put_row(TL.a_hi, TL.a_lo, arow0, c);
-          ld_row(my.rm, lane, c);
-          tc::put_row(TL.b_hi, TL.b_lo, brow, c);
           my.vv[2][lane] = my.src[0][lane];
           my.vv[3][lane] = my.src[1][lane];
         } else {
-          ld_col(my.tm, lane, c);
-          tc::put_row(TL.a_hi, TL.a_lo, arow1, c);
           my.vv[0][lane] = my.src[2][lane] + linfac * my.src[3][lane];
           my.vv[1][lane] = my.src[3][lane];
         }
       }
-      for (int d = 0; d < ndmax; d++) {
+      // One MMA group per pass: operands, MMA (with the source mat-vec on the
+      // CUDA cores meanwhile), epilogue into the masters, barrier, next phase.
+      //   G1  [R; T~] x R   -> slot 0: P = R R  -> X;       slot 1: R T~ -> V = R - R T~
+      //   SER [X; G~] x X   -> slot 0: X X      -> X next;  slot 1: X G~ -> G~ += X + X G~
+      //   G2  [T~; V] x G~  -> slot 0: G~ T~    -> Z~;      slot 1: G~ V -> Y = V + G~ V
+      //   G3  [Z~; Y] x T~  -> slot 0: T~ Z~    -> T~';     slot 1: T~ Y -> R'
+      int phase = G1, d = 0, k = 0, mys = 0, smax = 0, xsel = 0;
+      for (;;) {
         const bool act = d < my_nd;
-        float dv[32], keep[32];
-        float m0 = 0.f, m1 = 0.f;
-        // ---- group 1: [R; T~] x R  ->  P = R R (slot 0), R T~ (slot 1); R v
-        issue();
-        if (act) matvec2(my.rm, my.vv[2 * slot], my.vv[2 * slot + 1], lane, m0, m1);
-        ok = wait();
-        if (!ok) break;
-        if (act) {
-          tc::tmem_ld32(dmine, dv);
-          if (slot == 0) {
-            // u0 = S+ + R v0, u1 = C+ + R v1;  X = P and its column-sum norm
-            my.uv[0][lane] = my.src[0][lane] + m0;
-            my.uv[1][lane] = my.src[1][lane] + m1;
-            st_col(my.xm, lane, dv);
-            float s = 0.f;
-#pragma unroll
-            for (int r = 0; r < 32; r++) s += fabsf(dv[r]);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) s = fmaxf(s, __shfl_xor_sync(0xffffffffu, s, o));
-            if (lane == 0) my.nrm = s;
-          } else {
-            // u2 = v0 + R v2, u3 = C- + R v3;  V = R - R T~ (kept in registers)
-            my.uv[2][lane] = my.vv[0][lane] + m0;
-            my.uv[3][lane] = my.src[3][lane] + m1;
-            float rc[32];
-            ld_col(my.rm, lane, rc);
-#pragma unroll
-            for (int r = 0; r < 32; r++) keep[r] = rc[r] - dv[r];
-          }
+        const bool on = (phase == SER) ? (mys > 0 && k <= mys) : act;
+        float* xc = xsel ? my.xb : my.xa;  // current series power
+        float* xn = xsel ? my.xa : my.xb;
+        if (on) {
+          const float* asrc;
+          const float* bsrc;
+          if (phase == G1) { asrc = slot ? my.tm : my.rm; bsrc = my.rm; }
+          else if (phase == SER) { asrc = slot ? my.gm : xc; bsrc = xc; }
+          else if (phase == G2) { asrc = slot ? my.vm : my.tm; bsrc = my.gm; }
+          else { asrc = slot ? my.vm : my.xa; bsrc = my.tm; }
+          build_operands(TL, asrc, bsrc, arow, brow, slot, lane);
         }
+        tc::fence_async_smem();
+        tc::fence_before_sync();
         __syncthreads();
-        // ---- G~ = (I - P)^-1 - I
-        const int stp0 = (d < s_nd[0]) ? series_steps(Q.st[0].nrm) : -2;
-        const int stp1 = (d < s_nd[1]) ? series_steps(Q.st[1].nrm) : -2;
-        for (int i = 0; i < 2; i++) {
-          if ((i == 0 ? stp0 : stp1) != -1) continue;
-          // ||P|| too large for the series: FP64 Gauss-Jordan on I - X (the tiles are free here)
-          double* M = reinterpret_cast<double*>(&TL);
-          InvScratch<32>& IS = *reinterpret_cast<InvScratch<32>*>(M + Team<32>::MAT);
-          TcItemState& D = Q.st[i];
-          for (int e = t; e < n * n; e += 128) {
-            const int cc = e >> 5, r = e & 31;
-            M[cc * Team<32>::LD + r] = (r == cc ? 1.0 : 0.0) - (double)D.xm[cc * MS + r];
-          }
-          __syncthreads();
-          if (ginv<32>(M, IS) && t == 0) s_status[i] |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-          for (int e = t; e < n * n; e += 128) {
-            const int cc = e >> 5, r = e & 31;
-            D.gm[cc * MS + r] = (float)(M[cc * Team<32>::LD + r] - (r == cc ? 1.0 : 0.0));
-          }
-          __syncthreads();
+        tc::fence_after_sync();
+        if (t == 0) tc::mma3(tslot, TL.a_hi, TL.a_lo, TL.b_hi, TL.b_lo, &mbar, tc::IDESC_M128_N64);
+        float m0 = 0.f, m1 = 0.f;
+        if (on && phase != SER) {
+          const float* mv = (phase == G1) ? my.rm : (phase == G2) ? my.gm : my.tm;
+          const float(*x)[32] = (phase == G1) ? my.vv : (phase == G2) ? my.uv : my.wv;
+          matvec2(mv, x[2 * slot], x[2 * slot + 1], lane, m0, m1);
         }
-        const int mys = mi ? stp1 : stp0;
-        const int smax = max(stp0, stp1);
-        if (act && mys == 0 && slot == 1) {  // G~ = X
-          float x[32];
-          ld_col(my.xm, lane, x);
-          st_col(my.gm, lane, x);
+        {
+          const bool mine = tc::mbar_wait(&mbar, parity);
+          parity ^= 1;
+          ok = __syncthreads_and(mine) != 0;  // one verdict for the whole CTA
+          tc::fence_after_sync();
         }
-        if (smax > 0) {
-          // series operands: A slot 0 = X, slot 1 = G~ = 0, B = X
-          if (mys > 0) {
-            float c[32];
+        if (!ok) break;
+        if (on) {
+          float dv[32], a[32];
+          tc::tmem_ld32(dmine, dv);
+          if (phase == G1) {
+            if (slot == 0) {  // X = P, its column-sum norm;  u0 = S+ + R v0, u1 = C+ + R v1
+              my.uv[0][lane] = my.src[0][lane] + m0;
+              my.uv[1][lane] = my.src[1][lane] + m1;
+              st_col(my.xa, lane, dv);
+              float sn = 0.f;
+#pragma unroll
+              for (int r = 0; r < 32; r++) sn += fabsf(dv[r]);
+#pragma unroll
+              for (int o = 16; o > 0; o >>= 1) sn = fmaxf(sn, __shfl_xor_sync(0xffffffffu, sn, o));
+              if (lane == 0) my.nrm = sn;
+            } else {  // V = R - R T~;  u2 = v0 + R v2, u3 = C- + R v3
+              my.uv[2][lane] = my.vv[0][lane] + m0;
+              my.uv[3][lane] = my.src[3][lane] + m1;
+              ld_col(my.rm, lane, a);
+#pragma unroll
+              for (int r = 0; r < 32; r++) a[r] = a[r] - dv[r];
+              st_col(my.vm, lane, a);
+            }
+          } else if (phase == SER) {
             if (slot == 0) {
-              ld_col(my.xm, lane, c);
-              tc::put_row(TL.a_hi, TL.a_lo, arow0, c);
-              ld_row(my.xm, lane, c);
-              tc::put_row(TL.b_hi, TL.b_lo, brow, c);
-            } else {
+              if (k < mys) st_col(xn, lane, dv);  // X = X X
+            } else {  // G~ += X + X G~
+              float g[32];
+              ld_col(xc, lane, a);
+              ld_col(my.gm, lane, g);
 #pragma unroll
-              for (int r = 0; r < 32; r++) c[r] = 0.f;
-              st_col(my.gm, lane, c);
-              tc::put_row(TL.a_hi, TL.a_lo, arow1, c);
+              for (int r = 0; r < 32; r++) g[r] = g[r] + (a[r] + dv[r]);
+              st_col(my.gm, lane, g);
             }
-          }
-          for (int k = 0; k <= smax; k++) {
-            issue();
-            ok = wait();
-            if (!ok) break;
-            const bool on = mys > 0 && k <= mys;
-            const bool last = k == mys;
-            if (on) {
-              tc::tmem_ld32(dmine, dv);
-              if (slot == 1) {  // G~ += X + X G~
-                float x[32], g[32];
-                ld_col(my.xm, lane, x);
-                ld_col(my.gm, lane, g);
+          } else if (phase == G2) {
+            // w = u + G~ u
+            my.wv[2 * slot][lane] = my.uv[2 * slot][lane] + m0;
+            my.wv[2 * slot + 1][lane] = my.uv[2 * slot + 1][lane] + m1;
+            if (slot == 0) {  // Z~ = (T~ - G~) + G~ T~
+              float g[32];
+              ld_col(my.tm, lane, a);
+              ld_col(my.gm, lane, g);
 #pragma unroll
-                for (int r = 0; r < 32; r++) g[r] = g[r] + (x[r] + dv[r]);
-                st_col(my.gm, lane, g);
-                if (!last) tc::put_row(TL.a_hi, TL.a_lo, arow1, g);
-              }
+              for (int r = 0; r < 32; r++) a[r] = (a[r] - g[r]) + dv[r];
+              st_col(my.xa, lane, a);
+            } else {  // Y = V + G~ V
+              ld_col(my.vm, lane, a);
+#pragma unroll
+              for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
+              st_col(my.vm, lane, a);
             }
-            __syncthreads();  // X read before it is replaced
-            if (on && slot == 0 && !last) {  // X = X X
-              st_col(my.xm, lane, dv);
-              tc::put_row(TL.a_hi, TL.a_lo, arow0, dv);
-              __syncwarp();
-              ld_row(my.xm, lane, dv);
-              tc::put_row(TL.b_hi, TL.b_lo, brow, dv);
-            }
-          }
-          if (!ok) break;
-        }
-        __syncthreads();  // G~ complete
-        // ---- group 2: [T~; V] x G~  ->  G~ T~ (slot 0), G~ V (slot 1); G~ u
-        if (act) {
-          float c[32];
-          if (slot == 0) {
-            ld_col(my.tm, lane, c);
-            tc::put_row(TL.a_hi, TL.a_lo, arow0, c);
           } else {
-            tc::put_row(TL.a_hi, TL.a_lo, arow1, keep);
-            ld_row(my.gm, lane, c);
-            tc::put_row(TL.b_hi, TL.b_lo, brow, c);
+            // T w = w - T~ w for my two vectors
+            const float a0 = my.wv[2 * slot][lane] - m0, a1 = my.wv[2 * slot + 1][lane] - m1;
+            float z[32];
+            if (slot == 0) {  // T~' = T~ + (Z~ - T~ Z~);  S+' = (S+ + a0) + f C+,  C+' = C+ + a1
+              ld_col(my.tm, lane, a);
+              ld_col(my.xa, lane, z);
+#pragma unroll
+              for (int r = 0; r < 32; r++) a[r] = a[r] + (z[r] - dv[r]);
+              st_col(my.tm, lane, a);
+              const float sp = (my.src[0][lane] + a0) + linfac * my.src[1][lane];
+              const float cp = my.src[1][lane] + a1;
+              my.src[0][lane] = sp;
+              my.src[1][lane] = cp;
+              my.vv[2][lane] = sp;
+              my.vv[3][lane] = cp;
+            } else {  // R' = R + (Y - T~ Y);  S-' = S- + a2,  C-' = C- + a3
+              ld_col(my.rm, lane, a);
+              ld_col(my.vm, lane, z);
+#pragma unroll
+              for (int r = 0; r < 32; r++) a[r] = a[r] + (z[r] - dv[r]);
+              st_col(my.rm, lane, a);
+              const float sm = my.src[2][lane] + a0;
+              const float cm = my.src[3][lane] + a1;
+              my.src[2][lane] = sm;
+              my.src[3][lane] = cm;
+              my.vv[0][lane] = sm + (2.0f * linfac) * cm;
+              my.vv[1][lane] = cm;
+            }
           }
         }
-        issue();
-        if (act) matvec2(my.gm, my.uv[2 * slot], my.uv[2 * slot + 1], lane, m0, m1);
-        ok = wait();
-        if (!ok) break;
-        if (act) {
-          // w = u + G~ u
-          my.wv[2 * slot][lane] = my.uv[2 * slot][lane] + m0;
-          my.wv[2 * slot + 1][lane] = my.uv[2 * slot + 1][lane] + m1;
-          tc::tmem_ld32(dmine, dv);
-          if (slot == 0) {  // Z~ = (T~ - G~) + G~ T~;  B = T~
-            float tt[32], g[32];
-            ld_col(my.tm, lane, tt);
-            ld_col(my.gm, lane, g);
-#pragma unroll
-            for (int r = 0; r < 32; r++) keep[r] = (tt[r] - g[r]) + dv[r];
-            tc::put_row(TL.a_hi, TL.a_lo, arow0, keep);
-            ld_row(my.tm, lane, tt);
-            tc::put_row(TL.b_hi, TL.b_lo, brow, tt);
-          } else {  // Y = V + G~ V
-#pragma unroll
-            for (int r = 0; r < 32; r++) keep[r] = keep[r] + dv[r];
-            tc::put_row(TL.a_hi, TL.a_lo, arow1, keep);
+        __syncthreads();  // masters complete before the next operands are built
+        // ---- next phase
+        if (phase == G1) {
+          const int stp0 = (d < s_nd[0]) ? series_steps(Q.st[0].nrm) : -2;
+          const int stp1 = (d < s_nd[1]) ? series_steps(Q.st[1].nrm) : -2;
+          for (int i = 0; i < 2; i++) {
+            if ((i == 0 ? stp0 : stp1) != -1) continue;
+            // ||P|| too large for the series: FP64 Gauss-Jordan on I - X (the tiles are free here)
+            double* M = reinterpret_cast<double*>(&TL);
+            InvScratch<32>& IS = *reinterpret_cast<InvScratch<32>*>(M + Team<32>::MAT);
+            TcItemState& D = Q.st[i];
+            for (int e = t; e < n * n; e += 128) {
+              const int cc = e >> 5, r = e & 31;
+              M[cc * Team<32>::LD + r] = (r == cc ? 1.0 : 0.0) - (double)D.xa[cc * MS + r];
+            }
+            __syncthreads();
+            if (ginv<32>(M, IS) && t == 0) s_status[i] |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+            for (int e = t; e < n * n; e += 128) {
+              const int cc = e >> 5, r = e & 31;
+              D.gm[cc * MS + r] = (float)(M[cc * Team<32>::LD + r] - (r == cc ? 1.0 : 0.0));
+            }
+            __syncthreads();
           }
-        }
-        // ---- group 3: [Z~; Y] x T~  ->  T~ Z~ (slot 0), T~ Y (slot 1); T~ w
-        issue();
-        if (act) matvec2(my.tm, my.wv[2 * slot], my.wv[2 * slot + 1], lane, m0, m1);
-        ok = wait();
-        if (!ok) break;
-        if (act) {
-          tc::tmem_ld32(dmine, dv);
-          // T w = w - T~ w for my two vectors
-          const float a0 = my.wv[2 * slot][lane] - m0, a1 = my.wv[2 * slot + 1][lane] - m1;
-          float c[32];
-          if (slot == 0) {
-            // T~' = T~ + (Z~ - T~ Z~) -> next A slot 1;  S+' = (S+ + a0) + f C+,  C+' = C+ + a1
-            ld_col(my.tm, lane, c);
+          mys = mi ? stp1 : stp0;
+          smax = max(stp0, stp1);
+          if (slot == 1 && mys >= 0) {  // G~ = X (no series), or G~ = 0 to start one
+            float g[32];
+            if (mys == 0) ld_col(my.xa, lane, g);
 #pragma unroll
-            for (int r = 0; r < 32; r++) c[r] = c[r] + (keep[r] - dv[r]);
-            st_col(my.tm, lane, c);
-            tc::put_row(TL.a_hi, TL.a_lo, arow1, c);
-            const float sp = (my.src[0][lane] + a0) + linfac * my.src[1][lane];
-            const float cp = my.src[1][lane] + a1;
-            my.src[0][lane] = sp;
-            my.src[1][lane] = cp;
-            my.vv[2][lane] = sp;
-            my.vv[3][lane] = cp;
-          } else {
-            // R' = R + (Y - T~ Y) -> next A slot 0 and B;  S-' = S- + a2,  C-' = C- + a3
-            ld_col(my.rm, lane, c);
-#pragma unroll
-            for (int r = 0; r < 32; r++) c[r] = c[r] + (keep[r] - dv[r]);
-            st_col(my.rm, lane, c);
-            tc::put_row(TL.a_hi, TL.a_lo, arow0, c);
-            __syncwarp();
-            ld_row(my.rm, lane, c);
-            tc::put_row(TL.b_hi, TL.b_lo, brow, c);
-            const float sm = my.src[2][lane] + a0;
-            const float cm = my.src[3][lane] + a1;
-            my.src[2][lane] = sm;
-            my.src[3][lane] = cm;
-            my.vv[0][lane] = sm + (2.0f * linfac) * cm;
-            my.vv[1][lane] = cm;
+            for (int r = 0; r < 32; r++) g[r] = (mys == 0) ? g[r] : 0.f;
+            st_col(my.gm, lane, g);
           }
+          __syncthreads();
+          k = 0;
+          xsel = 0;
+          phase = (smax > 0) ? SER : G2;
+        } else if (phase == SER) {
+          xsel ^= 1;
+          if (++k > smax) phase = G2;
+        } else if (phase == G2) {
+          phase = G3;
+        } else {
+          linfac = 2.0f * linfac;
+          if (++d >= ndmax) break;
+          phase = G1;
         }
-        linfac = 2.0f * linfac;
       }
       if (!ok && t == 0) {
         s_dead = 1;

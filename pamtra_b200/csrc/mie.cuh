@@ -256,16 +256,25 @@ __global__ void __launch_bounds__(32 * MIE_WARPS) k_mie(Batch b, Work w, pamtra_
       for (int i = lane; i < nquad; i += 32) { S.sump[0][i] = 0; S.sump[1][i] = 0; S.sump[2][i] = 0; S.sump[3][i] = 0; }
       __syncwarp();
       double sqe = 0.0, sqs = 0.0, sqb = 0.0;
-      for (int c0 = 0; c0 < nb; c0 += 32) {
-        const int ir = c0 + lane;
+      // Bins in passes of `chunk` bins with R = 32 / chunk lanes per bin:
+      // full passes of 32 bins, then the remainder split into powers of two
+      // (40 bins = 32 + 8: the 8-bin pass gives each bin 4 lanes, which share
+      // its angles), so every pass keeps all lanes busy.  Lane r of a bin
+      // takes angles i0 + g R + r; the bin sums reduce over lanes with the
+      // same r.
+      for (int c0 = 0; c0 < nb;) {
+        const int rem = nb - c0;
+        const int chunk = rem >= 32 ? 32 : (1 << (31 - __clz(rem)));
+        const int R = 32 / chunk;
+        const int r = lane & (R - 1);
+        const int ir = c0 + lane / R;
+        c0 += chunk;
         bool act = false;
         double wgt = 0.0, ndens = 0.0, deld = 0.0;
         int nm = 0;
-        if (ir < nb) {
-          deld = bdd[ir];
-          ndens = bnd[ir] / deld;
-          act = ndens > 0;
-        }
+        deld = bdd[ir];
+        ndens = bnd[ir] / deld;
+        act = ndens > 0;
         if (act) {
           double rho, dia;
           dens_diam(ir, rho, dia);
@@ -275,25 +284,30 @@ __global__ void __launch_bounds__(32 * MIE_WARPS) k_mie(Batch b, Work w, pamtra_
           if (nmie + 1 > NT_MAX) { nmie = NT_MAX - 1; status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE; }
           double qe, qs, qb;
           miecalc_cross(nmie, x, ms, ab, bb, qe, qs, qb);
-          const double r2 = (dia / 2.0) * (dia / 2.0);
-          qe = qe * r2 * PI;
-          qs = qs * r2 * PI;
-          qb = qb * r2 * PI;
-          qe = qe * ndens;
-          qs = qs * ndens;
-          qb = qb * ndens;
-          sqe = sqe + qe * deld;
-          sqs = sqs + qs * deld;
-          sqb = sqb + qb * deld;
+          if (r == 0) {
+            const double r2 = (dia / 2.0) * (dia / 2.0);
+            qe = qe * r2 * PI;
+            qs = qs * r2 * PI;
+            qb = qb * r2 * PI;
+            qe = qe * ndens;
+            qs = qs * ndens;
+            qb = qb * ndens;
+            sqe = sqe + qe * deld;
+            sqs = sqs + qs * deld;
+            sqb = sqb + qb * deld;
+          }
           nm = min(nmie, nterms);
           wgt = ndens;
         }
-        for (int i0 = 0; i0 < nquad; i0 += ANG_G) {
+        for (int i0 = 0; i0 < nquad; i0 += ANG_G * R) {
           double pp[ANG_G][4];
           if (act) {
             double mu[ANG_G];
 #pragma unroll
-            for (int g = 0; g < ANG_G; g++) mu[g] = (i0 + g < nquad) ? gx[i0 + g] : 0.0;
+            for (int g = 0; g < ANG_G; g++) {
+              const int i = i0 + g * R + r;
+              mu[g] = (i < nquad) ? gx[i] : 0.0;
+            }
             mieangle_group(nm, ab, bb, mu, pp);
 #pragma unroll
             for (int g = 0; g < ANG_G; g++)
@@ -307,10 +321,11 @@ __global__ void __launch_bounds__(32 * MIE_WARPS) k_mie(Batch b, Work w, pamtra_
           }
 #pragma unroll
           for (int g = 0; g < ANG_G; g++) {
-            const int i = i0 + g;
 #pragma unroll
-            for (int k = 0; k < 4; k++) pp[g][k] = warp_sum(pp[g][k]);
-            if (i < nquad && lane == (i & 31)) {
+            for (int k = 0; k < 4; k++)
+              for (int o = 16; o >= R; o >>= 1) pp[g][k] += __shfl_xor_sync(0xffffffffu, pp[g][k], o);
+            const int i = i0 + g * R + r;
+            if (i < nquad && lane < R) {
 #pragma unroll
               for (int k = 0; k < 4; k++) S.sump[k][i] += pp[g][k];
             }
