@@ -229,9 +229,11 @@ def _target_shape(args, local, eng, stream):
     from pamtra_b200 import batch as pbatch
     from pamtra_b200.workloads import target_batch
     dev = torch.device("cuda", local)
+    from pamtra_b200 import autotune
     b = target_batch(args.target_cols, seed=4)
     out = b.alloc_outputs(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    autotune.tune(b, local, eng=eng, stream=stream, outputs=out)
     with torch.cuda.stream(stream):
         for _ in range(2):
             pbatch.run(b, local, out, stream=stream, eng=eng)
@@ -250,7 +252,9 @@ def _target_shape(args, local, eng, stream):
     st_bad = int((out["status"] != 0).sum())
     from pamtra_b200._native import PREC_3XTF32
     sout = b.alloc_outputs(dev)
+    autotune.tune(b, local, precision=PREC_3XTF32, eng=eng, stream=stream, outputs=sout)
     sms_, sstages = _timed_steps(b, local, eng, stream, sout, PREC_3XTF32, 3, 2, flush)
+    eng.set_launch(autotune.DEFAULT)
     split = b.n_solves() / (np.mean(sms_) * 1e-3)
     split_err = float((sout["tb"] - out["tb"]).abs().max().item())
     singles = [pbatch.subset(b, [c]) for c in range(16)]
@@ -371,12 +375,15 @@ def main():
     from pamtra_b200 import build as pbuild
     from pamtra_b200._native import Engine
     from pamtra_b200.workloads import c2_pam
+    from pamtra_b200 import autotune
     pbuild.build()
     eng = Engine(local)
     b = pbatch.pack_pam(c2_pam(args.ncol, seed=2 + rank), FREQS)
     stream = torch.cuda.Stream(dev)
     out = b.alloc_outputs(dev, ssp=True)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    # launch shapes of the persistent kernels, tuned on this batch (untimed)
+    shape64, tune64 = autotune.tune(b, local, eng=eng, stream=stream, outputs=out)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             pbatch.run(b, local, out, stream=stream, eng=eng)
@@ -414,6 +421,25 @@ def main():
         t_total = float(tt.item())
     solves_step = b.n_solves()
     value = world * solves_step * args.steps / t_total
+    # ---- the same step replayed from a captured CUDA graph
+    graph, gout = pbatch.capture(b, local, stream=stream, eng=eng)
+    for _ in range(args.warmup):
+        graph.launch(stream)
+    stream.synchronize()
+    g_ms = []
+    for _ in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            graph.launch(stream)
+            e.record(stream)
+        e.synchronize()
+        g_ms.append(s.elapsed_time(e))
+    graph_same = bool(np.array_equal(gout["tb"].cpu().numpy(), out["tb"].cpu().numpy()))
+    graph.close()
+    del gout
+    graph_value = world * solves_step / (np.mean(g_ms) * 1e-3)
     # ---- end-to-end through the C ABI with host buffers
     hout = b.alloc_outputs(None, pinned=True)
     pbatch.run_host(b, local, hout, eng=eng)
@@ -432,7 +458,9 @@ def main():
     # ---- split-precision batched form (3xTF32 tcgen05 doubling) on the same columns
     from pamtra_b200._native import PREC_3XTF32
     sout = b.alloc_outputs(dev)
+    shape_s, _ = autotune.tune(b, local, precision=PREC_3XTF32, eng=eng, stream=stream, outputs=sout)
     sms_, sstages = _timed_steps(b, local, eng, stream, sout, PREC_3XTF32, args.steps, args.warmup, flush)
+    eng.set_launch(shape64)
     split_value = world * solves_step / (np.mean(sms_) * 1e-3)
     tb_split = sout["tb"].cpu().numpy()
     split_err_f64 = float(np.max(np.abs(tb_split - out["tb"].cpu().numpy())))
@@ -504,6 +532,13 @@ def main():
         "cpu_baseline": cpu,
         "clocks": clocks,
         "plain_fp64": {"value": plain_value, "unit": "solves/s", "form": "one column per call, FP64"},
+        "graph_replay": {"value": graph_value, "unit": "solves/s", "ms_per_step": float(np.mean(g_ms)),
+                         "tb_equals_direct": graph_same,
+                         "form": "the batched FP64 step captured once as a CUDA graph and replayed"},
+        "launch_shape": {"fp64": list(shape64), "split_3xtf32": list(shape_s),
+                         "fields": "mie warps/CTA, mie CTAs/SM, layer CTAs/SM, adding CTAs/SM (0 = as many as fit)",
+                         "stage_ms_per_candidate_fp64": tune64,
+                         "candidates": [list(c) for c in autotune.CANDIDATES]},
         "batched_over_plain": value / world / plain_value,
         "tb_err_vs_oracle_K": tb_err,
         "split_3xtf32": {"value": split_value, "unit": "solves/s", "ms_per_step": float(np.mean(sms_)),

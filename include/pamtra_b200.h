@@ -153,6 +153,30 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
                              const pamtra_b200_columns* cols, const pamtra_b200_outputs* out,
                              int32_t precision, void* stream);
 
+/* Launch shapes of the persistent kernels, chosen per workload by the
+ * autotuner (pamtra_b200/autotune.py); no counterpart in the reference, whose
+ * Fortran has no launch configuration.  params[0]: warps per Mie CTA (2, 4 or
+ * 8; 0 = 4), params[1..3]: CTAs per SM of the Mie, layer and adding kernels
+ * (0 = as many as fit).  Results do not depend on the launch shape. */
+#define PAMTRA_B200_NLAUNCH 4
+int32_t pamtra_b200_set_launch(pamtra_b200_ctx* ctx, const int32_t* params, int32_t n);
+int32_t pamtra_b200_get_launch(const pamtra_b200_ctx* ctx, int32_t* params, int32_t n);
+
+/* CUDA-graph form of pamtra_b200_run (no counterpart in the reference): one
+ * direct run on `stream` (synchronised) sizes the scratch arena and leaves
+ * the species table resident, then the launch sequence of the same call is
+ * captured.  pamtra_b200_graph_launch replays it on any stream: the kernels
+ * re-read the caller's input buffers, so new values in the same buffers
+ * (same shapes, same species table) give new results.  Replays fail with
+ * PAMTRA_B200_FATAL once the context's arena has been regrown by a larger
+ * batch; capture again then. */
+typedef struct pamtra_b200_graph pamtra_b200_graph;
+int32_t pamtra_b200_graph_capture(pamtra_b200_ctx* ctx, const pamtra_b200_settings* settings,
+                                  const pamtra_b200_columns* cols, const pamtra_b200_outputs* out,
+                                  int32_t precision, void* stream, pamtra_b200_graph** graph);
+int32_t pamtra_b200_graph_launch(pamtra_b200_graph* graph, void* stream);
+int32_t pamtra_b200_graph_destroy(pamtra_b200_graph* graph);
+
 /* Number of kernel launches the last pamtra_b200_run issued on ctx. */
 int32_t pamtra_b200_last_launch_count(const pamtra_b200_ctx* ctx);
 

@@ -51,7 +51,9 @@ EXPORTS = ["pamtra_b200_create", "pamtra_b200_destroy", "pamtra_b200_workspace_b
            "pamtra_b200_run", "pamtra_b200_run_host", "pamtra_b200_last_launch_count", "pamtra_b200_gas_r98",
            "pamtra_b200_eps_water_tkc", "pamtra_b200_minvert_batched", "pamtra_b200_set_timing",
            "pamtra_b200_stage_ms", "pamtra_b200_abi_sizes", "pamtra_b200_run_noalloc",
-           "pamtra_b200_mmult_3xtf32_batched"]
+           "pamtra_b200_mmult_3xtf32_batched", "pamtra_b200_set_launch", "pamtra_b200_get_launch",
+           "pamtra_b200_graph_capture", "pamtra_b200_graph_launch", "pamtra_b200_graph_destroy"]
+NLAUNCH = 4  # PAMTRA_B200_NLAUNCH: mie warps per CTA, mie / layer / adding CTAs per SM
 STAGES = ["prep", "psd", "mie", "layer", "adding"]
 
 _lib = None
@@ -92,6 +94,17 @@ def load():
                                               ctypes.POINTER(Outputs), _vp]
         l.pamtra_b200_mmult_3xtf32_batched.restype = _i32
         l.pamtra_b200_mmult_3xtf32_batched.argtypes = [_vp, _vp, _vp, _i32, _i32, _vp, _vp]
+        l.pamtra_b200_set_launch.restype = _i32
+        l.pamtra_b200_set_launch.argtypes = [_vp, ctypes.POINTER(_i32), _i32]
+        l.pamtra_b200_get_launch.restype = _i32
+        l.pamtra_b200_get_launch.argtypes = [_vp, ctypes.POINTER(_i32), _i32]
+        l.pamtra_b200_graph_capture.restype = _i32
+        l.pamtra_b200_graph_capture.argtypes = [_vp, ctypes.POINTER(Settings), ctypes.POINTER(Columns),
+                                                ctypes.POINTER(Outputs), _i32, _vp, ctypes.POINTER(_vp)]
+        l.pamtra_b200_graph_launch.restype = _i32
+        l.pamtra_b200_graph_launch.argtypes = [_vp, _vp]
+        l.pamtra_b200_graph_destroy.restype = _i32
+        l.pamtra_b200_graph_destroy.argtypes = [_vp]
         l.pamtra_b200_abi_sizes.restype = _i32
         l.pamtra_b200_abi_sizes.argtypes = [ctypes.POINTER(ctypes.c_size_t), _i32]
         _lib = l
@@ -174,6 +187,30 @@ class Engine(object):
         if err != 0:
             raise RuntimeError("pamtra_b200_run_host failed with code %d" % err)
 
+    def set_launch(self, params):
+        """Launch shapes of the persistent kernels: (mie warps per CTA, mie /
+        layer / adding CTAs per SM), 0 = default."""
+        arr = (_i32 * NLAUNCH)(*[int(v) for v in params])
+        if self.lib.pamtra_b200_set_launch(self.handle, arr, len(params)) != 0:
+            raise ValueError("invalid launch shape %r" % (tuple(params),))
+
+    def get_launch(self):
+        arr = (_i32 * NLAUNCH)()
+        self.lib.pamtra_b200_get_launch(self.handle, arr, NLAUNCH)
+        return tuple(int(v) for v in arr)
+
+    def capture(self, settings, columns, outputs, precision=PREC_FP64, stream=None):
+        """Run once on ``stream`` and capture the same call as a CUDA graph
+        (see :class:`Graph`).  The structs' buffers must stay alive and in
+        place while the graph is used."""
+        s = None if stream is None else stream.cuda_stream
+        g = _vp()
+        err = self.lib.pamtra_b200_graph_capture(self.handle, ctypes.byref(settings), ctypes.byref(columns),
+                                                 ctypes.byref(outputs), int(precision), s, ctypes.byref(g))
+        if err != 0 or not g:
+            raise RuntimeError("pamtra_b200_graph_capture failed with code %d" % err)
+        return Graph(self, g, (settings, columns, outputs))
+
     def reserve(self, nbytes):
         if self.lib.pamtra_b200_reserve(self.handle, int(nbytes)) != 0:
             raise MemoryError("cannot reserve %d bytes of device scratch" % nbytes)
@@ -192,6 +229,32 @@ class Engine(object):
         buf = (ctypes.c_float * len(STAGES))()
         self.lib.pamtra_b200_stage_ms(self.handle, buf, len(STAGES))
         return dict(zip(STAGES, [float(v) for v in buf]))
+
+
+class Graph(object):
+    """A captured launch sequence of one batch (pamtra_b200_graph_*)."""
+
+    def __init__(self, eng, handle, keep):
+        self.eng = eng
+        self.handle = handle
+        self._keep = keep  # the structs whose pointers the graph holds
+
+    def launch(self, stream=None):
+        s = None if stream is None else stream.cuda_stream
+        err = self.eng.lib.pamtra_b200_graph_launch(self.handle, s)
+        if err != 0:
+            raise RuntimeError("pamtra_b200_graph_launch failed with code %d (arena regrown? capture again)" % err)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.eng.lib.pamtra_b200_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def workspace_bytes(columns, species=None, precision=PREC_FP64):

@@ -401,3 +401,18 @@ def run_host(batch, device=0, outputs=None, precision=PREC_FP64, stream=None, en
     out = outputs if outputs is not None else batch.alloc_outputs(None, pinned=pinned)
     eng.run_host(batch.settings, batch.columns(arrs), eng.make_outputs(out), precision, stream)
     return out
+
+
+def capture(batch, device=0, outputs=None, precision=PREC_FP64, stream=None, eng=None):
+    """CUDA graph of one batched run (inputs resident on ``device``): replay
+    with ``graph.launch(stream)``; the kernels re-read the batch's device
+    buffers, so values updated in place give new results.  Returns
+    (graph, outputs)."""
+    import torch
+    eng = eng or engine(device)
+    dev = torch.device("cuda", device)
+    arrs = batch.device_arrays(dev)
+    out = outputs if outputs is not None else batch.alloc_outputs(dev)
+    g = eng.capture(batch.settings, batch.columns(arrs), eng.make_outputs(out), precision, stream)
+    g._keep = g._keep + (batch, out)
+    return g, out

@@ -254,6 +254,13 @@ int occupancy_blocks(const void* func, int threads, size_t smem, int sms) {
   return nb * sms;
 }
 
+// Persistent grid: `cps` CTAs per SM when set (capped at the resident
+// maximum), else the resident maximum.
+int persistent_grid(const void* func, int threads, size_t smem, int sms, int cps) {
+  const int full = occupancy_blocks(func, threads, smem, sms);
+  return cps > 0 ? std::min(full, cps * sms) : full;
+}
+
 }  // namespace
 
 namespace {
@@ -381,6 +388,11 @@ struct pamtra_b200_ctx {
   int last_launches = 0;
   char* stage = nullptr;  // device staging for run_host
   size_t stage_bytes = 0;
+  // launch shapes (pamtra_b200_set_launch; 0 = occupancy default)
+  int mie_warps = MIE_WARPS;  // warps per k_mie CTA (2, 4 or 8)
+  int mie_cps = 0;            // k_mie CTAs per SM
+  int layer_cps = 0;          // k_layer / k_layer_tc CTAs per SM
+  int adding_cps = 0;         // k_adding CTAs per SM
   // optional per-stage timing (events recorded on the run's stream)
   int timing = 0;
   cudaEvent_t ev[16] = {};
@@ -419,7 +431,7 @@ static int set_smem_attrs() {
     auto set = [](const void* f, size_t bytes) {
       if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) rc = 1;
     };
-    set((const void*)k_mie, MIE_WARPS * sizeof(MieSmem));
+    set((const void*)k_mie, MIE_MAX_WARPS * sizeof(MieSmem));
     set((const void*)k_layer<8>, sizeof(LayerSmem<8>));
     set((const void*)k_layer<16>, sizeof(LayerSmem<16>));
     set((const void*)k_layer<32>, sizeof(LayerSmem<32>));
@@ -524,12 +536,103 @@ int32_t pamtra_b200_reserve(pamtra_b200_ctx* ctx, size_t bytes) {
   return PAMTRA_B200_OK;
 }
 
+// ---------------------------------------------------------------- CUDA graphs
+struct pamtra_b200_graph {
+  pamtra_b200_ctx* ctx = nullptr;
+  const char* arena = nullptr;  // the arena the captured launches address
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int launches = 0;
+};
+
+int32_t pamtra_b200_graph_capture(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st,
+                                  const pamtra_b200_columns* cols, const pamtra_b200_outputs* out, int32_t precision,
+                                  void* stream_, pamtra_b200_graph** gout) {
+  if (!ctx || !gout) return PAMTRA_B200_FATAL;
+  *gout = nullptr;
+  cudaSetDevice(ctx->device);
+  cudaStream_t stream = (cudaStream_t)stream_;
+  // one direct run sizes the arena, fills the tables and leaves the species
+  // table resident, so the captured sequence has no host-side waits
+  const int timing = ctx->timing;
+  ctx->timing = 0;
+  int32_t rc = pamtra_b200_run(ctx, st, cols, out, precision, stream);
+  if (rc == PAMTRA_B200_OK && cudaStreamSynchronize(stream) != cudaSuccess) rc = PAMTRA_B200_FATAL;
+  cudaStream_t cs = nullptr;
+  if (rc == PAMTRA_B200_OK && cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) rc = PAMTRA_B200_FATAL;
+  pamtra_b200_graph* g = nullptr;
+  if (rc == PAMTRA_B200_OK) {
+    g = new pamtra_b200_graph();
+    g->ctx = ctx;
+    g->arena = ctx->arena;
+    if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) rc = PAMTRA_B200_FATAL;
+    if (rc == PAMTRA_B200_OK) {
+      const int32_t rr = pamtra_b200_run(ctx, st, cols, out, precision, cs);
+      const cudaError_t ce = cudaStreamEndCapture(cs, &g->graph);
+      if (rr != PAMTRA_B200_OK || ce != cudaSuccess || ctx->arena != g->arena) rc = PAMTRA_B200_FATAL;
+      g->launches = ctx->last_launches;
+    }
+    if (rc == PAMTRA_B200_OK && cudaGraphInstantiate(&g->exec, g->graph, 0) != cudaSuccess) rc = PAMTRA_B200_FATAL;
+  }
+  if (cs) cudaStreamDestroy(cs);
+  ctx->timing = timing;
+  cudaGetLastError();
+  if (rc != PAMTRA_B200_OK) {
+    if (g) {
+      if (g->exec) cudaGraphExecDestroy(g->exec);
+      if (g->graph) cudaGraphDestroy(g->graph);
+      delete g;
+    }
+    return rc;
+  }
+  *gout = g;
+  return PAMTRA_B200_OK;
+}
+
+int32_t pamtra_b200_graph_launch(pamtra_b200_graph* g, void* stream) {
+  if (!g || !g->exec) return PAMTRA_B200_FATAL;
+  if (g->ctx->arena != g->arena) return PAMTRA_B200_FATAL;  // the arena was regrown after the capture
+  cudaSetDevice(g->ctx->device);
+  g->ctx->last_launches = g->launches;
+  return cudaGraphLaunch(g->exec, (cudaStream_t)stream) == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
+}
+
+int32_t pamtra_b200_graph_destroy(pamtra_b200_graph* g) {
+  if (!g) return PAMTRA_B200_OK;
+  cudaSetDevice(g->ctx->device);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return PAMTRA_B200_OK;
+}
+
 int32_t pamtra_b200_last_launch_count(const pamtra_b200_ctx* ctx) { return ctx ? ctx->last_launches : 0; }
 
 int32_t pamtra_b200_abi_sizes(size_t* out, int32_t n) {
   const size_t sz[4] = {sizeof(pamtra_b200_settings), sizeof(pamtra_b200_species), sizeof(pamtra_b200_columns),
                         sizeof(pamtra_b200_outputs)};
   for (int i = 0; i < n && i < 4; i++) out[i] = sz[i];
+  return PAMTRA_B200_OK;
+}
+
+int32_t pamtra_b200_set_launch(pamtra_b200_ctx* ctx, const int32_t* params, int32_t n) {
+  if (!ctx || (n > 0 && !params) || n < 0 || n > PAMTRA_B200_NLAUNCH) return PAMTRA_B200_FATAL;
+  int v[PAMTRA_B200_NLAUNCH] = {MIE_WARPS, 0, 0, 0};
+  for (int i = 0; i < n; i++) v[i] = params[i];
+  if (!(v[0] == 0 || v[0] == 2 || v[0] == 4 || v[0] == 8)) return PAMTRA_B200_FATAL;
+  for (int i = 1; i < PAMTRA_B200_NLAUNCH; i++)
+    if (v[i] < 0 || v[i] > 32) return PAMTRA_B200_FATAL;
+  ctx->mie_warps = v[0] ? v[0] : MIE_WARPS;
+  ctx->mie_cps = v[1];
+  ctx->layer_cps = v[2];
+  ctx->adding_cps = v[3];
+  return PAMTRA_B200_OK;
+}
+
+int32_t pamtra_b200_get_launch(const pamtra_b200_ctx* ctx, int32_t* params, int32_t n) {
+  if (!ctx || !params || n < 0) return PAMTRA_B200_FATAL;
+  const int v[PAMTRA_B200_NLAUNCH] = {ctx->mie_warps, ctx->mie_cps, ctx->layer_cps, ctx->adding_cps};
+  for (int i = 0; i < n && i < PAMTRA_B200_NLAUNCH; i++) params[i] = v[i];
   return PAMTRA_B200_OK;
 }
 
@@ -672,9 +775,10 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   mark(ctx, stream, STG_PSD);
   const int sms = ctx->sm_count;
   if (H > 0) {
-    const size_t sm_mie = MIE_WARPS * sizeof(MieSmem);
-    int g = occupancy_blocks((const void*)k_mie, 32 * MIE_WARPS, sm_mie, sms);
-    k_mie<<<g, 32 * MIE_WARPS, sm_mie, stream>>>(b, w, *st); launches++;
+    const int mw = ctx->mie_warps;
+    const size_t sm_mie = mw * sizeof(MieSmem);
+    int g = persistent_grid((const void*)k_mie, 32 * mw, sm_mie, sms, ctx->mie_cps);
+    k_mie<<<g, 32 * mw, sm_mie, stream>>>(b, w, *st); launches++;
     if (w.wtab[0] && (mask & 1)) {
       k_scat_weights<8><<<SCAT_NPI * ((2 * 8 * 8 + 127) / 128), 128, 0, stream>>>(ctx->wtab[0], w.wt_need, w.wt_ready, ctx->lob_mu);
       launches++;
@@ -691,10 +795,10 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   mark(ctx, stream, STG_MIE);
   double* ssp = out->scatter_matrix;
   if (mask & 1) {
-    int g = occupancy_blocks((const void*)k_layer<8>, RTCfg<8>::T, sizeof(LayerSmem<8>), sms);
+    int g = persistent_grid((const void*)k_layer<8>, RTCfg<8>::T, sizeof(LayerSmem<8>), sms, ctx->layer_cps);
     if (H > 0) { k_layer<8><<<g, RTCfg<8>::T, sizeof(LayerSmem<8>), stream>>>(b, w, *st, ssp); launches++; }
     mark(ctx, stream, STG_LAYER);
-    g = occupancy_blocks((const void*)k_adding<8>, RTCfg<8>::T, sizeof(AddSmem<8>), sms);
+    g = persistent_grid((const void*)k_adding<8>, RTCfg<8>::T, sizeof(AddSmem<8>), sms, ctx->adding_cps);
     k_adding<8><<<g, RTCfg<8>::T, sizeof(AddSmem<8>), stream>>>(b, w, *st, *out); launches++;
     mark(ctx, stream, STG_ADDING);
   }
@@ -703,22 +807,23 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
       // two CTAs (two item pairs) per SM by shared memory; the persistent CTAs
       // take pairs of items from a counter
       const size_t smb = layer_tc_smem<16>();
-      const int g = 2 * sms;
+      const int g = (ctx->layer_cps == 1 ? 1 : 2) * sms;
       k_layer_tc<16><<<g, 128, smb, stream>>>(b, w, *st, ssp); launches++;
     } else if (H > 0) {
-      int g = occupancy_blocks((const void*)k_layer<16>, RTCfg<16>::T, sizeof(LayerSmem<16>), sms);
+      int g = persistent_grid((const void*)k_layer<16>, RTCfg<16>::T, sizeof(LayerSmem<16>), sms, ctx->layer_cps);
       k_layer<16><<<g, RTCfg<16>::T, sizeof(LayerSmem<16>), stream>>>(b, w, *st, ssp); launches++;
     }
     mark(ctx, stream, STG_LAYER);
-    const int g = occupancy_blocks((const void*)k_adding<16>, RTCfg<16>::T, sizeof(AddSmem<16>), sms);
+    const int g = persistent_grid((const void*)k_adding<16>, RTCfg<16>::T, sizeof(AddSmem<16>), sms, ctx->adding_cps);
     k_adding<16><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out); launches++;
     mark(ctx, stream, STG_ADDING);
   }
   if (mask & 4) {
-    int g = occupancy_blocks((const void*)k_layer<32>, RTCfg<32>::T, sizeof(LayerSmem<32>), sms);
+    int g = persistent_grid((const void*)k_layer<32>, RTCfg<32>::T, sizeof(LayerSmem<32>), sms, ctx->layer_cps);
     if (H > 0) { k_layer<32><<<g, RTCfg<32>::T, sizeof(LayerSmem<32>), stream>>>(b, w, *st, ssp); launches++; }
     mark(ctx, stream, STG_LAYER);
-    g = std::min(occupancy_blocks((const void*)k_adding<32>, RTCfg<32>::T, sizeof(AddSmem<32>), sms), pl.add_grid);
+    g = std::min(persistent_grid((const void*)k_adding<32>, RTCfg<32>::T, sizeof(AddSmem<32>), sms, ctx->adding_cps),
+                 pl.add_grid);
     k_adding<32><<<g, RTCfg<32>::T, sizeof(AddSmem<32>), stream>>>(b, w, *st, *out); launches++;
     mark(ctx, stream, STG_ADDING);
   }

@@ -105,9 +105,10 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b) {
                : "d"(a), "d"(b));
 }
 
-enum MMMode { MM_SET = 0, MM_ACC = 1, MM_IMINUS = 2 };
+enum MMMode { MM_SET = 0, MM_ACC = 1, MM_IMINUS = 2, MM_IPLUS = 3 };
 
-// C = A*B (MM_SET), C = D + A*B (MM_ACC) or C = I - A*B (MM_IMINUS).
+// C = A*B (MM_SET), C = D + A*B (MM_ACC), C = I - A*B (MM_IMINUS) or
+// C = I + A*B (MM_IPLUS).
 // Each warp computes one 16 x 16 tile with 2 x 2 DMMA fragments per k-step
 // of 4.  Without INPLACE, C must not alias A or B; with INPLACE the team
 // synchronises between reading the operands and writing C, so C may be A,
@@ -126,7 +127,8 @@ __device__ __forceinline__ void mm(const double* A, const double* B, double* C, 
 #pragma unroll
       for (int i = 0; i < 2; i++) {
         const int row = row0 + rt * 8 + g, col = col0 + ct * 8 + 2 * q + i;
-        c[rt][ct][i] = (MODE == MM_ACC) ? D[col * LD + row] : ((MODE == MM_IMINUS) ? (row == col ? 1.0 : 0.0) : 0.0);
+        c[rt][ct][i] = (MODE == MM_ACC) ? D[col * LD + row]
+                                        : ((MODE == MM_IMINUS || MODE == MM_IPLUS) ? (row == col ? 1.0 : 0.0) : 0.0);
       }
   const double sgn = (MODE == MM_IMINUS) ? -1.0 : 1.0;
 #pragma unroll 4
@@ -273,10 +275,15 @@ __device__ int ginv(double* A, InvScratch<n>& S) {
 }
 
 // G = (I - X)^-1 in FP64.  X (in buffer P) is overwritten.  When the row-sum
-// norm of X is below 0.74 the inverse is the product (I + X)(I + X^2)(I + X^4)...
-// truncated where ||X||^(2^m) < 2^-54 (relative truncation error below the
-// FP64 rounding unit); otherwise Gauss-Jordan with partial pivoting is used.
-// Returns the buffer holding the inverse (P or G); *sing set on a zero pivot.
+// norm of X is below 0.74 the inverse is a truncated Neumann series whose
+// remainder is below 2^-54 relative (the FP64 rounding unit), evaluated with
+// the fewer products of two forms:
+//   Horner    G = I + X (I + X (... (I + X)))   k products, remainder ||X||^(k+2)
+//   squaring  G = (I + X)(I + X^2)(I + X^4)...  2 (m-1) products, remainder ||X||^(2^m)
+// (Horner wins for the thin layers of the first doublings, where ||X|| is
+// tiny and G = I + X needs no product at all); otherwise Gauss-Jordan with
+// partial pivoting.  Returns the buffer holding the inverse (P or G); *sing
+// set on a zero pivot.
 template <int n>
 __device__ double* inv_iminus(double* P, double* G, InvScratch<n>& S, int* sing) {
   constexpr int LD = Team<n>::LD, T = Team<n>::T;
@@ -300,6 +307,24 @@ __device__ double* inv_iminus(double* P, double* G, InvScratch<n>& S, int* sing)
   while (pw > 5.0e-17 && m < 8) {
     pw = pw * pw;
     m++;
+  }
+  int kh = 0;  // Horner products
+  double ph = nrm * nrm;
+  while (ph > 5.0e-17 && kh < 2 * (m - 1)) {
+    ph = ph * nrm;
+    kh++;
+  }
+  if (m < 8 && ph <= 5.0e-17 && kh < 2 * (m - 1)) {
+    for (int e = t; e < n * n; e += T) {
+      const int col = e / n, row = e % n;
+      G[col * LD + row] = ((row == col) ? 1.0 : 0.0) + P[col * LD + row];
+    }
+    team_sync();
+    for (int k = 0; k < kh; k++) {
+      mm<n, MM_IPLUS, true>(P, G, G);  // G = I + X G
+      team_sync();
+    }
+    return G;
   }
   if (m >= 8) {
     // Gauss-Jordan on I - X

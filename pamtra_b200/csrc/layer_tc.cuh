@@ -48,8 +48,7 @@ struct TcItemState {
 };
 
 struct TcTiles {
-  float a_hi[128 * 32], a_lo[128 * 32];  // A tile pair (128 rows)
-  float b_hi[64 * 32], b_lo[64 * 32];    // B tile pair (64 rows: 32 per item)
+  float b_hi[64 * 32], b_lo[64 * 32];  // B tile pair (64 rows: 32 per item); the A pair lives in TMEM
 };
 
 union __align__(128) TcScratch {
@@ -86,15 +85,21 @@ __device__ __forceinline__ void st_col(float* m, int col, const float (&v)[32]) 
   for (int r = 0; r < 32; r += 4) *reinterpret_cast<float4*>(m + col * S + r) = make_float4(v[r], v[r + 1], v[r + 2], v[r + 3]);
 }
 
-// Operands of one group for the calling thread: A row `arow` from column
-// `lane` of master `asrc`, and K-chunks 4h..4h+3 of B row `brow` (row `lane`
-// of master `bsrc`, read down its columns: conflict-free), split into TF32
-// hi / lo pairs.  The two warps of an item cover the B row's two halves.
-__device__ __forceinline__ void build_operands(TcTiles& TL, const float* asrc, const float* bsrc, int arow,
-                                               int brow, int h, int lane) {
-  float c[32];
-  ld_col(asrc, lane, c);
-  tc::put_row(TL.a_hi, TL.a_lo, arow, c);
+// Operands of one group for the calling thread, split into TF32 hi / lo
+// pairs: its A row (column `lane` of master `asrc`) into its own TMEM lane
+// at columns ta_hi / ta_lo, and K-chunks 4h..4h+3 of B row `brow` (row
+// `lane` of master `bsrc`, read down its columns: conflict-free) into shared
+// memory.  The two warps of an item cover the B row's two halves.
+__device__ __forceinline__ void build_operands(TcTiles& TL, const float* asrc, const float* bsrc, uint32_t ta_hi,
+                                               uint32_t ta_lo, int brow, int h, int lane) {
+  {
+    float c[32], lo[32];
+    ld_col(asrc, lane, c);
+#pragma unroll
+    for (int r = 0; r < 32; r++) tc::split(c[r], c[r], lo[r]);
+    tc::tmem_st32(ta_hi, c);
+    tc::tmem_st32(ta_lo, lo);
+  }
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int k0 = 16 * h + 4 * q;
@@ -127,10 +132,14 @@ __device__ __forceinline__ void matvec2(const float* __restrict__ M, const float
   y1 = a1;
 }
 
-// Number of squarings of the series for ||X|| = nrm (any sub-multiplicative
-// norm): s >= 1 means s + 1 MMAs, 0 means G~ = X, -1 the FP64 fallback.
+// Series plan for ||X|| = nrm (any sub-multiplicative norm), by the relative
+// remainder it leaves: s >= 1 repeated squaring in s + 1 MMAs (remainder
+// nrm^(2^(s+1) - 1)), 0: G~ = X (nrm), SERIES_H1: G~ = X + X X in one MMA
+// (nrm^2), -1: the FP64 fallback.
+constexpr int SERIES_H1 = -3;
 __device__ __forceinline__ int series_steps(float nrm) {
   if (!(nrm < NEUMANN_MAX_NORM)) return -1;
+  if (nrm > NEUMANN_TOL && nrm * nrm <= NEUMANN_TOL) return SERIES_H1;
   float pw = nrm;  // nrm^(2^(s+1) - 1)
   float pk = nrm;  // nrm^(2^s)
   int s = 0;
@@ -164,7 +173,7 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
   const int P = min(w.counters[0], w.pmax);
   const int nitems = P * Fm;
   scat_weights_mark_ready<N>(w);
-  if (warp == 0) tc::tmem_alloc(&tslot, 64);
+  if (warp == 0) tc::tmem_alloc(&tslot, 128);  // D: columns 0..63, A hi: 64..95, A lo: 96..127
   if (t == 0) {
     tc::mbar_init(&mbar, 1);
     s_dead = 0;
@@ -172,9 +181,9 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  const uint32_t dmine = tslot + ((uint32_t)(warp * 32) << 16) + 32u * mi;  // my lanes, my item's columns
-  const int arow = 32 * warp + lane;  // A row = D lane of this thread
-  const int brow = 32 * mi + lane;    // B row of my item for my lane
+  const uint32_t lanes = (uint32_t)(warp * 32) << 16;  // A row = D lane of this thread
+  const uint32_t dmine = tslot + lanes + 32u * mi;       // my lanes, my item's columns of D
+  const int brow = 32 * mi + lane;                       // B row of my item for my lane
   uint32_t parity = 0;
 
   for (;;) {
@@ -236,10 +245,10 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
       //   SER [X; G~] x X   -> slot 0: X X      -> X next;  slot 1: X G~ -> G~ += X + X G~
       //   G2  [T~; V] x G~  -> slot 0: G~ T~    -> Z~;      slot 1: G~ V -> Y = V + G~ V
       //   G3  [Z~; Y] x T~  -> slot 0: T~ Z~    -> T~';     slot 1: T~ Y -> R'
-      int phase = G1, d = 0, k = 0, mys = 0, smax = 0, xsel = 0;
+      int phase = G1, d = 0, k = 0, mys = 0, myg = 0, gmax = 0, xsel = 0;  // plan, MMAs: mine / the pair's
       for (;;) {
         const bool act = d < my_nd;
-        const bool on = (phase == SER) ? (mys > 0 && k <= mys) : act;
+        const bool on = (phase == SER) ? (k < myg) : act;
         float* xc = xsel ? my.xb : my.xa;  // current series power
         float* xn = xsel ? my.xa : my.xb;
         if (on) {
@@ -249,13 +258,13 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
           else if (phase == SER) { asrc = slot ? my.gm : xc; bsrc = xc; }
           else if (phase == G2) { asrc = slot ? my.vm : my.tm; bsrc = my.gm; }
           else { asrc = slot ? my.vm : my.xa; bsrc = my.tm; }
-          build_operands(TL, asrc, bsrc, arow, brow, slot, lane);
+          build_operands(TL, asrc, bsrc, tslot + lanes + 64u, tslot + lanes + 96u, brow, slot, lane);
         }
         tc::fence_async_smem();
         tc::fence_before_sync();
         __syncthreads();
         tc::fence_after_sync();
-        if (t == 0) tc::mma3(tslot, TL.a_hi, TL.a_lo, TL.b_hi, TL.b_lo, &mbar, tc::IDESC_M128_N64);
+        if (t == 0) tc::mma3_ta(tslot, tslot + 64u, tslot + 96u, TL.b_hi, TL.b_lo, &mbar, tc::IDESC_M128_N64);
         float m0 = 0.f, m1 = 0.f;
         if (on && phase != SER) {
           const float* mv = (phase == G1) ? my.rm : (phase == G2) ? my.gm : my.tm;
@@ -292,7 +301,14 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
               st_col(my.vm, lane, a);
             }
           } else if (phase == SER) {
-            if (slot == 0) {
+            if (mys == SERIES_H1) {
+              if (slot == 0) {  // G~ = X + X X
+                ld_col(xc, lane, a);
+#pragma unroll
+                for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
+                st_col(my.gm, lane, a);
+              }
+            } else if (slot == 0) {
               if (k < mys) st_col(xn, lane, dv);  // X = X X
             } else {  // G~ += X + X G~
               float g[32];
@@ -374,8 +390,10 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
             __syncthreads();
           }
           mys = mi ? stp1 : stp0;
-          smax = max(stp0, stp1);
-          if (slot == 1 && mys >= 0) {  // G~ = X (no series), or G~ = 0 to start one
+          myg = (mys >= 1) ? mys + 1 : (mys == SERIES_H1 ? 1 : 0);
+          gmax = max((stp0 >= 1) ? stp0 + 1 : (stp0 == SERIES_H1 ? 1 : 0),
+                     (stp1 >= 1) ? stp1 + 1 : (stp1 == SERIES_H1 ? 1 : 0));
+          if (slot == 1 && (mys >= 0 || mys == SERIES_H1)) {  // G~ = X (no series), or G~ = 0 to start one
             float g[32];
             if (mys == 0) ld_col(my.xa, lane, g);
 #pragma unroll
@@ -385,10 +403,10 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
           __syncthreads();
           k = 0;
           xsel = 0;
-          phase = (smax > 0) ? SER : G2;
+          phase = (gmax > 0) ? SER : G2;
         } else if (phase == SER) {
           xsel ^= 1;
-          if (++k > smax) phase = G2;
+          if (++k >= gmax) phase = G2;
         } else if (phase == G2) {
           phase = G3;
         } else {
@@ -429,7 +447,7 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  if (warp == 0) tc::tmem_dealloc(tslot, 64);
+  if (warp == 0) tc::tmem_dealloc(tslot, 128);
 }
 
 }  // namespace pb

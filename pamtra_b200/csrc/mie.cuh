@@ -7,7 +7,8 @@
 
 namespace pb {
 
-constexpr int MIE_WARPS = 4;
+constexpr int MIE_WARPS = 4;      // default warps per CTA
+constexpr int MIE_MAX_WARPS = 8;  // largest launch shape (pamtra_b200_set_launch)
 constexpr int NQ_MAX = 256;   // Gauss points per series (nquad)
 constexpr int NT_MAX = 128;   // Mie terms per bin
 constexpr int ANG_G = 2;      // angles per pass over a bin's Mie coefficients
@@ -188,7 +189,7 @@ __device__ __forceinline__ void mieangle_group(int nterms, const cplx* ab, const
 // Bins are spread over lanes; per-angle phase functions and the efficiencies
 // are summed over bins with warp shuffles; the Legendre projection is a
 // lane-per-quadrature-point series reduced with shuffles.
-__global__ void __launch_bounds__(32 * MIE_WARPS) k_mie(Batch b, Work w, pamtra_b200_settings st) {
+__global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st) {
   extern __shared__ double smem_raw[];
   MieSmem& S = reinterpret_cast<MieSmem*>(smem_raw)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;

@@ -96,6 +96,38 @@ __device__ __forceinline__ void mma3(uint32_t d_tmem, const float* a_hi, const f
                : "memory");
 }
 
+// D[tmem] (+)= A * B^T over K = 8 with A read from tensor memory (lanes =
+// rows of A, one TF32 value per column) and B from shared memory (one thread)
+__device__ __forceinline__ void mma_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t accumulate,
+                                       uint32_t idesc) {
+  asm volatile(
+      "{\n\t"
+      ".reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t"
+      "}\n"
+      :
+      : "r"(d_tmem), "r"(a_tmem), "l"(b), "r"(idesc), "r"(accumulate));
+}
+
+// 3xTF32 product with the A pair in tensor memory (columns a_hi..a_hi+31 and
+// a_lo..a_lo+31 of lanes 0..127) and the B pair in shared memory:
+// D = A * B^T, small terms first.  One thread; completion on `mbar`.
+__device__ __forceinline__ void mma3_ta(uint32_t d_tmem, uint32_t a_hi, uint32_t a_lo, const float* b_hi,
+                                        const float* b_lo, uint64_t* mbar, uint32_t idesc) {
+  const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+#pragma unroll
+  for (int s = 0; s < TILE_K / 8; s++) mma_ta(d_tmem, a_lo + 8 * s, desc_k(bh + 256 * s), s > 0, idesc);
+#pragma unroll
+  for (int s = 0; s < TILE_K / 8; s++) mma_ta(d_tmem, a_hi + 8 * s, desc_k(bl + 256 * s), 1, idesc);
+#pragma unroll
+  for (int s = 0; s < TILE_K / 8; s++) mma_ta(d_tmem, a_hi + 8 * s, desc_k(bh + 256 * s), 1, idesc);
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+               :
+               : "r"(smem_u32(mbar))
+               : "memory");
+}
+
 __device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" : : "r"(smem_u32(mbar)), "r"(count) : "memory");
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -154,6 +186,29 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 32; i++) v[i] = __uint_as_float(r[i]);
+}
+
+// Store 32 FP32 values into 32 consecutive columns of this thread's lane
+// (warp w writes lanes 32w..32w+31), and wait for the stores to complete.
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};"
+      :
+      : "r"(taddr), "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+        "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+        "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+        "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+        "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+        "r"(__float_as_uint(v[15])), "r"(__float_as_uint(v[16])), "r"(__float_as_uint(v[17])),
+        "r"(__float_as_uint(v[18])), "r"(__float_as_uint(v[19])), "r"(__float_as_uint(v[20])),
+        "r"(__float_as_uint(v[21])), "r"(__float_as_uint(v[22])), "r"(__float_as_uint(v[23])),
+        "r"(__float_as_uint(v[24])), "r"(__float_as_uint(v[25])), "r"(__float_as_uint(v[26])),
+        "r"(__float_as_uint(v[27])), "r"(__float_as_uint(v[28])), "r"(__float_as_uint(v[29])),
+        "r"(__float_as_uint(v[30])), "r"(__float_as_uint(v[31]))
+      : "memory");
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 // Write one 32-value row of a tile pair (hi, lo) from FP32 values.
