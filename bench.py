@@ -9,11 +9,17 @@ layers over 0-12 km, cloud liquid (exp, 40 bins) and rain (Marshall-Palmer,
 50 bins) in layers 5-25 with mixing ratios log-uniform over 0.01-2 g/kg,
 frequencies 23.8, 31.4, 89 and 150 GHz, NUMMU = 16, FP64.
 
-  value  : batched solves/s with inputs resident in HBM (device-timed,
-           CUDA events on the launching stream, L2 flushed between steps)
+  value  : batched FP64 form (PREC_FP64_BATCHED: one inverse per adding
+           combine) in solves/s with inputs resident in HBM (device-timed,
+           CUDA events on the launching stream, L2 flushed between steps),
+           launch shapes from the autotuner
   e2e    : same metric through the C ABI with host buffers (pinned), the
            host<->device copies inside the timed region
-  plain  : the plain form (one column per call) on a sample of columns
+  plain  : the plain form (one column per call, the reference operation
+           order PREC_FP64) on a sample of columns
+  split_3xtf32 / target_shape / serving / graph_replay: the split-precision
+           form, the 150-layer 4-species shape, the request loop and the
+           CUDA-graph replay of the same step
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 Under torchrun each rank runs its own columns (weak scaling, no collective on
@@ -182,8 +188,8 @@ def fp64_peak_tflops(dev):
 
 
 # k_layer<16> DRAM traffic per (layer, frequency) item: ncu capture of the
-# 256-column run (21,504 items): 13.1 MB read + 349.2 MB written per launch
-LAYER_TRAFFIC_PER_ITEM = (13.093632e6 + 349.194752e6) / 21504
+# 256-column run (21,504 items): 16.9 MB read + 349.5 MB written per launch
+LAYER_TRAFFIC_PER_ITEM = (16.933632e6 + 349.538304e6) / 21504
 
 
 def layer_flops(nd, N):
@@ -233,10 +239,11 @@ def _target_shape(args, local, eng, stream):
     b = target_batch(args.target_cols, seed=4)
     out = b.alloc_outputs(dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    autotune.tune(b, local, eng=eng, stream=stream, outputs=out)
+    from pamtra_b200._native import PREC_FP64_BATCHED as BF
+    autotune.tune(b, local, precision=BF, eng=eng, stream=stream, outputs=out)
     with torch.cuda.stream(stream):
         for _ in range(2):
-            pbatch.run(b, local, out, stream=stream, eng=eng)
+            pbatch.run(b, local, out, precision=BF, stream=stream, eng=eng)
     stream.synchronize()
     ms = []
     for _ in range(3):
@@ -244,7 +251,7 @@ def _target_shape(args, local, eng, stream):
             flush.zero_()
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record(stream)
-            pbatch.run(b, local, out, stream=stream, eng=eng)
+            pbatch.run(b, local, out, precision=BF, stream=stream, eng=eng)
             e.record(stream)
         e.synchronize()
         ms.append(s.elapsed_time(e))
@@ -272,7 +279,7 @@ def _target_shape(args, local, eng, stream):
     e.synchronize()
     plain = sum(sb.n_solves() for sb in singles) / (s.elapsed_time(e) * 1e-3)
     tb = out["tb"].cpu().numpy()
-    same = all(np.array_equal(so["tb"].cpu().numpy()[0], tb[c]) for c, so in enumerate(souts))
+    plain_diff = max(float(np.max(np.abs(so["tb"].cpu().numpy()[0] - tb[c]))) for c, so in enumerate(souts))
     del flush
     return {"workload": "%d columns x 150 layers (0-15 km), NUMMU=16, 4 Mie species (cloud water, cloud ice, "
                         "snow, rain; 40 bins each), f = 23.8/31.4/89/150 GHz" % args.target_cols,
@@ -280,7 +287,9 @@ def _target_shape(args, local, eng, stream):
             "batched_3xtf32": split, "batched_3xtf32_over_plain": split / plain,
             "tb_err_3xtf32_vs_fp64_K": split_err, "stage_ms_3xtf32": sstages,
             "unit": "solves/s", "batched_ms_per_step": float(np.mean(ms)), "status_nonzero": st_bad,
-            "plain_sample_columns": 16, "plain_equals_batched_bitwise": bool(same)}
+            "plain_sample_columns": 16, "plain_vs_batched_fp64_tb_max_diff_K": plain_diff,
+            "forms": "batched FP64: one-inverse adding (PREC_FP64_BATCHED); plain: one column per call in the "
+                     "reference operation order (PREC_FP64)"}
 
 
 def _serving(args, local):
@@ -291,7 +300,8 @@ def _serving(args, local):
     reqs = serve.request_stream(args.serve_requests, seed=5, max_cols=512, nfreq_range=(1, 32))
     arr = serve.poisson_arrivals(len(reqs), 200.0, seed=6)
     warm = serve.request_stream(3, seed=7, max_cols=16, nfreq_range=(1, 4))
-    srv = serve.Server(local, slots=3, hbm_fraction=0.5, max_cols=2048)
+    from pamtra_b200._native import PREC_FP64_BATCHED
+    srv = serve.Server(local, slots=3, hbm_fraction=0.5, max_cols=2048, precision=PREC_FP64_BATCHED)
     for b in warm:
         srv.submit(b)
     srv.drain()
@@ -383,10 +393,11 @@ def main():
     out = b.alloc_outputs(dev, ssp=True)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     # launch shapes of the persistent kernels, tuned on this batch (untimed)
-    shape64, tune64 = autotune.tune(b, local, eng=eng, stream=stream, outputs=out)
+    from pamtra_b200._native import PREC_FP64_BATCHED as BF
+    shape64, tune64 = autotune.tune(b, local, precision=BF, eng=eng, stream=stream, outputs=out)
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
-            pbatch.run(b, local, out, stream=stream, eng=eng)
+            pbatch.run(b, local, out, precision=BF, stream=stream, eng=eng)
     stream.synchronize()
     status = out["status"].cpu().numpy()
     nd = out["num_doubles"].cpu().numpy()
@@ -405,7 +416,7 @@ def main():
             flush.zero_()
             s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             s.record(stream)
-            pbatch.run(b, local, out, stream=stream, eng=eng)
+            pbatch.run(b, local, out, precision=BF, stream=stream, eng=eng)
             e.record(stream)
         e.synchronize()
         times.append(s.elapsed_time(e))
@@ -422,7 +433,7 @@ def main():
     solves_step = b.n_solves()
     value = world * solves_step * args.steps / t_total
     # ---- the same step replayed from a captured CUDA graph
-    graph, gout = pbatch.capture(b, local, stream=stream, eng=eng)
+    graph, gout = pbatch.capture(b, local, precision=BF, stream=stream, eng=eng)
     for _ in range(args.warmup):
         graph.launch(stream)
     stream.synchronize()
@@ -442,11 +453,11 @@ def main():
     graph_value = world * solves_step / (np.mean(g_ms) * 1e-3)
     # ---- end-to-end through the C ABI with host buffers
     hout = b.alloc_outputs(None, pinned=True)
-    pbatch.run_host(b, local, hout, eng=eng)
+    pbatch.run_host(b, local, hout, precision=BF, eng=eng)
     e2e_t = []
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        pbatch.run_host(b, local, hout, eng=eng)
+        pbatch.run_host(b, local, hout, precision=BF, eng=eng)
         e2e_t.append(time.perf_counter() - t0)
     e2e_total = sum(e2e_t)
     if dist is not None:
@@ -480,6 +491,12 @@ def main():
         e.record(stream)
     e.synchronize()
     plain_value = nplain * len(FREQS) / (s.elapsed_time(e) * 1e-3)
+    # the plain form on the first columns of the batch: agreement with the batched form
+    tb_b = out["tb"].cpu().numpy()
+    plain_diff = 0.0
+    for c in range(4):
+        po = pbatch.run(pbatch.subset(b, [c]), local, eng=eng)
+        plain_diff = max(plain_diff, float(np.max(np.abs(po["tb"].cpu().numpy()[0] - tb_b[c]))))
 
     if rank != 0:
         if dist is not None:
@@ -531,7 +548,10 @@ def main():
         "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clocks,
-        "plain_fp64": {"value": plain_value, "unit": "solves/s", "form": "one column per call, FP64"},
+        "plain_fp64": {"value": plain_value, "unit": "solves/s",
+                       "form": "one column per call, FP64 in the reference operation order (PREC_FP64)",
+                       "tb_max_diff_vs_batched_K": plain_diff},
+        "batched_form": "FP64, one-inverse adding combine (PREC_FP64_BATCHED)",
         "graph_replay": {"value": graph_value, "unit": "solves/s", "ms_per_step": float(np.mean(g_ms)),
                          "tb_equals_direct": graph_same,
                          "form": "the batched FP64 step captured once as a CUDA graph and replayed"},

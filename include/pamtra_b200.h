@@ -60,10 +60,17 @@ extern "C" {
 #define PAMTRA_B200_DIST_LOGN 6
 #define PAMTRA_B200_DIST_DISABLED 7
 
-/* precision of the doubling / adding matrix products */
-#define PAMTRA_B200_PREC_FP64 0      /* plain and batched FP64 */
-#define PAMTRA_B200_PREC_3XTF32 1    /* batched form: layer doubling products as 3xTF32 tcgen05 MMAs
-                                       (NUMMU = 16; NUMMU 8 / 32 and the adding stay FP64) */
+/* precision / form of the doubling and adding solves */
+#define PAMTRA_B200_PREC_FP64 0          /* FP64 in the reference's operation order: COMBINE_LAYERS4
+                                           (src/radintg4.f90:447-513) with its two inverses per
+                                           combine; the plain drop-in form */
+#define PAMTRA_B200_PREC_3XTF32 1        /* batched form: layer doubling products as 3xTF32 tcgen05
+                                           MMAs (NUMMU = 16; NUMMU 8 / 32 double in FP64), FP64
+                                           adding with one inverse per combine */
+#define PAMTRA_B200_PREC_FP64_BATCHED 2  /* batched form in FP64: as PREC_FP64, but each adding
+                                           combine derives the minus-side inverse from the
+                                           plus-side one (Gm R2 = R2 Gp, Gm = I + R2 Gp R1p):
+                                           one inverse and ten products instead of two and twelve */
 
 /* Settings: the nmlSet keys on the passive Mie path
  * (src/settings.f90:454-573; python/pyPamtra/core.py:89-157). */

@@ -15,8 +15,9 @@ from .packing import Settings, Species, SPECIES_DTYPE
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libpamtra_b200.so")
 
-PREC_FP64 = 0
-PREC_3XTF32 = 1
+PREC_FP64 = 0           # reference operation order (plain drop-in)
+PREC_3XTF32 = 1         # batched: 3xTF32 tensor-core doubling, one-inverse adding
+PREC_FP64_BATCHED = 2   # batched: FP64, one-inverse adding
 
 ST_NORM = 0x100
 ST_PSD = 0x200

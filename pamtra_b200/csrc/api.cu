@@ -439,6 +439,9 @@ static int set_smem_attrs() {
     set((const void*)k_adding<8>, sizeof(AddSmem<8>));
     set((const void*)k_adding<16>, sizeof(AddSmem<16>));
     set((const void*)k_adding<32>, sizeof(AddSmem<32>));
+    set((const void*)k_adding<8, true>, sizeof(AddSmem<8>));
+    set((const void*)k_adding<16, true>, sizeof(AddSmem<16>));
+    set((const void*)k_adding<32, true>, sizeof(AddSmem<32>));
     set((const void*)k_minvert<64>, Team<64>::MAT * 8 + sizeof(InvScratch<64>));
   });
   return rc;
@@ -659,7 +662,10 @@ int32_t pamtra_b200_stage_ms(pamtra_b200_ctx* ctx, float* ms, int32_t n) {
 int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, const pamtra_b200_columns* cols,
                         const pamtra_b200_outputs* out, int32_t precision, void* stream_) {
   if (!ctx || !st || !cols || !out || !out->tb) return PAMTRA_B200_FATAL;
-  if (precision != PAMTRA_B200_PREC_FP64 && precision != PAMTRA_B200_PREC_3XTF32) return PAMTRA_B200_FATAL;
+  if (precision != PAMTRA_B200_PREC_FP64 && precision != PAMTRA_B200_PREC_3XTF32 &&
+      precision != PAMTRA_B200_PREC_FP64_BATCHED)
+    return PAMTRA_B200_FATAL;
+  const bool one_inv = precision != PAMTRA_B200_PREC_FP64;  // one inverse per adding combine
   if (cols->ncol < 1 || cols->max_nlyrs < 2 || cols->max_nfreq < 1 || cols->noutlevels < 1 || cols->nhydro < 0)
     return PAMTRA_B200_FATAL;
   if (cols->nhydro > 0 && !cols->species) return PAMTRA_B200_FATAL;
@@ -799,7 +805,9 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     if (H > 0) { k_layer<8><<<g, RTCfg<8>::T, sizeof(LayerSmem<8>), stream>>>(b, w, *st, ssp); launches++; }
     mark(ctx, stream, STG_LAYER);
     g = persistent_grid((const void*)k_adding<8>, RTCfg<8>::T, sizeof(AddSmem<8>), sms, ctx->adding_cps);
-    k_adding<8><<<g, RTCfg<8>::T, sizeof(AddSmem<8>), stream>>>(b, w, *st, *out); launches++;
+    if (one_inv) k_adding<8, true><<<g, RTCfg<8>::T, sizeof(AddSmem<8>), stream>>>(b, w, *st, *out);
+    else k_adding<8><<<g, RTCfg<8>::T, sizeof(AddSmem<8>), stream>>>(b, w, *st, *out);
+    launches++;
     mark(ctx, stream, STG_ADDING);
   }
   if (mask & 2) {
@@ -815,7 +823,9 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     }
     mark(ctx, stream, STG_LAYER);
     const int g = persistent_grid((const void*)k_adding<16>, RTCfg<16>::T, sizeof(AddSmem<16>), sms, ctx->adding_cps);
-    k_adding<16><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out); launches++;
+    if (one_inv) k_adding<16, true><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out);
+    else k_adding<16><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out);
+    launches++;
     mark(ctx, stream, STG_ADDING);
   }
   if (mask & 4) {
@@ -824,7 +834,9 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     mark(ctx, stream, STG_LAYER);
     g = std::min(persistent_grid((const void*)k_adding<32>, RTCfg<32>::T, sizeof(AddSmem<32>), sms, ctx->adding_cps),
                  pl.add_grid);
-    k_adding<32><<<g, RTCfg<32>::T, sizeof(AddSmem<32>), stream>>>(b, w, *st, *out); launches++;
+    if (one_inv) k_adding<32, true><<<g, RTCfg<32>::T, sizeof(AddSmem<32>), stream>>>(b, w, *st, *out);
+    else k_adding<32><<<g, RTCfg<32>::T, sizeof(AddSmem<32>), stream>>>(b, w, *st, *out);
+    launches++;
     mark(ctx, stream, STG_ADDING);
   }
   if (out->angles_deg) { k_angles<<<1, 32, 0, stream>>>(out->angles_deg, ctx->lob_mu, cc.max_nummu); launches++; }

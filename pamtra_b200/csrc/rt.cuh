@@ -489,7 +489,7 @@ struct AddSmem {
   static constexpr int NS = (N == 32) ? 6 : 10;  // matrices in shared memory
   double m[NS][MAT];
   double sp[n], sm[n], s2p[n], s2m[n], t1[n], t2[n], nsp[n], nsm[n];
-  double wv[n], wv2[n];
+  double wv[n], wv2[n], u1[n], u2[n];
   double sky[n], gnd[n], uprad[n], dnrad[n];
   double mu[N], wq[N];
   InvScratch<n> inv;
@@ -518,7 +518,7 @@ __device__ __forceinline__ void ew_diag(double* A, const double* d) {
   }
 }
 
-template <int N>
+template <int N, bool ONE_INV = false>
 __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_b200_settings st,
                                                         pamtra_b200_outputs out) {
   constexpr int n = RTCfg<N>::n, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT, T = RTCfg<N>::T;
@@ -638,6 +638,66 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
         team_sync();
         if (t < n) { S.sp[t] = S.nsp[t]; S.sm[t] = S.nsm[t]; }
         sstate = 2;
+        team_sync();
+        continue;
+      }
+      if (ONE_INV) {
+        // ---- COMBINE_LAYERS4 with one inverse.  With Gp = (I - R1p R2)^-1
+        // the minus-side inverse Gm = (I - R2 R1p)^-1 satisfies
+        //   Gm R2 = R2 Gp   and   Gm = I + R2 Gp R1p,
+        // so R1m' = R1m + T1m Gm R2 T1p = R1m + (T1m R2)(Gp T1p),
+        //    T1m' = T1m Gm T2 = T1m (T2 + R2 (Gp R1p T2)),
+        //    Gm w = w + R2 Gp (R1p w) for the S- chain:
+        // ten products and one inverse per combine instead of twelve and two.
+        mm<n, MM_SET>(Rp, R2, G);
+        team_sync();
+        {
+          int sg = 0;
+          double* gi = inv_iminus<n>(G, X, S.inv, &sg);
+          if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+          if (gi != G) { X = G; G = gi; }
+        }
+        mm<n, MM_SET>(Rp, T2, X);  // R1p T2
+        if (t < n) {
+          S.wv[t] = S.sp[t] + mv_row<n>(Rp, S.s2m, t);   // S+ chain
+          S.nsm[t] = S.s2m[t] + mv_row<n>(R2, S.sp, t);  // S- chain: w
+        }
+        team_sync();
+        mm<n, MM_SET>(G, X, Y);  // Y = Gp R1p T2
+        if (t < n) {
+          S.wv2[t] = mv_row<n>(G, S.wv, t);
+          S.u1[t] = mv_row<n>(Rp, S.nsm, t);
+        }
+        team_sync();
+        mm<n, MM_ACC>(T2, Y, Z, R2);  // new R+ = R2 + T2 Gp R1p T2
+        if (t < n) {
+          S.nsp[t] = S.s2p[t] + mv_row<n>(T2, S.wv2, t);
+          S.u2[t] = mv_row<n>(G, S.u1, t);
+        }
+        team_sync();
+        mm<n, MM_SET>(G, Tp, X);  // W = Gp T1p
+        if (t < n) S.u1[t] = S.nsm[t] + mv_row<n>(R2, S.u2, t);  // Gm w
+        team_sync();
+        mm<n, MM_SET>(T2, X, Rp);  // new T+ = T2 W (old R+ is dead)
+        if (t < n) S.nsm[t] = S.sm[t] + mv_row<n>(Tm, S.u1, t);
+        team_sync();
+        mm<n, MM_SET>(Tm, R2, G);  // V = T1m R2 (Gp is dead)
+        team_sync();
+        mm<n, MM_ACC>(G, X, Rm, Rm);   // new R- = R1m + V W
+        mm<n, MM_ACC>(R2, Y, Tp, T2);  // U = T2 + R2 Y (old T+ is dead)
+        team_sync();
+        mm<n, MM_SET>(Tm, Tp, X);  // new T- = T1m U
+        team_sync();
+        {
+          // roles: new R+ = Z, new R- = Rm, new T+ = Rp, new T- = X
+          double *oRp = Rp, *oTp = Tp, *oTm = Tm, *oX = X, *oZ = Z;
+          Rp = oZ;
+          Tp = oRp;
+          Tm = oX;
+          Z = oTp;
+          X = oTm;
+        }
+        if (t < n) { S.sp[t] = S.nsp[t]; S.sm[t] = S.nsm[t]; }
         team_sync();
         continue;
       }

@@ -408,16 +408,18 @@ def test_split_precision_target_shape(native):
 
 
 def test_split_precision_uneven(native):
-    # NUMMU 16 columns take the tensor-core doubling, NUMMU 8 / 32 the FP64 one
-    from pamtra_b200._native import PREC_3XTF32, PREC_FP64
+    # NUMMU 16 columns take the tensor-core doubling, NUMMU 8 / 32 the FP64
+    # one; both forms share the one-inverse FP64 adding
+    from pamtra_b200._native import PREC_3XTF32, PREC_FP64, PREC_FP64_BATCHED
     b = wl.uneven_batch(24, seed=13, nfreq_range=(2, 5))
     f64 = _run_prec(b, PREC_FP64)
+    f64b = _run_prec(b, PREC_FP64_BATCHED)
     s = _run_prec(b, PREC_3XTF32)
     assert np.array_equal(s["status"], f64["status"])
     nmu = b.host["nummu"]
     d = np.abs(s["tb"] - f64["tb"])
     assert np.max(d) <= SPLIT_TB_TOL
-    assert np.all(d[nmu != 16] == 0.0)
+    assert np.array_equal(s["tb"][nmu != 16], f64b["tb"][nmu != 16])
 
 
 def test_split_precision_pairing_independent(native):
@@ -435,3 +437,34 @@ def test_split_precision_pairing_independent(native):
     assert np.array_equal(sub["tb"], full["tb"][1:])
     again = _run_prec(b, PREC_3XTF32)
     assert np.array_equal(again["tb"], full["tb"])
+
+
+# ----------------------------------------------------------------- batched FP64 form (one-inverse adding)
+def test_fp64_batched_form_matches_plain_order(oracle_mod, native):
+    # The batched FP64 form derives each combine's minus-side inverse from
+    # the plus-side one; it stays within 1e-10 K of the reference operation
+    # order, is run-to-run reproducible and matches the oracle.
+    from pamtra_b200._native import PREC_FP64, PREC_FP64_BATCHED
+    b = pbatch.pack_pam(wl.c2_pam(48, seed=41), wl.C2_FREQS)
+    ref = _run_prec(b, PREC_FP64)
+    got = _run_prec(b, PREC_FP64_BATCHED)
+    assert np.array_equal(got["status"], ref["status"])
+    assert np.max(np.abs(got["tb"] - ref["tb"])) < 1e-10
+    again = _run_prec(b, PREC_FP64_BATCHED)
+    assert np.array_equal(again["tb"], got["tb"])
+    for c in (0, 47):
+        err, t, _, _, _ = oracle_mod.run_column(oracle_mod.settings(b.settings), b.species, b.host, c, wl.C2_FREQS)
+        assert err == 0
+        assert np.max(np.abs(got["tb"][c] - t)) < TB_TOL
+
+
+def test_fp64_batched_form_uneven(native):
+    # every NUMMU and surface path through the one-inverse combine
+    from pamtra_b200._native import PREC_FP64, PREC_FP64_BATCHED
+    b = wl.uneven_batch(24, seed=43, nfreq_range=(2, 5))
+    ref = _run_prec(b, PREC_FP64)
+    got = _run_prec(b, PREC_FP64_BATCHED)
+    assert np.array_equal(got["status"], ref["status"])
+    ok = ref["status"] == 0
+    d = np.abs(got["tb"] - ref["tb"])
+    assert np.max(d) < 1e-10, np.max(d)
