@@ -88,7 +88,16 @@ typedef struct pamtra_b200_settings {
   int32_t hydro_limit_density_area;
   int32_t outpol_vh;                 /* nmlSet['outpol'] == 'VH' */
   int32_t nummu;                     /* default quadrature angles per hemisphere */
+  /* active "simple" radar (radar_mode 'simple', src/radar_simulator.f90:161-176) */
+  int32_t active;                    /* nmlSet['active']: fill outputs.ze / att_* */
+  int32_t radar_attenuation;         /* PAMTRA_B200_ATT_*: nmlSet['radar_attenuation'] */
+  double radar_k2;                   /* nmlSet['radar_k2'], |K|^2 of the radar equation */
 } pamtra_b200_settings;
+
+/* radar_attenuation codes */
+#define PAMTRA_B200_ATT_DISABLED 0
+#define PAMTRA_B200_ATT_BOTTOM_UP 1
+#define PAMTRA_B200_ATT_TOP_DOWN 2
 
 /* One descriptor-file row (python/pyPamtra/descriptorFile.py:19-20);
  * string fields are encoded: dist (PAMTRA_B200_DIST_*), scat = mie-sphere. */
@@ -129,6 +138,12 @@ typedef struct pamtra_b200_outputs {
   double* salbedo;       /* [ncol][max_nfreq][max_nlyrs] */
   double* scatter_matrix;/* [ncol][max_nfreq][max_nlyrs][4][n][n], n = 2*max_nummu, row=(i2,j2) */
   int32_t* num_doubles;  /* [ncol][max_nfreq][max_nlyrs] bottom-up, -1 = non-scattering */
+  /* simple radar (settings.active), [ncol][max_nfreq][max_nlyrs] bottom-up, NULL to skip:
+   * ze dBZ (-9999 where no hydrometeor or no backscatter), att_hydro / att_atmo
+   * one-way attenuation in dB (src/radar_simulator.f90:123-176, src/run_rt.f90:119-121) */
+  double* ze;
+  double* att_hydro;
+  double* att_atmo;
 } pamtra_b200_outputs;
 
 typedef struct pamtra_b200_ctx pamtra_b200_ctx;

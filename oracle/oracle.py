@@ -34,13 +34,16 @@ class OrcSettings(ctypes.Structure):
         ("hydro_limit_density_area", ctypes.c_int32),
         ("outpol_vh", ctypes.c_int32),
         ("nummu", ctypes.c_int32),
+        ("active", ctypes.c_int32),
+        ("radar_attenuation", ctypes.c_int32),
+        ("radar_k2", ctypes.c_double),
     ]
 
 
 class OrcDebug(ctypes.Structure):
     _fields_ = [(k, ctypes.c_void_p) for k in
                 ("kextatmo", "kexttot", "salbedo", "nlegen", "legen", "present", "scatter_matrix", "ext",
-                 "emis", "num_doubles")]
+                 "emis", "num_doubles", "back", "ze", "att_hydro", "att_atmo")]
 
 
 def build():
@@ -85,7 +88,9 @@ def settings(pk_settings):
 
 
 def run_column(st, species, cols, c, freqs, debug=False):
-    """Run column ``c`` of packed ``cols`` (pamtra_b200.packing.profile_columns)."""
+    """Run column ``c`` of packed ``cols`` (pamtra_b200.packing.profile_columns).
+    ``debug`` True returns all intermediates, "radar" only the simple-radar
+    outputs (back, ze, att_hydro, att_atmo; filled when ``st.active``)."""
     l = lib()
     L = int(cols["nlyrs"][c])
     Lmax = int(cols["max_nlyrs"])
@@ -104,12 +109,18 @@ def run_column(st, species, cols, c, freqs, debug=False):
     ang = np.zeros(2 * N)
     dbg = None
     out_dbg = None
-    if debug:
+    if debug == "radar":
+        out_dbg = dict(back=np.zeros((nf, L)), ze=np.zeros((nf, L)), att_hydro=np.zeros((nf, L)),
+                       att_atmo=np.zeros((nf, L)))
+        dbg = OrcDebug(**{k: v.ctypes.data for k, v in out_dbg.items()})
+    elif debug:
         n = 2 * N
         out_dbg = dict(kextatmo=np.zeros((nf, L)), kexttot=np.zeros((nf, L)), salbedo=np.zeros((nf, L)),
                        nlegen=np.zeros((nf, L), np.int32), legen=np.zeros((nf, L, 3, MAXNLEG)),
                        present=np.zeros(L, np.int32), scatter_matrix=np.zeros((nf, L, 4, n, n)),
-                       ext=np.zeros((nf, L)), emis=np.zeros((nf, L)), num_doubles=np.zeros((nf, L), np.int32))
+                       ext=np.zeros((nf, L)), emis=np.zeros((nf, L)), num_doubles=np.zeros((nf, L), np.int32),
+                       back=np.zeros((nf, L)), ze=np.zeros((nf, L)), att_hydro=np.zeros((nf, L)),
+                       att_atmo=np.zeros((nf, L)))
         dbg = OrcDebug(**{k: v.ctypes.data for k, v in out_dbg.items()})
     sp = np.ascontiguousarray(species)
     refl = bytes([int(cols["sfc_refl"][c]) & 0xFF])
@@ -138,13 +149,24 @@ def run_pamtra(pam, freqs, nummu=16, debug=False):
     err_all = 0
     ang = None
     dbgs = []
+    Lm, nf = int(cols["max_nlyrs"]), len(freqs)
+    ze = np.full((nx * ny, Lm, nf), -9999.0)
+    ath = np.zeros((nx * ny, Lm, nf))
+    ata = np.zeros((nx * ny, Lm, nf))
     for c in range(nx * ny):
-        err, t, e, a, d = run_column(st, sp, cols, c, freqs, debug)
+        err, t, e, a, d = run_column(st, sp, cols, c, freqs, debug or ("radar" if st.active else False))
         err_all = max(err_all, err)
         tb[c], em[c], ang = t, e, a
+        if st.active:
+            L = int(cols["nlyrs"][c])
+            ze[c, :L], ath[c, :L], ata[c, :L] = d["ze"].T, d["att_hydro"].T, d["att_atmo"].T
         dbgs.append(d)
     r = dict(tb=tb.reshape(nx, ny, nout, 2 * N, len(freqs), 2),
              emissivity=em.reshape(nx, ny, 2, len(freqs), N), angles_deg=ang)
+    if st.active:
+        r["Ze"] = ze.reshape(nx, ny, Lm, nf, 1, 1)
+        r["Att_hydro"] = ath.reshape(nx, ny, Lm, nf, 1)
+        r["Att_atmo"] = ata.reshape(nx, ny, Lm, nf)
     if debug:
         r["debug"] = dbgs
     return r, err_all

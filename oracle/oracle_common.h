@@ -93,6 +93,9 @@ typedef struct {
   int32_t hydro_limit_density_area;
   int32_t outpol_vh;
   int32_t nummu;
+  int32_t active;             // nmlSet['active'] (simple radar)
+  int32_t radar_attenuation;  // 0 disabled, 1 bottom-up, 2 top-down
+  double radar_k2;            // nmlSet['radar_k2']
 } orc_settings;
 
 // One descriptor-file row (python/pyPamtra/descriptorFile.py:19-20).
@@ -117,6 +120,10 @@ typedef struct {
   double* ext;             // [nfreq][L]            extinction matrix diagonal
   double* emis;            // [nfreq][L]            emission vector I component
   int32_t* num_doubles;    // [nfreq][L]            bottom-up order
+  double* back;            // [nfreq][L]            volumetric backscattering cross section, m^2/m^3
+  double* ze;              // [nfreq][L]            simple radar, dBZ (-9999 without hydrometeors)
+  double* att_hydro;       // [nfreq][L]            dB
+  double* att_atmo;        // [nfreq][L]            dB
 } orc_debug;
 
 }

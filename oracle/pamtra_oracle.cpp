@@ -1306,6 +1306,51 @@ void internal_radiance(int n, const Layer& up, const Layer& dn, const double* in
 }
 
 // src/rt_utilities.f90:687-735 CONVERT_OUTPUT (UNITS='T', FLUXCODE=0)
+// Simple radar of one column at one frequency: src/radar_simulator.f90:123-176
+// (radar_mode 'simple', polarisation NN, radar_nPeaks = 1) called per layer
+// with hydrometeors in the layer order of src/hydrometeor_extinction.f90:96-106
+// (top-down when radar_attenuation = 'top-down'), and the gas attenuation of
+// src/run_rt.f90:119-121.  Initial values as src/vars_output.f90:150-152.
+void radar_simple(const orc_settings& st, int L, double freq, const std::vector<double>& hgt_lev,
+                  const std::vector<int>& present, const std::vector<double>& kexthydro,
+                  const std::vector<double>& back, const std::vector<double>& kextatmo, std::vector<double>& ze,
+                  std::vector<double>& att_hydro, std::vector<double>& att_atmo) {
+  ze.assign(L, -9999.0);
+  att_hydro.assign(L, 0.0);
+  att_atmo.assign(L, 0.0);
+  std::vector<double> dh(L);
+  for (int z = 0; z < L; z++) {
+    dh[z] = hgt_lev[z + 1] - hgt_lev[z];
+    att_atmo[z] = 10.0 * std::log10(std::exp(kextatmo[z] * dh[z]));
+  }
+  const double K2 = st.radar_k2;
+  const double wavelength = C_LIGHT / (freq * 1.e9);
+  const double pi5 = (PI * PI) * (PI * PI) * PI, w2 = wavelength * wavelength, w4 = w2 * w2;
+  const bool down = st.radar_attenuation == 2;
+  for (int k = 0; k < L; k++) {
+    const int iz = down ? L - 1 - k : k;
+    if (!present[iz]) continue;
+    att_hydro[iz] = 10.0 * std::log10(std::exp(kexthydro[iz] * dh[iz]));
+    double ze_back = 1.e18 * (1.0 / (K2 * pi5)) * back[iz] * w4;
+    double pia = 0.0;
+    if (st.radar_attenuation != 0) {
+      if (k > 0) {
+        double sh = 0.0, sa = 0.0;
+        for (int j = 0; j < k; j++) {
+          const int jz = down ? L - 1 - j : j;
+          sh = sh + att_hydro[jz];
+          sa = sa + att_atmo[jz];
+        }
+        pia = 2 * (sh + sa);
+      }
+      pia = pia + att_hydro[iz] + att_atmo[iz];
+    }
+    pia = std::pow(10.0, 0.1 * pia);
+    ze_back = ze_back / pia;
+    ze[iz] = (ze_back == 0.0) ? -9999.0 : 10 * std::log10(ze_back);
+  }
+}
+
 double rad_to_tb(double rad, double wl) {
   if (rad > 0.0) return 1.4388e4 / (wl * std::log(1.0 + 1.1911e8 / (rad * p5(wl))));
   if (rad == 0.0) return 0.0;
@@ -1399,9 +1444,9 @@ int orc_run_column(const orc_settings* st, const orc_species* sp, int nhydro, in
         if (gas_r98(freq, a.temp[z], a.rho_vap[z], a.press[z], &kgas[z])) return 2;
     // hydrometeors (src/hydrometeor_extinction.f90)
     std::vector<std::vector<double>> scat(L);
-    std::vector<double> extk(L, 0.0), emk(L, 0.0);
+    std::vector<double> extk(L, 0.0), emk(L, 0.0), kext_h(L, 0.0), back_h(L, 0.0);
     for (int z = 0; z < L; z++) {
-      double kexttot = 0.0, salbedo = 0.0;
+      double kexttot = 0.0, salbedo = 0.0, backtot = 0.0;
       double legen_coef[3][MAXNLEG];
       std::memset(legen_coef, 0, sizeof(legen_coef));
       int nlegen_coef = 0;
@@ -1435,6 +1480,7 @@ int orc_run_column(const orc_settings* st, const orc_species* sp, int nhydro, in
         if (calc_mie_spheres(*st, freq * 1e9, s.liq_ice, bn, ndens, refre, refim, mo)) return 2;
         nlegen_coef = std::max(nlegen_coef, mo.nlegen);
         kexttot = kexttot + mo.kext;
+        backtot = backtot + mo.back;  // rt_back (scatProperties.f90:922)
         if (kexttot == 0.0) salbedo = 0.0;
         else salbedo = salbedo + (mo.salb * mo.kext);
         if (nlegen_coef > 0)
@@ -1443,6 +1489,8 @@ int orc_run_column(const orc_settings* st, const orc_species* sp, int nhydro, in
         if (kexttot < 0.0 || std::isnan(kexttot)) return 2;
         if (nlegen_coef > MAXNLEG - 1) return 2;
       }
+      kext_h[z] = kexttot;
+      back_h[z] = backtot;
       // finalize_rt3_scatProperties
       salbedo = salbedo / kexttot;
       for (int k = 0; k < 3; k++)
@@ -1471,6 +1519,17 @@ int orc_run_column(const orc_settings* st, const orc_species* sp, int nhydro, in
     }
     if (dbg && dbg->present && fi == 0)
       for (int z = 0; z < L; z++) dbg->present[z] = present[z];
+    if (dbg && st->active) {
+      std::vector<double> ze, ath, ata;
+      radar_simple(*st, L, freq, a.hgt_lev, present, kext_h, back_h, kgas, ze, ath, ata);
+      for (int z = 0; z < L; z++) {
+        size_t o = (size_t)fi * L + z;
+        if (dbg->back) dbg->back[o] = back_h[z];
+        if (dbg->ze) dbg->ze[o] = ze[z];
+        if (dbg->att_hydro) dbg->att_hydro[o] = ath[z];
+        if (dbg->att_atmo) dbg->att_atmo[o] = ata[z];
+      }
+    }
 
     // rt4: flip to top-down (src/rt4.f90:274-305) and radtran4
     std::vector<Layer> lay(L + 1);

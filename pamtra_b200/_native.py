@@ -45,7 +45,8 @@ class Columns(ctypes.Structure):
 class Outputs(ctypes.Structure):
     """Mirror of ``pamtra_b200_outputs``."""
     _fields_ = [("tb", _vp), ("emissivity", _vp), ("angles_deg", _vp), ("status", _vp), ("kextatmo", _vp),
-                ("kexttot", _vp), ("salbedo", _vp), ("scatter_matrix", _vp), ("num_doubles", _vp)]
+                ("kexttot", _vp), ("salbedo", _vp), ("scatter_matrix", _vp), ("num_doubles", _vp),
+                ("ze", _vp), ("att_hydro", _vp), ("att_atmo", _vp)]
 
 
 EXPORTS = ["pamtra_b200_create", "pamtra_b200_destroy", "pamtra_b200_workspace_bytes", "pamtra_b200_reserve",
@@ -168,7 +169,7 @@ class Engine(object):
     def make_outputs(outs):
         o = Outputs()
         for k in ("tb", "emissivity", "angles_deg", "status", "kextatmo", "kexttot", "salbedo", "scatter_matrix",
-                  "num_doubles"):
+                  "num_doubles", "ze", "att_hydro", "att_atmo"):
             setattr(o, k, _ptr(outs.get(k)))
         return o
 

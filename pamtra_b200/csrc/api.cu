@@ -173,6 +173,58 @@ __global__ void k_ssp_out(Batch b, Work w, pamtra_b200_outputs out) {
   if (out.num_doubles) out.num_doubles[idx] = (p >= 0) ? w.lay_nd[item] : -1;
 }
 
+// Simple radar per (column, frequency): src/radar_simulator.f90:123-176
+// (radar_mode 'simple', one polarisation, no noise) over the layers in the
+// reference's loop order (top-down when the attenuation is integrated from
+// the top, src/hydrometeor_extinction.f90:96-106), with the gas attenuation
+// of src/run_rt.f90:119-121.  Layers without hydrometeors keep Ze = -9999
+// and zero hydrometeor attenuation.
+__global__ void k_radar(Batch b, Work w, pamtra_b200_settings st, pamtra_b200_outputs out) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
+  if (u >= b.ncol * Fm) return;
+  const int c = u / Fm, f = u % Fm;
+  const size_t o = ((size_t)c * Fm + f) * Lm;
+  const int L = (f < b.col_nfreq(c)) ? b.nlyrs[c] : 0;
+  for (int z = 0; z < Lm; z++) {
+    if (out.ze) out.ze[o + z] = -9999.0;
+    if (out.att_hydro) out.att_hydro[o + z] = 0.0;
+    if (out.att_atmo) out.att_atmo[o + z] = 0.0;
+  }
+  if (L == 0) return;
+  const double* hl = w.hgt_lev + (size_t)c * (Lm + 1);
+  const double wavelength = C_LIGHT / (b.freq(c, f) * 1.e9);  // m
+  const double K2 = st.radar_k2;
+  const bool down = st.radar_attenuation == PAMTRA_B200_ATT_TOP_DOWN;
+  const double pi2 = PI * PI, w2 = wavelength * wavelength;
+  const double pi5 = (pi2 * pi2) * PI, w4 = w2 * w2;  // pi**5, wavelength**4
+  double acc_h = 0.0, acc_a = 0.0;  // hydrometeor / gas attenuation of the layers already passed (dB)
+  for (int k = 0; k < L; k++) {
+    const int z = down ? L - 1 - k : k;
+    const double dh = hl[z + 1] - hl[z];
+    const double att_atmo = 10.0 * log10(exp(w.kgas[((size_t)c * Fm + f) * Lm + z] * dh));
+    if (out.att_atmo) out.att_atmo[o + z] = att_atmo;
+    const int p = w.pres_idx[(size_t)c * Lm + z];
+    double att_hydro = 0.0;
+    if (p >= 0) {
+      const size_t item = (size_t)p * Fm + f;
+      att_hydro = 10.0 * log10(exp(w.m_kext[item] * dh));
+      double ze_back = 1.e18 * (1.0 / (K2 * pi5)) * w.m_back[item] * w4;
+      double pia = 0.0;
+      if (st.radar_attenuation != PAMTRA_B200_ATT_DISABLED) {
+        if (k > 0) pia = 2.0 * (acc_h + acc_a);
+        pia = pia + att_hydro + att_atmo;
+      }
+      pia = pow(10.0, 0.1 * pia);
+      ze_back = ze_back / pia;
+      if (out.att_hydro) out.att_hydro[o + z] = att_hydro;
+      if (out.ze) out.ze[o + z] = (ze_back == 0.0) ? -9999.0 : 10.0 * log10(ze_back);
+    }
+    acc_h = acc_h + att_hydro;
+    acc_a = acc_a + att_atmo;
+  }
+}
+
 __global__ void k_status_out(Work w, int32_t* out, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) out[i] = w.status[i];
@@ -182,7 +234,8 @@ struct Plan {
   size_t total;
   size_t o_hgt_lev, o_temp_lev, o_temp, o_press, o_rho_vap, o_q_hum, o_gtemp, o_outlev, o_kgas;
   size_t o_slot_st, o_slot_nb, o_bd, o_bdd, o_bnd, o_brho, o_bmass;
-  size_t o_pres_idx, o_plist, o_counters, o_mkext, o_msalb, o_mnleg, o_mlegen, o_lay, o_laynd, o_status, o_colst;
+  size_t o_pres_idx, o_plist, o_counters, o_mkext, o_msalb, o_mback, o_mnleg, o_mlegen, o_lay, o_laynd, o_status,
+      o_colst;
   size_t o_species, o_addscr;
   int add_grid;  // CTAs of k_adding<32> the scratch is sized for
   int pmax;
@@ -235,6 +288,7 @@ Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms) {
   const size_t items = (size_t)std::max(1, p.pmax) * Fm;
   p.o_mkext = take(items * 8);
   p.o_msalb = take(items * 8);
+  p.o_mback = take(items * 8);
   p.o_mnleg = take(items * 4);
   p.o_mlegen = take(items * 3 * MAXNLEG * 8);
   p.o_lay = take(items * p.lay_stride * 8);
@@ -736,6 +790,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   w.pres_idx = (int*)(A + pl.o_pres_idx); w.plist = (int*)(A + pl.o_plist); w.pmax = pl.pmax;
   w.counters = (int*)(A + pl.o_counters);
   w.m_kext = (double*)(A + pl.o_mkext); w.m_salb = (double*)(A + pl.o_msalb); w.m_nleg = (int*)(A + pl.o_mnleg);
+  w.m_back = (double*)(A + pl.o_mback);
   w.m_legen = (double*)(A + pl.o_mlegen);
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
@@ -844,6 +899,9 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     k_ssp_out<<<(unsigned)((ngas + 255) / 256), 256, 0, stream>>>(b, w, *out); launches++;
   }
   if (out->kextatmo) cudaMemcpyAsync(out->kextatmo, w.kgas, ngas * 8, cudaMemcpyDeviceToDevice, stream);
+  if (st->active && (out->ze || out->att_hydro || out->att_atmo)) {
+    k_radar<<<(unsigned)((C * Fm + 127) / 128), 128, 0, stream>>>(b, w, *st, *out); launches++;
+  }
   if (out->status) {
     k_status_out<<<(unsigned)((C * Fm + 255) / 256), 256, 0, stream>>>(w, out->status, (int)(C * Fm)); launches++;
   }
@@ -887,6 +945,9 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
   size_t o_sa = add(nullptr, ho->salbedo ? C * Fm * Lm * 8 : 0);
   size_t o_sc = add(nullptr, ho->scatter_matrix ? C * Fm * Lm * 4 * NA * NA * 8 : 0);
   size_t o_nd = add(nullptr, ho->num_doubles ? C * Fm * Lm * 4 : 0);
+  size_t o_ze = add(nullptr, ho->ze ? C * Fm * Lm * 8 : 0);
+  size_t o_ah = add(nullptr, ho->att_hydro ? C * Fm * Lm * 8 : 0);
+  size_t o_aa = add(nullptr, ho->att_atmo ? C * Fm * Lm * 8 : 0);
   if (off > ctx->stage_bytes) {
     cudaStreamSynchronize(stream);
     cudaFree(ctx->stage);
@@ -927,6 +988,9 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
   dout.salbedo = ho->salbedo ? (double*)(D + o_sa) : nullptr;
   dout.scatter_matrix = ho->scatter_matrix ? (double*)(D + o_sc) : nullptr;
   dout.num_doubles = ho->num_doubles ? (int32_t*)(D + o_nd) : nullptr;
+  dout.ze = ho->ze ? (double*)(D + o_ze) : nullptr;
+  dout.att_hydro = ho->att_hydro ? (double*)(D + o_ah) : nullptr;
+  dout.att_atmo = ho->att_atmo ? (double*)(D + o_aa) : nullptr;
   if (dout.scatter_matrix) cudaMemsetAsync(dout.scatter_matrix, 0, C * Fm * Lm * 4 * NA * NA * 8, stream);
   int32_t rc = pamtra_b200_run(ctx, st, &dc, &dout, precision, stream);
   if (rc != PAMTRA_B200_OK) return rc;
@@ -940,6 +1004,9 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
   if (ho->scatter_matrix)
     cudaMemcpyAsync(ho->scatter_matrix, dout.scatter_matrix, C * Fm * Lm * 4 * NA * NA * 8, cudaMemcpyDeviceToHost, stream);
   if (ho->num_doubles) cudaMemcpyAsync(ho->num_doubles, dout.num_doubles, C * Fm * Lm * 4, cudaMemcpyDeviceToHost, stream);
+  if (ho->ze) cudaMemcpyAsync(ho->ze, dout.ze, C * Fm * Lm * 8, cudaMemcpyDeviceToHost, stream);
+  if (ho->att_hydro) cudaMemcpyAsync(ho->att_hydro, dout.att_hydro, C * Fm * Lm * 8, cudaMemcpyDeviceToHost, stream);
+  if (ho->att_atmo) cudaMemcpyAsync(ho->att_atmo, dout.att_atmo, C * Fm * Lm * 8, cudaMemcpyDeviceToHost, stream);
   if (cudaStreamSynchronize(stream) != cudaSuccess) return PAMTRA_B200_FATAL;
   return PAMTRA_B200_OK;
 }
@@ -1103,6 +1170,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   w.pres_idx = (int*)(A + pl.o_pres_idx); w.plist = (int*)(A + pl.o_plist); w.pmax = pl.pmax;
   w.counters = (int*)(A + pl.o_counters);
   w.m_kext = (double*)(A + pl.o_mkext); w.m_salb = (double*)(A + pl.o_msalb); w.m_nleg = (int*)(A + pl.o_mnleg);
+  w.m_back = (double*)(A + pl.o_mback);
   w.m_legen = (double*)(A + pl.o_mlegen);
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
@@ -1137,6 +1205,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   if (out->kexttot || out->salbedo || out->num_doubles)
     k_ssp_out<<<(unsigned)((Fm * Lm + 255) / 256), 256, 0, stream>>>(b, w, *out);
   if (out->kextatmo) cudaMemcpyAsync(out->kextatmo, w.kgas, Fm * Lm * 8, cudaMemcpyDeviceToDevice, stream);
+  if (st->active && (out->ze || out->att_hydro || out->att_atmo)) k_radar<<<1, 128, 0, stream>>>(b, w, *st, *out);
   if (out->status) k_status_out<<<1, 256, 0, stream>>>(w, out->status, (int)Fm);
   return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
 }

@@ -210,7 +210,7 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
     const double wl = C_LIGHT / (freq * 1e9);
     const double T = w.temp[(size_t)c * Lm + z];
     for (int jj = lane; jj < MAXNLEG; jj += 32) { S.legc[0][jj] = 0.0; S.legc[1][jj] = 0.0; S.legc[2][jj] = 0.0; }
-    double kexttot = 0.0, salbedo = 0.0;
+    double kexttot = 0.0, salbedo = 0.0, backtot = 0.0;
     int nlegen_coef = 0;
     int status = 0;
     for (int h = 0; h < H; h++) {
@@ -381,9 +381,11 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
         status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_MIE;
         break;
       }
-      // species sums (scatProperties.f90:920-949)
+      // species sums (scatProperties.f90:920-949); the backscattering sum is
+      // radar_simulator's input (mie_spheres.f90:263, scatProperties.f90:922)
       nlegen_coef = max(nlegen_coef, nlegen_h);
       kexttot = kexttot + extinction;
+      backtot = backtot + sqb;
       if (kexttot == 0.0) salbedo = 0.0;
       else salbedo = salbedo + (salb_h * extinction);
       for (int jj = lane; jj < nlegen_coef; jj += 32) {
@@ -409,6 +411,7 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
     if (lane == 0) {
       w.m_kext[item] = kexttot;
       w.m_salb[item] = salbedo;
+      w.m_back[item] = backtot;
       w.m_nleg[item] = nlegen_coef;
       if (w.wt_need && nlegen_coef > 0) {
         const int numpts = 2 * ((nlegen_coef + 1) / 2) + 4;

@@ -54,6 +54,7 @@ struct Work {
   int* counters;                       // [16] 0: P, 1: mie work, 2: rt work, 3: adding work
   // single-scattering per item
   double *m_kext, *m_salb;             // [pmax*Fm]
+  double* m_back;                      // [pmax*Fm] volumetric backscattering cross section, m^2/m^3
   int* m_nleg;                         // [pmax*Fm]
   double* m_legen;                     // [pmax*Fm][3][MAXNLEG]
   // layer R, T, S per item (R,T padded n x (n+2), symmetric +/-)

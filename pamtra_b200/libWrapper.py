@@ -4,8 +4,10 @@
 Same signature and return value ``(results, pamError[, module])``; results
 carry the passive keys of ``pyPamtra.r`` (``tb``, ``emissivity``,
 ``angles_deg``; with ``save_ssp`` also ``kextatmo``, ``scatter_matrix``,
-``extinct_matrix``, ``emis_vector``) and the active keys filled with -9999
-as the reference does for unallocated outputs (libWrapper.py:214-223).
+``extinct_matrix``, ``emis_vector``); with ``active`` (radar_mode 'simple')
+``Ze``, ``Att_hydro``, ``Att_atmo`` and ``radar_hgt``; the other active keys
+filled with -9999 as the reference does for unallocated outputs
+(libWrapper.py:214-223).
 """
 
 import numpy as np
@@ -76,6 +78,9 @@ def PamtraFortranWrapper(sets, nmlSets, descriptorFile, descriptorFile4D, descri
         out["kexttot"] = np.zeros((ncol, nf, L))
         out["salbedo"] = np.zeros((ncol, nf, L))
         out["scatter_matrix"] = np.zeros((ncol, nf, L, 4, 2 * N, 2 * N))
+    if st.active:
+        for k in ("ze", "att_hydro", "att_atmo"):
+            out[k] = np.zeros((ncol, nf, L))
     mask = {8: 1, 16: 2, 32: 4}[N]
     eng = engine(device)
     c = eng.make_columns(arrs, sp, nmu_mask=mask, max_present=present_bound(cols, descriptorFile), max_nummu=N)
@@ -90,6 +95,23 @@ def PamtraFortranWrapper(sets, nmlSets, descriptorFile, descriptorFile4D, descri
     results["status"] = out["status"].reshape(nx, ny, nf)
     for k in ACTIVE_KEYS:
         results[k] = -9999 if k == "radar_quality" else missingNumber
+    if st.active:
+        # simple radar (src/radar_simulator.f90:161-176): Ze per polarisation;
+        # Mie spheres give the same backscatter for NN/HH/VV and none for HV/VH
+        # (src/scatProperties.f90:746-756)
+        pols = list(sets.get("radar_pol", ["NN"]))
+        ze = out["ze"].transpose(0, 2, 1)  # (ncol, L, nf)
+        zp = np.stack([ze if p.strip() in ("NN", "HH", "VV") else np.full_like(ze, missingNumber) for p in pols],
+                      axis=-1)
+        results["Ze"] = zp.reshape(nx, ny, L, nf, len(pols), 1)
+        results["Att_hydro"] = out["att_hydro"].transpose(0, 2, 1).reshape(nx, ny, L, nf, 1)
+        results["Att_atmo"] = out["att_atmo"].transpose(0, 2, 1).reshape(nx, ny, L, nf)
+        hgt = cols["hgt"].copy()
+        lev = cols["hgt_lev"]
+        mid = 0.5 * (lev[:, 1:] + lev[:, :-1])
+        hgt = np.where(np.isnan(hgt), mid, hgt)
+        valid = np.arange(L)[None, :] < cols["nlyrs"][:, None]
+        results["radar_hgt"] = np.where(valid, hgt, missingNumber).reshape(nx, ny, L)
     if save_ssp:
         # the reference keeps the values of the last column and frequency computed
         # (src/run_rt.f90:140-146, loop order pyPamtraLib.f90:119-133)

@@ -17,6 +17,8 @@ DIST_CODES = {"exp": 0, "exp_field_t": 1, "mgamma": 2, "mono": 3, "exp_cosmo_sno
 SCAT_CODES = {"mie-sphere": 0, "disabled": 1}
 
 MAXNLEG = 200
+# radar_attenuation codes (PAMTRA_B200_ATT_*)
+RADAR_ATTENUATION = {"disabled": 0, "bottom-up": 1, "top-down": 2}
 
 
 class Settings(ctypes.Structure):
@@ -35,6 +37,9 @@ class Settings(ctypes.Structure):
         ("hydro_limit_density_area", ctypes.c_int32),
         ("outpol_vh", ctypes.c_int32),
         ("nummu", ctypes.c_int32),
+        ("active", ctypes.c_int32),
+        ("radar_attenuation", ctypes.c_int32),
+        ("radar_k2", ctypes.c_double),
     ]
 
 
@@ -92,6 +97,14 @@ def settings_from_nml(nmlSet, nummu=16):
     s.hydro_limit_density_area = int(bool(nmlSet["hydro_limit_density_area"]))
     s.outpol_vh = int(outpol == "VH")
     s.nummu = int(nummu)
+    s.active = int(bool(nmlSet.get("active", False)))
+    att = str(nmlSet.get("radar_attenuation", "disabled")).strip()
+    if att not in RADAR_ATTENUATION:
+        raise ValueError("radar_attenuation must be one of %s" % sorted(RADAR_ATTENUATION))
+    s.radar_attenuation = RADAR_ATTENUATION[att]
+    s.radar_k2 = float(nmlSet.get("radar_k2", 0.93))
+    if s.active and str(nmlSet.get("radar_mode", "simple")).strip() != "simple":
+        raise NotImplementedError("radar_mode %r: only 'simple' is on this path" % nmlSet["radar_mode"])
     return s
 
 

@@ -468,3 +468,44 @@ def test_fp64_batched_form_uneven(native):
     ok = ref["status"] == 0
     d = np.abs(got["tb"] - ref["tb"])
     assert np.max(d) < 1e-10, np.max(d)
+
+
+# ----------------------------------------------------------------- simple radar (active, radar_mode 'simple')
+def test_simple_radar_golden_fixture(oracle_mod, native):
+    # Ze and Att_hydro of the reference's golden scenario (its nmlSet has
+    # active=True, radar_mode='simple'), through the pyPamtra facade
+    pam = wl.golden_pam()
+    pam.runPamtra(wl.GOLDEN_FREQS)
+    gold = np.load(GOLDEN)
+    np.testing.assert_allclose(pam.r["Ze"], gold["Ze"], rtol=1e-5)
+    np.testing.assert_allclose(pam.r["Att_hydro"], gold["Att_hydro"], rtol=1e-5)
+    ref, err = oracle_mod.run_pamtra(wl.golden_pam(), wl.GOLDEN_FREQS)
+    assert err == 0
+    np.testing.assert_allclose(pam.r["Ze"], ref["Ze"], rtol=REL_TOL, atol=1e-12)
+    np.testing.assert_allclose(pam.r["Att_hydro"], ref["Att_hydro"], rtol=REL_TOL, atol=1e-15)
+    np.testing.assert_allclose(pam.r["Att_atmo"], ref["Att_atmo"], rtol=REL_TOL, atol=1e-15)
+
+
+@pytest.mark.parametrize("attenuation", ["bottom-up", "top-down"])
+def test_simple_radar_path_integrated_attenuation(oracle_mod, native, attenuation):
+    # two-way path-integrated attenuation from the surface or from the top
+    # (src/radar_simulator.f90:130-156), over columns with clouds and rain
+    pam = wl.c1_pam()
+    pam.nmlSet["radar_attenuation"] = attenuation
+    pam.nmlSet["radar_polarisation"] = "NN,HV"
+    pam.runPamtra(wl.C1_FREQS)
+    p2 = wl.c1_pam()
+    p2.nmlSet["radar_attenuation"] = attenuation
+    ref, err = oracle_mod.run_pamtra(p2, wl.C1_FREQS)
+    assert err == 0
+    ze = pam.r["Ze"]
+    assert ze.shape[-2:] == (2, 1)
+    np.testing.assert_allclose(ze[..., 0:1, :], ref["Ze"], rtol=REL_TOL, atol=1e-12)
+    assert np.all(ze[..., 1, :] == -9999.0)  # no cross-polar backscatter from spheres
+    np.testing.assert_allclose(pam.r["Att_hydro"], ref["Att_hydro"], rtol=REL_TOL, atol=1e-15)
+    np.testing.assert_allclose(pam.r["Att_atmo"], ref["Att_atmo"], rtol=REL_TOL, atol=1e-15)
+    # attenuation lowers the reflectivity where hydrometeors lie beyond
+    p3 = wl.c1_pam()
+    p3.runPamtra(wl.C1_FREQS)
+    has = ze[..., 0, 0] > -9999
+    assert np.all(ze[..., 0, 0][has] <= p3.r["Ze"][..., 0, 0][has] + 1e-12)

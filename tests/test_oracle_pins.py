@@ -100,3 +100,19 @@ def test_c1_oracle_runs(oracle_mod):
     d = r["debug"][0]
     assert list(np.nonzero(d["present"])[0]) == list(range(5, 26))
     assert np.all(d["num_doubles"][:, 5:26] > 0)
+
+
+def test_oracle_simple_radar_matches_golden(oracle_mod):
+    # the reference's golden scenario runs the active 'simple' radar beside
+    # the passive path (nmlSet active=True, radar_mode='simple'); its Ze and
+    # Att_hydro pin the oracle's restatement of radar_simulator at the
+    # reference test's tolerance (tests/test_regression.py:34-39)
+    from pamtra_b200.workloads import golden_pam, GOLDEN_FREQS
+    pam = golden_pam()
+    assert pam.nmlSet["active"] and pam.nmlSet["radar_mode"] == "simple"
+    r, err = oracle_mod.run_pamtra(pam, GOLDEN_FREQS)
+    assert err == 0
+    gold = np.load(GOLDEN)
+    np.testing.assert_allclose(r["Ze"], gold["Ze"], rtol=1e-5)
+    np.testing.assert_allclose(r["Att_hydro"], gold["Att_hydro"], rtol=1e-5)
+    assert (r["Ze"][0, 0, 1:3] > -9999).all() and np.all(r["Ze"][0, 0, 0] == -9999)
