@@ -55,6 +55,8 @@ def _args():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=24, help="requests in the serving replay (0 = skip)")
     ap.add_argument("--target-cols", type=int, default=1024, help="columns of the 150-layer target batch (0 = skip)")
+    ap.add_argument("--uneven-cols", type=int, default=2048, help="columns of the uneven batch (0 = skip)")
+    ap.add_argument("--mieheavy-cols", type=int, default=1024, help="columns of the Mie-heavy batch (0 = skip)")
     return ap.parse_args()
 
 
@@ -292,6 +294,73 @@ def _target_shape(args, local, eng, stream):
                      "reference operation order (PREC_FP64)"}
 
 
+def _config_line(name, b, local, eng, stream, nplain=8, reps=2):
+    """Batched FP64 and split-precision solves/s on one workload (tuned launch
+    shapes, device-timed, L2 flushed) against the plain form (one column per
+    call, reference order) on its first ``nplain`` columns.  A batch whose
+    scratch exceeds a third of the free device memory runs as NUMMU-grouped
+    chunks (batch.chunk_columns), one after another inside each timed step."""
+    import torch
+    from pamtra_b200 import autotune
+    from pamtra_b200 import batch as pbatch
+    from pamtra_b200._native import PREC_3XTF32, PREC_FP64_BATCHED
+    dev = torch.device("cuda", local)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    free, _ = torch.cuda.mem_get_info(dev)
+    chunks = [pbatch.subset(b, idx) for idx in pbatch.chunk_columns(b, free // 3)]
+    res = {"unit": "solves/s", "columns": b.ncol, "solves_per_step": b.n_solves(), "chunks": len(chunks)}
+    tbs = {}
+    for label, prec in (("batched_fp64", PREC_FP64_BATCHED), ("batched_3xtf32", PREC_3XTF32)):
+        outs = [cb.alloc_outputs(dev) for cb in chunks]
+        for cb, o in zip(chunks, outs):  # tune each chunk signature once, untimed
+            autotune.apply(cb, local, precision=prec, eng=eng, stream=stream, outputs=o, reps=1)
+            pbatch.run(cb, local, o, precision=prec, stream=stream, eng=eng)
+        stream.synchronize()
+        ms = []
+        for _ in range(reps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                s0.record(stream)
+                for cb, o in zip(chunks, outs):
+                    autotune.apply(cb, local, precision=prec, eng=eng)
+                    pbatch.run(cb, local, o, precision=prec, stream=stream, eng=eng)
+                e0.record(stream)
+            e0.synchronize()
+            ms.append(s0.elapsed_time(e0))
+        res[label] = b.n_solves() / (np.mean(ms) * 1e-3)
+        res[label + "_ms_per_step"] = float(np.mean(ms))
+        tbs[label] = [o["tb"].cpu().numpy() for o in outs]
+        res[label + "_status_nonzero"] = int(sum(int((o["status"] != 0).sum()) for o in outs))
+        del outs
+    eng.set_launch(autotune.DEFAULT)
+    singles = [pbatch.subset(b, [c]) for c in range(nplain)]
+    souts = [sb.alloc_outputs(dev) for sb in singles]
+    for sb, so in zip(singles, souts):
+        pbatch.run(sb, local, so, stream=stream, eng=eng)
+    stream.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        s.record(stream)
+        for sb, so in zip(singles, souts):
+            pbatch.run(sb, local, so, stream=stream, eng=eng)
+        e.record(stream)
+    e.synchronize()
+    res["plain_fp64"] = sum(sb.n_solves() for sb in singles) / (s.elapsed_time(e) * 1e-3)
+    res["plain_sample_columns"] = nplain
+    res["batched_fp64_over_plain"] = res["batched_fp64"] / res["plain_fp64"]
+    res["batched_3xtf32_over_plain"] = res["batched_3xtf32"] / res["plain_fp64"]
+    err = 0.0
+    for a, c in zip(tbs["batched_3xtf32"], tbs["batched_fp64"]):
+        ok = c > -9000
+        if np.any(ok):
+            err = max(err, float(np.max(np.abs(a - c)[ok])))
+    res["tb_err_3xtf32_vs_fp64_K"] = err
+    res["workload"] = name
+    del flush
+    return res
+
+
 def _serving(args, local):
     """Replay a seeded Poisson stream (200 requests/s) of uneven requests
     through the continuous-batching server; the plain form (one column per
@@ -504,6 +573,16 @@ def main():
             dist.destroy_process_group()
         return
     target = _target_shape(args, local, eng, stream) if args.target_cols > 0 else None
+    from pamtra_b200 import workloads as wl
+    uneven = _config_line("%d columns, layers uniform 40-150, 1-5 species (cloud water, cloud ice, snow, graupel, "
+                          "rain; exp or mgamma with mu 0-4; 20-80 bins; ice 100-900 kg/m3), 8-32 frequencies in "
+                          "10-183 GHz, NUMMU 8/16/32 per column" % args.uneven_cols,
+                          wl.uneven_batch(args.uneven_cols, seed=3), local, eng, stream) \
+        if args.uneven_cols > 0 else None
+    mieheavy = _config_line("%d columns x 100 layers, 4 species x 200 bins up to 10 mm (rain, snow, graupel, "
+                            "cloud ice), f = 89/157/176.31/190.31 GHz, NUMMU 16" % args.mieheavy_cols,
+                            wl.mie_heavy_batch(args.mieheavy_cols, seed=6), local, eng, stream) \
+        if args.mieheavy_cols > 0 else None
     serving = _serving(args, local) if args.serve_requests > 0 else None
     # ---- roofline of the dominant kernel (doubling stage)
     peak = fp64_peak_tflops(dev)
@@ -569,6 +648,8 @@ def main():
                                  "thin-layer init, adding and surface in FP64"},
         "stage_ms": {k: v / args.steps for k, v in stage_tot.items()},
         "target_shape": target,
+        "uneven": uneven,
+        "mie_heavy": mieheavy,
         "serving": serving,
         "status_nonzero": int(np.count_nonzero(status)),
     }

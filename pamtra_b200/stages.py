@@ -1,6 +1,6 @@
 """Per-stage device times of the batched forward path on the seeded workloads.
 
-``python -m pamtra_b200.stages [--workload c2|target|uneven] [--ncol N]
+``python -m pamtra_b200.stages [--workload c2|target|uneven|mieheavy] [--ncol N]
 [--precision fp64|fp64b|3xtf32|both|all] [--reps K]`` runs one untimed and
 K timed batches per precision (fp64: the reference operation order, fp64b:
 the batched FP64 form, 3xtf32: the split-precision form) through
@@ -26,6 +26,8 @@ def _batch(name, ncol):
         return wl.target_batch(ncol, seed=4)
     if name == "uneven":
         return wl.uneven_batch(ncol, seed=3)
+    if name == "mieheavy":
+        return wl.mie_heavy_batch(ncol, seed=6)
     raise ValueError("unknown workload %r" % name)
 
 
@@ -68,7 +70,7 @@ def run(name, ncol, precisions, reps, device=0):
 def main(argv=None):
     warnings.simplefilter("ignore")
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("--workload", default="c2", choices=["c2", "target", "uneven"])
+    ap.add_argument("--workload", default="c2", choices=["c2", "target", "uneven", "mieheavy"])
     ap.add_argument("--ncol", type=int, default=256)
     ap.add_argument("--precision", default="both", choices=["fp64", "3xtf32", "fp64b", "both", "all"])
     ap.add_argument("--reps", type=int, default=2)

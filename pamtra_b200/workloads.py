@@ -23,6 +23,10 @@ mixing), 8-32 frequencies per column from 10-183 GHz and NUMMU from
 
 ``target_batch`` is the 150-layer, 16-angle, 4-species shape: 150 layers
 over 0-15 km with cloud water, cloud ice, snow and rain in overlapping bands.
+
+``mie_heavy_batch`` is the Mie-heavy workload: 100 layers over 0-12 km, rain,
+snow, graupel and cloud ice with 200 bins each (sizes up to 10 mm, size
+parameters up to about 19 at 190 GHz), at 89, 157, 176.31 and 190.31 GHz.
 """
 
 import warnings
@@ -248,3 +252,22 @@ def target_batch(ncol=1024, seed=4):
     top = np.full(ncol, 15000.0)
     qs = [[10 ** rng.uniform(-5.0, np.log10(2e-3)) for _ in kinds] for _ in range(ncol)]
     return _packed(st, sp, 0, nly, [TARGET_FREQS], None, [kinds] * ncol, qs, top, rng, 150, 4, False)
+
+
+MIE_HEAVY_FREQS = [89.0, 157.0, 176.31, 190.31]
+
+
+def mie_heavy_batch(ncol=2048, seed=6):
+    """Mie-heavy columns: 100 layers, four species of 200 bins (rain up to
+    6 mm, snow up to 10 mm, graupel up to 8 mm, cloud ice up to 2 mm), shared
+    species table and frequencies 89/157/176.31/190.31 GHz."""
+    rng = np.random.default_rng(seed)
+    st = _settings(16)
+    kinds = ["rwc", "swc", "gwc", "iwc"]
+    sp = np.empty(4, dtype=packing.SPECIES_DTYPE)
+    for j, k in enumerate(kinds):
+        sp[j] = _species_row(k, np.random.default_rng(200 + j), nbin=200, gamma=(k != "rwc"), rho=400.0)
+    nly = np.full(ncol, 100)
+    top = np.full(ncol, 12000.0)
+    qs = [[10 ** rng.uniform(-5.0, np.log10(2e-3)) for _ in kinds] for _ in range(ncol)]
+    return _packed(st, sp, 0, nly, [MIE_HEAVY_FREQS], None, [kinds] * ncol, qs, top, rng, 100, 4, False)
