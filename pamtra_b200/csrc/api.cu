@@ -867,10 +867,11 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   }
   if (mask & 2) {
     if (H > 0 && precision == PAMTRA_B200_PREC_3XTF32) {
-      // two CTAs (two item pairs) per SM by shared memory; the persistent CTAs
-      // take pairs of items from a counter
+      // three CTAs (three item pairs) per SM by shared memory, registers and
+      // tensor memory (3 x 128 columns); the persistent CTAs take pairs of
+      // items from a counter
       const size_t smb = layer_tc_smem<16>();
-      const int g = (ctx->layer_cps == 1 ? 1 : 2) * sms;
+      const int g = (ctx->layer_cps > 0 ? std::min(ctx->layer_cps, 3) : 3) * sms;
       k_layer_tc<16><<<g, 128, smb, stream>>>(b, w, *st, ssp); launches++;
     } else if (H > 0) {
       int g = persistent_grid((const void*)k_layer<16>, RTCfg<16>::T, sizeof(LayerSmem<16>), sms, ctx->layer_cps);

@@ -34,15 +34,19 @@
 
 namespace pb {
 
-constexpr int MS = 36;  // column stride of the FP32 masters: quarter-warp float4 accesses are conflict-free
+// FP32 masters: 32 x 32, column-major with the 4-float chunks of column c
+// XOR-swizzled by c mod 8, so a quarter warp reading one chunk of eight
+// neighbouring columns (column loads) and a warp reading one row-slice of a
+// column (row loads, mat-vecs) both hit 32 distinct banks without padding.
+__device__ __forceinline__ int midx(int r, int c) { return c * 32 + ((((r >> 2) ^ (c & 7)) << 2) | (r & 3)); }
 
-// FP32 state of one item of the pair (column-major masters, column c at [c * MS]).
+// FP32 state of one item of the pair.
 struct TcItemState {
-  float rm[32 * MS], tm[32 * MS], gm[32 * MS];  // R, T~, G~
-  float vm[32 * MS];                            // V = R T, then Y = G R T
-  float xa[32 * MS], xb[32 * MS];               // series powers X (ping-pong); Z~ in xa
-  float src[4][32];                             // S+ linear, S+ constant, S- linear, S- constant
-  float vv[4][32], uv[4][32], wv[4][32];        // right-hand vectors of the three groups
+  float rm[1024], tm[1024], gm[1024];    // R, T~, G~
+  float vm[1024];                        // V = R T, then Y = G R T
+  float xa[1024];                        // series power X, then Z~
+  float src[4][32];                      // S+ linear, S+ constant, S- linear, S- constant
+  float vv[4][32], uv[4][32], wv[4][32]; // right-hand vectors of the three groups
   float nrm;
   int pad_[3];
 };
@@ -51,9 +55,22 @@ struct TcTiles {
   float b_hi[64 * 32], b_lo[64 * 32];  // B tile pair (64 rows: 32 per item); the A pair lives in TMEM
 };
 
+// FP64 set-up scratch of one item (layer_setup): thin-layer R and T,
+// Legendre coefficients, azimuth table, quadrature and sources.
+struct TcSetupSmem {
+  static constexpr int n = 32, MAT = RTCfg<16>::MAT;
+  double r[MAT], t[MAT];
+  double coef[3 * MAXNLEG];
+  double az[2 * KMAX];
+  double lin[2 * n], cst[2 * n];
+  double mu[16], wq[16], nrm[16];
+  int item, stat;
+  __device__ __forceinline__ double* mat(int i) { return i == 0 ? r : i == 1 ? t : i == 4 ? az : coef; }
+};
+
 union __align__(128) TcScratch {
   TcTiles tl;
-  LayerSmem<16> setup;  // the FP64 set-up of one item at a time
+  TcSetupSmem setup;  // the FP64 set-up of one item at a time
 };
 
 struct TcPairSmem {
@@ -70,19 +87,18 @@ constexpr size_t layer_tc_smem() {
   return sizeof(TcPairSmem);
 }
 
-// thread-owned column helpers (column-major masters, column stride S)
-template <int S = MS>
+// thread-owned column helpers of the masters
 __device__ __forceinline__ void ld_col(const float* m, int col, float (&v)[32]) {
 #pragma unroll
   for (int r = 0; r < 32; r += 4) {
-    const float4 q = *reinterpret_cast<const float4*>(m + col * S + r);
+    const float4 q = *reinterpret_cast<const float4*>(m + midx(r, col));
     v[r] = q.x; v[r + 1] = q.y; v[r + 2] = q.z; v[r + 3] = q.w;
   }
 }
-template <int S = MS>
 __device__ __forceinline__ void st_col(float* m, int col, const float (&v)[32]) {
 #pragma unroll
-  for (int r = 0; r < 32; r += 4) *reinterpret_cast<float4*>(m + col * S + r) = make_float4(v[r], v[r + 1], v[r + 2], v[r + 3]);
+  for (int r = 0; r < 32; r += 4)
+    *reinterpret_cast<float4*>(m + midx(r, col)) = make_float4(v[r], v[r + 1], v[r + 2], v[r + 3]);
 }
 
 // Operands of one group for the calling thread, split into TF32 hi / lo
@@ -104,10 +120,10 @@ __device__ __forceinline__ void build_operands(TcTiles& TL, const float* asrc, c
   for (int q = 0; q < 4; q++) {
     const int k0 = 16 * h + 4 * q;
     float4 hi, lo;
-    tc::split(bsrc[(k0 + 0) * MS + lane], hi.x, lo.x);
-    tc::split(bsrc[(k0 + 1) * MS + lane], hi.y, lo.y);
-    tc::split(bsrc[(k0 + 2) * MS + lane], hi.z, lo.z);
-    tc::split(bsrc[(k0 + 3) * MS + lane], hi.w, lo.w);
+    tc::split(bsrc[midx(lane, k0 + 0)], hi.x, lo.x);
+    tc::split(bsrc[midx(lane, k0 + 1)], hi.y, lo.y);
+    tc::split(bsrc[midx(lane, k0 + 2)], hi.z, lo.z);
+    tc::split(bsrc[midx(lane, k0 + 3)], hi.w, lo.w);
     const int o = (brow >> 3) * tc::RG_FLOATS + (k0 >> 2) * 32 + (brow & 7) * 4;
     *reinterpret_cast<float4*>(TL.b_hi + o) = hi;
     *reinterpret_cast<float4*>(TL.b_lo + o) = lo;
@@ -122,7 +138,7 @@ __device__ __forceinline__ void matvec2(const float* __restrict__ M, const float
   for (int k = 0; k < 32; k += 4) {
     const float4 p = *reinterpret_cast<const float4*>(x0 + k);
     const float4 q = *reinterpret_cast<const float4*>(x1 + k);
-    const float m0 = M[k * MS + r], m1 = M[(k + 1) * MS + r], m2 = M[(k + 2) * MS + r], m3 = M[(k + 3) * MS + r];
+    const float m0 = M[midx(r, k)], m1 = M[midx(r, k + 1)], m2 = M[midx(r, k + 2)], m3 = M[midx(r, k + 3)];
     a0 = fmaf(m0, p.x, a0); a1 = fmaf(m0, q.x, a1);
     a0 = fmaf(m1, p.y, a0); a1 = fmaf(m1, q.y, a1);
     a0 = fmaf(m2, p.z, a0); a1 = fmaf(m2, q.z, a1);
@@ -152,14 +168,14 @@ __device__ __forceinline__ int series_steps(float nrm) {
 }
 
 template <int N>
-__global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b200_settings st,
+__global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b200_settings st,
                                                      double* __restrict__ ssp_scat) {
   static_assert(N == 16, "the split-precision layer kernel is built for NUMMU = 16");
   constexpr int n = 32, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT;
   enum { G1 = 0, SER = 1, G2 = 2, G3 = 3 };
   extern __shared__ __align__(1024) double smem_raw[];
   TcPairSmem& Q = *reinterpret_cast<TcPairSmem*>(smem_raw);
-  LayerSmem<N>& S = Q.u.setup;
+  TcSetupSmem& S = Q.u.setup;
   TcTiles& TL = Q.u.tl;
   __shared__ uint64_t mbar;
   __shared__ uint32_t tslot;
@@ -200,13 +216,13 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
       LayerItem it;
       const bool valid = item < nitems && layer_setup<N>(b, w, st, ssp_scat, S, item, it);
       if (valid && it.nd == 0) {
-        layer_store<N>(w, item, S.m[0], S.m[1], S.lin);
+        layer_store<N>(w, item, S.r, S.t, S.lin);
       } else if (valid) {
         TcItemState& D = Q.st[i];
         for (int e = t; e < n * n; e += 128) {
           const int cc = e >> 5, r = e & 31;
-          D.rm[cc * MS + r] = (float)S.m[0][cc * LD + r];
-          D.tm[cc * MS + r] = (float)((r == cc ? 1.0 : 0.0) - S.m[1][cc * LD + r]);
+          D.rm[midx(r, cc)] = (float)S.r[cc * LD + r];
+          D.tm[midx(r, cc)] = (float)((r == cc ? 1.0 : 0.0) - S.t[cc * LD + r]);
         }
         if (t < n) {
           D.src[0][t] = (float)S.lin[t];
@@ -245,17 +261,15 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
       //   SER [X; G~] x X   -> slot 0: X X      -> X next;  slot 1: X G~ -> G~ += X + X G~
       //   G2  [T~; V] x G~  -> slot 0: G~ T~    -> Z~;      slot 1: G~ V -> Y = V + G~ V
       //   G3  [Z~; Y] x T~  -> slot 0: T~ Z~    -> T~';     slot 1: T~ Y -> R'
-      int phase = G1, d = 0, k = 0, mys = 0, myg = 0, gmax = 0, xsel = 0;  // plan, MMAs: mine / the pair's
+      int phase = G1, d = 0, k = 0, mys = 0, myg = 0, gmax = 0;  // series plan, MMAs: mine / the pair's
       for (;;) {
         const bool act = d < my_nd;
         const bool on = (phase == SER) ? (k < myg) : act;
-        float* xc = xsel ? my.xb : my.xa;  // current series power
-        float* xn = xsel ? my.xa : my.xb;
         if (on) {
           const float* asrc;
           const float* bsrc;
           if (phase == G1) { asrc = slot ? my.tm : my.rm; bsrc = my.rm; }
-          else if (phase == SER) { asrc = slot ? my.gm : xc; bsrc = xc; }
+          else if (phase == SER) { asrc = slot ? my.gm : my.xa; bsrc = my.xa; }
           else if (phase == G2) { asrc = slot ? my.vm : my.tm; bsrc = my.gm; }
           else { asrc = slot ? my.vm : my.xa; bsrc = my.tm; }
           build_operands(TL, asrc, bsrc, tslot + lanes + 64u, tslot + lanes + 96u, brow, slot, lane);
@@ -266,6 +280,8 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
         tc::fence_after_sync();
         if (t == 0) tc::mma3_ta(tslot, tslot + 64u, tslot + 96u, TL.b_hi, TL.b_lo, &mbar, tc::IDESC_M128_N64);
         float m0 = 0.f, m1 = 0.f;
+        float xk[32];  // slot 1 of a series step: its column of X, taken before slot 0 replaces X
+        if (on && phase == SER && slot == 1) ld_col(my.xa, lane, xk);
         if (on && phase != SER) {
           const float* mv = (phase == G1) ? my.rm : (phase == G2) ? my.gm : my.tm;
           const float(*x)[32] = (phase == G1) ? my.vv : (phase == G2) ? my.uv : my.wv;
@@ -303,16 +319,17 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
           } else if (phase == SER) {
             if (mys == SERIES_H1) {
               if (slot == 0) {  // G~ = X + X X
-                ld_col(xc, lane, a);
+                ld_col(my.xa, lane, a);
 #pragma unroll
                 for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
                 st_col(my.gm, lane, a);
               }
             } else if (slot == 0) {
-              if (k < mys) st_col(xn, lane, dv);  // X = X X
+              if (k < mys) st_col(my.xa, lane, dv);  // X = X X (slot 1 took its column of X before)
             } else {  // G~ += X + X G~
               float g[32];
-              ld_col(xc, lane, a);
+#pragma unroll
+              for (int r = 0; r < 32; r++) a[r] = xk[r];
               ld_col(my.gm, lane, g);
 #pragma unroll
               for (int r = 0; r < 32; r++) g[r] = g[r] + (a[r] + dv[r]);
@@ -379,13 +396,13 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
             TcItemState& D = Q.st[i];
             for (int e = t; e < n * n; e += 128) {
               const int cc = e >> 5, r = e & 31;
-              M[cc * Team<32>::LD + r] = (r == cc ? 1.0 : 0.0) - (double)D.xa[cc * MS + r];
+              M[cc * Team<32>::LD + r] = (r == cc ? 1.0 : 0.0) - (double)D.xa[midx(r, cc)];
             }
             __syncthreads();
             if (ginv<32>(M, IS) && t == 0) s_status[i] |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
             for (int e = t; e < n * n; e += 128) {
               const int cc = e >> 5, r = e & 31;
-              D.gm[cc * MS + r] = (float)(M[cc * Team<32>::LD + r] - (r == cc ? 1.0 : 0.0));
+              D.gm[midx(r, cc)] = (float)(M[cc * Team<32>::LD + r] - (r == cc ? 1.0 : 0.0));
             }
             __syncthreads();
           }
@@ -402,10 +419,8 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
           }
           __syncthreads();
           k = 0;
-          xsel = 0;
           phase = (gmax > 0) ? SER : G2;
         } else if (phase == SER) {
-          xsel ^= 1;
           if (++k >= gmax) phase = G2;
         } else if (phase == G2) {
           phase = G3;
@@ -428,8 +443,8 @@ __global__ void __launch_bounds__(128, 2) k_layer_tc(Batch b, Work w, pamtra_b20
         double* out = w.lay + (size_t)(base + i) * w.lay_stride;
         for (int e = t; e < n * n; e += 128) {
           const int cc = e >> 5, r = e & 31;
-          out[cc * LD + r] = (double)D.rm[cc * MS + r];
-          out[MAT + cc * LD + r] = (r == cc ? 1.0 : 0.0) - (double)D.tm[cc * MS + r];
+          out[cc * LD + r] = (double)D.rm[midx(r, cc)];
+          out[MAT + cc * LD + r] = (r == cc ? 1.0 : 0.0) - (double)D.tm[midx(r, cc)];
         }
         if (t < n) {
           out[2 * MAT + t] = (double)D.src[0][t];

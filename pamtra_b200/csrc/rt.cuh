@@ -57,6 +57,8 @@ struct LayerSmem {
   double mu[N], wq[N], nrm[N];
   InvScratch<n> inv;
   int item, stat;
+  // set-up buffers (layer_setup): R, T, coefficients, azimuth table
+  __device__ __forceinline__ double* mat(int i) { return m[i]; }
 };
 
 // Azimuth weights of scatcnv (src/scatcnv.f90:103-192 with SUM_LEGENDRE,
@@ -144,9 +146,9 @@ struct LayerItem {
 // INITIAL_SOURCE4 of one (present layer, frequency) item: leaves the
 // thin-layer R (S.m[0]) and T (S.m[1]) and the sources S.lin / S.cst in
 // shared memory.  Returns false when the item is not for this N.
-template <int N>
+template <int N, class SM>
 __device__ __forceinline__ bool layer_setup(const Batch& b, const Work& w, const pamtra_b200_settings& st,
-                                            double* __restrict__ ssp_scat, LayerSmem<N>& S, int item,
+                                            double* __restrict__ ssp_scat, SM& S, int item,
                                             LayerItem& it) {
   constexpr int n = RTCfg<N>::n, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT, T = RTCfg<N>::T;
   const int t = threadIdx.x;
@@ -164,12 +166,10 @@ __device__ __forceinline__ bool layer_setup(const Batch& b, const Work& w, const
     const double planck0 = planck(tl[z + 1], wl), planck1 = planck(tl[z], wl);
     const int nleg = w.m_nleg[item];
     const double kext = w.m_kext[item], salb = w.m_salb[item];
-    double* Rb = S.m[0];
-    double* Tb = S.m[1];
-    double* Gb = S.m[2];
-    double* Wb = S.m[3];
-    (void)Wb;
-    double* Yb = S.m[4];
+    double* Rb = S.mat(0);
+    double* Tb = S.mat(1);
+    double* Gb = S.mat(2);
+    double* Yb = S.mat(4);
     double ext = 0.0, emis = 0.0;
     int status = 0;
     // ---------------- scatcnv (src/scatcnv.f90) into P1 (Tb) and P2 (Rb)
@@ -178,7 +178,7 @@ __device__ __forceinline__ bool layer_setup(const Batch& b, const Work& w, const
       emis = (1.0 - salb) * kext;
       const double cst = kext * salb / (4.0 * 3.1415926535897932384);
       const double* lg = w.m_legen + (size_t)item * 3 * MAXNLEG;
-      double* coef = Gb;          // [3][MAXNLEG], may run on into Wb (n = 16)
+      double* coef = Gb;          // [3][MAXNLEG] (S.mat(2) provides that many; for n = 16 the next matrix)
       double* cphi = Yb;          // [KMAX]
       double* sphi = Yb + KMAX;   // [KMAX]
       const int numpts = 2 * ((nleg + 1) / 2) + 4;
