@@ -24,6 +24,7 @@
 #include "rt.cuh"
 #include "tc.cuh"
 #include "layer_tc.cuh"
+#include "layer_tc64.cuh"
 #include "work.cuh"
 
 using namespace pb;
@@ -490,6 +491,7 @@ static int set_smem_attrs() {
     set((const void*)k_layer<16>, sizeof(LayerSmem<16>));
     set((const void*)k_layer<32>, sizeof(LayerSmem<32>));
     set((const void*)k_layer_tc<16>, layer_tc_smem<16>());
+    set((const void*)k_layer_tc64, layer_tc64_smem());
     set((const void*)k_adding<8>, sizeof(AddSmem<8>));
     set((const void*)k_adding<16>, sizeof(AddSmem<16>));
     set((const void*)k_adding<32>, sizeof(AddSmem<32>));
@@ -886,7 +888,12 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   }
   if (mask & 4) {
     int g = persistent_grid((const void*)k_layer<32>, RTCfg<32>::T, sizeof(LayerSmem<32>), sms, ctx->layer_cps);
-    if (H > 0) { k_layer<32><<<g, RTCfg<32>::T, sizeof(LayerSmem<32>), stream>>>(b, w, *st, ssp); launches++; }
+    if (H > 0 && precision == PAMTRA_B200_PREC_3XTF32) {
+      // one item per CTA, one CTA per SM (165 KB shared memory, 256 TMEM columns)
+      k_layer_tc64<<<sms, 128, layer_tc64_smem(), stream>>>(b, w, *st, ssp); launches++;
+    } else if (H > 0) {
+      k_layer<32><<<g, RTCfg<32>::T, sizeof(LayerSmem<32>), stream>>>(b, w, *st, ssp); launches++;
+    }
     mark(ctx, stream, STG_LAYER);
     g = std::min(persistent_grid((const void*)k_adding<32>, RTCfg<32>::T, sizeof(AddSmem<32>), sms, ctx->adding_cps),
                  pl.add_grid);

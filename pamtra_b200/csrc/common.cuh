@@ -202,9 +202,9 @@ __device__ __forceinline__ void pivot_candidates(int i, int k, double v, InvScra
 // pivot search of the next column is fused into the elimination, leaving
 // two team barriers per step.  Returns nonzero to every thread if a pivot
 // was exactly zero.
-template <int n>
+template <int n, int T = Team<n>::T>
 __device__ int ginv(double* A, InvScratch<n>& S) {
-  constexpr int LD = Team<n>::LD, T = Team<n>::T, CG = T / n, NC = n / CG, NGW = (n + 31) / 32;
+  constexpr int LD = Team<n>::LD, CG = T / n, NC = n / CG, NGW = (n + 31) / 32;
   const int t = threadIdx.x, i = t % n, cg = t / n;
   if (cg == 0) pivot_candidates<n>(i, 0, A[i], S);
   if (t == 0) S.sing = 0;

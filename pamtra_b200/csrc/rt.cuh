@@ -146,11 +146,11 @@ struct LayerItem {
 // INITIAL_SOURCE4 of one (present layer, frequency) item: leaves the
 // thin-layer R (S.m[0]) and T (S.m[1]) and the sources S.lin / S.cst in
 // shared memory.  Returns false when the item is not for this N.
-template <int N, class SM>
+template <int N, class SM, int T = RTCfg<N>::T>
 __device__ __forceinline__ bool layer_setup(const Batch& b, const Work& w, const pamtra_b200_settings& st,
                                             double* __restrict__ ssp_scat, SM& S, int item,
                                             LayerItem& it) {
-  constexpr int n = RTCfg<N>::n, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT, T = RTCfg<N>::T;
+  constexpr int n = RTCfg<N>::n, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT;
   const int t = threadIdx.x;
   const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
     const int p = item / Fm, fi = item % Fm;
@@ -359,10 +359,10 @@ __device__ __forceinline__ bool layer_setup(const Batch& b, const Work& w, const
 }
 
 // Write the layer R, T and S+/S- of an item (FP64, the layout k_adding reads).
-template <int N>
+template <int N, int T = RTCfg<N>::T>
 __device__ __forceinline__ void layer_store(const Work& w, int item, const double* Rb, const double* Tb,
                                             const double* lin) {
-  constexpr int n = RTCfg<N>::n, MAT = RTCfg<N>::MAT, T = RTCfg<N>::T;
+  constexpr int n = RTCfg<N>::n, MAT = RTCfg<N>::MAT;
   const int t = threadIdx.x;
   double* out = w.lay + (size_t)item * w.lay_stride;
   for (int e = t; e < MAT; e += T) { out[e] = Rb[e]; out[MAT + e] = Tb[e]; }

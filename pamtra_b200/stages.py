@@ -17,7 +17,7 @@ import json
 import warnings
 
 
-def _batch(name, ncol):
+def _batch(name, ncol, nummu=None):
     from . import batch as pbatch
     from . import workloads as wl
     if name == "c2":
@@ -25,20 +25,20 @@ def _batch(name, ncol):
     if name == "target":
         return wl.target_batch(ncol, seed=4)
     if name == "uneven":
-        return wl.uneven_batch(ncol, seed=3)
+        return wl.uneven_batch(ncol, seed=3, nummu_choices=(nummu,) if nummu else (8, 16, 32))
     if name == "mieheavy":
         return wl.mie_heavy_batch(ncol, seed=6)
     raise ValueError("unknown workload %r" % name)
 
 
-def run(name, ncol, precisions, reps, device=0):
+def run(name, ncol, precisions, reps, device=0, nummu=None):
     import numpy as np
     import torch
 
     from . import batch as pbatch
     from ._native import Engine
     eng = Engine(device)
-    b = _batch(name, ncol)
+    b = _batch(name, ncol, nummu)
     stream = torch.cuda.Stream(torch.device("cuda", device))
     lines, tbs = [], []
     for prec in precisions:
@@ -74,9 +74,10 @@ def main(argv=None):
     ap.add_argument("--ncol", type=int, default=256)
     ap.add_argument("--precision", default="both", choices=["fp64", "3xtf32", "fp64b", "both", "all"])
     ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--nummu", type=int, default=0, choices=[0, 8, 16, 32], help="uneven workload: one NUMMU only")
     a = ap.parse_args(argv)
     precs = {"fp64": [0], "3xtf32": [1], "fp64b": [2], "both": [0, 1], "all": [0, 2, 1]}[a.precision]
-    for ln in run(a.workload, a.ncol, precs, a.reps):
+    for ln in run(a.workload, a.ncol, precs, a.reps, nummu=a.nummu or None):
         print(json.dumps(ln))
 
 

@@ -408,7 +408,7 @@ def test_split_precision_target_shape(native):
 
 
 def test_split_precision_uneven(native):
-    # NUMMU 16 columns take the tensor-core doubling, NUMMU 8 / 32 the FP64
+    # NUMMU 16 and 32 columns take the tensor-core doubling, NUMMU 8 the FP64
     # one; both forms share the one-inverse FP64 adding
     from pamtra_b200._native import PREC_3XTF32, PREC_FP64, PREC_FP64_BATCHED
     b = wl.uneven_batch(24, seed=13, nfreq_range=(2, 5))
@@ -419,7 +419,25 @@ def test_split_precision_uneven(native):
     nmu = b.host["nummu"]
     d = np.abs(s["tb"] - f64["tb"])
     assert np.max(d) <= SPLIT_TB_TOL
-    assert np.array_equal(s["tb"][nmu != 16], f64b["tb"][nmu != 16])
+    assert np.max(d[nmu == 32]) > 0.0  # NUMMU 32 ran in split precision
+    assert np.array_equal(s["tb"][nmu == 8], f64b["tb"][nmu == 8])
+
+
+def test_split_precision_nummu_32(oracle_mod, native):
+    # the n = 64 split-precision kernel (one item per CTA, K = 64 operand tiles)
+    # against the oracle and the FP64 form, and run-to-run reproducible
+    from pamtra_b200._native import PREC_3XTF32, PREC_FP64
+    b = wl.uneven_batch(12, seed=47, nummu_choices=(32,), nfreq_range=(2, 3))
+    f64 = _run_prec(b, PREC_FP64)
+    s = _run_prec(b, PREC_3XTF32)
+    assert int(np.count_nonzero(s["status"])) == 0
+    assert np.max(np.abs(s["tb"] - f64["tb"])) <= SPLIT_TB_TOL
+    again = _run_prec(b, PREC_3XTF32)
+    assert np.array_equal(again["tb"], s["tb"])
+    for c in (0, 11):
+        err, t, N, nf = _oracle_packed_column(oracle_mod, b, c)
+        assert err == 0 and N == 32
+        assert np.max(np.abs(s["tb"][c][:, :2 * N, :nf, :] - t)) <= SPLIT_TB_TOL
 
 
 def test_split_precision_pairing_independent(native):
