@@ -65,7 +65,7 @@ extern "C" {
                                            (src/radintg4.f90:447-513) with its two inverses per
                                            combine; the plain drop-in form */
 #define PAMTRA_B200_PREC_3XTF32 1        /* batched form: layer doubling products as 3xTF32 tcgen05
-                                           MMAs (NUMMU = 16; NUMMU 8 / 32 double in FP64), FP64
+                                           MMAs (NUMMU 16 and 32; NUMMU 8 doubles in FP64), FP64
                                            adding with one inverse per combine */
 #define PAMTRA_B200_PREC_FP64_BATCHED 2  /* batched form in FP64: as PREC_FP64, but each adding
                                            combine derives the minus-side inverse from the
