@@ -53,7 +53,7 @@ def _args():
     ap.add_argument("--ncol", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=0, help="columns for the CPU baseline (0 = 2 per core)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--serve-requests", type=int, default=24, help="requests in the serving replay (0 = skip)")
+    ap.add_argument("--serve-requests", type=int, default=16, help="requests in the serving replay (0 = skip)")
     ap.add_argument("--target-cols", type=int, default=1024, help="columns of the 150-layer target batch (0 = skip)")
     ap.add_argument("--uneven-cols", type=int, default=2048, help="columns of the uneven batch (0 = skip)")
     ap.add_argument("--mieheavy-cols", type=int, default=1024, help="columns of the Mie-heavy batch (0 = skip)")
@@ -363,33 +363,32 @@ def _config_line(name, b, local, eng, stream, nplain=8, reps=2):
 
 def _serving(args, local):
     """Replay a seeded Poisson stream (200 requests/s) of uneven requests
-    through the continuous-batching server; the plain form (one column per
-    call, one slot) serves the first three requests of the same stream."""
+    through the continuous-batching server: the batched split-precision and
+    batched FP64 forms (three slots) on the whole stream, the plain form (one
+    column per call, one slot) on its first three requests."""
     from pamtra_b200 import serve
+    from pamtra_b200._native import PREC_3XTF32, PREC_FP64, PREC_FP64_BATCHED
     reqs = serve.request_stream(args.serve_requests, seed=5, max_cols=512, nfreq_range=(1, 32))
     arr = serve.poisson_arrivals(len(reqs), 200.0, seed=6)
     warm = serve.request_stream(3, seed=7, max_cols=16, nfreq_range=(1, 4))
-    from pamtra_b200._native import PREC_FP64_BATCHED
-    srv = serve.Server(local, slots=3, hbm_fraction=0.5, max_cols=2048, precision=PREC_FP64_BATCHED)
-    for b in warm:
-        srv.submit(b)
-    srv.drain()
-    done, wall = serve.replay(srv, reqs, arr)
-    nb = srv.batches_launched
-    srv.close()
-    solves = sum(r.n_solves() for r in done)
-    errs = sum(1 for r in done if r.error)
     res = {"stream": "%d requests, Poisson 200/s (seed 6); each 1-512 columns of 40-150 layers, 1-5 species, "
-                     "1-32 frequencies in 10-183 GHz, NUMMU in {8,16,32}" % len(reqs),
-           "batched_fp64": dict(serve.latency_stats(done), solves_per_s=solves / wall, solves=solves,
-                                wall_s=wall, batches=nb - len(warm), requests_with_error=errs, slots=3)}
-    k = min(3, len(reqs))
-    psrv = serve.Server(local, slots=1, hbm_fraction=0.2, max_cols=1)
-    pdone, pwall = serve.replay(psrv, reqs[:k], arr[:k])
-    psrv.close()
-    psolves = sum(r.n_solves() for r in pdone)
-    res["plain_fp64"] = dict(serve.latency_stats(pdone), solves_per_s=psolves / pwall, solves=psolves,
-                             wall_s=pwall, requests=k)
+                     "1-32 frequencies in 10-183 GHz, NUMMU in {8,16,32}" % len(reqs)}
+    for label, prec, slots, cols, nreq in (("batched_3xtf32", PREC_3XTF32, 3, 2048, len(reqs)),
+                                           ("batched_fp64", PREC_FP64_BATCHED, 3, 2048, len(reqs)),
+                                           ("plain_fp64", PREC_FP64, 1, 1, min(3, len(reqs)))):
+        srv = serve.Server(local, slots=slots, hbm_fraction=0.5 if slots > 1 else 0.2, max_cols=cols,
+                           precision=prec)
+        for b in warm:
+            srv.submit(b)
+        srv.drain()
+        nb0 = srv.batches_launched
+        done, wall = serve.replay(srv, reqs[:nreq], arr[:nreq])
+        nb = srv.batches_launched - nb0
+        srv.close()
+        solves = sum(r.n_solves() for r in done)
+        res[label] = dict(serve.latency_stats(done), solves_per_s=solves / wall, solves=solves, wall_s=wall,
+                          batches=nb, requests_with_error=sum(1 for r in done if r.error), slots=slots,
+                          requests=nreq)
     return res
 
 

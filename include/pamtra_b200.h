@@ -124,6 +124,14 @@ typedef struct pamtra_b200_columns {
   const double* groundtemp;   /* [ncol], NaN = lowest level temperature */
   const double* obs_height;   /* [ncol][noutlevels] m */
   const int8_t* sfc_refl;     /* [ncol] 'S', 'L' or 'F' */
+  /* full size spectra (nmlSet['hydro_fullspec'], src/hydrometeor_extinction.f90:122-151):
+   * when fs_d is not NULL the size distributions are taken from these arrays
+   * instead of being derived from hydro_q / hydro_n / hydro_reff.
+   * [ncol][max_nlyrs][nhydro][fs_nbin], fs_d_bound [..][fs_nbin + 1]; the
+   * bin width is d_bound[i+1] - d_bound[i]; a slot takes part when its
+   * number concentrations sum above zero (or hydro_threshold <= 0). */
+  int32_t fs_nbin;
+  const double *fs_d, *fs_d_bound, *fs_n, *fs_rho, *fs_mass;
 } pamtra_b200_columns;
 
 typedef struct pamtra_b200_outputs {
@@ -251,8 +259,8 @@ int32_t pamtra_b200_mmult_3xtf32_batched(const double* a, const double* b, doubl
  * allocator.  All pointers in `cols` and `out` are DEVICE pointers,
  * `cols->species` included.  Limits: ncol = 1, max_nlyrs <= 64,
  * max_nfreq <= 4, nhydro <= 4, nbin <= 64 per species, nummu 8 or 16,
- * noutlevels <= 2; larger requests return PAMTRA_B200_FATAL |
- * PAMTRA_B200_ST_SIZE without running.  The first call on a device (with
+ * noutlevels <= 2, no full spectra (fs_d NULL); other requests return
+ * PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE without running.  The first call on a device (with
  * that device current) resolves the array's device address with
  * cudaGetSymbolAddress and fills the quadrature and line tables; make that
  * first call before any stream capture.  Every call shares the one array and

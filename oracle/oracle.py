@@ -40,6 +40,11 @@ class OrcSettings(ctypes.Structure):
     ]
 
 
+class OrcFullspec(ctypes.Structure):
+    _fields_ = [("nbin", ctypes.c_int32), ("d", ctypes.c_void_p), ("d_bound", ctypes.c_void_p),
+                ("n", ctypes.c_void_p), ("rho", ctypes.c_void_p), ("mass", ctypes.c_void_p)]
+
+
 class OrcDebug(ctypes.Structure):
     _fields_ = [(k, ctypes.c_void_p) for k in
                 ("kextatmo", "kexttot", "salbedo", "nlegen", "legen", "present", "scatter_matrix", "ext",
@@ -63,6 +68,8 @@ def lib():
                                      dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, dp, ctypes.c_double, ctypes.c_int,
                                      dp, ctypes.c_char, ctypes.c_int, dp, dp, dp, dp,
                                      ctypes.POINTER(OrcDebug)]
+        l.orc_run_column_fs.restype = ctypes.c_int
+        l.orc_run_column_fs.argtypes = l.orc_run_column.argtypes + [ctypes.POINTER(OrcFullspec)]
         l.orc_gas_r98.restype = ctypes.c_int
         l.orc_gas_r98.argtypes = [ctypes.c_double] * 4 + [dp]
         l.orc_eps_water_tkc.restype = None
@@ -124,12 +131,20 @@ def run_column(st, species, cols, c, freqs, debug=False):
         dbg = OrcDebug(**{k: v.ctypes.data for k, v in out_dbg.items()})
     sp = np.ascontiguousarray(species)
     refl = bytes([int(cols["sfc_refl"][c]) & 0xFF])
-    err = l.orc_run_column(ctypes.byref(st), sp.ctypes.data if H else None, H, L,
-                           _p(hl["hgt_lev"]), _p(hl["temp_lev"]), _p(hl["press_lev"]), _p(hl["relhum_lev"]),
-                           _p(ly["hgt"]), _p(ly["temp"]), _p(ly["press"]), _p(ly["relhum"]),
-                           _p(hq["hydro_q"]), _p(hq["hydro_n"]), _p(hq["hydro_reff"]),
-                           float(cols["groundtemp"][c]), nout, _p(obs), refl, nf, _p(fr), _p(tb), _p(em),
-                           _p(ang), ctypes.byref(dbg) if dbg is not None else None)
+    args = [ctypes.byref(st), sp.ctypes.data if H else None, H, L,
+            _p(hl["hgt_lev"]), _p(hl["temp_lev"]), _p(hl["press_lev"]), _p(hl["relhum_lev"]),
+            _p(ly["hgt"]), _p(ly["temp"]), _p(ly["press"]), _p(ly["relhum"]),
+            _p(hq["hydro_q"]), _p(hq["hydro_n"]), _p(hq["hydro_reff"]),
+            float(cols["groundtemp"][c]), nout, _p(obs), refl, nf, _p(fr), _p(tb), _p(em),
+            _p(ang), ctypes.byref(dbg) if dbg is not None else None]
+    if cols.get("fs_d") is not None:
+        # full spectra of this column, [L][H][nbin] (+1 for the bin bounds)
+        fsa = {k: f64(cols[k][c, :L]) for k in ("fs_d", "fs_d_bound", "fs_n", "fs_rho", "fs_mass")}
+        fs = OrcFullspec(int(cols["fs_nbin"]), *[fsa[k].ctypes.data for k in
+                                                  ("fs_d", "fs_d_bound", "fs_n", "fs_rho", "fs_mass")])
+        err = l.orc_run_column_fs(*(args + [ctypes.byref(fs)]))
+    else:
+        err = l.orc_run_column(*args)
     return err, tb, em, ang, out_dbg
 
 
@@ -139,8 +154,11 @@ def run_pamtra(pam, freqs, nummu=16, debug=False):
     ``angles_deg`` and the error code."""
     from pamtra_b200 import packing
     st = settings(packing.settings_from_nml(pam.nmlSet, nummu))
-    sp = packing.species_from_df(pam.df.data)
+    fullspec = bool(pam.nmlSet.get("hydro_fullspec", False))
+    sp = packing.species_from_df(pam.df.data, fullspec)
     cols = packing.profile_columns(pam.p, pam.df.nhydro)
+    if fullspec:
+        packing.fullspec_columns(cols, pam.df.dataFullSpec)
     nx, ny = int(pam.p["ngridx"]), int(pam.p["ngridy"])
     nout = int(cols["noutlevels"])
     N = nummu

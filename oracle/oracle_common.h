@@ -108,6 +108,13 @@ typedef struct {
   double p_1, p_2, p_3, p_4, d_1, d_2;
 } orc_species;
 
+// Full size spectra (nmlSet['hydro_fullspec'], src/hydrometeor_extinction.f90:122-151)
+// of one column: [L][nhydro][nbin], d_bound [L][nhydro][nbin + 1].
+typedef struct {
+  int32_t nbin;
+  const double *d, *d_bound, *n, *rho, *mass;
+} orc_fullspec;
+
 // Optional per-(layer,freq) intermediates for parity tests.
 typedef struct {
   double* kextatmo;        // [nfreq][L]            Np/m, bottom-up layer order

@@ -1387,12 +1387,32 @@ void orc_e_sat(double T, double* e) { *e = e_sat_gg_water(T); }
 // bottom-up [L+1], layer arrays [L], hydro arrays [L][H]; NaN = missing.
 // tb: [noutlevels][2N][nfreq][2]; emissivity: [2][nfreq][N]; angles: [2N].
 // Returns 0, or the reference error code (2) on a fatal condition.
+int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro, int L, const double* hgt_lev,
+                      const double* temp_lev, const double* press_lev, const double* relhum_lev, const double* hgt,
+                      const double* temp, const double* press, const double* relhum, const double* hydro_q,
+                      const double* hydro_n, const double* hydro_reff, double groundtemp, int noutlevels,
+                      const double* obs_height, char sfc_refl, int nfreq, const double* freqs, double* tb,
+                      double* emissivity_out, double* angles_deg, orc_debug* dbg, const orc_fullspec* fs);
+
 int orc_run_column(const orc_settings* st, const orc_species* sp, int nhydro, int L, const double* hgt_lev,
                    const double* temp_lev, const double* press_lev, const double* relhum_lev, const double* hgt,
                    const double* temp, const double* press, const double* relhum, const double* hydro_q,
                    const double* hydro_n, const double* hydro_reff, double groundtemp, int noutlevels,
                    const double* obs_height, char sfc_refl, int nfreq, const double* freqs, double* tb,
                    double* emissivity_out, double* angles_deg, orc_debug* dbg) {
+  return orc_run_column_fs(st, sp, nhydro, L, hgt_lev, temp_lev, press_lev, relhum_lev, hgt, temp, press, relhum,
+                           hydro_q, hydro_n, hydro_reff, groundtemp, noutlevels, obs_height, sfc_refl, nfreq, freqs,
+                           tb, emissivity_out, angles_deg, dbg, nullptr);
+}
+
+// As orc_run_column; with `fs` the size distributions come from the given
+// full spectra instead of hydro_q / hydro_n / hydro_reff.
+int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro, int L, const double* hgt_lev,
+                      const double* temp_lev, const double* press_lev, const double* relhum_lev, const double* hgt,
+                      const double* temp, const double* press, const double* relhum, const double* hydro_q,
+                      const double* hydro_n, const double* hydro_reff, double groundtemp, int noutlevels,
+                      const double* obs_height, char sfc_refl, int nfreq, const double* freqs, double* tb,
+                      double* emissivity_out, double* angles_deg, orc_debug* dbg, const orc_fullspec* fs) {
   const int N = st->nummu, n = 2 * N;
   Atmo a;
   a.L = L;
@@ -1455,6 +1475,43 @@ int orc_run_column(const orc_settings* st, const orc_species* sp, int nhydro, in
       for (int h = 0; h < nhydro; h++) qsum += hydro_q[z * nhydro + h];
       for (int h = 0; h < nhydro; h++) {
         const orc_species& s = sp[h];
+        if (fs) {
+          // src/hydrometeor_extinction.f90:122-151
+          const int nb = fs->nbin;
+          const size_t o = ((size_t)z * nhydro + h) * nb, ob = ((size_t)z * nhydro + h) * (nb + 1);
+          double nsum = 0.0;
+          for (int i = 0; i < nb; i++) nsum += fs->n[o + i];
+          if (!(nsum > 0.0 || st->hydro_threshold <= 0)) continue;
+          pres = true;
+          if (s.dist == D_DISABLED) continue;  // scat_name 'disabled' (src/scatProperties.f90:203)
+          Bins bn;
+          bn.nbin = nb;
+          bn.d_ds.assign(fs->d + o, fs->d + o + nb);
+          bn.diam = bn.d_ds;
+          bn.n_ds.assign(fs->n + o, fs->n + o + nb);
+          bn.dens.assign(fs->rho + o, fs->rho + o + nb);
+          bn.mass.assign(fs->mass + o, fs->mass + o + nb);
+          bn.delta_d.resize(nb);
+          for (int i = 0; i < nb; i++) bn.delta_d[i] = fs->d_bound[ob + i + 1] - fs->d_bound[ob + i];
+          std::vector<double> ndens(nb);
+          for (int i = 0; i < nb; i++) ndens[i] = bn.n_ds[i] / bn.delta_d[i];
+          double refre, refim;
+          if (s.liq_ice == 1) ref_water(a.temp[z] - F(273.15f), freq, refre, refim);
+          else ref_ice(a.temp[z], freq, refre, refim);
+          MieOut mo;
+          if (calc_mie_spheres(*st, freq * 1e9, s.liq_ice, bn, ndens, refre, refim, mo)) return 2;
+          nlegen_coef = std::max(nlegen_coef, mo.nlegen);
+          kexttot = kexttot + mo.kext;
+          backtot = backtot + mo.back;
+          if (kexttot == 0.0) salbedo = 0.0;
+          else salbedo = salbedo + (mo.salb * mo.kext);
+          if (nlegen_coef > 0)
+            for (int jj = 0; jj < nlegen_coef; jj++)
+              for (int k = 0; k < 3; k++) legen_coef[k][jj] = legen_coef[k][jj] + (mo.legen[k][jj] * mo.salb * mo.kext);
+          if (kexttot < 0.0 || std::isnan(kexttot)) return 2;
+          if (nlegen_coef > MAXNLEG - 1) return 2;
+          continue;
+        }
         if (s.dist == D_DISABLED) continue;
         double qall = (st->hydro_includehydroinrhoair && !std::isnan(qsum)) ? qsum : 0.0;
         double q_h = q2abs(hydro_q[z * nhydro + h], a.temp[z], a.press[z], a.q_hum[z], qall);

@@ -39,7 +39,8 @@ class Columns(ctypes.Structure):
                 ("freqs", _vp), ("hgt_lev", _vp), ("temp_lev", _vp), ("press_lev", _vp), ("relhum_lev", _vp),
                 ("hgt", _vp), ("temp", _vp), ("press", _vp), ("relhum", _vp), ("hydro_q", _vp),
                 ("hydro_n", _vp), ("hydro_reff", _vp), ("groundtemp", _vp), ("obs_height", _vp),
-                ("sfc_refl", _vp)]
+                ("sfc_refl", _vp), ("fs_nbin", _i32), ("fs_d", _vp), ("fs_d_bound", _vp), ("fs_n", _vp),
+                ("fs_rho", _vp), ("fs_mass", _vp)]
 
 
 class Outputs(ctypes.Structure):
@@ -161,8 +162,9 @@ class Engine(object):
         c.species = species.ctypes.data if len(species) else None
         for k in ("nlyrs", "nummu", "nfreq", "freqs", "hgt_lev", "temp_lev", "press_lev", "relhum_lev", "hgt",
                   "temp", "press", "relhum", "hydro_q", "hydro_n", "hydro_reff", "groundtemp", "obs_height",
-                  "sfc_refl"):
+                  "sfc_refl", "fs_d", "fs_d_bound", "fs_n", "fs_rho", "fs_mass"):
             setattr(c, k, _ptr(arrs.get(k)))
+        c.fs_nbin = int(arrs.get("fs_nbin", 0))
         return c
 
     @staticmethod

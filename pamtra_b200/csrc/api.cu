@@ -260,7 +260,9 @@ Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms) {
   const size_t C = c->ncol, Lm = c->max_nlyrs, H = c->nhydro, Fm = c->max_nfreq;
   int mb = 1;
   const size_t nsp = c->species_stride ? C * H : H;
-  for (size_t i = 0; i < nsp; i++) mb = std::max(mb, c->species[i].dist == PAMTRA_B200_DIST_MONO ? 2 : c->species[i].nbin);
+  if (c->fs_d) mb = std::max(mb, c->fs_nbin);
+  else
+    for (size_t i = 0; i < nsp; i++) mb = std::max(mb, c->species[i].dist == PAMTRA_B200_DIST_MONO ? 2 : c->species[i].nbin);
   p.max_nbin = mb;
   int mask = c->nummu_mask ? c->nummu_mask : (default_nummu == 8 ? 1 : default_nummu == 16 ? 2 : 4);
   p.maxN = (mask & 4) ? 32 : (mask & 2) ? 16 : 8;
@@ -726,6 +728,8 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     return PAMTRA_B200_FATAL;
   if (cols->nhydro > 0 && !cols->species) return PAMTRA_B200_FATAL;
   if (!(st->nummu == 8 || st->nummu == 16 || st->nummu == 32)) return PAMTRA_B200_FATAL;
+  if (cols->fs_d && (cols->fs_nbin < 1 || !cols->fs_d_bound || !cols->fs_n || !cols->fs_rho || !cols->fs_mass))
+    return PAMTRA_B200_FATAL;
   cudaStream_t stream = (cudaStream_t)stream_;
   cudaSetDevice(ctx->device);
   pamtra_b200_species dummy{};
@@ -780,6 +784,8 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   b.hgt = cc.hgt; b.temp = cc.temp; b.press = cc.press; b.relhum = cc.relhum;
   b.hydro_q = cc.hydro_q; b.hydro_n = cc.hydro_n; b.hydro_reff = cc.hydro_reff;
   b.groundtemp = cc.groundtemp; b.obs_height = cc.obs_height; b.sfc_refl = cc.sfc_refl;
+  b.fs_nbin = cc.fs_nbin; b.fs_d = cc.fs_d; b.fs_d_bound = cc.fs_d_bound; b.fs_n = cc.fs_n; b.fs_rho = cc.fs_rho;
+  b.fs_mass = cc.fs_mass;
 
   Work w{};
   w.hgt_lev = (double*)(A + pl.o_hgt_lev); w.temp_lev = (double*)(A + pl.o_temp_lev);
@@ -830,7 +836,9 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   mark(ctx, stream, STG_PREP);
   if (H > 0) {
     const size_t ns = C * Lm * H;
-    k_psd<<<(unsigned)((ns + 127) / 128), 128, 0, stream>>>(b, w, *st); launches++;
+    if (cc.fs_d) k_fullspec<<<(unsigned)((ns + 127) / 128), 128, 0, stream>>>(b, w, *st);
+    else k_psd<<<(unsigned)((ns + 127) / 128), 128, 0, stream>>>(b, w, *st);
+    launches++;
   } else {
     cudaMemsetAsync(w.slot_st, 0, 1, stream);
   }
@@ -921,6 +929,8 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
 int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, const pamtra_b200_columns* hc,
                              const pamtra_b200_outputs* ho, int32_t precision, void* stream_) {
   if (!ctx || !st || !hc || !ho || !ho->tb) return PAMTRA_B200_FATAL;
+  if (hc->fs_d && (hc->fs_nbin < 1 || !hc->fs_d_bound || !hc->fs_n || !hc->fs_rho || !hc->fs_mass))
+    return PAMTRA_B200_FATAL;
   cudaStream_t stream = (cudaStream_t)stream_;
   cudaSetDevice(ctx->device);
   const size_t C = hc->ncol, Lm = hc->max_nlyrs, Fm = hc->max_nfreq, H = hc->nhydro, NO = hc->noutlevels;
@@ -944,6 +954,10 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
   size_t o_q = add(hc->hydro_q, C * Lm * H * 8), o_n = add(hc->hydro_n, C * Lm * H * 8);
   size_t o_re = add(hc->hydro_reff, C * Lm * H * 8);
   size_t o_g = add(hc->groundtemp, C * 8), o_ob = add(hc->obs_height, C * NO * 8), o_sr = add(hc->sfc_refl, C);
+  const size_t FB = hc->fs_d ? C * Lm * H * (size_t)hc->fs_nbin : 0;
+  size_t o_fd = add(hc->fs_d, FB * 8), o_fdb = add(hc->fs_d ? hc->fs_d_bound : nullptr, (FB + C * Lm * H) * 8);
+  size_t o_fn = add(hc->fs_d ? hc->fs_n : nullptr, FB * 8), o_fr = add(hc->fs_d ? hc->fs_rho : nullptr, FB * 8);
+  size_t o_fm = add(hc->fs_d ? hc->fs_mass : nullptr, FB * 8);
   size_t o_tb = add(nullptr, C * NO * NA * Fm * 2 * 8);
   size_t o_em = add(nullptr, ho->emissivity ? C * 2 * Fm * hc->max_nummu * 8 : 0);
   size_t o_an = add(nullptr, ho->angles_deg ? NA * 8 : 0);
@@ -986,6 +1000,13 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
   dc.groundtemp = (const double*)dp(hc->groundtemp, o_g);
   dc.obs_height = (const double*)dp(hc->obs_height, o_ob);
   dc.sfc_refl = (const int8_t*)dp(hc->sfc_refl, o_sr);
+  if (hc->fs_d) {
+    dc.fs_d = (const double*)(D + o_fd);
+    dc.fs_d_bound = (const double*)(D + o_fdb);
+    dc.fs_n = (const double*)(D + o_fn);
+    dc.fs_rho = (const double*)(D + o_fr);
+    dc.fs_mass = (const double*)(D + o_fm);
+  }
   pamtra_b200_outputs dout{};
   dout.tb = (double*)(D + o_tb);
   dout.emissivity = ho->emissivity ? (double*)(D + o_em) : nullptr;
@@ -1097,7 +1118,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
       cols->max_nfreq < 1 || cols->max_nfreq > PAMTRA_B200_NOALLOC_MAX_NFREQ || cols->nhydro < 0 ||
       cols->nhydro > PAMTRA_B200_NOALLOC_MAX_NHYDRO || cols->noutlevels < 1 || cols->noutlevels > 2 ||
       !(cols->max_nummu == 8 || cols->max_nummu == 16) || !(st->nummu == 8 || st->nummu == 16) ||
-      (cols->nhydro > 0 && !cols->species))
+      (cols->nhydro > 0 && !cols->species) || cols->fs_d)
     return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PAMTRA_B200_FATAL;

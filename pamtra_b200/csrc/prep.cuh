@@ -588,6 +588,43 @@ __global__ void k_psd(Batch b, Work w, pamtra_b200_settings st) {
   w.slot_st[s_idx] = 2;
 }
 
+// Size distributions given as full spectra (src/hydrometeor_extinction.f90:122-151):
+// bins, densities and masses are taken as given, the bin widths from the bin
+// bounds; a slot takes part when its number concentrations sum above zero, or
+// for every slot when hydro_threshold <= 0.  One thread per (column, layer,
+// species) slot, as k_psd.
+__global__ void k_fullspec(Batch b, Work w, pamtra_b200_settings st) {
+  const size_t s_idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int Lm = b.max_nlyrs, H = b.nhydro;
+  if (s_idx >= (size_t)b.ncol * Lm * H) return;
+  const int z = (s_idx / H) % Lm;
+  const int c = s_idx / ((size_t)H * Lm);
+  w.slot_st[s_idx] = 0;
+  w.slot_nb[s_idx] = 0;
+  if (z >= b.nlyrs[c]) return;
+  const int nb = b.fs_nbin;
+  const double* n = b.fs_n + s_idx * nb;
+  double nsum = 0.0;
+  for (int i = 0; i < nb; i++) nsum += n[i];
+  if (!(nsum > 0.0 || st.hydro_threshold <= 0)) return;
+  w.slot_st[s_idx] = 1;
+  if (b.species_of(c, s_idx % H).dist == PAMTRA_B200_DIST_DISABLED) return;  // scat_name 'disabled'
+  const double* d = b.fs_d + s_idx * nb;
+  const double* db = b.fs_d_bound + s_idx * (nb + 1);
+  const double* rho = b.fs_rho + s_idx * nb;
+  const double* mass = b.fs_mass + s_idx * nb;
+  const size_t base = s_idx * (size_t)b.max_nbin;
+  for (int i = 0; i < nb; i++) {
+    w.b_d[base + i] = d[i];
+    w.b_dd[base + i] = db[i + 1] - db[i];
+    w.b_nd[base + i] = n[i];
+    w.b_rho[base + i] = rho[i];
+    w.b_mass[base + i] = mass[i];
+  }
+  w.slot_nb[s_idx] = nb;
+  w.slot_st[s_idx] = 2;
+}
+
 // Compaction of hydrometeor-bearing layers: pres_idx[c][z] = compact index
 // (column-major order, deterministic) or -1; plist[p] = c*Lm + z.  One block.
 __global__ void k_compact(Batch b, Work w) {

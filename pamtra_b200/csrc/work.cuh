@@ -21,6 +21,9 @@ struct Batch {
   const double* groundtemp;
   const double* obs_height;
   const int8_t* sfc_refl;
+  // full size spectra [C][Lm][H][fs_nbin] (d_bound: fs_nbin + 1); fs_d NULL = derived
+  int fs_nbin;
+  const double *fs_d, *fs_d_bound, *fs_n, *fs_rho, *fs_mass;
 
   __device__ __forceinline__ int col_nfreq(int c) const { return nfreq ? nfreq[c] : max_nfreq; }
   __device__ __forceinline__ double freq(int c, int f) const {

@@ -100,3 +100,30 @@ class pamDescriptorFile(object):
         (the reference's ``data4D``, libWrapper.py:117-121)."""
         assert key in self.names
         self.data4D[key] = np.asarray(arr, dtype=float)
+
+    def addFullSpectra(self):
+        """Create the full-spectrum arrays of ``dataFullSpec``, shaped
+        (ngridx, ngridy, max_nlyrs, nhydro, nbin) (``d_bound_ds``: nbin + 1)
+        and zero-filled, as descriptorFile.py:173-234 does; the caller fills
+        them and sets ``nmlSet['hydro_fullspec'] = True``.  Species must be added
+        first, all with the same ``nbin``; of their descriptor rows only
+        ``liq_ice`` and ``scat_name`` are used then.  ``rho_ds`` is the particle
+        density (kg/m3), ``d_ds`` the diameter the scattering is computed at
+        (m), ``d_bound_ds`` the bin edges (m), ``n_ds`` the number
+        concentration per bin (1/m3, not normalised by the bin width),
+        ``mass_ds`` the particle mass (kg).  ``area_ds``, ``as_ratio``,
+        ``canting``, ``fallvelocity`` and the ``rg_*`` parameters are created for
+        the reference's radar and SSRGA paths and not read by the passive Mie
+        path."""
+        assert len(self.data) > 0
+        assert np.min(self.data["nbin"]) == np.max(self.data["nbin"])
+        self.fs_nbin = int(np.max(self.data["nbin"]))
+        par = self.parent
+        shp = par._shape4D + (self.fs_nbin,)
+        par._shape5D = shp
+        par._shape5Dplus = par._shape4D + (self.fs_nbin + 1,)
+        for key in ("rho_ds", "d_ds", "n_ds", "mass_ds", "area_ds", "as_ratio", "canting", "fallvelocity"):
+            self.dataFullSpec[key] = np.zeros(shp)
+        self.dataFullSpec["d_bound_ds"] = np.zeros(par._shape5Dplus)
+        for key, v in (("rg_kappa_ds", 0.19), ("rg_beta_ds", 0.23), ("rg_gamma_ds", 5. / 3.), ("rg_zeta_ds", 1.)):
+            self.dataFullSpec[key] = np.full(shp, v)

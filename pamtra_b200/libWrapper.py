@@ -23,19 +23,25 @@ ACTIVE_KEYS = ["Ze", "Att_hydro", "Att_atmo", "radar_hgt", "radar_moments", "rad
                "psd_mass", "psd_area", "psd_bscat"]
 
 
-def present_bound(cols, df_data):
+def present_bound(cols, df_data, hydro_threshold=None):
     """Upper bound on the number of (column, layer) pairs that can carry
-    hydrometeors (src/hydrometeor_extinction.f90:276-283 presence test)."""
+    hydrometeors (src/hydrometeor_extinction.f90:276-283 presence test; for
+    full spectra the test of lines 142-148)."""
     if len(df_data) == 0:
         return 0
+    L = cols["max_nlyrs"]
+    valid = np.arange(L)[None, :] < cols["nlyrs"][:, None]
+    if cols.get("fs_d") is not None:
+        if hydro_threshold is not None and hydro_threshold <= 0:
+            return int(np.sum(valid))
+        nsum = cols["fs_n"].sum(axis=-1)  # (ncol, L, H)
+        return int(np.sum(np.any(nsum > 0, axis=-1) & valid))
     if np.any(np.asarray(df_data["moment_in"]) == 0):
         return int(np.sum(cols["nlyrs"]))
     any_q = np.zeros(cols["hydro_q"].shape[:2], dtype=bool)
     for k in ("hydro_q", "hydro_n", "hydro_reff"):
         a = cols[k]
         any_q |= np.any((a != 0) | np.isnan(a), axis=-1)
-    L = cols["max_nlyrs"]
-    valid = np.arange(L)[None, :] < cols["nlyrs"][:, None]
     return int(np.sum(any_q & valid))
 
 
@@ -57,16 +63,21 @@ def PamtraFortranWrapper(sets, nmlSets, descriptorFile, descriptorFile4D, descri
     ``sets['freqs']`` on the GPU (host buffers in, host arrays out)."""
     if descriptorFile4D:
         raise NotImplementedError("4D descriptor fields are not on this path")
-    if nmlSets.get("hydro_fullspec", False):
-        raise NotImplementedError("hydro_fullspec input is not on this path")
     if not nmlSets.get("passive", True):
         raise NotImplementedError("passive=False: only the passive path is built")
     freqs = list(sets["freqs"])
     nf = len(freqs)
     st = packing.settings_from_nml(nmlSets, nummu)
-    sp = packing.species_from_df(descriptorFile)
+    fullspec = bool(nmlSets.get("hydro_fullspec", False))
+    sp = packing.species_from_df(descriptorFile, fullspec)
     nhydro = len(sp)
     cols = packing.profile_columns(profile, nhydro)
+    if fullspec:
+        # full spectra replace the moment-based size distributions
+        # (libWrapper.py:191-202 of the reference)
+        if not descriptorFileFS:
+            raise ValueError("hydro_fullspec needs the arrays of descriptorFile.addFullSpectra()")
+        packing.fullspec_columns(cols, descriptorFileFS)
     arrs = host_inputs(cols, freqs)
     ncol, L, nout = cols["ncol"], cols["max_nlyrs"], cols["noutlevels"]
     N = nummu
@@ -83,7 +94,8 @@ def PamtraFortranWrapper(sets, nmlSets, descriptorFile, descriptorFile4D, descri
             out[k] = np.zeros((ncol, nf, L))
     mask = {8: 1, 16: 2, 32: 4}[N]
     eng = engine(device)
-    c = eng.make_columns(arrs, sp, nmu_mask=mask, max_present=present_bound(cols, descriptorFile), max_nummu=N)
+    c = eng.make_columns(arrs, sp, nmu_mask=mask, max_present=present_bound(cols, descriptorFile, st.hydro_threshold),
+                         max_nummu=N)
     o = eng.make_outputs(out)
     eng.run_host(st, c, o, precision)
 

@@ -78,8 +78,6 @@ def settings_from_nml(nmlSet, nummu=16):
         raise NotImplementedError("gas_mod %r: only R98 is on this path" % nmlSet["gas_mod"])
     if str(nmlSet.get("liq_mod", "TKC")).strip() != "TKC":
         raise NotImplementedError("liq_mod %r: only TKC is on this path" % nmlSet["liq_mod"])
-    if nmlSet.get("hydro_fullspec", False):
-        raise NotImplementedError("hydro_fullspec input is not on this path")
     outpol = str(nmlSet.get("outpol", "VH")).strip()
     if outpol not in ("VH", "IQ"):
         raise ValueError("outpol must be VH or IQ")
@@ -119,12 +117,18 @@ def disabled_species():
     return r
 
 
-def species_from_df(data):
-    """Descriptor recarray -> structured array of ``pamtra_b200_species``."""
+def species_from_df(data, fullspec=False):
+    """Descriptor recarray -> structured array of ``pamtra_b200_species``.
+    With ``fullspec`` (sizes from ``dataFullSpec``) ``dist_name`` is not read
+    (src/hydrometeor_extinction.f90:122-151); a species whose ``scat_name`` is
+    'disabled' still marks its layers as carrying hydrometeors but adds no
+    scattering (src/scatProperties.f90:203)."""
     out = np.zeros(len(data), dtype=SPECIES_DTYPE)
     for i, row in enumerate(data):
         dist = str(row["dist_name"]).strip()
         scat = str(row["scat_name"]).strip()
+        if fullspec:
+            dist = "exp"
         if dist not in DIST_CODES or dist == "exp_cosmo_snow":
             raise NotImplementedError("dist_name %r is not on this path" % dist)
         if scat not in SCAT_CODES:
@@ -137,6 +141,31 @@ def species_from_df(data):
                   "d_1", "d_2"):
             out[i][k] = float(row[k])
     return out
+
+
+FULLSPEC_KEYS = ("d_ds", "d_bound_ds", "n_ds", "rho_ds", "mass_ds")
+
+
+def fullspec_columns(cols, dataFullSpec):
+    """Add the full spectra of ``dataFullSpec`` (descriptorFile.addFullSpectra)
+    to packed ``cols`` as ``fs_d``, ``fs_d_bound``, ``fs_n``, ``fs_rho``,
+    ``fs_mass``: C-contiguous float64, one row per column,
+    [max_nlyrs][nhydro][nbin] (``fs_d_bound``: nbin + 1), plus ``fs_nbin``."""
+    ncol, L = cols["ncol"], cols["max_nlyrs"]
+    nh = cols["hydro_q"].shape[-1]
+    for k in FULLSPEC_KEYS:
+        if k not in dataFullSpec:
+            raise ValueError("hydro_fullspec: dataFullSpec[%r] is missing" % k)
+    nb = int(np.asarray(dataFullSpec["d_ds"]).shape[-1])
+    for k in FULLSPEC_KEYS:
+        tail = nb + 1 if k == "d_bound_ds" else nb
+        a = np.asarray(dataFullSpec[k], dtype=np.float64)
+        if a.size != ncol * L * nh * tail:
+            raise ValueError("hydro_fullspec: dataFullSpec[%r] has shape %s, expected (ngridx, ngridy, %d, %d, %d)"
+                             % (k, a.shape, L, nh, tail))
+        cols["fs_" + k[:-3]] = np.ascontiguousarray(a.reshape(ncol, L, nh, tail))
+    cols["fs_nbin"] = nb
+    return cols
 
 
 def profile_columns(p, nhydro):

@@ -271,3 +271,52 @@ def mie_heavy_batch(ncol=2048, seed=6):
     top = np.full(ncol, 12000.0)
     qs = [[10 ** rng.uniform(-5.0, np.log10(2e-3)) for _ in kinds] for _ in range(ncol)]
     return _packed(st, sp, 0, nly, [MIE_HEAVY_FREQS], None, [kinds] * ncol, qs, top, rng, 100, 4, False)
+
+
+# ------------------------------------------------------------------ full size spectra
+ICE_FS = ("ice", 1.0, -1, 200.0, -99.0, -99.0, np.pi / 4.0, 2.0, 0, 40, "exp", 3000.0, 3e8, -99.0, -99.0, 100e-6,
+          1000e-6, "mie-sphere", "heymsfield10_particles", 0.0)
+RAIN_FS = ("rain", 1.0, 1, -99.0, -99.0, -99.0, -99.0, -99.0, 0, 40, "exp", 2000.0, 8e6, -99.0, -99.0, 100e-6,
+           6000e-6, "mie-sphere", "khvorostyanov01_drops", 0.0)
+
+
+def fullspec_pam(ncol=4, nlay=30, seed=7):
+    """Columns whose size distributions are given as full spectra
+    (``nmlSet['hydro_fullspec']``): soft ice spheres (200 kg/m3, 100-1000 um)
+    and rain (100 um - 6 mm), 40 bins each, on per-(column, layer) bin edges
+    with exponential spectra of seeded slope and intercept; about a quarter
+    of the (layer, species) slots are left empty."""
+    warnings.simplefilter("ignore")
+    rng = np.random.default_rng(seed)
+    cols = _columns(ncol, nlay, seed, q_cloud=0.0, q_rain=0.0)
+    pam = core.pyPamtra()
+    pam.df.addHydrometeor(ICE_FS)
+    pam.df.addHydrometeor(RAIN_FS)
+    pam.nmlSet["hydro_adaptive_grid"] = False
+    pam.nmlSet["emissivity"] = 0.5
+    pam.createProfile(hgt_lev=cols["hgt_lev"].reshape(ncol, 1, nlay + 1),
+                      temp_lev=cols["temp_lev"].reshape(ncol, 1, nlay + 1),
+                      press_lev=cols["press_lev"].reshape(ncol, 1, nlay + 1),
+                      relhum_lev=cols["relhum_lev"].reshape(ncol, 1, nlay + 1),
+                      hydro_q=np.zeros((ncol, 1, nlay, 2)), groundtemp=290.0, sfc_refl="S",
+                      obs_height=np.tile([833000.0, 0.0], (ncol, 1, 1)))
+    pam.nmlSet["hydro_fullspec"] = True
+    pam.df.addFullSpectra()
+    fs = pam.df.dataFullSpec
+    nb = pam.df.fs_nbin
+    for h, (d1, d2, rho) in enumerate(((100e-6, 1000e-6, 200.0), (100e-6, 6000e-6, 1000.0))):
+        jit = rng.uniform(0.9, 1.1, (ncol, 1, nlay, 1))
+        edges = np.exp(np.linspace(np.log(d1), np.log(d2), nb + 1))[None, None, None, :] * jit
+        fs["d_bound_ds"][..., h, :] = edges
+        d = 0.5 * (edges[..., 1:] + edges[..., :-1])
+        fs["d_ds"][..., h, :] = d
+        lam = 10 ** rng.uniform(3.0, 4.0, (ncol, 1, nlay, 1))
+        n0 = 10 ** rng.uniform(6.0, 8.0, (ncol, 1, nlay, 1))
+        n = n0 * np.exp(-lam * d) * np.diff(edges, axis=-1)
+        n *= (rng.uniform(size=(ncol, 1, nlay, 1)) > 0.25)
+        fs["n_ds"][..., h, :] = n
+        fs["rho_ds"][..., h, :] = rho
+        fs["mass_ds"][..., h, :] = np.pi / 6.0 * rho * d ** 3
+        fs["area_ds"][..., h, :] = np.pi / 4.0 * d ** 2
+        fs["as_ratio"][..., h, :] = 1.0
+    return pam
