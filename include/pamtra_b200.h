@@ -152,6 +152,17 @@ typedef struct pamtra_b200_outputs {
   double* ze;
   double* att_hydro;
   double* att_atmo;
+  /* save_psd (src/hydrometeor_extinction.f90:303-309): the size bins of the
+   * moment-based distributions, [ncol][max_nlyrs][nhydro][psd_nbin]: bin
+   * centre (m), width (m), number per bin (1/m3), particle mass (kg) and
+   * cross-section area (m2, -99 without an area-size relation); -9999 where
+   * a slot carries no particles, for full spectra input and beyond a
+   * species' bins.  psd_bscat: backscattering cross section per particle
+   * (m2) of each bin at the column's last frequency, for moment-based and
+   * full spectra alike, NaN for an empty bin (src/scatProperties.f90:914-917).
+   * psd_nbin >= every species' bin count; NULL psd_d skips all six. */
+  int32_t psd_nbin;
+  double *psd_d, *psd_deltad, *psd_n, *psd_mass, *psd_area, *psd_bscat;
 } pamtra_b200_outputs;
 
 typedef struct pamtra_b200_ctx pamtra_b200_ctx;
@@ -259,7 +270,8 @@ int32_t pamtra_b200_mmult_3xtf32_batched(const double* a, const double* b, doubl
  * allocator.  All pointers in `cols` and `out` are DEVICE pointers,
  * `cols->species` included.  Limits: ncol = 1, max_nlyrs <= 64,
  * max_nfreq <= 4, nhydro <= 4, nbin <= 64 per species, nummu 8 or 16,
- * noutlevels <= 2, no full spectra (fs_d NULL); other requests return
+ * noutlevels <= 2, no full spectra (fs_d NULL) and no save_psd outputs
+ * (psd_d NULL); other requests return
  * PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE without running.  The first call on a device (with
  * that device current) resolves the array's device address with
  * cudaGetSymbolAddress and fills the quadrature and line tables; make that

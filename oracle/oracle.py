@@ -45,10 +45,14 @@ class OrcFullspec(ctypes.Structure):
                 ("n", ctypes.c_void_p), ("rho", ctypes.c_void_p), ("mass", ctypes.c_void_p)]
 
 
+PSD_KEYS = ("psd_d", "psd_deltad", "psd_n", "psd_mass", "psd_area", "psd_bscat")
+
+
 class OrcDebug(ctypes.Structure):
     _fields_ = [(k, ctypes.c_void_p) for k in
                 ("kextatmo", "kexttot", "salbedo", "nlegen", "legen", "present", "scatter_matrix", "ext",
-                 "emis", "num_doubles", "back", "ze", "att_hydro", "att_atmo")]
+                 "emis", "num_doubles", "back", "ze", "att_hydro", "att_atmo")] + \
+        [("psd_nbin", ctypes.c_int32)] + [(k, ctypes.c_void_p) for k in PSD_KEYS]
 
 
 def build():
@@ -94,10 +98,11 @@ def settings(pk_settings):
     return s
 
 
-def run_column(st, species, cols, c, freqs, debug=False):
+def run_column(st, species, cols, c, freqs, debug=False, psd_nbin=0):
     """Run column ``c`` of packed ``cols`` (pamtra_b200.packing.profile_columns).
     ``debug`` True returns all intermediates, "radar" only the simple-radar
-    outputs (back, ze, att_hydro, att_atmo; filled when ``st.active``)."""
+    outputs (back, ze, att_hydro, att_atmo; filled when ``st.active``).
+    ``psd_nbin`` > 0 adds the save_psd bins, [L][nhydro][psd_nbin]."""
     l = lib()
     L = int(cols["nlyrs"][c])
     Lmax = int(cols["max_nlyrs"])
@@ -129,6 +134,14 @@ def run_column(st, species, cols, c, freqs, debug=False):
                        back=np.zeros((nf, L)), ze=np.zeros((nf, L)), att_hydro=np.zeros((nf, L)),
                        att_atmo=np.zeros((nf, L)))
         dbg = OrcDebug(**{k: v.ctypes.data for k, v in out_dbg.items()})
+    if psd_nbin > 0:
+        if out_dbg is None:
+            out_dbg = dict()
+            dbg = OrcDebug()
+        for k in PSD_KEYS:
+            out_dbg[k] = np.full((L, H, psd_nbin), -9999.0)
+            setattr(dbg, k, out_dbg[k].ctypes.data)
+        dbg.psd_nbin = psd_nbin
     sp = np.ascontiguousarray(species)
     refl = bytes([int(cols["sfc_refl"][c]) & 0xFF])
     args = [ctypes.byref(st), sp.ctypes.data if H else None, H, L,
@@ -168,16 +181,26 @@ def run_pamtra(pam, freqs, nummu=16, debug=False):
     ang = None
     dbgs = []
     Lm, nf = int(cols["max_nlyrs"]), len(freqs)
+    H = len(sp)
+    # save_psd: bins of the moment-based distributions (-9999 for full spectra)
+    # and per-bin backscattering cross sections
+    psd_nbin = max(2, int(np.max(pam.df.data["nbin"]))) if pam.nmlSet.get("save_psd", False) and H else 0
+    psd = {k: np.full((nx * ny, Lm, H, psd_nbin), -9999.0) for k in PSD_KEYS} if psd_nbin else None
     ze = np.full((nx * ny, Lm, nf), -9999.0)
     ath = np.zeros((nx * ny, Lm, nf))
     ata = np.zeros((nx * ny, Lm, nf))
     for c in range(nx * ny):
-        err, t, e, a, d = run_column(st, sp, cols, c, freqs, debug or ("radar" if st.active else False))
+        err, t, e, a, d = run_column(st, sp, cols, c, freqs, debug or ("radar" if st.active else False),
+                                     psd_nbin=psd_nbin)
         err_all = max(err_all, err)
         tb[c], em[c], ang = t, e, a
         if st.active:
             L = int(cols["nlyrs"][c])
             ze[c, :L], ath[c, :L], ata[c, :L] = d["ze"].T, d["att_hydro"].T, d["att_atmo"].T
+        if psd is not None:
+            L = int(cols["nlyrs"][c])
+            for k in PSD_KEYS:
+                psd[k][c, :L] = d[k]
         dbgs.append(d)
     r = dict(tb=tb.reshape(nx, ny, nout, 2 * N, len(freqs), 2),
              emissivity=em.reshape(nx, ny, 2, len(freqs), N), angles_deg=ang)
@@ -185,6 +208,9 @@ def run_pamtra(pam, freqs, nummu=16, debug=False):
         r["Ze"] = ze.reshape(nx, ny, Lm, nf, 1, 1)
         r["Att_hydro"] = ath.reshape(nx, ny, Lm, nf, 1)
         r["Att_atmo"] = ata.reshape(nx, ny, Lm, nf)
+    if psd is not None:
+        for k in PSD_KEYS:
+            r[k] = psd[k].reshape(nx, ny, Lm, H, psd_nbin)
     if debug:
         r["debug"] = dbgs
     return r, err_all

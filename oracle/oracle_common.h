@@ -131,6 +131,11 @@ typedef struct {
   double* ze;              // [nfreq][L]            simple radar, dBZ (-9999 without hydrometeors)
   double* att_hydro;       // [nfreq][L]            dB
   double* att_atmo;        // [nfreq][L]            dB
+  // save_psd bins [L][nhydro][psd_nbin] of the moment-based distributions
+  // (left untouched where none is computed; the caller fills -9999)
+  int32_t psd_nbin;
+  double *psd_d, *psd_deltad, *psd_n, *psd_mass, *psd_area;
+  double* psd_bscat;       // [L][nhydro][psd_nbin] m2 per particle, last frequency (also for full spectra)
 } orc_debug;
 
 }

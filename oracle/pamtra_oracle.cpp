@@ -791,6 +791,7 @@ struct MieOut {
   double kext = 0, salb = 0, back = 0;
   int nlegen = 0;
   double legen[4][MAXNLEG];
+  std::vector<double> back_spec;  // per bin, m2/m4 (0 where no particles)
 };
 
 // src/mie_spheres.f90:14-345 calc_mie_spheres
@@ -800,6 +801,7 @@ int calc_mie_spheres(const orc_settings& st, double freq_hz, int liq_ice, const 
   o.kext = o.salb = o.back = 0;
   o.nlegen = 0;
   const int nb = bn.nbin;
+  o.back_spec.assign(nb, 0.0);
   const double wavelength = C_LIGHT / freq_hz;
   cplx msphere;
   cplx m_ice = cmk(refre, -refim);
@@ -838,6 +840,7 @@ int calc_mie_spheres(const orc_settings& st, double freq_hz, int liq_ice, const 
     sumqe = sumqe + (qext * del_d_eff);
     sumqs = sumqs + (qscat * del_d_eff);
     sumqback = sumqback + (qback * del_d_eff);
+    o.back_spec[ir] = qback;
     nmie = std::min(nmie, nterms);
     for (int i = 0; i < nquad; i++) {
       double pp[4];
@@ -1454,7 +1457,16 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
   // hydrometeor presence per layer is frequency independent
   std::vector<int> present(L, 0);
 
+  // save_psd per-particle backscattering cross section of the last frequency
+  // (src/scatProperties.f90:914-917: back_spec / num_density, NaN where a bin is empty)
+  int fi_cur = 0;
+  auto save_bscat = [&](int z, int h, const MieOut& mo, const std::vector<double>& ndens) {
+    if (!dbg || !dbg->psd_bscat || fi_cur != nfreq - 1) return;
+    const size_t po = ((size_t)z * nhydro + h) * dbg->psd_nbin;
+    for (int i = 0; i < (int)ndens.size() && i < dbg->psd_nbin; i++) dbg->psd_bscat[po + i] = mo.back_spec[i] / ndens[i];
+  };
   for (int fi = 0; fi < nfreq; fi++) {
+    fi_cur = fi;
     const double freq = freqs[fi];
     const double wl = C_LIGHT / (freq * 1.e3);
     // gas (src/get_gasabs.f90)
@@ -1500,6 +1512,7 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
           else ref_ice(a.temp[z], freq, refre, refim);
           MieOut mo;
           if (calc_mie_spheres(*st, freq * 1e9, s.liq_ice, bn, ndens, refre, refim, mo)) return 2;
+          save_bscat(z, h, mo, ndens);
           nlegen_coef = std::max(nlegen_coef, mo.nlegen);
           kexttot = kexttot + mo.kext;
           backtot = backtot + mo.back;
@@ -1528,6 +1541,23 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
         bool any = false;
         for (int i = 0; i < bn.nbin; i++) any |= (bn.n_ds[i] > 0);
         if (!any) continue;
+        if (dbg && dbg->psd_d && fi == 0) {
+          // src/hydrometeor_extinction.f90:303-309; area: src/drop_size_dist.f90:168-182
+          const size_t po = ((size_t)z * nhydro + h) * dbg->psd_nbin;
+          for (int i = 0; i < bn.nbin && i < dbg->psd_nbin; i++) {
+            const double d = bn.d_ds[i];
+            double area = -99.;
+            if (s.alpha_as > 0. && s.beta_as > 0.) {
+              area = s.alpha_as * std::pow(d, s.beta_as);
+              if (s.liq_ice == -1 && st->hydro_limit_density_area && area > d * d) area = d * d;
+            }
+            dbg->psd_d[po + i] = d;
+            dbg->psd_deltad[po + i] = bn.delta_d[i];
+            dbg->psd_n[po + i] = bn.n_ds[i];
+            dbg->psd_mass[po + i] = bn.mass[i];
+            dbg->psd_area[po + i] = area;
+          }
+        }
         std::vector<double> ndens(bn.nbin);
         for (int i = 0; i < bn.nbin; i++) ndens[i] = bn.n_ds[i] / bn.delta_d[i];
         double refre, refim;
@@ -1535,6 +1565,7 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
         else ref_ice(a.temp[z], freq, refre, refim);
         MieOut mo;
         if (calc_mie_spheres(*st, freq * 1e9, s.liq_ice, bn, ndens, refre, refim, mo)) return 2;
+        save_bscat(z, h, mo, ndens);
         nlegen_coef = std::max(nlegen_coef, mo.nlegen);
         kexttot = kexttot + mo.kext;
         backtot = backtot + mo.back;  // rt_back (scatProperties.f90:922)

@@ -47,7 +47,8 @@ class Outputs(ctypes.Structure):
     """Mirror of ``pamtra_b200_outputs``."""
     _fields_ = [("tb", _vp), ("emissivity", _vp), ("angles_deg", _vp), ("status", _vp), ("kextatmo", _vp),
                 ("kexttot", _vp), ("salbedo", _vp), ("scatter_matrix", _vp), ("num_doubles", _vp),
-                ("ze", _vp), ("att_hydro", _vp), ("att_atmo", _vp)]
+                ("ze", _vp), ("att_hydro", _vp), ("att_atmo", _vp), ("psd_nbin", _i32), ("psd_d", _vp),
+                ("psd_deltad", _vp), ("psd_n", _vp), ("psd_mass", _vp), ("psd_area", _vp), ("psd_bscat", _vp)]
 
 
 EXPORTS = ["pamtra_b200_create", "pamtra_b200_destroy", "pamtra_b200_workspace_bytes", "pamtra_b200_reserve",
@@ -171,8 +172,11 @@ class Engine(object):
     def make_outputs(outs):
         o = Outputs()
         for k in ("tb", "emissivity", "angles_deg", "status", "kextatmo", "kexttot", "salbedo", "scatter_matrix",
-                  "num_doubles", "ze", "att_hydro", "att_atmo"):
+                  "num_doubles", "ze", "att_hydro", "att_atmo", "psd_d", "psd_deltad", "psd_n", "psd_mass",
+                  "psd_area", "psd_bscat"):
             setattr(o, k, _ptr(outs.get(k)))
+        if outs.get("psd_d") is not None:
+            o.psd_nbin = int(outs["psd_d"].shape[-1])
         return o
 
     def run(self, settings, columns, outputs, precision=PREC_FP64, stream=None):

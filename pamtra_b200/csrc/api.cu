@@ -730,6 +730,9 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   if (!(st->nummu == 8 || st->nummu == 16 || st->nummu == 32)) return PAMTRA_B200_FATAL;
   if (cols->fs_d && (cols->fs_nbin < 1 || !cols->fs_d_bound || !cols->fs_n || !cols->fs_rho || !cols->fs_mass))
     return PAMTRA_B200_FATAL;
+  if (out->psd_d && (out->psd_nbin < 1 || !out->psd_deltad || !out->psd_n || !out->psd_mass || !out->psd_area ||
+                     !out->psd_bscat))
+    return PAMTRA_B200_FATAL;
   cudaStream_t stream = (cudaStream_t)stream_;
   cudaSetDevice(ctx->device);
   pamtra_b200_species dummy{};
@@ -795,6 +798,8 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   w.slot_st = (int8_t*)(A + pl.o_slot_st); w.slot_nb = (int*)(A + pl.o_slot_nb);
   w.b_d = (double*)(A + pl.o_bd); w.b_dd = (double*)(A + pl.o_bdd); w.b_nd = (double*)(A + pl.o_bnd);
   w.b_rho = (double*)(A + pl.o_brho); w.b_mass = (double*)(A + pl.o_bmass);
+  w.psd_d = out->psd_d; w.psd_dd = out->psd_deltad; w.psd_n = out->psd_n; w.psd_mass = out->psd_mass;
+  w.psd_area = out->psd_area; w.psd_bscat = out->psd_bscat; w.psd_nbin = out->psd_nbin;
   w.pres_idx = (int*)(A + pl.o_pres_idx); w.plist = (int*)(A + pl.o_plist); w.pmax = pl.pmax;
   w.counters = (int*)(A + pl.o_counters);
   w.m_kext = (double*)(A + pl.o_mkext); w.m_salb = (double*)(A + pl.o_msalb); w.m_nleg = (int*)(A + pl.o_mnleg);
@@ -830,6 +835,13 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   cudaMemsetAsync(w.col_status, 0, C * 4, stream);
   const size_t ntb = C * cc.noutlevels * 2 * cc.max_nummu * Fm * 2;
   k_fill_d<<<(unsigned)((ntb + 255) / 256), 256, 0, stream>>>(out->tb, -9999.0, ntb); launches++;
+  if (w.psd_d && H > 0) {
+    const size_t npsd = C * Lm * H * (size_t)w.psd_nbin;
+    for (double* a : {w.psd_d, w.psd_dd, w.psd_n, w.psd_mass, w.psd_area, w.psd_bscat}) {
+      k_fill_d<<<(unsigned)((npsd + 255) / 256), 256, 0, stream>>>(a, -9999.0, npsd);
+      launches++;
+    }
+  }
   k_atmo<<<(unsigned)((C + 127) / 128), 128, 0, stream>>>(b, w); launches++;
   const size_t ngas = C * Fm * Lm;
   k_gas<<<(unsigned)((ngas + 255) / 256), 256, 0, stream>>>(b, w, st->lgas_extinction); launches++;
@@ -931,6 +943,9 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
   if (!ctx || !st || !hc || !ho || !ho->tb) return PAMTRA_B200_FATAL;
   if (hc->fs_d && (hc->fs_nbin < 1 || !hc->fs_d_bound || !hc->fs_n || !hc->fs_rho || !hc->fs_mass))
     return PAMTRA_B200_FATAL;
+  if (ho->psd_d && (ho->psd_nbin < 1 || !ho->psd_deltad || !ho->psd_n || !ho->psd_mass || !ho->psd_area ||
+                    !ho->psd_bscat))
+    return PAMTRA_B200_FATAL;
   cudaStream_t stream = (cudaStream_t)stream_;
   cudaSetDevice(ctx->device);
   const size_t C = hc->ncol, Lm = hc->max_nlyrs, Fm = hc->max_nfreq, H = hc->nhydro, NO = hc->noutlevels;
@@ -970,6 +985,9 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
   size_t o_ze = add(nullptr, ho->ze ? C * Fm * Lm * 8 : 0);
   size_t o_ah = add(nullptr, ho->att_hydro ? C * Fm * Lm * 8 : 0);
   size_t o_aa = add(nullptr, ho->att_atmo ? C * Fm * Lm * 8 : 0);
+  const size_t NP = ho->psd_d ? C * Lm * H * (size_t)ho->psd_nbin : 0;
+  size_t o_psd[6];
+  for (int i = 0; i < 6; i++) o_psd[i] = add(nullptr, NP * 8);
   if (off > ctx->stage_bytes) {
     cudaStreamSynchronize(stream);
     cudaFree(ctx->stage);
@@ -1020,6 +1038,15 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
   dout.ze = ho->ze ? (double*)(D + o_ze) : nullptr;
   dout.att_hydro = ho->att_hydro ? (double*)(D + o_ah) : nullptr;
   dout.att_atmo = ho->att_atmo ? (double*)(D + o_aa) : nullptr;
+  if (ho->psd_d) {
+    dout.psd_nbin = ho->psd_nbin;
+    dout.psd_d = (double*)(D + o_psd[0]);
+    dout.psd_deltad = (double*)(D + o_psd[1]);
+    dout.psd_n = (double*)(D + o_psd[2]);
+    dout.psd_mass = (double*)(D + o_psd[3]);
+    dout.psd_area = (double*)(D + o_psd[4]);
+    dout.psd_bscat = (double*)(D + o_psd[5]);
+  }
   if (dout.scatter_matrix) cudaMemsetAsync(dout.scatter_matrix, 0, C * Fm * Lm * 4 * NA * NA * 8, stream);
   int32_t rc = pamtra_b200_run(ctx, st, &dc, &dout, precision, stream);
   if (rc != PAMTRA_B200_OK) return rc;
@@ -1036,6 +1063,14 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
   if (ho->ze) cudaMemcpyAsync(ho->ze, dout.ze, C * Fm * Lm * 8, cudaMemcpyDeviceToHost, stream);
   if (ho->att_hydro) cudaMemcpyAsync(ho->att_hydro, dout.att_hydro, C * Fm * Lm * 8, cudaMemcpyDeviceToHost, stream);
   if (ho->att_atmo) cudaMemcpyAsync(ho->att_atmo, dout.att_atmo, C * Fm * Lm * 8, cudaMemcpyDeviceToHost, stream);
+  if (ho->psd_d) {
+    cudaMemcpyAsync(ho->psd_d, dout.psd_d, NP * 8, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(ho->psd_deltad, dout.psd_deltad, NP * 8, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(ho->psd_n, dout.psd_n, NP * 8, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(ho->psd_mass, dout.psd_mass, NP * 8, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(ho->psd_area, dout.psd_area, NP * 8, cudaMemcpyDeviceToHost, stream);
+    cudaMemcpyAsync(ho->psd_bscat, dout.psd_bscat, NP * 8, cudaMemcpyDeviceToHost, stream);
+  }
   if (cudaStreamSynchronize(stream) != cudaSuccess) return PAMTRA_B200_FATAL;
   return PAMTRA_B200_OK;
 }
@@ -1118,7 +1153,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
       cols->max_nfreq < 1 || cols->max_nfreq > PAMTRA_B200_NOALLOC_MAX_NFREQ || cols->nhydro < 0 ||
       cols->nhydro > PAMTRA_B200_NOALLOC_MAX_NHYDRO || cols->noutlevels < 1 || cols->noutlevels > 2 ||
       !(cols->max_nummu == 8 || cols->max_nummu == 16) || !(st->nummu == 8 || st->nummu == 16) ||
-      (cols->nhydro > 0 && !cols->species) || cols->fs_d)
+      (cols->nhydro > 0 && !cols->species) || cols->fs_d || out->psd_d)
     return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PAMTRA_B200_FATAL;

@@ -213,6 +213,8 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
     double kexttot = 0.0, salbedo = 0.0, backtot = 0.0;
     int nlegen_coef = 0;
     int status = 0;
+    // save_psd per-bin backscatter: written at the column's last frequency
+    double* const bscat = (w.psd_bscat && f == b.col_nfreq(c) - 1) ? w.psd_bscat : nullptr;
     for (int h = 0; h < H; h++) {
       const size_t s_idx = ((size_t)c * Lm + z) * H + h;
       if (w.slot_st[s_idx] != 2) continue;
@@ -271,7 +273,7 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
         const int ir = c0 + lane / R;
         c0 += chunk;
         bool act = false;
-        double wgt = 0.0, ndens = 0.0, deld = 0.0;
+        double wgt = 0.0, ndens = 0.0, deld = 0.0, qb_bin = 0.0;
         int nm = 0;
         deld = bdd[ir];
         ndens = bnd[ir] / deld;
@@ -296,10 +298,14 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
             sqe = sqe + qe * deld;
             sqs = sqs + qs * deld;
             sqb = sqb + qb * deld;
+            qb_bin = qb;
           }
           nm = min(nmie, nterms);
           wgt = ndens;
         }
+        // per-particle cross section as back_spec / num_density of
+        // src/scatProperties.f90:916 (0 / 0 = NaN for an empty bin)
+        if (bscat && r == 0 && ir < w.psd_nbin) bscat[s_idx * (size_t)w.psd_nbin + ir] = qb_bin / ndens;
         for (int i0 = 0; i0 < nquad; i0 += ANG_G * R) {
           double pp[ANG_G][4];
           if (act) {

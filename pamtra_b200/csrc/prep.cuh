@@ -550,6 +550,23 @@ __global__ void k_psd(Batch b, Work w, pamtra_b200_settings st) {
   }
   w.slot_nb[s_idx] = nbin;
   if (!any) return;  // hydrometeor_extinction.f90:294-298: layer present, species skipped
+  if (w.psd_d) {
+    // save_psd (hydrometeor_extinction.f90:303-309; area of drop_size_dist.f90:168-182)
+    const size_t po = s_idx * (size_t)w.psd_nbin;
+    for (int i = 0; i < nbin && i < w.psd_nbin; i++) {
+      const double d = d_ds[i];
+      double area = -99.;
+      if (s.alpha_as > 0. && s.beta_as > 0.) {
+        area = s.alpha_as * pow(d, s.beta_as);
+        if (s.liq_ice == -1 && st.hydro_limit_density_area && area > d * d) area = d * d;
+      }
+      w.psd_d[po + i] = d;
+      w.psd_dd[po + i] = del[i];
+      w.psd_n[po + i] = nds[i];
+      w.psd_mass[po + i] = mass[i];
+      w.psd_area[po + i] = area;
+    }
+  }
   // scattering density / diameter (drop_size_dist.f90:198-208, make_soft_spheroid.f90)
   if (s.liq_ice == 1) {
     for (int i = 0; i < nbin; i++) rho[i] = RHO_WATER;

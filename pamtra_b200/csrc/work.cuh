@@ -50,6 +50,9 @@ struct Work {
   int8_t* slot_st;                     // [S] 0 absent, 1 present w/o bins, 2 bins, 3 fatal
   int* slot_nb;                        // [S]
   double *b_d, *b_dd, *b_nd, *b_rho, *b_mass;  // [S][max_nbin]
+  // save_psd outputs [S][psd_nbin] (NULL psd_d: not requested)
+  double *psd_d, *psd_dd, *psd_n, *psd_mass, *psd_area, *psd_bscat;
+  int psd_nbin;
   // compaction
   int* pres_idx;                       // [C][Lm]
   int* plist;                          // [pmax]

@@ -5,7 +5,8 @@ Same signature and return value ``(results, pamError[, module])``; results
 carry the passive keys of ``pyPamtra.r`` (``tb``, ``emissivity``,
 ``angles_deg``; with ``save_ssp`` also ``kextatmo``, ``scatter_matrix``,
 ``extinct_matrix``, ``emis_vector``); with ``active`` (radar_mode 'simple')
-``Ze``, ``Att_hydro``, ``Att_atmo`` and ``radar_hgt``; the other active keys
+``Ze``, ``Att_hydro``, ``Att_atmo`` and ``radar_hgt``; with ``save_psd`` the
+``psd_*`` bins and per-bin backscatter; the other active keys
 filled with -9999 as the reference does for unallocated outputs
 (libWrapper.py:214-223).
 """
@@ -18,6 +19,7 @@ from ._native import PREC_FP64, engine
 
 missingNumber = -9999.0
 
+PSD_KEYS = ("psd_d", "psd_deltad", "psd_n", "psd_mass", "psd_area", "psd_bscat")
 ACTIVE_KEYS = ["Ze", "Att_hydro", "Att_atmo", "radar_hgt", "radar_moments", "radar_edges", "radar_slopes",
                "radar_quality", "radar_snr", "radar_spectra", "radar_vel", "psd_d", "psd_deltad", "psd_n",
                "psd_mass", "psd_area", "psd_bscat"]
@@ -92,6 +94,12 @@ def PamtraFortranWrapper(sets, nmlSets, descriptorFile, descriptorFile4D, descri
     if st.active:
         for k in ("ze", "att_hydro", "att_atmo"):
             out[k] = np.zeros((ncol, nf, L))
+    # save_psd: bins of the moment-based size distributions, sized as
+    # src/vars_output.f90:175-193 (max descriptor nbin, at least 2)
+    psd_nbin = max(2, int(np.max(descriptorFile["nbin"]))) if nmlSets.get("save_psd", False) and nhydro else 0
+    if psd_nbin:
+        for k in PSD_KEYS:
+            out[k] = np.zeros((ncol, L, nhydro, psd_nbin))
     mask = {8: 1, 16: 2, 32: 4}[N]
     eng = engine(device)
     c = eng.make_columns(arrs, sp, nmu_mask=mask, max_present=present_bound(cols, descriptorFile, st.hydro_threshold),
@@ -107,6 +115,14 @@ def PamtraFortranWrapper(sets, nmlSets, descriptorFile, descriptorFile4D, descri
     results["status"] = out["status"].reshape(nx, ny, nf)
     for k in ACTIVE_KEYS:
         results[k] = -9999 if k == "radar_quality" else missingNumber
+    if psd_nbin:
+        for k in PSD_KEYS:
+            results[k] = out[k].reshape(nx, ny, L, nhydro, psd_nbin)
+        if str(list(sets.get("radar_pol", ["NN"]))[0]).strip() in ("HV", "VH"):
+            # psd_bscat is taken for the first polarisation; Mie spheres have no
+            # cross-polar backscatter (src/scatProperties.f90:746-756)
+            b = results["psd_bscat"]
+            results["psd_bscat"] = np.where(b == missingNumber, b, 0.0 * b)
     if st.active:
         # simple radar (src/radar_simulator.f90:161-176): Ze per polarisation;
         # Mie spheres give the same backscatter for NN/HH/VV and none for HV/VH
