@@ -50,6 +50,7 @@ extern "C" {
 #define PAMTRA_B200_ST_NAN 0x2000      /* NaN in extinction / coefficients */
 #define PAMTRA_B200_ST_SIZE 0x4000     /* a size limit of this library was exceeded */
 #define PAMTRA_B200_ST_TIMEOUT 0x8000  /* a bounded wait on the tensor core gave up */
+#define PAMTRA_B200_ST_RANGE 0x10000   /* input outside a model's range (liq_mod 'Ray' above 299.79 GHz) */
 
 /* dist_name codes (src/make_dist_param.f90) */
 #define PAMTRA_B200_DIST_EXP 0
@@ -92,7 +93,19 @@ typedef struct pamtra_b200_settings {
   int32_t active;                    /* nmlSet['active']: fill outputs.ze / att_* */
   int32_t radar_attenuation;         /* PAMTRA_B200_ATT_*: nmlSet['radar_attenuation'] */
   double radar_k2;                   /* nmlSet['radar_k2'], |K|^2 of the radar equation */
+  int32_t liq_mod;                   /* PAMTRA_B200_LIQ_*: nmlSet['liq_mod'] (src/eps_water.f90:39-63) */
+  int32_t gas_mod;                   /* PAMTRA_B200_GAS_*: nmlSet['gas_mod'] (src/get_gasabs.f90:78-102) */
 } pamtra_b200_settings;
+
+/* liquid water permittivity models (nmlSet['liq_mod']) */
+#define PAMTRA_B200_LIQ_TKC 0  /* Turner, Kneifel and Cadeddu 2016 (default) */
+#define PAMTRA_B200_LIQ_ELL 1  /* Ellison 2007 */
+#define PAMTRA_B200_LIQ_LIE 2  /* Liebe, Hufford and Manabe 1991 */
+#define PAMTRA_B200_LIQ_RAY 3  /* Ray 1972, wavelengths above 1 mm */
+#define PAMTRA_B200_LIQ_STO 4  /* Stogryn et al. 1995 */
+/* gas absorption models (nmlSet['gas_mod']) */
+#define PAMTRA_B200_GAS_R98 0  /* Rosenkranz 1998 (default) */
+#define PAMTRA_B200_GAS_L93 1  /* Liebe MPM93 */
 
 /* radar_attenuation codes */
 #define PAMTRA_B200_ATT_DISABLED 0
@@ -244,6 +257,17 @@ int32_t pamtra_b200_gas_r98(const double* freq, const double* temp, const double
 /* TKC water permittivity (src/eps_water.f90:653), element-wise; T in degC. */
 int32_t pamtra_b200_eps_water_tkc(const double* t_c, const double* freq, double* eps_re, double* eps_im,
                                   int32_t n, void* stream);
+
+/* get_eps_water (src/eps_water.f90:6-70) for a PAMTRA_B200_LIQ_* model,
+ * element-wise: salinity s (ppt), T in degC, f in GHz; status[i] is
+ * PAMTRA_B200_FATAL | PAMTRA_B200_ST_RANGE where the model has no value. */
+int32_t pamtra_b200_get_eps_water(int32_t liq_mod, const double* s, const double* t_c, const double* freq,
+                                  double* eps_re, double* eps_im, int32_t* status, int32_t n, void* stream);
+
+/* MPM93 absorption (src/mpm93.f90, called as src/get_gasabs.f90:78-86),
+ * element-wise: pressure and water vapour pressure in Pa, T in K; Np/m. */
+int32_t pamtra_b200_gas_l93(const double* freq, const double* press, const double* vap, const double* temp,
+                            double* kext, int32_t n, void* stream);
 
 /* Matrix inverse with partial pivoting of `count` column-major n x n matrices
  * (replaces MINVERT, src/radmat.f90:155), n in {16,32,64}. */

@@ -37,6 +37,8 @@ class OrcSettings(ctypes.Structure):
         ("active", ctypes.c_int32),
         ("radar_attenuation", ctypes.c_int32),
         ("radar_k2", ctypes.c_double),
+        ("liq_mod", ctypes.c_int32),
+        ("gas_mod", ctypes.c_int32),
     ]
 
 
@@ -76,6 +78,10 @@ def lib():
         l.orc_run_column_fs.argtypes = l.orc_run_column.argtypes + [ctypes.POINTER(OrcFullspec)]
         l.orc_gas_r98.restype = ctypes.c_int
         l.orc_gas_r98.argtypes = [ctypes.c_double] * 4 + [dp]
+        l.orc_get_eps_water.restype = ctypes.c_int
+        l.orc_get_eps_water.argtypes = [ctypes.c_int] + [ctypes.c_double] * 3 + [dp, dp]
+        l.orc_gas_l93.restype = ctypes.c_double
+        l.orc_gas_l93.argtypes = [ctypes.c_double] * 4
         l.orc_eps_water_tkc.restype = None
         l.orc_eps_water_tkc.argtypes = [ctypes.c_double, ctypes.c_double, dp, dp]
         l.orc_lobatto.argtypes = [ctypes.c_int, dp, dp]
@@ -220,6 +226,21 @@ def gas_r98(f, T, rhowv, p):
     k = ctypes.c_double()
     err = lib().orc_gas_r98(f, T, rhowv, p, ctypes.byref(k))
     return err, k.value
+
+
+LIQ_MODS = {"TKC": 0, "Ell": 1, "Lie": 2, "Ray": 3, "Sto": 4}
+
+
+def get_eps_water(liq_mod, s, T_c, f):
+    """(errorstatus, eps) of get_eps_water (src/eps_water.f90:6-70)."""
+    re, im = ctypes.c_double(), ctypes.c_double()
+    err = lib().orc_get_eps_water(LIQ_MODS[liq_mod], s, T_c, f, ctypes.byref(re), ctypes.byref(im))
+    return err, complex(re.value, im.value)
+
+
+def gas_l93(f, press, vap, T):
+    """MPM93 absorption in Np/m (pressures in Pa, T in K)."""
+    return lib().orc_gas_l93(f, press, vap, T)
 
 
 def eps_water_tkc(T_c, f):

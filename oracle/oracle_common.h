@@ -96,6 +96,8 @@ typedef struct {
   int32_t active;             // nmlSet['active'] (simple radar)
   int32_t radar_attenuation;  // 0 disabled, 1 bottom-up, 2 top-down
   double radar_k2;            // nmlSet['radar_k2']
+  int32_t liq_mod;            // 0 TKC, 1 Ell, 2 Lie, 3 Ray, 4 Sto (src/eps_water.f90:39-63)
+  int32_t gas_mod;            // 0 R98, 1 L93 (src/get_gasabs.f90:78-102)
 } orc_settings;
 
 // One descriptor-file row (python/pyPamtra/descriptorFile.py:19-20).

@@ -233,6 +233,295 @@ int gas_r98(double f, double T, double rhowv, double pres, double* kext) {
   return 0;
 }
 
+
+// ---------------------------------------------------------------- other liquid water models
+// src/eps_water.f90 (nmlSet['liq_mod']).  gfortran semantics restated: a
+// literal without kind is a REAL(4) value (float literal here) promoted in
+// mixed expressions; the routines' pi parameter is that REAL(4) value; a
+// complex constant (0.,1.) times a real is (0, 1*x); CMPLX without KIND is
+// COMPLEX(4).  Salinity is 0 (src/scatProperties.f90:228).
+static const double PI4 = (double)3.141592653589793f;
+
+// eps_water_ellison (src/eps_water.f90:85-158)
+cplx eps_water_ellison(double s, double T, double f) {
+  static const float a[18] = {0.46606917e-02f, -0.26087876e-04f, -0.63926782e-05f, 0.63000075e+01f,
+                              0.26242021e-02f, -0.42984155e-02f, 0.34414691e-04f, 0.17667420e-03f,
+                              -0.20491560e-06f, 0.58366888e+03f, 0.12634992e+03f, 0.69227972e-04f,
+                              0.38957681e-06f, 0.30742330e+03f, 0.12634992e+03f, 0.37245044e+01f,
+                              0.92609781e-02f, -0.26093754e-01f};
+  auto A = [&](int i) { return (double)a[i - 1]; };
+  double p = s * (37.5109f + 5.45216f * s + 0.014409f * p2(s)) / (1004.75f + 182.283f * s + p2(s));
+  double alpha_0 = (6.9431f + 3.2841f * s - 0.099486f * p2(s)) / (84.85f + 69.024f * s + p2(s));
+  double alpha_1 = 49.843f - 0.2276f * s + 0.00198f * p2(s);
+  double sig_s35 = 2.903602f + 8.607e-02f * T + 4.738817e-04f * p2(T) - 2.991e-06f * p3(T) + 4.3041e-09f * (p2(T) * p2(T));
+  double eps_s = 87.85306f * std::exp(-0.00456992f * T - A(1) * s - A(2) * p2(s) - A(3) * s * T);
+  double eps_1 = A(4) * std::exp(-A(5) * T - A(6) * s - A(7) * s * T);
+  double tau_1 = (A(8) + A(9) * s) * std::exp(A(10) / (T + A(11)));
+  double tau_2 = (A(12) + A(13) * s) * std::exp(A(14) / (T + A(15)));
+  double eps_inf = A(16) + A(17) * T + A(18) * s;
+  double q = 1 + (alpha_0 * (T - 15)) / (T + alpha_1);
+  double sig = sig_s35 * p * q;
+  cplx t1 = cdiv(cmk(eps_s - eps_1, 0.0), cmk(1.0, -(2 * PI4 * f * tau_1)));
+  cplx t2 = cdiv(cmk(eps_1 - eps_inf, 0.0), cmk(1.0, -(2 * PI4 * f * tau_2)));
+  cplx e = cadd(cadd(t1, t2), cmk(eps_inf, 0.0));
+  return cadd(e, cmk(0.0, (double)17.9751f * sig / f));
+}
+
+// eps_water_liebe (src/eps_water.f90:160-207)
+cplx eps_water_liebe(double T, double f) {
+  double T_K = T + 273.15f;
+  double theta_1 = 1. - 300. / T_K;
+  double fp = 20.1f * std::exp(7.88f * theta_1);
+  double fs = 39.8f * fp;
+  double eps_0 = 77.66f - 103.3f * theta_1;
+  double eps_1 = 0.0671f * eps_0;
+  double eps_2 = 3.52f;
+  cplx e = cadd(cdiv(cmk(eps_0 - eps_1, 0.0), cmplx4(1., -f / fp)), cdiv(cmk(eps_1 - eps_2, 0.0), cmplx4(1., -f / fs)));
+  return cadd(e, cmk(eps_2, 0.0));
+}
+
+// eps_water_ray (src/eps_water.f90:209-596), the Ray (1972) formula branch
+// for wavelengths above 1 mm; returns 2 for shorter wavelengths (tabulated
+// optical constants, not restated) and outside 0.2 um - 10 cm.
+int eps_water_ray(double T, double f, cplx& eps) {
+  double wl = (double)(1.e6f * 2.99792458e8f) / (f * 1.e9f);
+  if (wl < (double)0.2f || wl > 100000.0) return 2;
+  if (!(wl > 1000.0)) return 2;
+  double T1 = T + 273.0f, T2 = T - 25.0f, xl = wl / 10000.0f;
+  double sigma = 12.5664e8f;
+  double alpha = -16.8129f / T1 + 0.0609265f;
+  double eps_s = 78.54f * (1.0f - 4.579e-3f * T2 + 1.19e-5f * p2(T2) - 2.8e-8f * p3(T2));
+  double eps_inf = 5.27137f + 0.0216474f * T - 0.00131198f * p2(T);
+  double xlams = 0.00033836f * std::exp(2513.98f / T1);
+  double powtrm = std::pow(xlams / xl, 1.f - alpha);
+  double denom = 1.f + 2 * powtrm * std::sin(PI4 * alpha / 2) + std::pow(xlams / xl, 2.f * (1.f - alpha));
+  double eps_r = eps_inf + (eps_s - eps_inf) * (1.0f + powtrm * std::sin(PI4 * alpha / 2)) / denom;
+  double eps_i = (sigma * xl / (double)18.8496e10f) + (eps_s - eps_inf) * powtrm * std::cos(PI4 * alpha / 2) / denom;
+  cplx n = csqrt_(cmk(eps_r, eps_i));
+  double rn = n.re, cn = n.im;
+  if (!(wl > 3000.0f))
+    cn = cn + 0.39f * std::exp(-std::pow(std::fabs(std::log10(wl / 17.0f) / 0.45f), (double)1.3f)) +
+         0.41f * std::exp(-std::pow(std::fabs(std::log10(wl / 62.0f) / 0.35f), (double)1.7f)) +
+         0.25f * std::exp(-std::pow(std::fabs(std::log10(wl / 300.0f) / 0.47f), 3.0));
+  eps = cmul(cmk(rn, cn), cmk(rn, cn));
+  return 0;
+}
+
+// eps_water_stogryn (src/eps_water.f90:598-651)
+cplx eps_water_stogryn(double s, double T, double f) {
+  double p = s * (37.5109f + 5.45216f * s + 0.014409f * p2(s)) / (1004.75f + 182.283f * s + p2(s));
+  double alpha_0 = (6.9431f + 3.2841f * s - 0.099486f * p2(s)) / (84.85f + 69.024f * s + p2(s));
+  double alpha_1 = 49.843f - 0.2276f * s + 0.00198f * p2(s);
+  double sig_s35 = 2.903602f + 8.607e-02f * T + 4.738817e-04f * p2(T) - 2.991e-06f * p3(T) + 4.3041e-09f * (p2(T) * p2(T));
+  double a = 1.f - (s * (0.03838f + 0.00218f * s) * (79.88f + T)) / ((12.01f + s) * (52.53f + T));
+  double b = 1.f - s * ((0.03409f + 0.002817f * s) / (7.69f + s)) -
+             s * T * ((0.00246f + 0.00141f * T) / (188.f - 7.57f * T + p2(T)));
+  double es = (37088.6f - 82.168f * T) / (421.854f + T);
+  double eps_s = es * a;
+  double eps_1 = (0.0787f * es) * a;
+  double tpt1 = ((255.04f + 0.7246f * T) / ((49.25f + T) * (45.f + T))) * b;
+  double tpt2 = 0.00628f;
+  double eps_inf = 4.05f + 0.0186f * T;
+  double q = 1 + (alpha_0 * (T - 15)) / (T + alpha_1);
+  double sig = sig_s35 * p * q;
+  cplx t1 = cdiv(cmk(eps_s - eps_1, 0.0), cmk(1.0, -(f * tpt1)));
+  cplx t2 = cdiv(cmk(eps_1 - eps_inf, 0.0), cmk(1.0, -(f * tpt2)));
+  cplx e = cadd(cadd(t1, t2), cmk(eps_inf, 0.0));
+  return cadd(e, cmk(0.0, (double)17.9751f * sig / f));
+}
+
+cplx eps_water_tkc(double T, double f);
+
+// src/ref_water.f90 + get_eps_water (src/eps_water.f90:39-63) for every liq_mod;
+// returns 2 where the model has no value.
+int ref_water_mod(int liq_mod, double T_c, double f, double& refre, double& refim) {
+  cplx e;
+  switch (liq_mod) {
+    case 1: e = eps_water_ellison(0.0, T_c, f); break;
+    case 2: e = eps_water_liebe(T_c, f); break;
+    case 3:
+      if (eps_water_ray(T_c, f, e)) return 2;
+      break;
+    case 4: e = eps_water_stogryn(0.0, T_c, f); break;
+    default: e = eps_water_tkc(T_c, f); break;
+  }
+  cplx r = csqrt_(e);
+  refre = r.re;
+  refim = r.im;
+  return 0;
+}
+
+// ---------------------------------------------------------------- gas_mod 'L93'
+// src/mpm93.f90: line catalogue of Liebe, Hufford and Cotton (1993) as the
+// reference declares it (REAL(4) literals, :131-222).
+static const float L93_F0O2[44] = {
+    50.474239f, 50.987747f, 51.503349f, 52.021412f, 52.542393f, 53.066906f, 53.595749f, 54.130001f,
+    54.671158f, 55.221367f, 55.783802f, 56.264774f, 56.363388f, 56.968204f, 57.612484f, 58.323875f,
+    58.446590f, 59.164207f, 59.590984f, 60.306061f, 60.434776f, 61.150558f, 61.800156f, 62.411217f,
+    62.486259f, 62.997978f, 63.568520f, 64.127769f, 64.678902f, 65.224068f, 65.764771f, 66.302094f,
+    66.836830f, 67.369598f, 67.900864f, 68.431007f, 68.960312f, 118.750343f, 368.498352f, 424.763123f,
+    487.249359f, 715.393127f, 773.839661f, 834.145325f};
+static const float L93_A1[44] = {
+    0.094f, 0.246f, 0.608f, 1.414f, 3.102f, 6.410f, 12.470f, 22.800f,
+    39.180f, 63.160f, 95.350f, 54.890f, 134.400f, 176.300f, 214.100f, 238.600f,
+    145.700f, 240.400f, 211.200f, 212.400f, 246.100f, 250.400f, 229.800f, 193.300f,
+    151.700f, 150.300f, 108.700f, 73.350f, 46.350f, 27.480f, 15.300f, 8.009f,
+    3.946f, 1.832f, 0.801f, 0.330f, 0.128f, 94.500f, 6.790f, 63.800f,
+    23.500f, 9.960f, 67.100f, 18.000f};
+static const float L93_A2[44] = {
+    9.694f, 8.694f, 7.744f, 6.844f, 6.004f, 5.224f, 4.484f, 3.814f,
+    3.194f, 2.624f, 2.119f, 0.015f, 1.660f, 1.260f, 0.915f, 0.626f,
+    0.084f, 0.391f, 0.212f, 0.212f, 0.391f, 0.626f, 0.915f, 1.260f,
+    0.083f, 1.665f, 2.115f, 2.620f, 3.195f, 3.815f, 4.485f, 5.225f,
+    6.005f, 6.845f, 7.745f, 8.695f, 9.695f, 0.009f, 0.049f, 0.044f,
+    0.049f, 0.145f, 0.130f, 0.147f};
+static const float L93_A3[44] = {
+    0.890f, 0.910f, 0.940f, 0.970f, 0.990f, 1.020f, 1.050f, 1.070f,
+    1.100f, 1.130f, 1.170f, 1.730f, 1.200f, 1.240f, 1.280f, 1.330f,
+    1.520f, 1.390f, 1.430f, 1.450f, 1.360f, 1.310f, 1.270f, 1.230f,
+    1.540f, 1.200f, 1.170f, 1.130f, 1.100f, 1.070f, 1.050f, 1.020f,
+    0.990f, 0.970f, 0.940f, 0.920f, 0.900f, 1.630f, 1.920f, 1.930f,
+    1.920f, 1.810f, 1.820f, 1.810f};
+static const float L93_A4[44] = {
+    0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f,
+    0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f,
+    0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f,
+    0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f,
+    0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.000f, 0.600f, 0.600f,
+    0.600f, 0.600f, 0.600f, 0.600f};
+static const float L93_A5[44] = {
+    0.240f, 0.220f, 0.197f, 0.166f, 0.136f, 0.131f, 0.230f, 0.335f,
+    0.374f, 0.258f, -0.166f, 0.390f, -0.297f, -0.416f, -0.613f, -0.205f,
+    0.748f, -0.722f, 0.765f, -0.705f, 0.697f, 0.104f, 0.570f, 0.360f,
+    -0.498f, 0.239f, 0.108f, -0.311f, -0.421f, -0.375f, -0.267f, -0.168f,
+    -0.169f, -0.200f, -0.228f, -0.240f, -0.250f, -0.036f, 0.000f, 0.000f,
+    0.000f, 0.000f, 0.000f, 0.000f};
+static const float L93_A6[44] = {
+    0.790f, 0.780f, 0.774f, 0.764f, 0.751f, 0.714f, 0.584f, 0.431f,
+    0.305f, 0.339f, 0.705f, -0.113f, 0.753f, 0.742f, 0.697f, 0.051f,
+    -0.146f, 0.266f, -0.090f, 0.081f, -0.324f, -0.067f, -0.761f, -0.777f,
+    0.097f, -0.768f, -0.706f, -0.332f, -0.298f, -0.423f, -0.575f, -0.700f,
+    -0.735f, -0.744f, -0.753f, -0.760f, -0.765f, 0.009f, 0.000f, 0.000f,
+    0.000f, 0.000f, 0.000f, 0.000f};
+static const float L93_F0H2O[35] = {
+    22.235081f, 67.803963f, 119.995941f, 183.310089f, 321.225647f, 325.152924f, 336.222595f, 380.197357f,
+    390.134521f, 437.346680f, 439.150818f, 443.018280f, 448.001068f, 470.888947f, 474.689117f, 488.491119f,
+    503.568542f, 504.482697f, 547.676453f, 552.020935f, 556.935974f, 620.700806f, 645.866150f, 658.005310f,
+    752.033203f, 841.053955f, 859.962341f, 899.306702f, 902.616150f, 906.207336f, 916.171570f, 923.118408f,
+    970.315002f, 987.926758f, 1780.000000f};
+static const float L93_B1[35] = {
+    0.01130f, 0.00012f, 0.00008f, 0.24200f, 0.00483f, 0.14990f, 0.00011f, 1.15200f,
+    0.00046f, 0.00650f, 0.09218f, 0.01976f, 1.03200f, 0.03297f, 0.12620f, 0.02520f,
+    0.00390f, 0.00130f, 0.97010f, 1.47700f, 48.74000f, 0.50120f, 0.00713f, 0.03022f,
+    23.96000f, 0.00140f, 0.01472f, 0.00605f, 0.00426f, 0.01876f, 0.83400f, 0.00869f,
+    0.89720f, 13.21000f, 2230.00000f};
+static const float L93_B2[35] = {
+    2.143f, 8.735f, 8.356f, 0.668f, 6.181f, 1.540f, 9.829f, 1.048f,
+    7.350f, 5.050f, 3.596f, 5.050f, 1.405f, 3.599f, 2.381f, 2.853f,
+    6.733f, 6.733f, 0.114f, 0.114f, 0.159f, 2.200f, 8.580f, 7.820f,
+    0.396f, 8.180f, 7.989f, 7.917f, 8.432f, 5.111f, 1.442f, 10.220f,
+    1.920f, 0.258f, 0.952f};
+static const float L93_B3[35] = {
+    2.811f, 2.858f, 2.948f, 3.050f, 2.303f, 2.783f, 2.693f, 2.873f,
+    2.152f, 1.845f, 2.100f, 1.860f, 2.632f, 2.152f, 2.355f, 2.602f,
+    1.612f, 1.612f, 2.600f, 2.600f, 3.210f, 2.438f, 1.800f, 3.210f,
+    3.060f, 1.590f, 3.060f, 2.985f, 2.865f, 2.408f, 2.670f, 2.900f,
+    2.550f, 2.985f, 17.620f};
+static const float L93_B4[35] = {
+    4.80f, 4.93f, 4.78f, 5.30f, 4.69f, 4.85f, 4.74f, 5.38f,
+    4.81f, 4.23f, 4.29f, 4.23f, 4.84f, 4.57f, 4.65f, 5.04f,
+    3.98f, 4.01f, 4.50f, 4.50f, 4.11f, 4.68f, 4.00f, 4.14f,
+    4.09f, 5.76f, 4.09f, 4.53f, 5.10f, 4.70f, 4.78f, 5.00f,
+    4.94f, 4.55f, 30.50f};
+static const float L93_B5[35] = {
+    0.69f, 0.69f, 0.70f, 0.64f, 0.67f, 0.68f, 0.69f, 0.54f,
+    0.63f, 0.60f, 0.63f, 0.60f, 0.66f, 0.66f, 0.65f, 0.69f,
+    0.61f, 0.61f, 0.70f, 0.70f, 0.69f, 0.71f, 0.60f, 0.69f,
+    0.68f, 0.33f, 0.68f, 0.68f, 0.70f, 0.70f, 0.70f, 0.70f,
+    0.64f, 0.68f, 2.00f};
+static const float L93_B6[35] = {
+    1.00f, 0.82f, 0.79f, 0.85f, 0.54f, 0.74f, 0.61f, 0.89f,
+    0.55f, 0.48f, 0.52f, 0.50f, 0.67f, 0.65f, 0.64f, 0.72f,
+    0.43f, 0.45f, 1.00f, 1.00f, 1.00f, 0.68f, 0.50f, 1.00f,
+    0.84f, 0.45f, 0.84f, 0.90f, 0.95f, 0.53f, 0.78f, 0.80f,
+    0.67f, 0.90f, 5.00f};
+
+
+// COMPLEX(4) division, Smith's method in single precision (gfortran
+// -fcx-fortran-rules).
+static void cdiv4(float ar, float ai, float br, float bi, float& qr, float& qi) {
+  float tr, ti, ratio, div;
+  if (std::fabs(br) < std::fabs(bi)) {
+    ratio = br / bi;
+    div = (br * ratio) + bi;
+    tr = (ar * ratio) + ai;
+    ti = (ai * ratio) - ar;
+  } else {
+    ratio = bi / br;
+    div = (bi * ratio) + br;
+    tr = (ai * ratio) + ar;
+    ti = ai - (ar * ratio);
+  }
+  qr = tr / div;
+  qi = ti / div;
+}
+
+// ZF of src/mpm93.f90:269-270 and :300-301
+static cplx l93_zf(double freq, double f0, double delta, double gamma) {
+  float q1r, q1i, q2r, q2i;
+  cdiv4(1.f, (float)(-delta), (float)(f0 - freq), (float)(-gamma), q1r, q1i);
+  cdiv4(1.f, (float)delta, (float)(f0 + freq), (float)gamma, q2r, q2i);
+  float dr = q1r - q2r, di = q1i - q2i;  // COMPLEX(4) difference
+  double r = freq / f0;
+  return cmk(r * (double)dr, r * (double)di);
+}
+
+// mpm93 (src/mpm93.f90:1-359, W = 0) called as src/get_gasabs.f90:78-86:
+// Pbkpa = p / 1e3, Ekpa = e / 1e3, Tc = T - t_abs; result in Np/m.
+double gas_l93(double freq, double press, double vap, double T) {
+  const double t_abs = 273.15;
+  double Pbkpa = press / 1.e3, Ekpa = vap / 1.e3, Tc = T - t_abs;
+  double V = 300.0 / (Tc + t_abs);
+  double Pb = 10.0 * Pbkpa, E = 10.0 * Ekpa;
+  double P = Pb - E;
+  if (P < 0) {
+    P = 0.0;
+    Pb = E;
+  }
+  cplx ZN = cmk(0.0, 0.0);
+  for (int i = 0; i < 44; i++) {
+    double S = (double)L93_A1[i] * P * p3(V) * std::exp((double)L93_A2[i] * (1.0 - V)) * 1.e-6;
+    double GAMMA = (double)L93_A3[i] * (P * std::pow(V, 0.8 - (double)L93_A4[i]) + 1.1 * E * V) * 1.e-3;
+    GAMMA = std::pow(p2(GAMMA) + p2(25.0 * 0.6e-4), 0.5);
+    double DELTA = ((double)L93_A5[i] + (double)L93_A6[i] * V) * (P + E) * std::pow(V, (double)0.8f) * 1.e-3;
+    cplx ZF = l93_zf(freq, L93_F0O2[i], DELTA, GAMMA);
+    ZN = cadd(ZN, cscale(ZF, S));
+  }
+  double AT1 = 0.182 * freq * ZN.im;
+  if (AT1 < 0.) AT1 = 0.0;
+  double So = 6.14e-5 * P * p2(V);
+  double GAMMAo = 0.56e-3 * (P + E) * std::pow(V, (double)0.8f);
+  cplx ZFo = cdiv(cmk(freq, 0.0), cmplx4(freq, GAMMAo));
+  ZFo = cmk(-ZFo.re, -ZFo.im);
+  double Sn = 1.40e-12 * p2(P) * std::pow(V, 3.5);
+  cplx ZFn = cmplx4(0., freq / (1.93e-5 * std::pow(freq, 1.5) + 1.0));
+  ZN = cadd(cscale(ZFo, So), cscale(ZFn, Sn));
+  double AT2 = 0.182 * freq * ZN.im;
+  ZN = cmk(0.0, 0.0);
+  for (int i = 0; i < 35; i++) {
+    double S = (double)L93_B1[i] * E * std::pow(V, 3.5) * std::exp((double)L93_B2[i] * (1.0 - V));
+    double GAMH = (double)L93_B3[i] * (P * std::pow(V, (double)L93_B5[i]) +
+                                       (double)L93_B4[i] * E * std::pow(V, (double)L93_B6[i])) * 1.e-3;
+    double GAMD2 = 1.e-12 / V * p2((double)1.46f * (double)L93_F0H2O[i]);
+    GAMH = 0.535 * GAMH + std::pow(0.217 * p2(GAMH) + GAMD2, 0.5);
+    cplx ZF = l93_zf(freq, L93_F0H2O[i], 0.0, GAMH);
+    ZN = cadd(ZN, cscale(ZF, S));
+  }
+  double AT3 = 0.182 * freq * ZN.im;
+  double AT4 = 0.0;  // cloud term, W = 0
+  return 0.23026 * (AT1 + AT2 + AT3 + AT4) / 1.e3;
+}
+
 // ---------------------------------------------------------------- PSD
 // src/conversions.f90:5-24
 double q2abs(double spec, double t, double p, double qv, double qall) {
@@ -637,13 +926,6 @@ cplx eps_water_tkc(double T, double f) {
   t2 = (tau_2 * delta_2) / (1.0 + x2 * x2);
   double eps2 = w * (t1 + t2);
   return cmplx4(eps1, eps2);  // CMPLX without KIND (eps_water.f90:749)
-}
-
-// src/ref_water.f90 (TKC): returns refre, refim (positive)
-void ref_water(double T_c, double f, double& refre, double& refim) {
-  cplx r = csqrt_(eps_water_tkc(T_c, f));
-  refre = r.re;
-  refim = r.im;
 }
 
 // src/eps_ice.f90 + src/ref_ice.f90
@@ -1369,6 +1651,28 @@ int orc_gas_r98(double f, double T, double rhowv, double pres, double* kext) {
   return gas_r98(f, T, rhowv, pres, kext);
 }
 
+// get_eps_water (src/eps_water.f90:6-70) for liq_mod code 0..4; returns 2
+// where the model has no value.
+int orc_get_eps_water(int liq_mod, double s, double T_c, double f, double* re, double* im) {
+  cplx e;
+  switch (liq_mod) {
+    case 0: e = eps_water_tkc(T_c, f); break;
+    case 1: e = eps_water_ellison(s, T_c, f); break;
+    case 2: e = eps_water_liebe(T_c, f); break;
+    case 3:
+      if (eps_water_ray(T_c, f, e)) return 2;
+      break;
+    case 4: e = eps_water_stogryn(s, T_c, f); break;
+    default: return 2;
+  }
+  *re = e.re;
+  *im = e.im;
+  return 0;
+}
+
+// mpm93 as get_gasabs calls it: p, e in Pa, T in K; Np/m
+double orc_gas_l93(double f, double press, double vap, double T) { return gas_l93(f, press, vap, T); }
+
 void orc_eps_water_tkc(double T_c, double f, double* re, double* im) {
   cplx e = eps_water_tkc(T_c, f);
   *re = e.re;
@@ -1472,8 +1776,10 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
     // gas (src/get_gasabs.f90)
     std::vector<double> kgas(L, 0.0);
     if (st->lgas_extinction)
-      for (int z = 0; z < L; z++)
-        if (gas_r98(freq, a.temp[z], a.rho_vap[z], a.press[z], &kgas[z])) return 2;
+      for (int z = 0; z < L; z++) {
+        if (st->gas_mod == 1) kgas[z] = gas_l93(freq, a.press[z], a.vapor_pressure[z], a.temp[z]);
+        else if (gas_r98(freq, a.temp[z], a.rho_vap[z], a.press[z], &kgas[z])) return 2;
+      }
     // hydrometeors (src/hydrometeor_extinction.f90)
     std::vector<std::vector<double>> scat(L);
     std::vector<double> extk(L, 0.0), emk(L, 0.0), kext_h(L, 0.0), back_h(L, 0.0);
@@ -1508,8 +1814,11 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
           std::vector<double> ndens(nb);
           for (int i = 0; i < nb; i++) ndens[i] = bn.n_ds[i] / bn.delta_d[i];
           double refre, refim;
-          if (s.liq_ice == 1) ref_water(a.temp[z] - F(273.15f), freq, refre, refim);
-          else ref_ice(a.temp[z], freq, refre, refim);
+          if (s.liq_ice == 1) {
+            if (ref_water_mod(st->liq_mod, a.temp[z] - F(273.15f), freq, refre, refim)) return 2;
+          } else {
+            ref_ice(a.temp[z], freq, refre, refim);
+          }
           MieOut mo;
           if (calc_mie_spheres(*st, freq * 1e9, s.liq_ice, bn, ndens, refre, refim, mo)) return 2;
           save_bscat(z, h, mo, ndens);
@@ -1561,8 +1870,11 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
         std::vector<double> ndens(bn.nbin);
         for (int i = 0; i < bn.nbin; i++) ndens[i] = bn.n_ds[i] / bn.delta_d[i];
         double refre, refim;
-        if (s.liq_ice == 1) ref_water(a.temp[z] - F(273.15f), freq, refre, refim);  // 273.15 is default REAL (scatProperties.f90:227)
-        else ref_ice(a.temp[z], freq, refre, refim);
+        if (s.liq_ice == 1) {  // 273.15 is default REAL (scatProperties.f90:227)
+          if (ref_water_mod(st->liq_mod, a.temp[z] - F(273.15f), freq, refre, refim)) return 2;
+        } else {
+          ref_ice(a.temp[z], freq, refre, refim);
+        }
         MieOut mo;
         if (calc_mie_spheres(*st, freq * 1e9, s.liq_ice, bn, ndens, refre, refim, mo)) return 2;
         save_bscat(z, h, mo, ndens);

@@ -26,6 +26,8 @@ ST_GAS = 0x800
 ST_PIVOT = 0x1000
 ST_NAN = 0x2000
 ST_SIZE = 0x4000
+ST_TIMEOUT = 0x8000
+ST_RANGE = 0x10000
 
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -56,7 +58,8 @@ EXPORTS = ["pamtra_b200_create", "pamtra_b200_destroy", "pamtra_b200_workspace_b
            "pamtra_b200_eps_water_tkc", "pamtra_b200_minvert_batched", "pamtra_b200_set_timing",
            "pamtra_b200_stage_ms", "pamtra_b200_abi_sizes", "pamtra_b200_run_noalloc",
            "pamtra_b200_mmult_3xtf32_batched", "pamtra_b200_set_launch", "pamtra_b200_get_launch",
-           "pamtra_b200_graph_capture", "pamtra_b200_graph_launch", "pamtra_b200_graph_destroy"]
+           "pamtra_b200_graph_capture", "pamtra_b200_graph_launch", "pamtra_b200_graph_destroy",
+           "pamtra_b200_get_eps_water", "pamtra_b200_gas_l93"]
 NLAUNCH = 4  # PAMTRA_B200_NLAUNCH: mie warps per CTA, mie / layer / adding CTAs per SM
 STAGES = ["prep", "psd", "mie", "layer", "adding"]
 
@@ -87,6 +90,10 @@ def load():
         l.pamtra_b200_gas_r98.argtypes = [_vp] * 6 + [_i32, _vp]
         l.pamtra_b200_eps_water_tkc.restype = _i32
         l.pamtra_b200_eps_water_tkc.argtypes = [_vp] * 4 + [_i32, _vp]
+        l.pamtra_b200_get_eps_water.restype = _i32
+        l.pamtra_b200_get_eps_water.argtypes = [_i32] + [_vp] * 6 + [_i32, _vp]
+        l.pamtra_b200_gas_l93.restype = _i32
+        l.pamtra_b200_gas_l93.argtypes = [_vp] * 5 + [_i32, _vp]
         l.pamtra_b200_minvert_batched.restype = _i32
         l.pamtra_b200_minvert_batched.argtypes = [_vp, _vp, _vp, _i32, _i32, _vp]
         l.pamtra_b200_set_timing.restype = _i32

@@ -233,7 +233,7 @@ __global__ void k_status_out(Work w, int32_t* out, int n) {
 
 struct Plan {
   size_t total;
-  size_t o_hgt_lev, o_temp_lev, o_temp, o_press, o_rho_vap, o_q_hum, o_gtemp, o_outlev, o_kgas;
+  size_t o_hgt_lev, o_temp_lev, o_temp, o_press, o_rho_vap, o_q_hum, o_vap, o_gtemp, o_outlev, o_kgas;
   size_t o_slot_st, o_slot_nb, o_bd, o_bdd, o_bnd, o_brho, o_bmass;
   size_t o_pres_idx, o_plist, o_counters, o_mkext, o_msalb, o_mback, o_mnleg, o_mlegen, o_lay, o_laynd, o_status,
       o_colst;
@@ -275,6 +275,7 @@ Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms) {
   p.o_press = take(C * Lm * 8);
   p.o_rho_vap = take(C * Lm * 8);
   p.o_q_hum = take(C * Lm * 8);
+  p.o_vap = take(C * Lm * 8);
   p.o_gtemp = take(C * 8);
   p.o_outlev = take(C * std::max(1, c->noutlevels) * 4);
   p.o_kgas = take(C * Fm * Lm * 8);
@@ -728,6 +729,9 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     return PAMTRA_B200_FATAL;
   if (cols->nhydro > 0 && !cols->species) return PAMTRA_B200_FATAL;
   if (!(st->nummu == 8 || st->nummu == 16 || st->nummu == 32)) return PAMTRA_B200_FATAL;
+  if (st->liq_mod < PAMTRA_B200_LIQ_TKC || st->liq_mod > PAMTRA_B200_LIQ_STO ||
+      (st->gas_mod != PAMTRA_B200_GAS_R98 && st->gas_mod != PAMTRA_B200_GAS_L93))
+    return PAMTRA_B200_FATAL;
   if (cols->fs_d && (cols->fs_nbin < 1 || !cols->fs_d_bound || !cols->fs_n || !cols->fs_rho || !cols->fs_mass))
     return PAMTRA_B200_FATAL;
   if (out->psd_d && (out->psd_nbin < 1 || !out->psd_deltad || !out->psd_n || !out->psd_mass || !out->psd_area ||
@@ -793,7 +797,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   Work w{};
   w.hgt_lev = (double*)(A + pl.o_hgt_lev); w.temp_lev = (double*)(A + pl.o_temp_lev);
   w.temp = (double*)(A + pl.o_temp); w.press = (double*)(A + pl.o_press);
-  w.rho_vap = (double*)(A + pl.o_rho_vap); w.q_hum = (double*)(A + pl.o_q_hum);
+  w.rho_vap = (double*)(A + pl.o_rho_vap); w.q_hum = (double*)(A + pl.o_q_hum); w.vap = (double*)(A + pl.o_vap);
   w.gtemp = (double*)(A + pl.o_gtemp); w.outlev = (int*)(A + pl.o_outlev); w.kgas = (double*)(A + pl.o_kgas);
   w.slot_st = (int8_t*)(A + pl.o_slot_st); w.slot_nb = (int*)(A + pl.o_slot_nb);
   w.b_d = (double*)(A + pl.o_bd); w.b_dd = (double*)(A + pl.o_bdd); w.b_nd = (double*)(A + pl.o_bnd);
@@ -844,7 +848,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   }
   k_atmo<<<(unsigned)((C + 127) / 128), 128, 0, stream>>>(b, w); launches++;
   const size_t ngas = C * Fm * Lm;
-  k_gas<<<(unsigned)((ngas + 255) / 256), 256, 0, stream>>>(b, w, st->lgas_extinction); launches++;
+  k_gas<<<(unsigned)((ngas + 255) / 256), 256, 0, stream>>>(b, w, st->lgas_extinction, st->gas_mod); launches++;
   mark(ctx, stream, STG_PREP);
   if (H > 0) {
     const size_t ns = C * Lm * H;
@@ -1097,6 +1101,46 @@ int32_t pamtra_b200_eps_water_tkc(const double* t_c, const double* freq, double*
   return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
 }
 
+__global__ void k_eps_water_elem(int liq_mod, const double* s, const double* tc, const double* f, double* re,
+                                 double* im, int32_t* st, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int bad = 0;
+  cplx e;
+  switch (liq_mod) {
+    case PAMTRA_B200_LIQ_ELL: e = eps_water_ellison(s[i], tc[i], f[i]); break;
+    case PAMTRA_B200_LIQ_LIE: e = eps_water_liebe(tc[i], f[i]); break;
+    case PAMTRA_B200_LIQ_RAY: e = eps_water_ray(tc[i], f[i], &bad); break;
+    case PAMTRA_B200_LIQ_STO: e = eps_water_stogryn(s[i], tc[i], f[i]); break;
+    default: e = eps_water_tkc(tc[i], f[i]); break;
+  }
+  re[i] = e.re;
+  im[i] = e.im;
+  if (st) st[i] = bad ? (PAMTRA_B200_FATAL | PAMTRA_B200_ST_RANGE) : 0;
+}
+
+int32_t pamtra_b200_get_eps_water(int32_t liq_mod, const double* s, const double* t_c, const double* freq,
+                                  double* eps_re, double* eps_im, int32_t* status, int32_t n, void* stream) {
+  if (n <= 0) return PAMTRA_B200_OK;
+  if (liq_mod < PAMTRA_B200_LIQ_TKC || liq_mod > PAMTRA_B200_LIQ_STO || !s) return PAMTRA_B200_FATAL;
+  k_eps_water_elem<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(liq_mod, s, t_c, freq, eps_re, eps_im, status,
+                                                                     n);
+  return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
+}
+
+__global__ void k_l93_elem(const double* f, const double* p, const double* e, const double* T, double* k, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  k[i] = gas_l93(f[i], p[i], e[i], T[i]);
+}
+
+int32_t pamtra_b200_gas_l93(const double* freq, const double* press, const double* vap, const double* temp,
+                            double* kext, int32_t n, void* stream) {
+  if (n <= 0) return PAMTRA_B200_OK;
+  k_l93_elem<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(freq, press, vap, temp, kext, n);
+  return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
+}
+
 int32_t pamtra_b200_minvert_batched(const double* a, double* ainv, int32_t* status, int32_t n, int32_t count,
                                     void* stream) {
   if (count <= 0) return PAMTRA_B200_OK;
@@ -1153,7 +1197,8 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
       cols->max_nfreq < 1 || cols->max_nfreq > PAMTRA_B200_NOALLOC_MAX_NFREQ || cols->nhydro < 0 ||
       cols->nhydro > PAMTRA_B200_NOALLOC_MAX_NHYDRO || cols->noutlevels < 1 || cols->noutlevels > 2 ||
       !(cols->max_nummu == 8 || cols->max_nummu == 16) || !(st->nummu == 8 || st->nummu == 16) ||
-      (cols->nhydro > 0 && !cols->species) || cols->fs_d || out->psd_d)
+      (cols->nhydro > 0 && !cols->species) || cols->fs_d || out->psd_d || st->liq_mod < PAMTRA_B200_LIQ_TKC ||
+      st->liq_mod > PAMTRA_B200_LIQ_STO || (st->gas_mod != PAMTRA_B200_GAS_R98 && st->gas_mod != PAMTRA_B200_GAS_L93))
     return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return PAMTRA_B200_FATAL;
@@ -1202,9 +1247,9 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   // scratch layout (same plan as the arena of pamtra_b200_run); bins are
   // sized for PAMTRA_B200_NOALLOC_MAX_NBIN
   pamtra_b200_columns cc = *cols;
-  pamtra_b200_species plan_sp{};
-  plan_sp.nbin = PAMTRA_B200_NOALLOC_MAX_NBIN;
-  cc.species = &plan_sp;
+  pamtra_b200_species plan_sp[PAMTRA_B200_NOALLOC_MAX_NHYDRO] = {};  // one entry per species slot make_plan reads
+  for (auto& s : plan_sp) s.nbin = PAMTRA_B200_NOALLOC_MAX_NBIN;
+  cc.species = plan_sp;
   cc.species_stride = 0;
   const int nh = cc.nhydro;
   cc.nhydro = nh > 0 ? nh : 0;
@@ -1226,7 +1271,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   Work w{};
   w.hgt_lev = (double*)(A + pl.o_hgt_lev); w.temp_lev = (double*)(A + pl.o_temp_lev);
   w.temp = (double*)(A + pl.o_temp); w.press = (double*)(A + pl.o_press);
-  w.rho_vap = (double*)(A + pl.o_rho_vap); w.q_hum = (double*)(A + pl.o_q_hum);
+  w.rho_vap = (double*)(A + pl.o_rho_vap); w.q_hum = (double*)(A + pl.o_q_hum); w.vap = (double*)(A + pl.o_vap);
   w.gtemp = (double*)(A + pl.o_gtemp); w.outlev = (int*)(A + pl.o_outlev); w.kgas = (double*)(A + pl.o_kgas);
   w.slot_st = (int8_t*)(A + pl.o_slot_st); w.slot_nb = (int*)(A + pl.o_slot_nb);
   w.b_d = (double*)(A + pl.o_bd); w.b_dd = (double*)(A + pl.o_bdd); w.b_nd = (double*)(A + pl.o_bnd);
@@ -1248,7 +1293,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   const size_t ntb = (size_t)cc.noutlevels * 2 * cc.max_nummu * Fm * 2;
   k_fill_d<<<(unsigned)((ntb + 255) / 256), 256, 0, stream>>>(out->tb, -9999.0, ntb);
   k_atmo<<<1, 128, 0, stream>>>(b, w);
-  k_gas<<<(unsigned)((Fm * Lm + 255) / 256), 256, 0, stream>>>(b, w, st->lgas_extinction);
+  k_gas<<<(unsigned)((Fm * Lm + 255) / 256), 256, 0, stream>>>(b, w, st->lgas_extinction, st->gas_mod);
   if (nh > 0) k_psd<<<(unsigned)((Lm * nh + 127) / 128), 128, 0, stream>>>(b, w, *st);
   k_compact<<<1, 1024, 0, stream>>>(b, w);
   int sms = 0;

@@ -45,8 +45,118 @@ __device__ cplx eps_water_tkc(double T, double f) {
   return cmplx4(eps1, eps2);  // CMPLX without KIND (eps_water.f90:749)
 }
 
-// src/ref_water.f90 (liq_mod TKC): m = sqrt(eps), (refre, refim) with refim > 0
-__device__ cplx ref_water(double T_c, double f) { return csqrt_(eps_water_tkc(T_c, f)); }
+// The other liquid water models of src/eps_water.f90 (nmlSet['liq_mod']),
+// salinity 0 as src/scatProperties.f90:228 passes it; T in degC, f in GHz.
+// Literals without a kind in the reference are REAL(4) values promoted to
+// REAL(8) (written as float literals here), its pi parameter is the REAL(4)
+// value of 3.141592653589793, and CMPLX without KIND rounds both parts to
+// REAL(4).
+constexpr double PI_R4 = (double)3.141592653589793f;
+
+// eps_water_ellison (src/eps_water.f90:85-158, after Maetzler 2006, 5.2.5.4)
+__device__ cplx eps_water_ellison(double s, double T, double f) {
+  const double a1 = 0.46606917e-02f, a2 = -0.26087876e-04f, a3 = -0.63926782e-05f, a4 = 0.63000075e+01f,
+               a5 = 0.26242021e-02f, a6 = -0.42984155e-02f, a7 = 0.34414691e-04f, a8 = 0.17667420e-03f,
+               a9 = -0.20491560e-06f, a10 = 0.58366888e+03f, a11 = 0.12634992e+03f, a12 = 0.69227972e-04f,
+               a13 = 0.38957681e-06f, a14 = 0.30742330e+03f, a15 = 0.12634992e+03f, a16 = 0.37245044e+01f,
+               a17 = 0.92609781e-02f, a18 = -0.26093754e-01f;
+  const double T2 = T * T, T4 = T2 * T2;
+  const double p = s * (37.5109f + 5.45216f * s + 0.014409f * (s * s)) / (1004.75f + 182.283f * s + s * s);
+  const double alpha_0 = (6.9431f + 3.2841f * s - 0.099486f * (s * s)) / (84.85f + 69.024f * s + s * s);
+  const double alpha_1 = 49.843f - 0.2276f * s + 0.00198f * (s * s);
+  const double sig_s35 = 2.903602f + 8.607e-02f * T + 4.738817e-04f * T2 - 2.991e-06f * (T2 * T) + 4.3041e-09f * T4;
+  const double eps_s = 87.85306f * exp(-0.00456992f * T - a1 * s - a2 * (s * s) - a3 * s * T);
+  const double eps_1 = a4 * exp(-a5 * T - a6 * s - a7 * s * T);
+  const double tau_1 = (a8 + a9 * s) * exp(a10 / (T + a11));
+  const double tau_2 = (a12 + a13 * s) * exp(a14 / (T + a15));
+  const double eps_inf = a16 + a17 * T + a18 * s;
+  const double q = 1 + (alpha_0 * (T - 15)) / (T + alpha_1);
+  const double sig = sig_s35 * p * q;
+  const cplx d1 = cmk(1.0, -(2.0 * PI_R4 * f * tau_1)), d2 = cmk(1.0, -(2.0 * PI_R4 * f * tau_2));
+  cplx e = cadd(cdiv(cmk(eps_s - eps_1, 0.0), d1), cdiv(cmk(eps_1 - eps_inf, 0.0), d2));
+  e = cadd(e, cmk(eps_inf, 0.0));
+  return cadd(e, cmk(0.0, (double)17.9751f * sig / f));
+}
+
+// eps_water_liebe (src/eps_water.f90:160-207, Liebe, Hufford and Manabe 1991)
+__device__ cplx eps_water_liebe(double T, double f) {
+  const double T_K = T + 273.15f;
+  const double theta_1 = 1. - 300. / T_K;
+  const double fp = 20.1f * exp(7.88f * theta_1);
+  const double fs = 39.8f * fp;
+  const double eps_0 = 77.66f - 103.3f * theta_1;
+  const double eps_1 = 0.0671f * eps_0;
+  const double eps_2 = 3.52f;
+  cplx e = cadd(cdiv(cmk(eps_0 - eps_1, 0.0), cmplx4(1.0, -f / fp)), cdiv(cmk(eps_1 - eps_2, 0.0), cmplx4(1.0, -f / fs)));
+  return cadd(e, cmk(eps_2, 0.0));
+}
+
+// eps_water_ray (src/eps_water.f90:209-596, Ray 1972) for wavelengths above
+// 1 mm (f below 299.79 GHz); the tabulated optical constants of shorter
+// wavelengths are not on this path: *bad is set there.
+__device__ cplx eps_water_ray(double T, double f, int* bad) {
+  const double wl = (double)(1.e6f * 2.99792458e8f) / (f * 1.e9f);  // microns
+  if (wl < (double)0.2f || wl > 100000.0 || !(wl > 1000.0)) {
+    *bad = 1;
+    return cmk(1.0, 0.0);
+  }
+  const double T1 = T + 273.0f, T2 = T - 25.0f, xl = wl / 10000.0f;
+  const double sigma = 12.5664e8f;
+  const double alpha = -16.8129f / T1 + 0.0609265f;
+  const double eps_s = 78.54f * (1.0f - 4.579e-3f * T2 + 1.19e-5f * (T2 * T2) - 2.8e-8f * (T2 * T2 * T2));
+  const double eps_inf = 5.27137f + 0.0216474f * T - 0.00131198f * (T * T);
+  const double xlams = 0.00033836f * exp(2513.98f / T1);
+  const double powtrm = pow(xlams / xl, 1.f - alpha);
+  const double sn = sin(PI_R4 * alpha / 2), cs = cos(PI_R4 * alpha / 2);
+  const double denom = 1.f + 2 * powtrm * sn + pow(xlams / xl, 2.f * (1.f - alpha));
+  const double eps_r = eps_inf + (eps_s - eps_inf) * (1.0f + powtrm * sn) / denom;
+  const double eps_i = (sigma * xl / (double)18.8496e10f) + (eps_s - eps_inf) * powtrm * cs / denom;
+  const cplx n = csqrt_(cmk(eps_r, eps_i));
+  double rn = n.re, cn = n.im;
+  if (!(wl > 3000.0f)) {
+    // remaining absorption bands (Ray eq. 8, table 2)
+    cn = cn + 0.39f * exp(-pow(fabs(log10(wl / 17.0f) / 0.45f), (double)1.3f)) +
+         0.41f * exp(-pow(fabs(log10(wl / 62.0f) / 0.35f), (double)1.7f)) +
+         0.25f * exp(-pow(fabs(log10(wl / 300.0f) / 0.47f), 3.0));
+  }
+  return cmul(cmk(rn, cn), cmk(rn, cn));
+}
+
+// eps_water_stogryn (src/eps_water.f90:598-651, after Maetzler 2006, 5.2.4.2)
+__device__ cplx eps_water_stogryn(double s, double T, double f) {
+  const double T2 = T * T, T4 = T2 * T2;
+  const double p = s * (37.5109f + 5.45216f * s + 0.014409f * (s * s)) / (1004.75f + 182.283f * s + s * s);
+  const double alpha_0 = (6.9431f + 3.2841f * s - 0.099486f * (s * s)) / (84.85f + 69.024f * s + s * s);
+  const double alpha_1 = 49.843f - 0.2276f * s + 0.00198f * (s * s);
+  const double sig_s35 = 2.903602f + 8.607e-02f * T + 4.738817e-04f * T2 - 2.991e-06f * (T2 * T) + 4.3041e-09f * T4;
+  const double a = 1.f - (s * (0.03838f + 0.00218f * s) * (79.88f + T)) / ((12.01f + s) * (52.53f + T));
+  const double b = 1.f - s * ((0.03409f + 0.002817f * s) / (7.69f + s)) -
+                   s * T * ((0.00246f + 0.00141f * T) / (188.f - 7.57f * T + T2));
+  const double eps_s = ((37088.6f - 82.168f * T) / (421.854f + T)) * a;
+  const double eps_1 = (0.0787f * ((37088.6f - 82.168f * T) / (421.854f + T))) * a;
+  const double tpt1 = ((255.04f + 0.7246f * T) / ((49.25f + T) * (45.f + T))) * b;
+  const double tpt2 = 0.00628f;
+  const double eps_inf = 4.05f + 0.0186f * T;
+  const double q = 1 + (alpha_0 * (T - 15)) / (T + alpha_1);
+  const double sig = sig_s35 * p * q;
+  cplx e = cadd(cdiv(cmk(eps_s - eps_1, 0.0), cmk(1.0, -(f * tpt1))), cdiv(cmk(eps_1 - eps_inf, 0.0), cmk(1.0, -(f * tpt2))));
+  e = cadd(e, cmk(eps_inf, 0.0));
+  return cadd(e, cmk(0.0, (double)17.9751f * sig / f));
+}
+
+// src/ref_water.f90 with src/eps_water.f90:39-63 (get_eps_water): m = sqrt(eps),
+// (refre, refim) with refim > 0; *bad set where the model has no value.
+__device__ cplx ref_water(double T_c, double f, int liq_mod, int* bad) {
+  cplx e;
+  switch (liq_mod) {
+    case PAMTRA_B200_LIQ_ELL: e = eps_water_ellison(0.0, T_c, f); break;
+    case PAMTRA_B200_LIQ_LIE: e = eps_water_liebe(T_c, f); break;
+    case PAMTRA_B200_LIQ_RAY: e = eps_water_ray(T_c, f, bad); break;
+    case PAMTRA_B200_LIQ_STO: e = eps_water_stogryn(0.0, T_c, f); break;
+    default: e = eps_water_tkc(T_c, f); break;
+  }
+  return csqrt_(e);
+}
 
 // src/eps_ice.f90 + src/ref_ice.f90 (Maetzler ice)
 __device__ cplx ref_ice(double T, double f) {
@@ -226,7 +336,12 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
       const double* bnd = w.b_nd + base;
       const double* brho = w.b_rho + base;
       const double* bmass = w.b_mass + base;
-      cplx mref = (sp.liq_ice == 1) ? ref_water(T - F(273.15f), freq) : ref_ice(T, freq);
+      int bad_ref = 0;
+      cplx mref = (sp.liq_ice == 1) ? ref_water(T - F(273.15f), freq, st.liq_mod, &bad_ref) : ref_ice(T, freq);
+      if (bad_ref) {
+        status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_RANGE;
+        break;
+      }
       const cplx m_ice = cmk(mref.re, -mref.im);
       // density / diameter of bin i (frequency-dependent soft spheroids of
       // make_soft_spheroid.f90:109-114 resolved here)

@@ -91,6 +91,7 @@ __global__ void k_atmo(Batch b, Work w) {
     t[z] = tz;
     p[z] = pz;
     double vp = rz * e_sat_gg_water(tz);
+    w.vap[(size_t)c * Lm + z] = vp;
     rv[z] = vp / (tz * R_V);
     qh[z] = R_V / R_D * vp / (pz - (1.0 - R_V / R_D) * vp);
   }
@@ -175,8 +176,182 @@ __device__ int gas_r98(double f, double T, double rhowv, double pres, double* ke
   return 0;
 }
 
+// ---------------------------------------------------------------- gas (MPM93)
+// Line catalogue of Liebe, Hufford and Cotton (1993), as the reference holds
+// it in REAL(4) (src/mpm93.f90:131-222): oxygen {f0 GHz, a1..a6}, water
+// vapour {f0 GHz, b1..b6}.
+__constant__ float c_l93_o2[44][7] = {
+    {50.474239f, 0.094f, 9.694f, 0.890f, 0.000f, 0.240f, 0.790f},
+    {50.987747f, 0.246f, 8.694f, 0.910f, 0.000f, 0.220f, 0.780f},
+    {51.503349f, 0.608f, 7.744f, 0.940f, 0.000f, 0.197f, 0.774f},
+    {52.021412f, 1.414f, 6.844f, 0.970f, 0.000f, 0.166f, 0.764f},
+    {52.542393f, 3.102f, 6.004f, 0.990f, 0.000f, 0.136f, 0.751f},
+    {53.066906f, 6.410f, 5.224f, 1.020f, 0.000f, 0.131f, 0.714f},
+    {53.595749f, 12.470f, 4.484f, 1.050f, 0.000f, 0.230f, 0.584f},
+    {54.130001f, 22.800f, 3.814f, 1.070f, 0.000f, 0.335f, 0.431f},
+    {54.671158f, 39.180f, 3.194f, 1.100f, 0.000f, 0.374f, 0.305f},
+    {55.221367f, 63.160f, 2.624f, 1.130f, 0.000f, 0.258f, 0.339f},
+    {55.783802f, 95.350f, 2.119f, 1.170f, 0.000f, -0.166f, 0.705f},
+    {56.264774f, 54.890f, 0.015f, 1.730f, 0.000f, 0.390f, -0.113f},
+    {56.363388f, 134.400f, 1.660f, 1.200f, 0.000f, -0.297f, 0.753f},
+    {56.968204f, 176.300f, 1.260f, 1.240f, 0.000f, -0.416f, 0.742f},
+    {57.612484f, 214.100f, 0.915f, 1.280f, 0.000f, -0.613f, 0.697f},
+    {58.323875f, 238.600f, 0.626f, 1.330f, 0.000f, -0.205f, 0.051f},
+    {58.446590f, 145.700f, 0.084f, 1.520f, 0.000f, 0.748f, -0.146f},
+    {59.164207f, 240.400f, 0.391f, 1.390f, 0.000f, -0.722f, 0.266f},
+    {59.590984f, 211.200f, 0.212f, 1.430f, 0.000f, 0.765f, -0.090f},
+    {60.306061f, 212.400f, 0.212f, 1.450f, 0.000f, -0.705f, 0.081f},
+    {60.434776f, 246.100f, 0.391f, 1.360f, 0.000f, 0.697f, -0.324f},
+    {61.150558f, 250.400f, 0.626f, 1.310f, 0.000f, 0.104f, -0.067f},
+    {61.800156f, 229.800f, 0.915f, 1.270f, 0.000f, 0.570f, -0.761f},
+    {62.411217f, 193.300f, 1.260f, 1.230f, 0.000f, 0.360f, -0.777f},
+    {62.486259f, 151.700f, 0.083f, 1.540f, 0.000f, -0.498f, 0.097f},
+    {62.997978f, 150.300f, 1.665f, 1.200f, 0.000f, 0.239f, -0.768f},
+    {63.568520f, 108.700f, 2.115f, 1.170f, 0.000f, 0.108f, -0.706f},
+    {64.127769f, 73.350f, 2.620f, 1.130f, 0.000f, -0.311f, -0.332f},
+    {64.678902f, 46.350f, 3.195f, 1.100f, 0.000f, -0.421f, -0.298f},
+    {65.224068f, 27.480f, 3.815f, 1.070f, 0.000f, -0.375f, -0.423f},
+    {65.764771f, 15.300f, 4.485f, 1.050f, 0.000f, -0.267f, -0.575f},
+    {66.302094f, 8.009f, 5.225f, 1.020f, 0.000f, -0.168f, -0.700f},
+    {66.836830f, 3.946f, 6.005f, 0.990f, 0.000f, -0.169f, -0.735f},
+    {67.369598f, 1.832f, 6.845f, 0.970f, 0.000f, -0.200f, -0.744f},
+    {67.900864f, 0.801f, 7.745f, 0.940f, 0.000f, -0.228f, -0.753f},
+    {68.431007f, 0.330f, 8.695f, 0.920f, 0.000f, -0.240f, -0.760f},
+    {68.960312f, 0.128f, 9.695f, 0.900f, 0.000f, -0.250f, -0.765f},
+    {118.750343f, 94.500f, 0.009f, 1.630f, 0.000f, -0.036f, 0.009f},
+    {368.498352f, 6.790f, 0.049f, 1.920f, 0.600f, 0.000f, 0.000f},
+    {424.763123f, 63.800f, 0.044f, 1.930f, 0.600f, 0.000f, 0.000f},
+    {487.249359f, 23.500f, 0.049f, 1.920f, 0.600f, 0.000f, 0.000f},
+    {715.393127f, 9.960f, 0.145f, 1.810f, 0.600f, 0.000f, 0.000f},
+    {773.839661f, 67.100f, 0.130f, 1.820f, 0.600f, 0.000f, 0.000f},
+    {834.145325f, 18.000f, 0.147f, 1.810f, 0.600f, 0.000f, 0.000f},
+};
+__constant__ float c_l93_h2o[35][7] = {
+    {22.235081f, 0.01130f, 2.143f, 2.811f, 4.80f, 0.69f, 1.00f},
+    {67.803963f, 0.00012f, 8.735f, 2.858f, 4.93f, 0.69f, 0.82f},
+    {119.995941f, 0.00008f, 8.356f, 2.948f, 4.78f, 0.70f, 0.79f},
+    {183.310089f, 0.24200f, 0.668f, 3.050f, 5.30f, 0.64f, 0.85f},
+    {321.225647f, 0.00483f, 6.181f, 2.303f, 4.69f, 0.67f, 0.54f},
+    {325.152924f, 0.14990f, 1.540f, 2.783f, 4.85f, 0.68f, 0.74f},
+    {336.222595f, 0.00011f, 9.829f, 2.693f, 4.74f, 0.69f, 0.61f},
+    {380.197357f, 1.15200f, 1.048f, 2.873f, 5.38f, 0.54f, 0.89f},
+    {390.134521f, 0.00046f, 7.350f, 2.152f, 4.81f, 0.63f, 0.55f},
+    {437.346680f, 0.00650f, 5.050f, 1.845f, 4.23f, 0.60f, 0.48f},
+    {439.150818f, 0.09218f, 3.596f, 2.100f, 4.29f, 0.63f, 0.52f},
+    {443.018280f, 0.01976f, 5.050f, 1.860f, 4.23f, 0.60f, 0.50f},
+    {448.001068f, 1.03200f, 1.405f, 2.632f, 4.84f, 0.66f, 0.67f},
+    {470.888947f, 0.03297f, 3.599f, 2.152f, 4.57f, 0.66f, 0.65f},
+    {474.689117f, 0.12620f, 2.381f, 2.355f, 4.65f, 0.65f, 0.64f},
+    {488.491119f, 0.02520f, 2.853f, 2.602f, 5.04f, 0.69f, 0.72f},
+    {503.568542f, 0.00390f, 6.733f, 1.612f, 3.98f, 0.61f, 0.43f},
+    {504.482697f, 0.00130f, 6.733f, 1.612f, 4.01f, 0.61f, 0.45f},
+    {547.676453f, 0.97010f, 0.114f, 2.600f, 4.50f, 0.70f, 1.00f},
+    {552.020935f, 1.47700f, 0.114f, 2.600f, 4.50f, 0.70f, 1.00f},
+    {556.935974f, 48.74000f, 0.159f, 3.210f, 4.11f, 0.69f, 1.00f},
+    {620.700806f, 0.50120f, 2.200f, 2.438f, 4.68f, 0.71f, 0.68f},
+    {645.866150f, 0.00713f, 8.580f, 1.800f, 4.00f, 0.60f, 0.50f},
+    {658.005310f, 0.03022f, 7.820f, 3.210f, 4.14f, 0.69f, 1.00f},
+    {752.033203f, 23.96000f, 0.396f, 3.060f, 4.09f, 0.68f, 0.84f},
+    {841.053955f, 0.00140f, 8.180f, 1.590f, 5.76f, 0.33f, 0.45f},
+    {859.962341f, 0.01472f, 7.989f, 3.060f, 4.09f, 0.68f, 0.84f},
+    {899.306702f, 0.00605f, 7.917f, 2.985f, 4.53f, 0.68f, 0.90f},
+    {902.616150f, 0.00426f, 8.432f, 2.865f, 5.10f, 0.70f, 0.95f},
+    {906.207336f, 0.01876f, 5.111f, 2.408f, 4.70f, 0.70f, 0.53f},
+    {916.171570f, 0.83400f, 1.442f, 2.670f, 4.78f, 0.70f, 0.78f},
+    {923.118408f, 0.00869f, 10.220f, 2.900f, 5.00f, 0.70f, 0.80f},
+    {970.315002f, 0.89720f, 1.920f, 2.550f, 4.94f, 0.64f, 0.67f},
+    {987.926758f, 13.21000f, 0.258f, 2.985f, 4.55f, 0.68f, 0.90f},
+    {1780.000000f, 2230.00000f, 0.952f, 17.620f, 30.50f, 2.00f, 5.00f},
+};
+
+struct cplxf {
+  float re, im;
+};
+// Smith-style division in single precision, as gfortran emits it for
+// COMPLEX(4) operands (-fcx-fortran-rules).
+__device__ __forceinline__ cplxf cdivf(cplxf a, cplxf b) {
+  float tr, ti, ratio, div;
+  if (fabsf(b.re) < fabsf(b.im)) {
+    ratio = b.re / b.im;
+    div = (b.re * ratio) + b.im;
+    tr = (a.re * ratio) + a.im;
+    ti = (a.im * ratio) - a.re;
+  } else {
+    ratio = b.im / b.re;
+    div = (b.im * ratio) + b.re;
+    tr = (a.im * ratio) + a.re;
+    ti = a.im - (a.re * ratio);
+  }
+  return {tr / div, ti / div};
+}
+
+// Line shape term of src/mpm93.f90:269-270 / 300-301:
+// f/f0 [CMPLX(1,-d)/CMPLX(f0-f,-g) - CMPLX(1,d)/CMPLX(f0+f,g)], where CMPLX
+// without KIND makes each quotient single precision.
+__device__ __forceinline__ cplx l93_shape(double f, double f0, double d, double g) {
+  const cplxf q1 = cdivf({1.f, (float)(-d)}, {(float)(f0 - f), (float)(-g)});
+  const cplxf q2 = cdivf({1.f, (float)d}, {(float)(f0 + f), (float)g});
+  const double r = f / f0;
+  return cmk(r * (double)(q1.re - q2.re), r * (double)(q1.im - q2.im));
+}
+
+// src/mpm93.f90 (gas_mod 'L93'): oxygen lines, dry-air continuum and water
+// vapour pseudo-line continuum of Liebe's MPM93 with the cloud term at
+// W = 0, as src/get_gasabs.f90:78-86 calls it (pressure and vapour pressure
+// in Pa, T in K); returns Np/m.
+__device__ double gas_l93(double freq, double press, double vap, double T) {
+  const double Tc = T - 273.15;
+  const double V = 300.0 / (Tc + 273.15);
+  double Pb = 10.0 * (press / 1.e3);
+  const double E = 10.0 * (vap / 1.e3);
+  double P = Pb - E;
+  if (P < 0) {
+    P = 0.0;
+    Pb = E;
+  }
+  const double V08 = pow(V, (double)0.8f), V3 = (V * V) * V, V35 = pow(V, 3.5);
+  double zr = 0.0, zi = 0.0;
+  for (int i = 0; i < 44; i++) {
+    const float* a = c_l93_o2[i];
+    const double f0 = a[0];
+    const double S = (double)a[1] * P * V3 * exp((double)a[2] * (1.0 - V)) * 1.e-6;
+    double g = (double)a[3] * (P * pow(V, 0.8 - (double)a[4]) + 1.1 * E * V) * 1.e-3;
+    g = pow(g * g + (25.0 * 0.6e-4) * (25.0 * 0.6e-4), (double)0.5f);
+    const double d = ((double)a[5] + (double)a[6] * V) * (P + E) * V08 * 1.e-3;
+    const cplx zf = l93_shape(freq, f0, d, g);
+    zr = zr + S * zf.re;
+    zi = zi + S * zf.im;
+  }
+  double at1 = 0.182 * freq * zi;
+  if (at1 < 0.) at1 = 0.0;
+  // dry air continuum
+  const double So = 6.14e-5 * P * (V * V);
+  const double gamo = 0.56e-3 * (P + E) * V08;
+  const cplx zfo = cdiv(cmk(-freq, 0.0), cmk((double)(float)freq, (double)(float)gamo));
+  const double Sn = 1.40e-12 * (P * P) * V35;
+  const double zfn = (double)(float)(freq / (1.93e-5 * pow(freq, (double)1.5f) + 1.0));
+  const double at2 = 0.182 * freq * (So * zfo.im + Sn * zfn);
+  // water vapour
+  zr = 0.0;
+  zi = 0.0;
+  for (int i = 0; i < 35; i++) {
+    const float* b = c_l93_h2o[i];
+    const double f0 = b[0];
+    const double S = (double)b[1] * E * V35 * exp((double)b[2] * (1.0 - V));
+    double gh = (double)b[3] * (P * pow(V, (double)b[5]) + (double)b[4] * E * pow(V, (double)b[6])) * 1.e-3;
+    const double fd = (double)1.46f * f0;
+    const double gd2 = 1.e-12 / V * (fd * fd);
+    gh = 0.535 * gh + pow(0.217 * (gh * gh) + gd2, (double)0.5f);
+    const cplx zf = l93_shape(freq, f0, 0.0, gh);
+    zr = zr + S * zf.re;
+    zi = zi + S * zf.im;
+  }
+  const double at3 = 0.182 * freq * zi;
+  return 0.23026 * (at1 + at2 + at3) / 1.e3;
+}
+
 // one thread per (column, frequency, layer)
-__global__ void k_gas(Batch b, Work w, int lgas) {
+__global__ void k_gas(Batch b, Work w, int lgas, int gas_mod) {
   const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
   if (idx >= (size_t)b.ncol * Fm * Lm) return;
@@ -185,12 +360,17 @@ __global__ void k_gas(Batch b, Work w, int lgas) {
   const int c = idx / ((size_t)Lm * Fm);
   double k = 0.0;
   if (z < b.nlyrs[c] && f < b.col_nfreq(c) && lgas) {
-    int st = gas_r98(b.freq(c, f), w.temp[(size_t)c * Lm + z], w.rho_vap[(size_t)c * Lm + z],
-                     w.press[(size_t)c * Lm + z], &k);
-    if (st) atomicOr(&w.status[(size_t)c * Fm + f], st);
+    const size_t lz = (size_t)c * Lm + z;
+    if (gas_mod == PAMTRA_B200_GAS_L93) {
+      k = gas_l93(b.freq(c, f), w.press[lz], w.vap[lz], w.temp[lz]);
+    } else {
+      int st = gas_r98(b.freq(c, f), w.temp[lz], w.rho_vap[lz], w.press[lz], &k);
+      if (st) atomicOr(&w.status[(size_t)c * Fm + f], st);
+    }
   }
   w.kgas[idx] = k;
 }
+
 
 // ---------------------------------------------------------------- PSD
 __device__ __forceinline__ double q2abs(double spec, double t, double p, double qv, double qall) {

@@ -42,7 +42,7 @@ struct Batch {
 struct Work {
   // atmosphere
   double *hgt_lev, *temp_lev;          // [C][Lm+1]
-  double *temp, *press, *rho_vap, *q_hum;  // [C][Lm]
+  double *temp, *press, *rho_vap, *q_hum, *vap;  // [C][Lm]; vap: vapour pressure, Pa
   double* gtemp;                       // [C]
   int* outlev;                         // [C][nout]
   double* kgas;                        // [C][Fm][Lm]

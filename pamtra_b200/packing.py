@@ -16,6 +16,10 @@ DIST_CODES = {"exp": 0, "exp_field_t": 1, "mgamma": 2, "mono": 3, "exp_cosmo_sno
 # scat_name codes: only Mie spheres are on this path
 SCAT_CODES = {"mie-sphere": 0, "disabled": 1}
 
+# nmlSet['liq_mod'] / nmlSet['gas_mod'] codes (PAMTRA_B200_LIQ_* / _GAS_*)
+LIQ_MODS = {"TKC": 0, "Ell": 1, "Lie": 2, "Ray": 3, "Sto": 4}
+GAS_MODS = {"R98": 0, "L93": 1}
+
 MAXNLEG = 200
 # radar_attenuation codes (PAMTRA_B200_ATT_*)
 RADAR_ATTENUATION = {"disabled": 0, "bottom-up": 1, "top-down": 2}
@@ -40,6 +44,8 @@ class Settings(ctypes.Structure):
         ("active", ctypes.c_int32),
         ("radar_attenuation", ctypes.c_int32),
         ("radar_k2", ctypes.c_double),
+        ("liq_mod", ctypes.c_int32),
+        ("gas_mod", ctypes.c_int32),
     ]
 
 
@@ -74,10 +80,14 @@ def settings_from_nml(nmlSet, nummu=16):
     """Validate the namelist keys this path honours and build the settings
     struct.  Options whose reference branch is not on the passive Mie path
     raise NotImplementedError instead of silently changing behaviour."""
-    if str(nmlSet.get("gas_mod", "R98")).strip() != "R98":
-        raise NotImplementedError("gas_mod %r: only R98 is on this path" % nmlSet["gas_mod"])
-    if str(nmlSet.get("liq_mod", "TKC")).strip() != "TKC":
-        raise NotImplementedError("liq_mod %r: only TKC is on this path" % nmlSet["liq_mod"])
+    gas = str(nmlSet.get("gas_mod", "R98")).strip()
+    if gas not in GAS_MODS:
+        # settings.f90:286-287
+        raise ValueError("gas_mod has to be L93 or R98")
+    liq = str(nmlSet.get("liq_mod", "TKC")).strip()
+    if liq not in LIQ_MODS:
+        # eps_water.f90:59-63
+        raise ValueError("Do not know liq_mod: %s" % liq)
     outpol = str(nmlSet.get("outpol", "VH")).strip()
     if outpol not in ("VH", "IQ"):
         raise ValueError("outpol must be VH or IQ")
@@ -101,6 +111,8 @@ def settings_from_nml(nmlSet, nummu=16):
         raise ValueError("radar_attenuation must be one of %s" % sorted(RADAR_ATTENUATION))
     s.radar_attenuation = RADAR_ATTENUATION[att]
     s.radar_k2 = float(nmlSet.get("radar_k2", 0.93))
+    s.liq_mod = LIQ_MODS[liq]
+    s.gas_mod = GAS_MODS[gas]
     if s.active and str(nmlSet.get("radar_mode", "simple")).strip() != "simple":
         raise NotImplementedError("radar_mode %r: only 'simple' is on this path" % nmlSet["radar_mode"])
     return s

@@ -69,12 +69,10 @@ def test_packing_codes():
     assert sp["liq_ice"].tolist() == [1, -1]
     st = packing.settings_from_nml(pam.nmlSet)
     assert st.emissivity == 0.6 and st.outpol_vh == 1 and st.nummu == 16
-    bad = dict(pam.nmlSet, gas_mod="L93")
-    with pytest.raises(NotImplementedError):
-        packing.settings_from_nml(bad)
-    bad = dict(pam.nmlSet, liq_mod="Ell")
-    with pytest.raises(NotImplementedError):
-        packing.settings_from_nml(bad)
+    assert packing.settings_from_nml(dict(pam.nmlSet, gas_mod="L93")).gas_mod == packing.GAS_MODS["L93"]
+    assert packing.settings_from_nml(dict(pam.nmlSet, liq_mod="Ell")).liq_mod == packing.LIQ_MODS["Ell"]
+    with pytest.raises(ValueError):
+        packing.settings_from_nml(dict(pam.nmlSet, gas_mod="MPM"))
 
 
 def test_present_bound_covers_hydrometeor_layers():
