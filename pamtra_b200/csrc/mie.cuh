@@ -54,7 +54,7 @@ __device__ cplx eps_water_tkc(double T, double f) {
 constexpr double PI_R4 = (double)3.141592653589793f;
 
 // eps_water_ellison (src/eps_water.f90:85-158, after Maetzler 2006, 5.2.5.4)
-__device__ cplx eps_water_ellison(double s, double T, double f) {
+__device__ __noinline__ cplx eps_water_ellison(double s, double T, double f) {
   const double a1 = 0.46606917e-02f, a2 = -0.26087876e-04f, a3 = -0.63926782e-05f, a4 = 0.63000075e+01f,
                a5 = 0.26242021e-02f, a6 = -0.42984155e-02f, a7 = 0.34414691e-04f, a8 = 0.17667420e-03f,
                a9 = -0.20491560e-06f, a10 = 0.58366888e+03f, a11 = 0.12634992e+03f, a12 = 0.69227972e-04f,
@@ -79,7 +79,7 @@ __device__ cplx eps_water_ellison(double s, double T, double f) {
 }
 
 // eps_water_liebe (src/eps_water.f90:160-207, Liebe, Hufford and Manabe 1991)
-__device__ cplx eps_water_liebe(double T, double f) {
+__device__ __noinline__ cplx eps_water_liebe(double T, double f) {
   const double T_K = T + 273.15f;
   const double theta_1 = 1. - 300. / T_K;
   const double fp = 20.1f * exp(7.88f * theta_1);
@@ -94,7 +94,7 @@ __device__ cplx eps_water_liebe(double T, double f) {
 // eps_water_ray (src/eps_water.f90:209-596, Ray 1972) for wavelengths above
 // 1 mm (f below 299.79 GHz); the tabulated optical constants of shorter
 // wavelengths are not on this path: *bad is set there.
-__device__ cplx eps_water_ray(double T, double f, int* bad) {
+__device__ __noinline__ cplx eps_water_ray(double T, double f, int* bad) {
   const double wl = (double)(1.e6f * 2.99792458e8f) / (f * 1.e9f);  // microns
   if (wl < (double)0.2f || wl > 100000.0 || !(wl > 1000.0)) {
     *bad = 1;
@@ -123,7 +123,7 @@ __device__ cplx eps_water_ray(double T, double f, int* bad) {
 }
 
 // eps_water_stogryn (src/eps_water.f90:598-651, after Maetzler 2006, 5.2.4.2)
-__device__ cplx eps_water_stogryn(double s, double T, double f) {
+__device__ __noinline__ cplx eps_water_stogryn(double s, double T, double f) {
   const double T2 = T * T, T4 = T2 * T2;
   const double p = s * (37.5109f + 5.45216f * s + 0.014409f * (s * s)) / (1004.75f + 182.283f * s + s * s);
   const double alpha_0 = (6.9431f + 3.2841f * s - 0.099486f * (s * s)) / (84.85f + 69.024f * s + s * s);
