@@ -235,7 +235,7 @@ struct Plan {
   size_t total;
   size_t o_hgt_lev, o_temp_lev, o_temp, o_press, o_rho_vap, o_q_hum, o_vap, o_gtemp, o_outlev, o_kgas;
   size_t o_slot_st, o_slot_nb, o_bd, o_bdd, o_bnd, o_brho, o_bmass;
-  size_t o_pres_idx, o_plist, o_counters, o_mkext, o_msalb, o_mback, o_mnleg, o_mlegen, o_lay, o_laynd, o_status,
+  size_t o_pres_idx, o_plist, o_counters, o_mkext, o_msalb, o_mback, o_mrefr, o_mnleg, o_mlegen, o_lay, o_laynd, o_status,
       o_colst;
   size_t o_species, o_addscr;
   int add_grid;  // CTAs of k_adding<32> the scratch is sized for
@@ -293,6 +293,7 @@ Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms) {
   p.o_mkext = take(items * 8);
   p.o_msalb = take(items * 8);
   p.o_mback = take(items * 8);
+  p.o_mrefr = take(items * 4 * 8);
   p.o_mnleg = take(items * 4);
   p.o_mlegen = take(items * 3 * MAXNLEG * 8);
   p.o_lay = take(items * p.lay_stride * 8);
@@ -807,7 +808,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   w.pres_idx = (int*)(A + pl.o_pres_idx); w.plist = (int*)(A + pl.o_plist); w.pmax = pl.pmax;
   w.counters = (int*)(A + pl.o_counters);
   w.m_kext = (double*)(A + pl.o_mkext); w.m_salb = (double*)(A + pl.o_msalb); w.m_nleg = (int*)(A + pl.o_mnleg);
-  w.m_back = (double*)(A + pl.o_mback);
+  w.m_back = (double*)(A + pl.o_mback); w.m_refr = (double*)(A + pl.o_mrefr);
   w.m_legen = (double*)(A + pl.o_mlegen);
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
@@ -865,6 +866,8 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     const int mw = ctx->mie_warps;
     const size_t sm_mie = mw * sizeof(MieSmem);
     int g = persistent_grid((const void*)k_mie, 32 * mw, sm_mie, sms, ctx->mie_cps);
+    const size_t nref = (size_t)std::max(1, pl.pmax) * Fm;
+    k_refr<<<(unsigned)((nref + 127) / 128), 128, 0, stream>>>(b, w, *st); launches++;
     k_mie<<<g, 32 * mw, sm_mie, stream>>>(b, w, *st); launches++;
     if (w.wtab[0] && (mask & 1)) {
       k_scat_weights<8><<<SCAT_NPI * ((2 * 8 * 8 + 127) / 128), 128, 0, stream>>>(ctx->wtab[0], w.wt_need, w.wt_ready, ctx->lob_mu);
@@ -1279,7 +1282,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   w.pres_idx = (int*)(A + pl.o_pres_idx); w.plist = (int*)(A + pl.o_plist); w.pmax = pl.pmax;
   w.counters = (int*)(A + pl.o_counters);
   w.m_kext = (double*)(A + pl.o_mkext); w.m_salb = (double*)(A + pl.o_msalb); w.m_nleg = (int*)(A + pl.o_mnleg);
-  w.m_back = (double*)(A + pl.o_mback);
+  w.m_back = (double*)(A + pl.o_mback); w.m_refr = (double*)(A + pl.o_mrefr);
   w.m_legen = (double*)(A + pl.o_mlegen);
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
@@ -1300,6 +1303,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if (nh > 0) {
     const size_t sm_mie = MIE_WARPS * sizeof(MieSmem);
+    k_refr<<<(unsigned)(((size_t)std::max(1, pl.pmax) * Fm + 127) / 128), 128, 0, stream>>>(b, w, *st);
     k_mie<<<sms, 32 * MIE_WARPS, sm_mie, stream>>>(b, w, *st);
   }
   if (mask & 1) {

@@ -293,6 +293,30 @@ __device__ __forceinline__ void mieangle_group(int nterms, const cplx* ab, const
   }
 }
 
+// Refractive indices of liquid water (nmlSet['liq_mod']) and ice of every
+// (present layer, frequency) item, ahead of k_mie (src/scatProperties.f90:
+// 225-236): one thread per item; NaN marks a water model without a value.
+__global__ void k_refr(Batch b, Work w, pamtra_b200_settings st) {
+  const size_t item = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
+  const int P = min(w.counters[0], w.pmax);
+  if (item >= (size_t)P * Fm) return;
+  const int p = (int)(item / Fm), f = (int)(item % Fm);
+  const int cz = w.plist[p];
+  const int c = cz / Lm, z = cz % Lm;
+  if (f >= b.col_nfreq(c)) return;
+  const double freq = b.freq(c, f);
+  const double T = w.temp[(size_t)c * Lm + z];
+  int bad = 0;
+  const cplx mw = ref_water(T - F(273.15f), freq, st.liq_mod, &bad);
+  const cplx mi = ref_ice(T, freq);
+  double* o = w.m_refr + item * 4;
+  o[0] = bad ? __longlong_as_double(0x7ff8000000000000ll) : mw.re;
+  o[1] = mw.im;
+  o[2] = mi.re;
+  o[3] = mi.im;
+}
+
 // One warp per (present layer, frequency) item; species loop in descriptor
 // order.  src/scatProperties.f90:62-1002 (mie-sphere branch and the species
 // sums :920-949, finalize :993) with src/mie_spheres.f90:14-345 per species.
@@ -336,9 +360,9 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
       const double* bnd = w.b_nd + base;
       const double* brho = w.b_rho + base;
       const double* bmass = w.b_mass + base;
-      int bad_ref = 0;
-      cplx mref = (sp.liq_ice == 1) ? ref_water(T - F(273.15f), freq, st.liq_mod, &bad_ref) : ref_ice(T, freq);
-      if (bad_ref) {
+      const double* mr = w.m_refr + (size_t)item * 4 + (sp.liq_ice == 1 ? 0 : 2);
+      const cplx mref = cmk(mr[0], mr[1]);
+      if (isnan(mref.re)) {
         status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_RANGE;
         break;
       }

@@ -61,6 +61,7 @@ struct Work {
   // single-scattering per item
   double *m_kext, *m_salb;             // [pmax*Fm]
   double* m_back;                      // [pmax*Fm] volumetric backscattering cross section, m^2/m^3
+  double* m_refr;                      // [pmax*Fm][4] refractive index of water (re, im), ice (re, im); NaN: none
   int* m_nleg;                         // [pmax*Fm]
   double* m_legen;                     // [pmax*Fm][3][MAXNLEG]
   // layer R, T, S per item (R,T padded n x (n+2), symmetric +/-)
