@@ -11,6 +11,7 @@ kernels; there is no CPU path.
 
 import calendar
 import datetime
+import os
 import pickle
 import time
 import warnings
@@ -355,3 +356,68 @@ class pyPamtra(object):
         self.r, self.p, self.nmlSet, self.set = d["r"], d["p"], d["nmlSet"], d["set"]
         self.df.data = d["df"]
         self.df.nhydro = len(d["df"])
+
+    def dumpForRT4(self, runFile, path, prefix="sca_"):
+        """Write the input files of Frank Evans' stand-alone RT4 program for
+        profile (0, 0) after a run with ``nmlSet['save_ssp']`` at 16 angles
+        (core.py:2595-2697): ``runFile`` lists, from the top level down, the
+        level height (km), level temperature (K), gas extinction of the layer
+        below (1/km) and the name of that layer's scattering file, which
+        ``path`` receives (``prefix`` + 3-digit layer index) with the phase
+        matrices, extinction matrices and emission vectors in RT4's Lobatto
+        layout, all per km.  As in the reference, the level-0 line takes its
+        scattering file from index -1 (the top layer) and a layer gets a file
+        when any of its hydrometeor mixing ratios is nonzero."""
+        os.makedirs(path, exist_ok=True)
+        N = 16
+        mu = np.cos(np.deg2rad(self.r["angles_deg"][N:]))
+        nlev = self._shape3Dplus[2]
+        ge = np.zeros(nlev)
+        ge[1:nlev] = self.r["kextatmo"] * 1.e3
+        sm = self.r["scatter_matrix"] * 1.e3   # (L, 2, N, 2, N, 4)
+        em = self.r["extinct_matrix"] * 1.e3   # (L, 2, 2, N, 2)
+        ev = self.r["emis_vector"] * 1.e3      # (L, 2, N, 2)
+        e = lambda x: "%.12e" % x
+        m = lambda x: "%.9f" % x
+        zero = e(0.0)
+        zrow = " ".join([zero] * 4) + "\n"
+
+        def row4(a, b):
+            return e(a) + " " + e(b) + " " + zero + " " + zero + "\n"
+
+        lines = []
+        for zz in range(nlev - 1, -1, -1):
+            lay = zz - 1   # the layer below level zz (-1 at the bottom level, as the reference indexes)
+            if np.all(self.p["hydro_q"][0, 0, lay] == 0.):
+                scat_file = " " * 12
+            else:
+                scat_file = prefix + "%03d" % lay + ".txt"
+                out = ["  16   0 'LOBATTO        '\n\n"]
+                # phase matrix blocks: (outgoing sign, incoming sign) -> quadrant
+                for si, quads in ((1.0, ((1.0, 0), (-1.0, 2))), (-1.0, ((1.0, 1), (-1.0, 3)))):
+                    for i in range(N):
+                        for sj, q in quads:
+                            for j in range(N):
+                                out.append(m(si * mu[i]) + "    " + m(sj * mu[j]) + "    0\n")
+                                for k in range(2):
+                                    out.append(row4(sm[lay, k, j, 0, i, q], sm[lay, k, j, 1, i, q]))
+                                out.append(zrow)
+                                out.append(zrow)
+                out.append("\n")
+                for h, sh in ((0, 1.0), (1, -1.0)):
+                    for i in range(N):
+                        out.append(m(sh * mu[i]) + "\n")
+                        for k in range(2):
+                            out.append(row4(em[lay, k, 0, i, h], em[lay, k, 1, i, h]))
+                        out.append(zrow)
+                        out.append(zrow)
+                out.append("\n")
+                for h, sh in ((0, 1.0), (1, -1.0)):
+                    for i in range(N):
+                        out.append(m(sh * mu[i]) + "  " + row4(ev[lay, 0, i, h], ev[lay, 1, i, h]))
+                with open(os.path.join(path, scat_file), "w") as sf:
+                    sf.write("".join(out))
+            lines.append("%3.2f" % (self.p["hgt_lev"][0, 0, zz] / 1.e3) + " " + "%3.2f" % self.p["temp_lev"][0, 0, zz] +
+                         " " + "%3.6f" % ge[zz] + "  '" + scat_file + "'\n")
+        with open(runFile, "w") as f:
+            f.write("".join(lines))
