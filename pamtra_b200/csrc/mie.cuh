@@ -184,6 +184,14 @@ __device__ cplx eps_mix_m(cplx eps1, double mix_de) {
   return cmplx4(em_real, em_imag);  // CMPLX without KIND (eps_mix.f90:44)
 }
 
+// a / b as a conj(b) / |b|^2 (one division); the Mie coefficient
+// denominators stay within a few hundred orders of magnitude of 1, so |b|^2
+// neither overflows nor underflows.
+__device__ __forceinline__ cplx cdiv_rcp(cplx a, cplx b) {
+  const double s = 1.0 / (b.re * b.re + b.im * b.im);
+  return cmk((a.re * b.re + a.im * b.im) * s, (a.im * b.re - a.re * b.im) * s);
+}
+
 __device__ __forceinline__ int mie_nstop(double x) { return (int)(x + 4.0 * pow(x, F(0.3334f)) + 2); }
 
 // src/mie_scat_utilities.f90:8-116 miecalc + miecross for one particle: Mie
@@ -199,7 +207,11 @@ __device__ void miecalc_cross(int nterms, double x, cplx mn, cplx* ab, cplx* bb,
   cplx d = cmk(0.0, 0.0);
   for (int n = nn; n >= 2; n--) {
     cplx ny = cscale(yinv, (double)n);
-    d = csub(ny, cdiv(cmk(1.0, 0.0), cadd(d, ny)));
+    // 1 / z as conj(z) / |z|^2: one division on the recurrence's critical path
+    // instead of Smith's three (|z| stays far from the overflow range here)
+    const cplx z = cadd(d, ny);
+    const double s = 1.0 / (z.re * z.re + z.im * z.im);
+    d = cmk(ny.re - z.re * s, ny.im + z.im * s);
     if (n - 1 <= nterms) ab[n - 2] = d;  // d(n-1) stored at index n-2
   }
   double psim = cos(x), psin = sin(x), chim = -sin(x), chin = cos(x);
@@ -216,10 +228,10 @@ __device__ void miecalc_cross(int nterms, double x, cplx mn, cplx* ab, cplx* bb,
     const cplx dn = ab[n - 1];
     cplx ctmp = cmul(dn, minv);
     ctmp.re = ctmp.re + n / x;
-    cplx an = cdiv(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
+    cplx an = cdiv_rcp(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
     ctmp = cmul(m, dn);
     ctmp.re = ctmp.re + n / x;
-    cplx bn = cdiv(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
+    cplx bn = cdiv_rcp(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
     ab[n - 1] = an;
     bb[n - 1] = bn;
     sum1 = sum1 + (2 * n + 1) * (an.re + bn.re);
@@ -342,7 +354,6 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
     if (f >= b.col_nfreq(c)) continue;
     const double freq = b.freq(c, f);
     const double wl = C_LIGHT / (freq * 1e9);
-    const double T = w.temp[(size_t)c * Lm + z];
     for (int jj = lane; jj < MAXNLEG; jj += 32) { S.legc[0][jj] = 0.0; S.legc[1][jj] = 0.0; S.legc[2][jj] = 0.0; }
     double kexttot = 0.0, salbedo = 0.0, backtot = 0.0;
     int nlegen_coef = 0;
