@@ -454,6 +454,7 @@ def main():
     from pamtra_b200._native import Engine
     from pamtra_b200.workloads import c2_pam
     from pamtra_b200 import autotune
+    from pamtra_b200 import replicas
     pbuild.build()
     eng = Engine(local)
     b = pbatch.pack_pam(c2_pam(args.ncol, seed=2 + rank), FREQS)
@@ -494,10 +495,7 @@ def main():
     clocks = sampler.stop()
     eng.set_timing(False)
     t_total = sum(times) * 1e-3
-    if dist is not None:
-        tt = torch.tensor([t_total], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_total = float(tt.item())
+    t_total = replicas.max_over_ranks(t_total)
     solves_step = b.n_solves()
     value = world * solves_step * args.steps / t_total
     # ---- the same step replayed from a captured CUDA graph
@@ -528,10 +526,7 @@ def main():
         pbatch.run_host(b, local, hout, precision=BF, eng=eng)
         e2e_t.append(time.perf_counter() - t0)
     e2e_total = sum(e2e_t)
-    if dist is not None:
-        tt = torch.tensor([e2e_total], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_total = float(tt.item())
+    e2e_total = replicas.max_over_ranks(e2e_total)
     h2d = sum(v.nbytes for v in b.host.values() if isinstance(v, np.ndarray))
     d2h = sum(v.nbytes for v in hout.values())
     # ---- split-precision batched form (3xTF32 tcgen05 doubling) on the same columns
