@@ -215,22 +215,23 @@ __device__ void miecalc_cross(int nterms, double x, cplx mn, cplx* ab, cplx* bb,
     if (n - 1 <= nterms) ab[n - 2] = d;  // d(n-1) stored at index n-2
   }
   double psim = cos(x), psin = sin(x), chim = -sin(x), chin = cos(x);
+  const double xinv = 1.0 / x;  // (2n-1)/x and n/x as products
   double sum1 = 0.0, sum2 = 0.0;
   cplx sum3 = cmk(0.0, 0.0);
   for (int n = 1; n <= nterms; n++) {
     double tmp = psin;
-    psin = (2 * n - 1) / x * psin - psim;
+    psin = (2 * n - 1) * xinv * psin - psim;
     psim = tmp;
     tmp = chin;
-    chin = (2 * n - 1) / x * chin - chim;
+    chin = (2 * n - 1) * xinv * chin - chim;
     chim = tmp;
     const cplx xin = cmplx4(psin, -chin), xim = cmplx4(psim, -chim);
     const cplx dn = ab[n - 1];
     cplx ctmp = cmul(dn, minv);
-    ctmp.re = ctmp.re + n / x;
+    ctmp.re = ctmp.re + n * xinv;
     cplx an = cdiv_rcp(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
     ctmp = cmul(m, dn);
-    ctmp.re = ctmp.re + n / x;
+    ctmp.re = ctmp.re + n * xinv;
     cplx bn = cdiv_rcp(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
     ab[n - 1] = an;
     bb[n - 1] = bn;
@@ -285,13 +286,16 @@ __device__ __forceinline__ void mieangle_group(int nterms, const cplx* ab, const
     const double dn = (double)n, dn1 = (double)(n + 1), d2n1 = (double)(2 * n + 1);
 #pragma unroll
     for (int g = 0; g < ANG_G; g++) {
-      const double taun = dn * mu[g] * pin[g] - dn1 * pim[g];
+      // tau_n = n mu pi_n - (n+1) pi_{n-1}, pi_{n+1} = ((2n+1) mu pi_n - (n+1) pi_{n-1}) / n
+      // with mu pi_n and (n+1) pi_{n-1} formed once (fused, five operations)
+      const double mp = mu[g] * pin[g], q = dn1 * pim[g];
+      const double taun = fma(dn, mp, -q);
       s1r[g] = fma(c, fma(a.re, pin[g], b.re * taun), s1r[g]);
       s1i[g] = fma(c, fma(a.im, pin[g], b.im * taun), s1i[g]);
       s2r[g] = fma(c, fma(b.re, pin[g], a.re * taun), s2r[g]);
       s2i[g] = fma(c, fma(b.im, pin[g], a.im * taun), s2i[g]);
       const double tmp = pin[g];
-      pin[g] = (d2n1 * mu[g] * pin[g] - dn1 * pim[g]) * rn;
+      pin[g] = fma(d2n1, mp, -q) * rn;
       pim[g] = tmp;
     }
   }
