@@ -301,9 +301,10 @@ __device__ __forceinline__ void mieangle_group(int nterms, const cplx* ab, const
   }
 #pragma unroll
   for (int g = 0; g < ANG_G; g++) {
-    const double as1 = hypot(s1r[g], s1i[g]), as2 = hypot(s2r[g], s2i[g]);
-    p[g][0] = 0.5 * (as2 * as2 + as1 * as1);
-    p[g][1] = 0.5 * (as2 * as2 - as1 * as1);
+    // |S1|^2, |S2|^2 directly (the reference squares abs(), i.e. hypot)
+    const double as1 = s1r[g] * s1r[g] + s1i[g] * s1i[g], as2 = s2r[g] * s2r[g] + s2i[g] * s2i[g];
+    p[g][0] = 0.5 * (as2 + as1);
+    p[g][1] = 0.5 * (as2 - as1);
     p[g][2] = s2r[g] * s1r[g] - (-s2i[g]) * s1i[g];
     p[g][3] = s1r[g] * s2i[g] + (-s1i[g]) * s2r[g];
   }
