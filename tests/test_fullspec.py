@@ -127,3 +127,36 @@ def test_fullspec_gpu_disabled_species(oracle_mod, native):
     pam.runPamtra(freqs)
     assert pam.fortError == 0
     assert np.max(np.abs(pam.r["tb"] - ref["tb"])) < TB_TOL
+
+
+def test_fullspec_packing_and_presence():
+    from pamtra_b200 import libWrapper, packing
+    pam = wl.fullspec_pam(ncol=3, nlay=8, seed=5)
+    cols = packing.profile_columns(pam.p, pam.df.nhydro)
+    packing.fullspec_columns(cols, pam.df.dataFullSpec)
+    assert cols["fs_nbin"] == 40 and cols["fs_d"].shape == (3, 8, 2, 40)
+    assert cols["fs_d_bound"].shape == (3, 8, 2, 41)
+    # presence: layers where any species' spectrum sums above zero, or all with threshold <= 0
+    nsum = pam.df.dataFullSpec["n_ds"].reshape(3, 8, 2, 40).sum(-1)
+    assert libWrapper.present_bound(cols, pam.df.data) == int(np.sum(np.any(nsum > 0, axis=-1)))
+    assert libWrapper.present_bound(cols, pam.df.data, hydro_threshold=0.0) == 3 * 8
+    bad = dict(pam.df.dataFullSpec)
+    del bad["mass_ds"]
+    with pytest.raises(ValueError):
+        packing.fullspec_columns(packing.profile_columns(pam.p, pam.df.nhydro), bad)
+    bad = dict(pam.df.dataFullSpec, d_bound_ds=pam.df.dataFullSpec["d_ds"])
+    with pytest.raises(ValueError):
+        packing.fullspec_columns(packing.profile_columns(pam.p, pam.df.nhydro), bad)
+
+
+def test_oracle_fullspec_psd_outputs(oracle_mod):
+    """With full spectra the bins are not saved (the reference saves them in
+    the moment-based branch only), the per-bin backscatter is."""
+    pam = wl.fullspec_pam(ncol=1, nlay=6, seed=9)
+    pam.nmlSet["save_psd"] = True
+    r, err = oracle_mod.run_pamtra(pam, [89.0])
+    assert err == 0
+    assert np.all(r["psd_d"] == -9999)
+    n = pam.df.dataFullSpec["n_ds"].reshape(r["psd_bscat"].shape)
+    b = r["psd_bscat"]
+    assert np.all(b[n > 0] > 0)
