@@ -246,30 +246,7 @@ __device__ void miecalc_cross(int nterms, double x, cplx mn, cplx* ab, cplx* bb,
   qback = t.re * sum3.re - t.im * (-sum3.im);
 }
 
-// src/mie_scat_utilities.f90:119-160 mieangle
-__device__ __forceinline__ void mieangle(int nterms, const cplx* ab, const cplx* bb, double mu, double p[4]) {
-  cplx s1 = cmk(0.0, 0.0), s2 = cmk(0.0, 0.0);
-  double pin = 1.0, pim = 0.0;
-  for (int n = 1; n <= nterms; n++) {
-    double taun = n * mu * pin - (n + 1) * pim;
-    double c = (double)((float)(2 * n + 1) / (float)(n * (n + 1)));  // REAL(4) division
-    const cplx a = ab[n - 1], b = bb[n - 1];
-    s1.re = fma(c, fma(a.re, pin, b.re * taun), s1.re);
-    s1.im = fma(c, fma(a.im, pin, b.im * taun), s1.im);
-    s2.re = fma(c, fma(b.re, pin, a.re * taun), s2.re);
-    s2.im = fma(c, fma(b.im, pin, a.im * taun), s2.im);
-    double tmp = pin;
-    pin = ((2 * n + 1) * mu * pin - (n + 1) * pim) / n;
-    pim = tmp;
-  }
-  double as1 = hypot(s1.re, s1.im), as2 = hypot(s2.re, s2.im);
-  p[0] = 0.5 * (as2 * as2 + as1 * as1);
-  p[1] = 0.5 * (as2 * as2 - as1 * as1);
-  p[2] = s2.re * s1.re - (-s2.im) * s1.im;
-  p[3] = s1.re * s2.im + (-s1.im) * s2.re;
-}
-
-// mieangle for ANG_G angles of one particle at once: the coefficients a_n,
+// src/mie_scat_utilities.f90:119-160 mieangle for ANG_G angles of one particle at once: the coefficients a_n,
 // b_n are read once per n for all angles, and the pi_n recurrence multiplies
 // by the tabulated 1/n.
 __device__ __forceinline__ void mieangle_group(int nterms, const cplx* ab, const cplx* bb, const double (&mu)[ANG_G],
