@@ -98,6 +98,29 @@ def _warm(_):
     return 0
 
 
+def cpu_model():
+    """Host CPU model name (from /proc/cpuinfo)."""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.lower().startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def cpu_single_core(batch, idxs, freqs):
+    """The oracle on one host core (one worker, no pool) over ``idxs``:
+    solves/s and wall seconds."""
+    st_fields = {k: getattr(batch.settings, k) for k, _ in batch.settings._fields_}
+    cols = {k: (v[idxs] if isinstance(v, np.ndarray) and v.ndim >= 1 and v.shape[0] == batch.ncol else v)
+            for k, v in batch.host.items()}
+    _oracle_chunk((st_fields, batch.species, cols, [0], freqs))  # warm-up: library load
+    out, wall = _oracle_chunk((st_fields, batch.species, cols, list(range(len(idxs))), freqs))
+    return len(idxs) * len(freqs) / wall, wall
+
+
 def cpu_baseline(batch, idxs, freqs, cores, pool):
     """Time the oracle (C++ restatement of the reference) on host cores,
     one single-threaded worker per core (the reference's runParallelPamtra
@@ -494,6 +517,7 @@ def main():
     torch.cuda.synchronize()
     clocks = sampler.stop()
     eng.set_timing(False)
+    layer_products = eng.layer_products(stream)
     t_total = sum(times) * 1e-3
     t_total = replicas.max_over_ranks(t_total)
     solves_step = b.n_solves()
@@ -591,7 +615,14 @@ def main():
                                   "(21,504 items), scaled by the %d items of this launch" % items,
                 "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe); "
                                "MEASURED_PEAKS.json carries bf16 and HBM only",
-                "flops_per_launch": flops, "kernel_ms": t_layer * 1e3}
+                "flops_per_launch": flops, "kernel_ms": t_layer * 1e3,
+                "achieved_executed": 2.0 * 32 ** 3 * layer_products / t_layer / 1e12 if t_layer > 0 else None,
+                "executed_products_per_launch": layer_products,
+                "executed_note": "n x n products the kernel issued (5 per doubling plus the Neumann/Horner "
+                                 "series, Gauss-Jordan counted as one), 2 n^3 FLOP each, n = 32; the algorithmic "
+                                 "figure counts 6 products and one inverse per doubling"}
+    roofline["frac_executed"] = roofline["achieved_executed"] / peak if peak and roofline["achieved_executed"] \
+        else None
     # ---- CPU baseline + TB error vs the oracle on the same columns
     cpu = None
     tb_err = None
@@ -603,13 +634,18 @@ def main():
         pool = make_pool(cores)
         cval, wall, tbs = cpu_baseline(b, idxs, FREQS, cores, pool)
         pool.close()
+        one_val, one_wall = cpu_single_core(b, idxs[:max(2, nsamp // (2 * cores))], FREQS)
         tb_gpu = out["tb"].cpu().numpy()
         tb_err = max(float(np.max(np.abs(tb_gpu[c] - tbs[c]))) for c in idxs)
         split_err_oracle = max(float(np.max(np.abs(tb_split[c] - tbs[c]))) for c in idxs)
         cpu = {"value": cval, "unit": "solves/s", "cores": cores, "kind": "port",
                "sample": "%d random columns x %d frequencies of the same workload, one worker process per core; "
                          "C++ FP64 restatement of the reference Fortran (no Fortran compiler on this image)"
-                         % (nsamp, len(FREQS))}
+                         % (nsamp, len(FREQS)),
+               "single_core": {"value": one_val, "unit": "solves/s", "cores": 1,
+                               "sample": "%d of those columns x %d frequencies in one process"
+                                         % (max(2, nsamp // (2 * cores)), len(FREQS)), "wall_s": one_wall},
+               "cpu_model": cpu_model(), "wall_s": wall}
     line = {
         "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_total / args.steps, "higher_is_better": True,
@@ -642,6 +678,9 @@ def main():
                                  "thin-layer init, adding and surface in FP64"},
         "stage_ms": {k: v / args.steps for k, v in stage_tot.items()},
         "target_shape": target,
+        "target_batched_fp64_over_plain": target["batched_over_plain"] if target else None,
+        "target_batched_3xtf32_over_plain": target["batched_3xtf32_over_plain"] if target else None,
+        "c2_3xtf32_over_fp64": split_value / value if value else None,
         "uneven": uneven,
         "mie_heavy": mieheavy,
         "serving": serving,

@@ -128,7 +128,9 @@ typedef struct pamtra_b200_columns {
   int32_t nummu_mask;         /* bit 0: N=8, bit 1: N=16, bit 2: N=32 present; 0 = settings.nummu only */
   const pamtra_b200_species* species;  /* HOST pointer, [ncol or 1][nhydro] (copied by the library) */
   const int32_t* nlyrs;       /* [ncol] */
-  const int32_t* nummu;       /* [ncol] in {8,16,32}; NULL = settings.nummu */
+  const int32_t* nummu;       /* [ncol] in {8,16,32}; NULL = settings.nummu.  A column whose value is
+                                 not 8/16/32, not in nummu_mask or above max_nummu is solved by no
+                                 kernel and gets PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE in status */
   const int32_t* nfreq;       /* [ncol]; NULL = max_nfreq for all */
   const double* freqs;        /* [ncol][max_nfreq] GHz, or [max_nfreq] if nfreq == NULL */
   const double *hgt_lev, *temp_lev, *press_lev, *relhum_lev;   /* [ncol][max_nlyrs+1] */
@@ -231,6 +233,25 @@ int32_t pamtra_b200_graph_capture(pamtra_b200_ctx* ctx, const pamtra_b200_settin
 int32_t pamtra_b200_graph_launch(pamtra_b200_graph* graph, void* stream);
 int32_t pamtra_b200_graph_destroy(pamtra_b200_graph* graph);
 
+/* Bound on each wait for a tensor-core MMA of the split-precision kernels
+ * (no counterpart in the reference, whose Fortran has no device waits).
+ * A wait that polls the MMA's completion barrier `polls` times without
+ * success gives up: the items that CTA holds or takes afterwards get
+ * PAMTRA_B200_FATAL | PAMTRA_B200_ST_TIMEOUT in outputs->status and are not
+ * computed, and the CTA lets its last MMA finish before it frees its tensor
+ * memory, so the context stays usable.  The default is
+ * PAMTRA_B200_WAIT_LIMIT_DEFAULT polls, far above any MMA's latency; 0 makes
+ * every wait give up at once (to exercise that path). */
+#define PAMTRA_B200_WAIT_LIMIT_DEFAULT (1u << 24)
+int32_t pamtra_b200_set_wait_limit(pamtra_b200_ctx* ctx, uint32_t polls);
+
+/* n x n matrix products the FP64 doubling kernels (k_layer<N>) of the last
+ * pamtra_b200_run on ctx issued, inverses by Gauss-Jordan counted as one:
+ * the executed counterpart of the algorithmic count of DOUBLING_INTEGRATION4
+ * (src/radintg4.f90:174-309: six products and one inverse per doubling).
+ * The split-precision kernels are not counted.  Waits for `stream`. */
+int32_t pamtra_b200_layer_products(pamtra_b200_ctx* ctx, uint64_t* out, void* stream);
+
 /* Number of kernel launches the last pamtra_b200_run issued on ctx. */
 int32_t pamtra_b200_last_launch_count(const pamtra_b200_ctx* ctx);
 
@@ -296,10 +317,16 @@ int32_t pamtra_b200_mmult_3xtf32_batched(const double* a, const double* b, doubl
  * max_nfreq <= 4, nhydro <= 4, nbin <= 64 per species, nummu 8 or 16,
  * noutlevels <= 2, no full spectra (fs_d NULL) and no save_psd outputs
  * (psd_d NULL); other requests return
- * PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE without running.  The first call on a device (with
- * that device current) resolves the array's device address with
- * cudaGetSymbolAddress and fills the quadrature and line tables; make that
- * first call before any stream capture.  Every call shares the one array and
+ * PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE without running, and so does a
+ * quadrature (settings.nummu or nummu_mask) wider than max_nummu.  The first
+ * call on a device (with that device current) is the set-up: CUDA loads this
+ * library's device code and its static arrays on that device at first use
+ * (lazy module loading, the default), which takes device memory for the
+ * module and synchronises; the call then resolves the array's device address
+ * with cudaGetSymbolAddress, fills the quadrature and line tables and
+ * synchronises the stream.  Make that first call once per device outside any
+ * no-allocation or latency-critical region, and before any stream capture;
+ * later calls allocate nothing and do not synchronise.  Every call shares the one array and
  * clears what must start at zero, so calls that overlap on the GPU (other
  * streams, other host threads) race: serialise them. */
 #define PAMTRA_B200_NOALLOC_SCRATCH_MIB 8

@@ -28,6 +28,7 @@ ST_NAN = 0x2000
 ST_SIZE = 0x4000
 ST_TIMEOUT = 0x8000
 ST_RANGE = 0x10000
+WAIT_LIMIT_DEFAULT = 1 << 24  # PAMTRA_B200_WAIT_LIMIT_DEFAULT
 
 _vp = ctypes.c_void_p
 _i32 = ctypes.c_int32
@@ -59,7 +60,8 @@ EXPORTS = ["pamtra_b200_create", "pamtra_b200_destroy", "pamtra_b200_workspace_b
            "pamtra_b200_stage_ms", "pamtra_b200_abi_sizes", "pamtra_b200_run_noalloc",
            "pamtra_b200_mmult_3xtf32_batched", "pamtra_b200_set_launch", "pamtra_b200_get_launch",
            "pamtra_b200_graph_capture", "pamtra_b200_graph_launch", "pamtra_b200_graph_destroy",
-           "pamtra_b200_get_eps_water", "pamtra_b200_gas_l93"]
+           "pamtra_b200_get_eps_water", "pamtra_b200_gas_l93", "pamtra_b200_set_wait_limit",
+           "pamtra_b200_layer_products"]
 NLAUNCH = 4  # PAMTRA_B200_NLAUNCH: mie warps per CTA, mie / layer / adding CTAs per SM
 STAGES = ["prep", "psd", "mie", "layer", "adding"]
 
@@ -116,6 +118,10 @@ def load():
         l.pamtra_b200_graph_launch.argtypes = [_vp, _vp]
         l.pamtra_b200_graph_destroy.restype = _i32
         l.pamtra_b200_graph_destroy.argtypes = [_vp]
+        l.pamtra_b200_set_wait_limit.restype = _i32
+        l.pamtra_b200_set_wait_limit.argtypes = [_vp, ctypes.c_uint32]
+        l.pamtra_b200_layer_products.restype = _i32
+        l.pamtra_b200_layer_products.argtypes = [_vp, ctypes.POINTER(ctypes.c_uint64), _vp]
         l.pamtra_b200_abi_sizes.restype = _i32
         l.pamtra_b200_abi_sizes.argtypes = [ctypes.POINTER(ctypes.c_size_t), _i32]
         _lib = l
@@ -235,6 +241,20 @@ class Engine(object):
 
     def last_launch_count(self):
         return int(self.lib.pamtra_b200_last_launch_count(self.handle))
+
+    def set_wait_limit(self, polls=WAIT_LIMIT_DEFAULT):
+        """Polls of each wait on a tensor-core MMA before it gives up
+        (status ST_TIMEOUT); 0 gives up at once."""
+        if self.lib.pamtra_b200_set_wait_limit(self.handle, int(polls)) != 0:
+            raise RuntimeError("pamtra_b200_set_wait_limit failed")
+
+    def layer_products(self, stream=None):
+        """n x n products the FP64 doubling kernels of the last run issued."""
+        v = ctypes.c_uint64(0)
+        s = None if stream is None else stream.cuda_stream
+        if self.lib.pamtra_b200_layer_products(self.handle, ctypes.byref(v), s) != 0:
+            raise RuntimeError("pamtra_b200_layer_products failed")
+        return int(v.value)
 
     def set_timing(self, on):
         self.lib.pamtra_b200_set_timing(self.handle, int(bool(on)))

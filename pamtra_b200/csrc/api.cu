@@ -452,6 +452,8 @@ struct pamtra_b200_ctx {
   int mie_cps = 0;            // k_mie CTAs per SM
   int layer_cps = 0;          // k_layer / k_layer_tc CTAs per SM
   int adding_cps = 0;         // k_adding CTAs per SM
+  uint32_t spin_limit = tc::MBAR_SPIN_LIMIT;  // polls per wait on a tensor-core MMA
+  const int* last_counters = nullptr;          // work counters of the last run (in the arena)
   // optional per-stage timing (events recorded on the run's stream)
   int timing = 0;
   cudaEvent_t ev[16] = {};
@@ -699,6 +701,28 @@ int32_t pamtra_b200_get_launch(const pamtra_b200_ctx* ctx, int32_t* params, int3
   return PAMTRA_B200_OK;
 }
 
+int32_t pamtra_b200_layer_products(pamtra_b200_ctx* ctx, uint64_t* out, void* stream) {
+  if (!ctx || !out) return PAMTRA_B200_FATAL;
+  *out = 0;
+  if (!ctx->last_counters || ctx->last_counters < (const int*)ctx->arena ||
+      ctx->last_counters >= (const int*)(ctx->arena + ctx->arena_bytes))
+    return PAMTRA_B200_FATAL;
+  cudaSetDevice(ctx->device);
+  unsigned long long v = 0;
+  if (cudaMemcpyAsync(&v, ctx->last_counters + COUNTER_PRODUCTS, sizeof(v), cudaMemcpyDeviceToHost,
+                      (cudaStream_t)stream) != cudaSuccess ||
+      cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess)
+    return PAMTRA_B200_FATAL;
+  *out = v;
+  return PAMTRA_B200_OK;
+}
+
+int32_t pamtra_b200_set_wait_limit(pamtra_b200_ctx* ctx, uint32_t polls) {
+  if (!ctx) return PAMTRA_B200_FATAL;
+  ctx->spin_limit = polls;
+  return PAMTRA_B200_OK;
+}
+
 int32_t pamtra_b200_set_timing(pamtra_b200_ctx* ctx, int32_t enable) {
   if (!ctx) return PAMTRA_B200_FATAL;
   ctx->timing = enable ? 1 : 0;
@@ -787,6 +811,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   b.ncol = cc.ncol; b.max_nlyrs = cc.max_nlyrs; b.nhydro = cc.nhydro; b.max_nfreq = cc.max_nfreq;
   b.noutlevels = cc.noutlevels; b.max_nummu = cc.max_nummu; b.max_nbin = pl.max_nbin;
   b.species_stride = cc.species_stride; b.default_nummu = st->nummu; b.species = d_species;
+  b.nummu_mask = mask;
   b.nlyrs = cc.nlyrs; b.nummu = cc.nummu; b.nfreq = cc.nfreq; b.freqs = cc.freqs; b.freq_per_col = cc.nfreq != nullptr;
   b.hgt_lev = cc.hgt_lev; b.temp_lev = cc.temp_lev; b.press_lev = cc.press_lev; b.relhum_lev = cc.relhum_lev;
   b.hgt = cc.hgt; b.temp = cc.temp; b.press = cc.press; b.relhum = cc.relhum;
@@ -813,6 +838,8 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
   w.add_scr = (double*)(A + pl.o_addscr);
+  w.spin_limit = ctx->spin_limit;
+  ctx->last_counters = w.counters;
   // scatcnv weight tables (context-resident; a table that cannot be allocated
   // leaves the direct azimuth sums in place)
   if (cc.nhydro > 0) {
@@ -1257,15 +1284,18 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   const int nh = cc.nhydro;
   cc.nhydro = nh > 0 ? nh : 0;
   Plan pl = make_plan(&cc, st->nummu, 0);
-  if (pl.total > NOALLOC_SCRATCH_BYTES || pl.maxN > 16) return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
+  // the widest quadrature launched must fit the caller's output rows (2 * max_nummu angles)
+  if (pl.total > NOALLOC_SCRATCH_BYTES || pl.maxN > 16 || pl.maxN > cc.max_nummu)
+    return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
   const int mask = cc.nummu_mask ? cc.nummu_mask : (st->nummu == 8 ? 1 : 2);
-  if (mask & 4) return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
+  if (mask & ~3) return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
   char* A = D.scratch;
   const size_t gqn = (size_t)NOALLOC_GQ * (NOALLOC_GQ + 1) / 2;
   Batch b{};
   b.ncol = 1; b.max_nlyrs = cc.max_nlyrs; b.nhydro = nh; b.max_nfreq = cc.max_nfreq;
   b.noutlevels = cc.noutlevels; b.max_nummu = cc.max_nummu; b.max_nbin = pl.max_nbin;
   b.species_stride = 0; b.default_nummu = st->nummu; b.species = cols->species;  // device pointer here
+  b.nummu_mask = mask;
   b.nlyrs = cc.nlyrs; b.nummu = cc.nummu; b.nfreq = cc.nfreq; b.freqs = cc.freqs; b.freq_per_col = cc.nfreq != nullptr;
   b.hgt_lev = cc.hgt_lev; b.temp_lev = cc.temp_lev; b.press_lev = cc.press_lev; b.relhum_lev = cc.relhum_lev;
   b.hgt = cc.hgt; b.temp = cc.temp; b.press = cc.press; b.relhum = cc.relhum;
@@ -1286,6 +1316,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   w.m_legen = (double*)(A + pl.o_mlegen);
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
+  w.spin_limit = tc::MBAR_SPIN_LIMIT;
   w.gq_x = D.tables; w.gq_w = D.tables + gqn; w.gq_max = NOALLOC_GQ;
   w.lob_mu = D.tables + 2 * gqn; w.lob_w = D.tables + 2 * gqn + 56;
   const size_t Lm = cc.max_nlyrs, Fm = cc.max_nfreq;

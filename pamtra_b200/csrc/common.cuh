@@ -283,9 +283,10 @@ __device__ int ginv(double* A, InvScratch<n>& S) {
 // (Horner wins for the thin layers of the first doublings, where ||X|| is
 // tiny and G = I + X needs no product at all); otherwise Gauss-Jordan with
 // partial pivoting.  Returns the buffer holding the inverse (P or G); *sing
-// set on a zero pivot.
+// set on a zero pivot; *nprod (if given) grows by the n x n products the
+// inverse took (Gauss-Jordan counted as one: n^3 multiply-adds).
 template <int n>
-__device__ double* inv_iminus(double* P, double* G, InvScratch<n>& S, int* sing) {
+__device__ double* inv_iminus(double* P, double* G, InvScratch<n>& S, int* sing, int* nprod = nullptr) {
   constexpr int LD = Team<n>::LD, T = Team<n>::T;
   const int t = threadIdx.x;
   // infinity norm of X
@@ -324,6 +325,7 @@ __device__ double* inv_iminus(double* P, double* G, InvScratch<n>& S, int* sing)
       mm<n, MM_IPLUS, true>(P, G, G);  // G = I + X G
       team_sync();
     }
+    if (nprod) *nprod += kh;
     return G;
   }
   if (m >= 8) {
@@ -334,6 +336,7 @@ __device__ double* inv_iminus(double* P, double* G, InvScratch<n>& S, int* sing)
     }
     team_sync();
     if (ginv<n>(P, S)) *sing = 1;
+    if (nprod) *nprod += 1;
     return P;
   }
   // G = I + X
@@ -348,6 +351,7 @@ __device__ double* inv_iminus(double* P, double* G, InvScratch<n>& S, int* sing)
     mm<n, MM_ACC, true>(G, P, G, G);  // G = G + G P
     team_sync();
   }
+  if (nprod) *nprod += 2 * (m - 1);
   return G;
 }
 

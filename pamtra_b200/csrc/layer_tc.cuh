@@ -167,6 +167,19 @@ __device__ __forceinline__ int series_steps(float nrm) {
   return s;
 }
 
+// An item a CTA takes after one of its waits on the tensor core gave up: its
+// (column, frequency) gets PAMTRA_B200_ST_TIMEOUT and no layer is computed.
+template <int N>
+__device__ __forceinline__ void mark_timed_out(const Batch& b, const Work& w, int item) {
+  const int Fm = b.max_nfreq, Lm = b.max_nlyrs;
+  const int p = item / Fm, fi = item % Fm;
+  const int c = w.plist[p] / Lm;
+  if (fi < b.col_nfreq(c) && b.col_nummu(c) == N) {
+    w.lay_nd[item] = 0;
+    atomicOr(&w.status[(size_t)c * Fm + fi], PAMTRA_B200_FATAL | PAMTRA_B200_ST_TIMEOUT);
+  }
+}
+
 template <int N>
 __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b200_settings st,
                                                      double* __restrict__ ssp_scat) {
@@ -207,7 +220,11 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
     if (t == 0) s_base = atomicAdd(&w.counters[3], 2);
     __syncthreads();
     const int base = s_base;
-    if (base >= nitems || s_dead) break;
+    if (base >= nitems) break;
+    if (s_dead) {  // after a timed-out wait: report the remaining items, compute nothing
+      if (t < 2 && base + t < nitems) mark_timed_out<N>(b, w, base + t);
+      continue;
+    }
     // ---- FP64 set-up of both items (one at a time through the shared scratch)
     for (int i = 0; i < 2; i++) {
       const int item = base + i;
@@ -288,7 +305,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
           matvec2(mv, x[2 * slot], x[2 * slot + 1], lane, m0, m1);
         }
         {
-          const bool mine = tc::mbar_wait(&mbar, parity);
+          const bool mine = tc::mbar_wait(&mbar, parity, w.spin_limit);
           parity ^= 1;
           ok = __syncthreads_and(mine) != 0;  // one verdict for the whole CTA
           tc::fence_after_sync();
@@ -458,6 +475,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
     }
   }
   // a timed-out CTA lets its last MMA finish before the memory is released
+  // (with the default limit, whatever limit the run's waits had)
   if (s_dead) tc::mbar_wait(&mbar, parity ^ 1);
   tc::fence_before_sync();
   __syncthreads();

@@ -171,10 +171,15 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
   for (;;) {
     __syncthreads();
     if (t == 0) s_item = atomicAdd(&w.counters[4], 1);
-    if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
     __syncthreads();
     const int item = s_item;
-    if (item >= nitems || s_dead) break;
+    if (item >= nitems) break;
+    if (s_dead) {  // after a timed-out wait: report the remaining items, compute nothing
+      if (t == 0) mark_timed_out<N>(b, w, item);
+      continue;
+    }
+    if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
+    __syncthreads();
     LayerItem it;
     if (!layer_setup<N, Tc64Setup, 128>(b, w, st, ssp_scat, S, item, it)) continue;
     const int nd = it.nd;
@@ -239,7 +244,7 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
           matvec2_64(mv, x[2 * slot], x[2 * slot + 1], col, m0, m1);
         }
         {
-          const bool mine = tc::mbar_wait(&mbar, parity);
+          const bool mine = tc::mbar_wait(&mbar, parity, w.spin_limit);
           parity ^= 1;
           ok = __syncthreads_and(mine) != 0;
           tc::fence_after_sync();
@@ -410,6 +415,7 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
     }
   }
   // a timed-out CTA lets its last MMA finish before the memory is released
+  // (with the default limit, whatever limit the run's waits had)
   if (s_dead) tc::mbar_wait(&mbar, parity ^ 1);
   tc::fence_before_sync();
   __syncthreads();

@@ -37,9 +37,17 @@ __global__ void k_atmo(Batch b, Work w) {
   double* p = w.press + (size_t)c * Lm;
   double* rv = w.rho_vap + (size_t)c * Lm;
   double* qh = w.q_hum + (size_t)c * Lm;
-  if (L < 2 || L > Lm) {
+  // A column whose quadrature is not 8, 16 or 32, not among the launched
+  // ones, or wider than the output rows is solved by no kernel: report it
+  // on every frequency of the column instead of leaving -9999 silently.
+  const int nm = b.col_nummu(c);
+  const int nbit = (nm == 8) ? 1 : (nm == 16) ? 2 : (nm == 32) ? 4 : 0;
+  const bool bad_l = L < 2 || L > Lm;
+  if (bad_l || !(nbit & b.nummu_mask) || nm > b.max_nummu) {
     w.col_status[c] |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
-    return;
+    const int nf = min(b.col_nfreq(c), b.max_nfreq);
+    for (int f = 0; f < nf; f++) w.status[(size_t)c * b.max_nfreq + f] |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
+    if (bad_l) return;
   }
   // layer heights first (only needs levels), then the level variables
   // Use local copies: h, r, plev (the level pressure and humidity are only

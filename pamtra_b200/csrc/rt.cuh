@@ -404,6 +404,7 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
     // per step: W = T G, then R' = R + W (R T) and T' = W T; the source
     // chains use W u for T G u.
     constexpr int NV = (4 * n + T - 1) / T;
+    int nprod = 5 * nd;  // n x n products issued for this item (counted by thread 0)
     for (int itd = 0; itd < nd; itd++) {
       mm<n, MM_SET>(Rb, Rb, Gb);  // R+ R-
       // v = [S- + f C-, C-, S+, C+]
@@ -419,7 +420,7 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
       team_sync();
       {
         int sg = 0;
-        double* gi = inv_iminus<n>(Gb, Wb, S.inv, &sg);  // GAMMA = inv(I - R+ R-)
+        double* gi = inv_iminus<n>(Gb, Wb, S.inv, &sg, &nprod);  // GAMMA = inv(I - R+ R-)
         if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
         if (gi != Gb) { Wb = Gb; Gb = gi; }
       }
@@ -474,6 +475,8 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
     if (t == 0) {
       w.lay_nd[item] = nd;
       if (status) atomicOr(&w.status[(size_t)c * Fm + fi], status);
+      if (nprod) atomicAdd(reinterpret_cast<unsigned long long*>(w.counters + COUNTER_PRODUCTS),
+                           (unsigned long long)nprod);
     }
   }
 }

@@ -133,10 +133,11 @@ __device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
   asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
-// Wait for phase `parity` of `mbar` to complete; false after the spin limit.
-__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
+// Wait for phase `parity` of `mbar` to complete; false after `limit` polls
+// (a limit of 0 gives up without polling).
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity, uint32_t limit = MBAR_SPIN_LIMIT) {
   const uint32_t a = smem_u32(mbar);
-  for (uint32_t i = 0; i < MBAR_SPIN_LIMIT; i++) {
+  for (uint32_t i = 0; i < limit; i++) {
     uint32_t done;
     asm volatile(
         "{\n\t"

@@ -9,6 +9,7 @@ namespace pb {
 struct Batch {
   int ncol, max_nlyrs, nhydro, max_nfreq, noutlevels, max_nummu, max_nbin, species_stride;
   int default_nummu;
+  int nummu_mask;  // quadratures launched: bit 0 N = 8, bit 1 N = 16, bit 2 N = 32
   const pamtra_b200_species* species;
   const int* nlyrs;
   const int* nummu;
@@ -57,7 +58,8 @@ struct Work {
   int* pres_idx;                       // [C][Lm]
   int* plist;                          // [pmax]
   int pmax;
-  int* counters;                       // [16] 0: P, 1: mie work, 2: rt work, 3: adding work
+  int* counters;                       // [16] 0: P, 1: mie work, 2-4: layer work, 5-7: adding work,
+                                       // 8-9: n x n products of the FP64 layer kernel (uint64)
   // single-scattering per item
   double *m_kext, *m_salb;             // [pmax*Fm]
   double* m_back;                      // [pmax*Fm] volumetric backscattering cross section, m^2/m^3
@@ -74,6 +76,8 @@ struct Work {
   const double* wtab[3];               // [numpts index][l][5][2 N^2], see scat_weight_offset
   int* wt_need;                        // [3][SCAT_NPI] numpts values seen (set by k_mie)
   int* wt_ready;                       // [3][SCAT_NPI] tables already computed
+  // polls of each wait on a tensor-core MMA before it gives up (PAMTRA_B200_ST_TIMEOUT)
+  uint32_t spin_limit;
   // status
   int* status;                         // [C][Fm]
   int* col_status;                     // [C]
@@ -84,6 +88,8 @@ struct Work {
   const double* lob_mu;                // Lobatto nodes for N = 8,16,32 at offsets 0, 8, 24
   const double* lob_w;
 };
+
+constexpr int COUNTER_PRODUCTS = 8;  // counters[8..9]: 8-byte aligned (the arena slice is 256-aligned)
 
 __host__ __device__ __forceinline__ int lob_off(int N) { return N == 8 ? 0 : (N == 16 ? 8 : 24); }
 __host__ __device__ __forceinline__ int nmu_index(int N) { return N == 8 ? 0 : (N == 16 ? 1 : 2); }
