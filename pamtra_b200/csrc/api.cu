@@ -237,7 +237,8 @@ struct Plan {
   size_t o_slot_st, o_slot_nb, o_bd, o_bdd, o_bnd, o_brho, o_bmass;
   size_t o_pres_idx, o_plist, o_counters, o_mkext, o_msalb, o_mback, o_mrefr, o_mnleg, o_mlegen, o_lay, o_laynd, o_status,
       o_colst;
-  size_t o_species, o_addscr;
+  size_t o_species, o_addscr, o_mieslab;
+  int mie_nslab;  // k_mie warps the slabs are sized for
   int add_grid;  // CTAs of k_adding<32> the scratch is sized for
   int pmax;
   int max_nbin;
@@ -249,7 +250,7 @@ size_t lay_stride_for(int N) {
   return (lay_stride_n(N) + 1) & ~(size_t)1;  // keep 16-byte alignment of each item
 }
 
-Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms) {
+Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms, int mie_slabs) {
   Plan p{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -303,6 +304,9 @@ Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms) {
   p.o_species = take(std::max<size_t>(nsp, 1) * sizeof(pamtra_b200_species));
   p.add_grid = (mask & 4) ? std::max(1, sms) : 0;
   p.o_addscr = take((size_t)p.add_grid * (10 - AddSmem<32>::NS) * RTCfg<32>::MAT * 8);
+  // one slab per k_mie warp; more warps than (layer, frequency) items would idle
+  p.mie_nslab = c->nhydro > 0 ? (int)std::min<size_t>((size_t)mie_slabs, items) : 0;
+  p.o_mieslab = take((size_t)p.mie_nslab * MIE_SLAB * 8);
   p.total = take(0) + 256;
   return p;
 }
@@ -474,13 +478,12 @@ static void mark(pamtra_b200_ctx* ctx, cudaStream_t s, int stage) {
 // c_n of mieangle in REAL(4) arithmetic (host float division is IEEE, as on
 // the device) and 1/n
 static int upload_mie_constants() {
-  double c[NT_MAX + 1], r[NT_MAX + 1];
+  static_assert(MAXNLEG > NT_MAX, "1/n table covers the Mie terms");
+  double c[NT_MAX + 1], r[MAXNLEG];
   c[0] = 0.0;
   r[0] = 0.0;
-  for (int n = 1; n <= NT_MAX; n++) {
-    c[n] = (double)((float)(2 * n + 1) / (float)(n * (n + 1)));
-    r[n] = 1.0 / n;
-  }
+  for (int n = 1; n <= NT_MAX; n++) c[n] = (double)((float)(2 * n + 1) / (float)(n * (n + 1)));
+  for (int n = 1; n < MAXNLEG; n++) r[n] = 1.0 / n;
   return (cudaMemcpyToSymbol(c_mie_c, c, sizeof(c)) != cudaSuccess ||
           cudaMemcpyToSymbol(c_mie_inv, r, sizeof(r)) != cudaSuccess) ? 1 : 0;
 }
@@ -585,7 +588,7 @@ size_t pamtra_b200_workspace_bytes(const pamtra_b200_columns* cols, int32_t prec
   if (!cols || !cols->species) return 0;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return make_plan(cols, 16, sms).total;
+  return make_plan(cols, 16, sms, sms * MIE_SLAB_WARPS_PER_SM).total;
 }
 
 int32_t pamtra_b200_reserve(pamtra_b200_ctx* ctx, size_t bytes) {
@@ -767,7 +770,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   pamtra_b200_species dummy{};
   pamtra_b200_columns cc = *cols;
   if (cc.nhydro == 0) { cc.species = &dummy; cc.species_stride = 0; }
-  Plan pl = make_plan(&cc, st->nummu, ctx->sm_count);
+  Plan pl = make_plan(&cc, st->nummu, ctx->sm_count, ctx->sm_count * MIE_SLAB_WARPS_PER_SM);
   if (pl.max_nbin > MAXBIN) return PAMTRA_B200_FATAL;
   if (pl.total > ctx->arena_bytes) {
     cudaStreamSynchronize(stream);
@@ -838,6 +841,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
   w.add_scr = (double*)(A + pl.o_addscr);
+  w.mie_slab = (double*)(A + pl.o_mieslab); w.mie_nslab = pl.mie_nslab;
   w.spin_limit = ctx->spin_limit;
   ctx->last_counters = w.counters;
   // scatcnv weight tables (context-resident; a table that cannot be allocated
@@ -892,7 +896,8 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   if (H > 0) {
     const int mw = ctx->mie_warps;
     const size_t sm_mie = mw * sizeof(MieSmem);
-    int g = persistent_grid((const void*)k_mie, 32 * mw, sm_mie, sms, ctx->mie_cps);
+    int g = std::min(persistent_grid((const void*)k_mie, 32 * mw, sm_mie, sms, ctx->mie_cps),
+                     std::max(1, pl.mie_nslab / mw));
     const size_t nref = (size_t)std::max(1, pl.pmax) * Fm;
     k_refr<<<(unsigned)((nref + 127) / 128), 128, 0, stream>>>(b, w, *st); launches++;
     k_mie<<<g, 32 * mw, sm_mie, stream>>>(b, w, *st); launches++;
@@ -1206,6 +1211,8 @@ constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)PAMTRA_B200_NOALLOC_SCRATCH_MIB
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
 // quadrature tables of the allocation-free path (filled at per-device set-up)
 constexpr int NOALLOC_GQ = 256;
+// k_mie warps of the allocation-free path (each takes a coefficient slab of the scratch)
+constexpr int NOALLOC_MIE_SLABS = 16;
 static __device__ __align__(256) double g_noalloc_tables[2 * (NOALLOC_GQ * (NOALLOC_GQ + 1) / 2) + 2 * 56];
 
 namespace {
@@ -1283,7 +1290,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   cc.species_stride = 0;
   const int nh = cc.nhydro;
   cc.nhydro = nh > 0 ? nh : 0;
-  Plan pl = make_plan(&cc, st->nummu, 0);
+  Plan pl = make_plan(&cc, st->nummu, 0, NOALLOC_MIE_SLABS);
   // the widest quadrature launched must fit the caller's output rows (2 * max_nummu angles)
   if (pl.total > NOALLOC_SCRATCH_BYTES || pl.maxN > 16 || pl.maxN > cc.max_nummu)
     return PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;
@@ -1317,6 +1324,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
   w.spin_limit = tc::MBAR_SPIN_LIMIT;
+  w.mie_slab = (double*)(A + pl.o_mieslab); w.mie_nslab = pl.mie_nslab;
   w.gq_x = D.tables; w.gq_w = D.tables + gqn; w.gq_max = NOALLOC_GQ;
   w.lob_mu = D.tables + 2 * gqn; w.lob_w = D.tables + 2 * gqn + 56;
   const size_t Lm = cc.max_nlyrs, Fm = cc.max_nfreq;
@@ -1335,7 +1343,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   if (nh > 0) {
     const size_t sm_mie = MIE_WARPS * sizeof(MieSmem);
     k_refr<<<(unsigned)(((size_t)std::max(1, pl.pmax) * Fm + 127) / 128), 128, 0, stream>>>(b, w, *st);
-    k_mie<<<sms, 32 * MIE_WARPS, sm_mie, stream>>>(b, w, *st);
+    k_mie<<<NOALLOC_MIE_SLABS / MIE_WARPS, 32 * MIE_WARPS, sm_mie, stream>>>(b, w, *st);
   }
   if (mask & 1) {
     if (nh > 0) k_layer<8><<<sms, RTCfg<8>::T, sizeof(LayerSmem<8>), stream>>>(b, w, *st, out->scatter_matrix);

@@ -7,23 +7,35 @@
 
 namespace pb {
 
+#ifndef MIE_MAXNREG
+#define MIE_MAXNREG 128  // registers per k_mie thread: four 4-warp CTAs per SM
+#endif
 constexpr int MIE_WARPS = 4;      // default warps per CTA
 constexpr int MIE_MAX_WARPS = 8;  // largest launch shape (pamtra_b200_set_launch)
 constexpr int NQ_MAX = 256;   // Gauss points per series (nquad)
 constexpr int NT_MAX = 128;   // Mie terms per bin
-constexpr int ANG_G = 2;      // angles per pass over a bin's Mie coefficients
 
+// Shared memory of one warp of k_mie: the phase-function sums of the
+// current species per quadrature point (P11, P12, P33), the weights of the
+// bins of the current pass and the staging of one round of work items.
 struct MieSmem {
-  double sump[4][NQ_MAX];
-  double legh[3][MAXNLEG];
-  double legc[3][MAXNLEG];
+  double sump[3][NQ_MAX];
+  double stg[3][32];
+  double bw[32], bd[32];
+  int bn[32], sti[32];
 };
+// Coefficient slab of one warp in global scratch: up to 32 bins x kmax rows
+// of (a_n, b_n); 4096 doubles hold 32 bins up to 32 terms (size parameters
+// up to about 20), fewer bins per pass beyond that (8 at the 127-term limit).
+constexpr int MIE_SLAB = 4096;
+constexpr int MIE_SLAB_WARPS_PER_SM = 16;  // slabs reserved per SM (caps the k_mie grid; the resident maximum)
 
 // Per-term constants: c_n = (2n+1) / (n(n+1)) of mieangle evaluated in REAL(4)
 // as the reference does (mie_scat_utilities.f90:139), and 1/n, which replaces
 // the divisions by n in the pi_n and Legendre recurrences (the reference
 // divides; the products differ from the quotients in the last bit only).
-__constant__ double c_mie_c[NT_MAX + 1], c_mie_inv[NT_MAX + 1];
+// c_mie_inv covers the Legendre orders too (l <= MAXNLEG - 1 > NT_MAX).
+__constant__ double c_mie_c[NT_MAX + 1], c_mie_inv[MAXNLEG];
 
 // src/eps_water.f90:653-757 eps_water_tkc (T in degC, f in GHz)
 __device__ cplx eps_water_tkc(double T, double f) {
@@ -194,99 +206,6 @@ __device__ __forceinline__ cplx cdiv_rcp(cplx a, cplx b) {
 
 __device__ __forceinline__ int mie_nstop(double x) { return (int)(x + 4.0 * pow(x, F(0.3334f)) + 2); }
 
-// src/mie_scat_utilities.f90:8-116 miecalc + miecross for one particle: Mie
-// coefficients a_n (into ab[0..]) and b_n (into bb[0..]), 1-based n stored at n-1.
-__device__ void miecalc_cross(int nterms, double x, cplx mn, cplx* ab, cplx* bb, double& qext, double& qscat,
-                              double& qback) {
-  const cplx m = cconj(mn);
-  const cplx y = cscale(m, x);
-  const int nn = nterms + 15;
-  // n / y and d / m through the reciprocals of y and m (one complex division each per particle)
-  const cplx yinv = cdiv(cmk(1.0, 0.0), y), minv = cdiv(cmk(1.0, 0.0), m);
-  // downward recurrence d(n-1) = n/y - 1/(d(n) + n/y), d(nn) = 0; keep d(1..nterms)
-  cplx d = cmk(0.0, 0.0);
-  for (int n = nn; n >= 2; n--) {
-    cplx ny = cscale(yinv, (double)n);
-    // 1 / z as conj(z) / |z|^2: one division on the recurrence's critical path
-    // instead of Smith's three (|z| stays far from the overflow range here)
-    const cplx z = cadd(d, ny);
-    const double s = 1.0 / (z.re * z.re + z.im * z.im);
-    d = cmk(ny.re - z.re * s, ny.im + z.im * s);
-    if (n - 1 <= nterms) ab[n - 2] = d;  // d(n-1) stored at index n-2
-  }
-  double psim = cos(x), psin = sin(x), chim = -sin(x), chin = cos(x);
-  const double xinv = 1.0 / x;  // (2n-1)/x and n/x as products
-  double sum1 = 0.0, sum2 = 0.0;
-  cplx sum3 = cmk(0.0, 0.0);
-  for (int n = 1; n <= nterms; n++) {
-    double tmp = psin;
-    psin = (2 * n - 1) * xinv * psin - psim;
-    psim = tmp;
-    tmp = chin;
-    chin = (2 * n - 1) * xinv * chin - chim;
-    chim = tmp;
-    const cplx xin = cmplx4(psin, -chin), xim = cmplx4(psim, -chim);
-    const cplx dn = ab[n - 1];
-    cplx ctmp = cmul(dn, minv);
-    ctmp.re = ctmp.re + n * xinv;
-    cplx an = cdiv_rcp(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
-    ctmp = cmul(m, dn);
-    ctmp.re = ctmp.re + n * xinv;
-    cplx bn = cdiv_rcp(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
-    ab[n - 1] = an;
-    bb[n - 1] = bn;
-    sum1 = sum1 + (2 * n + 1) * (an.re + bn.re);
-    sum2 = sum2 + (2 * n + 1) * ((an.re * an.re - an.im * (-an.im)) + (bn.re * bn.re - bn.im * (-bn.im)));
-    double fac = (double)((float)(2 * n + 1) * ((n & 1) ? -1.0f : 1.0f));
-    sum3 = cadd(sum3, cscale(csub(an, bn), fac));
-  }
-  qext = 2.0 / (x * x) * sum1;
-  qscat = 2.0 / (x * x) * sum2;
-  cplx t = cscale(sum3, 1.0 / (x * x));
-  qback = t.re * sum3.re - t.im * (-sum3.im);
-}
-
-// src/mie_scat_utilities.f90:119-160 mieangle for ANG_G angles of one particle at once: the coefficients a_n,
-// b_n are read once per n for all angles, and the pi_n recurrence multiplies
-// by the tabulated 1/n.
-__device__ __forceinline__ void mieangle_group(int nterms, const cplx* ab, const cplx* bb, const double (&mu)[ANG_G],
-                                               double (&p)[ANG_G][4]) {
-  double pin[ANG_G], pim[ANG_G], s1r[ANG_G], s1i[ANG_G], s2r[ANG_G], s2i[ANG_G];
-#pragma unroll
-  for (int g = 0; g < ANG_G; g++) {
-    pin[g] = 1.0; pim[g] = 0.0;
-    s1r[g] = 0.0; s1i[g] = 0.0; s2r[g] = 0.0; s2i[g] = 0.0;
-  }
-  for (int n = 1; n <= nterms; n++) {
-    const cplx a = ab[n - 1], b = bb[n - 1];
-    const double c = c_mie_c[n], rn = c_mie_inv[n];
-    const double dn = (double)n, dn1 = (double)(n + 1), d2n1 = (double)(2 * n + 1);
-#pragma unroll
-    for (int g = 0; g < ANG_G; g++) {
-      // tau_n = n mu pi_n - (n+1) pi_{n-1}, pi_{n+1} = ((2n+1) mu pi_n - (n+1) pi_{n-1}) / n
-      // with mu pi_n and (n+1) pi_{n-1} formed once (fused, five operations)
-      const double mp = mu[g] * pin[g], q = dn1 * pim[g];
-      const double taun = fma(dn, mp, -q);
-      s1r[g] = fma(c, fma(a.re, pin[g], b.re * taun), s1r[g]);
-      s1i[g] = fma(c, fma(a.im, pin[g], b.im * taun), s1i[g]);
-      s2r[g] = fma(c, fma(b.re, pin[g], a.re * taun), s2r[g]);
-      s2i[g] = fma(c, fma(b.im, pin[g], a.im * taun), s2i[g]);
-      const double tmp = pin[g];
-      pin[g] = fma(d2n1, mp, -q) * rn;
-      pim[g] = tmp;
-    }
-  }
-#pragma unroll
-  for (int g = 0; g < ANG_G; g++) {
-    // |S1|^2, |S2|^2 directly (the reference squares abs(), i.e. hypot)
-    const double as1 = s1r[g] * s1r[g] + s1i[g] * s1i[g], as2 = s2r[g] * s2r[g] + s2i[g] * s2i[g];
-    p[g][0] = 0.5 * (as2 + as1);
-    p[g][1] = 0.5 * (as2 - as1);
-    p[g][2] = s2r[g] * s1r[g] - (-s2i[g]) * s1i[g];
-    p[g][3] = s1r[g] * s2i[g] + (-s1i[g]) * s2r[g];
-  }
-}
-
 // Refractive indices of liquid water (nmlSet['liq_mod']) and ice of every
 // (present layer, frequency) item, ahead of k_mie (src/scatProperties.f90:
 // 225-236): one thread per item; NaN marks a water model without a value.
@@ -311,20 +230,133 @@ __global__ void k_refr(Batch b, Work w, pamtra_b200_settings st) {
   o[3] = mi.im;
 }
 
+// Per-bin Mie coefficients a_n, b_n of mie_scat_utilities.f90:8-116
+// (miecalc + miecross) written into a column of the warp's coefficient slab:
+// row n-1 holds (a_n.re, a_n.im, b_n.re, b_n.im), rows ldc doubles apart.
+// The downward log-derivative recurrence parks d_n in the same rows first.
+// Returns the efficiencies; rows 0 .. nterms-1 are written.
+__device__ __noinline__ void miecalc_slab(int nterms, double x, cplx mn, double* __restrict__ col, int ldc, double& qext,
+                             double& qscat, double& qback) {
+  const cplx m = cconj(mn);
+  const cplx y = cscale(m, x);
+  const int nn = nterms + 15;
+  const cplx yinv = cdiv(cmk(1.0, 0.0), y), minv = cdiv(cmk(1.0, 0.0), m);
+  // downward recurrence d(n-1) = n/y - 1/(d(n) + n/y), d(nn) = 0; keep d(1..nterms)
+  cplx d = cmk(0.0, 0.0);
+#pragma unroll 1
+  for (int n = nn; n >= 2; n--) {
+    const cplx ny = cscale(yinv, (double)n);
+    // 1 / z as conj(z) / |z|^2: one division on the recurrence's critical path
+    const cplx z = cadd(d, ny);
+    const double s = 1.0 / (z.re * z.re + z.im * z.im);
+    d = cmk(ny.re - z.re * s, ny.im + z.im * s);
+    if (n - 1 <= nterms) *reinterpret_cast<double2*>(col + (size_t)(n - 2) * ldc) = make_double2(d.re, d.im);
+  }
+  double sx, cx;
+  sincos(x, &sx, &cx);
+  double psim = cx, psin = sx, chim = -sx, chin = cx;
+  const double xinv = 1.0 / x;
+  double sum1 = 0.0, sum2 = 0.0;
+  cplx sum3 = cmk(0.0, 0.0);
+#pragma unroll 1
+  for (int n = 1; n <= nterms; n++) {
+    double tmp = psin;
+    psin = (2 * n - 1) * xinv * psin - psim;
+    psim = tmp;
+    tmp = chin;
+    chin = (2 * n - 1) * xinv * chin - chim;
+    chim = tmp;
+    const cplx xin = cmplx4(psin, -chin), xim = cmplx4(psim, -chim);
+    double* row = col + (size_t)(n - 1) * ldc;
+    const double2 dv = *reinterpret_cast<const double2*>(row);
+    const cplx dn = cmk(dv.x, dv.y);
+    cplx ctmp = cmul(dn, minv);
+    ctmp.re = ctmp.re + n * xinv;
+    const cplx an = cdiv_rcp(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
+    ctmp = cmul(m, dn);
+    ctmp.re = ctmp.re + n * xinv;
+    const cplx bn = cdiv_rcp(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
+    *reinterpret_cast<double2*>(row) = make_double2(an.re, an.im);
+    *reinterpret_cast<double2*>(row + 2) = make_double2(bn.re, bn.im);
+    sum1 = sum1 + (2 * n + 1) * (an.re + bn.re);
+    sum2 = sum2 + (2 * n + 1) * ((an.re * an.re - an.im * (-an.im)) + (bn.re * bn.re - bn.im * (-bn.im)));
+    const double fac = (double)((float)(2 * n + 1) * ((n & 1) ? -1.0f : 1.0f));
+    sum3 = cadd(sum3, cscale(csub(an, bn), fac));
+  }
+  qext = 2.0 / (x * x) * sum1;
+  qscat = 2.0 / (x * x) * sum2;
+  const cplx t = cscale(sum3, 1.0 / (x * x));
+  qback = t.re * sum3.re - t.im * (-sum3.im);
+}
+
+// Phase-matrix elements P11, P12 (= P21) and P33 of one angle, summed over
+// the four bins j0 .. j0+3 of a pass with their weights (mieangle,
+// mie_scat_utilities.f90:119-160, and the PSD sums of mie_spheres.f90:
+// 239-249).  The pi_n / tau_n recurrence of the angle runs once for the four
+// bins; c_n pi_n and c_n tau_n multiply each bin's a_n, b_n from the slab
+// (rows of bins without particles, and rows past a bin's own term count,
+// hold zeros).
+__device__ __noinline__ void mie_angle4(const double* __restrict__ slab, int ldc, int j0, int nmax, double mu,
+                                           const double* __restrict__ wt, const double* __restrict__ dd, int nj,
+                                           double (&f)[3]) {
+  double s[4][4];
+#pragma unroll
+  for (int j = 0; j < 4; j++) s[j][0] = s[j][1] = s[j][2] = s[j][3] = 0.0;
+  double pin = 1.0, pim = 0.0;
+  const double* row = slab + 4 * j0;
+  for (int n = 1; n <= nmax; n++, row += ldc) {
+    const double c = c_mie_c[n], rn = c_mie_inv[n];
+    // tau_n = n mu pi_n - (n+1) pi_{n-1}, pi_{n+1} = ((2n+1) mu pi_n - (n+1) pi_{n-1}) / n
+    const double mp = mu * pin, q = (double)(n + 1) * pim;
+    const double taun = fma((double)n, mp, -q);
+    const double cp = c * pin, ct = c * taun;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+      const double2 a = *reinterpret_cast<const double2*>(row + 4 * j);
+      const double2 bq = *reinterpret_cast<const double2*>(row + 4 * j + 2);
+      s[j][0] = fma(a.x, cp, fma(bq.x, ct, s[j][0]));   // S1 = sum c (a pi + b tau)
+      s[j][1] = fma(a.y, cp, fma(bq.y, ct, s[j][1]));
+      s[j][2] = fma(bq.x, cp, fma(a.x, ct, s[j][2]));   // S2 = sum c (b pi + a tau)
+      s[j][3] = fma(bq.y, cp, fma(a.y, ct, s[j][3]));
+    }
+    const double tmp = pin;
+    pin = fma((double)(2 * n + 1), mp, -q) * rn;
+    pim = tmp;
+  }
+  f[0] = f[1] = f[2] = 0.0;
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    if (j >= nj || !(wt[j] > 0.0)) continue;
+    // |S1|^2, |S2|^2 directly (the reference squares abs(), i.e. hypot)
+    const double as1 = s[j][0] * s[j][0] + s[j][1] * s[j][1], as2 = s[j][2] * s[j][2] + s[j][3] * s[j][3];
+    const double p0 = 0.5 * (as2 + as1), p1 = 0.5 * (as2 - as1);
+    const double p2 = s[j][2] * s[j][0] - (-s[j][3]) * s[j][1];
+    f[0] = f[0] + (p0 * wt[j]) * dd[j];
+    f[1] = f[1] + (p1 * wt[j]) * dd[j];
+    f[2] = f[2] + (p2 * wt[j]) * dd[j];
+  }
+}
+
 // One warp per (present layer, frequency) item; species loop in descriptor
 // order.  src/scatProperties.f90:62-1002 (mie-sphere branch and the species
 // sums :920-949, finalize :993) with src/mie_spheres.f90:14-345 per species.
-// Bins are spread over lanes; per-angle phase functions and the efficiencies
-// are summed over bins with warp shuffles; the Legendre projection is a
-// lane-per-quadrature-point series reduced with shuffles.
-__global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st) {
+// Per species the bins go in passes of up to 32: lanes over bins compute
+// the Mie coefficients into the warp's slab (phase A), then lanes over
+// (group of four bins, angle) work items form the phase-function sums of
+// the pass (phase B); each round of 32 items adds into the per-angle sums
+// in lane order, so every result is independent of the launch shape.  The
+// Legendre projection runs lanes over quadrature points with shuffle sums.
+// The species sums accumulate in the item's coefficient output row.
+__global__ void __maxnreg__(MIE_MAXNREG) k_mie(Batch b, Work w, pamtra_b200_settings st) {
   extern __shared__ double smem_raw[];
   MieSmem& S = reinterpret_cast<MieSmem*>(smem_raw)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
+  const int gwarp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (gwarp >= w.mie_nslab) return;
+  double* const slab = w.mie_slab + (size_t)gwarp * MIE_SLAB;
   const int Lm = b.max_nlyrs, Fm = b.max_nfreq, H = b.nhydro;
   const int P = min(w.counters[0], w.pmax);
   const int nitems = P * Fm;
-  cplx ab[NT_MAX], bb[NT_MAX];
   for (;;) {
     int item = 0;
     if (lane == 0) item = atomicAdd(&w.counters[1], 1);
@@ -336,7 +368,8 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
     if (f >= b.col_nfreq(c)) continue;
     const double freq = b.freq(c, f);
     const double wl = C_LIGHT / (freq * 1e9);
-    for (int jj = lane; jj < MAXNLEG; jj += 32) { S.legc[0][jj] = 0.0; S.legc[1][jj] = 0.0; S.legc[2][jj] = 0.0; }
+    double* const legc = w.m_legen + (size_t)item * 3 * MAXNLEG;  // species sums, then the result
+    for (int jj = lane; jj < 3 * MAXNLEG; jj += 32) legc[jj] = 0.0;
     double kexttot = 0.0, salbedo = 0.0, backtot = 0.0;
     int nlegen_coef = 0;
     int status = 0;
@@ -345,7 +378,9 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
     for (int h = 0; h < H; h++) {
       const size_t s_idx = ((size_t)c * Lm + z) * H + h;
       if (w.slot_st[s_idx] != 2) continue;
-      const pamtra_b200_species sp = b.species_of(c, h);
+      const pamtra_b200_species* spp = b.species + (size_t)c * b.species_stride + h;
+      const int sp_liq_ice = spp->liq_ice;
+      const double sp_as_ratio = spp->as_ratio;
       const int nb = w.slot_nb[s_idx];
       const size_t base = s_idx * (size_t)b.max_nbin;
       const double* bd = w.b_d + base;
@@ -353,7 +388,7 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
       const double* bnd = w.b_nd + base;
       const double* brho = w.b_rho + base;
       const double* bmass = w.b_mass + base;
-      const double* mr = w.m_refr + (size_t)item * 4 + (sp.liq_ice == 1 ? 0 : 2);
+      const double* mr = w.m_refr + (size_t)item * 4 + (sp_liq_ice == 1 ? 0 : 2);
       const cplx mref = cmk(mr[0], mr[1]);
       if (isnan(mref.re)) {
         status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_RANGE;
@@ -367,7 +402,7 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
         dia = bd[i];
         if (rho == -1.0) {
           const double mind = st.hydro_softsphere_min_density;
-          rho = (sp.as_ratio == -20.) ? 0.863 * freq + 115.0 : 0.815 * freq + 11.2;
+          rho = (sp_as_ratio == -20.) ? 0.863 * freq + 115.0 : 0.815 * freq + 11.2;
           if (rho < mind) rho = mind;
           dia = pow((6.0 * bmass[i]) / (PI * rho), 1.0 / 3.0);
           if (st.hydro_limit_density_area) {
@@ -388,90 +423,109 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
       }
       const double* gx = w.gq_x + (size_t)nquad * (nquad - 1) / 2;
       const double* gw = w.gq_w + (size_t)nquad * (nquad - 1) / 2;
-      for (int i = lane; i < nquad; i += 32) { S.sump[0][i] = 0; S.sump[1][i] = 0; S.sump[2][i] = 0; S.sump[3][i] = 0; }
-      __syncwarp();
-      double sqe = 0.0, sqs = 0.0, sqb = 0.0;
-      // Bins in passes of `chunk` bins with R = 32 / chunk lanes per bin:
-      // full passes of 32 bins, then the remainder split into powers of two
-      // (40 bins = 32 + 8: the 8-bin pass gives each bin 4 lanes, which share
-      // its angles), so every pass keeps all lanes busy.  Lane r of a bin
-      // takes angles i0 + g R + r; the bin sums reduce over lanes with the
-      // same r.
-      for (int c0 = 0; c0 < nb;) {
-        const int rem = nb - c0;
-        const int chunk = rem >= 32 ? 32 : (1 << (31 - __clz(rem)));
-        const int R = 32 / chunk;
-        const int r = lane & (R - 1);
-        const int ir = c0 + lane / R;
-        c0 += chunk;
-        bool act = false;
-        double wgt = 0.0, ndens = 0.0, deld = 0.0, qb_bin = 0.0;
-        int nm = 0;
-        deld = bdd[ir];
-        ndens = bnd[ir] / deld;
-        act = ndens > 0;
-        if (act) {
+      for (int i = lane; i < nquad; i += 32) { S.sump[0][i] = 0; S.sump[1][i] = 0; S.sump[2][i] = 0; }
+      // rows the slab needs: every active bin's own series length, at least nterms
+      int kmax = nterms;
+      for (int ir = lane; ir < nb; ir += 32) {
+        if (bnd[ir] / bdd[ir] > 0) {
           double rho, dia;
           dens_diam(ir, rho, dia);
-          const cplx ms = (sp.liq_ice == -1 && rho != 917.0) ? eps_mix_m(m_ice, rho) : m_ice;
-          const double x = PI * dia / wl;
-          int nmie = mie_nstop(x);
-          if (nmie + 1 > NT_MAX) { nmie = NT_MAX - 1; status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE; }
-          double qe, qs, qb;
-          miecalc_cross(nmie, x, ms, ab, bb, qe, qs, qb);
-          if (r == 0) {
-            const double r2 = (dia / 2.0) * (dia / 2.0);
-            qe = qe * r2 * PI;
-            qs = qs * r2 * PI;
-            qb = qb * r2 * PI;
-            qe = qe * ndens;
-            qs = qs * ndens;
-            qb = qb * ndens;
-            sqe = sqe + qe * deld;
-            sqs = sqs + qs * deld;
-            sqb = sqb + qb * deld;
-            qb_bin = qb;
-          }
-          nm = min(nmie, nterms);
-          wgt = ndens;
-        }
-        // per-particle cross section as back_spec / num_density of
-        // src/scatProperties.f90:916 (0 / 0 = NaN for an empty bin)
-        if (bscat && r == 0 && ir < w.psd_nbin) bscat[s_idx * (size_t)w.psd_nbin + ir] = qb_bin / ndens;
-        for (int i0 = 0; i0 < nquad; i0 += ANG_G * R) {
-          double pp[ANG_G][4];
-          if (act) {
-            double mu[ANG_G];
-#pragma unroll
-            for (int g = 0; g < ANG_G; g++) {
-              const int i = i0 + g * R + r;
-              mu[g] = (i < nquad) ? gx[i] : 0.0;
-            }
-            mieangle_group(nm, ab, bb, mu, pp);
-#pragma unroll
-            for (int g = 0; g < ANG_G; g++)
-#pragma unroll
-              for (int k = 0; k < 4; k++) pp[g][k] = pp[g][k] * wgt * deld;
-          } else {
-#pragma unroll
-            for (int g = 0; g < ANG_G; g++)
-#pragma unroll
-              for (int k = 0; k < 4; k++) pp[g][k] = 0.0;
-          }
-#pragma unroll
-          for (int g = 0; g < ANG_G; g++) {
-#pragma unroll
-            for (int k = 0; k < 4; k++)
-              for (int o = 16; o >= R; o >>= 1) pp[g][k] += __shfl_xor_sync(0xffffffffu, pp[g][k], o);
-            const int i = i0 + g * R + r;
-            if (i < nquad && lane < R) {
-#pragma unroll
-              for (int k = 0; k < 4; k++) S.sump[k][i] += pp[g][k];
-            }
-          }
+          kmax = max(kmax, min(mie_nstop(PI * dia / wl), NT_MAX - 1));
         }
       }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
+      // bins per pass, a multiple of 4 so that no group of four bins runs past the slab's columns
+      const int bp = min(32, MIE_SLAB / (4 * kmax)) & ~3;
+      const int ldc = 4 * bp;
       __syncwarp();
+      double sqe = 0.0, sqs = 0.0, sqb = 0.0;
+      for (int c0 = 0; c0 < nb; c0 += bp) {
+        const int cb = min(bp, nb - c0);
+        // ---- phase A: lane j < bp owns bin c0 + j (column j of the slab)
+        if (lane < bp) {
+          const int ir = c0 + lane;
+          int nm = 0;
+          double wgt = 0.0, deld = 0.0, qb_bin = 0.0, ndens = 0.0;
+          double* col = slab + 4 * lane;
+          if (lane < cb) {
+            deld = bdd[ir];
+            ndens = bnd[ir] / deld;
+            if (ndens > 0) {
+              double rho, dia;
+              dens_diam(ir, rho, dia);
+              const cplx ms = (sp_liq_ice == -1 && rho != 917.0) ? eps_mix_m(m_ice, rho) : m_ice;
+              const double x = PI * dia / wl;
+              int nmie = mie_nstop(x);
+              if (nmie + 1 > NT_MAX) { nmie = NT_MAX - 1; status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE; }
+              double qe, qs, qb;
+              miecalc_slab(nmie, x, ms, col, ldc, qe, qs, qb);
+              const double r2 = (dia / 2.0) * (dia / 2.0);
+              qe = qe * r2 * PI;
+              qs = qs * r2 * PI;
+              qb = qb * r2 * PI;
+              qe = qe * ndens;
+              qs = qs * ndens;
+              qb = qb * ndens;
+              sqe = sqe + qe * deld;
+              sqs = sqs + qs * deld;
+              sqb = sqb + qb * deld;
+              qb_bin = qb;
+              nm = min(nmie, nterms);
+              wgt = ndens;
+            }
+            // per-particle cross section as back_spec / num_density of
+            // src/scatProperties.f90:916 (0 / 0 = NaN for an empty bin)
+            if (bscat && ir < w.psd_nbin) bscat[s_idx * (size_t)w.psd_nbin + ir] = qb_bin / ndens;
+          }
+          for (int n = nm; n < nterms; n++)
+            *reinterpret_cast<double4*>(col + (size_t)n * ldc) = make_double4(0.0, 0.0, 0.0, 0.0);
+          S.bw[lane] = wgt;
+          S.bd[lane] = deld;
+          S.bn[lane] = nm;
+        }
+        __syncwarp();
+        // ---- phase B: item u = g * nquad + i: angle i over the bins 4g .. 4g+3 of the pass
+        const int G = (cb + 3) / 4;
+        const int nu = G * nquad;
+        for (int u0 = 0; u0 < nu; u0 += 32) {
+          const int u = u0 + lane;
+          double fk[3] = {0.0, 0.0, 0.0};
+          int ia = -1;
+          if (u < nu) {
+            const int g = u / nquad, i = u - g * nquad;
+            ia = i;
+            const int j0 = 4 * g, nj = min(4, cb - j0);
+            int nmax = 0;
+            for (int j = 0; j < nj; j++) nmax = max(nmax, S.bn[j0 + j]);
+            mie_angle4(slab, ldc, j0, nmax, gx[i], S.bw + j0, S.bd + j0, nj, fk);
+          }
+          if (nquad >= 32) {
+            // the 32 items of a round have distinct angles
+            if (ia >= 0) {
+              S.sump[0][ia] += fk[0];
+              S.sump[1][ia] += fk[1];
+              S.sump[2][ia] += fk[2];
+            }
+          } else {
+            // angles repeat within the round: lane i adds the items of angle i in lane order
+            S.stg[0][lane] = fk[0];
+            S.stg[1][lane] = fk[1];
+            S.stg[2][lane] = fk[2];
+            S.sti[lane] = ia;
+            __syncwarp();
+            if (lane < nquad) {
+              double a0 = S.sump[0][lane], a1 = S.sump[1][lane], a2 = S.sump[2][lane];
+              for (int L = 0; L < 32; L++)
+                if (S.sti[L] == lane) { a0 += S.stg[0][L]; a1 += S.stg[1][L]; a2 += S.stg[2][L]; }
+              S.sump[0][lane] = a0;
+              S.sump[1][lane] = a1;
+              S.sump[2][lane] = a2;
+            }
+          }
+          __syncwarp();
+        }
+      }
       sqe = warp_sum(sqe);
       sqs = warp_sum(sqs);
       sqb = warp_sum(sqb);
@@ -482,37 +536,59 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
       for (int i = lane; i < nquad; i += 32) {
         const double wt = gw[i];
 #pragma unroll
-        for (int k = 0; k < 4; k++) S.sump[k][i] = tmp * S.sump[k][i] * wt;
+        for (int k = 0; k < 3; k++) S.sump[k][i] = tmp * S.sump[k][i] * wt;
       }
       __syncwarp();
-      // Legendre projection: coef_l = sum_i sump(i) P_l(mu_i), l = 0..nlegen
-      constexpr int NQL = NQ_MAX / 32;
-      double pl[NQL], pl1[NQL], pl2[NQL];
-#pragma unroll
-      for (int q = 0; q < NQL; q++) { pl[q] = 1.0; pl1[q] = 1.0; pl2[q] = 0.0; }
+      // Legendre projection: coef_l = sum_i sump(i) P_l(mu_i), l = 0..nlegen,
+      // in chunks of 64 quadrature points (two per lane); the chunk sums of
+      // each order go into the slab (legh), in chunk order
+      double* const legh = slab;  // [3][MAXNLEG]; the coefficients of the pass are no longer needed
       const double thr = F(1.0e-7f);
-      int last = -1;
-      for (int l = 0; l <= nlegen; l++) {
-        double acc[3] = {0.0, 0.0, 0.0};
+      for (int q0 = 0; q0 < nquad; q0 += 64) {
+        const int i0 = q0 + lane, i1 = q0 + 32 + lane;
+        const double mu0 = (i0 < nquad) ? gx[i0] : 0.0, mu1 = (i1 < nquad) ? gx[i1] : 0.0;
+        double s0[3], s1[3];
 #pragma unroll
-        for (int q = 0; q < NQL; q++) {
-          const int i = lane + 32 * q;
-          if (i < nquad) {
-            const double mu = gx[i];
-            if (l > 0) pl[q] = ((2 * l - 1) * mu * pl1[q] - (l - 1) * pl2[q]) * c_mie_inv[l];
+        for (int k = 0; k < 3; k++) {
+          s0[k] = (i0 < nquad) ? S.sump[k][i0] : 0.0;
+          s1[k] = (i1 < nquad) ? S.sump[k][i1] : 0.0;
+        }
+        double pa = 1.0, pa1 = 1.0, pa2 = 0.0, pb = 1.0, pb1 = 1.0, pb2 = 0.0;
+        for (int l = 0; l <= nlegen; l++) {
+          if (l > 0) {
+            pa = ((2 * l - 1) * mu0 * pa1 - (l - 1) * pa2) * c_mie_inv[l];
+            pb = ((2 * l - 1) * mu1 * pb1 - (l - 1) * pb2) * c_mie_inv[l];
+          }
+          double acc[3];
 #pragma unroll
-            for (int k = 0; k < 3; k++) acc[k] = fma(S.sump[k][i], pl[q], acc[k]);
-            pl2[q] = pl1[q];
-            pl1[q] = pl[q];
+          for (int k = 0; k < 3; k++) acc[k] = fma(s1[k], pb, fma(s0[k], pa, 0.0));
+          pa2 = pa1;
+          pa1 = pa;
+          pb2 = pb1;
+          pb1 = pb;
+#pragma unroll
+          for (int k = 0; k < 3; k++) acc[k] = warp_sum(acc[k]);
+          if (lane == 0) {
+#pragma unroll
+            for (int k = 0; k < 3; k++) legh[k * MAXNLEG + l] = (q0 == 0) ? acc[k] : legh[k * MAXNLEG + l] + acc[k];
           }
         }
+      }
+      // orders past this species' series are zero in the species sums (mie_spheres.f90:309-316)
+      for (int l = nlegen + 1 + lane; l < MAXNLEG; l += 32) {
+#pragma unroll
+        for (int k = 0; k < 3; k++) legh[k * MAXNLEG + l] = 0.0;
+      }
+      __syncwarp();
+      int last = -1;
+      for (int l = lane; l <= nlegen; l += 32) {
         const double fac = (double)((float)(2 * l + 1) / 2.0f);  // REAL(4) division, exact
 #pragma unroll
-        for (int k = 0; k < 3; k++) acc[k] = fac * warp_sum(acc[k]);
-        if (lane == 0) { S.legh[0][l] = acc[0]; S.legh[1][l] = acc[1]; S.legh[2][l] = acc[2]; }
-        if (acc[0] > thr) last = l;
+        for (int k = 0; k < 3; k++) legh[k * MAXNLEG + l] = fac * legh[k * MAXNLEG + l];
+        if (legh[l] > thr) last = l;
       }
-      for (int l = nlegen + 1 + lane; l < MAXNLEG; l += 32) { S.legh[0][l] = 0; S.legh[1][l] = 0; S.legh[2][l] = 0; }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) last = max(last, __shfl_xor_sync(0xffffffffu, last, o));
       __syncwarp();
       const int nlegen_h = (last >= 0) ? last : nlegen;  // mie_spheres.f90:307-314
       if (!(extinction > 0) || !(scatter > 0) || !(sqb > 0) || isnan(extinction)) {
@@ -528,21 +604,21 @@ __global__ void __maxnreg__(160) k_mie(Batch b, Work w, pamtra_b200_settings st)
       else salbedo = salbedo + (salb_h * extinction);
       for (int jj = lane; jj < nlegen_coef; jj += 32) {
 #pragma unroll
-        for (int k = 0; k < 3; k++) S.legc[k][jj] = S.legc[k][jj] + (S.legh[k][jj] * salb_h * extinction);
+        for (int k = 0; k < 3; k++)
+          legc[k * MAXNLEG + jj] = legc[k * MAXNLEG + jj] + (legh[k * MAXNLEG + jj] * salb_h * extinction);
       }
       __syncwarp();
       if (nlegen_coef > MAXNLEG - 1) { status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE; break; }
     }
-    // finalize_rt3_scatProperties (scatProperties.f90:993-1002)
+    // finalize_rt3_scatProperties (scatProperties.f90:993-1002), in place
     salbedo = salbedo / kexttot;
     const double den = salbedo * kexttot;
-    double* out = w.m_legen + (size_t)item * 3 * MAXNLEG;
     for (int jj = lane; jj <= nlegen_coef && jj < MAXNLEG; jj += 32) {
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        double v = S.legc[k][jj] / den;
+        const double v = legc[k * MAXNLEG + jj] / den;
         if (isnan(v) && nlegen_coef > 0) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_NAN;
-        out[k * MAXNLEG + jj] = v;
+        legc[k * MAXNLEG + jj] = v;
       }
     }
     status = __reduce_or_sync(0xffffffffu, status);

@@ -65,6 +65,8 @@ struct Work {
   double* m_back;                      // [pmax*Fm] volumetric backscattering cross section, m^2/m^3
   double* m_refr;                      // [pmax*Fm][4] refractive index of water (re, im), ice (re, im); NaN: none
   int* m_nleg;                         // [pmax*Fm]
+  double* mie_slab;                    // [mie_nslab][MIE_SLAB] per-warp Mie coefficient slabs of k_mie
+  int mie_nslab;
   double* m_legen;                     // [pmax*Fm][3][MAXNLEG]
   // layer R, T, S per item (R,T padded n x (n+2), symmetric +/-)
   double* lay;                         // [pmax*Fm][lay_stride]
