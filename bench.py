@@ -53,7 +53,8 @@ def _args():
     ap.add_argument("--ncol", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=0, help="columns for the CPU baseline (0 = 2 per core)")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--serve-requests", type=int, default=16, help="requests in the serving replay (0 = skip)")
+    ap.add_argument("--serve-requests", type=int, default=200, help="requests in the serving replay (0 = skip)")
+    ap.add_argument("--serve-plain", type=int, default=30, help="requests of the stream served by the plain form")
     ap.add_argument("--target-cols", type=int, default=1024, help="columns of the 150-layer target batch (0 = skip)")
     ap.add_argument("--uneven-cols", type=int, default=2048, help="columns of the uneven batch (0 = skip)")
     ap.add_argument("--mieheavy-cols", type=int, default=1024, help="columns of the Mie-heavy batch (0 = skip)")
@@ -385,33 +386,50 @@ def _config_line(name, b, local, eng, stream, nplain=8, reps=2):
 
 
 def _serving(args, local):
-    """Replay a seeded Poisson stream (200 requests/s) of uneven requests
-    through the continuous-batching server: the batched split-precision and
-    batched FP64 forms (three slots) on the whole stream, the plain form (one
-    column per call, one slot) on its first three requests."""
+    """Replay one seeded stream of uneven requests through the
+    continuous-batching server: the batched split-precision form at 200
+    requests/s (far above capacity: latency is queueing) and at half of the
+    capacity that run measured (latency is service), the batched FP64 form at
+    200 requests/s, and the plain form (one column per call) on the first
+    requests of the same stream at 200 requests/s."""
     from pamtra_b200 import serve
     from pamtra_b200._native import PREC_3XTF32, PREC_FP64, PREC_FP64_BATCHED
-    reqs = serve.request_stream(args.serve_requests, seed=5, max_cols=512, nfreq_range=(1, 32))
-    arr = serve.poisson_arrivals(len(reqs), 200.0, seed=6)
+    n = args.serve_requests
+    reqs = serve.request_stream(n, seed=5, max_cols=512, nfreq_range=(1, 32), sizes="loguniform")
     warm = serve.request_stream(3, seed=7, max_cols=16, nfreq_range=(1, 4))
-    res = {"stream": "%d requests, Poisson 200/s (seed 6); each 1-512 columns of 40-150 layers, 1-5 species, "
-                     "1-32 frequencies in 10-183 GHz, NUMMU in {8,16,32}" % len(reqs)}
-    for label, prec, slots, cols, nreq in (("batched_3xtf32", PREC_3XTF32, 3, 2048, len(reqs)),
-                                           ("batched_fp64", PREC_FP64_BATCHED, 3, 2048, len(reqs)),
-                                           ("plain_fp64", PREC_FP64, 1, 1, min(3, len(reqs)))):
+    res = {"stream": "%d requests (seed 5): each 1-512 columns (log-uniform) of 40-150 layers, 1-5 species, "
+                     "1-32 frequencies in 10-183 GHz, NUMMU in {8,16,32}; %d columns, %d solves in all"
+                     % (n, sum(b.ncol for b in reqs), sum(b.n_solves() for b in reqs))}
+
+    def one(prec, slots, cols, rate, nreq):
+        arr = serve.poisson_arrivals(nreq, rate, seed=6)
         srv = serve.Server(local, slots=slots, hbm_fraction=0.5 if slots > 1 else 0.2, max_cols=cols,
                            precision=prec)
         for b in warm:
             srv.submit(b)
         srv.drain()
-        nb0 = srv.batches_launched
-        done, wall = serve.replay(srv, reqs[:nreq], arr[:nreq])
+        nb0, ni0 = srv.batches_launched, len(srv.intervals)
+        done, wall = serve.replay(srv, reqs[:nreq], arr)
         nb = srv.batches_launched - nb0
+        iv = srv.intervals[ni0:]
         srv.close()
         solves = sum(r.n_solves() for r in done)
-        res[label] = dict(serve.latency_stats(done), solves_per_s=solves / wall, solves=solves, wall_s=wall,
-                          batches=nb, requests_with_error=sum(1 for r in done if r.error), slots=slots,
-                          requests=nreq)
+        ov = serve.overlapping_pairs(iv)
+        return dict(serve.latency_stats(done), rate_req_s=rate, requests=nreq, solves=solves,
+                    solves_per_s=solves / wall, wall_s=wall, batches=nb, slots=slots,
+                    requests_with_error=sum(1 for r in done if r.error),
+                    overlapping_batch_pairs=len(ov), overlap_ms=float(sum(o for _, _, o in ov)))
+
+    hi = one(PREC_3XTF32, 3, 2048, 200.0, n)
+    low_rate = 0.5 * n / hi["wall_s"]
+    res["batched_3xtf32"] = {"rate_200": hi, "rate_half_capacity": one(PREC_3XTF32, 3, 2048, low_rate, n)}
+    res["batched_fp64"] = {"rate_200": one(PREC_FP64_BATCHED, 3, 2048, 200.0, n)}
+    nplain = min(n, args.serve_plain)
+    res["plain_fp64"] = {"rate_200": one(PREC_FP64, 1, 1, 200.0, nplain)}
+    res["note"] = ("rate_200 offers far more work than any form can serve, so its latencies are queueing "
+                   "delay; rate_half_capacity offers half of the requests/s the batched split-precision form "
+                   "completed at rate_200, so its latencies are service time. The plain form serves the "
+                   "first %d requests of the same stream." % nplain)
     return res
 
 

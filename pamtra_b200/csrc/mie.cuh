@@ -231,10 +231,11 @@ __global__ void k_refr(Batch b, Work w, pamtra_b200_settings st) {
 }
 
 // Per-bin Mie coefficients a_n, b_n of mie_scat_utilities.f90:8-116
-// (miecalc + miecross) written into a column of the warp's coefficient slab:
-// row n-1 holds (a_n.re, a_n.im, b_n.re, b_n.im), rows ldc doubles apart.
-// The downward log-derivative recurrence parks d_n in the same rows first.
-// Returns the efficiencies; rows 0 .. nterms-1 are written.
+// (miecalc + miecross) written into a column of the warp's coefficient slab
+// as their sum and difference: row n-1 holds (u_n.re, u_n.im, v_n.re,
+// v_n.im), u_n = a_n + b_n, v_n = a_n - b_n, rows ldc doubles apart.  The
+// downward log-derivative recurrence parks d_n in the same rows first.
+// Returns the efficiencies (from a_n, b_n); rows 0 .. nterms-1 are written.
 __device__ __noinline__ void miecalc_slab(int nterms, double x, cplx mn, double* __restrict__ col, int ldc, double& qext,
                              double& qscat, double& qback) {
   const cplx m = cconj(mn);
@@ -276,8 +277,8 @@ __device__ __noinline__ void miecalc_slab(int nterms, double x, cplx mn, double*
     ctmp = cmul(m, dn);
     ctmp.re = ctmp.re + n * xinv;
     const cplx bn = cdiv_rcp(cmk(ctmp.re * psin - psim, ctmp.im * psin), csub(cmul(ctmp, xin), xim));
-    *reinterpret_cast<double2*>(row) = make_double2(an.re, an.im);
-    *reinterpret_cast<double2*>(row + 2) = make_double2(bn.re, bn.im);
+    *reinterpret_cast<double2*>(row) = make_double2(an.re + bn.re, an.im + bn.im);
+    *reinterpret_cast<double2*>(row + 2) = make_double2(an.re - bn.re, an.im - bn.im);
     sum1 = sum1 + (2 * n + 1) * (an.re + bn.re);
     sum2 = sum2 + (2 * n + 1) * ((an.re * an.re - an.im * (-an.im)) + (bn.re * bn.re - bn.im * (-bn.im)));
     const double fac = (double)((float)(2 * n + 1) * ((n & 1) ? -1.0f : 1.0f));
@@ -290,18 +291,27 @@ __device__ __noinline__ void miecalc_slab(int nterms, double x, cplx mn, double*
 }
 
 // Phase-matrix elements P11, P12 (= P21) and P33 of one angle, summed over
-// the four bins j0 .. j0+3 of a pass with their weights (mieangle,
+// the bins j0 .. j0+MIE_GROUP-1 of a pass with their weights (mieangle,
 // mie_scat_utilities.f90:119-160, and the PSD sums of mie_spheres.f90:
-// 239-249).  The pi_n / tau_n recurrence of the angle runs once for the four
-// bins; c_n pi_n and c_n tau_n multiply each bin's a_n, b_n from the slab
-// (rows of bins without particles, and rows past a bin's own term count,
-// hold zeros).
-__device__ __noinline__ void mie_angle4(const double* __restrict__ slab, int ldc, int j0, int nmax, double mu,
-                                           const double* __restrict__ wt, const double* __restrict__ dd, int nj,
-                                           double (&f)[3]) {
-  double s[4][4];
+// 239-249).  With S+ = S1 + S2 = sum c_n u_n (pi_n + tau_n) and
+// S- = S1 - S2 = sum c_n v_n (pi_n - tau_n) each term costs two complex
+// multiply-adds instead of four, and
+//   P11 = (|S1|^2 + |S2|^2) / 2 = (|S+|^2 + |S-|^2) / 4,
+//   P12 = (|S2|^2 - |S1|^2) / 2 = -Re(S+ conj(S-)) / 2,
+//   P33 = Re(S2 conj(S1))       = (|S+|^2 - |S-|^2) / 4.
+// The pi_n / tau_n recurrence of the angle runs once for the group (rows
+// of bins without particles, and rows past a bin's own term count, hold
+// zeros).
+#ifndef MIE_GROUP_BINS
+#define MIE_GROUP_BINS 4
+#endif
+constexpr int MIE_GROUP = MIE_GROUP_BINS;  // bins per work item (4 or 8)
+__device__ __forceinline__ void mie_angle_group(const double* __restrict__ slab, int ldc, int j0, int nmax, double mu,
+                                                const double* __restrict__ wt, const double* __restrict__ dd, int nj,
+                                                double (&f)[3]) {
+  double s[MIE_GROUP][4];  // S+ (re, im), S- (re, im)
 #pragma unroll
-  for (int j = 0; j < 4; j++) s[j][0] = s[j][1] = s[j][2] = s[j][3] = 0.0;
+  for (int j = 0; j < MIE_GROUP; j++) s[j][0] = s[j][1] = s[j][2] = s[j][3] = 0.0;
   double pin = 1.0, pim = 0.0;
   const double* row = slab + 4 * j0;
   for (int n = 1; n <= nmax; n++, row += ldc) {
@@ -309,15 +319,15 @@ __device__ __noinline__ void mie_angle4(const double* __restrict__ slab, int ldc
     // tau_n = n mu pi_n - (n+1) pi_{n-1}, pi_{n+1} = ((2n+1) mu pi_n - (n+1) pi_{n-1}) / n
     const double mp = mu * pin, q = (double)(n + 1) * pim;
     const double taun = fma((double)n, mp, -q);
-    const double cp = c * pin, ct = c * taun;
+    const double cpl = c * (pin + taun), cmi = c * (pin - taun);
 #pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const double2 a = *reinterpret_cast<const double2*>(row + 4 * j);
-      const double2 bq = *reinterpret_cast<const double2*>(row + 4 * j + 2);
-      s[j][0] = fma(a.x, cp, fma(bq.x, ct, s[j][0]));   // S1 = sum c (a pi + b tau)
-      s[j][1] = fma(a.y, cp, fma(bq.y, ct, s[j][1]));
-      s[j][2] = fma(bq.x, cp, fma(a.x, ct, s[j][2]));   // S2 = sum c (b pi + a tau)
-      s[j][3] = fma(bq.y, cp, fma(a.y, ct, s[j][3]));
+    for (int j = 0; j < MIE_GROUP; j++) {
+      const double2 u = *reinterpret_cast<const double2*>(row + 4 * j);
+      const double2 v = *reinterpret_cast<const double2*>(row + 4 * j + 2);
+      s[j][0] = fma(u.x, cpl, s[j][0]);
+      s[j][1] = fma(u.y, cpl, s[j][1]);
+      s[j][2] = fma(v.x, cmi, s[j][2]);
+      s[j][3] = fma(v.y, cmi, s[j][3]);
     }
     const double tmp = pin;
     pin = fma((double)(2 * n + 1), mp, -q) * rn;
@@ -325,15 +335,62 @@ __device__ __noinline__ void mie_angle4(const double* __restrict__ slab, int ldc
   }
   f[0] = f[1] = f[2] = 0.0;
 #pragma unroll
-  for (int j = 0; j < 4; j++) {
+  for (int j = 0; j < MIE_GROUP; j++) {
     if (j >= nj || !(wt[j] > 0.0)) continue;
-    // |S1|^2, |S2|^2 directly (the reference squares abs(), i.e. hypot)
-    const double as1 = s[j][0] * s[j][0] + s[j][1] * s[j][1], as2 = s[j][2] * s[j][2] + s[j][3] * s[j][3];
-    const double p0 = 0.5 * (as2 + as1), p1 = 0.5 * (as2 - as1);
-    const double p2 = s[j][2] * s[j][0] - (-s[j][3]) * s[j][1];
+    const double ap = s[j][0] * s[j][0] + s[j][1] * s[j][1], am = s[j][2] * s[j][2] + s[j][3] * s[j][3];
+    const double p0 = 0.25 * (ap + am), p2 = 0.25 * (ap - am);
+    const double p1 = -0.5 * (s[j][0] * s[j][2] + s[j][1] * s[j][3]);
     f[0] = f[0] + (p0 * wt[j]) * dd[j];
     f[1] = f[1] + (p1 * wt[j]) * dd[j];
     f[2] = f[2] + (p2 * wt[j]) * dd[j];
+  }
+}
+
+// Phase B of one pass (whole warp): item u = g * nquad + i is angle i over
+// the bins of group g of the pass.  Out of line so that the kernel's state
+// is saved once per pass and the items keep the registers for their sums.
+// Each round of 32 items adds into the per-angle sums in lane order.
+__device__ __noinline__ void mie_pass_sums(MieSmem& S, const double* __restrict__ slab, int ldc, int cb, int nquad,
+                                           const double* __restrict__ gx) {
+  const int lane = threadIdx.x & 31;
+  const int G = (cb + MIE_GROUP - 1) / MIE_GROUP;
+  const int nu = G * nquad;
+  for (int u0 = 0; u0 < nu; u0 += 32) {
+    const int u = u0 + lane;
+    double fk[3] = {0.0, 0.0, 0.0};
+    int ia = -1;
+    if (u < nu) {
+      const int g = u / nquad, i = u - g * nquad;
+      ia = i;
+      const int j0 = MIE_GROUP * g, nj = min(MIE_GROUP, cb - j0);
+      int nmax = 0;
+      for (int j = 0; j < nj; j++) nmax = max(nmax, S.bn[j0 + j]);
+      mie_angle_group(slab, ldc, j0, nmax, gx[i], S.bw + j0, S.bd + j0, nj, fk);
+    }
+    if (nquad >= 32) {
+      // the 32 items of a round have distinct angles
+      if (ia >= 0) {
+        S.sump[0][ia] += fk[0];
+        S.sump[1][ia] += fk[1];
+        S.sump[2][ia] += fk[2];
+      }
+    } else {
+      // angles repeat within the round: lane i adds the items of angle i in lane order
+      S.stg[0][lane] = fk[0];
+      S.stg[1][lane] = fk[1];
+      S.stg[2][lane] = fk[2];
+      S.sti[lane] = ia;
+      __syncwarp();
+      if (lane < nquad) {
+        double a0 = S.sump[0][lane], a1 = S.sump[1][lane], a2 = S.sump[2][lane];
+        for (int L = 0; L < 32; L++)
+          if (S.sti[L] == lane) { a0 += S.stg[0][L]; a1 += S.stg[1][L]; a2 += S.stg[2][L]; }
+        S.sump[0][lane] = a0;
+        S.sump[1][lane] = a1;
+        S.sump[2][lane] = a2;
+      }
+    }
+    __syncwarp();
   }
 }
 
@@ -342,7 +399,7 @@ __device__ __noinline__ void mie_angle4(const double* __restrict__ slab, int ldc
 // sums :920-949, finalize :993) with src/mie_spheres.f90:14-345 per species.
 // Per species the bins go in passes of up to 32: lanes over bins compute
 // the Mie coefficients into the warp's slab (phase A), then lanes over
-// (group of four bins, angle) work items form the phase-function sums of
+// (group of bins, angle) work items form the phase-function sums of
 // the pass (phase B); each round of 32 items adds into the per-angle sums
 // in lane order, so every result is independent of the launch shape.  The
 // Legendre projection runs lanes over quadrature points with shuffle sums.
@@ -435,8 +492,8 @@ __global__ void __maxnreg__(MIE_MAXNREG) k_mie(Batch b, Work w, pamtra_b200_sett
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
-      // bins per pass, a multiple of 4 so that no group of four bins runs past the slab's columns
-      const int bp = min(32, MIE_SLAB / (4 * kmax)) & ~3;
+      // bins per pass, a multiple of the group size so that no group runs past the slab's columns
+      const int bp = min(32, MIE_SLAB / (4 * kmax)) & ~(MIE_GROUP - 1);
       const int ldc = 4 * bp;
       __syncwarp();
       double sqe = 0.0, sqs = 0.0, sqb = 0.0;
@@ -485,46 +542,8 @@ __global__ void __maxnreg__(MIE_MAXNREG) k_mie(Batch b, Work w, pamtra_b200_sett
           S.bn[lane] = nm;
         }
         __syncwarp();
-        // ---- phase B: item u = g * nquad + i: angle i over the bins 4g .. 4g+3 of the pass
-        const int G = (cb + 3) / 4;
-        const int nu = G * nquad;
-        for (int u0 = 0; u0 < nu; u0 += 32) {
-          const int u = u0 + lane;
-          double fk[3] = {0.0, 0.0, 0.0};
-          int ia = -1;
-          if (u < nu) {
-            const int g = u / nquad, i = u - g * nquad;
-            ia = i;
-            const int j0 = 4 * g, nj = min(4, cb - j0);
-            int nmax = 0;
-            for (int j = 0; j < nj; j++) nmax = max(nmax, S.bn[j0 + j]);
-            mie_angle4(slab, ldc, j0, nmax, gx[i], S.bw + j0, S.bd + j0, nj, fk);
-          }
-          if (nquad >= 32) {
-            // the 32 items of a round have distinct angles
-            if (ia >= 0) {
-              S.sump[0][ia] += fk[0];
-              S.sump[1][ia] += fk[1];
-              S.sump[2][ia] += fk[2];
-            }
-          } else {
-            // angles repeat within the round: lane i adds the items of angle i in lane order
-            S.stg[0][lane] = fk[0];
-            S.stg[1][lane] = fk[1];
-            S.stg[2][lane] = fk[2];
-            S.sti[lane] = ia;
-            __syncwarp();
-            if (lane < nquad) {
-              double a0 = S.sump[0][lane], a1 = S.sump[1][lane], a2 = S.sump[2][lane];
-              for (int L = 0; L < 32; L++)
-                if (S.sti[L] == lane) { a0 += S.stg[0][L]; a1 += S.stg[1][L]; a2 += S.stg[2][L]; }
-              S.sump[0][lane] = a0;
-              S.sump[1][lane] = a1;
-              S.sump[2][lane] = a2;
-            }
-          }
-          __syncwarp();
-        }
+        // ---- phase B: the phase-function sums of the pass
+        mie_pass_sums(S, slab, ldc, cb, nquad, gx);
       }
       sqe = warp_sum(sqe);
       sqs = warp_sum(sqs);
