@@ -56,8 +56,8 @@ def _args():
     ap.add_argument("--serve-requests", type=int, default=200, help="requests in the serving replay (0 = skip)")
     ap.add_argument("--serve-plain", type=int, default=30, help="requests of the stream served by the plain form")
     ap.add_argument("--target-cols", type=int, default=1024, help="columns of the 150-layer target batch (0 = skip)")
-    ap.add_argument("--uneven-cols", type=int, default=2048, help="columns of the uneven batch (0 = skip)")
-    ap.add_argument("--mieheavy-cols", type=int, default=1024, help="columns of the Mie-heavy batch (0 = skip)")
+    ap.add_argument("--uneven-cols", type=int, default=16384, help="columns of the uneven batch (0 = skip)")
+    ap.add_argument("--mieheavy-cols", type=int, default=2048, help="columns of the Mie-heavy batch (0 = skip)")
     return ap.parse_args()
 
 
@@ -81,6 +81,65 @@ def _oracle_chunk(task):
         err, tb, _, _, _ = oracle.run_column(st, species, cols, c, freqs)
         out.append((c, err, tb))
     return out, time.perf_counter() - t0
+
+
+def _oracle_packed(task):
+    """Oracle TB of columns of a small packed batch with per-column NUMMU,
+    frequency lists and species (the worker side of oracle_tb_errors)."""
+    st_fields, species, stride, host, cols = task
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    out = []
+    H = int(host["nhydro"])
+    for c in cols:
+        st = oracle.OrcSettings(**st_fields)
+        if host.get("nummu") is not None:
+            st.nummu = int(host["nummu"][c])
+        sp = species[c * H:(c + 1) * H] if stride else species
+        freqs = list(host["freqs"][c, :int(host["nfreq"][c])]) if host.get("nfreq") is not None \
+            else list(host["freqs"])
+        err, tb, _, _, _ = oracle.run_column(st, sp, host, c, freqs)
+        out.append((c, err, tb, int(st.nummu), len(freqs)))
+    return out
+
+
+def oracle_sample(b, k=8):
+    """Columns of ``b`` for the oracle check: the cheapest ones of each NUMMU
+    (CPU cost ~ N^3 x layers x frequencies), up to ``k`` in all."""
+    h = b.host
+    C = b.ncol
+    nmu = np.asarray(h["nummu"]) if h.get("nummu") is not None else np.full(C, b.max_nummu)
+    nf = np.asarray(h["nfreq"]) if h.get("nfreq") is not None else np.full(C, int(h["max_nfreq"]))
+    cost = nmu.astype(np.float64) ** 3 * np.asarray(h["nlyrs"]) * nf
+    picks = []
+    for N, quota in ((8, k // 2), (16, k // 4 + (k % 4 > 0)), (32, max(1, k // 8))):
+        cand = np.nonzero(nmu == N)[0]
+        picks += cand[np.argsort(cost[cand])][:quota].tolist()
+    if len(picks) < k:
+        rest = [int(c) for c in np.argsort(cost) if int(c) not in picks]
+        picks += rest[:k - len(picks)]
+    return sorted(picks[:k])
+
+
+def oracle_tb_errors(b, idxs, tbs, pool):
+    """Max |TB - oracle TB| (K) over the columns ``idxs`` for each TB array
+    in ``tbs`` (name -> [C][nout][2N][F][2]); one oracle task per column."""
+    from pamtra_b200 import batch as pbatch
+    sub = pbatch.subset(b, idxs)
+    st_fields = {k: getattr(b.settings, k) for k, _ in b.settings._fields_}
+    tasks = [(st_fields, sub.species, sub.species_stride, sub.host, [j]) for j in range(len(idxs))]
+    res = pool.map(_oracle_packed, tasks)
+    errs = {name: 0.0 for name in tbs}
+    bad = 0
+    for out in res:
+        for j, err, tb, N, nf in out:
+            if err:
+                bad += 1
+                continue
+            c = idxs[j]
+            for name, t in tbs.items():
+                errs[name] = max(errs[name], float(np.max(np.abs(t[c][:, :2 * N, :nf, :] - tb))))
+    return errs, bad
 
 
 def make_pool(cores):
@@ -318,46 +377,63 @@ def _target_shape(args, local, eng, stream):
                      "reference operation order (PREC_FP64)"}
 
 
-def _config_line(name, b, local, eng, stream, nplain=8, reps=2):
-    """Batched FP64 and split-precision solves/s on one workload (tuned launch
-    shapes, device-timed, L2 flushed) against the plain form (one column per
-    call, reference order) on its first ``nplain`` columns.  A batch whose
-    scratch exceeds a third of the free device memory runs as NUMMU-grouped
-    chunks (batch.chunk_columns), one after another inside each timed step."""
+def _config_line(name, b, local, eng, stream, pool, nplain=8, reps=1, noracle=8):
+    """Batched FP64 and split-precision solves/s on one workload at its
+    stated size (default launch shapes, device-timed, L2 flushed) against the
+    plain form (one column per call, reference order) on its first
+    ``nplain`` columns, with the TB error of both batched forms against the
+    oracle on ``noracle`` sampled columns.  A batch whose scratch exceeds a
+    third of the free device memory runs as NUMMU-grouped chunks
+    (batch.chunk_columns), one after another inside each timed step."""
     import torch
     from pamtra_b200 import autotune
     from pamtra_b200 import batch as pbatch
     from pamtra_b200._native import PREC_3XTF32, PREC_FP64_BATCHED
     dev = torch.device("cuda", local)
+    eng.set_launch(autotune.DEFAULT)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
     free, _ = torch.cuda.mem_get_info(dev)
-    chunks = [pbatch.subset(b, idx) for idx in pbatch.chunk_columns(b, free // 3)]
-    res = {"unit": "solves/s", "columns": b.ncol, "solves_per_step": b.n_solves(), "chunks": len(chunks)}
-    tbs = {}
+    idx_chunks = pbatch.chunk_columns(b, free // 3)
+    res = {"unit": "solves/s", "columns": b.ncol, "solves_per_step": b.n_solves(), "chunks": len(idx_chunks),
+           "launch_shape": list(autotune.DEFAULT)}
+    full = {}
     for label, prec in (("batched_fp64", PREC_FP64_BATCHED), ("batched_3xtf32", PREC_3XTF32)):
-        outs = [cb.alloc_outputs(dev) for cb in chunks]
-        for cb, o in zip(chunks, outs):  # tune each chunk signature once, untimed
-            autotune.apply(cb, local, precision=prec, eng=eng, stream=stream, outputs=o, reps=1)
-            pbatch.run(cb, local, o, precision=prec, stream=stream, eng=eng)
+        # untimed warm-up on the first chunk (arena, tables)
+        cb0 = pbatch.subset(b, idx_chunks[0])
+        pbatch.run(cb0, local, cb0.alloc_outputs(dev), precision=prec, stream=stream, eng=eng)
         stream.synchronize()
         ms = []
+        tb_full = None
         for _ in range(reps):
             with torch.cuda.stream(stream):
                 flush.zero_()
+            stream.synchronize()
+            tot = 0.0
+            parts = []
+            for idx in idx_chunks:
+                cb = pbatch.subset(b, idx)
+                o = cb.alloc_outputs(dev)
+                arrs = cb.device_arrays(dev)  # inputs resident before the timed launch
+                torch.cuda.synchronize(dev)
                 s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 s0.record(stream)
-                for cb, o in zip(chunks, outs):
-                    autotune.apply(cb, local, precision=prec, eng=eng)
-                    pbatch.run(cb, local, o, precision=prec, stream=stream, eng=eng)
+                pbatch.run(cb, local, o, precision=prec, stream=stream, eng=eng)
                 e0.record(stream)
-            e0.synchronize()
-            ms.append(s0.elapsed_time(e0))
+                e0.synchronize()
+                tot += s0.elapsed_time(e0)
+                parts.append((idx, o["tb"].cpu().numpy(), int((o["status"] != 0).sum())))
+                del o, arrs
+                cb._dev = None
+            ms.append(tot)
+            tb_full = parts
         res[label] = b.n_solves() / (np.mean(ms) * 1e-3)
         res[label + "_ms_per_step"] = float(np.mean(ms))
-        tbs[label] = [o["tb"].cpu().numpy() for o in outs]
-        res[label + "_status_nonzero"] = int(sum(int((o["status"] != 0).sum()) for o in outs))
-        del outs
-    eng.set_launch(autotune.DEFAULT)
+        res[label + "_status_nonzero"] = int(sum(p[2] for p in tb_full))
+        C, nout, F, N = b.ncol, int(b.host["noutlevels"]), int(b.host["max_nfreq"]), b.max_nummu
+        tb = np.full((C, nout, 2 * N, F, 2), -9999.0)
+        for idx, t, _ in tb_full:
+            tb[idx, :, :t.shape[2], :t.shape[3], :] = t
+        full[label] = tb
     singles = [pbatch.subset(b, [c]) for c in range(nplain)]
     souts = [sb.alloc_outputs(dev) for sb in singles]
     for sb, so in zip(singles, souts):
@@ -374,12 +450,15 @@ def _config_line(name, b, local, eng, stream, nplain=8, reps=2):
     res["plain_sample_columns"] = nplain
     res["batched_fp64_over_plain"] = res["batched_fp64"] / res["plain_fp64"]
     res["batched_3xtf32_over_plain"] = res["batched_3xtf32"] / res["plain_fp64"]
-    err = 0.0
-    for a, c in zip(tbs["batched_3xtf32"], tbs["batched_fp64"]):
-        ok = c > -9000
-        if np.any(ok):
-            err = max(err, float(np.max(np.abs(a - c)[ok])))
-    res["tb_err_3xtf32_vs_fp64_K"] = err
+    a3, a64 = full["batched_3xtf32"], full["batched_fp64"]
+    ok = a64 > -9000
+    res["tb_err_3xtf32_vs_fp64_K"] = float(np.max(np.abs(a3 - a64)[ok])) if np.any(ok) else None
+    if pool is not None and noracle > 0:
+        idxs = oracle_sample(b, noracle)
+        errs, bad = oracle_tb_errors(b, idxs, {"fp64": a64, "3xtf32": a3}, pool)
+        res["tb_err_vs_oracle_K"] = {"batched_fp64": errs["fp64"], "batched_3xtf32": errs["3xtf32"],
+                                     "columns": idxs, "oracle_errors": bad,
+                                     "sample": "the cheapest columns of each NUMMU for the CPU oracle"}
     res["workload"] = name
     del flush
     return res
@@ -608,16 +687,19 @@ def main():
             dist.barrier()
             dist.destroy_process_group()
         return
+    # one spawned pool of oracle workers for the CPU baseline and the oracle checks
+    cores = os.cpu_count() or 1
+    pool = make_pool(cores) if not args.no_cpu else None
     target = _target_shape(args, local, eng, stream) if args.target_cols > 0 else None
     from pamtra_b200 import workloads as wl
     uneven = _config_line("%d columns, layers uniform 40-150, 1-5 species (cloud water, cloud ice, snow, graupel, "
                           "rain; exp or mgamma with mu 0-4; 20-80 bins; ice 100-900 kg/m3), 8-32 frequencies in "
                           "10-183 GHz, NUMMU 8/16/32 per column" % args.uneven_cols,
-                          wl.uneven_batch(args.uneven_cols, seed=3), local, eng, stream) \
+                          wl.uneven_batch(args.uneven_cols, seed=3), local, eng, stream, pool) \
         if args.uneven_cols > 0 else None
     mieheavy = _config_line("%d columns x 100 layers, 4 species x 200 bins up to 10 mm (rain, snow, graupel, "
                             "cloud ice), f = 89/157/176.31/190.31 GHz, NUMMU 16" % args.mieheavy_cols,
-                            wl.mie_heavy_batch(args.mieheavy_cols, seed=6), local, eng, stream) \
+                            wl.mie_heavy_batch(args.mieheavy_cols, seed=6), local, eng, stream, pool) \
         if args.mieheavy_cols > 0 else None
     serving = _serving(args, local) if args.serve_requests > 0 else None
     # ---- roofline of the dominant kernel (doubling stage)
@@ -645,11 +727,9 @@ def main():
     cpu = None
     tb_err = None
     split_err_oracle = None
-    if not args.no_cpu:
-        cores = os.cpu_count() or 1
+    if pool is not None:
         nsamp = args.cpu_sample or min(b.ncol, 8 * cores)
         idxs = sorted(np.random.default_rng(7).choice(b.ncol, size=nsamp, replace=False).tolist())
-        pool = make_pool(cores)
         cval, wall, tbs = cpu_baseline(b, idxs, FREQS, cores, pool)
         pool.close()
         one_val, one_wall = cpu_single_core(b, idxs[:max(2, nsamp // (2 * cores))], FREQS)
@@ -695,14 +775,41 @@ def main():
                          "form": "doubling products as 3xTF32 tcgen05 MMAs (FP32 accumulation in TMEM); "
                                  "thin-layer init, adding and surface in FP64"},
         "stage_ms": {k: v / args.steps for k, v in stage_tot.items()},
+        "serving": serving,
         "target_shape": target,
-        "target_batched_fp64_over_plain": target["batched_over_plain"] if target else None,
-        "target_batched_3xtf32_over_plain": target["batched_3xtf32_over_plain"] if target else None,
-        "c2_3xtf32_over_fp64": split_value / value if value else None,
         "uneven": uneven,
         "mie_heavy": mieheavy,
-        "serving": serving,
         "status_nonzero": int(np.count_nonzero(status)),
+    }
+
+    def g(d, *ks):
+        for k in ks:
+            if d is None:
+                return None
+            d = d.get(k)
+        return d
+    # the figures that matter, last on the line
+    line["summary"] = {
+        "c2_batched_fp64": value, "c2_batched_3xtf32": split_value, "c2_plain_fp64": plain_value,
+        "c2_fp64_over_plain": value / world / plain_value, "c2_3xtf32_over_fp64": split_value / value,
+        "c2_tb_err_vs_oracle_K": {"fp64": tb_err, "3xtf32": split_err_oracle},
+        "target_fp64_over_plain": g(target, "batched_over_plain"),
+        "target_3xtf32_over_plain": g(target, "batched_3xtf32_over_plain"),
+        "target_3xtf32_over_fp64": (target["batched_3xtf32"] / target["batched_fp64"]) if target else None,
+        "uneven_cols": g(uneven, "columns"), "uneven_fp64": g(uneven, "batched_fp64"),
+        "uneven_3xtf32": g(uneven, "batched_3xtf32"), "uneven_3xtf32_over_plain": g(uneven, "batched_3xtf32_over_plain"),
+        "uneven_tb_err_vs_oracle_K": g(uneven, "tb_err_vs_oracle_K"),
+        "mieheavy_cols": g(mieheavy, "columns"), "mieheavy_fp64": g(mieheavy, "batched_fp64"),
+        "mieheavy_3xtf32": g(mieheavy, "batched_3xtf32"),
+        "mieheavy_3xtf32_over_plain": g(mieheavy, "batched_3xtf32_over_plain"),
+        "mieheavy_tb_err_vs_oracle_K": g(mieheavy, "tb_err_vs_oracle_K"),
+        "serving_3xtf32_rate200_p50_p99_ms": [g(serving, "batched_3xtf32", "rate_200", "p50_ms"),
+                                              g(serving, "batched_3xtf32", "rate_200", "p99_ms")],
+        "serving_3xtf32_halfcap_p50_p99_ms": [g(serving, "batched_3xtf32", "rate_half_capacity", "p50_ms"),
+                                              g(serving, "batched_3xtf32", "rate_half_capacity", "p99_ms")],
+        "serving_solves_per_s": {"3xtf32": g(serving, "batched_3xtf32", "rate_200", "solves_per_s"),
+                                 "fp64": g(serving, "batched_fp64", "rate_200", "solves_per_s"),
+                                 "plain": g(serving, "plain_fp64", "rate_200", "solves_per_s")},
     }
     print(json.dumps(line))
     if dist is not None:

@@ -53,6 +53,7 @@ struct LayerSmem {
   static constexpr int n = RTCfg<N>::n, MAT = RTCfg<N>::MAT;
   double m[5][MAT];  // R, T, G, W, Y; during scatcnv G (and W) hold the coefficients, Y the azimuth table
   double lin[2 * n], cst[2 * n];
+  double lin2[2 * n], cst2[2 * n];  // the other half of the doubled source buffers
   double v[4][n], u[4][n];
   double mu[N], wq[N], nrm[N];
   InvScratch<n> inv;
@@ -402,19 +403,24 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
     // ---------------- DOUBLING_INTEGRATION4, SYMMETRIC (src/radintg4.f90:174-309)
     // R' = R + T G R T and T' = T G T with G = (I - R R)^-1, as five products
     // per step: W = T G, then R' = R + W (R T) and T' = W T; the source
-    // chains use W u for T G u.
+    // chains use W u for T G u.  R R and R T only read R and T, so they
+    // share the first phase.
     constexpr int NV = (4 * n + T - 1) / T;
     int nprod = 5 * nd;  // n x n products issued for this item (counted by thread 0)
+    // sources S+ / S- (linear and constant parts), double-buffered so that a
+    // step writes the new ones while other threads still read the old
+    double *lin = S.lin, *cst = S.cst, *lin_n = S.lin2, *cst_n = S.cst2;
     for (int itd = 0; itd < nd; itd++) {
       mm<n, MM_SET>(Rb, Rb, Gb);  // R+ R-
+      mm<n, MM_SET>(Rb, Tb, Yb);  // Y = R T
       // v = [S- + f C-, C-, S+, C+]
       for (int o = t; o < 4 * n; o += T) {
         const int r = o % n, k = o / n;
         double v;
-        if (k == 0) v = S.lin[n + r] + linfac * S.cst[n + r];
-        else if (k == 1) v = S.cst[n + r];
-        else if (k == 2) v = S.lin[r];
-        else v = S.cst[r];
+        if (k == 0) v = lin[n + r] + linfac * cst[n + r];
+        else if (k == 1) v = cst[n + r];
+        else if (k == 2) v = lin[r];
+        else v = cst[r];
         S.v[k][r] = v;
       }
       team_sync();
@@ -430,48 +436,36 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
         const int r = o % n, k = o / n;
         const double a = mv_row<n>(Rb, S.v[k], r);
         double u;
-        if (k == 0) u = S.lin[r] + a;
-        else if (k == 1) u = S.cst[r] + a;
+        if (k == 0) u = lin[r] + a;
+        else if (k == 1) u = cst[r] + a;
         else if (k == 2) u = S.v[0][r] + a;
-        else u = S.cst[n + r] + a;
+        else u = cst[n + r] + a;
         S.u[k][r] = u;
       }
       team_sync();
-      // Y = R T;  new sources from W u
-      mm<n, MM_SET>(Rb, Tb, Yb);
-      double onew[NV];
+      // new sources from W u, then R' = R + W Y and T' = W T (into the G
+      // buffer): nothing of this phase reads what it writes
 #pragma unroll
       for (int s = 0; s < NV; s++) {
         const int o = t + s * T;
         if (o < 4 * n) {
           const int r = o % n, k = o / n;
           const double a = mv_row<n>(Wb, S.u[k], r);
-          if (k == 0) onew[s] = (S.lin[r] + a) + linfac * S.cst[r];
-          else if (k == 1) onew[s] = S.cst[r] + a;
-          else if (k == 2) onew[s] = S.lin[n + r] + a;
-          else onew[s] = S.cst[n + r] + a;
+          if (k == 0) lin_n[r] = (lin[r] + a) + linfac * cst[r];
+          else if (k == 1) cst_n[r] = cst[r] + a;
+          else if (k == 2) lin_n[n + r] = lin[n + r] + a;
+          else cst_n[n + r] = cst[n + r] + a;
         }
       }
-      team_sync();
-      // R' = R + W Y;  T' = W T (into the G buffer)
       mm<n, MM_ACC>(Wb, Yb, Rb, Rb);
       mm<n, MM_SET>(Wb, Tb, Gb);
-#pragma unroll
-      for (int s = 0; s < NV; s++) {
-        const int o = t + s * T;
-        if (o < 4 * n) {
-          const int r = o % n, k = o / n;
-          if (k == 0) S.lin[r] = onew[s];
-          else if (k == 1) S.cst[r] = onew[s];
-          else if (k == 2) S.lin[n + r] = onew[s];
-          else S.cst[n + r] = onew[s];
-        }
-      }
       { double* tmp = Tb; Tb = Gb; Gb = tmp; }
+      { double* tmp = lin; lin = lin_n; lin_n = tmp; }
+      { double* tmp = cst; cst = cst_n; cst_n = tmp; }
       linfac = 2.0 * linfac;
       team_sync();
     }
-    layer_store<N>(w, item, Rb, Tb, S.lin);
+    layer_store<N>(w, item, Rb, Tb, lin);
     if (t == 0) {
       w.lay_nd[item] = nd;
       if (status) atomicOr(&w.status[(size_t)c * Fm + fi], status);
@@ -592,10 +586,8 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
           }
         } else {
           // general stack + clear layer
-          if (t < n) {
-            S.nsp[t] = S.s2p[t] + S.t2[t] * (S.sp[t] + mv_row<n>(Rp, S.s2m, t));
-            S.nsm[t] = S.sm[t] + mv_row<n>(Tm, S.s2m, t);
-          }
+          if (t < n) S.nsp[t] = S.s2p[t] + S.t2[t] * (S.sp[t] + mv_row<n>(Rp, S.s2m, t));
+          else if (t < 2 * n) S.nsm[t - n] = S.sm[t - n] + mv_row<n>(Tm, S.s2m, t - n);
           team_sync();
           for (int e = t; e < n * n; e += T) {
             const int col = e / n, row = e % n, a = col * LD + row;
@@ -625,10 +617,8 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
       }
       if (sstate == 1) {
         // clear stack (t1, sp, sm) + scattering layer
-        if (t < n) {
-          S.nsp[t] = S.s2p[t] + mv_row<n>(T2, S.sp, t);
-          S.nsm[t] = S.sm[t] + S.t1[t] * (S.s2m[t] + mv_row<n>(R2, S.sp, t));
-        }
+        if (t < n) S.nsp[t] = S.s2p[t] + mv_row<n>(T2, S.sp, t);
+        else if (t < 2 * n) S.nsm[t - n] = S.sm[t - n] + S.t1[t - n] * (S.s2m[t - n] + mv_row<n>(R2, S.sp, t - n));
         for (int e = t; e < n * n; e += T) {
           const int col = e / n, row = e % n, a = col * LD + row;
           const double t1i = S.t1[row], t1j = S.t1[col];
@@ -661,22 +651,17 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
           if (gi != G) { X = G; G = gi; }
         }
         mm<n, MM_SET>(Rp, T2, X);  // R1p T2
-        if (t < n) {
-          S.wv[t] = S.sp[t] + mv_row<n>(Rp, S.s2m, t);   // S+ chain
-          S.nsm[t] = S.s2m[t] + mv_row<n>(R2, S.sp, t);  // S- chain: w
-        }
+        // the two chains of a phase run on different warps
+        if (t < n) S.wv[t] = S.sp[t] + mv_row<n>(Rp, S.s2m, t);                    // S+ chain
+        else if (t < 2 * n) S.nsm[t - n] = S.s2m[t - n] + mv_row<n>(R2, S.sp, t - n);  // S- chain: w
         team_sync();
         mm<n, MM_SET>(G, X, Y);  // Y = Gp R1p T2
-        if (t < n) {
-          S.wv2[t] = mv_row<n>(G, S.wv, t);
-          S.u1[t] = mv_row<n>(Rp, S.nsm, t);
-        }
+        if (t < n) S.wv2[t] = mv_row<n>(G, S.wv, t);
+        else if (t < 2 * n) S.u1[t - n] = mv_row<n>(Rp, S.nsm, t - n);
         team_sync();
         mm<n, MM_ACC>(T2, Y, Z, R2);  // new R+ = R2 + T2 Gp R1p T2
-        if (t < n) {
-          S.nsp[t] = S.s2p[t] + mv_row<n>(T2, S.wv2, t);
-          S.u2[t] = mv_row<n>(G, S.u1, t);
-        }
+        if (t < n) S.nsp[t] = S.s2p[t] + mv_row<n>(T2, S.wv2, t);
+        else if (t < 2 * n) S.u2[t - n] = mv_row<n>(G, S.u1, t - n);
         team_sync();
         mm<n, MM_SET>(G, Tp, X);  // W = Gp T1p
         if (t < n) S.u1[t] = S.nsm[t] + mv_row<n>(R2, S.u2, t);  // Gm w
