@@ -67,7 +67,9 @@ extern "C" {
                                            combine; the plain drop-in form */
 #define PAMTRA_B200_PREC_3XTF32 1        /* batched form: layer doubling products as 3xTF32 tcgen05
                                            MMAs (NUMMU 16 and 32; NUMMU 8 doubles in FP64), FP64
-                                           adding with one inverse per combine */
+                                           adding with one inverse per combine; the Legendre
+                                           coefficients of the phase matrices are stored in FP32
+                                           (computed and expanded in FP64) */
 #define PAMTRA_B200_PREC_FP64_BATCHED 2  /* batched form in FP64: as PREC_FP64, but each adding
                                            combine derives the minus-side inverse from the
                                            plus-side one (Gm R2 = R2 Gp, Gm = I + R2 Gp R1p):
@@ -213,8 +215,10 @@ int32_t pamtra_b200_run_host(pamtra_b200_ctx* ctx, const pamtra_b200_settings* s
  * autotuner (pamtra_b200/autotune.py); no counterpart in the reference, whose
  * Fortran has no launch configuration.  params[0]: warps per Mie CTA (2, 4 or
  * 8; 0 = 4), params[1..3]: CTAs per SM of the Mie, layer and adding kernels
- * (0 = as many as fit).  Results do not depend on the launch shape. */
-#define PAMTRA_B200_NLAUNCH 4
+ * (0 = as many as fit), params[4]: size bins per Mie work item, the tile of
+ * the phase-function sums (4 or 8; 0 = 4).  Results do not depend on the
+ * launch shape. */
+#define PAMTRA_B200_NLAUNCH 5
 int32_t pamtra_b200_set_launch(pamtra_b200_ctx* ctx, const int32_t* params, int32_t n);
 int32_t pamtra_b200_get_launch(const pamtra_b200_ctx* ctx, int32_t* params, int32_t n);
 

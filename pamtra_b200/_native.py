@@ -62,7 +62,7 @@ EXPORTS = ["pamtra_b200_create", "pamtra_b200_destroy", "pamtra_b200_workspace_b
            "pamtra_b200_graph_capture", "pamtra_b200_graph_launch", "pamtra_b200_graph_destroy",
            "pamtra_b200_get_eps_water", "pamtra_b200_gas_l93", "pamtra_b200_set_wait_limit",
            "pamtra_b200_layer_products"]
-NLAUNCH = 4  # PAMTRA_B200_NLAUNCH: mie warps per CTA, mie / layer / adding CTAs per SM
+NLAUNCH = 5  # PAMTRA_B200_NLAUNCH: mie warps per CTA, mie / layer / adding CTAs per SM, mie bins per item
 STAGES = ["prep", "psd", "mie", "layer", "adding"]
 
 _lib = None
@@ -210,7 +210,7 @@ class Engine(object):
 
     def set_launch(self, params):
         """Launch shapes of the persistent kernels: (mie warps per CTA, mie /
-        layer / adding CTAs per SM), 0 = default."""
+        layer / adding CTAs per SM, mie bins per work item), 0 = default."""
         arr = (_i32 * NLAUNCH)(*[int(v) for v in params])
         if self.lib.pamtra_b200_set_launch(self.handle, arr, len(params)) != 0:
             raise ValueError("invalid launch shape %r" % (tuple(params),))

@@ -7,8 +7,11 @@ precision, and power-of-two buckets of columns, layers, frequencies and
 species) the tuner times candidate shapes with the library's per-stage CUDA
 events and keeps, stage by stage, the fastest:
 
-* Mie: warps per CTA (2, 4, 8) and CTAs per SM,
-* layer doubling: CTAs per SM,
+* Mie: warps per CTA (2, 4, 8), CTAs per SM, and the tile of its
+  phase-function sums (size bins per work item: 4 or 8, two compiled
+  instantiations of the kernel),
+* layer doubling: CTAs per SM (FP64 teams, or item pairs of the
+  split-precision kernel),
 * adding: CTAs per SM,
 
 The stages are separate kernels, so one timed run per candidate row measures
@@ -29,16 +32,18 @@ import numpy as np
 
 from ._native import PREC_FP64, engine
 
-# candidate rows: (mie warps, mie CTAs/SM, layer CTAs/SM, adding CTAs/SM); 0 = as many as fit
+# candidate rows: (mie warps, mie CTAs/SM, layer CTAs/SM, adding CTAs/SM, mie bins per work
+# item); 0 = as many as fit (CTAs) or the default (warps, bins)
 CANDIDATES = [
-    (4, 0, 0, 0),
-    (8, 0, 1, 1),
-    (2, 0, 2, 0),
-    (4, 2, 3, 1),
-    (8, 1, 0, 0),
+    (4, 0, 0, 0, 4),
+    (8, 0, 1, 1, 8),
+    (2, 0, 2, 0, 4),
+    (4, 2, 3, 1, 8),
+    (8, 1, 0, 0, 4),
+    (4, 0, 0, 2, 8),
 ]
-STAGE_KNOBS = {"mie": (0, 1), "layer": (2,), "adding": (3,)}
-DEFAULT = (4, 0, 0, 0)
+STAGE_KNOBS = {"mie": (0, 1, 4), "layer": (2,), "adding": (3,)}
+DEFAULT = (4, 0, 0, 0, 4)
 
 _cache = {}
 

@@ -239,6 +239,7 @@ struct Plan {
       o_colst;
   size_t o_species, o_addscr, o_mieslab;
   int mie_nslab;  // k_mie warps the slabs are sized for
+  bool f32_coef;
   int add_grid;  // CTAs of k_adding<32> the scratch is sized for
   int pmax;
   int max_nbin;
@@ -250,7 +251,7 @@ size_t lay_stride_for(int N) {
   return (lay_stride_n(N) + 1) & ~(size_t)1;  // keep 16-byte alignment of each item
 }
 
-Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms, int mie_slabs) {
+Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms, int mie_slabs, bool f32_coef = false) {
   Plan p{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -296,7 +297,8 @@ Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms, int mie
   p.o_mback = take(items * 8);
   p.o_mrefr = take(items * 4 * 8);
   p.o_mnleg = take(items * 4);
-  p.o_mlegen = take(items * 3 * MAXNLEG * 8);
+  p.f32_coef = f32_coef;  // Legendre coefficients stored in FP32 (split-precision form)
+  p.o_mlegen = take(items * 3 * MAXNLEG * (f32_coef ? 4 : 8));
   p.o_lay = take(items * p.lay_stride * 8);
   p.o_laynd = take(items * 4);
   p.o_status = take(C * Fm * 4);
@@ -306,7 +308,7 @@ Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms, int mie
   p.o_addscr = take((size_t)p.add_grid * (10 - AddSmem<32>::NS) * RTCfg<32>::MAT * 8);
   // one slab per k_mie warp; more warps than (layer, frequency) items would idle
   p.mie_nslab = c->nhydro > 0 ? (int)std::min<size_t>((size_t)mie_slabs, items) : 0;
-  p.o_mieslab = take((size_t)p.mie_nslab * MIE_SLAB * 8);
+  p.o_mieslab = take((size_t)p.mie_nslab * MIE_SLAB_STRIDE * 8);
   p.total = take(0) + 256;
   return p;
 }
@@ -456,6 +458,7 @@ struct pamtra_b200_ctx {
   int mie_cps = 0;            // k_mie CTAs per SM
   int layer_cps = 0;          // k_layer / k_layer_tc CTAs per SM
   int adding_cps = 0;         // k_adding CTAs per SM
+  int mie_group = MIE_GROUP;  // bins per k_mie work item (4 or 8)
   uint32_t spin_limit = tc::MBAR_SPIN_LIMIT;  // polls per wait on a tensor-core MMA
   const int* last_counters = nullptr;          // work counters of the last run (in the arena)
   // optional per-stage timing (events recorded on the run's stream)
@@ -495,7 +498,8 @@ static int set_smem_attrs() {
     auto set = [](const void* f, size_t bytes) {
       if (cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess) rc = 1;
     };
-    set((const void*)k_mie, MIE_MAX_WARPS * sizeof(MieSmem));
+    set((const void*)k_mie<4>, MIE_MAX_WARPS * sizeof(MieSmem));
+    set((const void*)k_mie<8>, MIE_MAX_WARPS * sizeof(MieSmem));
     set((const void*)k_layer<8>, sizeof(LayerSmem<8>));
     set((const void*)k_layer<16>, sizeof(LayerSmem<16>));
     set((const void*)k_layer<32>, sizeof(LayerSmem<32>));
@@ -584,11 +588,10 @@ int32_t pamtra_b200_destroy(pamtra_b200_ctx* ctx) {
 }
 
 size_t pamtra_b200_workspace_bytes(const pamtra_b200_columns* cols, int32_t precision) {
-  (void)precision;
   if (!cols || !cols->species) return 0;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return make_plan(cols, 16, sms, sms * MIE_SLAB_WARPS_PER_SM).total;
+  return make_plan(cols, 16, sms, sms * MIE_SLAB_WARPS_PER_SM, precision == PAMTRA_B200_PREC_3XTF32).total;
 }
 
 int32_t pamtra_b200_reserve(pamtra_b200_ctx* ctx, size_t bytes) {
@@ -685,21 +688,24 @@ int32_t pamtra_b200_abi_sizes(size_t* out, int32_t n) {
 
 int32_t pamtra_b200_set_launch(pamtra_b200_ctx* ctx, const int32_t* params, int32_t n) {
   if (!ctx || (n > 0 && !params) || n < 0 || n > PAMTRA_B200_NLAUNCH) return PAMTRA_B200_FATAL;
-  int v[PAMTRA_B200_NLAUNCH] = {MIE_WARPS, 0, 0, 0};
+  int v[PAMTRA_B200_NLAUNCH] = {MIE_WARPS, 0, 0, 0, 0};
   for (int i = 0; i < n; i++) v[i] = params[i];
   if (!(v[0] == 0 || v[0] == 2 || v[0] == 4 || v[0] == 8)) return PAMTRA_B200_FATAL;
-  for (int i = 1; i < PAMTRA_B200_NLAUNCH; i++)
+  for (int i = 1; i < 4; i++)
     if (v[i] < 0 || v[i] > 32) return PAMTRA_B200_FATAL;
+  if (!(v[4] == 0 || v[4] == 4 || v[4] == 8)) return PAMTRA_B200_FATAL;
   ctx->mie_warps = v[0] ? v[0] : MIE_WARPS;
   ctx->mie_cps = v[1];
   ctx->layer_cps = v[2];
   ctx->adding_cps = v[3];
+  ctx->mie_group = v[4] ? v[4] : MIE_GROUP;
   return PAMTRA_B200_OK;
 }
 
 int32_t pamtra_b200_get_launch(const pamtra_b200_ctx* ctx, int32_t* params, int32_t n) {
   if (!ctx || !params || n < 0) return PAMTRA_B200_FATAL;
-  const int v[PAMTRA_B200_NLAUNCH] = {ctx->mie_warps, ctx->mie_cps, ctx->layer_cps, ctx->adding_cps};
+  const int v[PAMTRA_B200_NLAUNCH] = {ctx->mie_warps, ctx->mie_cps, ctx->layer_cps, ctx->adding_cps,
+                                     ctx->mie_group};
   for (int i = 0; i < n && i < PAMTRA_B200_NLAUNCH; i++) params[i] = v[i];
   return PAMTRA_B200_OK;
 }
@@ -770,7 +776,8 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   pamtra_b200_species dummy{};
   pamtra_b200_columns cc = *cols;
   if (cc.nhydro == 0) { cc.species = &dummy; cc.species_stride = 0; }
-  Plan pl = make_plan(&cc, st->nummu, ctx->sm_count, ctx->sm_count * MIE_SLAB_WARPS_PER_SM);
+  Plan pl = make_plan(&cc, st->nummu, ctx->sm_count, ctx->sm_count * MIE_SLAB_WARPS_PER_SM,
+                      precision == PAMTRA_B200_PREC_3XTF32);
   if (pl.max_nbin > MAXBIN) return PAMTRA_B200_FATAL;
   if (pl.total > ctx->arena_bytes) {
     cudaStreamSynchronize(stream);
@@ -837,7 +844,8 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   w.counters = (int*)(A + pl.o_counters);
   w.m_kext = (double*)(A + pl.o_mkext); w.m_salb = (double*)(A + pl.o_msalb); w.m_nleg = (int*)(A + pl.o_mnleg);
   w.m_back = (double*)(A + pl.o_mback); w.m_refr = (double*)(A + pl.o_mrefr);
-  w.m_legen = (double*)(A + pl.o_mlegen);
+  w.m_legen = pl.f32_coef ? nullptr : (double*)(A + pl.o_mlegen);
+  w.m_legen32 = pl.f32_coef ? (float*)(A + pl.o_mlegen) : nullptr;
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
   w.add_scr = (double*)(A + pl.o_addscr);
@@ -896,11 +904,13 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   if (H > 0) {
     const int mw = ctx->mie_warps;
     const size_t sm_mie = mw * sizeof(MieSmem);
-    int g = std::min(persistent_grid((const void*)k_mie, 32 * mw, sm_mie, sms, ctx->mie_cps),
-                     std::max(1, pl.mie_nslab / mw));
+    const void* kmie = ctx->mie_group == 8 ? (const void*)k_mie<8> : (const void*)k_mie<4>;
+    int g = std::min(persistent_grid(kmie, 32 * mw, sm_mie, sms, ctx->mie_cps), std::max(1, pl.mie_nslab / mw));
     const size_t nref = (size_t)std::max(1, pl.pmax) * Fm;
     k_refr<<<(unsigned)((nref + 127) / 128), 128, 0, stream>>>(b, w, *st); launches++;
-    k_mie<<<g, 32 * mw, sm_mie, stream>>>(b, w, *st); launches++;
+    if (ctx->mie_group == 8) k_mie<8><<<g, 32 * mw, sm_mie, stream>>>(b, w, *st);
+    else k_mie<4><<<g, 32 * mw, sm_mie, stream>>>(b, w, *st);
+    launches++;
     if (w.wtab[0] && (mask & 1)) {
       k_scat_weights<8><<<SCAT_NPI * ((2 * 8 * 8 + 127) / 128), 128, 0, stream>>>(ctx->wtab[0], w.wt_need, w.wt_ready, ctx->lob_mu);
       launches++;
@@ -1320,7 +1330,8 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   w.counters = (int*)(A + pl.o_counters);
   w.m_kext = (double*)(A + pl.o_mkext); w.m_salb = (double*)(A + pl.o_msalb); w.m_nleg = (int*)(A + pl.o_mnleg);
   w.m_back = (double*)(A + pl.o_mback); w.m_refr = (double*)(A + pl.o_mrefr);
-  w.m_legen = (double*)(A + pl.o_mlegen);
+  w.m_legen = pl.f32_coef ? nullptr : (double*)(A + pl.o_mlegen);
+  w.m_legen32 = pl.f32_coef ? (float*)(A + pl.o_mlegen) : nullptr;
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
   w.spin_limit = tc::MBAR_SPIN_LIMIT;
@@ -1343,7 +1354,7 @@ extern "C" int32_t pamtra_b200_run_noalloc(const pamtra_b200_settings* st, const
   if (nh > 0) {
     const size_t sm_mie = MIE_WARPS * sizeof(MieSmem);
     k_refr<<<(unsigned)(((size_t)std::max(1, pl.pmax) * Fm + 127) / 128), 128, 0, stream>>>(b, w, *st);
-    k_mie<<<NOALLOC_MIE_SLABS / MIE_WARPS, 32 * MIE_WARPS, sm_mie, stream>>>(b, w, *st);
+    k_mie<MIE_GROUP><<<NOALLOC_MIE_SLABS / MIE_WARPS, 32 * MIE_WARPS, sm_mie, stream>>>(b, w, *st);
   }
   if (mask & 1) {
     if (nh > 0) k_layer<8><<<sms, RTCfg<8>::T, sizeof(LayerSmem<8>), stream>>>(b, w, *st, out->scatter_matrix);

@@ -16,18 +16,20 @@ constexpr int NQ_MAX = 256;   // Gauss points per series (nquad)
 constexpr int NT_MAX = 128;   // Mie terms per bin
 
 // Shared memory of one warp of k_mie: the phase-function sums of the
-// current species per quadrature point (P11, P12, P33), the weights of the
-// bins of the current pass and the staging of one round of work items.
+// current species per quadrature point (P11, P12, P33) and the weights and
+// term counts of the bins of the current pass.
 struct MieSmem {
   double sump[3][NQ_MAX];
-  double stg[3][32];
   double bw[32], bd[32];
-  int bn[32], sti[32];
+  int bn[32];
 };
 // Coefficient slab of one warp in global scratch: up to 32 bins x kmax rows
 // of (a_n, b_n); 4096 doubles hold 32 bins up to 32 terms (size parameters
 // up to about 20), fewer bins per pass beyond that (8 at the 127-term limit).
 constexpr int MIE_SLAB = 4096;
+// each warp's slab region: the coefficients, then the item's species sums of
+// the Legendre coefficients [3][MAXNLEG] (FP64 whatever the storage of the result)
+constexpr int MIE_SLAB_STRIDE = MIE_SLAB + 3 * MAXNLEG;
 constexpr int MIE_SLAB_WARPS_PER_SM = 16;  // slabs reserved per SM (caps the k_mie grid; the resident maximum)
 
 // Per-term constants: c_n = (2n+1) / (n(n+1)) of mieangle evaluated in REAL(4)
@@ -291,7 +293,7 @@ __device__ __noinline__ void miecalc_slab(int nterms, double x, cplx mn, double*
 }
 
 // Phase-matrix elements P11, P12 (= P21) and P33 of one angle, summed over
-// the bins j0 .. j0+MIE_GROUP-1 of a pass with their weights (mieangle,
+// the bins j0 .. j0+GB-1 of a pass with their weights (mieangle,
 // mie_scat_utilities.f90:119-160, and the PSD sums of mie_spheres.f90:
 // 239-249).  With S+ = S1 + S2 = sum c_n u_n (pi_n + tau_n) and
 // S- = S1 - S2 = sum c_n v_n (pi_n - tau_n) each term costs two complex
@@ -302,16 +304,14 @@ __device__ __noinline__ void miecalc_slab(int nterms, double x, cplx mn, double*
 // The pi_n / tau_n recurrence of the angle runs once for the group (rows
 // of bins without particles, and rows past a bin's own term count, hold
 // zeros).
-#ifndef MIE_GROUP_BINS
-#define MIE_GROUP_BINS 4
-#endif
-constexpr int MIE_GROUP = MIE_GROUP_BINS;  // bins per work item (4 or 8)
+constexpr int MIE_GROUP = 4;  // default bins per work item (the launch shape chooses 4 or 8)
+template <int GB>
 __device__ __forceinline__ void mie_angle_group(const double* __restrict__ slab, int ldc, int j0, int nmax, double mu,
                                                 const double* __restrict__ wt, const double* __restrict__ dd, int nj,
-                                                double (&f)[3]) {
-  double s[MIE_GROUP][4];  // S+ (re, im), S- (re, im)
+                                                double* sum0, double* sum1, double* sum2) {
+  double s[GB][4];  // S+ (re, im), S- (re, im)
 #pragma unroll
-  for (int j = 0; j < MIE_GROUP; j++) s[j][0] = s[j][1] = s[j][2] = s[j][3] = 0.0;
+  for (int j = 0; j < GB; j++) s[j][0] = s[j][1] = s[j][2] = s[j][3] = 0.0;
   double pin = 1.0, pim = 0.0;
   const double* row = slab + 4 * j0;
   for (int n = 1; n <= nmax; n++, row += ldc) {
@@ -321,7 +321,7 @@ __device__ __forceinline__ void mie_angle_group(const double* __restrict__ slab,
     const double taun = fma((double)n, mp, -q);
     const double cpl = c * (pin + taun), cmi = c * (pin - taun);
 #pragma unroll
-    for (int j = 0; j < MIE_GROUP; j++) {
+    for (int j = 0; j < GB; j++) {
       const double2 u = *reinterpret_cast<const double2*>(row + 4 * j);
       const double2 v = *reinterpret_cast<const double2*>(row + 4 * j + 2);
       s[j][0] = fma(u.x, cpl, s[j][0]);
@@ -333,62 +333,46 @@ __device__ __forceinline__ void mie_angle_group(const double* __restrict__ slab,
     pin = fma((double)(2 * n + 1), mp, -q) * rn;
     pim = tmp;
   }
-  f[0] = f[1] = f[2] = 0.0;
+  // add each bin's weighted elements to the angle's sums in bin order, so
+  // that the sums do not depend on the number of bins per work item
+  double a0 = sum0[0], a1 = sum1[0], a2 = sum2[0];
 #pragma unroll
-  for (int j = 0; j < MIE_GROUP; j++) {
+  for (int j = 0; j < GB; j++) {
     if (j >= nj || !(wt[j] > 0.0)) continue;
     const double ap = s[j][0] * s[j][0] + s[j][1] * s[j][1], am = s[j][2] * s[j][2] + s[j][3] * s[j][3];
     const double p0 = 0.25 * (ap + am), p2 = 0.25 * (ap - am);
     const double p1 = -0.5 * (s[j][0] * s[j][2] + s[j][1] * s[j][3]);
-    f[0] = f[0] + (p0 * wt[j]) * dd[j];
-    f[1] = f[1] + (p1 * wt[j]) * dd[j];
-    f[2] = f[2] + (p2 * wt[j]) * dd[j];
+    a0 = a0 + (p0 * wt[j]) * dd[j];
+    a1 = a1 + (p1 * wt[j]) * dd[j];
+    a2 = a2 + (p2 * wt[j]) * dd[j];
   }
+  sum0[0] = a0;
+  sum1[0] = a1;
+  sum2[0] = a2;
 }
 
 // Phase B of one pass (whole warp): item u = g * nquad + i is angle i over
-// the bins of group g of the pass.  Out of line so that the kernel's state
+// the bins of group g of the pass.  A round takes min(32, nquad) consecutive
+// items, so its angles are distinct and each lane adds into its angle's sums
+// without conflicts; rounds go in order, so every angle receives its bins in
+// bin order whatever the group size.  Out of line so that the kernel's state
 // is saved once per pass and the items keep the registers for their sums.
-// Each round of 32 items adds into the per-angle sums in lane order.
+template <int GB>
 __device__ __noinline__ void mie_pass_sums(MieSmem& S, const double* __restrict__ slab, int ldc, int cb, int nquad,
                                            const double* __restrict__ gx) {
   const int lane = threadIdx.x & 31;
-  const int G = (cb + MIE_GROUP - 1) / MIE_GROUP;
+  const int G = (cb + GB - 1) / GB;
   const int nu = G * nquad;
-  for (int u0 = 0; u0 < nu; u0 += 32) {
+  const int W = min(32, nquad);
+  for (int u0 = 0; u0 < nu; u0 += W) {
     const int u = u0 + lane;
-    double fk[3] = {0.0, 0.0, 0.0};
-    int ia = -1;
-    if (u < nu) {
+    if (lane < W && u < nu) {
       const int g = u / nquad, i = u - g * nquad;
-      ia = i;
-      const int j0 = MIE_GROUP * g, nj = min(MIE_GROUP, cb - j0);
+      const int j0 = GB * g, nj = min(GB, cb - j0);
       int nmax = 0;
       for (int j = 0; j < nj; j++) nmax = max(nmax, S.bn[j0 + j]);
-      mie_angle_group(slab, ldc, j0, nmax, gx[i], S.bw + j0, S.bd + j0, nj, fk);
-    }
-    if (nquad >= 32) {
-      // the 32 items of a round have distinct angles
-      if (ia >= 0) {
-        S.sump[0][ia] += fk[0];
-        S.sump[1][ia] += fk[1];
-        S.sump[2][ia] += fk[2];
-      }
-    } else {
-      // angles repeat within the round: lane i adds the items of angle i in lane order
-      S.stg[0][lane] = fk[0];
-      S.stg[1][lane] = fk[1];
-      S.stg[2][lane] = fk[2];
-      S.sti[lane] = ia;
-      __syncwarp();
-      if (lane < nquad) {
-        double a0 = S.sump[0][lane], a1 = S.sump[1][lane], a2 = S.sump[2][lane];
-        for (int L = 0; L < 32; L++)
-          if (S.sti[L] == lane) { a0 += S.stg[0][L]; a1 += S.stg[1][L]; a2 += S.stg[2][L]; }
-        S.sump[0][lane] = a0;
-        S.sump[1][lane] = a1;
-        S.sump[2][lane] = a2;
-      }
+      mie_angle_group<GB>(slab, ldc, j0, nmax, gx[i], S.bw + j0, S.bd + j0, nj, &S.sump[0][i], &S.sump[1][i],
+                          &S.sump[2][i]);
     }
     __syncwarp();
   }
@@ -404,13 +388,14 @@ __device__ __noinline__ void mie_pass_sums(MieSmem& S, const double* __restrict_
 // in lane order, so every result is independent of the launch shape.  The
 // Legendre projection runs lanes over quadrature points with shuffle sums.
 // The species sums accumulate in the item's coefficient output row.
+template <int GB>
 __global__ void __maxnreg__(MIE_MAXNREG) k_mie(Batch b, Work w, pamtra_b200_settings st) {
   extern __shared__ double smem_raw[];
   MieSmem& S = reinterpret_cast<MieSmem*>(smem_raw)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const int gwarp = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (gwarp >= w.mie_nslab) return;
-  double* const slab = w.mie_slab + (size_t)gwarp * MIE_SLAB;
+  double* const slab = w.mie_slab + (size_t)gwarp * MIE_SLAB_STRIDE;
   const int Lm = b.max_nlyrs, Fm = b.max_nfreq, H = b.nhydro;
   const int P = min(w.counters[0], w.pmax);
   const int nitems = P * Fm;
@@ -425,7 +410,7 @@ __global__ void __maxnreg__(MIE_MAXNREG) k_mie(Batch b, Work w, pamtra_b200_sett
     if (f >= b.col_nfreq(c)) continue;
     const double freq = b.freq(c, f);
     const double wl = C_LIGHT / (freq * 1e9);
-    double* const legc = w.m_legen + (size_t)item * 3 * MAXNLEG;  // species sums, then the result
+    double* const legc = slab + MIE_SLAB;  // species sums
     for (int jj = lane; jj < 3 * MAXNLEG; jj += 32) legc[jj] = 0.0;
     double kexttot = 0.0, salbedo = 0.0, backtot = 0.0;
     int nlegen_coef = 0;
@@ -493,7 +478,7 @@ __global__ void __maxnreg__(MIE_MAXNREG) k_mie(Batch b, Work w, pamtra_b200_sett
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) kmax = max(kmax, __shfl_xor_sync(0xffffffffu, kmax, o));
       // bins per pass, a multiple of the group size so that no group runs past the slab's columns
-      const int bp = min(32, MIE_SLAB / (4 * kmax)) & ~(MIE_GROUP - 1);
+      const int bp = min(32, MIE_SLAB / (4 * kmax)) & ~(GB - 1);
       const int ldc = 4 * bp;
       __syncwarp();
       double sqe = 0.0, sqs = 0.0, sqb = 0.0;
@@ -543,7 +528,7 @@ __global__ void __maxnreg__(MIE_MAXNREG) k_mie(Batch b, Work w, pamtra_b200_sett
         }
         __syncwarp();
         // ---- phase B: the phase-function sums of the pass
-        mie_pass_sums(S, slab, ldc, cb, nquad, gx);
+        mie_pass_sums<GB>(S, slab, ldc, cb, nquad, gx);
       }
       sqe = warp_sum(sqe);
       sqs = warp_sum(sqs);
@@ -629,15 +614,22 @@ __global__ void __maxnreg__(MIE_MAXNREG) k_mie(Batch b, Work w, pamtra_b200_sett
       __syncwarp();
       if (nlegen_coef > MAXNLEG - 1) { status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE; break; }
     }
-    // finalize_rt3_scatProperties (scatProperties.f90:993-1002), in place
+    // finalize_rt3_scatProperties (scatProperties.f90:993-1002) into the
+    // item's coefficient row: FP64, or FP32 storage in the split-precision form
     salbedo = salbedo / kexttot;
     const double den = salbedo * kexttot;
-    for (int jj = lane; jj <= nlegen_coef && jj < MAXNLEG; jj += 32) {
+    double* const out64 = w.m_legen ? w.m_legen + (size_t)item * 3 * MAXNLEG : nullptr;
+    float* const out32 = w.m_legen32 ? w.m_legen32 + (size_t)item * 3 * MAXNLEG : nullptr;
+    for (int jj = lane; jj < MAXNLEG; jj += 32) {
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        const double v = legc[k * MAXNLEG + jj] / den;
-        if (isnan(v) && nlegen_coef > 0) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_NAN;
-        legc[k * MAXNLEG + jj] = v;
+        double v = 0.0;
+        if (jj <= nlegen_coef) {
+          v = legc[k * MAXNLEG + jj] / den;
+          if (isnan(v) && nlegen_coef > 0) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_NAN;
+        }
+        if (out64) out64[k * MAXNLEG + jj] = v;
+        else out32[k * MAXNLEG + jj] = (float)v;
       }
     }
     status = __reduce_or_sync(0xffffffffu, status);

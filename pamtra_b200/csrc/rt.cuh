@@ -178,16 +178,17 @@ __device__ __forceinline__ bool layer_setup(const Batch& b, const Work& w, const
       ext = kext;
       emis = (1.0 - salb) * kext;
       const double cst = kext * salb / (4.0 * 3.1415926535897932384);
-      const double* lg = w.m_legen + (size_t)item * 3 * MAXNLEG;
+      const double* lg = w.m_legen ? w.m_legen + (size_t)item * 3 * MAXNLEG : nullptr;
+      const float* lg32 = w.m_legen32 ? w.m_legen32 + (size_t)item * 3 * MAXNLEG : nullptr;
       double* coef = Gb;          // [3][MAXNLEG] (S.mat(2) provides that many; for n = 16 the next matrix)
       double* cphi = Yb;          // [KMAX]
       double* sphi = Yb + KMAX;   // [KMAX]
       const int numpts = 2 * ((nleg + 1) / 2) + 4;
       const int K = numpts / 2 + 1;
       for (int l = t; l <= nleg; l += T) {
-        coef[l] = cst * lg[l];
-        coef[MAXNLEG + l] = cst * lg[MAXNLEG + l];
-        coef[2 * MAXNLEG + l] = cst * lg[2 * MAXNLEG + l];
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+          coef[k * MAXNLEG + l] = cst * (lg ? lg[k * MAXNLEG + l] : (double)lg32[k * MAXNLEG + l]);
       }
       const double* W = w.wtab[nmu_index(N)];
       if (W) {

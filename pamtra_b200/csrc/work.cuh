@@ -65,9 +65,10 @@ struct Work {
   double* m_back;                      // [pmax*Fm] volumetric backscattering cross section, m^2/m^3
   double* m_refr;                      // [pmax*Fm][4] refractive index of water (re, im), ice (re, im); NaN: none
   int* m_nleg;                         // [pmax*Fm]
-  double* mie_slab;                    // [mie_nslab][MIE_SLAB] per-warp Mie coefficient slabs of k_mie
+  double* mie_slab;                    // [mie_nslab][MIE_SLAB_STRIDE] per-warp Mie slabs of k_mie
   int mie_nslab;
-  double* m_legen;                     // [pmax*Fm][3][MAXNLEG]
+  double* m_legen;                     // [pmax*Fm][3][MAXNLEG] normalised Legendre coefficients (FP64 storage)
+  float* m_legen32;                    // the same in FP32 storage (split-precision form); exactly one is set
   // layer R, T, S per item (R,T padded n x (n+2), symmetric +/-)
   double* lay;                         // [pmax*Fm][lay_stride]
   size_t lay_stride;

@@ -116,3 +116,21 @@ def test_phase_matrices_nummu(oracle_mod, native, nummu):
     pbatch.run(b, 0, out)
     torch.cuda.synchronize()
     assert _compare(b, out, oracle_mod, nummu) > 20
+
+
+def test_mie_heavy_slice_split_form(oracle_mod, native):
+    """The batched split-precision form (3xTF32 doubling, Legendre
+    coefficients stored in FP32) on the Mie-heavy slice: every TB within
+    0.05 K of the FP64 oracle."""
+    import torch
+    from pamtra_b200._native import PREC_3XTF32
+    dev = torch.device("cuda", 0)
+    b = _c4_slice()
+    out = b.alloc_outputs(dev)
+    pbatch.run(b, 0, out, precision=PREC_3XTF32)
+    torch.cuda.synchronize()
+    tb = out["tb"].cpu().numpy()
+    assert not np.any(out["status"].cpu().numpy())
+    for c in range(b.ncol):
+        tr, _ = _oracle(oracle_mod, b, c, 16, psd=False)
+        assert np.max(np.abs(tb[c] - tr)) < 0.05
