@@ -409,7 +409,9 @@ def test_split_precision_target_shape(native):
 
 def test_split_precision_uneven(native):
     # NUMMU 16 and 32 columns take the tensor-core doubling, NUMMU 8 the FP64
-    # one; both forms share the one-inverse FP64 adding
+    # one; both forms share the one-inverse FP64 adding.  The split form
+    # stores the Legendre coefficients in FP32, so its NUMMU 8 columns differ
+    # from the batched FP64 form only by that rounding (micro-kelvin).
     from pamtra_b200._native import PREC_3XTF32, PREC_FP64, PREC_FP64_BATCHED
     b = wl.uneven_batch(24, seed=13, nfreq_range=(2, 5))
     f64 = _run_prec(b, PREC_FP64)
@@ -420,7 +422,8 @@ def test_split_precision_uneven(native):
     d = np.abs(s["tb"] - f64["tb"])
     assert np.max(d) <= SPLIT_TB_TOL
     assert np.max(d[nmu == 32]) > 0.0  # NUMMU 32 ran in split precision
-    assert np.array_equal(s["tb"][nmu == 8], f64b["tb"][nmu == 8])
+    d8 = np.abs(s["tb"][nmu == 8] - f64b["tb"][nmu == 8])
+    assert np.max(d8) < 1e-4
 
 
 def test_split_precision_nummu_32(oracle_mod, native):
