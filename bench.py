@@ -273,8 +273,8 @@ def fp64_peak_tflops(dev):
 
 
 # k_layer<16> DRAM traffic per (layer, frequency) item: ncu capture of the
-# 256-column run (21,504 items): 16.9 MB read + 349.5 MB written per launch
-LAYER_TRAFFIC_PER_ITEM = (16.933632e6 + 349.538304e6) / 21504
+# 256-column run (21,504 items): 17.7 MB read + 348.3 MB written per launch
+LAYER_TRAFFIC_PER_ITEM = (17.698560e6 + 348.297472e6) / 21504
 
 
 def layer_flops(nd, N):

@@ -16,9 +16,8 @@
 // columns transposes them in registers first (warp_transpose32).
 
 // A product X * Y with FP32 operands is formed as
-//     X_hi Y_hi + X_hi Y_lo + X_lo Y_hi,   X_hi = rna_tf32(X), X_lo = rna_tf32(X - X_hi)
-// with FP32 accumulation in tensor memory (the dropped X_lo Y_lo term is
-// below 2^-22 relative).
+//     X_hi Y_hi + X_hi Y_lo + X_lo Y_hi,   X_hi = X truncated to TF32, X_lo = X - X_hi
+// with FP32 accumulation in tensor memory (see split()).
 #pragma once
 #include <cstdint>
 
@@ -50,15 +49,15 @@ __device__ __forceinline__ uint64_t desc(uint32_t addr, uint32_t lbo, uint32_t s
 }
 __device__ __forceinline__ uint64_t desc_k(uint32_t addr) { return desc(addr, 128, 1024); }
 
-__device__ __forceinline__ float rna_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
-
+// hi = x truncated to TF32 (its top 19 bits, one logic operation), lo = x -
+// hi (exact in FP32); the tensor core reads only the TF32 bits of lo, so lo
+// needs no conversion.  Each operand then carries about 2^-20 relative error,
+// the size of the dropped lo * lo term.  (Rounding both halves with
+// cvt.rna.tf32 is 2^-22 but costs two conversions per element: the split
+// kernels are bound by this CUDA-core work, not by the tensor pipe.)
 __device__ __forceinline__ void split(float x, float& hi, float& lo) {
-  hi = rna_tf32(x);
-  lo = rna_tf32(x - hi);
+  hi = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
+  lo = x - hi;
 }
 
 // D[tmem] (+)= A * B^T over K = 8 from the given descriptors (one thread)
