@@ -154,6 +154,59 @@ __device__ __forceinline__ void mm(const double* A, const double* B, double* C, 
       }
 }
 
+// Two products with the same left factor in one pass over K:
+// C1 = A B1 (+ D1) and C2 = A B2 (+ D2), modes MM_SET / MM_ACC each.  The A
+// fragments are loaded once for both (six operand loads per k-step for eight
+// DMMAs instead of eight), and each element accumulates in the same order as
+// in mm(), so the results are bit-identical to two mm() calls.  C1 and C2
+// must not alias A, B1 or B2.
+template <int n, int MODE1, int MODE2>
+__device__ __forceinline__ void mm2(const double* A, const double* B1, double* C1, const double* D1,
+                                    const double* B2, double* C2, const double* D2) {
+  constexpr int LD = Team<n>::LD, WT = n / 16;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int row0 = (warp / WT) * 16, col0 = (warp % WT) * 16;
+  const int g = lane >> 2, q = lane & 3;
+  double c[2][2][2], e[2][2][2];
+#pragma unroll
+  for (int rt = 0; rt < 2; rt++)
+#pragma unroll
+    for (int ct = 0; ct < 2; ct++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int row = row0 + rt * 8 + g, col = col0 + ct * 8 + 2 * q + i;
+        c[rt][ct][i] = (MODE1 == MM_ACC) ? D1[col * LD + row] : 0.0;
+        e[rt][ct][i] = (MODE2 == MM_ACC) ? D2[col * LD + row] : 0.0;
+      }
+#pragma unroll 4
+  for (int kk = 0; kk < n; kk += 4) {
+    const double a0 = A[(kk + q) * LD + row0 + g];
+    const double a1 = A[(kk + q) * LD + row0 + 8 + g];
+    const double b0 = B1[(col0 + g) * LD + kk + q];
+    const double b1 = B1[(col0 + 8 + g) * LD + kk + q];
+    const double f0 = B2[(col0 + g) * LD + kk + q];
+    const double f1 = B2[(col0 + 8 + g) * LD + kk + q];
+    dmma(c[0][0], a0, b0);
+    dmma(e[0][0], a0, f0);
+    dmma(c[0][1], a0, b1);
+    dmma(e[0][1], a0, f1);
+    dmma(c[1][0], a1, b0);
+    dmma(e[1][0], a1, f0);
+    dmma(c[1][1], a1, b1);
+    dmma(e[1][1], a1, f1);
+  }
+#pragma unroll
+  for (int rt = 0; rt < 2; rt++)
+#pragma unroll
+    for (int ct = 0; ct < 2; ct++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int row = row0 + rt * 8 + g, col = col0 + ct * 8 + 2 * q + i;
+        C1[col * LD + row] = c[rt][ct][i];
+        C2[col * LD + row] = e[rt][ct][i];
+      }
+}
+
 // row `row` of M * x (k-ascending FMA chain)
 template <int n>
 __device__ __forceinline__ double mv_row(const double* __restrict__ M, const double* __restrict__ x, int row) {

@@ -643,7 +643,12 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
         //    T1m' = T1m Gm T2 = T1m (T2 + R2 (Gp R1p T2)),
         //    Gm w = w + R2 Gp (R1p w) for the S- chain:
         // ten products and one inverse per combine instead of twelve and two.
-        mm<n, MM_SET>(Rp, R2, G);
+        // Products that share their left factor run in one pass (mm2), and the
+        // two source chains of a phase run on different warps:
+        //   Rp [R2, T2] -> Gp (inverted next), Z = R1p T2
+        mm2<n, MM_SET, MM_SET>(Rp, R2, G, nullptr, T2, Z, nullptr);
+        if (t < n) S.wv[t] = S.sp[t] + mv_row<n>(Rp, S.s2m, t);                    // S+ chain
+        else if (t < 2 * n) S.nsm[t - n] = S.s2m[t - n] + mv_row<n>(R2, S.sp, t - n);  // S- chain: w
         team_sync();
         {
           int sg = 0;
@@ -651,29 +656,22 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
           if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
           if (gi != G) { X = G; G = gi; }
         }
-        mm<n, MM_SET>(Rp, T2, X);  // R1p T2
-        // the two chains of a phase run on different warps
-        if (t < n) S.wv[t] = S.sp[t] + mv_row<n>(Rp, S.s2m, t);                    // S+ chain
-        else if (t < 2 * n) S.nsm[t - n] = S.s2m[t - n] + mv_row<n>(R2, S.sp, t - n);  // S- chain: w
-        team_sync();
-        mm<n, MM_SET>(G, X, Y);  // Y = Gp R1p T2
+        //   Gp [Z, T1p] -> Y = Gp R1p T2, X = W = Gp T1p
+        mm2<n, MM_SET, MM_SET>(G, Z, Y, nullptr, Tp, X, nullptr);
         if (t < n) S.wv2[t] = mv_row<n>(G, S.wv, t);
         else if (t < 2 * n) S.u1[t - n] = mv_row<n>(Rp, S.nsm, t - n);
         team_sync();
-        mm<n, MM_ACC>(T2, Y, Z, R2);  // new R+ = R2 + T2 Gp R1p T2
+        //   T2 [Y, W] -> new R+ = R2 + T2 Y (into Z), new T+ = T2 W (into Rp: old R+ is dead)
+        mm2<n, MM_ACC, MM_SET>(T2, Y, Z, R2, X, Rp, nullptr);
         if (t < n) S.nsp[t] = S.s2p[t] + mv_row<n>(T2, S.wv2, t);
         else if (t < 2 * n) S.u2[t - n] = mv_row<n>(G, S.u1, t - n);
         team_sync();
-        mm<n, MM_SET>(G, Tp, X);  // W = Gp T1p
-        if (t < n) S.u1[t] = S.nsm[t] + mv_row<n>(R2, S.u2, t);  // Gm w
-        team_sync();
-        mm<n, MM_SET>(T2, X, Rp);  // new T+ = T2 W (old R+ is dead)
-        if (t < n) S.nsm[t] = S.sm[t] + mv_row<n>(Tm, S.u1, t);
-        team_sync();
         mm<n, MM_SET>(Tm, R2, G);  // V = T1m R2 (Gp is dead)
+        if (t < n) S.u1[t] = S.nsm[t] + mv_row<n>(R2, S.u2, t);  // Gm w
         team_sync();
         mm<n, MM_ACC>(G, X, Rm, Rm);   // new R- = R1m + V W
         mm<n, MM_ACC>(R2, Y, Tp, T2);  // U = T2 + R2 Y (old T+ is dead)
+        if (t < n) S.nsm[t] = S.sm[t] + mv_row<n>(Tm, S.u1, t);
         team_sync();
         mm<n, MM_SET>(Tm, Tp, X);  // new T- = T1m U
         team_sync();
