@@ -134,3 +134,36 @@ def test_mie_heavy_slice_split_form(oracle_mod, native):
     for c in range(b.ncol):
         tr, _ = _oracle(oracle_mod, b, c, 16, psd=False)
         assert np.max(np.abs(tb[c] - tr)) < 0.05
+
+
+def _large_particles(ncol=1, nlay=12, seed=37):
+    """Ice spheres of 900 kg/m3 up to 3 cm and rain up to 8 mm at 89 and
+    190.31 GHz: size parameters up to about 60 (about 80 Mie terms, 160
+    Legendre orders, 161 quadrature angles), so the coefficient slab takes
+    fewer than 32 bins per pass and the Legendre projection runs in several
+    chunks of quadrature points."""
+    rng = np.random.default_rng(seed)
+    st = wl._settings(16)
+    sp = np.empty(2, dtype=packing.SPECIES_DTYPE)
+    for j, k in enumerate(("gwc", "rwc")):
+        sp[j] = wl._species_row(k, np.random.default_rng(300 + j), nbin=100, gamma=False, rho=900.0)
+    sp[0]["d_1"], sp[0]["d_2"], sp[0]["p_2"] = 1.0e-4, 3.0e-2, 5.0e-3
+    sp[1]["d_1"], sp[1]["d_2"] = 1.0e-4, 8.0e-3
+    nly = np.full(ncol, nlay)
+    top = np.full(ncol, 6000.0)
+    qs = [[10 ** rng.uniform(-3.5, -2.7) for _ in range(2)] for _ in range(ncol)]
+    return wl._packed(st, sp, 0, nly, [[89.0, 190.31]], None, [["gwc", "rwc"]] * ncol, qs, top, rng, nlay, 2, False)
+
+
+def test_long_mie_series(oracle_mod, native):
+    import torch
+    dev = torch.device("cuda", 0)
+    b = _large_particles()
+    out = _outputs(b, dev)
+    pbatch.run(b, 0, out)
+    torch.cuda.synchronize()
+    _, d = _oracle(oracle_mod, b, 0, 16, psd=False)
+    # about 77 Mie terms: the projection runs over 2 x 77 orders (past the
+    # 128-entry Mie-term table) and 155 quadrature points (three chunks)
+    assert int(np.max(d["nlegen"])) > 100
+    assert _compare(b, out, oracle_mod, 16) > 10
