@@ -40,6 +40,17 @@ namespace pb {
 // column (row loads, mat-vecs) both hit 32 distinct banks without padding.
 __device__ __forceinline__ int midx(int r, int c) { return c * 32 + ((((r >> 2) ^ (c & 7)) << 2) | (r & 3)); }
 
+// The eight in-column offsets of row r (one per value of c mod 8): element
+// (r, c) sits at c * 32 + off[c & 7].  A thread reading a whole row computes
+// them once instead of swizzling every address.
+struct RowOff {
+  int o[8];
+  __device__ __forceinline__ explicit RowOff(int r) {
+#pragma unroll
+    for (int j = 0; j < 8; j++) o[j] = (((r >> 2) ^ j) << 2) | (r & 3);
+  }
+};
+
 // FP32 state of one item of the pair.
 struct TcItemState {
   float rm[1024], tm[1024], gm[1024];    // R, T~, G~
@@ -107,7 +118,7 @@ __device__ __forceinline__ void st_col(float* m, int col, const float (&v)[32]) 
 // `lane` of master `bsrc`, read down its columns: conflict-free) into shared
 // memory.  The two warps of an item cover the B row's two halves.
 __device__ __forceinline__ void build_operands(TcTiles& TL, const float* asrc, const float* bsrc, uint32_t ta_hi,
-                                               uint32_t ta_lo, int brow, int h, int lane) {
+                                               uint32_t ta_lo, int brow, int h, int lane, const RowOff& ro) {
   {
     float c[32], lo[32];
     ld_col(asrc, lane, c);
@@ -120,10 +131,11 @@ __device__ __forceinline__ void build_operands(TcTiles& TL, const float* asrc, c
   for (int q = 0; q < 4; q++) {
     const int k0 = 16 * h + 4 * q;
     float4 hi, lo;
-    tc::split(bsrc[midx(lane, k0 + 0)], hi.x, lo.x);
-    tc::split(bsrc[midx(lane, k0 + 1)], hi.y, lo.y);
-    tc::split(bsrc[midx(lane, k0 + 2)], hi.z, lo.z);
-    tc::split(bsrc[midx(lane, k0 + 3)], hi.w, lo.w);
+    const float* bc = bsrc + k0 * 32;  // k0 = 16 h + 4 q: (k0 + j) mod 8 = (4 q + j) mod 8
+    tc::split(bc[0 * 32 + ro.o[(4 * q + 0) & 7]], hi.x, lo.x);
+    tc::split(bc[1 * 32 + ro.o[(4 * q + 1) & 7]], hi.y, lo.y);
+    tc::split(bc[2 * 32 + ro.o[(4 * q + 2) & 7]], hi.z, lo.z);
+    tc::split(bc[3 * 32 + ro.o[(4 * q + 3) & 7]], hi.w, lo.w);
     const int o = (brow >> 3) * tc::RG_FLOATS + (k0 >> 2) * 32 + (brow & 7) * 4;
     *reinterpret_cast<float4*>(TL.b_hi + o) = hi;
     *reinterpret_cast<float4*>(TL.b_lo + o) = lo;
@@ -132,13 +144,14 @@ __device__ __forceinline__ void build_operands(TcTiles& TL, const float* asrc, c
 
 // (M x0)[r] and (M x1)[r] for a master M (k-ascending FMA chains)
 __device__ __forceinline__ void matvec2(const float* __restrict__ M, const float* __restrict__ x0,
-                                        const float* __restrict__ x1, int r, float& y0, float& y1) {
+                                        const float* __restrict__ x1, const RowOff& ro, float& y0, float& y1) {
   float a0 = 0.f, a1 = 0.f;
 #pragma unroll
   for (int k = 0; k < 32; k += 4) {
     const float4 p = *reinterpret_cast<const float4*>(x0 + k);
     const float4 q = *reinterpret_cast<const float4*>(x1 + k);
-    const float m0 = M[midx(r, k)], m1 = M[midx(r, k + 1)], m2 = M[midx(r, k + 2)], m3 = M[midx(r, k + 3)];
+    const float m0 = M[k * 32 + ro.o[k & 7]], m1 = M[(k + 1) * 32 + ro.o[(k + 1) & 7]];
+    const float m2 = M[(k + 2) * 32 + ro.o[(k + 2) & 7]], m3 = M[(k + 3) * 32 + ro.o[(k + 3) & 7]];
     a0 = fmaf(m0, p.x, a0); a1 = fmaf(m0, q.x, a1);
     a0 = fmaf(m1, p.y, a0); a1 = fmaf(m1, q.y, a1);
     a0 = fmaf(m2, p.z, a0); a1 = fmaf(m2, q.z, a1);
@@ -213,6 +226,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
   const uint32_t lanes = (uint32_t)(warp * 32) << 16;  // A row = D lane of this thread
   const uint32_t dmine = tslot + lanes + 32u * mi;       // my lanes, my item's columns of D
   const int brow = 32 * mi + lane;                       // B row of my item for my lane
+  const RowOff rowoff(lane);                             // my row of the masters
   uint32_t parity = 0;
 
   for (;;) {
@@ -289,7 +303,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
           else if (phase == SER) { asrc = slot ? my.gm : my.xa; bsrc = my.xa; }
           else if (phase == G2) { asrc = slot ? my.vm : my.tm; bsrc = my.gm; }
           else { asrc = slot ? my.vm : my.xa; bsrc = my.tm; }
-          build_operands(TL, asrc, bsrc, tslot + lanes + 64u, tslot + lanes + 96u, brow, slot, lane);
+          build_operands(TL, asrc, bsrc, tslot + lanes + 64u, tslot + lanes + 96u, brow, slot, lane, rowoff);
         }
         tc::fence_async_smem();
         tc::fence_before_sync();
@@ -302,7 +316,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
         if (on && phase != SER) {
           const float* mv = (phase == G1) ? my.rm : (phase == G2) ? my.gm : my.tm;
           const float(*x)[32] = (phase == G1) ? my.vv : (phase == G2) ? my.uv : my.wv;
-          matvec2(mv, x[2 * slot], x[2 * slot + 1], lane, m0, m1);
+          matvec2(mv, x[2 * slot], x[2 * slot + 1], rowoff, m0, m1);
         }
         {
           const bool mine = tc::mbar_wait(&mbar, parity, w.spin_limit);
