@@ -550,6 +550,29 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
     double *G = mats[6], *X = mats[7], *Y = mats[8], *Z = mats[9];
     // stack state: 0 empty, 1 clear (R = 0, T = diag t1 on both sides), 2 general
     int sstate = 0;
+    // The next scattering layer's R, T and S blocks are read into registers
+    // while the current combine runs (batched forms, N <= 16: the kernel's
+    // occupancy is set by shared memory, so the registers are free).
+    constexpr bool PREFETCH = ONE_INV && N <= 16;
+    constexpr int PFE = (MAT + T - 1) / T;
+    double pfR[PREFETCH ? PFE : 1], pfT[PREFETCH ? PFE : 1], pfS[2];
+    int pf_pidx = -1;
+    auto prefetch = [&](int kfrom) {
+      pf_pidx = -1;
+      for (int kk = kfrom; kk < L; kk++) {
+        const int p = w.pres_idx[(size_t)c * Lm + (L - 1 - kk)];
+        if (p >= 0) { pf_pidx = p; break; }
+      }
+      if (pf_pidx < 0) return;
+      const double* src = w.lay + ((size_t)pf_pidx * Fm + fi) * w.lay_stride;
+#pragma unroll
+      for (int q = 0; q < PFE; q++) {
+        const int e = t + q * T;
+        if (e < MAT) { pfR[q] = src[e]; pfT[q] = src[MAT + e]; }
+      }
+      if (t < n) { pfS[0] = src[2 * MAT + t]; pfS[1] = src[2 * MAT + n + t]; }
+    };
+    if (PREFETCH) prefetch(0);
     for (int k = 0; k < L; k++) {  // top-down layer index
       const int z = L - 1 - k;
       const int pidx = w.pres_idx[(size_t)c * Lm + z];
@@ -602,8 +625,16 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
         team_sync();
         continue;
       }
-      // scattering layer: fetch R2, T2, S2 from the arena
-      {
+      // scattering layer: its R2, T2, S2 from the arena (prefetched), then the next one's
+      if (PREFETCH) {
+#pragma unroll
+        for (int q = 0; q < PFE; q++) {
+          const int e = t + q * T;
+          if (e < MAT) { R2[e] = pfR[q]; T2[e] = pfT[q]; }
+        }
+        if (t < n) { S.s2p[t] = pfS[0]; S.s2m[t] = pfS[1]; }
+        prefetch(k + 1);
+      } else {
         const double* src = w.lay + ((size_t)pidx * Fm + fi) * w.lay_stride;
         for (int e = t; e < MAT; e += T) { R2[e] = src[e]; T2[e] = src[MAT + e]; }
         for (int e = t; e < n; e += T) { S.s2p[e] = src[2 * MAT + e]; S.s2m[e] = src[2 * MAT + n + e]; }
