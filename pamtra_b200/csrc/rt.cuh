@@ -51,7 +51,12 @@ __host__ __device__ __forceinline__ size_t lay_stride_n(int N) {
 template <int N>
 struct LayerSmem {
   static constexpr int n = RTCfg<N>::n, MAT = RTCfg<N>::MAT;
-  double m[5][MAT];  // R, T, G, W, Y; during scatcnv G (and W) hold the coefficients, Y the azimuth table
+  // matrices: R, T, G, W (and Y = R T as a fifth for N != 16).  For N = 16
+  // four matrices keep the block under 45.6 KB, so five CTAs fit per SM; the
+  // doubling then forms Y in G's buffer once G is consumed.  During scatcnv
+  // G (and W for N = 8) hold the coefficients, the last matrix the azimuth table.
+  static constexpr int NM = (N == 16) ? 4 : 5;
+  double m[NM][MAT];
   double lin[2 * n], cst[2 * n];
   double lin2[2 * n], cst2[2 * n];  // the other half of the doubled source buffers
   double v[4][n], u[4][n];
@@ -59,7 +64,7 @@ struct LayerSmem {
   InvScratch<n> inv;
   int item, stat;
   // set-up buffers (layer_setup): R, T, coefficients, azimuth table
-  __device__ __forceinline__ double* mat(int i) { return m[i]; }
+  __device__ __forceinline__ double* mat(int i) { return m[i < NM ? i : NM - 1]; }
 };
 
 // Azimuth weights of scatcnv (src/scatcnv.f90:103-192 with SUM_LEGENDRE,
@@ -372,7 +377,7 @@ __device__ __forceinline__ void layer_store(const Work& w, int item, const doubl
 }
 
 template <int N>
-__global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch b, Work w, pamtra_b200_settings st,
+__global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 5 : 1)) k_layer(Batch b, Work w, pamtra_b200_settings st,
                                                        double* __restrict__ ssp_scat) {
   constexpr int n = RTCfg<N>::n, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT, T = RTCfg<N>::T;
   (void)LD;
@@ -400,7 +405,8 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
     double* Tb = S.m[1];
     double* Gb = S.m[2];
     double* Wb = S.m[3];
-    double* Yb = S.m[4];
+    double* Yb = S.mat(4);  // = Gb's buffer role for N = 16 (see below)
+    constexpr bool FOUR = LayerSmem<N>::NM == 4;
     // ---------------- DOUBLING_INTEGRATION4, SYMMETRIC (src/radintg4.f90:174-309)
     // R' = R + T G R T and T' = T G T with G = (I - R R)^-1, as five products
     // per step: W = T G, then R' = R + W (R T) and T' = W T; the source
@@ -413,7 +419,7 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
     double *lin = S.lin, *cst = S.cst, *lin_n = S.lin2, *cst_n = S.cst2;
     for (int itd = 0; itd < nd; itd++) {
       mm<n, MM_SET>(Rb, Rb, Gb);  // R+ R-
-      mm<n, MM_SET>(Rb, Tb, Yb);  // Y = R T
+      if (!FOUR) mm<n, MM_SET>(Rb, Tb, Yb);  // Y = R T
       // v = [S- + f C-, C-, S+, C+]
       for (int o = t; o < 4 * n; o += T) {
         const int r = o % n, k = o / n;
@@ -445,7 +451,10 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
       }
       team_sync();
       // new sources from W u, then R' = R + W Y and T' = W T (into the G
-      // buffer): nothing of this phase reads what it writes
+      // buffer): nothing of this phase reads what it writes.  With four
+      // matrices Y = R T goes into G's buffer here (G is consumed), and T' is
+      // formed in place in T.
+      if (FOUR) mm<n, MM_SET>(Rb, Tb, Gb);
 #pragma unroll
       for (int s = 0; s < NV; s++) {
         const int o = t + s * T;
@@ -458,9 +467,15 @@ __global__ void __launch_bounds__(RTCfg<N>::T, (N == 16 ? 4 : 1)) k_layer(Batch 
           else cst_n[n + r] = cst[n + r] + a;
         }
       }
-      mm<n, MM_ACC>(Wb, Yb, Rb, Rb);
-      mm<n, MM_SET>(Wb, Tb, Gb);
-      { double* tmp = Tb; Tb = Gb; Gb = tmp; }
+      if (FOUR) {
+        team_sync();                           // Y complete
+        mm<n, MM_ACC>(Wb, Gb, Rb, Rb);         // R' = R + W Y
+        mm<n, MM_SET, true>(Wb, Tb, Tb);       // T' = W T (reads W and T, barrier, writes T)
+      } else {
+        mm<n, MM_ACC>(Wb, Yb, Rb, Rb);
+        mm<n, MM_SET>(Wb, Tb, Gb);
+        { double* tmp = Tb; Tb = Gb; Gb = tmp; }
+      }
       { double* tmp = lin; lin = lin_n; lin_n = tmp; }
       { double* tmp = cst; cst = cst_n; cst_n = tmp; }
       linfac = 2.0 * linfac;
