@@ -156,3 +156,12 @@ def test_latency_stats_and_arrivals():
             self.latency = lat
     st = serve.latency_stats([R(x / 1000.0) for x in range(1, 101)])
     assert abs(st["p50_ms"] - 50.5) < 1e-9 and abs(st["p99_ms"] - 99.01) < 1e-9
+
+
+def test_bench_oracle_sample_prefers_cheap_columns():
+    import bench
+    b = wl.uneven_batch(64, seed=62, nfreq_range=(2, 9))
+    idxs = bench.oracle_sample(b, 8)
+    assert len(idxs) == 8 and idxs == sorted(set(idxs))
+    nmu = np.asarray(b.host["nummu"])
+    assert {8, 16, 32} & set(nmu[idxs].tolist()) == set(np.unique(nmu).tolist()) & {8, 16, 32}
