@@ -50,7 +50,7 @@ extern "C" {
 #define PAMTRA_B200_ST_NAN 0x2000      /* NaN in extinction / coefficients */
 #define PAMTRA_B200_ST_SIZE 0x4000     /* a size limit of this library was exceeded */
 #define PAMTRA_B200_ST_TIMEOUT 0x8000  /* a bounded wait on the tensor core gave up */
-#define PAMTRA_B200_ST_RANGE 0x10000   /* input outside a model's range (liq_mod 'Ray' above 299.79 GHz) */
+#define PAMTRA_B200_ST_RANGE 0x10000   /* input outside a model's range (liq_mod 'Ray' outside 0.2 um - 10 cm wavelength) */
 
 /* dist_name codes (src/make_dist_param.f90) */
 #define PAMTRA_B200_DIST_EXP 0

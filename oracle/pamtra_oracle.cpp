@@ -37,6 +37,7 @@
 // (radmat.f90:201-233).  gfortran MATMUL is restated as k-ascending dot
 // products.
 #include "oracle_common.h"
+#include "ray_table.inc"
 
 #include <algorithm>
 #include <cstdio>
@@ -280,13 +281,28 @@ cplx eps_water_liebe(double T, double f) {
   return cadd(e, cmk(eps_2, 0.0));
 }
 
-// eps_water_ray (src/eps_water.f90:209-596), the Ray (1972) formula branch
-// for wavelengths above 1 mm; returns 2 for shorter wavelengths (tabulated
-// optical constants, not restated) and outside 0.2 um - 10 cm.
+// eps_water_ray (src/eps_water.f90:215-592): 0.2 um - 1 mm linear
+// interpolation in the tabulated optical constants (:515-537, first table
+// wavelength at or above wl, scanning from the second), 1 mm - 10 cm the
+// Ray (1972) formula (:539-585); returns 2 outside 0.2 um - 10 cm (the
+// reference stops there).
 int eps_water_ray(double T, double f, cplx& eps) {
   double wl = (double)(1.e6f * 2.99792458e8f) / (f * 1.e9f);
-  if (wl < (double)0.2f || wl > 100000.0) return 2;
-  if (!(wl > 1000.0)) return 2;
+  if (wl < (double)0.2f || wl > 100000.0 || wl != wl) return 2;
+  if (!(wl > 1000.0)) {
+    int i1 = RAY_NUMWAT - 3, i2 = RAY_NUMWAT - 2;
+    for (int i = 1; i < RAY_NUMWAT; ++i) {
+      if (wl > (double)ray_wl[i]) continue;
+      i1 = i - 1;
+      i2 = i;
+      break;
+    }
+    double fac = (wl - (double)ray_wl[i1]) / ((double)ray_wl[i2] - (double)ray_wl[i1]);
+    double rn = (double)ray_rn[i1] + fac * ((double)ray_rn[i2] - (double)ray_rn[i1]);
+    double cn = (double)ray_cn[i1] + fac * ((double)ray_cn[i2] - (double)ray_cn[i1]);
+    eps = cmul(cmk(rn, cn), cmk(rn, cn));
+    return 0;
+  }
   double T1 = T + 273.0f, T2 = T - 25.0f, xl = wl / 10000.0f;
   double sigma = 12.5664e8f;
   double alpha = -16.8129f / T1 + 0.0609265f;

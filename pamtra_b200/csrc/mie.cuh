@@ -4,6 +4,7 @@
 #pragma once
 #include "common.cuh"
 #include "work.cuh"
+#include "ray_table.cuh"
 
 namespace pb {
 
@@ -105,14 +106,32 @@ __device__ __noinline__ cplx eps_water_liebe(double T, double f) {
   return cadd(e, cmk(eps_2, 0.0));
 }
 
-// eps_water_ray (src/eps_water.f90:209-596, Ray 1972) for wavelengths above
-// 1 mm (f below 299.79 GHz); the tabulated optical constants of shorter
-// wavelengths are not on this path: *bad is set there.
+// eps_water_ray (src/eps_water.f90:215-592): below 1 mm wavelength (f above
+// 299.79 GHz) linear interpolation in the tabulated optical constants of
+// 0.2-1000 um (:515-537; the interval is the one ending at the first table
+// wavelength >= wl, found here by bisection over the ascending table instead
+// of the reference's linear scan), 1 mm - 10 cm the Ray (1972) formula;
+// *bad is set outside 0.2 um - 10 cm, where the reference stops.
 __device__ __noinline__ cplx eps_water_ray(double T, double f, int* bad) {
   const double wl = (double)(1.e6f * 2.99792458e8f) / (f * 1.e9f);  // microns
-  if (wl < (double)0.2f || wl > 100000.0 || !(wl > 1000.0)) {
+  if (wl < (double)0.2f || wl > 100000.0 || !(wl == wl)) {
     *bad = 1;
     return cmk(1.0, 0.0);
+  }
+  if (!(wl > 1000.0)) {
+    // smallest i in [1, RAY_NUMWAT) with wl <= ray_wl[i]; ray_wl[last] = 1000
+    int lo = 1, hi = RAY_NUMWAT - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (wl > (double)ray_wl[mid]) lo = mid + 1;
+      else hi = mid;
+    }
+    const int i1 = lo - 1, i2 = lo;
+    const double w1 = ray_wl[i1], w2 = ray_wl[i2];
+    const double fac = (wl - w1) / (w2 - w1);
+    const double rn = (double)ray_rn[i1] + fac * ((double)ray_rn[i2] - (double)ray_rn[i1]);
+    const double cn = (double)ray_cn[i1] + fac * ((double)ray_cn[i2] - (double)ray_cn[i1]);
+    return cmul(cmk(rn, cn), cmk(rn, cn));
   }
   const double T1 = T + 273.0f, T2 = T - 25.0f, xl = wl / 10000.0f;
   const double sigma = 12.5664e8f;

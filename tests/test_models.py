@@ -30,10 +30,63 @@ def test_oracle_water_models_near_tkc_pin(oracle_mod, liq_mod):
 
 
 def test_oracle_ray_range(oracle_mod):
-    # formula branch only: wavelengths 1 mm .. 10 cm
+    # 0.2 um .. 10 cm: table below 1 mm (f above 299.79 GHz), formula above
     assert oracle_mod.get_eps_water("Ray", 0.0, 10.0, 150.0)[0] == 0
-    assert oracle_mod.get_eps_water("Ray", 0.0, 10.0, 350.0)[0] == 2
-    assert oracle_mod.get_eps_water("Ray", 0.0, 10.0, 2.0)[0] == 2
+    assert oracle_mod.get_eps_water("Ray", 0.0, 10.0, 350.0)[0] == 0
+    assert oracle_mod.get_eps_water("Ray", 0.0, 10.0, 1.4e6)[0] == 0  # 0.214 um
+    assert oracle_mod.get_eps_water("Ray", 0.0, 10.0, 1.6e6)[0] == 2  # below 0.2 um
+    assert oracle_mod.get_eps_water("Ray", 0.0, 10.0, 2.0)[0] == 2  # above 10 cm
+
+
+def _ray_table():
+    import re
+    from pathlib import Path
+    text = (Path(__file__).resolve().parents[1] / "oracle" / "ray_table.inc").read_text()
+    tabs = {}
+    for name in ("ray_wl", "ray_rn", "ray_cn"):
+        body = re.search(r"%s\[RAY_NUMWAT\] = \{(.*?)\};" % name, text, re.S).group(1)
+        tabs[name] = np.array([float(v.rstrip("f")) for v in body.replace(",", " ").split()], dtype=np.float32)
+    return tabs
+
+
+def test_ray_table_shape():
+    t = _ray_table()
+    wl = t["ray_wl"].astype(np.float64)
+    assert all(len(v) == 518 for v in t.values())
+    assert wl[0] == np.float32(0.2) and wl[-1] == 1000.0 and np.all(np.diff(wl) > 0)
+    # Hale and Querry: visible water n about 1.33, almost transparent
+    vis = (wl > 0.4) & (wl < 0.7)
+    assert np.all(np.abs(t["ray_rn"][vis] - 1.333) < 0.01) and np.all(t["ray_cn"][vis] < 1e-7)
+
+
+def test_oracle_ray_table_interpolation(oracle_mod):
+    """The table branch at and between table wavelengths: eps = (rn + i cn)^2
+    of the linear interpolation in the interval ending at the first table
+    wavelength >= wl (src/eps_water.f90:522-537), with the wavelength from
+    the frequency as the reference forms it (single-precision constants)."""
+    t = _ray_table()
+    wl = t["ray_wl"].astype(np.float64)
+    rn, cn = t["ray_rn"].astype(np.float64), t["ray_cn"].astype(np.float64)
+    c = float(np.float32(1.e6) * np.float32(2.99792458e8))
+    rng = np.random.default_rng(5)
+    for f in list(rng.uniform(300.0, 1.4e6, 60)) + [c / (wl[100] * 1e9), c / (wl[-1] * 1e9)]:
+        w = c / (f * 1e9)
+        i2 = max(1, int(np.searchsorted(wl, w, side="left")))
+        i1 = i2 - 1
+        fac = (w - wl[i1]) / (wl[i2] - wl[i1])
+        n = complex(rn[i1] + fac * (rn[i2] - rn[i1]), cn[i1] + fac * (cn[i2] - cn[i1]))
+        err, eps = oracle_mod.get_eps_water("Ray", 0.0, 10.0, f)
+        assert err == 0
+        np.testing.assert_allclose([eps.real, eps.imag], [(n * n).real, (n * n).imag], rtol=1e-12, atol=1e-300)
+
+
+def test_oracle_ray_continuity_at_1mm(oracle_mod):
+    # the Downing-Williams value at 1000 um and Ray's formula just above agree
+    # within a few percent at room temperature (the table has no temperature)
+    fcut = float(np.float32(1.e6) * np.float32(2.99792458e8)) / 1000.0 / 1e9
+    below = oracle_mod.get_eps_water("Ray", 0.0, 20.0, fcut * 1.0001)[1]
+    above = oracle_mod.get_eps_water("Ray", 0.0, 20.0, fcut * 0.9999)[1]
+    assert abs(np.sqrt(below) - np.sqrt(above)) / abs(np.sqrt(above)) < 0.05
 
 
 def test_oracle_salinity_lowers_static_permittivity(oracle_mod):
@@ -78,7 +131,7 @@ def test_model_kernels_match_oracle(oracle_mod, native):
     lib = native.load()
     s = rng.choice([0.0, 35.0], n)
     tc = rng.uniform(-30.0, 40.0, n)
-    fr = rng.uniform(3.5, 500.0, n)
+    fr = np.concatenate([rng.uniform(3.5, 500.0, n - 40), 10 ** rng.uniform(2.7, 6.2, 40)])  # table branch too
     td = [torch.from_numpy(x).to(dev) for x in (s, tc, fr)]
     for i, m in enumerate(MODELS):
         er = torch.zeros(n, dtype=torch.float64, device=dev)
