@@ -65,15 +65,20 @@ extern "C" {
 #define PAMTRA_B200_PREC_FP64 0          /* FP64 in the reference's operation order: COMBINE_LAYERS4
                                            (src/radintg4.f90:447-513) with its two inverses per
                                            combine; the plain drop-in form */
-#define PAMTRA_B200_PREC_3XTF32 1        /* batched form: layer doubling products as 3xTF32 tcgen05
-                                           MMAs (NUMMU 16 and 32; NUMMU 8 doubles in FP64), FP64
-                                           adding with one inverse per combine; the Legendre
+#define PAMTRA_B200_PREC_3XTF32 1        /* batched split-precision form: layer doubling products
+                                           as 3xTF32 tcgen05 MMAs (NUMMU 16 and 32; NUMMU 8 doubles
+                                           in FP64); for NUMMU 16 the adding products too (stack in
+                                           FP32, the (I - R R)^-1 of each combine, the surface
+                                           coupling and the radiances in FP64), for NUMMU 8 and 32
+                                           FP64 adding with one inverse per combine; the Legendre
                                            coefficients of the phase matrices are stored in FP32
                                            (computed and expanded in FP64) */
 #define PAMTRA_B200_PREC_FP64_BATCHED 2  /* batched form in FP64: as PREC_FP64, but each adding
                                            combine derives the minus-side inverse from the
                                            plus-side one (Gm R2 = R2 Gp, Gm = I + R2 Gp R1p):
                                            one inverse and ten products instead of two and twelve */
+#define PAMTRA_B200_PREC_3XTF32_FP64ADD 3 /* as PREC_3XTF32 with the adding in FP64 for every NUMMU
+                                           (PREC_FP64_BATCHED's adding) */
 
 /* Settings: the nmlSet keys on the passive Mie path
  * (src/settings.f90:454-573; python/pyPamtra/core.py:89-157). */

@@ -16,8 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libpamtra_b200.so")
 
 PREC_FP64 = 0           # reference operation order (plain drop-in)
-PREC_3XTF32 = 1         # batched: 3xTF32 tensor-core doubling, one-inverse adding
+PREC_3XTF32 = 1         # batched: 3xTF32 tensor-core doubling and (NUMMU 16) adding, FP64 inverses
 PREC_FP64_BATCHED = 2   # batched: FP64, one-inverse adding
+PREC_3XTF32_FP64ADD = 3  # batched: 3xTF32 doubling, FP64 one-inverse adding
 
 ST_NORM = 0x100
 ST_PSD = 0x200

@@ -1,0 +1,518 @@
+// Split-precision adding of the batched form (NUMMU = 16, n = 32): the
+// COMBINE_LAYERS4 products (src/radintg4.f90:447-513, one-inverse form) run
+// as 3xTF32 tcgen05 MMAs with FP32 accumulation; the (I - R1+ R2)^-1 solve of
+// every combine stays FP64 (Neumann series on the FP64 tensor path or
+// Gauss-Jordan), and so do the surface coupling and the internal radiances
+// (k_adding_finish, the FP64 code of k_adding).
+//
+// Per (column, frequency) unit the stack (R+, R-, T+, T-, S+, S-) is held in
+// FP32 masters in shared memory.  With Gp = (I - R1+ R2)^-1 a combine is five
+// MMA passes and the FP64 inverse:
+//   P1  Rp x [R2, T2]        -> Gin = Rp R2 (inverted in FP64 -> G), Z = Rp T2
+//   P2  G  x [Z, Tp]         -> Y = G Z,  W = G Tp
+//   P3  T2 x [Y, W]          -> Rp' = R2 + T2 Y,  Tp' = T2 W
+//   P4  [Tm x R2, R2 x Y]    -> V = Tm R2,  U = T2 + R2 Y
+//   P5  [V x W, Tm x U]      -> Rm' = Rm + V W,  Tm' = Tm U
+// and the source chains (FP32 matrix-vector products on the CUDA cores,
+// overlapped with the MMAs): w = S1+ + Rp S2-, Gp w, S+' = S2+ + T2 Gp w;
+// m = S2- + R2 S1+, Gm m = m + R2 Gp (Rp m), S-' = S1- + Tm Gm m.
+//
+// Pairing as in k_layer_tc: one CTA (4 warps) carries two units in lockstep;
+// warp 2i + p owns product p of unit i (its D lanes hold the columns of the
+// product).  Passes whose two products share the left factor (P1-P3) use
+// N = 64 (B = the two units' left factors); P4 and P5 use N = 128 (B = four
+// left factors) and read the diagonal 32 x 32 blocks of D.  Off-diagonal
+// blocks are computed and ignored, so a unit's results do not depend on its
+// partner.  Consecutive units are the frequencies of one column, whose
+// scattering layers coincide, so the pair rarely waits on itself.
+//
+// The layer records come from k_layer_tc in FP32 (the masters' swizzled
+// layout) and are copied into shared memory with cp.async while the previous
+// combine's last pass runs.
+#pragma once
+#include "layer_tc.cuh"
+
+namespace pb {
+
+// FP32 stack record of one (column, frequency) unit, handed to k_adding_finish
+constexpr int STK_RP = 0, STK_RM = 1024, STK_TP = 2048, STK_TM = 3072, STK_SP = 4096, STK_SM = 4128, STK_T1 = 4160,
+              STK_HDR = 4192, STK_FLOATS = 4224;  // header: sstate, status (int bits)
+
+struct AddTcItem {
+  float m[8][1024];  // masters; roles (R+, R-, T+, T-, R2, T2, G, Z) fixed except T+ <-> G each combine
+  float sp[32], sm[32], s2p[32], s2m[32], t1[32];
+  float t2[32], c2p[32], c2m[32];  // a clear layer (never the prefetch target)
+  float nsp[32], nsm[32], wv[32], wv2[32], u1[32], u2[32], mw[32], u1b[32];
+};
+
+struct AddTcTiles {
+  float b_hi[128 * 32], b_lo[128 * 32];  // B tile pair, up to 128 rows
+};
+struct AddTcInv {
+  double P[Team<32>::MAT], G[Team<32>::MAT];
+  InvScratch<32> inv;
+};
+union __align__(128) AddTcScratch {
+  AddTcTiles tl;
+  AddTcInv fp;  // FP64 inverse of one unit at a time
+};
+
+struct AddTcSmem {
+  AddTcItem it[2];
+  AddTcScratch u;
+  double mu[16], wq[16];
+};
+static_assert(sizeof(AddTcItem) % 16 == 0, "alignment of the masters");
+
+constexpr size_t add_tc_smem() { return sizeof(AddTcSmem); }
+
+// barrier of the two warps of unit i (named barrier 1 + i, 64 threads)
+__device__ __forceinline__ void unit_sync(int i) {
+  if (i == 0) asm volatile("bar.sync 1, 64;" ::: "memory");
+  else asm volatile("bar.sync 2, 64;" ::: "memory");
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(tc::smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// row r of M times x (k ascending), M a swizzled master
+__device__ __forceinline__ float mv32(const float* __restrict__ M, const float* __restrict__ x, const RowOff& ro) {
+  float a = 0.f;
+#pragma unroll
+  for (int k = 0; k < 32; k += 4) {
+    const float4 p = *reinterpret_cast<const float4*>(x + k);
+    a = fmaf(M[k * 32 + ro.o[k & 7]], p.x, a);
+    a = fmaf(M[(k + 1) * 32 + ro.o[(k + 1) & 7]], p.y, a);
+    a = fmaf(M[(k + 2) * 32 + ro.o[(k + 2) & 7]], p.z, a);
+    a = fmaf(M[(k + 3) * 32 + ro.o[(k + 3) & 7]], p.w, a);
+  }
+  return a;
+}
+
+// B row `brow` <- row `lane` of master bsrc, all 32 K values (N = 128 passes)
+__device__ __forceinline__ void build_b_full(AddTcTiles& TL, const float* bsrc, int brow, const RowOff& ro) {
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    const int k0 = 4 * q;
+    float4 hi, lo;
+    const float* bc = bsrc + k0 * 32;
+    tc::split(bc[0 * 32 + ro.o[(k0 + 0) & 7]], hi.x, lo.x);
+    tc::split(bc[1 * 32 + ro.o[(k0 + 1) & 7]], hi.y, lo.y);
+    tc::split(bc[2 * 32 + ro.o[(k0 + 2) & 7]], hi.z, lo.z);
+    tc::split(bc[3 * 32 + ro.o[(k0 + 3) & 7]], hi.w, lo.w);
+    const int o = (brow >> 3) * tc::RG_FLOATS + q * 32 + (brow & 7) * 4;
+    *reinterpret_cast<float4*>(TL.b_hi + o) = hi;
+    *reinterpret_cast<float4*>(TL.b_lo + o) = lo;
+  }
+}
+
+// A row of this thread <- column `lane` of master asrc (hi / lo into TMEM)
+__device__ __forceinline__ void build_a(const float* asrc, uint32_t ta_hi, uint32_t ta_lo, int lane) {
+  float c[32], lo[32];
+  ld_col(asrc, lane, c);
+#pragma unroll
+  for (int r = 0; r < 32; r++) tc::split(c[r], c[r], lo[r]);
+  tc::tmem_st32(ta_hi, c);
+  tc::tmem_st32(ta_lo, lo);
+}
+
+// B rows 32 mi + lane, K-half h <- row `lane` of master bsrc (N = 64 passes)
+__device__ __forceinline__ void build_b_half(AddTcTiles& TL, const float* bsrc, int brow, int h, const RowOff& ro) {
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int k0 = 16 * h + 4 * q;
+    float4 hi, lo;
+    const float* bc = bsrc + k0 * 32;
+    tc::split(bc[0 * 32 + ro.o[(4 * q + 0) & 7]], hi.x, lo.x);
+    tc::split(bc[1 * 32 + ro.o[(4 * q + 1) & 7]], hi.y, lo.y);
+    tc::split(bc[2 * 32 + ro.o[(4 * q + 2) & 7]], hi.z, lo.z);
+    tc::split(bc[3 * 32 + ro.o[(4 * q + 3) & 7]], hi.w, lo.w);
+    const int o = (brow >> 3) * tc::RG_FLOATS + (k0 >> 2) * 32 + (brow & 7) * 4;
+    *reinterpret_cast<float4*>(TL.b_hi + o) = hi;
+    *reinterpret_cast<float4*>(TL.b_lo + o) = lo;
+  }
+}
+
+// Issue the copy of layer record `item` into masters R2 / T2 and the layer
+// sources (the 64 threads of the unit).
+__device__ __forceinline__ void lay32_fetch(const Work& w, int item, AddTcItem& U, int r2, int t2, int u) {
+  const float* rec = reinterpret_cast<const float*>(w.lay + (size_t)item * w.lay_stride);
+  for (int q = u; q < 256; q += 64) {
+    cp_async16(&U.m[r2][4 * q], rec + LAY32_R + 4 * q);
+    cp_async16(&U.m[t2][4 * q], rec + LAY32_T + 4 * q);
+  }
+  if (u < 8) cp_async16(&U.s2p[4 * u], rec + LAY32_SP + 4 * u);
+  else if (u < 16) cp_async16(&U.s2m[4 * (u - 8)], rec + LAY32_SM + 4 * (u - 8));
+}
+
+// next scattering layer at or below top-down index k0 of column c (-1: none)
+__device__ __forceinline__ int next_scat(const Batch& b, const Work& w, int c, int L, int k0, int& pidx) {
+  const int Lm = b.max_nlyrs;
+  for (int k = k0; k < L; k++) {
+    const int p = w.pres_idx[(size_t)c * Lm + (L - 1 - k)];
+    if (p >= 0) { pidx = p; return k; }
+  }
+  pidx = -1;
+  return -1;
+}
+
+template <int N>
+__global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b200_settings st) {
+  static_assert(N == 16, "the split-precision adding kernel is built for NUMMU = 16");
+  constexpr int n = 32;
+  enum { P1 = 0, P2, P3, P4, P5 };
+  enum { RP = 0, RM, TP, TM, R2, T2, GG, ZZ };
+  extern __shared__ __align__(1024) double smem_raw[];
+  AddTcSmem& Q = *reinterpret_cast<AddTcSmem*>(smem_raw);
+  AddTcTiles& TL = Q.u.tl;
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tslot;
+  __shared__ int s_base, s_dead, s_gg[2];
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int mi = warp >> 1, slot = warp & 1, u = t & 63;
+  AddTcItem& U = Q.it[mi];
+  const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
+  const int nunits = b.ncol * Fm;
+  if (warp == 0) tc::tmem_alloc(&tslot, 256);  // D: columns 0..127, A hi: 128..159, A lo: 160..191
+  if (t == 0) {
+    tc::mbar_init(&mbar, 1);
+    s_dead = 0;
+  }
+  if (t < N) { Q.mu[t] = w.lob_mu[lob_off(N) + t]; Q.wq[t] = w.lob_w[lob_off(N) + t]; }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t lanes = (uint32_t)(warp * 32) << 16;
+  const uint32_t ta_hi = tslot + lanes + 128u, ta_lo = tslot + lanes + 160u;
+  const RowOff ro(lane);
+  uint32_t parity = 0;
+
+  for (;;) {
+    __syncthreads();
+    if (t == 0) s_base = atomicAdd(&w.counters[6], 2);
+    __syncthreads();
+    const int base = s_base;
+    if (base >= nunits) break;
+    // ---- my unit
+    const int unit = base + mi;
+    int c = 0, fi = 0, L = 0, status = 0;
+    bool valid = false;
+    if (unit < nunits) {
+      c = unit / Fm;
+      fi = unit % Fm;
+      valid = fi < b.col_nfreq(c) && b.col_nummu(c) == N;
+    }
+    double wl = 0.0;
+    if (valid) {
+      L = b.nlyrs[c];
+      wl = C_LIGHT / (b.freq(c, fi) * 1.e3);
+      status = w.col_status[c];
+    }
+    float* stk = w.add_stk + (size_t)unit * STK_FLOATS;
+    if (s_dead) {  // after a timed-out wait: report the unit, compute nothing
+      if (valid && u == 0) {
+        reinterpret_cast<int*>(stk + STK_HDR)[0] = 0;
+        reinterpret_cast<int*>(stk + STK_HDR)[1] = status | PAMTRA_B200_FATAL | PAMTRA_B200_ST_TIMEOUT;
+      }
+      continue;
+    }
+    const double* hl = w.hgt_lev + (size_t)c * (Lm + 1);
+    const double* tl = w.temp_lev + (size_t)c * (Lm + 1);
+    int tp = TP, gg = GG;   // T+ and G trade buffers every combine
+    int sstate = 0;         // 0 empty, 1 clear (t1, sp, sm), 2 general
+    int k = 0;              // next top-down layer
+    int pf_k = -1;          // layer whose record is in (or on its way to) R2 / T2
+    bool ok = true;
+    for (;;) {
+      // ---- advance my unit to its next combine (clear layers, the first scattering layer)
+      bool comb = false;
+      while (valid && k < L) {
+        const int z = L - 1 - k;
+        const int pidx = w.pres_idx[(size_t)c * Lm + z];
+        if (pidx < 0) {
+          // NONSCATTER_LAYER4 (src/radintg4.f90:79-117)
+          if (u < n) {
+            const int jj = u >> 1, i = u & 1;
+            const double zdiff = fabs(hl[z + 1] - hl[z]);
+            const double gas = fmax(w.kgas[((size_t)c * Fm + fi) * Lm + z], 0.0);
+            const double dtau = zdiff * gas;
+            const double p0 = planck(tl[z + 1], wl), p1 = planck(tl[z], wl);
+            U.t2[u] = (float)exp(-dtau / Q.mu[jj]);
+            double a = 0.0, bq = 0.0;
+            if (dtau > 0.0 && i == 0) {
+              const double path = dtau / Q.mu[jj];
+              const double slope = (p1 - p0) / path;
+              a = p1 - slope - (p1 - slope * (1.0 + path)) * exp(-path);
+              bq = p0 + slope - (p0 + slope * (1.0 + path)) * exp(-path);
+            }
+            U.c2p[u] = (float)a;
+            U.c2m[u] = (float)bq;
+          }
+          unit_sync(mi);
+          if (sstate == 0) {
+            if (u < n) { U.t1[u] = U.t2[u]; U.sp[u] = U.c2p[u]; U.sm[u] = U.c2m[u]; }
+            sstate = 1;
+          } else if (sstate == 1) {
+            if (u < n) {
+              const float sp = U.c2p[u] + U.t2[u] * U.sp[u];
+              const float sm = U.sm[u] + U.t1[u] * U.c2m[u];
+              U.t1[u] = U.t2[u] * U.t1[u];
+              U.sp[u] = sp;
+              U.sm[u] = sm;
+            }
+          } else {
+            if (u < n) U.nsp[u] = U.c2p[u] + U.t2[u] * (U.sp[u] + mv32(U.m[RP], U.c2m, ro));
+            else U.nsm[lane] = U.sm[lane] + mv32(U.m[TM], U.c2m, ro);
+            unit_sync(mi);
+            for (int s = u; s < 1024; s += 64) {
+              int r, cc;
+              midx_inv(s, r, cc);
+              const float t2i = U.t2[r], t2j = U.t2[cc];
+              U.m[RP][s] = t2i * (U.m[RP][s] * t2j);
+              U.m[tp][s] = t2i * U.m[tp][s];
+              U.m[TM][s] = U.m[TM][s] * t2j;
+            }
+            if (u < n) { U.sp[u] = U.nsp[u]; U.sm[u] = U.nsm[u]; }
+          }
+          unit_sync(mi);
+          k++;
+          continue;
+        }
+        // scattering layer: its record into R2 / T2
+        if (pf_k != k) lay32_fetch(w, pidx * Fm + fi, U, R2, T2, u);
+        cp_async_wait_all();
+        unit_sync(mi);
+        pf_k = -1;
+        if (sstate == 2) {
+          comb = true;
+          break;
+        }
+        if (sstate == 0) {
+          for (int s = u; s < 1024; s += 64) {
+            const float r2 = U.m[R2][s], t2 = U.m[T2][s];
+            U.m[RP][s] = r2; U.m[RM][s] = r2; U.m[tp][s] = t2; U.m[TM][s] = t2;
+          }
+          if (u < n) { U.sp[u] = U.s2p[u]; U.sm[u] = U.s2m[u]; }
+        } else {
+          // clear stack (t1, sp, sm) + scattering layer
+          if (u < n) U.nsp[u] = U.s2p[u] + mv32(U.m[T2], U.sp, ro);
+          else U.nsm[lane] = U.sm[lane] + U.t1[lane] * (U.s2m[lane] + mv32(U.m[R2], U.sp, ro));
+          for (int s = u; s < 1024; s += 64) {
+            int r, cc;
+            midx_inv(s, r, cc);
+            const float t1i = U.t1[r], t1j = U.t1[cc];
+            const float r2 = U.m[R2][s], t2 = U.m[T2][s];
+            U.m[RP][s] = r2;
+            U.m[RM][s] = t1i * (r2 * t1j);
+            U.m[tp][s] = t2 * t1j;
+            U.m[TM][s] = t1i * t2;
+          }
+          unit_sync(mi);
+          if (u < n) { U.sp[u] = U.nsp[u]; U.sm[u] = U.nsm[u]; }
+        }
+        sstate = 2;
+        unit_sync(mi);
+        k++;
+      }
+      const int pending = __syncthreads_or(comb && (t & 63) == 0);
+      if (!pending) break;
+      // ---- one combine of both units (a unit without one idles through the passes)
+      if (u == 0) s_gg[mi] = gg;  // published by the barriers of P1
+      for (int ph = P1; ph <= P5; ph++) {
+        const bool wide = ph >= P4;  // N = 128: four left factors
+        if (comb) {
+          int asrc, bsrc;
+          if (ph == P1) { asrc = slot ? T2 : R2; bsrc = RP; }
+          else if (ph == P2) { asrc = slot ? tp : ZZ; bsrc = gg; }
+          else if (ph == P3) { asrc = slot ? tp : ZZ; bsrc = T2; }   // W sits in T+'s buffer, Y in Z's
+          else if (ph == P4) { asrc = slot ? ZZ : R2; bsrc = slot ? R2 : TM; }
+          else { asrc = slot ? T2 : tp; bsrc = slot ? TM : ZZ; }      // U in T2's buffer, V in Z's
+          build_a(U.m[asrc], ta_hi, ta_lo, lane);
+          if (wide) build_b_full(TL, U.m[bsrc], 32 * warp + lane, ro);
+          else build_b_half(TL, U.m[bsrc], 32 * mi + lane, slot, ro);
+        }
+        tc::fence_async_smem();
+        tc::fence_before_sync();
+        __syncthreads();
+        tc::fence_after_sync();
+        if (t == 0)
+          tc::mma3_ta(tslot, tslot + 128u, tslot + 160u, TL.b_hi, TL.b_lo, &mbar,
+                      wide ? tc::IDESC_M128_N128 : tc::IDESC_M128_N64);
+        if (comb) {
+          // source chains on the CUDA cores while the MMA runs
+          if (ph == P1) {
+            if (slot == 0) U.wv[lane] = U.sp[lane] + mv32(U.m[RP], U.s2m, ro);
+            else U.mw[lane] = U.s2m[lane] + mv32(U.m[R2], U.sp, ro);
+          } else if (ph == P2) {
+            if (slot == 0) U.wv2[lane] = mv32(U.m[gg], U.wv, ro);
+            else U.u1[lane] = mv32(U.m[RP], U.mw, ro);
+          } else if (ph == P3) {
+            if (slot == 0) U.nsp[lane] = U.s2p[lane] + mv32(U.m[T2], U.wv2, ro);
+            else U.u2[lane] = mv32(U.m[gg], U.u1, ro);
+          } else if (ph == P4) {
+            if (slot == 0) U.u1b[lane] = U.mw[lane] + mv32(U.m[R2], U.u2, ro);
+          } else {
+            if (slot == 0) U.nsm[lane] = U.sm[lane] + mv32(U.m[TM], U.u1b, ro);
+            // R2, T2 and the layer sources are free now: fetch the next scattering layer
+            int pidx;
+            const int kn = next_scat(b, w, c, L, k + 1, pidx);
+            if (kn >= 0) lay32_fetch(w, pidx * Fm + fi, U, R2, T2, u);
+            pf_k = kn;
+          }
+        }
+        {
+          const bool mine = tc::mbar_wait(&mbar, parity, w.spin_limit);
+          parity ^= 1;
+          ok = __syncthreads_and(mine) != 0;
+          tc::fence_after_sync();
+        }
+        if (!ok) break;
+        if (comb) {
+          float dv[32], a[32];
+          tc::tmem_ld32(tslot + lanes + 32u * (wide ? warp : mi), dv);
+          if (ph == P1) {
+            st_col(U.m[slot ? ZZ : gg], lane, dv);  // Z = Rp T2;  Gin = Rp R2 (inverted below)
+          } else if (ph == P2) {
+            st_col(U.m[slot ? tp : ZZ], lane, dv);  // W = G Tp over T+;  Y = G Z over Z
+          } else if (ph == P3) {
+            if (slot == 0) {  // R+' = R2 + T2 Y
+              ld_col(U.m[R2], lane, a);
+#pragma unroll
+              for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
+              st_col(U.m[RP], lane, a);
+            } else {  // T+' = T2 W into G's buffer (G is dead)
+              st_col(U.m[gg], lane, dv);
+            }
+          } else if (ph == P4) {
+            if (slot == 0) {  // V = Tm R2 over Y (Z's buffer)
+              st_col(U.m[ZZ], lane, dv);
+            } else {  // U = T2 + R2 Y in place of T2
+              ld_col(U.m[T2], lane, a);
+#pragma unroll
+              for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
+              st_col(U.m[T2], lane, a);
+            }
+          } else {
+            if (slot == 0) {  // R-' = R- + V W
+              ld_col(U.m[RM], lane, a);
+#pragma unroll
+              for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
+              st_col(U.m[RM], lane, a);
+            } else {  // T-' = T- U
+              st_col(U.m[TM], lane, dv);
+            }
+          }
+        }
+        __syncthreads();
+        if (ph == P1) {
+          // FP64 (I - Gin)^-1 of each unit, one at a time through the scratch
+          for (int i = 0; i < 2; i++) {
+            const int on = __syncthreads_or(comb && mi == i);
+            if (!on) continue;
+            AddTcInv& F = Q.u.fp;
+            float* gm = Q.it[i].m[s_gg[i]];
+            for (int s = t; s < 1024; s += 128) {
+              int r, cc;
+              midx_inv(s, r, cc);
+              F.P[cc * Team<32>::LD + r] = (double)gm[s];
+            }
+            __syncthreads();
+            int sg = 0;
+            const double* Gi = inv_iminus<32>(F.P, F.G, F.inv, &sg);
+            if (sg && mi == i) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+            for (int s = t; s < 1024; s += 128) {
+              int r, cc;
+              midx_inv(s, r, cc);
+              gm[s] = (float)Gi[cc * Team<32>::LD + r];
+            }
+            __syncthreads();
+          }
+        }
+      }
+      if (!ok) break;
+      if (comb) {
+        const int o = tp; tp = gg; gg = o;  // T+' sits in G's buffer
+        if (u < n) { U.sp[u] = U.nsp[u]; U.sm[u] = U.nsm[u]; }
+        k++;
+      }
+      __syncthreads();
+    }
+    if (!ok) {
+      if (t == 0) s_dead = 1;
+      status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_TIMEOUT;
+      sstate = 0;
+      cp_async_wait_all();
+    }
+    // ---- the stack of my unit for k_adding_finish
+    if (valid) {
+      if (sstate == 2) {
+        for (int s = u; s < 1024; s += 64) {
+          stk[STK_RP + s] = U.m[RP][s];
+          stk[STK_RM + s] = U.m[RM][s];
+          stk[STK_TP + s] = U.m[tp][s];
+          stk[STK_TM + s] = U.m[TM][s];
+        }
+      }
+      if (u < n) {
+        stk[STK_SP + u] = U.sp[u];
+        stk[STK_SM + u] = U.sm[u];
+        stk[STK_T1 + u] = U.t1[u];
+      }
+      if (u == 0) {
+        reinterpret_cast<int*>(stk + STK_HDR)[0] = sstate;
+        reinterpret_cast<int*>(stk + STK_HDR)[1] = status;
+      }
+    }
+  }
+  if (s_dead) tc::mbar_wait(&mbar, parity ^ 1);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 0) tc::tmem_dealloc(tslot, 256);
+}
+
+// Surface, internal radiances and TB of the units k_adding_tc carried, in
+// FP64 from their FP32 stacks (the code of k_adding after its layer loop).
+template <int N>
+__global__ void __launch_bounds__(RTCfg<N>::T) k_adding_finish(Batch b, Work w, pamtra_b200_settings st,
+                                                               pamtra_b200_outputs out) {
+  constexpr int n = RTCfg<N>::n, LD = RTCfg<N>::LD, T = RTCfg<N>::T;
+  extern __shared__ double smem_raw[];
+  AddSmem<N>& S = *reinterpret_cast<AddSmem<N>*>(smem_raw);
+  const int t = threadIdx.x;
+  const int Fm = b.max_nfreq;
+  const int nunits = b.ncol * Fm;
+  if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
+  for (int unit = blockIdx.x; unit < nunits; unit += gridDim.x) {
+    const int c = unit / Fm, fi = unit % Fm;
+    if (fi >= b.col_nfreq(c) || b.col_nummu(c) != N) continue;
+    const float* stk = w.add_stk + (size_t)unit * STK_FLOATS;
+    const int sstate = reinterpret_cast<const int*>(stk + STK_HDR)[0];
+    const int status = reinterpret_cast<const int*>(stk + STK_HDR)[1];
+    double *Rp = S.m[0], *Rm = S.m[1], *Tp = S.m[2], *Tm = S.m[3];
+    if (sstate == 2) {
+      for (int s = t; s < 1024; s += T) {
+        int r, cc;
+        midx_inv(s, r, cc);
+        Rp[cc * LD + r] = stk[STK_RP + s];
+        Rm[cc * LD + r] = stk[STK_RM + s];
+        Tp[cc * LD + r] = stk[STK_TP + s];
+        Tm[cc * LD + r] = stk[STK_TM + s];
+      }
+    }
+    if (t < n) {
+      S.sp[t] = stk[STK_SP + t];
+      S.sm[t] = stk[STK_SM + t];
+      S.t1[t] = stk[STK_T1 + t];
+    }
+    team_sync();
+    const double wl = C_LIGHT / (b.freq(c, fi) * 1.e3);
+    adding_finish<N>(b, w, st, out, S, c, fi, b.nlyrs[c], wl, sstate, status, Rp, Rm, Tp, Tm, S.m[4], S.m[5],
+                     S.m[6], S.m[7], S.m[8]);
+    team_sync();
+  }
+}
+
+}  // namespace pb

@@ -25,6 +25,7 @@
 #include "tc.cuh"
 #include "layer_tc.cuh"
 #include "layer_tc64.cuh"
+#include "add_tc.cuh"
 #include "work.cuh"
 
 using namespace pb;
@@ -237,9 +238,10 @@ struct Plan {
   size_t o_slot_st, o_slot_nb, o_bd, o_bdd, o_bnd, o_brho, o_bmass;
   size_t o_pres_idx, o_plist, o_counters, o_mkext, o_msalb, o_mback, o_mrefr, o_mnleg, o_mlegen, o_lay, o_laynd, o_status,
       o_colst;
-  size_t o_species, o_addscr, o_mieslab;
+  size_t o_species, o_addscr, o_mieslab, o_addstk;
   int mie_nslab;  // k_mie warps the slabs are sized for
   bool f32_coef;
+  bool tc_add;  // split-precision adding for NUMMU 16 (FP32 layer records, stacks)
   int add_grid;  // CTAs of k_adding<32> the scratch is sized for
   int pmax;
   int max_nbin;
@@ -251,7 +253,8 @@ size_t lay_stride_for(int N) {
   return (lay_stride_n(N) + 1) & ~(size_t)1;  // keep 16-byte alignment of each item
 }
 
-Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms, int mie_slabs, bool f32_coef = false) {
+Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms, int mie_slabs, bool f32_coef = false,
+               bool tc_add = false) {
   Plan p{};
   size_t off = 0;
   auto take = [&](size_t bytes) {
@@ -309,6 +312,8 @@ Plan make_plan(const pamtra_b200_columns* c, int default_nummu, int sms, int mie
   // one slab per k_mie warp; more warps than (layer, frequency) items would idle
   p.mie_nslab = c->nhydro > 0 ? (int)std::min<size_t>((size_t)mie_slabs, items) : 0;
   p.o_mieslab = take((size_t)p.mie_nslab * MIE_SLAB_STRIDE * 8);
+  p.tc_add = tc_add && (mask & 2);
+  p.o_addstk = take(p.tc_add ? C * Fm * STK_FLOATS * 4 : 0);
   p.total = take(0) + 256;
   return p;
 }
@@ -512,6 +517,8 @@ static int set_smem_attrs() {
     set((const void*)k_adding<16, true>, sizeof(AddSmem<16>));
     set((const void*)k_adding<32, true>, sizeof(AddSmem<32>));
     set((const void*)k_minvert<64>, Team<64>::MAT * 8 + sizeof(InvScratch<64>));
+    set((const void*)k_adding_tc<16>, add_tc_smem());
+    set((const void*)k_adding_finish<16>, sizeof(AddSmem<16>));
   });
   return rc;
 }
@@ -591,7 +598,8 @@ size_t pamtra_b200_workspace_bytes(const pamtra_b200_columns* cols, int32_t prec
   if (!cols || !cols->species) return 0;
   int dev = 0, sms = 148;
   if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return make_plan(cols, 16, sms, sms * MIE_SLAB_WARPS_PER_SM, precision == PAMTRA_B200_PREC_3XTF32).total;
+  const bool split = precision == PAMTRA_B200_PREC_3XTF32 || precision == PAMTRA_B200_PREC_3XTF32_FP64ADD;
+  return make_plan(cols, 16, sms, sms * MIE_SLAB_WARPS_PER_SM, split, precision == PAMTRA_B200_PREC_3XTF32).total;
 }
 
 int32_t pamtra_b200_reserve(pamtra_b200_ctx* ctx, size_t bytes) {
@@ -756,9 +764,11 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
                         const pamtra_b200_outputs* out, int32_t precision, void* stream_) {
   if (!ctx || !st || !cols || !out || !out->tb) return PAMTRA_B200_FATAL;
   if (precision != PAMTRA_B200_PREC_FP64 && precision != PAMTRA_B200_PREC_3XTF32 &&
-      precision != PAMTRA_B200_PREC_FP64_BATCHED)
+      precision != PAMTRA_B200_PREC_FP64_BATCHED && precision != PAMTRA_B200_PREC_3XTF32_FP64ADD)
     return PAMTRA_B200_FATAL;
   const bool one_inv = precision != PAMTRA_B200_PREC_FP64;  // one inverse per adding combine
+  // split precision: 3xTF32 doubling (and, for PREC_3XTF32, adding of NUMMU 16)
+  const bool split = precision == PAMTRA_B200_PREC_3XTF32 || precision == PAMTRA_B200_PREC_3XTF32_FP64ADD;
   if (cols->ncol < 1 || cols->max_nlyrs < 2 || cols->max_nfreq < 1 || cols->noutlevels < 1 || cols->nhydro < 0)
     return PAMTRA_B200_FATAL;
   if (cols->nhydro > 0 && !cols->species) return PAMTRA_B200_FATAL;
@@ -776,7 +786,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   pamtra_b200_species dummy{};
   pamtra_b200_columns cc = *cols;
   if (cc.nhydro == 0) { cc.species = &dummy; cc.species_stride = 0; }
-  Plan pl = make_plan(&cc, st->nummu, ctx->sm_count, ctx->sm_count * MIE_SLAB_WARPS_PER_SM,
+  Plan pl = make_plan(&cc, st->nummu, ctx->sm_count, ctx->sm_count * MIE_SLAB_WARPS_PER_SM, split,
                       precision == PAMTRA_B200_PREC_3XTF32);
   if (pl.max_nbin > MAXBIN) return PAMTRA_B200_FATAL;
   if (pl.total > ctx->arena_bytes) {
@@ -847,6 +857,8 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
   w.m_legen = pl.f32_coef ? nullptr : (double*)(A + pl.o_mlegen);
   w.m_legen32 = pl.f32_coef ? (float*)(A + pl.o_mlegen) : nullptr;
   w.lay = (double*)(A + pl.o_lay); w.lay_stride = pl.lay_stride; w.lay_nd = (int*)(A + pl.o_laynd);
+  w.lay32 = pl.tc_add ? 1 : 0;
+  w.add_stk = pl.tc_add ? (float*)(A + pl.o_addstk) : nullptr;
   w.status = (int*)(A + pl.o_status); w.col_status = (int*)(A + pl.o_colst);
   w.add_scr = (double*)(A + pl.o_addscr);
   w.mie_slab = (double*)(A + pl.o_mieslab); w.mie_nslab = pl.mie_nslab;
@@ -937,7 +949,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     mark(ctx, stream, STG_ADDING);
   }
   if (mask & 2) {
-    if (H > 0 && precision == PAMTRA_B200_PREC_3XTF32) {
+    if (H > 0 && split) {
       // three CTAs (three item pairs) per SM by shared memory, registers and
       // tensor memory (3 x 128 columns); the persistent CTAs take pairs of
       // items from a counter
@@ -949,15 +961,24 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
       k_layer<16><<<g, RTCfg<16>::T, sizeof(LayerSmem<16>), stream>>>(b, w, *st, ssp); launches++;
     }
     mark(ctx, stream, STG_LAYER);
-    const int g = persistent_grid((const void*)k_adding<16>, RTCfg<16>::T, sizeof(AddSmem<16>), sms, ctx->adding_cps);
-    if (one_inv) k_adding<16, true><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out);
-    else k_adding<16><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out);
-    launches++;
+    if (pl.tc_add) {
+      // two CTAs (two unit pairs) per SM by shared memory and tensor memory
+      // (2 x 256 columns); the FP64 surface and radiance part follows
+      k_adding_tc<16><<<2 * sms, 128, add_tc_smem(), stream>>>(b, w, *st);
+      const int gf = persistent_grid((const void*)k_adding_finish<16>, RTCfg<16>::T, sizeof(AddSmem<16>), sms, 0);
+      k_adding_finish<16><<<gf, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out);
+      launches += 2;
+    } else {
+      const int g = persistent_grid((const void*)k_adding<16>, RTCfg<16>::T, sizeof(AddSmem<16>), sms, ctx->adding_cps);
+      if (one_inv) k_adding<16, true><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out);
+      else k_adding<16><<<g, RTCfg<16>::T, sizeof(AddSmem<16>), stream>>>(b, w, *st, *out);
+      launches++;
+    }
     mark(ctx, stream, STG_ADDING);
   }
   if (mask & 4) {
     int g = persistent_grid((const void*)k_layer<32>, RTCfg<32>::T, sizeof(LayerSmem<32>), sms, ctx->layer_cps);
-    if (H > 0 && precision == PAMTRA_B200_PREC_3XTF32) {
+    if (H > 0 && split) {
       // one item per CTA, one CTA per SM (165 KB shared memory, 256 TMEM columns)
       k_layer_tc64<<<sms, 128, layer_tc64_smem(), stream>>>(b, w, *st, ssp); launches++;
     } else if (H > 0) {

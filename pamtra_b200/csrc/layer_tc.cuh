@@ -51,6 +51,32 @@ struct RowOff {
   }
 };
 
+// FP32 layer record of one (present layer, frequency) item (in its w.lay slot),
+// read by the split-precision adding (k_adding_tc): R, T, S+, S-
+constexpr int LAY32_R = 0, LAY32_T = 1024, LAY32_SP = 2048, LAY32_SM = 2080, LAY32_FLOATS = 2112;
+
+// storage index s of a swizzled master -> (row, column)
+__device__ __forceinline__ void midx_inv(int s, int& r, int& c) {
+  c = s >> 5;
+  const int p = s & 31;
+  r = ((((p >> 2) ^ (c & 7))) << 2) | (p & 3);
+}
+
+// Write the FP32 layer record from FP64 R, T (column-major, leading dimension
+// LD) and the sources lin (S+ then S-), with T threads.
+template <int LD, int T>
+__device__ __forceinline__ void lay32_store(const Work& w, int item, const double* R, const double* Tm_,
+                                            const double* lin) {
+  float* rec = reinterpret_cast<float*>(w.lay + (size_t)item * w.lay_stride);
+  for (int s = threadIdx.x; s < 1024; s += T) {
+    int r, c;
+    midx_inv(s, r, c);
+    rec[LAY32_R + s] = (float)R[c * LD + r];
+    rec[LAY32_T + s] = (float)Tm_[c * LD + r];
+  }
+  for (int e = threadIdx.x; e < 64; e += T) rec[LAY32_SP + e] = (float)lin[e];
+}
+
 // FP32 state of one item of the pair.
 struct TcItemState {
   float rm[1024], tm[1024], gm[1024];    // R, T~, G~
@@ -247,7 +273,8 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
       LayerItem it;
       const bool valid = item < nitems && layer_setup<N>(b, w, st, ssp_scat, S, item, it);
       if (valid && it.nd == 0) {
-        layer_store<N>(w, item, S.r, S.t, S.lin);
+        if (w.lay32) lay32_store<LD, 128>(w, item, S.r, S.t, S.lin);
+        else layer_store<N>(w, item, S.r, S.t, S.lin);
       } else if (valid) {
         TcItemState& D = Q.st[i];
         for (int e = t; e < n * n; e += 128) {
@@ -467,10 +494,24 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
         s_status[1] |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_TIMEOUT;
       }
       __syncthreads();
-      // ---- layer R, T = I - T~, S+/S- in FP64
+      // ---- layer R, T = I - T~, S+/S- in FP64 (FP32 records for the split adding)
       for (int i = 0; i < 2; i++) {
         if (s_nd[i] == 0) continue;
         const TcItemState& D = Q.st[i];
+        if (w.lay32) {
+          float* rec = reinterpret_cast<float*>(w.lay + (size_t)(base + i) * w.lay_stride);
+          for (int s = t; s < n * n; s += 128) {
+            int r, cc;
+            midx_inv(s, r, cc);
+            rec[LAY32_R + s] = D.rm[s];
+            rec[LAY32_T + s] = (r == cc ? 1.0f : 0.0f) - D.tm[s];
+          }
+          if (t < n) {
+            rec[LAY32_SP + t] = D.src[0][t];
+            rec[LAY32_SM + t] = D.src[2][t];
+          }
+          continue;
+        }
         double* out = w.lay + (size_t)(base + i) * w.lay_stride;
         for (int e = t; e < n * n; e += 128) {
           const int cc = e >> 5, r = e & 31;

@@ -531,6 +531,169 @@ __device__ __forceinline__ void ew_diag(double* A, const double* d) {
   }
 }
 
+// End of the adding for one (column, frequency) unit: the stack (Rp, Rm, Tp,
+// Tm with sources S.sp / S.sm, or a clear stack t1 / sp / sm when sstate <= 1)
+// on the surface, the internal radiances at the output levels, TB, status.
+// R2, T2, G, X, Y are scratch matrices (G and X may be swapped by the
+// inverses).
+template <int N>
+__device__ __forceinline__ void adding_finish(const Batch& b, const Work& w, const pamtra_b200_settings& st,
+                                              const pamtra_b200_outputs& out, AddSmem<N>& S, int c, int fi,
+                                              int L, double wl, int sstate, int status, double* Rp, double* Rm,
+                                              double* Tp, double* Tm, double* R2, double* T2, double* G,
+                                              double* X, double* Y) {
+  constexpr int n = RTCfg<N>::n, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT, T = RTCfg<N>::T;
+  const int t = threadIdx.x;
+  const int Fm = b.max_nfreq;
+  // materialise a clear (or empty) stack
+  if (sstate <= 1) {
+    if (sstate == 0 && t < n) { S.t1[t] = 1.0; S.sp[t] = 0.0; S.sm[t] = 0.0; }
+    team_sync();
+    ew_diag<n>(Tp, S.t1);
+    ew_diag<n>(Tm, S.t1);
+    ew_zero<n>(Rp);
+    ew_zero<n>(Rm);
+    team_sync();
+  }
+  // surface (src/sfc_matrices.f90; default emissivity sfc_optics.f90:79-81)
+  // and sky (src/surface.f90:169-195)
+  const char refl = (char)b.sfc_refl[c];
+  const double e = st.emissivity, rr = 1.0 - e;
+  const double pg = planck(w.gtemp[c], wl), psky = planck(SKY_TEMP, wl);
+  for (int ee = t; ee < n * n; ee += T) {  // R2 := surface R- (R+ = 0), T2 := I
+    const int col = ee / n, row = ee % n;
+    double v = 0.0;
+    if (refl == 'S' || refl == 'F') {
+      const double r1 = (rr + rr) / 2.0, r2 = (rr - rr) / 2.0;
+      if ((row >> 1) == (col >> 1)) v = ((row & 1) == (col & 1)) ? r1 : r2;
+    } else if (refl == 'L') {
+      if ((row & 1) == 0 && (col & 1) == 0) v = 2.0 * rr * S.mu[col >> 1] * S.wq[col >> 1];
+    }
+    R2[col * LD + row] = v;
+    T2[col * LD + row] = (row == col) ? 1.0 : 0.0;
+  }
+  if (refl != 'S' && refl != 'F' && refl != 'L') status |= PAMTRA_B200_WARNING;
+  if (t < n) {
+    const int i = t & 1;
+    double gv = 0.0;
+    if (refl == 'S' || refl == 'F') {
+      const double r1 = (rr + rr) / 2.0, r2 = (rr - rr) / 2.0;
+      gv = (i == 0) ? (1.0 - r1) * pg : -r2 * pg;
+    } else if (refl == 'L') {
+      gv = (i == 0) ? e * pg : 0.0;
+    }
+    S.gnd[t] = gv;
+    S.sky[t] = (i == 0) ? (1.0 - 0.0) * psky : 0.0;
+    S.s2m[t] = 0.0;  // the surface carries no source in the adding
+  }
+  team_sync();
+  // output levels: L+1 -> (stack, surface); 1 -> (empty, stack on surface)
+  int lev_order[2] = {-1, -1};
+  for (int io = 0; io < b.noutlevels; io++) {
+    const int lev = w.outlev[(size_t)c * b.noutlevels + io];
+    if (lev == L + 1) lev_order[0] = io;
+    else if (lev == 1) lev_order[1] = io;
+    else status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;  // intermediate levels not supported
+  }
+  for (int pass = 0; pass < 2; pass++) {
+    const int io = lev_order[pass];
+    if (io < 0) continue;
+    if (pass == 1) {
+      // down stack for level 1: (stack) on top of (surface), minus side only
+      mm<n, MM_SET>(R2, Rp, G);  // GAMMAm = inv(I - Rsfc R1p)
+      team_sync();
+      {
+        int sg = 0;
+        double* gi = inv_iminus<n>(G, X, S.inv, &sg);
+        if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+        if (gi != G) { X = G; G = gi; }
+      }
+      mm<n, MM_SET>(R2, Tp, X);
+      if (t < n) S.wv[t] = 0.0 + mv_row<n>(R2, S.sp, t);
+      team_sync();
+      mm<n, MM_SET>(G, X, Y);
+      if (t < n) S.wv2[t] = mv_row<n>(G, S.wv, t);
+      team_sync();
+      mm<n, MM_ACC>(Tm, Y, Rm, Rm);
+      mm<n, MM_SET>(G, T2, X);
+      if (t < n) S.nsm[t] = S.sm[t] + mv_row<n>(Tm, S.wv2, t);
+      team_sync();
+      mm<n, MM_SET>(Tm, X, Y);  // new T- in Y
+      team_sync();
+      // up side: empty (R+ = 0, T+ = I, S+ = 0); down side: (new R-, new T-, new S-)
+      ew_zero<n>(Rp);
+      ew_ident<n>(Tp);
+      for (int ee = t; ee < MAT; ee += T) { R2[ee] = Rm[ee]; T2[ee] = Y[ee]; }
+      if (t < n) { S.sp[t] = 0.0; S.s2m[t] = S.nsm[t]; }
+      team_sync();
+    }
+    // INTERNAL_RADIANCE4 (src/radintg4.f90:119-172): up = (Rp, Tp, sp), down = (R2, T2, s2m)
+    mm<n, MM_SET>(Rp, R2, X);
+    if (t < n) S.wv[t] = mv_row<n>(T2, S.gnd, t);
+    team_sync();
+    double* Ginv;
+    {
+      int sg = 0;
+      Ginv = inv_iminus<n>(X, G, S.inv, &sg);
+      if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+    }
+    if (t < n) {
+      double s = mv_row<n>(Rp, S.wv, t);
+      s = mv_row<n>(Tp, S.sky, t) + s;
+      s = mv_row<n>(Rp, S.s2m, t) + s;
+      s = S.sp[t] + s;
+      S.wv2[t] = s;
+    }
+    team_sync();
+    if (t < n) S.dnrad[t] = mv_row<n>(Ginv, S.wv2, t);
+    team_sync();
+    mm<n, MM_SET>(R2, Rp, X);
+    if (t < n) S.wv[t] = mv_row<n>(Tp, S.sky, t);
+    team_sync();
+    {
+      int sg = 0;
+      Ginv = inv_iminus<n>(X, G, S.inv, &sg);
+      if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+    }
+    if (t < n) {
+      double s = mv_row<n>(R2, S.wv, t);
+      s = mv_row<n>(T2, S.gnd, t) + s;
+      s = mv_row<n>(R2, S.sp, t) + s;
+      s = S.s2m[t] + s;
+      S.wv2[t] = s;
+    }
+    team_sync();
+    if (t < n) S.uprad[t] = mv_row<n>(Ginv, S.wv2, t);
+    team_sync();
+    // collect_output + CONVERT_OUTPUT
+    if (t < N) {
+      const int jj = t;
+      double u0 = S.uprad[2 * jj], u1 = S.uprad[2 * jj + 1], d0 = S.dnrad[2 * jj], d1 = S.dnrad[2 * jj + 1];
+      if (st.outpol_vh) {
+        double iv = 0.5 * (u0 + u1), ih = 0.5 * (u0 - u1);
+        u0 = iv; u1 = ih;
+        iv = 0.5 * (d0 + d1); ih = 0.5 * (d0 - d1);
+        d0 = iv; d1 = ih;
+        u0 = 2.0 * u0; u1 = 2.0 * u1; d0 = 2.0 * d0; d1 = 2.0 * d1;
+      }
+      const int NA = 2 * b.max_nummu;
+      double* tbo = out.tb + ((size_t)c * b.noutlevels + io) * NA * Fm * 2;
+      const size_t up_i = ((size_t)(N - 1 - jj) * Fm + fi) * 2, dn_i = ((size_t)(N + jj) * Fm + fi) * 2;
+      tbo[up_i + 0] = rad_to_tb(u0, wl);
+      tbo[up_i + 1] = rad_to_tb(u1, wl);
+      tbo[dn_i + 0] = rad_to_tb(d0, wl);
+      tbo[dn_i + 1] = rad_to_tb(d1, wl);
+    }
+    team_sync();
+  }
+  if (t == 0) {
+    if (out.emissivity)
+      for (int i = 0; i < 2; i++)
+        for (int jj = 0; jj < N; jj++) out.emissivity[(((size_t)c * 2 + i) * Fm + fi) * b.max_nummu + jj] = e;
+    if (status) atomicOr(&w.status[(size_t)c * Fm + fi], status);
+  }
+}
+
 template <int N, bool ONE_INV = false>
 __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_b200_settings st,
                                                         pamtra_b200_outputs out) {
@@ -787,153 +950,7 @@ __global__ void __launch_bounds__(RTCfg<N>::T) k_adding(Batch b, Work w, pamtra_
       if (t < n) { S.sp[t] = S.nsp[t]; S.sm[t] = S.nsm[t]; }
       team_sync();
     }
-    // materialise a clear (or empty) stack
-    if (sstate <= 1) {
-      if (sstate == 0 && t < n) { S.t1[t] = 1.0; S.sp[t] = 0.0; S.sm[t] = 0.0; }
-      team_sync();
-      ew_diag<n>(Tp, S.t1);
-      ew_diag<n>(Tm, S.t1);
-      ew_zero<n>(Rp);
-      ew_zero<n>(Rm);
-      team_sync();
-    }
-    // surface (src/sfc_matrices.f90; default emissivity sfc_optics.f90:79-81)
-    // and sky (src/surface.f90:169-195)
-    const char refl = (char)b.sfc_refl[c];
-    const double e = st.emissivity, rr = 1.0 - e;
-    const double pg = planck(w.gtemp[c], wl), psky = planck(SKY_TEMP, wl);
-    for (int ee = t; ee < n * n; ee += T) {  // R2 := surface R- (R+ = 0), T2 := I
-      const int col = ee / n, row = ee % n;
-      double v = 0.0;
-      if (refl == 'S' || refl == 'F') {
-        const double r1 = (rr + rr) / 2.0, r2 = (rr - rr) / 2.0;
-        if ((row >> 1) == (col >> 1)) v = ((row & 1) == (col & 1)) ? r1 : r2;
-      } else if (refl == 'L') {
-        if ((row & 1) == 0 && (col & 1) == 0) v = 2.0 * rr * S.mu[col >> 1] * S.wq[col >> 1];
-      }
-      R2[col * LD + row] = v;
-      T2[col * LD + row] = (row == col) ? 1.0 : 0.0;
-    }
-    if (refl != 'S' && refl != 'F' && refl != 'L') status |= PAMTRA_B200_WARNING;
-    if (t < n) {
-      const int i = t & 1;
-      double gv = 0.0;
-      if (refl == 'S' || refl == 'F') {
-        const double r1 = (rr + rr) / 2.0, r2 = (rr - rr) / 2.0;
-        gv = (i == 0) ? (1.0 - r1) * pg : -r2 * pg;
-      } else if (refl == 'L') {
-        gv = (i == 0) ? e * pg : 0.0;
-      }
-      S.gnd[t] = gv;
-      S.sky[t] = (i == 0) ? (1.0 - 0.0) * psky : 0.0;
-      S.s2m[t] = 0.0;  // the surface carries no source in the adding
-    }
-    team_sync();
-    // output levels: L+1 -> (stack, surface); 1 -> (empty, stack on surface)
-    int lev_order[2] = {-1, -1};
-    for (int io = 0; io < b.noutlevels; io++) {
-      const int lev = w.outlev[(size_t)c * b.noutlevels + io];
-      if (lev == L + 1) lev_order[0] = io;
-      else if (lev == 1) lev_order[1] = io;
-      else status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_SIZE;  // intermediate levels not supported
-    }
-    for (int pass = 0; pass < 2; pass++) {
-      const int io = lev_order[pass];
-      if (io < 0) continue;
-      if (pass == 1) {
-        // down stack for level 1: (stack) on top of (surface), minus side only
-        mm<n, MM_SET>(R2, Rp, G);  // GAMMAm = inv(I - Rsfc R1p)
-        team_sync();
-        {
-          int sg = 0;
-          double* gi = inv_iminus<n>(G, X, S.inv, &sg);
-          if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-          if (gi != G) { X = G; G = gi; }
-        }
-        mm<n, MM_SET>(R2, Tp, X);
-        if (t < n) S.wv[t] = 0.0 + mv_row<n>(R2, S.sp, t);
-        team_sync();
-        mm<n, MM_SET>(G, X, Y);
-        if (t < n) S.wv2[t] = mv_row<n>(G, S.wv, t);
-        team_sync();
-        mm<n, MM_ACC>(Tm, Y, Rm, Rm);
-        mm<n, MM_SET>(G, T2, X);
-        if (t < n) S.nsm[t] = S.sm[t] + mv_row<n>(Tm, S.wv2, t);
-        team_sync();
-        mm<n, MM_SET>(Tm, X, Y);  // new T- in Y
-        team_sync();
-        // up side: empty (R+ = 0, T+ = I, S+ = 0); down side: (new R-, new T-, new S-)
-        ew_zero<n>(Rp);
-        ew_ident<n>(Tp);
-        for (int ee = t; ee < MAT; ee += T) { R2[ee] = Rm[ee]; T2[ee] = Y[ee]; }
-        if (t < n) { S.sp[t] = 0.0; S.s2m[t] = S.nsm[t]; }
-        team_sync();
-      }
-      // INTERNAL_RADIANCE4 (src/radintg4.f90:119-172): up = (Rp, Tp, sp), down = (R2, T2, s2m)
-      mm<n, MM_SET>(Rp, R2, X);
-      if (t < n) S.wv[t] = mv_row<n>(T2, S.gnd, t);
-      team_sync();
-      double* Ginv;
-      {
-        int sg = 0;
-        Ginv = inv_iminus<n>(X, G, S.inv, &sg);
-        if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-      }
-      if (t < n) {
-        double s = mv_row<n>(Rp, S.wv, t);
-        s = mv_row<n>(Tp, S.sky, t) + s;
-        s = mv_row<n>(Rp, S.s2m, t) + s;
-        s = S.sp[t] + s;
-        S.wv2[t] = s;
-      }
-      team_sync();
-      if (t < n) S.dnrad[t] = mv_row<n>(Ginv, S.wv2, t);
-      team_sync();
-      mm<n, MM_SET>(R2, Rp, X);
-      if (t < n) S.wv[t] = mv_row<n>(Tp, S.sky, t);
-      team_sync();
-      {
-        int sg = 0;
-        Ginv = inv_iminus<n>(X, G, S.inv, &sg);
-        if (sg) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-      }
-      if (t < n) {
-        double s = mv_row<n>(R2, S.wv, t);
-        s = mv_row<n>(T2, S.gnd, t) + s;
-        s = mv_row<n>(R2, S.sp, t) + s;
-        s = S.s2m[t] + s;
-        S.wv2[t] = s;
-      }
-      team_sync();
-      if (t < n) S.uprad[t] = mv_row<n>(Ginv, S.wv2, t);
-      team_sync();
-      // collect_output + CONVERT_OUTPUT
-      if (t < N) {
-        const int jj = t;
-        double u0 = S.uprad[2 * jj], u1 = S.uprad[2 * jj + 1], d0 = S.dnrad[2 * jj], d1 = S.dnrad[2 * jj + 1];
-        if (st.outpol_vh) {
-          double iv = 0.5 * (u0 + u1), ih = 0.5 * (u0 - u1);
-          u0 = iv; u1 = ih;
-          iv = 0.5 * (d0 + d1); ih = 0.5 * (d0 - d1);
-          d0 = iv; d1 = ih;
-          u0 = 2.0 * u0; u1 = 2.0 * u1; d0 = 2.0 * d0; d1 = 2.0 * d1;
-        }
-        const int NA = 2 * b.max_nummu;
-        double* tbo = out.tb + ((size_t)c * b.noutlevels + io) * NA * Fm * 2;
-        const size_t up_i = ((size_t)(N - 1 - jj) * Fm + fi) * 2, dn_i = ((size_t)(N + jj) * Fm + fi) * 2;
-        tbo[up_i + 0] = rad_to_tb(u0, wl);
-        tbo[up_i + 1] = rad_to_tb(u1, wl);
-        tbo[dn_i + 0] = rad_to_tb(d0, wl);
-        tbo[dn_i + 1] = rad_to_tb(d1, wl);
-      }
-      team_sync();
-    }
-    if (t == 0) {
-      if (out.emissivity)
-        for (int i = 0; i < 2; i++)
-          for (int jj = 0; jj < N; jj++) out.emissivity[(((size_t)c * 2 + i) * Fm + fi) * b.max_nummu + jj] = e;
-      if (status) atomicOr(&w.status[(size_t)c * Fm + fi], status);
-    }
+    adding_finish<N>(b, w, st, out, S, c, fi, L, wl, sstate, status, Rp, Rm, Tp, Tm, R2, T2, G, X, Y);
   }
 }
 

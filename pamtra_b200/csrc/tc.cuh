@@ -26,12 +26,13 @@ namespace tc {
 
 constexpr int TILE_K = 32;               // K extent of every operand tile
 constexpr int RG_FLOATS = 256;           // floats per 8-row group of an A tile (8 chunks x 32)
-// instruction descriptors: D = F32, A = B = TF32, both K-major, M = 128, N = 32 or 64
+// instruction descriptors: D = F32, A = B = TF32, both K-major, M = 128, N = 32, 64 or 128
 constexpr uint32_t idesc_tf32(uint32_t m, uint32_t n) {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((n >> 3) << 17) | ((m >> 4) << 24);
 }
 constexpr uint32_t IDESC_M128_N32 = idesc_tf32(128, 32);
 constexpr uint32_t IDESC_M128_N64 = idesc_tf32(128, 64);
+constexpr uint32_t IDESC_M128_N128 = idesc_tf32(128, 128);
 constexpr uint32_t MBAR_SPIN_LIMIT = 1u << 24;  // bounded waits on MMA completion
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {

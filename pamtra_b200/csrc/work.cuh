@@ -73,6 +73,8 @@ struct Work {
   double* lay;                         // [pmax*Fm][lay_stride]
   size_t lay_stride;
   int* lay_nd;                         // [pmax*Fm]
+  int lay32;                           // k_layer_tc writes FP32 layer records (add_tc.cuh) for k_adding_tc
+  float* add_stk;                      // [C*Fm][STK_FLOATS] FP32 adding stacks, k_adding_tc -> k_adding_finish
   // adding matrices that do not fit in shared memory (N = 32 only)
   double* add_scr;                     // [adding CTAs][4][MAT]
   // scatcnv weight tables per NUMMU index (0: N = 8, 1: 16, 2: 32); null = direct sums

@@ -1,9 +1,10 @@
 """Per-stage device times of the batched forward path on the seeded workloads.
 
 ``python -m pamtra_b200.stages [--workload c2|target|uneven|mieheavy] [--ncol N]
-[--precision fp64|fp64b|3xtf32|both|all] [--reps K]`` runs one untimed and
+[--precision fp64|fp64b|3xtf32|3xtf32d|both|all] [--reps K]`` runs one untimed and
 K timed batches per precision (fp64: the reference operation order, fp64b:
-the batched FP64 form, 3xtf32: the split-precision form) through
+the batched FP64 form, 3xtf32: the split-precision form, 3xtf32d: its
+doubling with the FP64 adding) through
 :func:`pamtra_b200.batch.run` and prints one JSON line per precision:
 milliseconds per stage (CUDA events the library records between its kernels
 on the run's stream), the number of (layer, frequency) items and their mean
@@ -57,7 +58,7 @@ def run(name, ncol, precisions, reps, device=0, nummu=None):
         nd = out["num_doubles"].cpu().numpy()
         d = nd[nd > 0]
         tbs.append(out["tb"].cpu().numpy())
-        lines.append({"workload": name, "columns": b.ncol, "precision": ["fp64", "3xtf32", "fp64_batched"][prec],
+        lines.append({"workload": name, "columns": b.ncol, "precision": ["fp64", "3xtf32", "fp64_batched", "3xtf32_fp64add"][prec],
                       "stage_ms": tot, "items": int(np.count_nonzero(nd >= 0)),
                       "doublings_mean": float(d.mean()) if d.size else 0.0,
                       "status_nonzero": int((out["status"] != 0).sum())})
@@ -72,11 +73,11 @@ def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--workload", default="c2", choices=["c2", "target", "uneven", "mieheavy"])
     ap.add_argument("--ncol", type=int, default=256)
-    ap.add_argument("--precision", default="both", choices=["fp64", "3xtf32", "fp64b", "both", "all"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "3xtf32", "fp64b", "3xtf32d", "both", "all"])
     ap.add_argument("--reps", type=int, default=2)
     ap.add_argument("--nummu", type=int, default=0, choices=[0, 8, 16, 32], help="uneven workload: one NUMMU only")
     a = ap.parse_args(argv)
-    precs = {"fp64": [0], "3xtf32": [1], "fp64b": [2], "both": [0, 1], "all": [0, 2, 1]}[a.precision]
+    precs = {"fp64": [0], "3xtf32": [1], "fp64b": [2], "3xtf32d": [3], "both": [0, 1], "all": [0, 2, 1, 3]}[a.precision]
     for ln in run(a.workload, a.ncol, precs, a.reps, nummu=a.nummu or None):
         print(json.dumps(ln))
 
