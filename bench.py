@@ -650,15 +650,23 @@ def main():
     e2e_total = replicas.max_over_ranks(e2e_total)
     h2d = sum(v.nbytes for v in b.host.values() if isinstance(v, np.ndarray))
     d2h = sum(v.nbytes for v in hout.values())
-    # ---- split-precision batched form (3xTF32 tcgen05 doubling) on the same columns
-    from pamtra_b200._native import PREC_3XTF32
+    # ---- split-precision batched form (3xTF32 tcgen05 doubling and adding) on the same columns
+    from pamtra_b200._native import PREC_3XTF32, PREC_3XTF32_FP64ADD
     sout = b.alloc_outputs(dev)
     shape_s, _ = autotune.tune(b, local, precision=PREC_3XTF32, eng=eng, stream=stream, outputs=sout)
     sms_, sstages = _timed_steps(b, local, eng, stream, sout, PREC_3XTF32, args.steps, args.warmup, flush)
-    eng.set_launch(shape64)
     split_value = world * solves_step / (np.mean(sms_) * 1e-3)
     tb_split = sout["tb"].cpu().numpy()
     split_err_f64 = float(np.max(np.abs(tb_split - out["tb"].cpu().numpy())))
+    # the same with the FP64 adding (split-precision doubling only), for comparison
+    fout = b.alloc_outputs(dev)
+    fms_, fstages = _timed_steps(b, local, eng, stream, fout, PREC_3XTF32_FP64ADD, args.steps, args.warmup, flush)
+    eng.set_launch(shape64)
+    split_fa = {"value": world * solves_step / (np.mean(fms_) * 1e-3), "unit": "solves/s",
+                "ms_per_step": float(np.mean(fms_)), "stage_ms": fstages,
+                "tb_err_vs_fp64_batched_K": float(np.max(np.abs(fout["tb"].cpu().numpy() - out["tb"].cpu().numpy()))),
+                "form": "PREC_3XTF32_FP64ADD: the 3xTF32 doubling with the one-inverse FP64 adding"}
+    del fout
     # ---- plain form: one column per call
     nplain = 32
     plain_batches = [pbatch.pack_pam(c2_pam(1, seed=1000 + i), FREQS) for i in range(nplain)]
@@ -772,8 +780,10 @@ def main():
                          "over_plain": split_value / world / plain_value,
                          "tb_err_vs_fp64_batched_K": split_err_f64,
                          "tb_err_vs_oracle_K": split_err_oracle, "stage_ms": sstages,
-                         "form": "doubling products as 3xTF32 tcgen05 MMAs (FP32 accumulation in TMEM); "
-                                 "thin-layer init, adding and surface in FP64"},
+                         "form": "doubling and adding products as 3xTF32 tcgen05 MMAs (FP32 accumulation in "
+                                 "TMEM); thin-layer init, the (I - R R)^-1 of each combine, sources of the "
+                                 "doubling setup, surface and radiances in FP64",
+                         "with_fp64_adding": split_fa},
         "stage_ms": {k: v / args.steps for k, v in stage_tot.items()},
         "serving": serving,
         "target_shape": target,
@@ -792,6 +802,9 @@ def main():
     line["summary"] = {
         "c2_batched_fp64": value, "c2_batched_3xtf32": split_value, "c2_plain_fp64": plain_value,
         "c2_fp64_over_plain": value / world / plain_value, "c2_3xtf32_over_fp64": split_value / value,
+        "c2_3xtf32_fp64_adding": split_fa["value"],
+        "c2_adding_ms": {"fp64": stage_tot.get("adding", 0.0) / args.steps, "3xtf32": sstages.get("adding"),
+                         "3xtf32_fp64_adding": fstages.get("adding")},
         "c2_tb_err_vs_oracle_K": {"fp64": tb_err, "3xtf32": split_err_oracle},
         "target_fp64_over_plain": g(target, "batched_over_plain"),
         "target_3xtf32_over_plain": g(target, "batched_3xtf32_over_plain"),

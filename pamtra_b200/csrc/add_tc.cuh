@@ -2,51 +2,60 @@
 // COMBINE_LAYERS4 products (src/radintg4.f90:447-513, one-inverse form) run
 // as 3xTF32 tcgen05 MMAs with FP32 accumulation; the (I - R1+ R2)^-1 solve of
 // every combine stays FP64 (Neumann series on the FP64 tensor path or
-// Gauss-Jordan), and so do the surface coupling and the internal radiances
-// (k_adding_finish, the FP64 code of k_adding).
+// Gauss-Jordan), and so do the source vectors, the surface coupling and the
+// internal radiances (k_adding_finish, the FP64 code of k_adding).
 //
-// Per (column, frequency) unit the stack (R+, R-, T+, T-, S+, S-) is held in
-// FP32 masters in shared memory.  With Gp = (I - R1+ R2)^-1 a combine is five
-// MMA passes and the FP64 inverse:
-//   P1  Rp x [R2, T2]        -> Gin = Rp R2 (inverted in FP64 -> G), Z = Rp T2
-//   P2  G  x [Z, Tp]         -> Y = G Z,  W = G Tp
-//   P3  T2 x [Y, W]          -> Rp' = R2 + T2 Y,  Tp' = T2 W
-//   P4  [Tm x R2, R2 x Y]    -> V = Tm R2,  U = T2 + R2 Y
-//   P5  [V x W, Tm x U]      -> Rm' = Rm + V W,  Tm' = Tm U
-// and the source chains (FP32 matrix-vector products on the CUDA cores,
-// overlapped with the MMAs): w = S1+ + Rp S2-, Gp w, S+' = S2+ + T2 Gp w;
-// m = S2- + R2 S1+, Gm m = m + R2 Gp (Rp m), S-' = S1- + Tm Gm m.
+// Per (column, frequency) unit the stack (R+, R-, T+, T-) is held in FP32
+// masters in shared memory.  With G = (I - R1+ R2)^-1 a combine is five MMA
+// passes, each two products with one left factor, and the FP64 inverse
+// between the first two:
+//   P1  Rp x [R2, T2]   -> Gin = Rp R2 (inverted in FP64 -> G),  Z = Rp T2
+//   P2  G  x [Z, Tp]    -> Y = G Z,                 W = G Tp
+//   P3  T2 x [Y, W]     -> R+' = R2 + T2 Y,         T+' = T2 W
+//   P4  Tm x [R2, T2]   -> V = T1- R2,              Q = T1- T2
+//   P5  V  x [W, Y]     -> R-' = R- + V W,          T-' = Q + V Y
+// (T1-' = T1- (T2 + R2 Y) = Q + V Y).  The source chains run as FP32
+// matrix-vector products on the CUDA cores while the MMAs run:
+// w = S1+ + Rp S2-, G w, S+' = S2+ + T2 G w;  m = S2- + R2 S1+,
+// Gm m = m + R2 G (Rp m), S-' = S1- + T1- Gm m.
+// Carrying T~ = I - T and G~ = G - I instead (as the doubling does) was
+// measured no more accurate here: it helps transparent stacks and hurts
+// opaque ones, whose T~ is near I.
 //
 // Pairing as in k_layer_tc: one CTA (4 warps) carries two units in lockstep;
 // warp 2i + p owns product p of unit i (its D lanes hold the columns of the
-// product).  Passes whose two products share the left factor (P1-P3) use
-// N = 64 (B = the two units' left factors); P4 and P5 use N = 128 (B = four
-// left factors) and read the diagonal 32 x 32 blocks of D.  Off-diagonal
-// blocks are computed and ignored, so a unit's results do not depend on its
-// partner.  Consecutive units are the frequencies of one column, whose
-// scattering layers coincide, so the pair rarely waits on itself.
+// product); M = 128, N = 64 (B = the two units' left factors), K = 32.
+// Off-diagonal blocks are computed and ignored, so a unit's results do not
+// depend on its partner.  Consecutive units are the frequencies of one
+// column, whose scattering layers coincide, so the pair rarely waits on
+// itself.
 //
-// The layer records come from k_layer_tc in FP32 (the masters' swizzled
-// layout) and are copied into shared memory with cp.async while the previous
-// combine's last pass runs.
+// The layer records come from k_layer_tc in FP32 (R and T in the masters'
+// swizzled layout) and are copied into shared memory with cp.async while the
+// combine's last pass runs, into the buffers of W and Y (free once that pass
+// has its operands); the buffer roles rotate every combine.
 #pragma once
 #include "layer_tc.cuh"
 
 namespace pb {
 
-// FP32 stack record of one (column, frequency) unit, handed to k_adding_finish
+// FP32 stack record of one (column, frequency) unit, handed to
+// k_adding_finish: R+, R-, T+, T- (masters), S+, S-, the clear-stack
+// transmission t1, then the header (sstate, status as int).
 constexpr int STK_RP = 0, STK_RM = 1024, STK_TP = 2048, STK_TM = 3072, STK_SP = 4096, STK_SM = 4128, STK_T1 = 4160,
-              STK_HDR = 4192, STK_FLOATS = 4224;  // header: sstate, status (int bits)
+              STK_HDR = 4192, STK_FLOATS = 4224;
 
 struct AddTcItem {
-  float m[8][1024];  // masters; roles (R+, R-, T+, T-, R2, T2, G, Z) fixed except T+ <-> G each combine
-  float sp[32], sm[32], s2p[32], s2m[32], t1[32];
-  float t2[32], c2p[32], c2m[32];  // a clear layer (never the prefetch target)
+  float m[8][1024];                  // masters; roles rotate every combine
+  float s2p[32], s2m[32];            // the next layer's sources as fetched (cp.async target)
+  float d2p[32], d2m[32];            // the current layer's sources
+  float sp[32], sm[32], t1[32];      // stack sources; clear-stack transmission
+  float t2[32], c2p[32], c2m[32];    // a clear layer
   float nsp[32], nsm[32], wv[32], wv2[32], u1[32], u2[32], mw[32], u1b[32];
 };
 
 struct AddTcTiles {
-  float b_hi[128 * 32], b_lo[128 * 32];  // B tile pair, up to 128 rows
+  float b_hi[64 * 32], b_lo[64 * 32];  // B tile pair (64 rows: 32 per unit)
 };
 struct AddTcInv {
   double P[Team<32>::MAT], G[Team<32>::MAT];
@@ -66,7 +75,7 @@ static_assert(sizeof(AddTcItem) % 16 == 0, "alignment of the masters");
 
 constexpr size_t add_tc_smem() { return sizeof(AddTcSmem); }
 
-// barrier of the two warps of unit i (named barrier 1 + i, 64 threads)
+// barrier of the two warps of unit i (named barriers 1 and 2, 64 threads)
 __device__ __forceinline__ void unit_sync(int i) {
   if (i == 0) asm volatile("bar.sync 1, 64;" ::: "memory");
   else asm volatile("bar.sync 2, 64;" ::: "memory");
@@ -77,7 +86,7 @@ __device__ __forceinline__ void cp_async16(void* dst, const void* src) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// row r of M times x (k ascending), M a swizzled master
+// row `lane` of the master M times x (k ascending)
 __device__ __forceinline__ float mv32(const float* __restrict__ M, const float* __restrict__ x, const RowOff& ro) {
   float a = 0.f;
 #pragma unroll
@@ -91,51 +100,34 @@ __device__ __forceinline__ float mv32(const float* __restrict__ M, const float* 
   return a;
 }
 
-// B row `brow` <- row `lane` of master bsrc, all 32 K values (N = 128 passes)
-__device__ __forceinline__ void build_b_full(AddTcTiles& TL, const float* bsrc, int brow, const RowOff& ro) {
-#pragma unroll
-  for (int q = 0; q < 8; q++) {
-    const int k0 = 4 * q;
-    float4 hi, lo;
-    const float* bc = bsrc + k0 * 32;
-    tc::split(bc[0 * 32 + ro.o[(k0 + 0) & 7]], hi.x, lo.x);
-    tc::split(bc[1 * 32 + ro.o[(k0 + 1) & 7]], hi.y, lo.y);
-    tc::split(bc[2 * 32 + ro.o[(k0 + 2) & 7]], hi.z, lo.z);
-    tc::split(bc[3 * 32 + ro.o[(k0 + 3) & 7]], hi.w, lo.w);
-    const int o = (brow >> 3) * tc::RG_FLOATS + q * 32 + (brow & 7) * 4;
-    *reinterpret_cast<float4*>(TL.b_hi + o) = hi;
-    *reinterpret_cast<float4*>(TL.b_lo + o) = lo;
-  }
-}
-
 // A row of this thread <- column `lane` of master asrc (hi / lo into TMEM)
 __device__ __forceinline__ void build_a(const float* asrc, uint32_t ta_hi, uint32_t ta_lo, int lane) {
   float c[32], lo[32];
   ld_col(asrc, lane, c);
 #pragma unroll
-  for (int r = 0; r < 32; r++) tc::split(c[r], c[r], lo[r]);
+  for (int r = 0; r < 32; r++) tc::split_rn(c[r], c[r], lo[r]);
   tc::tmem_st32(ta_hi, c);
   tc::tmem_st32(ta_lo, lo);
 }
 
-// B rows 32 mi + lane, K-half h <- row `lane` of master bsrc (N = 64 passes)
-__device__ __forceinline__ void build_b_half(AddTcTiles& TL, const float* bsrc, int brow, int h, const RowOff& ro) {
+// B row `brow` (row `lane` of its unit's left factor bsrc), K-half h
+__device__ __forceinline__ void build_b(AddTcTiles& TL, const float* bsrc, int brow, int h, const RowOff& ro) {
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int k0 = 16 * h + 4 * q;
     float4 hi, lo;
     const float* bc = bsrc + k0 * 32;
-    tc::split(bc[0 * 32 + ro.o[(4 * q + 0) & 7]], hi.x, lo.x);
-    tc::split(bc[1 * 32 + ro.o[(4 * q + 1) & 7]], hi.y, lo.y);
-    tc::split(bc[2 * 32 + ro.o[(4 * q + 2) & 7]], hi.z, lo.z);
-    tc::split(bc[3 * 32 + ro.o[(4 * q + 3) & 7]], hi.w, lo.w);
+    tc::split_rn(bc[0 * 32 + ro.o[(4 * q + 0) & 7]], hi.x, lo.x);
+    tc::split_rn(bc[1 * 32 + ro.o[(4 * q + 1) & 7]], hi.y, lo.y);
+    tc::split_rn(bc[2 * 32 + ro.o[(4 * q + 2) & 7]], hi.z, lo.z);
+    tc::split_rn(bc[3 * 32 + ro.o[(4 * q + 3) & 7]], hi.w, lo.w);
     const int o = (brow >> 3) * tc::RG_FLOATS + (k0 >> 2) * 32 + (brow & 7) * 4;
     *reinterpret_cast<float4*>(TL.b_hi + o) = hi;
     *reinterpret_cast<float4*>(TL.b_lo + o) = lo;
   }
 }
 
-// Issue the copy of layer record `item` into masters R2 / T2 and the layer
+// Issue the copy of layer record `item` into masters r2 / t2 and the staged
 // sources (the 64 threads of the unit).
 __device__ __forceinline__ void lay32_fetch(const Work& w, int item, AddTcItem& U, int r2, int t2, int u) {
   const float* rec = reinterpret_cast<const float*>(w.lay + (size_t)item * w.lay_stride);
@@ -158,12 +150,21 @@ __device__ __forceinline__ int next_scat(const Batch& b, const Work& w, int c, i
   return -1;
 }
 
+// column `lane`: dst = x0 + dv
+__device__ __forceinline__ void epi_add(const float* x0, const float (&dv)[32], float* dst, int lane) {
+  float a[32];
+  ld_col(x0, lane, a);
+#pragma unroll
+  for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
+  st_col(dst, lane, a);
+}
+
 template <int N>
 __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b200_settings st) {
   static_assert(N == 16, "the split-precision adding kernel is built for NUMMU = 16");
   constexpr int n = 32;
   enum { P1 = 0, P2, P3, P4, P5 };
-  enum { RP = 0, RM, TP, TM, R2, T2, GG, ZZ };
+  enum { RP = 0, RM = 1, TM = 3 };  // fixed roles; T+, R2, T2, G and Z rotate
   extern __shared__ __align__(1024) double smem_raw[];
   AddTcSmem& Q = *reinterpret_cast<AddTcSmem*>(smem_raw);
   AddTcTiles& TL = Q.u.tl;
@@ -175,7 +176,7 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
   AddTcItem& U = Q.it[mi];
   const int Lm = b.max_nlyrs, Fm = b.max_nfreq;
   const int nunits = b.ncol * Fm;
-  if (warp == 0) tc::tmem_alloc(&tslot, 256);  // D: columns 0..127, A hi: 128..159, A lo: 160..191
+  if (warp == 0) tc::tmem_alloc(&tslot, 128);  // D: columns 0..63, A hi: 64..95, A lo: 96..127
   if (t == 0) {
     tc::mbar_init(&mbar, 1);
     s_dead = 0;
@@ -185,7 +186,9 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t lanes = (uint32_t)(warp * 32) << 16;
-  const uint32_t ta_hi = tslot + lanes + 128u, ta_lo = tslot + lanes + 160u;
+  const uint32_t ta_hi = tslot + lanes + 64u, ta_lo = tslot + lanes + 96u;
+  const uint32_t dmine = tslot + lanes + 32u * mi;
+  const int brow = 32 * mi + lane;
   const RowOff ro(lane);
   uint32_t parity = 0;
 
@@ -220,10 +223,11 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
     }
     const double* hl = w.hgt_lev + (size_t)c * (Lm + 1);
     const double* tl = w.temp_lev + (size_t)c * (Lm + 1);
-    int tp = TP, gg = GG;   // T+ and G trade buffers every combine
-    int sstate = 0;         // 0 empty, 1 clear (t1, sp, sm), 2 general
-    int k = 0;              // next top-down layer
-    int pf_k = -1;          // layer whose record is in (or on its way to) R2 / T2
+    int tp = 2, r2 = 4, t2 = 5, gg = 6, zz = 7;  // rotating roles: T+ (then W), R2 (then V), T2 (then Q),
+                                                 // G (Gin first, then T+'), Z (then Y)
+    int sstate = 0;   // 0 empty, 1 clear (t1, sp, sm), 2 general
+    int k = 0;        // next top-down layer
+    int pf_k = -1;    // layer whose record is in (or on its way to) r2 / t2
     bool ok = true;
     for (;;) {
       // ---- advance my unit to its next combine (clear layers, the first scattering layer)
@@ -263,6 +267,7 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
               U.sm[u] = sm;
             }
           } else {
+            // general stack + clear layer: R+ = t2 R+ t2, T+ = t2 T+, T- = T- t2
             if (u < n) U.nsp[u] = U.c2p[u] + U.t2[u] * (U.sp[u] + mv32(U.m[RP], U.c2m, ro));
             else U.nsm[lane] = U.sm[lane] + mv32(U.m[TM], U.c2m, ro);
             unit_sync(mi);
@@ -280,9 +285,11 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
           k++;
           continue;
         }
-        // scattering layer: its record into R2 / T2
-        if (pf_k != k) lay32_fetch(w, pidx * Fm + fi, U, R2, T2, u);
+        // scattering layer: its record into r2 / t2
+        if (pf_k != k) lay32_fetch(w, pidx * Fm + fi, U, r2, t2, u);
         cp_async_wait_all();
+        unit_sync(mi);
+        if (u < n) { U.d2p[u] = U.s2p[u]; U.d2m[u] = U.s2m[u]; }
         unit_sync(mi);
         pf_k = -1;
         if (sstate == 2) {
@@ -291,23 +298,23 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
         }
         if (sstate == 0) {
           for (int s = u; s < 1024; s += 64) {
-            const float r2 = U.m[R2][s], t2 = U.m[T2][s];
-            U.m[RP][s] = r2; U.m[RM][s] = r2; U.m[tp][s] = t2; U.m[TM][s] = t2;
+            const float rr = U.m[r2][s], tt = U.m[t2][s];
+            U.m[RP][s] = rr; U.m[RM][s] = rr; U.m[tp][s] = tt; U.m[TM][s] = tt;
           }
-          if (u < n) { U.sp[u] = U.s2p[u]; U.sm[u] = U.s2m[u]; }
+          if (u < n) { U.sp[u] = U.d2p[u]; U.sm[u] = U.d2m[u]; }
         } else {
           // clear stack (t1, sp, sm) + scattering layer
-          if (u < n) U.nsp[u] = U.s2p[u] + mv32(U.m[T2], U.sp, ro);
-          else U.nsm[lane] = U.sm[lane] + U.t1[lane] * (U.s2m[lane] + mv32(U.m[R2], U.sp, ro));
+          if (u < n) U.nsp[u] = U.d2p[u] + mv32(U.m[t2], U.sp, ro);
+          else U.nsm[lane] = U.sm[lane] + U.t1[lane] * (U.d2m[lane] + mv32(U.m[r2], U.sp, ro));
           for (int s = u; s < 1024; s += 64) {
             int r, cc;
             midx_inv(s, r, cc);
             const float t1i = U.t1[r], t1j = U.t1[cc];
-            const float r2 = U.m[R2][s], t2 = U.m[T2][s];
-            U.m[RP][s] = r2;
-            U.m[RM][s] = t1i * (r2 * t1j);
-            U.m[tp][s] = t2 * t1j;
-            U.m[TM][s] = t1i * t2;
+            const float rr = U.m[r2][s], tt = U.m[t2][s];
+            U.m[RP][s] = rr;
+            U.m[RM][s] = t1i * (rr * t1j);
+            U.m[tp][s] = tt * t1j;  // T+ = T2 t1
+            U.m[TM][s] = t1i * tt;  // T- = t1 T2
           }
           unit_sync(mi);
           if (u < n) { U.sp[u] = U.nsp[u]; U.sm[u] = U.nsm[u]; }
@@ -316,49 +323,46 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
         unit_sync(mi);
         k++;
       }
-      const int pending = __syncthreads_or(comb && (t & 63) == 0);
+      const int pending = __syncthreads_or(comb && u == 0);
       if (!pending) break;
       // ---- one combine of both units (a unit without one idles through the passes)
       if (u == 0) s_gg[mi] = gg;  // published by the barriers of P1
       for (int ph = P1; ph <= P5; ph++) {
-        const bool wide = ph >= P4;  // N = 128: four left factors
         if (comb) {
           int asrc, bsrc;
-          if (ph == P1) { asrc = slot ? T2 : R2; bsrc = RP; }
-          else if (ph == P2) { asrc = slot ? tp : ZZ; bsrc = gg; }
-          else if (ph == P3) { asrc = slot ? tp : ZZ; bsrc = T2; }   // W sits in T+'s buffer, Y in Z's
-          else if (ph == P4) { asrc = slot ? ZZ : R2; bsrc = slot ? R2 : TM; }
-          else { asrc = slot ? T2 : tp; bsrc = slot ? TM : ZZ; }      // U in T2's buffer, V in Z's
+          if (ph == P1) { bsrc = RP; asrc = slot ? t2 : r2; }
+          else if (ph == P2) { bsrc = gg; asrc = slot ? tp : zz; }
+          else if (ph == P3) { bsrc = t2; asrc = slot ? tp : zz; }
+          else if (ph == P4) { bsrc = TM; asrc = slot ? t2 : r2; }
+          else { bsrc = r2; asrc = slot ? zz : tp; }
           build_a(U.m[asrc], ta_hi, ta_lo, lane);
-          if (wide) build_b_full(TL, U.m[bsrc], 32 * warp + lane, ro);
-          else build_b_half(TL, U.m[bsrc], 32 * mi + lane, slot, ro);
+          build_b(TL, U.m[bsrc], brow, slot, ro);
         }
         tc::fence_async_smem();
         tc::fence_before_sync();
         __syncthreads();
         tc::fence_after_sync();
-        if (t == 0)
-          tc::mma3_ta(tslot, tslot + 128u, tslot + 160u, TL.b_hi, TL.b_lo, &mbar,
-                      wide ? tc::IDESC_M128_N128 : tc::IDESC_M128_N64);
+        if (t == 0) tc::mma3_ta(tslot, tslot + 64u, tslot + 96u, TL.b_hi, TL.b_lo, &mbar, tc::IDESC_M128_N64);
         if (comb) {
           // source chains on the CUDA cores while the MMA runs
           if (ph == P1) {
-            if (slot == 0) U.wv[lane] = U.sp[lane] + mv32(U.m[RP], U.s2m, ro);
-            else U.mw[lane] = U.s2m[lane] + mv32(U.m[R2], U.sp, ro);
+            if (slot == 0) U.wv[lane] = U.sp[lane] + mv32(U.m[RP], U.d2m, ro);
+            else U.mw[lane] = U.d2m[lane] + mv32(U.m[r2], U.sp, ro);
           } else if (ph == P2) {
             if (slot == 0) U.wv2[lane] = mv32(U.m[gg], U.wv, ro);
             else U.u1[lane] = mv32(U.m[RP], U.mw, ro);
           } else if (ph == P3) {
-            if (slot == 0) U.nsp[lane] = U.s2p[lane] + mv32(U.m[T2], U.wv2, ro);
+            if (slot == 0) U.nsp[lane] = U.d2p[lane] + mv32(U.m[t2], U.wv2, ro);
             else U.u2[lane] = mv32(U.m[gg], U.u1, ro);
           } else if (ph == P4) {
-            if (slot == 0) U.u1b[lane] = U.mw[lane] + mv32(U.m[R2], U.u2, ro);
+            if (slot == 0) U.u1b[lane] = U.mw[lane] + mv32(U.m[r2], U.u2, ro);
           } else {
             if (slot == 0) U.nsm[lane] = U.sm[lane] + mv32(U.m[TM], U.u1b, ro);
-            // R2, T2 and the layer sources are free now: fetch the next scattering layer
+            // W and Y (this pass's A operands) are free now: the next
+            // scattering layer goes into their buffers
             int pidx;
             const int kn = next_scat(b, w, c, L, k + 1, pidx);
-            if (kn >= 0) lay32_fetch(w, pidx * Fm + fi, U, R2, T2, u);
+            if (kn >= 0) lay32_fetch(w, pidx * Fm + fi, U, zz, tp, u);
             pf_k = kn;
           }
         }
@@ -370,44 +374,25 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
         }
         if (!ok) break;
         if (comb) {
-          float dv[32], a[32];
-          tc::tmem_ld32(tslot + lanes + 32u * (wide ? warp : mi), dv);
+          float dv[32];
+          tc::tmem_ld32(dmine, dv);
           if (ph == P1) {
-            st_col(U.m[slot ? ZZ : gg], lane, dv);  // Z = Rp T2;  Gin = Rp R2 (inverted below)
+            st_col(U.m[slot ? zz : gg], lane, dv);  // Gin = Rp R2;  Z = Rp T2
           } else if (ph == P2) {
-            st_col(U.m[slot ? tp : ZZ], lane, dv);  // W = G Tp over T+;  Y = G Z over Z
+            st_col(U.m[slot ? tp : zz], lane, dv);  // Y = G Z over Z;  W = G Tp over T+
           } else if (ph == P3) {
-            if (slot == 0) {  // R+' = R2 + T2 Y
-              ld_col(U.m[R2], lane, a);
-#pragma unroll
-              for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
-              st_col(U.m[RP], lane, a);
-            } else {  // T+' = T2 W into G's buffer (G is dead)
-              st_col(U.m[gg], lane, dv);
-            }
+            if (slot == 0) epi_add(U.m[r2], dv, U.m[RP], lane);  // R+' = R2 + T2 Y
+            else st_col(U.m[gg], lane, dv);                      // T+' = T2 W over G
           } else if (ph == P4) {
-            if (slot == 0) {  // V = Tm R2 over Y (Z's buffer)
-              st_col(U.m[ZZ], lane, dv);
-            } else {  // U = T2 + R2 Y in place of T2
-              ld_col(U.m[T2], lane, a);
-#pragma unroll
-              for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
-              st_col(U.m[T2], lane, a);
-            }
+            st_col(U.m[slot ? t2 : r2], lane, dv);  // V = Tm R2 over R2;  Q = Tm T2 over T2
           } else {
-            if (slot == 0) {  // R-' = R- + V W
-              ld_col(U.m[RM], lane, a);
-#pragma unroll
-              for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
-              st_col(U.m[RM], lane, a);
-            } else {  // T-' = T- U
-              st_col(U.m[TM], lane, dv);
-            }
+            if (slot == 0) epi_add(U.m[RM], dv, U.m[RM], lane);  // R-' = R- + V W
+            else epi_add(U.m[t2], dv, U.m[TM], lane);            // T-' = Q + V Y
           }
         }
         __syncthreads();
         if (ph == P1) {
-          // FP64 (I - Gin)^-1 of each unit, one at a time through the scratch
+          // FP64 G = (I - Gin)^-1 of each unit, one at a time through the scratch
           for (int i = 0; i < 2; i++) {
             const int on = __syncthreads_or(comb && mi == i);
             if (!on) continue;
@@ -433,7 +418,13 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
       }
       if (!ok) break;
       if (comb) {
-        const int o = tp; tp = gg; gg = o;  // T+' sits in G's buffer
+        // T+' is in G's buffer, the next layer in W's and Y's; V and Q are dead
+        const int o_tp = tp, o_r2 = r2, o_t2 = t2, o_gg = gg, o_zz = zz;
+        tp = o_gg;
+        r2 = o_zz;
+        t2 = o_tp;
+        gg = o_r2;
+        zz = o_t2;
         if (u < n) { U.sp[u] = U.nsp[u]; U.sm[u] = U.nsm[u]; }
         k++;
       }
@@ -470,7 +461,7 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  if (warp == 0) tc::tmem_dealloc(tslot, 256);
+  if (warp == 0) tc::tmem_dealloc(tslot, 128);
 }
 
 // Surface, internal radiances and TB of the units k_adding_tc carried, in

@@ -504,7 +504,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
             int r, cc;
             midx_inv(s, r, cc);
             rec[LAY32_R + s] = D.rm[s];
-            rec[LAY32_T + s] = (r == cc ? 1.0f : 0.0f) - D.tm[s];
+            rec[LAY32_T + s] = (r == cc ? 1.0f : 0.0f) - D.tm[s];  // T = I - T~
           }
           if (t < n) {
             rec[LAY32_SP + t] = D.src[0][t];

@@ -54,10 +54,23 @@ __device__ __forceinline__ uint64_t desc_k(uint32_t addr) { return desc(addr, 12
 // hi (exact in FP32); the tensor core reads only the TF32 bits of lo, so lo
 // needs no conversion.  Each operand then carries about 2^-20 relative error,
 // the size of the dropped lo * lo term.  (Rounding both halves with
-// cvt.rna.tf32 is 2^-22 but costs two conversions per element: the split
+// cvt.rna.tf32 is 2^-22 but costs two conversions per element: the doubling
 // kernels are bound by this CUDA-core work, not by the tensor pipe.)
 __device__ __forceinline__ void split(float x, float& hi, float& lo) {
   hi = __uint_as_float(__float_as_uint(x) & 0xffffe000u);
+  lo = x - hi;
+}
+
+// As split(), with hi rounded to the nearest TF32 value (half an ulp of the
+// 10-bit mantissa added to the bit pattern before the low 13 bits are
+// cleared: ties away from zero, one more integer operation).  lo = x - hi is
+// then of either sign, |lo| <= 2^-11 |x|, so the tensor core's truncation of
+// lo errs without bias.  Used by the adding, whose errors accumulate over a
+// long chain of combines (about half the TB error of the truncating split
+// there, measured), while in the doubling the extra operation cost more
+// (2.4 % of the split layer stage) than it gained.
+__device__ __forceinline__ void split_rn(float x, float& hi, float& lo) {
+  hi = __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
   lo = x - hi;
 }
 

@@ -409,7 +409,8 @@ def test_split_precision_target_shape(native):
 
 def test_split_precision_uneven(native):
     # NUMMU 16 and 32 columns take the tensor-core doubling, NUMMU 8 the FP64
-    # one; both forms share the one-inverse FP64 adding.  The split form
+    # one; NUMMU 16 columns also the tensor-core adding, NUMMU 8 and 32 the
+    # one-inverse FP64 adding of the batched FP64 form.  The split form
     # stores the Legendre coefficients in FP32, so its NUMMU 8 columns differ
     # from the batched FP64 form only by that rounding (micro-kelvin).
     from pamtra_b200._native import PREC_3XTF32, PREC_FP64, PREC_FP64_BATCHED
@@ -444,11 +445,11 @@ def test_split_precision_nummu_32(oracle_mod, native):
 
 
 def test_split_precision_pairing_independent(native):
-    # The split-precision layer kernel carries two items per tensor-core MMA;
-    # each item's result depends on its own operands only, so a column gives
-    # bit-identical TBs when the items around it (and hence the pairs) change.
-    # Three frequencies make the per-column item count odd, so dropping the
-    # first column re-pairs every later item.
+    # The split-precision layer and adding kernels carry two items (units)
+    # per tensor-core MMA; each one's result depends on its own operands
+    # only, so a column gives bit-identical TBs when the items around it (and
+    # hence the pairs) change.  Three frequencies make the per-column item
+    # count odd, so dropping the first column re-pairs every later item.
     from pamtra_b200._native import PREC_3XTF32
     freqs = [23.8, 31.4, 89.0]
     b = pbatch.pack_pam(wl.c2_pam(9, seed=21), freqs)
