@@ -63,7 +63,7 @@ struct AddTcInv {
 };
 union __align__(128) AddTcScratch {
   AddTcTiles tl;
-  AddTcInv fp;  // FP64 inverse of one unit at a time
+  AddTcInv fp[2];  // FP64 inverses of the two units (at once)
 };
 
 struct AddTcSmem {
@@ -150,6 +150,98 @@ __device__ __forceinline__ int next_scat(const Batch& b, const Work& w, int c, i
   return -1;
 }
 
+// One unit's n = 32 FP64 product by its two warps (wl = 0, 1 owns rows
+// 16 wl .. 16 wl + 15): C = A B (MM_SET), D + A B (MM_ACC) or I + A B
+// (MM_IPLUS), with the fragments and k order of mm(), so the results are
+// bit-identical to it.  With INPLACE the unit synchronises between reading
+// the operands and writing C.
+template <int MODE, bool INPLACE>
+__device__ __forceinline__ void mm_unit(const double* A, const double* B, double* C, const double* D, int wl, int mi) {
+  constexpr int LD = Team<32>::LD;
+  const int lane = threadIdx.x & 31;
+  const int row0 = 16 * wl, g = lane >> 2, q = lane & 3;
+  double c[2][4][2];
+#pragma unroll
+  for (int rt = 0; rt < 2; rt++)
+#pragma unroll
+    for (int ct = 0; ct < 4; ct++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int row = row0 + rt * 8 + g, col = ct * 8 + 2 * q + i;
+        c[rt][ct][i] = (MODE == MM_ACC) ? D[col * LD + row] : ((MODE == MM_IPLUS) ? (row == col ? 1.0 : 0.0) : 0.0);
+      }
+#pragma unroll 2
+  for (int kk = 0; kk < 32; kk += 4) {
+    const double a0 = A[(kk + q) * LD + row0 + g];
+    const double a1 = A[(kk + q) * LD + row0 + 8 + g];
+    double bb[4];
+#pragma unroll
+    for (int ct = 0; ct < 4; ct++) bb[ct] = B[(ct * 8 + g) * LD + kk + q];
+#pragma unroll
+    for (int ct = 0; ct < 4; ct++) {
+      dmma(c[0][ct], a0, bb[ct]);
+      dmma(c[1][ct], a1, bb[ct]);
+    }
+  }
+  if (INPLACE) unit_sync(mi);
+#pragma unroll
+  for (int rt = 0; rt < 2; rt++)
+#pragma unroll
+    for (int ct = 0; ct < 4; ct++)
+#pragma unroll
+      for (int i = 0; i < 2; i++) {
+        const int row = row0 + rt * 8 + g, col = ct * 8 + 2 * q + i;
+        C[col * LD + row] = c[rt][ct][i];
+      }
+}
+
+// (I - P)^-1 of one unit by its two warps, the Neumann series of
+// inv_iminus() (same plan from the infinity norm, Horner or repeated
+// squaring, same products): returns the buffer holding the inverse (P or
+// G), or nullptr when the norm asks for Gauss-Jordan (P left untouched).
+__device__ __forceinline__ double* inv_unit(double* P, double* G, int wl, int mi) {
+  constexpr int LD = Team<32>::LD;
+  const int lane = threadIdx.x & 31, u = threadIdx.x & 63;
+  double r = 0.0;
+#pragma unroll 8
+  for (int j = 0; j < 32; j++) r += fabs(P[j * LD + lane]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+  const double nrm = r;
+  int m = 1;
+  double pw = nrm;
+  while (pw > 5.0e-17 && m < 8) {
+    pw = pw * pw;
+    m++;
+  }
+  int kh = 0;
+  double ph = nrm * nrm;
+  while (ph > 5.0e-17 && kh < 2 * (m - 1)) {
+    ph = ph * nrm;
+    kh++;
+  }
+  if (m >= 8) return nullptr;
+  for (int e = u; e < 1024; e += 64) {
+    const int col = e >> 5, row = e & 31;
+    G[col * LD + row] = ((row == col) ? 1.0 : 0.0) + P[col * LD + row];
+  }
+  unit_sync(mi);
+  if (ph <= 5.0e-17 && kh < 2 * (m - 1)) {
+    for (int k = 0; k < kh; k++) {
+      mm_unit<MM_IPLUS, true>(P, G, G, nullptr, wl, mi);  // G = I + X G
+      unit_sync(mi);
+    }
+    return G;
+  }
+  for (int k = 1; k < m; k++) {
+    mm_unit<MM_SET, true>(P, P, P, nullptr, wl, mi);  // P = P^2
+    unit_sync(mi);
+    mm_unit<MM_ACC, true>(G, P, G, G, wl, mi);  // G = G + G P
+    unit_sync(mi);
+  }
+  return G;
+}
+
 // column `lane`: dst = x0 + dv
 __device__ __forceinline__ void epi_add(const float* x0, const float (&dv)[32], float* dst, int lane) {
   float a[32];
@@ -170,7 +262,7 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
   AddTcTiles& TL = Q.u.tl;
   __shared__ uint64_t mbar;
   __shared__ uint32_t tslot;
-  __shared__ int s_base, s_dead, s_gg[2];
+  __shared__ int s_base, s_dead, s_gg[2], s_gj[2];
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int mi = warp >> 1, slot = warp & 1, u = t & 63;
   AddTcItem& U = Q.it[mi];
@@ -392,25 +484,48 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
         }
         __syncthreads();
         if (ph == P1) {
-          // FP64 G = (I - Gin)^-1 of each unit, one at a time through the scratch
-          for (int i = 0; i < 2; i++) {
-            const int on = __syncthreads_or(comb && mi == i);
-            if (!on) continue;
-            AddTcInv& F = Q.u.fp;
-            float* gm = Q.it[i].m[s_gg[i]];
-            for (int s = t; s < 1024; s += 128) {
+          // FP64 G = (I - Gin)^-1: each unit's two warps invert its own, both
+          // units at once (the operand tiles are free until the next pass)
+          int gj = 0;
+          if (comb) {
+            AddTcInv& F = Q.u.fp[mi];
+            float* gm = U.m[gg];
+            for (int s = u; s < 1024; s += 64) {
               int r, cc;
               midx_inv(s, r, cc);
               F.P[cc * Team<32>::LD + r] = (double)gm[s];
             }
+            unit_sync(mi);
+            const double* Gi = inv_unit(F.P, F.G, slot, mi);
+            if (Gi) {
+              for (int s = u; s < 1024; s += 64) {
+                int r, cc;
+                midx_inv(s, r, cc);
+                gm[s] = (float)Gi[cc * Team<32>::LD + r];
+              }
+            } else {
+              gj = 1;
+            }
+          }
+          if (u == 0) s_gj[mi] = gj;
+          __syncthreads();
+          // ||Gin|| >= 0.74: Gauss-Jordan with partial pivoting, one unit at a
+          // time with the whole CTA (the fallback of inv_iminus)
+          for (int i = 0; i < 2; i++) {
+            if (!s_gj[i]) continue;
+            AddTcInv& F = Q.u.fp[i];
+            for (int e = t; e < 1024; e += 128) {
+              const int col = e >> 5, row = e & 31;
+              F.P[col * Team<32>::LD + row] = ((row == col) ? 1.0 : 0.0) - F.P[col * Team<32>::LD + row];
+            }
             __syncthreads();
-            int sg = 0;
-            const double* Gi = inv_iminus<32>(F.P, F.G, F.inv, &sg);
+            const int sg = ginv<32>(F.P, F.inv);
             if (sg && mi == i) status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+            float* gm = Q.it[i].m[s_gg[i]];
             for (int s = t; s < 1024; s += 128) {
               int r, cc;
               midx_inv(s, r, cc);
-              gm[s] = (float)Gi[cc * Team<32>::LD + r];
+              gm[s] = (float)F.P[cc * Team<32>::LD + r];
             }
             __syncthreads();
           }
