@@ -165,3 +165,17 @@ def test_bench_oracle_sample_prefers_cheap_columns():
     assert len(idxs) == 8 and idxs == sorted(set(idxs))
     nmu = np.asarray(b.host["nummu"])
     assert {8, 16, 32} & set(nmu[idxs].tolist()) == set(np.unique(nmu).tolist()) & {8, 16, 32}
+
+
+def test_split_adding_workspace():
+    # the split adding (PREC_3XTF32, NUMMU 16) adds one FP32 stack record of
+    # 4224 floats per (column, frequency) unit to the plan; the split
+    # doubling with the FP64 adding and the FP64 forms need none
+    from pamtra_b200._native import PREC_3XTF32, PREC_3XTF32_FP64ADD, PREC_FP64_BATCHED
+    b = pbatch.pack_pam(wl.c2_pam(16, seed=5), wl.C2_FREQS)
+    cols = b.columns(b.host)
+    w1 = workspace_bytes(cols, precision=PREC_3XTF32)
+    w3 = workspace_bytes(cols, precision=PREC_3XTF32_FP64ADD)
+    w2 = workspace_bytes(cols, precision=PREC_FP64_BATCHED)
+    assert w1 - w3 == 16 * len(wl.C2_FREQS) * 4224 * 4
+    assert w3 < w2  # FP32 Legendre coefficients in the split forms
