@@ -436,20 +436,23 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
         tc::fence_after_sync();
         if (t == 0) tc::mma3_ta(tslot, tslot + 64u, tslot + 96u, TL.b_hi, TL.b_lo, &mbar, tc::IDESC_M128_N64);
         if (comb) {
-          // source chains on the CUDA cores while the MMA runs
+          // source chains on the CUDA cores while the MMA runs: the S+ chain
+          // on slot 0, the S- chain on slot 1, except that warp 0 issues the
+          // MMAs meanwhile, so warp 1 runs both chains of unit 0
+          const bool cp = (mi == 0) ? (warp == 1) : (slot == 0), cm = (slot == 1);
           if (ph == P1) {
-            if (slot == 0) U.wv[lane] = U.sp[lane] + mv32(U.m[RP], U.d2m, ro);
-            else U.mw[lane] = U.d2m[lane] + mv32(U.m[r2], U.sp, ro);
+            if (cp) U.wv[lane] = U.sp[lane] + mv32(U.m[RP], U.d2m, ro);
+            if (cm) U.mw[lane] = U.d2m[lane] + mv32(U.m[r2], U.sp, ro);
           } else if (ph == P2) {
-            if (slot == 0) U.wv2[lane] = mv32(U.m[gg], U.wv, ro);
-            else U.u1[lane] = mv32(U.m[RP], U.mw, ro);
+            if (cp) U.wv2[lane] = mv32(U.m[gg], U.wv, ro);
+            if (cm) U.u1[lane] = mv32(U.m[RP], U.mw, ro);
           } else if (ph == P3) {
-            if (slot == 0) U.nsp[lane] = U.d2p[lane] + mv32(U.m[t2], U.wv2, ro);
-            else U.u2[lane] = mv32(U.m[gg], U.u1, ro);
+            if (cp) U.nsp[lane] = U.d2p[lane] + mv32(U.m[t2], U.wv2, ro);
+            if (cm) U.u2[lane] = mv32(U.m[gg], U.u1, ro);
           } else if (ph == P4) {
-            if (slot == 0) U.u1b[lane] = U.mw[lane] + mv32(U.m[r2], U.u2, ro);
+            if (cp) U.u1b[lane] = U.mw[lane] + mv32(U.m[r2], U.u2, ro);
           } else {
-            if (slot == 0) U.nsm[lane] = U.sm[lane] + mv32(U.m[TM], U.u1b, ro);
+            if (cp) U.nsm[lane] = U.sm[lane] + mv32(U.m[TM], U.u1b, ro);
             // W and Y (this pass's A operands) are free now: the next
             // scattering layer goes into their buffers
             int pidx;

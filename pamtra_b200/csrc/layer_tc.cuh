@@ -187,6 +187,27 @@ __device__ __forceinline__ void matvec2(const float* __restrict__ M, const float
   y1 = a1;
 }
 
+// (M x0..x3)[r] for a master M, one row load for four vectors (k-ascending
+// FMA chains, each bit-identical to matvec2's)
+__device__ __forceinline__ void matvec4(const float* __restrict__ M, const float (*__restrict__ x)[32],
+                                        const RowOff& ro, float (&y)[4]) {
+  float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll
+  for (int k = 0; k < 32; k += 4) {
+    const float4 p = *reinterpret_cast<const float4*>(x[0] + k);
+    const float4 q = *reinterpret_cast<const float4*>(x[1] + k);
+    const float4 r = *reinterpret_cast<const float4*>(x[2] + k);
+    const float4 v = *reinterpret_cast<const float4*>(x[3] + k);
+    const float m0 = M[k * 32 + ro.o[k & 7]], m1 = M[(k + 1) * 32 + ro.o[(k + 1) & 7]];
+    const float m2 = M[(k + 2) * 32 + ro.o[(k + 2) & 7]], m3 = M[(k + 3) * 32 + ro.o[(k + 3) & 7]];
+    a0 = fmaf(m0, p.x, a0); a1 = fmaf(m0, q.x, a1); a2 = fmaf(m0, r.x, a2); a3 = fmaf(m0, v.x, a3);
+    a0 = fmaf(m1, p.y, a0); a1 = fmaf(m1, q.y, a1); a2 = fmaf(m1, r.y, a2); a3 = fmaf(m1, v.y, a3);
+    a0 = fmaf(m2, p.z, a0); a1 = fmaf(m2, q.z, a1); a2 = fmaf(m2, r.z, a2); a3 = fmaf(m2, v.z, a3);
+    a0 = fmaf(m3, p.w, a0); a1 = fmaf(m3, q.w, a1); a2 = fmaf(m3, r.w, a2); a3 = fmaf(m3, v.w, a3);
+  }
+  y[0] = a0; y[1] = a1; y[2] = a2; y[3] = a3;
+}
+
 // Series plan for ||X|| = nrm (any sub-multiplicative norm), by the relative
 // remainder it leaves: s >= 1 repeated squaring in s + 1 MMAs (remainder
 // nrm^(2^(s+1) - 1)), 0: G~ = X (nrm), SERIES_H1: G~ = X + X X in one MMA
@@ -234,6 +255,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
   __shared__ int s_base, s_dead;
   __shared__ int s_valid[2], s_nd[2], s_status[2], s_c[2], s_fi[2];
   __shared__ float s_linfac[2];
+  __shared__ float s_mv[2][32];  // item 0, slot 0: its mat-vec results, computed by warp 1
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int mi = warp >> 1, slot = warp & 1;  // my item of the pair, my product
   TcItemState& my = Q.st[mi];
@@ -340,10 +362,22 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
         float m0 = 0.f, m1 = 0.f;
         float xk[32];  // slot 1 of a series step: its column of X, taken before slot 0 replaces X
         if (on && phase == SER && slot == 1) ld_col(my.xa, lane, xk);
-        if (on && phase != SER) {
+        if (on && phase != SER && warp != 0) {
+          // warp 0 spends this time issuing the MMAs: warp 1 takes the
+          // mat-vecs of both slots of item 0 (one matrix), warps 2 and 3
+          // those of their slot of item 1
           const float* mv = (phase == G1) ? my.rm : (phase == G2) ? my.gm : my.tm;
           const float(*x)[32] = (phase == G1) ? my.vv : (phase == G2) ? my.uv : my.wv;
-          matvec2(mv, x[2 * slot], x[2 * slot + 1], rowoff, m0, m1);
+          if (warp == 1) {
+            float y[4];
+            matvec4(mv, x, rowoff, y);
+            s_mv[0][lane] = y[0];
+            s_mv[1][lane] = y[1];
+            m0 = y[2];
+            m1 = y[3];
+          } else {
+            matvec2(mv, x[2 * slot], x[2 * slot + 1], rowoff, m0, m1);
+          }
         }
         {
           const bool mine = tc::mbar_wait(&mbar, parity, w.spin_limit);
@@ -355,6 +389,10 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
         if (on) {
           float dv[32], a[32];
           tc::tmem_ld32(dmine, dv);
+          if (warp == 0 && phase != SER) {
+            m0 = s_mv[0][lane];
+            m1 = s_mv[1][lane];
+          }
           if (phase == G1) {
             if (slot == 0) {  // X = P, its column-sum norm;  u0 = S+ + R v0, u1 = C+ + R v1
               my.uv[0][lane] = my.src[0][lane] + m0;
@@ -366,6 +404,14 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
 #pragma unroll
               for (int o = 16; o > 0; o >>= 1) sn = fmaxf(sn, __shfl_xor_sync(0xffffffffu, sn, o));
               if (lane == 0) my.nrm = sn;
+              // G~ = X when the series needs no step, else 0 to start it (the
+              // Gauss-Jordan fallback writes its own)
+              const int s0 = series_steps(sn);
+              if (s0 != -1) {
+#pragma unroll
+                for (int r = 0; r < 32; r++) a[r] = (s0 == 0) ? dv[r] : 0.f;
+                st_col(my.gm, lane, a);
+              }
             } else {  // V = R - R T~;  u2 = v0 + R v2, u3 = C- + R v3
               my.uv[2][lane] = my.vv[0][lane] + m0;
               my.uv[3][lane] = my.src[3][lane] + m1;
@@ -468,14 +514,6 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
           myg = (mys >= 1) ? mys + 1 : (mys == SERIES_H1 ? 1 : 0);
           gmax = max((stp0 >= 1) ? stp0 + 1 : (stp0 == SERIES_H1 ? 1 : 0),
                      (stp1 >= 1) ? stp1 + 1 : (stp1 == SERIES_H1 ? 1 : 0));
-          if (slot == 1 && (mys >= 0 || mys == SERIES_H1)) {  // G~ = X (no series), or G~ = 0 to start one
-            float g[32];
-            if (mys == 0) ld_col(my.xa, lane, g);
-#pragma unroll
-            for (int r = 0; r < 32; r++) g[r] = (mys == 0) ? g[r] : 0.f;
-            st_col(my.gm, lane, g);
-          }
-          __syncthreads();
           k = 0;
           phase = (gmax > 0) ? SER : G2;
         } else if (phase == SER) {
