@@ -91,6 +91,20 @@ __device__ __forceinline__ void matvec2_64(const float* __restrict__ M, const fl
   y1 = a1;
 }
 
+// (M x)[r] for a 64 x 64 master (the k-ascending FMA chain of matvec2_64)
+__device__ __forceinline__ float matvec1_64(const float* __restrict__ M, const float* __restrict__ x, int r) {
+  float a = 0.f;
+#pragma unroll 4
+  for (int k = 0; k < 64; k += 4) {
+    const float4 p = *reinterpret_cast<const float4*>(x + k);
+    a = fmaf(M[midx64(r, k)], p.x, a);
+    a = fmaf(M[midx64(r, k + 1)], p.y, a);
+    a = fmaf(M[midx64(r, k + 2)], p.z, a);
+    a = fmaf(M[midx64(r, k + 3)], p.w, a);
+  }
+  return a;
+}
+
 // Operands of one group for thread t: its A row (column `col` of `asrc`,
 // 64 values) split into TF32 hi / lo in its TMEM lane, and half h of B row
 // `brow` (row brow of `bsrc`, K = 32h .. 32h+31) in shared memory.
@@ -149,6 +163,7 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
   __shared__ uint64_t mbar;
   __shared__ uint32_t tslot;
   __shared__ int s_item, s_dead, s_status;
+  __shared__ float s_mv[2][32];  // warp 0's mat-vec results, computed by warps 1 and 2
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   const int slot = t >> 6, col = t & 63;  // my product and my column of it (= my A row, my D lane)
   const int Fm = b.max_nfreq;
@@ -241,7 +256,10 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
         if (phase != SER) {
           const float* mv = (phase == G1) ? my.rm : (phase == G2) ? my.gm : my.tm;
           const float(*x)[64] = (phase == G1) ? my.vv : (phase == G2) ? my.uv : my.wv;
-          matvec2_64(mv, x[2 * slot], x[2 * slot + 1], col, m0, m1);
+          // warp 0 spends this time issuing the MMAs: warps 1 and 2 take
+          // its two mat-vecs (rows 0..31, the vectors of slot 0)
+          if (warp != 0) matvec2_64(mv, x[2 * slot], x[2 * slot + 1], col, m0, m1);
+          if (warp == 1 || warp == 2) s_mv[warp - 1][lane] = matvec1_64(mv, x[warp - 1], lane);
         }
         {
           const bool mine = tc::mbar_wait(&mbar, parity, w.spin_limit);
@@ -250,6 +268,10 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
           tc::fence_after_sync();
         }
         if (!ok) break;
+        if (warp == 0 && phase != SER) {
+          m0 = s_mv[0][lane];
+          m1 = s_mv[1][lane];
+        }
         if (on) {
           float nsum = 0.f;
 #pragma unroll
