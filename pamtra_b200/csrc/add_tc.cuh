@@ -242,10 +242,12 @@ __device__ __forceinline__ double* inv_unit(double* P, double* G, int wl, int mi
   return G;
 }
 
-// column `lane`: dst = x0 + dv
-__device__ __forceinline__ void epi_add(const float* x0, const float (&dv)[32], float* dst, int lane) {
+// column `lane`: dst = x0 + dv, dv issued by tmem_ld32_issue (waited for
+// here, after the column of x0 is loaded)
+__device__ __forceinline__ void epi_add(const float* x0, float (&dv)[32], float* dst, int lane) {
   float a[32];
   ld_col(x0, lane, a);
+  tc::tmem_wait_ld(dv);
 #pragma unroll
   for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
   st_col(dst, lane, a);
@@ -470,15 +472,22 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
         if (!ok) break;
         if (comb) {
           float dv[32];
-          tc::tmem_ld32(dmine, dv);
+          tc::tmem_ld32_issue(dmine, dv);
           if (ph == P1) {
+            tc::tmem_wait_ld(dv);
             st_col(U.m[slot ? zz : gg], lane, dv);  // Gin = Rp R2;  Z = Rp T2
           } else if (ph == P2) {
+            tc::tmem_wait_ld(dv);
             st_col(U.m[slot ? tp : zz], lane, dv);  // Y = G Z over Z;  W = G Tp over T+
           } else if (ph == P3) {
-            if (slot == 0) epi_add(U.m[r2], dv, U.m[RP], lane);  // R+' = R2 + T2 Y
-            else st_col(U.m[gg], lane, dv);                      // T+' = T2 W over G
+            if (slot == 0) {
+              epi_add(U.m[r2], dv, U.m[RP], lane);  // R+' = R2 + T2 Y
+            } else {
+              tc::tmem_wait_ld(dv);
+              st_col(U.m[gg], lane, dv);  // T+' = T2 W over G
+            }
           } else if (ph == P4) {
+            tc::tmem_wait_ld(dv);
             st_col(U.m[slot ? t2 : r2], lane, dv);  // V = Tm R2 over R2;  Q = Tm T2 over T2
           } else {
             if (slot == 0) epi_add(U.m[RM], dv, U.m[RM], lane);  // R-' = R- + V W

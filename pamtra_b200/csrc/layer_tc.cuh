@@ -388,7 +388,9 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
         if (!ok) break;
         if (on) {
           float dv[32], a[32];
-          tc::tmem_ld32(dmine, dv);
+          // D is read while the masters' columns are loaded; every use of dv
+          // follows a tmem_wait_ld(dv)
+          tc::tmem_ld32_issue(dmine, dv);
           if (warp == 0 && phase != SER) {
             m0 = s_mv[0][lane];
             m1 = s_mv[1][lane];
@@ -397,6 +399,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
             if (slot == 0) {  // X = P, its column-sum norm;  u0 = S+ + R v0, u1 = C+ + R v1
               my.uv[0][lane] = my.src[0][lane] + m0;
               my.uv[1][lane] = my.src[1][lane] + m1;
+              tc::tmem_wait_ld(dv);
               st_col(my.xa, lane, dv);
               float sn = 0.f;
 #pragma unroll
@@ -416,6 +419,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
               my.uv[2][lane] = my.vv[0][lane] + m0;
               my.uv[3][lane] = my.src[3][lane] + m1;
               ld_col(my.rm, lane, a);
+              tc::tmem_wait_ld(dv);
 #pragma unroll
               for (int r = 0; r < 32; r++) a[r] = a[r] - dv[r];
               st_col(my.vm, lane, a);
@@ -424,17 +428,22 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
             if (mys == SERIES_H1) {
               if (slot == 0) {  // G~ = X + X X
                 ld_col(my.xa, lane, a);
+                tc::tmem_wait_ld(dv);
 #pragma unroll
                 for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
                 st_col(my.gm, lane, a);
               }
             } else if (slot == 0) {
-              if (k < mys) st_col(my.xa, lane, dv);  // X = X X (slot 1 took its column of X before)
+              if (k < mys) {  // X = X X (slot 1 took its column of X before)
+                tc::tmem_wait_ld(dv);
+                st_col(my.xa, lane, dv);
+              }
             } else {  // G~ += X + X G~
               float g[32];
 #pragma unroll
               for (int r = 0; r < 32; r++) a[r] = xk[r];
               ld_col(my.gm, lane, g);
+              tc::tmem_wait_ld(dv);
 #pragma unroll
               for (int r = 0; r < 32; r++) g[r] = g[r] + (a[r] + dv[r]);
               st_col(my.gm, lane, g);
@@ -447,11 +456,13 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
               float g[32];
               ld_col(my.tm, lane, a);
               ld_col(my.gm, lane, g);
+              tc::tmem_wait_ld(dv);
 #pragma unroll
               for (int r = 0; r < 32; r++) a[r] = (a[r] - g[r]) + dv[r];
               st_col(my.xa, lane, a);
             } else {  // Y = V + G~ V
               ld_col(my.vm, lane, a);
+              tc::tmem_wait_ld(dv);
 #pragma unroll
               for (int r = 0; r < 32; r++) a[r] = a[r] + dv[r];
               st_col(my.vm, lane, a);
@@ -463,6 +474,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
             if (slot == 0) {  // T~' = T~ + (Z~ - T~ Z~);  S+' = (S+ + a0) + f C+,  C+' = C+ + a1
               ld_col(my.tm, lane, a);
               ld_col(my.xa, lane, z);
+              tc::tmem_wait_ld(dv);
 #pragma unroll
               for (int r = 0; r < 32; r++) a[r] = a[r] + (z[r] - dv[r]);
               st_col(my.tm, lane, a);
@@ -475,6 +487,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
             } else {  // R' = R + (Y - T~ Y);  S-' = S- + a2,  C-' = C- + a3
               ld_col(my.rm, lane, a);
               ld_col(my.vm, lane, z);
+              tc::tmem_wait_ld(dv);
 #pragma unroll
               for (int r = 0; r < 32; r++) a[r] = a[r] + (z[r] - dv[r]);
               st_col(my.rm, lane, a);
@@ -486,6 +499,7 @@ __global__ void __launch_bounds__(128, 3) k_layer_tc(Batch b, Work w, pamtra_b20
               my.vv[1][lane] = cm;
             }
           }
+          tc::tmem_wait_ld(dv);  // the paths that did not read D
         }
         __syncthreads();  // masters complete before the next operands are built
         // ---- next phase
