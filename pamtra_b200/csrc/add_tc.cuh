@@ -100,31 +100,31 @@ __device__ __forceinline__ float mv32(const float* __restrict__ M, const float* 
   return a;
 }
 
-// A row of this thread <- column `lane` of master asrc (hi / lo into TMEM)
-__device__ __forceinline__ void build_a(const float* asrc, uint32_t ta_hi, uint32_t ta_lo, int lane) {
+// Operands of one pass for this thread: its A row (column `lane` of master
+// asrc, hi / lo into TMEM) and K-half h of B row `brow` (row `lane` of its
+// unit's left factor bsrc); the A stores run while B is built
+__device__ __forceinline__ void build_ab(AddTcTiles& TL, const float* asrc, const float* bsrc, uint32_t ta_hi,
+                                         uint32_t ta_lo, int brow, int h, int lane, const RowOff& ro) {
   float c[32], lo[32];
   ld_col(asrc, lane, c);
 #pragma unroll
   for (int r = 0; r < 32; r++) tc::split_rn(c[r], c[r], lo[r]);
-  tc::tmem_st32(ta_hi, c);
-  tc::tmem_st32(ta_lo, lo);
-}
-
-// B row `brow` (row `lane` of its unit's left factor bsrc), K-half h
-__device__ __forceinline__ void build_b(AddTcTiles& TL, const float* bsrc, int brow, int h, const RowOff& ro) {
+  tc::tmem_st32_issue(ta_hi, c);
+  tc::tmem_st32_issue(ta_lo, lo);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int k0 = 16 * h + 4 * q;
-    float4 hi, lo;
+    float4 bh, bl;
     const float* bc = bsrc + k0 * 32;
-    tc::split_rn(bc[0 * 32 + ro.o[(4 * q + 0) & 7]], hi.x, lo.x);
-    tc::split_rn(bc[1 * 32 + ro.o[(4 * q + 1) & 7]], hi.y, lo.y);
-    tc::split_rn(bc[2 * 32 + ro.o[(4 * q + 2) & 7]], hi.z, lo.z);
-    tc::split_rn(bc[3 * 32 + ro.o[(4 * q + 3) & 7]], hi.w, lo.w);
+    tc::split_rn(bc[0 * 32 + ro.o[(4 * q + 0) & 7]], bh.x, bl.x);
+    tc::split_rn(bc[1 * 32 + ro.o[(4 * q + 1) & 7]], bh.y, bl.y);
+    tc::split_rn(bc[2 * 32 + ro.o[(4 * q + 2) & 7]], bh.z, bl.z);
+    tc::split_rn(bc[3 * 32 + ro.o[(4 * q + 3) & 7]], bh.w, bl.w);
     const int o = (brow >> 3) * tc::RG_FLOATS + (k0 >> 2) * 32 + (brow & 7) * 4;
-    *reinterpret_cast<float4*>(TL.b_hi + o) = hi;
-    *reinterpret_cast<float4*>(TL.b_lo + o) = lo;
+    *reinterpret_cast<float4*>(TL.b_hi + o) = bh;
+    *reinterpret_cast<float4*>(TL.b_lo + o) = bl;
   }
+  tc::tmem_wait_st2(c, lo);
 }
 
 // Issue the copy of layer record `item` into masters r2 / t2 and the staged
@@ -429,8 +429,7 @@ __global__ void __launch_bounds__(128, 2) k_adding_tc(Batch b, Work w, pamtra_b2
           else if (ph == P3) { bsrc = t2; asrc = slot ? tp : zz; }
           else if (ph == P4) { bsrc = TM; asrc = slot ? t2 : r2; }
           else { bsrc = r2; asrc = slot ? zz : tp; }
-          build_a(U.m[asrc], ta_hi, ta_lo, lane);
-          build_b(TL, U.m[bsrc], brow, slot, ro);
+          build_ab(TL, U.m[asrc], U.m[bsrc], ta_hi, ta_lo, brow, slot, lane, ro);
         }
         tc::fence_async_smem();
         tc::fence_before_sync();

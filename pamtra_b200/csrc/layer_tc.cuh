@@ -145,27 +145,27 @@ __device__ __forceinline__ void st_col(float* m, int col, const float (&v)[32]) 
 // memory.  The two warps of an item cover the B row's two halves.
 __device__ __forceinline__ void build_operands(TcTiles& TL, const float* asrc, const float* bsrc, uint32_t ta_hi,
                                                uint32_t ta_lo, int brow, int h, int lane, const RowOff& ro) {
-  {
-    float c[32], lo[32];
-    ld_col(asrc, lane, c);
+  // the A stores run while the B half is built; their wait comes last
+  float c[32], lo[32];
+  ld_col(asrc, lane, c);
 #pragma unroll
-    for (int r = 0; r < 32; r++) tc::split(c[r], c[r], lo[r]);
-    tc::tmem_st32(ta_hi, c);
-    tc::tmem_st32(ta_lo, lo);
-  }
+  for (int r = 0; r < 32; r++) tc::split(c[r], c[r], lo[r]);
+  tc::tmem_st32_issue(ta_hi, c);
+  tc::tmem_st32_issue(ta_lo, lo);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int k0 = 16 * h + 4 * q;
-    float4 hi, lo;
+    float4 bh, bl;
     const float* bc = bsrc + k0 * 32;  // k0 = 16 h + 4 q: (k0 + j) mod 8 = (4 q + j) mod 8
-    tc::split(bc[0 * 32 + ro.o[(4 * q + 0) & 7]], hi.x, lo.x);
-    tc::split(bc[1 * 32 + ro.o[(4 * q + 1) & 7]], hi.y, lo.y);
-    tc::split(bc[2 * 32 + ro.o[(4 * q + 2) & 7]], hi.z, lo.z);
-    tc::split(bc[3 * 32 + ro.o[(4 * q + 3) & 7]], hi.w, lo.w);
+    tc::split(bc[0 * 32 + ro.o[(4 * q + 0) & 7]], bh.x, bl.x);
+    tc::split(bc[1 * 32 + ro.o[(4 * q + 1) & 7]], bh.y, bl.y);
+    tc::split(bc[2 * 32 + ro.o[(4 * q + 2) & 7]], bh.z, bl.z);
+    tc::split(bc[3 * 32 + ro.o[(4 * q + 3) & 7]], bh.w, bl.w);
     const int o = (brow >> 3) * tc::RG_FLOATS + (k0 >> 2) * 32 + (brow & 7) * 4;
-    *reinterpret_cast<float4*>(TL.b_hi + o) = hi;
-    *reinterpret_cast<float4*>(TL.b_lo + o) = lo;
+    *reinterpret_cast<float4*>(TL.b_hi + o) = bh;
+    *reinterpret_cast<float4*>(TL.b_lo + o) = bl;
   }
+  tc::tmem_wait_st2(c, lo);
 }
 
 // (M x0)[r] and (M x1)[r] for a master M (k-ascending FMA chains)

@@ -110,27 +110,34 @@ __device__ __forceinline__ float matvec1_64(const float* __restrict__ M, const f
 // `brow` (row brow of `bsrc`, K = 32h .. 32h+31) in shared memory.
 __device__ __forceinline__ void build_operands64(Tc64Tiles& TL, const float* asrc, const float* bsrc, uint32_t ta_hi,
                                                  uint32_t ta_lo, int col, int brow, int h) {
-#pragma unroll
-  for (int hh = 0; hh < 2; hh++) {
+  {
     float c[32], lo[32];
-    ld_col64(asrc, col, hh, c);
+    ld_col64(asrc, col, 0, c);
 #pragma unroll
     for (int r = 0; r < 32; r++) tc::split(c[r], c[r], lo[r]);
-    tc::tmem_st32(ta_hi + 32u * hh, c);
-    tc::tmem_st32(ta_lo + 32u * hh, lo);
+    tc::tmem_st32(ta_hi, c);
+    tc::tmem_st32(ta_lo, lo);
   }
+  // the second half's stores run while the B half is built; their wait comes last
+  float c[32], lo[32];
+  ld_col64(asrc, col, 1, c);
+#pragma unroll
+  for (int r = 0; r < 32; r++) tc::split(c[r], c[r], lo[r]);
+  tc::tmem_st32_issue(ta_hi + 32u, c);
+  tc::tmem_st32_issue(ta_lo + 32u, lo);
 #pragma unroll
   for (int q = 0; q < 8; q++) {
     const int k0 = 32 * h + 4 * q;
-    float4 hi, lo;
-    tc::split(bsrc[midx64(brow, k0 + 0)], hi.x, lo.x);
-    tc::split(bsrc[midx64(brow, k0 + 1)], hi.y, lo.y);
-    tc::split(bsrc[midx64(brow, k0 + 2)], hi.z, lo.z);
-    tc::split(bsrc[midx64(brow, k0 + 3)], hi.w, lo.w);
+    float4 bh, bl;
+    tc::split(bsrc[midx64(brow, k0 + 0)], bh.x, bl.x);
+    tc::split(bsrc[midx64(brow, k0 + 1)], bh.y, bl.y);
+    tc::split(bsrc[midx64(brow, k0 + 2)], bh.z, bl.z);
+    tc::split(bsrc[midx64(brow, k0 + 3)], bh.w, bl.w);
     const int o = (brow >> 3) * 512 + (k0 >> 2) * 32 + (brow & 7) * 4;
-    *reinterpret_cast<float4*>(TL.b_hi + o) = hi;
-    *reinterpret_cast<float4*>(TL.b_lo + o) = lo;
+    *reinterpret_cast<float4*>(TL.b_hi + o) = bh;
+    *reinterpret_cast<float4*>(TL.b_lo + o) = bl;
   }
+  tc::tmem_wait_st2(c, lo);
 }
 
 // 3xTF32 M = 128, N = 64, K = 64 product: A pair in TMEM, B pair in shared

@@ -250,6 +250,36 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) 
   asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
+// tmem_st32 without its wait, and the wait for two such stores: it names
+// both source arrays as operands, so they stay live and unchanged until the
+// stores have completed.
+__device__ __forceinline__ void tmem_st32_issue(uint32_t taddr, const float (&v)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], "
+      "{%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,"
+      "%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32};"
+      :
+      : "r"(taddr), "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]),
+        "f"(v[8]), "f"(v[9]), "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]),
+        "f"(v[16]), "f"(v[17]), "f"(v[18]), "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]),
+        "f"(v[24]), "f"(v[25]), "f"(v[26]), "f"(v[27]), "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31])
+      : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st2(float (&v)[32], float (&w)[32]) {
+  asm volatile("tcgen05.wait::st.sync.aligned;"
+               : "+f"(v[0]), "+f"(v[1]), "+f"(v[2]), "+f"(v[3]), "+f"(v[4]), "+f"(v[5]), "+f"(v[6]), "+f"(v[7]),
+                 "+f"(v[8]), "+f"(v[9]), "+f"(v[10]), "+f"(v[11]), "+f"(v[12]), "+f"(v[13]), "+f"(v[14]),
+                 "+f"(v[15]), "+f"(v[16]), "+f"(v[17]), "+f"(v[18]), "+f"(v[19]), "+f"(v[20]), "+f"(v[21]),
+                 "+f"(v[22]), "+f"(v[23]), "+f"(v[24]), "+f"(v[25]), "+f"(v[26]), "+f"(v[27]), "+f"(v[28]),
+                 "+f"(v[29]), "+f"(v[30]), "+f"(v[31]), "+f"(w[0]), "+f"(w[1]), "+f"(w[2]), "+f"(w[3]),
+                 "+f"(w[4]), "+f"(w[5]), "+f"(w[6]), "+f"(w[7]), "+f"(w[8]), "+f"(w[9]), "+f"(w[10]),
+                 "+f"(w[11]), "+f"(w[12]), "+f"(w[13]), "+f"(w[14]), "+f"(w[15]), "+f"(w[16]), "+f"(w[17]),
+                 "+f"(w[18]), "+f"(w[19]), "+f"(w[20]), "+f"(w[21]), "+f"(w[22]), "+f"(w[23]), "+f"(w[24]),
+                 "+f"(w[25]), "+f"(w[26]), "+f"(w[27]), "+f"(w[28]), "+f"(w[29]), "+f"(w[30]), "+f"(w[31])
+               :
+               : "memory");
+}
+
 // Write one 32-value row of a tile pair (hi, lo) from FP32 values.
 __device__ __forceinline__ void put_row(float* hi, float* lo, int r, const float (&v)[32]) {
 #pragma unroll
