@@ -20,14 +20,15 @@ def _np(out):
 
 
 @pytest.mark.gpu
-def test_graph_replay_matches_direct_run(native):
+@pytest.mark.parametrize("precision", [0, 1])
+def test_graph_replay_matches_direct_run(native, precision):
     import torch
     from pamtra_b200._native import Engine
     eng = Engine(0)
     b = pbatch.pack_pam(wl.c2_pam(64, seed=31), wl.C2_FREQS)
-    direct = _np(pbatch.run(b, 0, eng=eng))
+    direct = _np(pbatch.run(b, 0, precision=precision, eng=eng))
     stream = torch.cuda.Stream()
-    g, out = pbatch.capture(b, 0, stream=stream, eng=eng)
+    g, out = pbatch.capture(b, 0, precision=precision, stream=stream, eng=eng)
     out["tb"].zero_()
     g.launch(stream)
     stream.synchronize()
@@ -40,7 +41,7 @@ def test_graph_replay_matches_direct_run(native):
     stream.synchronize()
     b2 = pbatch.pack_pam(wl.c2_pam(64, seed=31), wl.C2_FREQS)
     b2.host["hydro_q"] = b2.host["hydro_q"] * 0.5
-    ref2 = _np(pbatch.run(b2, 0, eng=eng))
+    ref2 = _np(pbatch.run(b2, 0, precision=precision, eng=eng))
     assert np.array_equal(out["tb"].cpu().numpy(), ref2["tb"])
     assert not np.array_equal(ref2["tb"], direct["tb"])
     g.close()

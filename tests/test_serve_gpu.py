@@ -11,18 +11,22 @@ from pamtra_b200 import serve
 pytestmark = pytest.mark.gpu
 
 
-def _alone(b):
+def _alone(b, precision=0):
     import torch
-    out = pbatch.run(b, 0)
+    out = pbatch.run(b, 0, precision=precision)
     torch.cuda.synchronize()
     return {k: v.cpu().numpy() for k, v in out.items()}
 
 
-def test_results_same_alone_and_in_mix(native):
+# the reference-order FP64 form and the split-precision form, whose kernels
+# pair items and units of different columns inside one CTA (the pairs change
+# with the mix)
+@pytest.mark.parametrize("precision", [0, 1])
+def test_results_same_alone_and_in_mix(native, precision):
     reqs = serve.request_stream(7, seed=50, max_cols=24, nfreq_range=(1, 6))
-    alone = [_alone(b) for b in reqs]
+    alone = [_alone(b, precision) for b in reqs]
     # small arenas force chunking of the larger requests and merging of the small ones
-    srv = serve.Server(0, slots=3, arena_bytes=192 << 20, max_cols=48)
+    srv = serve.Server(0, slots=3, arena_bytes=192 << 20, max_cols=48, precision=precision)
     try:
         served = [srv.submit(b) for b in reqs]
         assert srv.drain(timeout=300)
