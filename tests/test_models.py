@@ -172,3 +172,16 @@ def test_models_column_matches_oracle(oracle_mod, native, liq_mod, gas_mod):
     assert np.max(np.abs(pam.r["tb"] - ref["tb"])) < 1e-6
     base, _ = oracle_mod.run_pamtra(wl.c1_pam(), wl.C1_FREQS)
     assert np.max(np.abs(ref["tb"] - base["tb"])) > 1e-3  # the model is not a no-op
+
+
+def test_ray_tables_agree():
+    # the device copy (pamtra_b200/csrc/ray_table.cuh) and the oracle's
+    # (oracle/ray_table.inc) come from one generator run: same literals
+    import re
+    from pathlib import Path
+    root = Path(__file__).resolve().parents[1]
+    dev = (root / "pamtra_b200" / "csrc" / "ray_table.cuh").read_text()
+    orc = (root / "oracle" / "ray_table.inc").read_text()
+    for name in ("ray_wl", "ray_rn", "ray_cn"):
+        vals = [re.search(r"%s\[RAY_NUMWAT\] = \{(.*?)\};" % name, t, re.S).group(1).split() for t in (dev, orc)]
+        assert vals[0] == vals[1] and len(vals[0]) == 518, name
