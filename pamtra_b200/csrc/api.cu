@@ -980,7 +980,7 @@ int32_t pamtra_b200_run(pamtra_b200_ctx* ctx, const pamtra_b200_settings* st, co
     int g = persistent_grid((const void*)k_layer<32>, RTCfg<32>::T, sizeof(LayerSmem<32>), sms, ctx->layer_cps);
     if (H > 0 && split) {
       // one item per CTA, one CTA per SM (165 KB shared memory, 256 TMEM columns)
-      k_layer_tc64<<<sms, 128, layer_tc64_smem(), stream>>>(b, w, *st, ssp); launches++;
+      k_layer_tc64<<<sms, 256, layer_tc64_smem(), stream>>>(b, w, *st, ssp); launches++;
     } else if (H > 0) {
       k_layer<32><<<g, RTCfg<32>::T, sizeof(LayerSmem<32>), stream>>>(b, w, *st, ssp); launches++;
     }

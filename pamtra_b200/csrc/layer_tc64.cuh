@@ -3,10 +3,13 @@
 // 64 x 64, so two of them already fill the MMA: with D = A B^T,
 //     A = [Ya^T; Yb^T]   (128 rows: the columns of the two right factors)
 //     B = X              (64 rows: the left factor; K = 64)
-// lane 64p + m of D is column m of X Yp.  Thread t owns lane t (product
-// p = t / 64, column t % 64) for the whole doubling, so its A row, its D lane
-// and its master column coincide.  The deviation forms, phases, series plans,
-// source recurrences and bounded waits are those of k_layer_tc<16>.
+// lane 64p + m of D is column m of X Yp.  Eight warps: warps w and w + 4
+// share the TMEM lanes 32 (w mod 4) .. 32 (w mod 4) + 31, so a thread owns
+// lane 32 (w mod 4) + lane (product p, column m) for the whole doubling and
+// half w / 4 of it: rows 32 h .. 32 h + 31 of its product column (D columns
+// 32 h ..), K = 32 h .. of its A row, a quarter of a B row and one mat-vec
+// entry.  The deviation forms, phases, series plans, source recurrences and
+// bounded waits are those of k_layer_tc<16>.
 #pragma once
 #include "layer_tc.cuh"
 
@@ -25,15 +28,14 @@ struct Tc64Item {
   float xa[4096];                          // series power X, then Z~
   float src[4][64];                        // S+ linear, S+ constant, S- linear, S- constant
   float vv[4][64], uv[4][64], wv[4][64];   // right-hand vectors of the three groups
-  float nrm_part[2];
-  int pad_[30];
+  int pad_[32];
 };
 
 struct Tc64Tiles {
   float b_hi[64 * 64], b_lo[64 * 64];  // B tile pair, K-major, K = 64 (row groups 2048 bytes apart)
 };
 
-// FP64 set-up scratch of the item (layer_setup with 128 threads).
+// FP64 set-up scratch of the item (layer_setup with 256 threads).
 struct Tc64Setup {
   static constexpr int n = 64, MAT = RTCfg<32>::MAT;
   double r[MAT], t[MAT];
@@ -105,29 +107,21 @@ __device__ __forceinline__ float matvec1_64(const float* __restrict__ M, const f
   return a;
 }
 
-// Operands of one group for thread t: its A row (column `col` of `asrc`,
-// 64 values) split into TF32 hi / lo in its TMEM lane, and half h of B row
-// `brow` (row brow of `bsrc`, K = 32h .. 32h+31) in shared memory.
+// Operands of one group for thread t: half hh (K = 32 hh .. 32 hh + 31) of
+// its A row (column `col` of `asrc`) split into TF32 hi / lo in its TMEM lane,
+// and K = kq .. kq + 15 of B row `brow` (row brow of `bsrc`) in shared memory;
+// the A stores run while the B part is built.
 __device__ __forceinline__ void build_operands64(Tc64Tiles& TL, const float* asrc, const float* bsrc, uint32_t ta_hi,
-                                                 uint32_t ta_lo, int col, int brow, int h) {
-  {
-    float c[32], lo[32];
-    ld_col64(asrc, col, 0, c);
-#pragma unroll
-    for (int r = 0; r < 32; r++) tc::split(c[r], c[r], lo[r]);
-    tc::tmem_st32(ta_hi, c);
-    tc::tmem_st32(ta_lo, lo);
-  }
-  // the second half's stores run while the B half is built; their wait comes last
+                                                 uint32_t ta_lo, int col, int hh, int brow, int kq) {
   float c[32], lo[32];
-  ld_col64(asrc, col, 1, c);
+  ld_col64(asrc, col, hh, c);
 #pragma unroll
   for (int r = 0; r < 32; r++) tc::split(c[r], c[r], lo[r]);
-  tc::tmem_st32_issue(ta_hi + 32u, c);
-  tc::tmem_st32_issue(ta_lo + 32u, lo);
+  tc::tmem_st32_issue(ta_hi + 32u * hh, c);
+  tc::tmem_st32_issue(ta_lo + 32u * hh, lo);
 #pragma unroll
-  for (int q = 0; q < 8; q++) {
-    const int k0 = 32 * h + 4 * q;
+  for (int q = 0; q < 4; q++) {
+    const int k0 = kq + 4 * q;
     float4 bh, bl;
     tc::split(bsrc[midx64(brow, k0 + 0)], bh.x, bl.x);
     tc::split(bsrc[midx64(brow, k0 + 1)], bh.y, bl.y);
@@ -158,7 +152,7 @@ __device__ __forceinline__ void mma3_k64(uint32_t d_tmem, uint32_t a_hi, uint32_
                : "memory");
 }
 
-__global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b200_settings st,
+__global__ void __launch_bounds__(256, 1) k_layer_tc64(Batch b, Work w, pamtra_b200_settings st,
                                                       double* __restrict__ ssp_scat) {
   constexpr int N = 32, n = 64, LD = RTCfg<N>::LD, MAT = RTCfg<N>::MAT;
   enum { G1 = 0, SER = 1, G2 = 2, G3 = 3 };
@@ -170,9 +164,12 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
   __shared__ uint64_t mbar;
   __shared__ uint32_t tslot;
   __shared__ int s_item, s_dead, s_status;
-  __shared__ float s_mv[2][32];  // warp 0's mat-vec results, computed by warps 1 and 2
+  __shared__ float s_mv[4][64];  // mat-vec results: vector, entry
+  __shared__ float s_ns[2][64];  // column abs-sums of P over the two halves of the rows
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
-  const int slot = t >> 6, col = t & 63;  // my product and my column of it (= my A row, my D lane)
+  const int q4 = warp & 3, hh = warp >> 2;      // my TMEM lane quarter; my half of the column (rows, A's K)
+  const int arow = 32 * q4 + lane;              // my A row = my D lane
+  const int slot = arow >> 6, col = arow & 63;  // my product and my column of it
   const int Fm = b.max_nfreq;
   const int P = min(w.counters[0], w.pmax);
   const int nitems = P * Fm;
@@ -185,7 +182,7 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  const uint32_t lanes = (uint32_t)(warp * 32) << 16;
+  const uint32_t lanes = (uint32_t)(q4 * 32) << 16;
   const uint32_t dmine = tslot + lanes;
   const uint32_t ahi = tslot + lanes + 64u, alo = tslot + lanes + 128u;
   uint32_t parity = 0;
@@ -203,13 +200,13 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
     if (t < N) { S.mu[t] = w.lob_mu[lob_off(N) + t]; S.wq[t] = w.lob_w[lob_off(N) + t]; }
     __syncthreads();
     LayerItem it;
-    if (!layer_setup<N, Tc64Setup, 128>(b, w, st, ssp_scat, S, item, it)) continue;
+    if (!layer_setup<N, Tc64Setup, 256>(b, w, st, ssp_scat, S, item, it)) continue;
     const int nd = it.nd;
     if (t == 0) s_status = it.status;
     if (nd == 0) {
-      layer_store<N, 128>(w, item, S.r, S.t, S.lin);
+      layer_store<N, 256>(w, item, S.r, S.t, S.lin);
     } else {
-      for (int e = t; e < n * n; e += 128) {
+      for (int e = t; e < n * n; e += 256) {
         const int cc = e >> 6, r = e & 63;
         my.rm[midx64(r, cc)] = (float)S.r[cc * LD + r];
         my.tm[midx64(r, cc)] = (float)((r == cc ? 1.0 : 0.0) - S.t[cc * LD + r]);
@@ -226,10 +223,10 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
     bool ok = true;
     if (nd > 0) {
       // v = [S- + f C-, C-, S+, C+] (thread t: entry col of the vectors of its slot)
-      if (slot == 0) {
+      if (hh == 0 && slot == 0) {
         my.vv[2][col] = my.src[0][col];
         my.vv[3][col] = my.src[1][col];
-      } else {
+      } else if (hh == 0) {
         my.vv[0][col] = my.src[2][col] + linfac * my.src[3][col];
         my.vv[1][col] = my.src[3][col];
       }
@@ -247,7 +244,7 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
           else if (phase == SER) { asrc = slot ? my.gm : my.xa; bsrc = my.xa; }
           else if (phase == G2) { asrc = slot ? my.vm : my.tm; bsrc = my.gm; }
           else { asrc = slot ? my.vm : my.xa; bsrc = my.tm; }
-          build_operands64(TL, asrc, bsrc, ahi, alo, col, col, slot);
+          build_operands64(TL, asrc, bsrc, ahi, alo, col, hh, col, 32 * slot + 16 * hh);
         }
         tc::fence_async_smem();
         tc::fence_before_sync();
@@ -255,18 +252,22 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
         tc::fence_after_sync();
         if (t == 0) mma3_k64(tslot, tslot + 64u, tslot + 128u, TL.b_hi, TL.b_lo, &mbar);
         float m0 = 0.f, m1 = 0.f;
-        float xk[2][32];  // slot 1 of a series step: its column of X, taken before slot 0 replaces X
-        if (phase == SER && slot == 1) {
-          ld_col64(my.xa, col, 0, xk[0]);
-          ld_col64(my.xa, col, 1, xk[1]);
-        }
+        float xk[32];  // slot 1 of a series step: its half column of X, taken before slot 0 replaces X
+        if (phase == SER && slot == 1) ld_col64(my.xa, col, hh, xk);
         if (phase != SER) {
           const float* mv = (phase == G1) ? my.rm : (phase == G2) ? my.gm : my.tm;
           const float(*x)[64] = (phase == G1) ? my.vv : (phase == G2) ? my.uv : my.wv;
-          // warp 0 spends this time issuing the MMAs: warps 1 and 2 take
-          // its two mat-vecs (rows 0..31, the vectors of slot 0)
-          if (warp != 0) matvec2_64(mv, x[2 * slot], x[2 * slot + 1], col, m0, m1);
-          if (warp == 1 || warp == 2) s_mv[warp - 1][lane] = matvec1_64(mv, x[warp - 1], lane);
+          // one vector entry per thread (vector 2 slot + hh, row col); warp 0
+          // issues the MMAs meanwhile, so warp 4 (the same rows) takes both
+          // vectors of slot 0 for rows 0..31
+          if (warp == 4) {
+            float y0, y1;
+            matvec2_64(mv, x[0], x[1], col, y0, y1);
+            s_mv[0][col] = y0;
+            s_mv[1][col] = y1;
+          } else if (warp != 0) {
+            s_mv[2 * slot + hh][col] = matvec1_64(mv, x[2 * slot + hh], col);
+          }
         }
         {
           const bool mine = tc::mbar_wait(&mbar, parity, w.spin_limit);
@@ -275,14 +276,14 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
           tc::fence_after_sync();
         }
         if (!ok) break;
-        if (warp == 0 && phase != SER) {
-          m0 = s_mv[0][lane];
-          m1 = s_mv[1][lane];
+        if (phase != SER) {
+          m0 = s_mv[2 * slot][col];
+          m1 = s_mv[2 * slot + 1][col];
         }
         if (on) {
           float nsum = 0.f;
-#pragma unroll
-          for (int h = 0; h < 2; h++) {
+          {
+            const int h = hh;  // my half of the column
             float dv[32], a[32];
             tc::tmem_ld32(dmine + 32u * h, dv);
             if (phase == G1) {
@@ -309,7 +310,7 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
               } else {  // G~ += X + X G~
                 ld_col64(my.gm, col, h, a);
 #pragma unroll
-                for (int r = 0; r < 32; r++) a[r] = a[r] + (xk[h][r] + dv[r]);
+                for (int r = 0; r < 32; r++) a[r] = a[r] + (xk[r] + dv[r]);
                 st_col64(my.gm, col, h, a);
               }
             } else if (phase == G2) {
@@ -343,22 +344,21 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
               }
             }
           }
-          // the vector parts (entry `col` of the slot's two vectors)
-          if (phase == G1) {
-            if (slot == 0) {  // u0 = S+ + R v0, u1 = C+ + R v1; norm of P over the slot's two warps
+          if (phase == G1 && slot == 0) s_ns[hh][col] = nsum;  // my half of the column's abs-sum
+          // the vector parts (entry `col` of the slot's two vectors), by the
+          // threads of the first halves
+          if (hh == 0 && phase == G1) {
+            if (slot == 0) {  // u0 = S+ + R v0, u1 = C+ + R v1
               my.uv[0][col] = my.src[0][col] + m0;
               my.uv[1][col] = my.src[1][col] + m1;
-#pragma unroll
-              for (int o = 16; o > 0; o >>= 1) nsum = fmaxf(nsum, __shfl_xor_sync(0xffffffffu, nsum, o));
-              if (lane == 0) my.nrm_part[warp] = nsum;
             } else {  // u2 = v0 + R v2, u3 = C- + R v3
               my.uv[2][col] = my.vv[0][col] + m0;
               my.uv[3][col] = my.src[3][col] + m1;
             }
-          } else if (phase == G2) {  // w = u + G~ u
+          } else if (hh == 0 && phase == G2) {  // w = u + G~ u
             my.wv[2 * slot][col] = my.uv[2 * slot][col] + m0;
             my.wv[2 * slot + 1][col] = my.uv[2 * slot + 1][col] + m1;
-          } else if (phase == G3) {  // T w = w - T~ w
+          } else if (hh == 0 && phase == G3) {  // T w = w - T~ w
             const float a0 = my.wv[2 * slot][col] - m0, a1 = my.wv[2 * slot + 1][col] - m1;
             if (slot == 0) {  // S+' = (S+ + a0) + f C+,  C+' = C+ + a1
               const float sp = (my.src[0][col] + a0) + linfac * my.src[1][col];
@@ -380,31 +380,31 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
         __syncthreads();  // masters complete before the next operands are built
         // ---- next phase
         if (phase == G1) {
-          const float nrm = fmaxf(my.nrm_part[0], my.nrm_part[1]);
+          // column-sum norm of P (every warp forms the same value)
+          float nrm = fmaxf(s_ns[0][lane] + s_ns[1][lane], s_ns[0][lane + 32] + s_ns[1][lane + 32]);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) nrm = fmaxf(nrm, __shfl_xor_sync(0xffffffffu, nrm, o));
           mys = series_steps(nrm);
           if (mys == -1) {
             // ||P|| too large for the series: FP64 Gauss-Jordan on I - X (the tiles are free here)
             double* M = Q.u.gj;
             InvScratch<64>& IS = *reinterpret_cast<InvScratch<64>*>(M + MAT);
-            for (int e = t; e < n * n; e += 128) {
+            for (int e = t; e < n * n; e += 256) {
               const int cc = e >> 6, r = e & 63;
               M[cc * LD + r] = (r == cc ? 1.0 : 0.0) - (double)my.xa[midx64(r, cc)];
             }
             __syncthreads();
-            if (ginv<64, 128>(M, IS) && t == 0) s_status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
-            for (int e = t; e < n * n; e += 128) {
+            if (ginv<64, 256>(M, IS) && t == 0) s_status |= PAMTRA_B200_FATAL | PAMTRA_B200_ST_PIVOT;
+            for (int e = t; e < n * n; e += 256) {
               const int cc = e >> 6, r = e & 63;
               my.gm[midx64(r, cc)] = (float)(M[cc * LD + r] - (r == cc ? 1.0 : 0.0));
             }
-          } else if (slot == 1) {  // G~ = X (no series), or G~ = 0 to start one
+          } else if (slot == 1) {  // G~ = X (no series), or G~ = 0 to start one (my half)
+            float g[32];
+            if (mys == 0) ld_col64(my.xa, col, hh, g);
 #pragma unroll
-            for (int h = 0; h < 2; h++) {
-              float g[32];
-              if (mys == 0) ld_col64(my.xa, col, h, g);
-#pragma unroll
-              for (int r = 0; r < 32; r++) g[r] = (mys == 0) ? g[r] : 0.f;
-              st_col64(my.gm, col, h, g);
-            }
+            for (int r = 0; r < 32; r++) g[r] = (mys == 0) ? g[r] : 0.f;
+            st_col64(my.gm, col, hh, g);
           }
           myg = (mys >= 1) ? mys + 1 : (mys == SERIES_H1 ? 1 : 0);
           __syncthreads();
@@ -427,7 +427,7 @@ __global__ void __launch_bounds__(128, 1) k_layer_tc64(Batch b, Work w, pamtra_b
       __syncthreads();
       // ---- layer R, T = I - T~, S+/S- in FP64
       double* out = w.lay + (size_t)item * w.lay_stride;
-      for (int e = t; e < n * n; e += 128) {
+      for (int e = t; e < n * n; e += 256) {
         const int cc = e >> 6, r = e & 63;
         out[cc * LD + r] = (double)my.rm[midx64(r, cc)];
         out[MAT + cc * LD + r] = (r == cc ? 1.0 : 0.0) - (double)my.tm[midx64(r, cc)];
