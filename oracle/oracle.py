@@ -85,6 +85,16 @@ def lib():
         l.orc_eps_water_tkc.restype = None
         l.orc_eps_water_tkc.argtypes = [ctypes.c_double, ctypes.c_double, dp, dp]
         l.orc_lobatto.argtypes = [ctypes.c_int, dp, dp]
+        fp = ctypes.POINTER(ctypes.c_float)
+        l.orc_tmatrix_single.restype = ctypes.c_int
+        l.orc_tmatrix_single.argtypes = [ctypes.c_int] + [ctypes.c_double] * 6 + [dp] * 4
+        l.orc_tmatrix_tmat.restype = ctypes.c_int
+        l.orc_tmatrix_tmat.argtypes = [ctypes.c_double] * 5 + [ctypes.c_int, fp, fp]
+        l.orc_tmatrix_species.restype = ctypes.c_int
+        l.orc_tmatrix_species.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                          ctypes.c_int, ctypes.c_int] + [dp] * 11
+        l.orc_miecalc.restype = ctypes.c_int
+        l.orc_miecalc.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int] + [dp] * 4
         l.orc_minvert.restype = ctypes.c_int
         l.orc_minvert.argtypes = [ctypes.c_int, dp, dp]
         l.orc_e_sat.argtypes = [ctypes.c_double, dp]
@@ -260,3 +270,64 @@ def minvert(A):
     out = np.zeros_like(A, order="F")
     err = lib().orc_minvert(A.shape[0], _p(A), _p(out))
     return err, out
+
+
+# ---------------------------------------------------------------- T-matrix branch
+
+
+def tmatrix_tmat(lam, mrr, mri, axi, as_ratio):
+    """Single-precision T-matrix of one spheroid (tmatrix_amplq, quad solve):
+    complex array [m = 0..nmax][block 11, 12, 21, 22][n1][n2], or None."""
+    cap = 101 * 4 * 100 * 100
+    re = np.zeros(cap, np.float32)
+    im = np.zeros(cap, np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    nmax = lib().orc_tmatrix_tmat(lam, mrr, mri, axi, as_ratio, cap, re.ctypes.data_as(fp), im.ctypes.data_as(fp))
+    if nmax <= 0:
+        return None
+    n = (nmax + 1) * 4 * nmax * nmax
+    return (re[:n] + 1j * im[:n].astype(np.complex64)).reshape(nmax + 1, 4, nmax, nmax)
+
+
+def tmatrix_single(nummu, frequency, mrr, mri, axi, as_ratio, beta=0.0):
+    """calc_single_tmatrix of one particle: dict of scatter_matrix
+    (Fortran order (2, nummu, 2, nummu, 2)), extinct_matrix (2, 2, nummu),
+    emis_vector (2, nummu), sback (2, 2); None on the reference's error."""
+    scat = np.zeros(2 * nummu * 2 * nummu * 2)
+    ext = np.zeros(4 * nummu)
+    emis = np.zeros(2 * nummu)
+    sb = np.zeros(4)
+    r = lib().orc_tmatrix_single(nummu, frequency, mrr, mri, axi, as_ratio, beta, _p(scat), _p(ext), _p(emis),
+                                 _p(sb))
+    if r:
+        return None
+    return {"scatter_matrix": scat.reshape((2, nummu, 2, nummu, 2), order="F"),
+            "extinct_matrix": ext.reshape((2, 2, nummu), order="F"),
+            "emis_vector": emis.reshape((2, nummu), order="F"), "sback": sb.reshape((2, 2), order="F")}
+
+
+def tmatrix_species(nummu, frequency, ref_re, ref_im, phase, dmax, del_d, ndens, density, as_ratio, canting):
+    """calc_tmatrix of one species at one frequency over its bins (arrays of
+    equal length); same keys as tmatrix_single plus back_spec per bin."""
+    nb = len(dmax)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (dmax, del_d, ndens, density, as_ratio, canting)]
+    scat = np.zeros(2 * nummu * 2 * nummu * 2)
+    ext = np.zeros(4 * nummu)
+    emis = np.zeros(2 * nummu)
+    back = np.zeros(nb)
+    sb = np.zeros(4)
+    r = lib().orc_tmatrix_species(nummu, frequency, ref_re, ref_im, phase, nb, *[_p(a) for a in arrs], _p(scat),
+                                  _p(ext), _p(emis), _p(back), _p(sb))
+    if r:
+        return None
+    return {"scatter_matrix": scat.reshape((2, nummu, 2, nummu, 2), order="F"),
+            "extinct_matrix": ext.reshape((2, 2, nummu), order="F"),
+            "emis_vector": emis.reshape((2, nummu), order="F"), "sback": sb.reshape((2, 2), order="F"),
+            "back_spec": back}
+
+
+def miecalc(x, mr, mi):
+    """Mie coefficients (a_n, b_n) of the oracle's miecalc (index m = mr - i mi)."""
+    ar, ai, br, bi = (np.zeros(10000) for _ in range(4))
+    n = lib().orc_miecalc(x, mr, mi, 10000, _p(ar), _p(ai), _p(br), _p(bi))
+    return (ar[:n] + 1j * ai[:n]), (br[:n] + 1j * bi[:n])

@@ -1703,6 +1703,30 @@ void orc_lobatto(int num, double* mu, double* w) {
 
 int orc_minvert(int n, const double* A, double* Ainv) { return minvert(n, A, Ainv); }
 
+// Mie coefficients a_n, b_n (miecalc, src/mie_scat_utilities.f90:8-75) of a
+// sphere of size parameter x and index m; returns the number of terms (at
+// most cap), or -1.
+int orc_miecalc(double x, double mr, double mi, int cap, double* a_re, double* a_im, double* b_re, double* b_im) {
+  int nterms = 0;
+  std::vector<cplx> a, b;
+  if (miecalc(nterms, x, cmk(mr, mi), a, b)) return -1;
+  for (int n = 0; n < nterms && n < cap; n++) {
+    a_re[n] = a[n + 1].re;
+    a_im[n] = a[n + 1].im;
+    b_re[n] = b[n + 1].re;
+    b_im[n] = b[n + 1].im;
+  }
+  return nterms;
+}
+
+// eps_mix((1,0), m, density) of src/eps_mix.f90 (the soft-spheroid mixing
+// the T-matrix branch applies per bin, src/tmatrix.f90:171-175).
+void orc_eps_mix_m(double re, double im, double dens, double* ore, double* oim) {
+  cplx e = eps_mix_m(cmk(re, im), dens);
+  *ore = e.re;
+  *oim = e.im;
+}
+
 void orc_e_sat(double T, double* e) { *e = e_sat_gg_water(T); }
 
 // Full passive path for one column (src/run_rt.f90 per frequency, with the
