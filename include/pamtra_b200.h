@@ -299,6 +299,44 @@ int32_t pamtra_b200_get_eps_water(int32_t liq_mod, const double* s, const double
 int32_t pamtra_b200_gas_l93(const double* freq, const double* press, const double* vap, const double* temp,
                             double* kext, int32_t n, void* stream);
 
+/* ---- T-matrix scattering of spheroids (scat_name 'tmatrix') ----
+ * calc_tmatrix (src/tmatrix.f90:14-433) for a batch of (species, layer,
+ * frequency) items of nbins bins each: per bin the T-matrix of a spheroid of
+ * the bin's aspect ratio and canting angle (tmatrix_amplq, the EBCM solve of
+ * src/tmatrix_amplq.lp.f, with NMAX and the Gauss points converged as there),
+ * its amplitude matrices over 30 scattering azimuths at the Lobatto angles
+ * (calc_single_tmatrix, src/tmatrix.f90:436-684), and the bin sums weighted
+ * by ndens * del_d.  Replaces the call at src/scatProperties.f90:289-306.
+ * All array pointers are host pointers (on_device = 0: copied in and out, the
+ * call returns when the results are on the host) or device pointers
+ * (on_device = 1: work queued on `stream`). */
+typedef struct {
+  int32_t n_items, nbins, nummu, on_device;  /* nummu in {8, 16, 32} */
+  const double* freq;     /* [n_items] Hz */
+  const double* ref_re;   /* [n_items] refractive index of water or pure ice (either sign of Im) */
+  const double* ref_im;
+  const int32_t* phase;   /* [n_items] 1 liquid, -1 ice (mixed with air where density != 917) */
+  const double* dmax;     /* [n_items][nbins] maximum dimension (m) */
+  const double* del_d;    /* [n_items][nbins] bin width (m) */
+  const double* ndens;    /* [n_items][nbins] number density per size (1/m^4); 0 = empty bin */
+  const double* density;  /* [n_items][nbins] particle density (kg/m^3) */
+  const double* as_ratio; /* [n_items][nbins] aspect ratio (< 1 oblate, > 1 prolate) */
+  const double* canting;  /* [n_items][nbins] canting angle beta (deg) */
+} pamtra_b200_tmatrix_in;
+typedef struct {
+  double* scatter_matrix; /* [n_items][2 * nummu * 2 * nummu * 2], Fortran order of scatter_matrix(2,nummu,2,nummu,2) */
+  double* extinct_matrix; /* [n_items][2 * 2 * nummu] */
+  double* emis_vector;    /* [n_items][2 * nummu] */
+  double* sback;          /* [n_items][2 * 2] */
+  double* back_spec;      /* [n_items][nbins] "NN" backscattering 4 pi ndens Sback(1,1) (m^-1 per m) */
+  int32_t* nmax;          /* [n_items][nbins] converged NMAX (0 empty bin); may be NULL */
+  int32_t* status;        /* [n_items] OR of the bins: FATAL | ST_RANGE for an invalid bin or a solve past
+                             NMAX 48 / 128 Gauss points (the reference allows 100 / 500) */
+} pamtra_b200_tmatrix_out;
+
+int32_t pamtra_b200_tmatrix(pamtra_b200_ctx* ctx, const pamtra_b200_tmatrix_in* in, pamtra_b200_tmatrix_out* out,
+                            void* stream);
+
 /* Matrix inverse with partial pivoting of `count` column-major n x n matrices
  * (replaces MINVERT, src/radmat.f90:155), n in {16,32,64}. */
 int32_t pamtra_b200_minvert_batched(const double* a, double* ainv, int32_t* status, int32_t n, int32_t count,

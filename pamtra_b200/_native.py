@@ -69,6 +69,18 @@ STAGES = ["prep", "psd", "mie", "layer", "adding"]
 _lib = None
 
 
+class TmatrixIn(ctypes.Structure):
+    _fields_ = [("n_items", ctypes.c_int32), ("nbins", ctypes.c_int32), ("nummu", ctypes.c_int32),
+                ("on_device", ctypes.c_int32)] + \
+        [(k, ctypes.c_void_p) for k in ("freq", "ref_re", "ref_im", "phase", "dmax", "del_d", "ndens", "density",
+                                        "as_ratio", "canting")]
+
+
+class TmatrixOut(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in ("scatter_matrix", "extinct_matrix", "emis_vector", "sback",
+                                               "back_spec", "nmax", "status")]
+
+
 def load():
     """Load the shared library (raises OSError if it was not built)."""
     global _lib
@@ -123,6 +135,8 @@ def load():
         l.pamtra_b200_set_wait_limit.argtypes = [_vp, ctypes.c_uint32]
         l.pamtra_b200_layer_products.restype = _i32
         l.pamtra_b200_layer_products.argtypes = [_vp, ctypes.POINTER(ctypes.c_uint64), _vp]
+        l.pamtra_b200_tmatrix.restype = _i32
+        l.pamtra_b200_tmatrix.argtypes = [_vp, ctypes.POINTER(TmatrixIn), ctypes.POINTER(TmatrixOut), _vp]
         l.pamtra_b200_abi_sizes.restype = _i32
         l.pamtra_b200_abi_sizes.argtypes = [ctypes.POINTER(ctypes.c_size_t), _i32]
         _lib = l

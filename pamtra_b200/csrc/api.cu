@@ -26,6 +26,7 @@
 #include "layer_tc.cuh"
 #include "layer_tc64.cuh"
 #include "add_tc.cuh"
+#include "tmatrix.cuh"
 #include "work.cuh"
 
 using namespace pb;
@@ -456,6 +457,8 @@ struct pamtra_b200_ctx {
   double* wtab[3] = {nullptr, nullptr, nullptr};
   int* wt_flags = nullptr;
   int last_launches = 0;
+  char* tm_buf = nullptr;  // T-matrix branch: inputs, per-bin results and the CTAs' scratch slots
+  size_t tm_bytes = 0;
   char* stage = nullptr;  // device staging for run_host
   size_t stage_bytes = 0;
   // launch shapes (pamtra_b200_set_launch; 0 = occupancy default)
@@ -582,6 +585,7 @@ int32_t pamtra_b200_destroy(pamtra_b200_ctx* ctx) {
   cudaFree(ctx->lob_mu);
   cudaFree(ctx->lob_w);
   cudaFree(ctx->stage);
+  cudaFree(ctx->tm_buf);
   for (double* p : ctx->wtab) cudaFree(p);
   cudaFree(ctx->wt_flags);
   for (auto& sg : ctx->sp_ring) {
@@ -1205,6 +1209,90 @@ int32_t pamtra_b200_gas_l93(const double* freq, const double* press, const doubl
   if (n <= 0) return PAMTRA_B200_OK;
   k_l93_elem<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(freq, press, vap, temp, kext, n);
   return cudaGetLastError() == cudaSuccess ? PAMTRA_B200_OK : PAMTRA_B200_FATAL;
+}
+
+// ---------------------------------------------------------------- T-matrix branch
+int32_t pamtra_b200_tmatrix(pamtra_b200_ctx* ctx, const pamtra_b200_tmatrix_in* in, pamtra_b200_tmatrix_out* out,
+                            void* stream_) {
+  if (!ctx || !in || !out) return PAMTRA_B200_FATAL;
+  const int ni = in->n_items, nb = in->nbins, nummu = in->nummu;
+  if (ni <= 0 || nb <= 0) return PAMTRA_B200_OK;
+  if (nummu != 8 && nummu != 16 && nummu != 32) return PAMTRA_B200_FATAL;
+  if ((size_t)ni * nb > (size_t)INT32_MAX / 4) return PAMTRA_B200_FATAL;
+  cudaSetDevice(ctx->device);
+  cudaStream_t stream = (cudaStream_t)stream_;
+  const size_t n = (size_t)ni * nb;
+  const size_t NS = (size_t)2 * nummu * 2 * nummu * 2, NE = 4 * (size_t)nummu, NM = 2 * (size_t)nummu;
+  // one 256-thread CTA per SM (254 registers per thread)
+  const int grid = (int)std::min<size_t>(n, (size_t)ctx->sm_count);
+  // device layout (8-byte units, each array 256-byte aligned)
+  size_t off = 0;
+  auto take = [&](size_t elems8) { const size_t o = off; off += (elems8 + 31) / 32 * 32; return o; };
+  const bool host = !in->on_device;
+  const size_t o_freq = take(ni), o_rre = take(ni), o_rim = take(ni), o_phase = take((ni + 1) / 2);
+  const size_t o_dmax = take(n), o_dd = take(n), o_nd = take(n), o_rho = take(n), o_asr = take(n), o_cant = take(n);
+  const size_t o_mrr = take(n), o_mri = take(n), o_axi = take(n), o_nde = take(n), o_pst = take((n + 1) / 2),
+               o_pnm = take((n + 1) / 2);
+  const size_t o_pscat = take(n * NS), o_pext = take(n * NE), o_pemis = take(n * NM), o_psb = take(n * 4);
+  const size_t o_scat = take((size_t)ni * NS), o_ext = take((size_t)ni * NE), o_emis = take((size_t)ni * NM),
+               o_sb = take((size_t)ni * 4), o_back = take(n), o_st = take(((size_t)ni + 1) / 2), o_cnt = take(1);
+  const size_t o_slot = take((size_t)grid * TM_SLOT_DOUBLES);
+  const size_t bytes = off * 8;
+  if (bytes > ctx->tm_bytes) {
+    cudaStreamSynchronize(stream);
+    cudaFree(ctx->tm_buf);
+    ctx->tm_buf = nullptr;
+    ctx->tm_bytes = 0;
+    if (cudaMalloc(&ctx->tm_buf, bytes) != cudaSuccess) return PAMTRA_B200_FATAL;
+    ctx->tm_bytes = bytes;
+  }
+  char* B = ctx->tm_buf;
+  auto D = [&](size_t o) { return reinterpret_cast<double*>(B + o * 8); };
+  auto I = [&](size_t o) { return reinterpret_cast<int*>(B + o * 8); };
+  const double *freq = in->freq, *rre = in->ref_re, *rim = in->ref_im, *dmax = in->dmax, *dd = in->del_d,
+               *nd = in->ndens, *rho = in->density, *asr = in->as_ratio, *cant = in->canting;
+  const int* phase = in->phase;
+  if (host) {
+    auto up = [&](size_t o, const void* src, size_t b) { cudaMemcpyAsync(B + o * 8, src, b, cudaMemcpyHostToDevice, stream); };
+    up(o_freq, freq, ni * 8); up(o_rre, rre, ni * 8); up(o_rim, rim, ni * 8); up(o_phase, phase, ni * 4);
+    up(o_dmax, dmax, n * 8); up(o_dd, dd, n * 8); up(o_nd, nd, n * 8); up(o_rho, rho, n * 8);
+    up(o_asr, asr, n * 8); up(o_cant, cant, n * 8);
+    freq = D(o_freq); rre = D(o_rre); rim = D(o_rim); phase = I(o_phase);
+    dmax = D(o_dmax); dd = D(o_dd); nd = D(o_nd); rho = D(o_rho); asr = D(o_asr); cant = D(o_cant);
+  }
+  k_tmat_prep<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(ni, nb, freq, rre, rim, phase, dmax, dd, nd, rho, asr, cant,
+                                                                D(o_mrr), D(o_mri), D(o_axi), D(o_nde), I(o_pst));
+  cudaMemsetAsync(I(o_cnt), 0, 4, stream);
+  TmArgs A;
+  A.n_items = ni; A.nbins = nb; A.nummu = nummu;
+  A.freq = freq; A.mrr = D(o_mrr); A.mri = D(o_mri); A.axi = D(o_axi); A.asr = asr; A.beta = cant; A.ndens = D(o_nde);
+  A.mu = ctx->lob_mu + lob_off(nummu); A.wq = ctx->lob_w + lob_off(nummu);
+  A.scat = D(o_pscat); A.ext = D(o_pext); A.emis = D(o_pemis); A.sback = D(o_psb);
+  A.nmax = (!host && out->nmax) ? out->nmax : I(o_pnm);
+  A.status = I(o_pst); A.scratch = D(o_slot); A.counter = I(o_cnt);
+  k_tmatrix<<<grid, TM_THREADS, 0, stream>>>(A);
+  double *scat = out->scatter_matrix, *ext = out->extinct_matrix, *emis = out->emis_vector, *sb = out->sback,
+         *back = out->back_spec;
+  int* st = out->status;
+  if (host) {
+    scat = D(o_scat); ext = D(o_ext); emis = D(o_emis); sb = D(o_sb); back = D(o_back); st = I(o_st);
+  }
+  k_tmat_sum<<<ni, 256, 0, stream>>>(ni, nb, nummu, D(o_nde), dd, D(o_pscat), D(o_pext), D(o_pemis), D(o_psb), I(o_pst),
+                                     scat, ext, emis, sb, back, st);
+  ctx->last_launches = 3;
+  if (cudaGetLastError() != cudaSuccess) return PAMTRA_B200_FATAL;
+  if (host) {
+    auto dn = [&](void* dst, size_t o, size_t b) { cudaMemcpyAsync(dst, B + o * 8, b, cudaMemcpyDeviceToHost, stream); };
+    dn(out->scatter_matrix, o_scat, (size_t)ni * NS * 8);
+    dn(out->extinct_matrix, o_ext, (size_t)ni * NE * 8);
+    dn(out->emis_vector, o_emis, (size_t)ni * NM * 8);
+    dn(out->sback, o_sb, (size_t)ni * 4 * 8);
+    dn(out->back_spec, o_back, n * 8);
+    dn(out->status, o_st, (size_t)ni * 4);
+    if (out->nmax) dn(out->nmax, o_pnm, n * 4);
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return PAMTRA_B200_FATAL;
+  }
+  return PAMTRA_B200_OK;
 }
 
 int32_t pamtra_b200_minvert_batched(const double* a, double* ainv, int32_t* status, int32_t n, int32_t count,

@@ -1,0 +1,99 @@
+"""T-matrix scattering of spheroids (scat_name ``'tmatrix'``) on the GPU.
+
+Host-side mirror of the reference's ``calc_tmatrix`` (src/tmatrix.f90:14-433),
+the routine ``calc_scatProperties`` calls for a species whose ``scat_name`` is
+``tmatrix`` (src/scatProperties.f90:289-306).  The work runs in the native
+library (``pamtra_b200_tmatrix``): one CUDA thread block per size bin solves
+the spheroid's T-matrix (EBCM, src/tmatrix_amplq.lp.f) in FP64, forms the
+amplitude matrices over 30 scattering azimuths at the Lobatto angles, and a
+second kernel sums the bins.  There is no CPU path.
+"""
+
+import ctypes
+
+import numpy as np
+
+from . import _native
+
+OUT_KEYS = ("scatter_matrix", "extinct_matrix", "emis_vector", "sback", "back_spec", "nmax", "status")
+
+
+def _shapes(n_items, nbins, nummu):
+    return {"scatter_matrix": (n_items, 2 * nummu * 2 * nummu * 2), "extinct_matrix": (n_items, 4 * nummu),
+            "emis_vector": (n_items, 2 * nummu), "sback": (n_items, 4), "back_spec": (n_items, nbins),
+            "nmax": (n_items, nbins), "status": (n_items,)}
+
+
+def calc_tmatrix_batch(freq, ref_index, phase, dmax, del_d, ndens, density, as_ratio, canting, nummu=16,
+                       eng=None, stream=None):
+    """calc_tmatrix for ``n_items`` (species, layer, frequency) items of
+    ``nbins`` bins: ``freq`` (Hz), ``ref_index`` (complex) and ``phase``
+    (1 liquid, -1 ice) per item, the bin arrays ``[n_items, nbins]`` (m, m,
+    1/m^4, kg/m^3, -, deg).
+
+    numpy inputs run through host buffers (copies in the call); torch CUDA
+    tensors stay on the device and the work is queued on ``stream``.
+    Returns a dict of flat outputs (see ``_shapes``) with the Fortran element
+    order of the reference's arrays inside each item."""
+    eng = eng or _native.engine()
+    on_dev = not isinstance(dmax, np.ndarray)
+    if on_dev:
+        import torch
+        dev = dmax.device
+        f64 = dict(dtype=torch.float64, device=dev)
+        n_items, nbins = dmax.shape
+        ri = torch.as_tensor(ref_index, device=dev)
+        args = {"freq": torch.as_tensor(freq, **f64).contiguous(), "ref_re": ri.real.to(torch.float64).contiguous(),
+                "ref_im": ri.imag.to(torch.float64).contiguous(),
+                "phase": torch.as_tensor(phase, dtype=torch.int32, device=dev).contiguous()}
+        for k, v in (("dmax", dmax), ("del_d", del_d), ("ndens", ndens), ("density", density),
+                     ("as_ratio", as_ratio), ("canting", canting)):
+            args[k] = torch.as_tensor(v, **f64).reshape(n_items, nbins).contiguous()
+        out = {k: torch.zeros(sh, dtype=torch.int32 if k in ("nmax", "status") else torch.float64, device=dev)
+               for k, sh in _shapes(n_items, nbins, nummu).items()}
+    else:
+        dmax = np.asarray(dmax, dtype=np.float64)
+        n_items, nbins = dmax.shape
+        ri = np.asarray(ref_index, dtype=np.complex128).reshape(n_items)
+        args = {"freq": np.ascontiguousarray(np.asarray(freq, dtype=np.float64).reshape(n_items)),
+                "ref_re": np.ascontiguousarray(ri.real), "ref_im": np.ascontiguousarray(ri.imag),
+                "phase": np.ascontiguousarray(np.asarray(phase, dtype=np.int32).reshape(n_items))}
+        for k, v in (("dmax", dmax), ("del_d", del_d), ("ndens", ndens), ("density", density),
+                     ("as_ratio", as_ratio), ("canting", canting)):
+            args[k] = np.ascontiguousarray(np.asarray(v, dtype=np.float64).reshape(n_items, nbins))
+        out = {k: np.zeros(sh, dtype=np.int32 if k in ("nmax", "status") else np.float64)
+               for k, sh in _shapes(n_items, nbins, nummu).items()}
+    ti = _native.TmatrixIn()
+    ti.n_items, ti.nbins, ti.nummu, ti.on_device = int(n_items), int(nbins), int(nummu), int(on_dev)
+    for k, v in args.items():
+        setattr(ti, k, _native._ptr(v))
+    to = _native.TmatrixOut()
+    for k in OUT_KEYS:
+        setattr(to, k, _native._ptr(out[k]))
+    if stream is None and on_dev:
+        import torch
+        stream = torch.cuda.current_stream(dmax.device).cuda_stream
+    err = eng.lib.pamtra_b200_tmatrix(eng.handle, ctypes.byref(ti), ctypes.byref(to), stream or None)
+    if err != 0:
+        raise RuntimeError("pamtra_b200_tmatrix failed (%d)" % err)
+    out["_keepalive"] = args
+    return out
+
+
+def calc_tmatrix(frequency, ref_index, phase, dmax, del_d, ndens, density, as_ratio, canting, nummu=16, eng=None):
+    """calc_tmatrix (src/tmatrix.f90:14) for one species at one frequency, with
+    the reference's argument meaning and output shapes: returns
+    (scatter_matrix (2, nummu, 2, nummu, 2), extinct_matrix (2, 2, nummu),
+    emis_vector (2, nummu), back_spec (nbins,) for radar_pol "NN",
+    Sback (2, 2)).  Raises RuntimeError where the reference reports a fatal
+    error (invalid bin, NMAX or Gauss-point limit)."""
+    o = calc_tmatrix_batch(np.array([frequency]), np.array([ref_index]), np.array([phase]),
+                           np.asarray(dmax, dtype=np.float64)[None, :], np.asarray(del_d)[None, :],
+                           np.asarray(ndens)[None, :], np.asarray(density)[None, :], np.asarray(as_ratio)[None, :],
+                           np.asarray(canting)[None, :], nummu=nummu, eng=eng)
+    if int(o["status"][0]) != 0:
+        raise RuntimeError("calc_tmatrix: status 0x%x" % int(o["status"][0]))
+    return (o["scatter_matrix"][0].reshape((2, nummu, 2, nummu, 2), order="F"),
+            o["extinct_matrix"][0].reshape((2, 2, nummu), order="F"),
+            o["emis_vector"][0].reshape((2, nummu), order="F"), o["back_spec"][0],
+            o["sback"][0].reshape((2, 2), order="F"))

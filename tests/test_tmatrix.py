@@ -1,0 +1,194 @@
+"""T-matrix branch (scat_name 'tmatrix', src/tmatrix.f90 + src/tmatrix_amplq.lp.f).
+
+CPU tests pin the quad-precision oracle by the sphere limit: for aspect ratio
+1 the T-matrix is diagonal with T11 = -b_n and T22 = -a_n (the Mie
+coefficients of the oracle's miecalc, itself pinned to the reference's golden
+fixture), and the extinction and backscattering cross-sections follow.  The
+reference stores T in single precision (REAL*4 common /TMAT/), so the pins
+hold to float rounding (a few 1e-7 relative).
+
+GPU tests compare ``pamtra_b200_tmatrix`` (FP64 solve, single-precision T as
+the reference stores it) with the oracle (REAL*16 solve like the reference)
+bin by bin and summed, over spheres, oblate and prolate spheroids, soft ice
+spheroids, canted particles (the full AMPL path), empty and invalid bins and
+NUMMU 8/16/32.  Tolerance: 2e-6 of each output array's largest magnitude
+(T rounded to single precision by both sides; FP64 vs REAL*16 solve).
+"""
+import numpy as np
+import pytest
+
+C = 299792458.0
+
+
+def _mie_cross(oracle_mod, f, mr, mi, axi):
+    k = 2 * np.pi * f / C
+    a, b = oracle_mod.miecalc(k * axi, mr, -mi)
+    n = np.arange(1, len(a) + 1)
+    cext = 2 * np.pi / k ** 2 * np.sum((2 * n + 1) * np.real(a + b))
+    cback = np.pi / k ** 2 * abs(np.sum((2 * n + 1) * (-1.0) ** n * (a - b))) ** 2
+    return a, b, cext, cback
+
+
+SPHERES = [(89e9, 1.78, 0.003, 0.5e-3), (150e9, 6.5, 2.8, 1.0e-3), (35e9, 1.3, 0.001, 3e-3)]
+
+
+@pytest.mark.parametrize("case", SPHERES)
+def test_oracle_sphere_tmatrix_is_mie(oracle_mod, case):
+    f, mr, mi, axi = case
+    T = oracle_mod.tmatrix_tmat(C / f, mr, mi, axi, 1.0)
+    a, b, _, _ = _mie_cross(oracle_mod, f, mr, mi, axi)
+    nmax = T.shape[2]
+    n = min(nmax, len(a))
+    for m in range(0, 3):
+        for blk, coef in ((0, b), (3, a)):
+            d = np.array([T[m, blk, k, k] for k in range(max(m - 1, 0), n)])
+            ref = -coef[max(m - 1, 0):n]
+            assert np.max(np.abs(d - ref)) <= 3e-7 * np.max(np.abs(coef)), (m, blk)
+        # the sphere does not couple orders or the two polarisation blocks
+        off = T[m, 0] - np.diag(np.diag(T[m, 0]))
+        assert np.max(np.abs(off)) < 1e-20
+        assert np.max(np.abs(T[m, 1])) < 1e-20 and np.max(np.abs(T[m, 2])) < 1e-20
+
+
+@pytest.mark.parametrize("case", SPHERES)
+def test_oracle_sphere_cross_sections(oracle_mod, case):
+    f, mr, mi, axi = case
+    r = oracle_mod.tmatrix_single(16, f, mr, mi, axi, 1.0)
+    _, _, cext, cback = _mie_cross(oracle_mod, f, mr, mi, axi)
+    ext = r["extinct_matrix"]
+    # forward extinction is the same at every incidence and unpolarised
+    assert np.allclose(ext[0, 0, :], cext, rtol=5e-7, atol=0)
+    assert np.max(np.abs(ext[0, 1, :])) < 1e-12 * cext
+    assert abs(4 * np.pi * r["sback"][0, 0] / cback - 1) < 2e-6
+    # a sphere does not depolarise the backscattered wave
+    assert abs(r["sback"][0, 1]) < 1e-12 * r["sback"][0, 0]
+
+
+def test_oracle_spheroid_symmetries(oracle_mod):
+    """Upright spheroid: the extinction matrix is symmetric, its 11 element
+    at nadir incidence equals the sphere-like unpolarised one, and an oblate
+    particle extinguishes horizontal polarisation more at grazing angles."""
+    r = oracle_mod.tmatrix_single(16, 89e9, 1.78, 0.003, 0.8e-3, 0.6)
+    ext = r["extinct_matrix"]
+    assert np.allclose(ext[0, 1, :], ext[1, 0, :], rtol=0, atol=0)
+    assert np.allclose(ext[0, 0, :], ext[1, 1, :], rtol=0, atol=0)
+    # at nadir (mu = 1) the polarisation term vanishes for an upright particle
+    assert abs(ext[0, 1, -1]) < 1e-6 * ext[0, 0, -1]
+    assert abs(ext[0, 1, 0]) > 1e-3 * ext[0, 0, 0]
+
+
+# ---------------------------------------------------------------- GPU parity
+
+def _run_gpu(items, nbins, nummu):
+    from pamtra_b200 import tmatrix as ptm
+    arr = {k: np.array([it[k] for it in items], dtype=np.float64).reshape(len(items), nbins)
+           for k in ("dmax", "del_d", "ndens", "density", "as_ratio", "canting")}
+    return ptm.calc_tmatrix_batch(np.array([it["freq"] for it in items]), np.array([it["ref"] for it in items]),
+                                  np.array([it["phase"] for it in items], dtype=np.int32), arr["dmax"], arr["del_d"],
+                                  arr["ndens"], arr["density"], arr["as_ratio"], arr["canting"], nummu=nummu)
+
+
+def _oracle_item(oracle_mod, it, nummu):
+    return oracle_mod.tmatrix_species(nummu, it["freq"], it["ref"].real, it["ref"].imag, it["phase"],
+                                      it["dmax"], it["del_d"], it["ndens"], it["density"], it["as_ratio"],
+                                      it["canting"])
+
+
+def _item(freq, ref, phase, dmax, ndens, density, as_ratio, canting, del_d=1e-4):
+    nb = len(dmax)
+    return {"freq": freq, "ref": complex(ref), "phase": phase, "dmax": list(dmax), "del_d": [del_d] * nb,
+            "ndens": list(ndens), "density": [density] * nb if np.isscalar(density) else list(density),
+            "as_ratio": [as_ratio] * nb if np.isscalar(as_ratio) else list(as_ratio),
+            "canting": [canting] * nb if np.isscalar(canting) else list(canting)}
+
+
+def _compare(out, refs, nummu, tol=2e-6):
+    for i, ref in enumerate(refs):
+        assert ref is not None
+        assert int(out["status"][i]) == 0
+        g = {"scatter_matrix": out["scatter_matrix"][i].reshape((2, nummu, 2, nummu, 2), order="F"),
+             "extinct_matrix": out["extinct_matrix"][i].reshape((2, 2, nummu), order="F"),
+             "emis_vector": out["emis_vector"][i].reshape((2, nummu), order="F"),
+             "sback": out["sback"][i].reshape((2, 2), order="F"), "back_spec": out["back_spec"][i]}
+        for k in g:
+            scale = np.max(np.abs(ref[k]))
+            err = np.max(np.abs(g[k] - ref[k]))
+            assert err <= tol * scale + 1e-300, (i, k, err, scale)
+
+
+@pytest.mark.gpu
+def test_gpu_tmatrix_matches_oracle(oracle_mod):
+    items = [
+        # rain: oblate drops
+        _item(89e9, 1.78 - 0.003j, 1, [0.4e-3, 1.2e-3, 2.0e-3], [1e7, 5e6, 0.0], 1000.0, [0.95, 0.8, 0.6], 0.0),
+        # water sphere, strongly absorbing
+        _item(150e9, 6.5 - 2.8j, 1, [0.6e-3, 1.6e-3], [2e6, 1e6], 1000.0, 1.0, 0.0),
+        # soft ice spheroids (mixed with air), prolate and oblate
+        _item(35e9, 1.78 - 0.0005j, -1, [1e-3, 3e-3, 5e-3], [1e6, 3e5, 1e5], [600.0, 300.0, 150.0],
+              [0.6, 1.5, 0.7], 0.0),
+    ]
+    # items have different bin counts: pad to three bins with empty ones
+    for it in items:
+        while len(it["dmax"]) < 3:
+            for k in ("dmax", "del_d", "density", "as_ratio", "canting"):
+                it[k].append(it[k][-1])
+            it["ndens"].append(0.0)
+    out = _run_gpu(items, 3, 16)
+    refs = [_oracle_item(oracle_mod, it, 16) for it in items]
+    _compare(out, refs, 16)
+    assert int(out["nmax"][0, 2]) == 0  # empty bin skipped
+
+
+@pytest.mark.gpu
+def test_gpu_tmatrix_canted_full_amplitude_path(oracle_mod):
+    items = [_item(89e9, 1.78 - 0.003j, 1, [1.0e-3, 1.8e-3], [1e6, 5e5], 1000.0, [0.8, 0.65], [20.0, 45.0])]
+    out = _run_gpu(items, 2, 16)
+    _compare(out, [_oracle_item(oracle_mod, it, 16) for it in items], 16)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nummu", [8, 32])
+def test_gpu_tmatrix_nummu(oracle_mod, nummu):
+    items = [_item(50e9, 1.78 - 0.001j, -1, [2e-3, 4e-3], [1e6, 2e5], 400.0, 0.6, 0.0)]
+    out = _run_gpu(items, 2, nummu)
+    _compare(out, [_oracle_item(oracle_mod, it, nummu) for it in items], nummu)
+
+
+@pytest.mark.gpu
+def test_gpu_tmatrix_sphere_limit_is_mie(oracle_mod):
+    f, mr, mi, axi = SPHERES[0]
+    it = _item(f, complex(mr, -mi), 1, [2 * axi], [1.0], 1000.0, 1.0, 0.0, del_d=1.0)
+    out = _run_gpu([it], 1, 16)
+    _, _, cext, cback = _mie_cross(oracle_mod, f, mr, mi, axi)
+    ext = out["extinct_matrix"][0].reshape((2, 2, 16), order="F")
+    assert np.allclose(ext[0, 0, :], cext, rtol=5e-7, atol=0)
+    assert abs(out["back_spec"][0, 0] / cback - 1) < 2e-6
+
+
+@pytest.mark.gpu
+def test_gpu_tmatrix_invalid_bins_report_status():
+    from pamtra_b200 import _native
+    items = [_item(89e9, 1.78 - 0.003j, 1, [1e-3, 1e-3], [1e6, 1e6], 1000.0, [0.8, -1.0], 0.0),
+             _item(89e9, 1.78 - 0.003j, 1, [1e-3, 1e-3], [1e6, 1e6], 1000.0, 0.8, 0.0)]
+    out = _run_gpu(items, 2, 16)
+    assert int(out["status"][0]) == (2 | _native.ST_RANGE)
+    assert int(out["status"][1]) == 0
+    assert np.all(np.isfinite(out["scatter_matrix"]))
+
+
+@pytest.mark.gpu
+def test_gpu_tmatrix_device_inputs_match_host(oracle_mod):
+    import torch
+    from pamtra_b200 import tmatrix as ptm
+    items = [_item(89e9, 1.78 - 0.003j, 1, [0.8e-3, 1.5e-3], [2e6, 1e6], 1000.0, [0.9, 0.7], 0.0)]
+    host = _run_gpu(items, 2, 16)
+    dev = torch.device("cuda", 0)
+    t = {k: torch.tensor([it[k] for it in items], dtype=torch.float64, device=dev)
+         for k in ("dmax", "del_d", "ndens", "density", "as_ratio", "canting")}
+    out = ptm.calc_tmatrix_batch(torch.tensor([89e9], device=dev, dtype=torch.float64),
+                                 torch.tensor([1.78 - 0.003j], dtype=torch.complex128, device=dev),
+                                 torch.tensor([1], device=dev),
+                                 t["dmax"], t["del_d"], t["ndens"], t["density"], t["as_ratio"], t["canting"])
+    torch.cuda.synchronize()
+    for k in ("scatter_matrix", "extinct_matrix", "emis_vector", "sback", "back_spec"):
+        assert np.array_equal(out[k].cpu().numpy(), host[k])
