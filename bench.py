@@ -58,6 +58,8 @@ def _args():
     ap.add_argument("--target-cols", type=int, default=1024, help="columns of the 150-layer target batch (0 = skip)")
     ap.add_argument("--uneven-cols", type=int, default=16384, help="columns of the uneven batch (0 = skip)")
     ap.add_argument("--mieheavy-cols", type=int, default=2048, help="columns of the Mie-heavy batch (0 = skip)")
+    ap.add_argument("--tmatrix-items", type=int, default=128,
+                    help="(layer, frequency) items of 32 bins in the T-matrix line (0 = skip)")
     return ap.parse_args()
 
 
@@ -513,6 +515,91 @@ def _serving(args, local):
 
 
 # ---------------------------------------------------------------- reference arm
+def _tmatrix_line(args, eng, dev, cpu_leg):
+    """The T-matrix branch (scat_name 'tmatrix', src/tmatrix.f90:14) on a
+    snow-like batch: soft ice spheroids (300 kg/m3, aspect ratio 0.6) in 32
+    bins of 0.2-4 mm at 89 GHz, NUMMU 16, upright, per (layer, frequency)
+    item; device-resident inputs for ``value``, host arrays through the C-ABI
+    for ``e2e``; canted particles (beta 20 deg, the full amplitude path) on
+    a smaller batch; the oracle (quad-precision restatement, one core) on the
+    first item as the CPU baseline and the parity check."""
+    import torch
+    from pamtra_b200 import tmatrix as ptm
+    ni, nb = args.tmatrix_items, 32
+
+    def arrays(n, beta):
+        d = np.linspace(0.2e-3, 4e-3, nb)[None, :].repeat(n, 0)
+        return dict(dmax=d, del_d=np.full_like(d, 1.2e-4), ndens=np.full_like(d, 1e6),
+                    density=np.full_like(d, 300.0), as_ratio=np.full_like(d, 0.6), canting=np.full_like(d, beta))
+
+    def timed(n, beta, steps):
+        a = arrays(n, beta)
+        t = {k: torch.tensor(v, dtype=torch.float64, device=dev) for k, v in a.items()}
+        fr = torch.full((n,), 89e9, dtype=torch.float64, device=dev)
+        ri = torch.full((n,), 1.78 - 0.002j, dtype=torch.complex128, device=dev)
+        ph = torch.full((n,), -1, dtype=torch.int32, device=dev)
+
+        def run():
+            return ptm.calc_tmatrix_batch(fr, ri, ph, t["dmax"], t["del_d"], t["ndens"], t["density"], t["as_ratio"],
+                                          t["canting"], eng=eng)
+        o = run()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            o = run()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps, o, a
+
+    ms, o, a = timed(ni, 0.0, 3)
+    nm = o["nmax"].cpu().numpy()
+    # e2e: numpy arrays through the host path of the C-ABI (copies in the call)
+    h = arrays(ni, 0.0)
+    fr, ri, ph = np.full(ni, 89e9), np.full(ni, 1.78 - 0.002j), np.full(ni, -1, dtype=np.int32)
+    ptm.calc_tmatrix_batch(fr, ri, ph, h["dmax"], h["del_d"], h["ndens"], h["density"], h["as_ratio"], h["canting"],
+                           eng=eng)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        oh = ptm.calc_tmatrix_batch(fr, ri, ph, h["dmax"], h["del_d"], h["ndens"], h["density"], h["as_ratio"],
+                                    h["canting"], eng=eng)
+    e2e_s = (time.perf_counter() - t0) / 3
+    h2d = sum(v.nbytes for v in h.values()) + fr.nbytes + ri.nbytes + ph.nbytes
+    d2h = sum(oh[k].nbytes for k in ("scatter_matrix", "extinct_matrix", "emis_vector", "sback", "back_spec", "status"))
+    nc = max(1, ni // 16)
+    ms_c, oc, _ = timed(nc, 20.0, 1)
+    line = {"value": ni * nb / (ms * 1e-3), "unit": "bins/s", "ms_per_step": ms,
+            "workload": "%d items x %d bins, soft ice spheroids 300 kg/m3, aspect ratio 0.6, 0.2-4 mm, 89 GHz, "
+                        "NUMMU 16, upright" % (ni, nb),
+            "nmax_range": [int(nm.min()), int(nm.max())], "status_nonzero": int(np.count_nonzero(o["status"].cpu().numpy())),
+            "e2e": {"value": ni * nb / e2e_s, "unit": "bins/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches_per_step": 3,
+            "canted": {"value": nc * nb / (ms_c * 1e-3), "unit": "bins/s", "items": nc, "beta_deg": 20.0,
+                       "form": "full AMPL per (incident angle, scattered angle, azimuth)"},
+            "bound": "latency: one FP64 CTA chain per bin (solves of order 2 (NMAX - m + 1) with a CTA barrier "
+                     "per pivot, then the angular sums); no tensor-core or HBM bound applies"}
+    if cpu_leg:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        t0 = time.perf_counter()
+        r = oracle.tmatrix_species(16, 89e9, 1.78, -0.002, -1, *[a[k][0] for k in ("dmax", "del_d", "ndens", "density",
+                                                                                  "as_ratio", "canting")])
+        cpu_s = time.perf_counter() - t0
+        err = 0.0
+        g = {"scatter_matrix": o["scatter_matrix"][0].cpu().numpy().reshape((2, 16, 2, 16, 2), order="F"),
+             "extinct_matrix": o["extinct_matrix"][0].cpu().numpy().reshape((2, 2, 16), order="F"),
+             "emis_vector": o["emis_vector"][0].cpu().numpy().reshape((2, 16), order="F"),
+             "back_spec": o["back_spec"][0].cpu().numpy()}
+        for k, v in g.items():
+            err = max(err, float(np.max(np.abs(v - r[k])) / np.max(np.abs(r[k]))))
+        line["cpu_baseline"] = {"value": nb / cpu_s, "unit": "bins/s", "cores": 1, "kind": "port",
+                                "sample": "the first item's %d bins, quad-precision T-matrix solve like the "
+                                          "reference's REAL*16 tmatrix_amplq" % nb}
+        line["max_rel_err_vs_oracle"] = err
+    return line
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -710,6 +797,7 @@ def main():
                             wl.mie_heavy_batch(args.mieheavy_cols, seed=6), local, eng, stream, pool) \
         if args.mieheavy_cols > 0 else None
     serving = _serving(args, local) if args.serve_requests > 0 else None
+    tmat = _tmatrix_line(args, eng, dev, not args.no_cpu) if args.tmatrix_items > 0 else None
     # ---- roofline of the dominant kernel (doubling stage)
     peak = fp64_peak_tflops(dev)
     t_layer = stage_tot.get("layer", 0.0) / args.steps * 1e-3
@@ -789,6 +877,7 @@ def main():
         "target_shape": target,
         "uneven": uneven,
         "mie_heavy": mieheavy,
+        "tmatrix": tmat,
         "status_nonzero": int(np.count_nonzero(status)),
     }
 
@@ -820,6 +909,9 @@ def main():
                                               g(serving, "batched_3xtf32", "rate_200", "p99_ms")],
         "serving_3xtf32_halfcap_p50_p99_ms": [g(serving, "batched_3xtf32", "rate_half_capacity", "p50_ms"),
                                               g(serving, "batched_3xtf32", "rate_half_capacity", "p99_ms")],
+        "tmatrix_bins_per_s": {"gpu": g(tmat, "value"), "e2e": g(tmat, "e2e", "value"),
+                               "cpu_1core": g(tmat, "cpu_baseline", "value"),
+                               "max_rel_err_vs_oracle": g(tmat, "max_rel_err_vs_oracle")},
         "serving_solves_per_s": {"3xtf32": g(serving, "batched_3xtf32", "rate_200", "solves_per_s"),
                                  "fp64": g(serving, "batched_fp64", "rate_200", "solves_per_s"),
                                  "plain": g(serving, "plain_fp64", "rate_200", "solves_per_s")},

@@ -273,8 +273,8 @@ int32_t pamtra_b200_last_launch_count(const pamtra_b200_ctx* ctx);
 int32_t pamtra_b200_set_timing(pamtra_b200_ctx* ctx, int32_t enable);
 int32_t pamtra_b200_stage_ms(pamtra_b200_ctx* ctx, float* ms, int32_t n);
 
-/* sizeof of the ABI structs, in order settings, species, columns, outputs
- * (for bindings to check their struct layouts). */
+/* sizeof of the ABI structs, in order settings, species, columns, outputs,
+ * tmatrix_in, tmatrix_out (for bindings to check their struct layouts). */
 int32_t pamtra_b200_abi_sizes(size_t* out, int32_t n);
 
 /* ---- single-stage entry points (parity tests of individual routines) ---- */

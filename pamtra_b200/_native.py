@@ -62,7 +62,7 @@ EXPORTS = ["pamtra_b200_create", "pamtra_b200_destroy", "pamtra_b200_workspace_b
            "pamtra_b200_mmult_3xtf32_batched", "pamtra_b200_set_launch", "pamtra_b200_get_launch",
            "pamtra_b200_graph_capture", "pamtra_b200_graph_launch", "pamtra_b200_graph_destroy",
            "pamtra_b200_get_eps_water", "pamtra_b200_gas_l93", "pamtra_b200_set_wait_limit",
-           "pamtra_b200_layer_products"]
+           "pamtra_b200_layer_products", "pamtra_b200_tmatrix"]
 NLAUNCH = 5  # PAMTRA_B200_NLAUNCH: mie warps per CTA, mie / layer / adding CTAs per SM, mie bins per item
 STAGES = ["prep", "psd", "mie", "layer", "adding"]
 
@@ -315,9 +315,10 @@ def workspace_bytes(columns, species=None, precision=PREC_FP64):
 
 
 def abi_sizes():
-    """(settings, species, columns, outputs) struct sizes as compiled."""
-    buf = (ctypes.c_size_t * 4)()
-    load().pamtra_b200_abi_sizes(buf, 4)
+    """(settings, species, columns, outputs, tmatrix_in, tmatrix_out) struct
+    sizes as compiled."""
+    buf = (ctypes.c_size_t * 6)()
+    load().pamtra_b200_abi_sizes(buf, 6)
     return tuple(int(v) for v in buf)
 
 

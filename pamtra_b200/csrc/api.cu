@@ -692,9 +692,9 @@ int32_t pamtra_b200_graph_destroy(pamtra_b200_graph* g) {
 int32_t pamtra_b200_last_launch_count(const pamtra_b200_ctx* ctx) { return ctx ? ctx->last_launches : 0; }
 
 int32_t pamtra_b200_abi_sizes(size_t* out, int32_t n) {
-  const size_t sz[4] = {sizeof(pamtra_b200_settings), sizeof(pamtra_b200_species), sizeof(pamtra_b200_columns),
-                        sizeof(pamtra_b200_outputs)};
-  for (int i = 0; i < n && i < 4; i++) out[i] = sz[i];
+  const size_t sz[6] = {sizeof(pamtra_b200_settings), sizeof(pamtra_b200_species), sizeof(pamtra_b200_columns),
+                        sizeof(pamtra_b200_outputs), sizeof(pamtra_b200_tmatrix_in), sizeof(pamtra_b200_tmatrix_out)};
+  for (int i = 0; i < n && i < 6; i++) out[i] = sz[i];
   return PAMTRA_B200_OK;
 }
 
@@ -1223,8 +1223,8 @@ int32_t pamtra_b200_tmatrix(pamtra_b200_ctx* ctx, const pamtra_b200_tmatrix_in* 
   cudaStream_t stream = (cudaStream_t)stream_;
   const size_t n = (size_t)ni * nb;
   const size_t NS = (size_t)2 * nummu * 2 * nummu * 2, NE = 4 * (size_t)nummu, NM = 2 * (size_t)nummu;
-  // one 256-thread CTA per SM (254 registers per thread)
-  const int grid = (int)std::min<size_t>(n, (size_t)ctx->sm_count);
+  // two 256-thread CTAs per SM (128 registers per thread), persistent
+  const int grid = (int)std::min<size_t>(n, (size_t)2 * ctx->sm_count);
   // device layout (8-byte units, each array 256-byte aligned)
   size_t off = 0;
   auto take = [&](size_t elems8) { const size_t o = off; off += (elems8 + 31) / 32 * 32; return o; };

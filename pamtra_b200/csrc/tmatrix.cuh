@@ -49,7 +49,9 @@ constexpr size_t TMO_AUG = TMO_D + 2 * (size_t)TM_NG * TM_NMAX;   // [TM_N2][2 T
 constexpr size_t TMO_P = TMO_AUG + 2 * (size_t)TM_N2 * 2 * TM_N2; // [TM_NMAX+1][TM_NA][4] complex
 constexpr size_t TMO_DVA = TMO_P + 2 * (size_t)(TM_NMAX + 1) * TM_NA * 4;  // [TM_NA][2][TM_NMAX]
 constexpr size_t TMO_Z = TMO_DVA + (size_t)TM_NA * 2 * TM_NMAX;   // [TM_NA][TM_NAZ][4]
-constexpr size_t TMO_T = TMO_Z + (size_t)TM_NA * TM_NAZ * 4;      // float2 [TM_NMAX+1][4][TM_NMAX][TM_NMAX]
+constexpr size_t TM_DIRD = 7;                                     // doubles of one direction record
+constexpr size_t TMO_G = TMO_Z + (size_t)TM_NA * TM_NAZ * 4;      // incident [32], scattered [TM_NA][TM_NAZ]
+constexpr size_t TMO_T = TMO_G + (32 + (size_t)TM_NA * TM_NAZ) * TM_DIRD;  // float2 [TM_NMAX+1][4][TM_NMAX][TM_NMAX]
 constexpr size_t TM_T_FLOAT2 = (size_t)(TM_NMAX + 1) * 4 * TM_NMAX * TM_NMAX;
 constexpr size_t TM_SLOT_DOUBLES = TMO_T + TM_T_FLOAT2;          // a float2 is one double wide
 
@@ -322,7 +324,7 @@ __device__ bool tm_setup(double* s, TmShared& sh, int nmax, int ngauss, double l
 // holds column j of T.  Whole CTA; returns the order of the system (2 nm),
 // or 0 when a pivot vanishes.
 __device__ int tm_solve(double* s, TmShared& sh, int m, int nmax, int ngauss, double ppi, double pir, double pii) {
-  const int t = threadIdx.x, ng = 2 * ngauss;
+  const int t = threadIdx.x;
   const int mm1 = (m == 0) ? 1 : m, nm = nmax - mm1 + 1, n2m = 2 * nm, ldw = 2 * n2m;
   const double* X = tm_node(s, 0);
   double *D1 = tm_d(s, 0), *D2 = tm_d(s, 1);
@@ -528,26 +530,25 @@ __device__ __forceinline__ void tm_vigampl(double x, int nmax, int m, F&& put) {
   }
 }
 
-// Geometry of AMPL (tmatrix_amplq.lp.f:618-795): the particle-frame polar
-// cosines of the incident (ctp) and scattered (ctp1) directions, their
-// azimuth difference and the polarisation rotations R and R1^-1, for angles
-// in degrees with the reference's 1e-8 offsets away from the singular values.
-struct TmGeom {
-  double ctp, ctp1, ph, R[2][2], R1[2][2];
+// Geometry of AMPL (tmatrix_amplq.lp.f:618-795) for one direction (polar tl,
+// azimuth pl in degrees, with the reference's 1e-8 offsets away from the
+// singular values): the particle-frame polar cosine, the particle-frame
+// azimuth and the lab -> particle polarisation rotation, inverted for the
+// scattered direction.  The incident and the scattered direction go through
+// the same steps in the reference, so a table of each (per incident angle,
+// per scattered angle and azimuth) gives the values of every AMPL call.
+struct TmDir {
+  double ctp, phip, M[2][2];
 };
-__device__ void tm_geom(double tl, double tl1, double pl, double pl1, double alpha, double beta, TmGeom& g) {
+__device__ void tm_dir(double tl, double pl, double alpha, double beta, bool invert, TmDir& d) {
   const double pin = 3.141592653589793, pin2 = pin * 0.5, pi = pin / 180.0;
   const double alph = alpha * pi;
-  double bet = beta * pi, thetl = tl * pi, phil = pl * pi, thetl1 = tl1 * pi, phil1 = pl1 * pi;
+  double bet = beta * pi, thetl = tl * pi, phil = pl * pi;
   const double eps = 1e-8;
   if (thetl < pin2) thetl = thetl + eps;
   if (thetl > pin2) thetl = thetl - eps;
-  if (thetl1 < pin2) thetl1 = thetl1 + eps;
-  if (thetl1 > pin2) thetl1 = thetl1 - eps;
   if (phil < pin) phil = phil + eps;
   if (phil > pin) phil = phil - eps;
-  if (phil1 < pin) phil1 = phil1 + eps;
-  if (phil1 > pin) phil1 = phil1 - eps;
   if (bet <= pin2 && pin2 - bet <= eps) bet = bet - eps;
   if (bet > pin2 && bet - pin2 <= eps) bet = bet + eps;
   const double cb = cos(bet), sb = sin(bet);
@@ -558,32 +559,17 @@ __device__ void tm_geom(double tl, double tl1, double pl, double pl1, double alp
   if (phip > 0.0 && sp < 0.0) phip = phip + pin;
   if (phip < 0.0 && sp > 0.0) phip = phip + pin;
   if (phip < 0.0) phip = phip + 2.0 * pin;
-  double ct1 = cos(thetl1), st1 = sin(thetl1), cp1 = cos(phil1 - alph), sp1 = sin(phil1 - alph);
-  const double ctp1 = ct1 * cb + st1 * sb * cp1, thetp1 = acos(ctp1);
-  const double cpp1 = cb * st1 * cp1 - sb * ct1, spp1 = st1 * sp1;
-  double phip1 = atan(spp1 / cpp1);
-  if (phip1 > 0.0 && sp1 < 0.0) phip1 = phip1 + pin;
-  if (phip1 < 0.0 && sp1 > 0.0) phip1 = phip1 + pin;
-  if (phip1 < 0.0) phip1 = phip1 + 2.0 * pin;
   const double ca = cos(alph), sa = sin(alph);
   const double B[3][3] = {{ca * cb, sa * cb, -sb}, {-sa, ca, 0.0}, {ca * sb, sa * sb, cb}};
   cp = cos(phil);
   sp = sin(phil);
-  cp1 = cos(phil1);
-  sp1 = sin(phil1);
   const double AL[3][2] = {{ct * cp, -sp}, {ct * sp, cp}, {-st, 0.0}};
-  const double AL1[3][2] = {{ct1 * cp1, -sp1}, {ct1 * sp1, cp1}, {-st1, 0.0}};
   ct = ctp;
   st = sin(thetp);
   cp = cos(phip);
   sp = sin(phip);
-  ct1 = ctp1;
-  st1 = sin(thetp1);
-  cp1 = cos(phip1);
-  sp1 = sin(phip1);
   const double AP[2][3] = {{ct * cp, ct * sp, -st}, {-sp, cp, 0.0}};
-  const double AP1[2][3] = {{ct1 * cp1, ct1 * sp1, -st1}, {-sp1, cp1, 0.0}};
-  double C[3][2];
+  double C[3][2], R[2][2];
 #pragma unroll
   for (int i = 0; i < 3; i++)
 #pragma unroll
@@ -600,35 +586,38 @@ __device__ void tm_geom(double tl, double tl1, double pl, double pl1, double alp
       double x = 0.0;
 #pragma unroll
       for (int k = 0; k < 3; k++) x = x + AP[i][k] * C[k][j];
-      g.R[i][j] = x;
+      R[i][j] = x;
     }
-#pragma unroll
-  for (int i = 0; i < 3; i++)
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-      double x = 0.0;
-#pragma unroll
-      for (int k = 0; k < 3; k++) x = x + B[i][k] * AL1[k][j];
-      C[i][j] = x;
-    }
-  double R1[2][2];
+  if (invert) {
+    const double dd = 1.0 / (R[0][0] * R[1][1] - R[0][1] * R[1][0]);
+    d.M[0][0] = R[1][1] * dd;
+    d.M[0][1] = -R[0][1] * dd;
+    d.M[1][0] = -R[1][0] * dd;
+    d.M[1][1] = R[0][0] * dd;
+  } else {
+    d.M[0][0] = R[0][0];
+    d.M[0][1] = R[0][1];
+    d.M[1][0] = R[1][0];
+    d.M[1][1] = R[1][1];
+  }
+  d.ctp = ctp;
+  d.phip = phip;
+}
+
+struct TmGeom {
+  double ctp, ctp1, ph, R[2][2], R1[2][2];
+};
+__device__ __forceinline__ void tm_geom_of(const TmDir& in, const TmDir& sc, TmGeom& g) {
+  g.ctp = in.ctp;
+  g.ctp1 = sc.ctp;
+  g.ph = sc.phip - in.phip;
 #pragma unroll
   for (int i = 0; i < 2; i++)
 #pragma unroll
     for (int j = 0; j < 2; j++) {
-      double x = 0.0;
-#pragma unroll
-      for (int k = 0; k < 3; k++) x = x + AP1[i][k] * C[k][j];
-      R1[i][j] = x;
+      g.R[i][j] = in.M[i][j];
+      g.R1[i][j] = sc.M[i][j];
     }
-  const double d = 1.0 / (R1[0][0] * R1[1][1] - R1[0][1] * R1[1][0]);
-  g.R1[0][0] = R1[1][1] * d;
-  g.R1[0][1] = -R1[0][1] * d;
-  g.R1[1][0] = -R1[1][0] * d;
-  g.R1[1][1] = R1[0][0] * d;
-  g.ctp = ctp;
-  g.ctp1 = ctp1;
-  g.ph = phip1 - phip;
 }
 
 // The particle-frame amplitudes (VV, VH, HV, HH) / k rotated to the lab
@@ -813,6 +802,8 @@ __device__ void tm_particle(const TmArgs& A, double* s, TmShared& sh, int p) {
   double* Zb = s + TMO_Z;
   cplx* P = reinterpret_cast<cplx*>(s + TMO_P);
   double* DVA = s + TMO_DVA;
+  TmDir* Gin = reinterpret_cast<TmDir*>(s + TMO_G);
+  TmDir* Gsc = Gin + 32;
   if (t < na) {
     const int kk = t / nummu, ll = t % nummu;
     double th = acos(A.mu[ll] * (kk == 0 ? 1.0 : -1.0)) * 180.0 / PI;
@@ -820,16 +811,28 @@ __device__ void tm_particle(const TmArgs& A, double* s, TmShared& sh, int p) {
     sh.thet[t] = th;
   }
   __syncthreads();
+  // direction tables: incident (phi0 = 0) per Lobatto angle, scattered per (angle, azimuth)
+  for (int e = t; e < nummu + na * TM_NAZ; e += TM_THREADS) {
+    if (e < nummu) {
+      double th0 = acos(A.mu[e] * 1.0) * 180.0 / PI;
+      if (th0 > 179.9999) th0 = 180.0;
+      tm_dir(th0, 0.0, 0.0, beta, false, Gin[e]);
+    } else {
+      const int a = (e - nummu) / TM_NAZ, k = (e - nummu) % TM_NAZ;
+      const double phi = 360.0 / (double)TM_NAZ * ((double)(k + 1) - 1.0);
+      tm_dir(sh.thet[a], phi, 0.0, beta, true, Gsc[(size_t)a * TM_NAZ + k]);
+    }
+  }
+  __syncthreads();
   for (int jj = 0; jj < nummu; jj++) {
     double thet0 = acos(A.mu[jj] * 1.0) * 180.0 / PI;
     if (thet0 > 179.9999) thet0 = 180.0;
     if (upright) {
       // polar parts per order m: P_m(a) for the four amplitudes
+      // upright: the scattered polar cosine does not depend on the azimuth
       if (t < na) {
-        TmGeom g;
-        tm_geom(thet0, sh.thet[t], 0.0, 0.0, 0.0, beta, g);
-        sh.cth[t] = g.ctp1;
-        if (t == 0) sh.accs[2] = g.ctp;
+        sh.cth[t] = Gsc[(size_t)t * TM_NAZ].ctp;
+        if (t == 0) sh.accs[2] = Gin[jj].ctp;
       }
       __syncthreads();
       const double cth0 = sh.accs[2];
@@ -900,16 +903,22 @@ __device__ void tm_particle(const TmArgs& A, double* s, TmShared& sh, int p) {
     // amplitudes per (scattered angle, azimuth) and their quadratic forms
     for (int e = t; e < na * TM_NAZ; e += TM_THREADS) {
       const int a = e / TM_NAZ, k = e % TM_NAZ;
-      const double phi = 360.0 / (double)TM_NAZ * ((double)(k + 1) - 1.0);
       TmGeom g;
-      tm_geom(thet0, sh.thet[a], 0.0, phi, 0.0, beta, g);
+      tm_geom_of(Gin[jj], Gsc[(size_t)a * TM_NAZ + k], g);
       cplx vv, vh, hv, hh;
       if (upright) {
         vv = P[((size_t)0 * TM_NA + a) * 4 + 0];
         hh = P[((size_t)0 * TM_NA + a) * 4 + 3];
         vh = hv = cmk(0.0, 0.0);
+        // cos(m ph), sin(m ph) by the angle-addition recurrence
+        double s1, c1;
+        sincos(g.ph, &s1, &c1);
+        double cm = 1.0, sm = 0.0;
         for (int m = 1; m <= nmax; m++) {
-          const double fc = 2.0 * cos(m * g.ph), fs = 2.0 * sin(m * g.ph);
+          const double cn = cm * c1 - sm * s1;
+          sm = sm * c1 + cm * s1;
+          cm = cn;
+          const double fc = 2.0 * cm, fs = 2.0 * sm;
           const cplx* pm = P + ((size_t)m * TM_NA + a) * 4;
           vv = cadd(vv, cscale(pm[0], fc));
           vh = cadd(vh, cscale(pm[1], fs));
@@ -983,7 +992,7 @@ __device__ void tm_particle(const TmArgs& A, double* s, TmShared& sh, int p) {
 }
 
 // Persistent CTAs over the particles of a launch, one scratch slot each.
-__global__ void __launch_bounds__(TM_THREADS, 1) k_tmatrix(TmArgs A) {
+__global__ void __launch_bounds__(TM_THREADS, 2) k_tmatrix(TmArgs A) {
   __shared__ TmShared sh;
   double* s = A.scratch + (size_t)blockIdx.x * TM_SLOT_DOUBLES;
   const int np = A.n_items * A.nbins;

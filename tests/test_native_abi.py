@@ -26,7 +26,8 @@ def test_struct_layouts(native):
     from pamtra_b200 import packing
     sizes = native.abi_sizes()
     assert sizes == (ctypes.sizeof(packing.Settings), ctypes.sizeof(packing.Species),
-                     ctypes.sizeof(native.Columns), ctypes.sizeof(native.Outputs))
+                     ctypes.sizeof(native.Columns), ctypes.sizeof(native.Outputs),
+                     ctypes.sizeof(native.TmatrixIn), ctypes.sizeof(native.TmatrixOut))
 
 
 def test_no_device_fails_loudly(native):
