@@ -192,3 +192,39 @@ def test_gpu_tmatrix_device_inputs_match_host(oracle_mod):
     torch.cuda.synchronize()
     for k in ("scatter_matrix", "extinct_matrix", "emis_vector", "sback", "back_spec"):
         assert np.array_equal(out[k].cpu().numpy(), host[k])
+
+
+def test_oracle_nonabsorbing_spheroid_conserves_energy(oracle_mod):
+    """mri = 0: extinction equals the scattering integrated over the sphere,
+    so the emission vector vanishes up to the quadrature and the
+    single-precision T."""
+    r = oracle_mod.tmatrix_single(16, 89e9, 1.78, 0.0, 0.8e-3, 0.6)
+    assert np.max(np.abs(r["emis_vector"][0])) < 5e-6 * np.max(r["extinct_matrix"][0, 0])
+
+
+def test_oracle_upside_down_spheroid_is_the_same_particle(oracle_mod):
+    """Canting 180 deg turns the spheroid over: the same particle, reached
+    through the rotated geometry of AMPL."""
+    r1 = oracle_mod.tmatrix_single(16, 89e9, 1.78, 0.003, 0.8e-3, 0.6, beta=0.0)
+    r2 = oracle_mod.tmatrix_single(16, 89e9, 1.78, 0.003, 0.8e-3, 0.6, beta=180.0)
+    for k in ("scatter_matrix", "extinct_matrix", "emis_vector", "sback"):
+        assert np.max(np.abs(r1[k] - r2[k])) <= 1e-12 * np.max(np.abs(r1[k])), k
+
+
+def test_oracle_reciprocity_of_the_azimuth_averaged_phase_function(oracle_mod):
+    """Z11 averaged over azimuth is symmetric in the incident and scattered
+    polar angles (reciprocity), to the single-precision T."""
+    S = oracle_mod.tmatrix_single(16, 89e9, 1.78, 0.003, 0.8e-3, 0.6)["scatter_matrix"]
+    for kk in (0, 1):
+        z = S[0, :, 0, :, kk]
+        assert np.max(np.abs(z - z.T)) <= 1e-5 * np.max(np.abs(z))
+
+
+@pytest.mark.gpu
+def test_gpu_upright_and_overturned_paths_agree():
+    """Canting 0 takes the separable amplitude sums, canting 180 the full AMPL
+    evaluation per azimuth; both describe the same particle."""
+    a = _run_gpu([_item(89e9, 1.78 - 0.003j, 1, [0.8e-3, 1.6e-3], [2e6, 1e6], 1000.0, 0.6, 0.0)], 2, 16)
+    b = _run_gpu([_item(89e9, 1.78 - 0.003j, 1, [0.8e-3, 1.6e-3], [2e6, 1e6], 1000.0, 0.6, 180.0)], 2, 16)
+    for k in ("scatter_matrix", "extinct_matrix", "emis_vector", "sback", "back_spec"):
+        assert np.max(np.abs(a[k] - b[k])) <= 5e-6 * np.max(np.abs(a[k])), k
