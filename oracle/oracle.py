@@ -76,6 +76,8 @@ def lib():
                                      ctypes.POINTER(OrcDebug)]
         l.orc_run_column_fs.restype = ctypes.c_int
         l.orc_run_column_fs.argtypes = l.orc_run_column.argtypes + [ctypes.POINTER(OrcFullspec)]
+        l.orc_run_column_tm.restype = ctypes.c_int
+        l.orc_run_column_tm.argtypes = l.orc_run_column_fs.argtypes + [ctypes.c_void_p, dp]
         l.orc_gas_r98.restype = ctypes.c_int
         l.orc_gas_r98.argtypes = [ctypes.c_double] * 4 + [dp]
         l.orc_get_eps_water.restype = ctypes.c_int
@@ -114,11 +116,14 @@ def settings(pk_settings):
     return s
 
 
-def run_column(st, species, cols, c, freqs, debug=False, psd_nbin=0):
+def run_column(st, species, cols, c, freqs, debug=False, psd_nbin=0, scat_code=None, canting=None):
     """Run column ``c`` of packed ``cols`` (pamtra_b200.packing.profile_columns).
     ``debug`` True returns all intermediates, "radar" only the simple-radar
     outputs (back, ze, att_hydro, att_atmo; filled when ``st.active``).
-    ``psd_nbin`` > 0 adds the save_psd bins, [L][nhydro][psd_nbin]."""
+    ``psd_nbin`` > 0 adds the save_psd bins, [L][nhydro][psd_nbin].
+    ``scat_code`` (per species, 1 = T-matrix spheroid of the species' aspect
+    ratio, 0 = Mie sphere) and ``canting`` (deg, per species) select the
+    scattering model of scatProperties.f90:289-367 (moment-based bins only)."""
     l = lib()
     L = int(cols["nlyrs"][c])
     Lmax = int(cols["max_nlyrs"])
@@ -172,6 +177,10 @@ def run_column(st, species, cols, c, freqs, debug=False, psd_nbin=0):
         fs = OrcFullspec(int(cols["fs_nbin"]), *[fsa[k].ctypes.data for k in
                                                   ("fs_d", "fs_d_bound", "fs_n", "fs_rho", "fs_mass")])
         err = l.orc_run_column_fs(*(args + [ctypes.byref(fs)]))
+    elif scat_code is not None:
+        sc = np.ascontiguousarray(np.asarray(scat_code, dtype=np.int32))
+        ct = f64(canting if canting is not None else np.zeros(H))
+        err = l.orc_run_column_tm(*(args + [None, sc.ctypes.data, _p(ct)]))
     else:
         err = l.orc_run_column(*args)
     return err, tb, em, ang, out_dbg

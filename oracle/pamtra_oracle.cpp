@@ -1402,9 +1402,11 @@ struct Layer {  // R,T (n x n, two parts each), S (n, two parts)
 // src/radintg4.f90:1-45 INITIALIZE4 + 51-73 INITIAL_SOURCE4 + 174-309 DOUBLING_INTEGRATION4
 void scattering_layer(int N, const std::vector<double>& mu, const std::vector<double>& w, double zdiff, double gas,
                       double planck0, double planck1, const std::vector<double>& scat, double ext_k, double emis_k,
-                      Layer& out, int& num_doubles) {
+                      Layer& out, int& num_doubles, const double* tm_ext = nullptr, const double* tm_emis = nullptr) {
   const int n = 2 * N;
-  double extinct = ext_k + gas;
+  // extinct_matrix(1) + gas (src/radtran4.f90:323); with T-matrix species the
+  // layer's matrices are theirs plus scatcnv's
+  double extinct = (tm_ext ? tm_ext[0] + ext_k : ext_k) + gas;
   double f = std::log(std::max(extinct * zdiff, 1.0e-7) / 1.0e-6) / (double)std::log(2.0f);
   num_doubles = 0;
   if (f > 0.0) num_doubles = (int)f + 1;
@@ -1417,6 +1419,7 @@ void scattering_layer(int N, const std::vector<double>& mu, const std::vector<do
       double e = (i == 0) ? gas : 0.0;
       double tmp = planck0 * delta_z / mu[j];
       double ev = (i == 0) ? emis_k : 0.0;
+      if (tm_emis) ev = tm_emis[i + 2 * j] + ((i == 0) ? emis_k : 0.0);
       lin[i + 2 * j] = tmp * (ev + e);
       lin[n + i + 2 * j] = tmp * (ev + e);
     }
@@ -1441,9 +1444,12 @@ void scattering_layer(int N, const std::vector<double>& mu, const std::vector<do
           R[n * n + mi] = C * tmp * w[j1] * Q3[qi];
           double diag = (i1 == i2 && j1 == j2) ? 1.0 : 0.0;
           double ex = 0.0;
-          if (j1 == j2) ex = ((i1 == i2) ? ext_k : 0.0) + gext;
+          // EXTINCT_MATRIX(I2, I1, J2, L) + GEXT
+          const double em = tm_ext ? tm_ext[i2 + 2 * (i1 + 2 * j2)] + ((i1 == i2) ? ext_k : 0.0)
+                                   : ((i1 == i2) ? ext_k : 0.0);
+          if (j1 == j2) ex = em + gext;
           T[mi] = diag - tmp * (ex - C * w[j1] * Q1[qi]);
-          if (j1 == j2) ex = ((i1 == i2) ? ext_k : 0.0) + gext;
+          if (j1 == j2) ex = em + gext;
           T[n * n + mi] = diag - tmp * (ex - C * w[j1] * Q4[qi]);
         }
       }
@@ -1663,6 +1669,12 @@ double rad_to_tb(double rad, double wl) {
 // ======================================================================
 extern "C" {
 
+// calc_tmatrix of one species at one frequency (tmatrix_oracle.cpp)
+int orc_tmatrix_species(int nummu, double frequency, double ref_re, double ref_im, int phase, int nbins,
+                        const double* dmax, const double* del_d, const double* ndens, const double* density,
+                        const double* as_ratio, const double* canting, double* scat, double* ext, double* emis,
+                        double* back_spec, double* sback);
+
 int orc_gas_r98(double f, double T, double rhowv, double pres, double* kext) {
   return gas_r98(f, T, rhowv, pres, kext);
 }
@@ -1752,6 +1764,14 @@ int orc_run_column(const orc_settings* st, const orc_species* sp, int nhydro, in
                            tb, emissivity_out, angles_deg, dbg, nullptr);
 }
 
+int orc_run_column_tm(const orc_settings* st, const orc_species* sp, int nhydro, int L, const double* hgt_lev,
+                      const double* temp_lev, const double* press_lev, const double* relhum_lev, const double* hgt,
+                      const double* temp, const double* press, const double* relhum, const double* hydro_q,
+                      const double* hydro_n, const double* hydro_reff, double groundtemp, int noutlevels,
+                      const double* obs_height, char sfc_refl, int nfreq, const double* freqs, double* tb,
+                      double* emissivity_out, double* angles_deg, orc_debug* dbg, const orc_fullspec* fs,
+                      const int* scat_code, const double* canting);
+
 // As orc_run_column; with `fs` the size distributions come from the given
 // full spectra instead of hydro_q / hydro_n / hydro_reff.
 int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro, int L, const double* hgt_lev,
@@ -1760,7 +1780,33 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
                       const double* hydro_n, const double* hydro_reff, double groundtemp, int noutlevels,
                       const double* obs_height, char sfc_refl, int nfreq, const double* freqs, double* tb,
                       double* emissivity_out, double* angles_deg, orc_debug* dbg, const orc_fullspec* fs) {
+  return orc_run_column_tm(st, sp, nhydro, L, hgt_lev, temp_lev, press_lev, relhum_lev, hgt, temp, press, relhum,
+                           hydro_q, hydro_n, hydro_reff, groundtemp, noutlevels, obs_height, sfc_refl, nfreq, freqs,
+                           tb, emissivity_out, angles_deg, dbg, fs, nullptr, nullptr);
+}
+
+// As orc_run_column_fs, with species whose scat_code[h] is 1 scattering as
+// T-matrix spheroids (scat_name 'tmatrix', src/scatProperties.f90:289-367) of
+// the species' aspect ratio and canting[h] (deg).  Their scattering matrix,
+// extinction matrix and emission vector are added to the layer's after
+// scatcnv (src/hydrometeor_extinction.f90:329-339); their extinction at the
+// 16th quadrature angle joins kexttot (src/scatProperties.f90:367, :921).
+// The reference leaves salb_hydro unset for them (:929-934); here it is 0,
+// which only matters for layers that also hold Mie species.
+int orc_run_column_tm(const orc_settings* st, const orc_species* sp, int nhydro, int L, const double* hgt_lev,
+                      const double* temp_lev, const double* press_lev, const double* relhum_lev, const double* hgt,
+                      const double* temp, const double* press, const double* relhum, const double* hydro_q,
+                      const double* hydro_n, const double* hydro_reff, double groundtemp, int noutlevels,
+                      const double* obs_height, char sfc_refl, int nfreq, const double* freqs, double* tb,
+                      double* emissivity_out, double* angles_deg, orc_debug* dbg, const orc_fullspec* fs,
+                      const int* scat_code, const double* canting) {
   const int N = st->nummu, n = 2 * N;
+  if (scat_code && fs)
+    for (int h = 0; h < nhydro; h++)
+      if (scat_code[h] == 1) return 2;  // per-bin aspect ratios of full spectra: not restated
+  if (scat_code && N < 16)
+    for (int h = 0; h < nhydro; h++)
+      if (scat_code[h] == 1) return 2;  // kext_hydro reads extinct_matrix(1,1,16,1)
   Atmo a;
   a.L = L;
   a.hgt_lev.assign(hgt_lev, hgt_lev + L + 1);
@@ -1823,6 +1869,9 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
     // hydrometeors (src/hydrometeor_extinction.f90)
     std::vector<std::vector<double>> scat(L);
     std::vector<double> extk(L, 0.0), emk(L, 0.0), kext_h(L, 0.0), back_h(L, 0.0);
+    // T-matrix species of each layer: scattering matrix (4 quadrants as scat),
+    // extinction matrix extinct_matrix(i2, i1, j) [2][2][N], emission vector [2][N]
+    std::vector<std::vector<double>> tm_scat(L), tm_ext(L), tm_emis(L);
     for (int z = 0; z < L; z++) {
       double kexttot = 0.0, salbedo = 0.0, backtot = 0.0;
       double legen_coef[3][MAXNLEG];
@@ -1915,6 +1964,45 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
         } else {
           ref_ice(a.temp[z], freq, refre, refim);
         }
+        if (scat_code && scat_code[h] == 1) {
+          // calc_tmatrix (src/scatProperties.f90:289-306): every bin with the
+          // species' aspect ratio and canting (negative or NaN read as 0, :284-287)
+          const int nb = bn.nbin;
+          double asr = s.as_ratio, cant = canting ? canting[h] : 0.0;
+          if (asr < 0 || std::isnan(asr)) asr = 0.0;
+          if (cant < 0 || std::isnan(cant)) cant = 0.0;
+          std::vector<double> asl(nb, asr), cl(nb, cant), bk(nb), ts((size_t)8 * N * N), te(4 * N), tv(2 * N), sb(4);
+          if (orc_tmatrix_species(N, freq * 1e9, refre, -refim, s.liq_ice, nb, bn.diam.data(), bn.delta_d.data(),
+                                  ndens.data(), bn.dens.data(), asl.data(), cl.data(), ts.data(), te.data(),
+                                  tv.data(), bk.data(), sb.data()))
+            return 2;
+          if (tm_scat[z].empty()) {
+            tm_scat[z].assign((size_t)4 * n * n, 0.0);
+            tm_ext[z].assign(4 * N, 0.0);
+            tm_emis[z].assign(2 * N, 0.0);
+          }
+          // scatter_matrix(i2, ll, i1, jj, kk) -> quadrant L = kk and L = 5 - kk
+          // (src/scatProperties.f90:316-317), rows (i2, ll), columns (i1, jj)
+          for (int kk = 0; kk < 2; kk++)
+            for (int jj = 0; jj < N; jj++)
+              for (int i1 = 0; i1 < 2; i1++)
+                for (int ll = 0; ll < N; ll++)
+                  for (int i2 = 0; i2 < 2; i2++) {
+                    const double v = ts[i2 + 2 * (ll + N * (i1 + 2 * (jj + N * kk)))];
+                    const size_t qi = (size_t)(i2 + 2 * ll) * n + (i1 + 2 * jj);
+                    tm_scat[z][(size_t)kk * n * n + qi] += v;
+                    tm_scat[z][(size_t)(3 - kk) * n * n + qi] += v;
+                  }
+          for (int e = 0; e < 4 * N; e++) tm_ext[z][e] += te[e];
+          for (int e = 0; e < 2 * N; e++) tm_emis[z][e] += tv[e];
+          const double kext_hydro = te[0 + 2 * (0 + 2 * 15)];  // extinct_matrix(1,1,16,1) (:367)
+          kexttot = kexttot + kext_hydro;
+          backtot = backtot + 4.0 * PI * sb[0];  // "NN": 4 pi Sback(1,1) (:322-358)
+          if (kexttot == 0.0) salbedo = 0.0;
+          else salbedo = salbedo + (0.0 * kext_hydro);
+          if (kexttot < 0.0 || std::isnan(kexttot)) return 2;
+          continue;
+        }
         MieOut mo;
         if (calc_mie_spheres(*st, freq * 1e9, s.liq_ice, bn, ndens, refre, refim, mo)) return 2;
         save_bscat(z, h, mo, ndens);
@@ -1937,10 +2025,14 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
         for (int jj = 0; jj < MAXNLEG; jj++) legen_coef[k][jj] = legen_coef[k][jj] / (salbedo * kexttot);
       if (fi == 0) present[z] = pres;
       scat[z].assign((size_t)4 * n * n, 0.0);
-      if (nlegen_coef > 0) {
-        scatcnv(N, nlegen_coef, legen_coef, kexttot, salbedo, scat[z], extk[z], emk[z]);
-        if (!st->lhyd_scattering) std::fill(scat[z].begin(), scat[z].end(), 0.0);
-        if (!st->lhyd_emission) emk[z] = 0.0;
+      if (nlegen_coef > 0) scatcnv(N, nlegen_coef, legen_coef, kexttot, salbedo, scat[z], extk[z], emk[z]);
+      // rt_* = (T-matrix species) + scatcnv (src/hydrometeor_extinction.f90:337-342)
+      if (!tm_scat[z].empty())
+        for (size_t e = 0; e < scat[z].size(); e++) scat[z][e] = tm_scat[z][e] + scat[z][e];
+      if (!st->lhyd_scattering) std::fill(scat[z].begin(), scat[z].end(), 0.0);
+      if (!st->lhyd_emission) {
+        emk[z] = 0.0;
+        std::fill(tm_emis[z].begin(), tm_emis[z].end(), 0.0);
       }
       if (dbg) {
         size_t o = (size_t)fi * L + z;
@@ -1986,6 +2078,8 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
         for (int j1 = 0; j1 < N; j1++)
           for (int l = 1; l <= 2; l++) {
             double sum = ((l == 1 || l == 2) ? emk[z] : 0.0) - extk[z];
+            if (!tm_ext[z].empty())  // EMIS_VECTOR(1,J1,L) - EXTINCT_MATRIX(1,1,J1,L)
+              sum = (tm_emis[z][0 + 2 * j1] + emk[z]) - (tm_ext[z][0 + 2 * (0 + 2 * j1)] + extk[z]);
             for (int j2 = 0; j2 < N; j2++) {
               size_t qi = (size_t)(0 + 2 * j2) * n + (0 + 2 * j1);
               sum = sum + 2.0 * 3.1415926535897932384 * qw[j2] *
@@ -1998,7 +2092,10 @@ int orc_run_column_fs(const orc_settings* st, const orc_species* sp, int nhydro,
       double planck1 = planck(t1, wl), planck0 = planck(t0, wl);
       int nd = -1;
       if (!present[z]) nonscatter_layer(N, mu, zdiff * gas, planck0, planck1, lay[layer]);
-      else scattering_layer(N, mu, qw, zdiff, gas, planck0, planck1, scat[z], extk[z], emk[z], lay[layer], nd);
+      else
+        scattering_layer(N, mu, qw, zdiff, gas, planck0, planck1, scat[z], extk[z], emk[z], lay[layer], nd,
+                         tm_ext[z].empty() ? nullptr : tm_ext[z].data(),
+                         tm_emis[z].empty() ? nullptr : tm_emis[z].data());
       if (dbg && dbg->num_doubles) dbg->num_doubles[(size_t)fi * L + z] = nd;
     }
     // surface (src/sfc_matrices.f90, default emissivity branch sfc_optics.f90:79-81)
