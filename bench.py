@@ -745,13 +745,18 @@ def main():
     split_value = world * solves_step / (np.mean(sms_) * 1e-3)
     tb_split = sout["tb"].cpu().numpy()
     split_err_f64 = float(np.max(np.abs(tb_split - out["tb"].cpu().numpy())))
-    # the same with the FP64 adding (split-precision doubling only), for comparison
+    # the same with the FP64 adding (split-precision doubling only), for comparison; its adding
+    # stage runs the FP64 kernel, so it takes the FP64 shape's adding CTAs per SM
     fout = b.alloc_outputs(dev)
+    shape_fa = list(shape_s)
+    shape_fa[3] = shape64[3]
+    eng.set_launch(shape_fa)
     fms_, fstages = _timed_steps(b, local, eng, stream, fout, PREC_3XTF32_FP64ADD, args.steps, args.warmup, flush)
     eng.set_launch(shape64)
     split_fa = {"value": world * solves_step / (np.mean(fms_) * 1e-3), "unit": "solves/s",
                 "ms_per_step": float(np.mean(fms_)), "stage_ms": fstages,
                 "tb_err_vs_fp64_batched_K": float(np.max(np.abs(fout["tb"].cpu().numpy() - out["tb"].cpu().numpy()))),
+                "launch_shape": shape_fa,
                 "form": "PREC_3XTF32_FP64ADD: the 3xTF32 doubling with the one-inverse FP64 adding"}
     del fout
     # ---- plain form: one column per call
