@@ -143,6 +143,10 @@ def species_from_df(data, fullspec=False):
             dist = "exp"
         if dist not in DIST_CODES or dist == "exp_cosmo_snow":
             raise NotImplementedError("dist_name %r is not on this path" % dist)
+        if scat == "tmatrix":
+            raise NotImplementedError(
+                "scat_name 'tmatrix' inside runPamtra is not wired into the forward run yet; the species' "
+                "single-scattering matrices are available from pamtra_b200.tmatrix.calc_tmatrix")
         if scat not in SCAT_CODES:
             raise NotImplementedError("scat_name %r is not on this path (mie-sphere only)" % scat)
         out[i]["liq_ice"] = int(row["liq_ice"])

@@ -277,3 +277,13 @@ def test_oracle_forward_oblate_spheroids_polarise(oracle_mod):
     pol_tm = np.max(np.abs(tb2[-1, :16, 0, 0] - tb2[-1, :16, 0, 1]))
     pol_mie = np.max(np.abs(tb0[-1, :16, 0, 0] - tb0[-1, :16, 0, 1]))
     assert pol_tm > 1.0 and pol_tm > 3 * pol_mie
+
+
+def test_tmatrix_species_in_run_pamtra_points_to_calc_tmatrix():
+    from pamtra_b200 import packing
+    from pamtra_b200 import workloads as wl
+    pam = wl.golden_pam()
+    data = pam.df.data.copy()
+    data["scat_name"][0] = "tmatrix"
+    with pytest.raises(NotImplementedError, match="calc_tmatrix"):
+        packing.species_from_df(data, False)
