@@ -340,3 +340,31 @@ def miecalc(x, mr, mi):
     ar, ai, br, bi = (np.zeros(10000) for _ in range(4))
     n = lib().orc_miecalc(x, mr, mi, 10000, _p(ar), _p(ai), _p(br), _p(bi))
     return (ar[:n] + 1j * ai[:n]), (br[:n] + 1j * bi[:n])
+
+
+_lib64 = None
+
+
+def tmatrix_tmat64(lam, mrr, mri, axi, as_ratio):
+    """As tmatrix_tmat, from the double-precision twin of the solve
+    (liboracle_tm64.so, entry orc64_tmatrix_tmat): the FP64 counterpart of the
+    REAL*16 computation, for measuring the FP64 envelope."""
+    global _lib64
+    if _lib64 is None:
+        lib()
+        path = os.path.join(HERE, "_build", "liboracle_tm64.so")
+        if not os.path.exists(path):
+            build()
+        _lib64 = ctypes.CDLL(path)
+        fp = ctypes.POINTER(ctypes.c_float)
+        _lib64.orc64_tmatrix_tmat.restype = ctypes.c_int
+        _lib64.orc64_tmatrix_tmat.argtypes = [ctypes.c_double] * 5 + [ctypes.c_int, fp, fp]
+    cap = 101 * 4 * 100 * 100
+    re = np.zeros(cap, np.float32)
+    im = np.zeros(cap, np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    nmax = _lib64.orc64_tmatrix_tmat(lam, mrr, mri, axi, as_ratio, cap, re.ctypes.data_as(fp), im.ctypes.data_as(fp))
+    if nmax <= 0:
+        return None
+    n = (nmax + 1) * 4 * nmax * nmax
+    return (re[:n] + 1j * im[:n].astype(np.complex64)).reshape(nmax + 1, 4, nmax, nmax)

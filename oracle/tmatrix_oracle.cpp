@@ -23,7 +23,9 @@
 // test-suite; the oracle is pinned by the sphere limit (aspect ratio 1
 // reproduces the Mie restatement's extinction and backscatter, which is pinned
 // to the reference's golden fixture).
+#ifndef TMO_DOUBLE
 #include <quadmath.h>
+#endif
 
 #include <cmath>
 #include <cstdint>
@@ -32,9 +34,41 @@
 
 #include "oracle_common.h"
 
+// Built twice: as the oracle (REAL*16 like the reference) and, with
+// -DTMO_DOUBLE, as a double-precision twin of the same steps whose entry
+// points carry the prefix orc64_.  The twin measures how far an FP64 solve
+// (the precision of the CUDA path) departs from the REAL*16 one.
+#ifdef TMO_DOUBLE
+#define TMO_NAME(x) orc64_##x
+#else
+#define TMO_NAME(x) orc_##x
+#endif
+
 namespace tmo {
 
+#ifdef TMO_DOUBLE
+typedef double Q;
+static inline Q qsqrt(Q x) { return std::sqrt(x); }
+static inline Q qcos(Q x) { return std::cos(x); }
+static inline Q qsin(Q x) { return std::sin(x); }
+static inline Q qcosh(Q x) { return std::cosh(x); }
+static inline Q qsinh(Q x) { return std::sinh(x); }
+static inline Q qpow(Q x, Q y) { return std::pow(x, y); }
+static inline Q qacos(Q x) { return std::acos(x); }
+static inline Q qfabs(Q x) { return std::fabs(x); }
+static const Q Q_NEWTON_TOL = (Q)1e-16, Q_TINY = (Q)1e-300;
+#else
 typedef __float128 Q;
+static inline Q qsqrt(Q x) { return sqrtq(x); }
+static inline Q qcos(Q x) { return cosq(x); }
+static inline Q qsin(Q x) { return sinq(x); }
+static inline Q qcosh(Q x) { return coshq(x); }
+static inline Q qsinh(Q x) { return sinhq(x); }
+static inline Q qpow(Q x, Q y) { return powq(x, y); }
+static inline Q qacos(Q x) { return acosq(x); }
+static inline Q qfabs(Q x) { return fabsq(x); }
+static const Q Q_NEWTON_TOL = (Q)1e-33, Q_TINY = (Q)1e-40;
+#endif
 
 struct CQ {
   Q r, i;
@@ -60,9 +94,9 @@ constexpr int NPNG1 = 500;
 static void gauss_legendre(int n, std::vector<Q>& z, std::vector<Q>& w) {
   z.assign(n, 0);
   w.assign(n, 0);
-  const Q pi = acosq((Q)-1);
+  const Q pi = qacos((Q)-1);
   for (int k = 0; k < (n + 1) / 2; k++) {
-    Q x = cosq(pi * ((Q)k + (Q)0.75) / ((Q)n + (Q)0.5));
+    Q x = qcos(pi * ((Q)k + (Q)0.75) / ((Q)n + (Q)0.5));
     Q dp = 1;
     for (int it = 0; it < 200; it++) {
       Q p0 = 1, p1 = x;
@@ -75,7 +109,7 @@ static void gauss_legendre(int n, std::vector<Q>& z, std::vector<Q>& w) {
       dp = ((Q)n) * (x * p1 - p0) / (x * x - 1);
       const Q dx = p1 / dp;
       x -= dx;
-      if (fabsq(dx) <= (Q)1e-33 * fabsq(x) || fabsq(dx) < (Q)1e-40) break;
+      if (qfabs(dx) <= Q_NEWTON_TOL * qfabs(x) || qfabs(dx) < Q_TINY) break;
     }
     Q p0 = 1, p1 = x;
     for (int j = 2; j <= n; j++) {
@@ -125,7 +159,7 @@ static void cons(Solve& S) {
     y = (Q)1 / ((Q)1 - y * y);
     S.ss[i] = y;
     S.ss[ng - 1 - i] = y;
-    y = sqrtq(y);
+    y = qsqrt(y);
     S.s[i] = y;
     S.s[ng - 1 - i] = y;
   }
@@ -138,10 +172,10 @@ static void rsp1(Solve& S, Q rev, Q eps) {
   const int ng = 2 * S.ngauss;
   S.r.assign(ng, 0);
   S.dr.assign(ng, 0);
-  const Q a = rev * powq(eps, (Q)1 / (Q)3);
+  const Q a = rev * qpow(eps, (Q)1 / (Q)3);
   const Q aa = a * a, ee = eps * eps, ee1 = ee - 1;
   for (int i = 0; i < S.ngauss; i++) {
-    const Q c = S.x[i], cc = c * c, ssv = 1 - cc, s = sqrtq(ssv);
+    const Q c = S.x[i], cc = c * c, ssv = 1 - cc, s = qsqrt(ssv);
     const Q rr = 1 / (ssv + ee * cc);
     S.r[i] = aa * rr;
     S.r[ng - 1 - i] = S.r[i];
@@ -159,7 +193,7 @@ static void rjb(Q x, Q* y, Q* u, int nmax, int nnmax) {
   z[L] = 1 / ((Q)(2 * L + 1) * xx);
   for (int i1 = L - 1; i1 >= 1; i1--) z[i1] = 1 / ((Q)(2 * i1 + 1) * xx - z[i1 + 1]);
   const Q z0 = 1 / (xx - z[1]);
-  const Q y0 = z0 * cosq(x) * xx;
+  const Q y0 = z0 * qcos(x) * xx;
   const Q y1 = y0 * z[1];
   u[0] = y0 - y1 * xx;
   y[0] = y1;
@@ -173,7 +207,7 @@ static void rjb(Q x, Q* y, Q* u, int nmax, int nnmax) {
 // RYB (tmatrix_amplq.lp.f:1416-1442): spherical Neumann y_n(x) by upward
 // recurrence and v_n = y_{n-1} - n y_n / x.
 static void ryb(Q x, Q* y, Q* v, int nmax) {
-  const Q c = cosq(x), s = sinq(x), x1 = 1 / x, x2 = x1 * x1, x3 = x2 * x1;
+  const Q c = qcos(x), s = qsin(x), x1 = 1 / x, x2 = x1 * x1, x3 = x2 * x1;
   std::vector<Q> t(nmax + 2);
   t[1] = -c * x2 - s * x1;
   t[2] = (-3 * x3 + x1) * c - 3 * x2 * s;
@@ -195,7 +229,7 @@ static void cjb(Q xr, Q xi, Q* yr, Q* yi, Q* ur, Q* ui, int nmax, int nnmax) {
     z[i1] = cdivq(cq(1, 0), a);
   }
   const CQ z0 = cdivq(cq(1, 0), cx - z[1]);
-  const CQ cosx = cq(cosq(xr) * coshq(xi), -sinq(xr) * sinhq(xi));
+  const CQ cosx = cq(qcos(xr) * qcosh(xi), -qsin(xr) * qsinh(xi));
   const CQ y0 = (z0 * cosx) * cx;
   CQ yprev = y0 * z[1];
   const CQ u1 = y0 - yprev * cx;
@@ -221,7 +255,7 @@ static void cjb(Q xr, Q xi, Q* yr, Q* yi, Q* ur, Q* ui, int nmax, int nnmax) {
 static int vary(Solve& S, Q lam, Q mrr, Q mri, Q a, Q eps) {
   const int ng = 2 * S.ngauss, nmax = S.nmax;
   rsp1(S, a, eps);
-  const Q pi = acosq((Q)-1) * (Q)2 / lam;
+  const Q pi = qacos((Q)-1) * (Q)2 / lam;
   S.ppi = pi * pi;
   S.pir = S.ppi * mrr;
   S.pii = S.ppi * mri;
@@ -233,7 +267,7 @@ static int vary(Solve& S, Q lam, Q mrr, Q mri, Q a, Q eps) {
   S.drr.assign(ng, 0);
   S.dri.assign(ng, 0);
   for (int i = 0; i < ng; i++) {
-    const Q vv = sqrtq(S.r[i]);
+    const Q vv = qsqrt(S.r[i]);
     v = vv * pi;
     if (v > ta) ta = v;
     const Q iv = 1 / v;
@@ -244,10 +278,10 @@ static int vary(Solve& S, Q lam, Q mrr, Q mri, Q a, Q eps) {
     zr[i] = v * mrr;
     zi[i] = v * mri;
   }
-  Q tb = ta * sqrtq(mrr * mrr + mri * mri);
+  Q tb = ta * qsqrt(mrr * mrr + mri * mri);
   if (tb < (Q)nmax) tb = (Q)nmax;
-  const int nnmax1 = (int)((Q)8 * sqrtq(ta > (Q)nmax ? ta : (Q)nmax) + (Q)3);
-  int nnmax2 = (int)(tb + (Q)4 * powq(tb, (Q)33333 / (Q)100000) + (Q)8 * sqrtq(tb));
+  const int nnmax1 = (int)((Q)8 * qsqrt(ta > (Q)nmax ? ta : (Q)nmax) + (Q)3);
+  int nnmax2 = (int)(tb + (Q)4 * qpow(tb, (Q)33333 / (Q)100000) + (Q)8 * qsqrt(tb));
   nnmax2 = nnmax2 - nmax + 5;
   if (nmax + nnmax2 >= 1200) return 1;
   const size_t T = (size_t)ng * nmax;
@@ -265,7 +299,7 @@ static int vary(Solve& S, Q lam, Q mrr, Q mri, Q a, Q eps) {
 // theta-derivative (dv2) for n = 1..nmax (index n - 1), zero below n = m.
 static void vig(Q x, int nmax, int m, Q* dv1, Q* dv2) {
   for (int n = 0; n < nmax; n++) dv1[n] = dv2[n] = 0;
-  const Q qs = sqrtq(1 - x * x), qs1 = 1 / qs;
+  const Q qs = qsqrt(1 - x * x), qs1 = 1 / qs;
   if (m == 0) {
     Q d1 = 1, d2 = x;
     for (int n = 1; n <= nmax; n++) {
@@ -289,7 +323,7 @@ static void vig(Q x, int nmax, int m, Q* dv1, Q* dv2) {
   Q d1 = 0, d2 = a;
   for (int n = m; n <= nmax; n++) {
     const Q qn = n, qn2 = 2 * n + 1, qn1 = n + 1;
-    const Q qnm = sqrtq(qn * qn - qmm), qnm1 = sqrtq(qn1 * qn1 - qmm);
+    const Q qnm = qsqrt(qn * qn - qmm), qnm1 = qsqrt(qn1 * qn1 - qmm);
     const Q d3 = (qn2 * x * d2 - qnm * d1) / qnm1;
     const Q der = qs1 * (-qn1 * qnm * d1 + qn * qnm1 * d3) / qn2;
     dv1[n - 1] = d2;
@@ -524,7 +558,7 @@ static int amplq(double lam_d, double mrr_d, double mri_d, double axi, double as
   const int ndgs = 2;
   const Q lam = lam_d, mrr = mrr_d, mri = mri_d;
   const Q a = (Q)(1.0 * axi);
-  const double pin = (double)acosq((Q)-1);
+  const double pin = (double)qacos((Q)-1);
   const double dlam = lam_d;
   const double xev = (double)((Q)(2.0 * pin) * a / (Q)dlam);
   const int ixxx = (int)(xev + 4.05 * std::pow(xev, 0.333333));
@@ -902,14 +936,14 @@ extern "C" {
 
 // calc_single_tmatrix for one particle (alpha = 0).  mri is the magnitude of
 // the imaginary part; returns 0 or 2 (the reference's fatal error).
-int orc_tmatrix_single(int nummu, double frequency, double mrr, double mri, double axi, double as_ratio,
+int TMO_NAME(tmatrix_single)(int nummu, double frequency, double mrr, double mri, double axi, double as_ratio,
                        double beta, double* scat, double* ext, double* emis, double* sback) {
   return tmo::single(nummu, frequency, mrr, std::fabs(mri), axi, as_ratio, 0.0, beta, scat, ext, emis, sback);
 }
 
 // The single-precision T-matrix of one particle: returns nmax (0 on error)
 // and fills re/im [(nmax+1)][4][nmax][nmax] when cap allows.
-int orc_tmatrix_tmat(double lam, double mrr, double mri, double axi, double as_ratio, int cap, float* re,
+int TMO_NAME(tmatrix_tmat)(double lam, double mrr, double mri, double axi, double as_ratio, int cap, float* re,
                      float* im) {
   tmo::TMat T;
   if (tmo::amplq(lam, mrr, std::fabs(mri), axi, as_ratio, T)) return 0;
@@ -923,7 +957,7 @@ int orc_tmatrix_tmat(double lam, double mrr, double mri, double axi, double as_r
 // bins with ndens = 0 are skipped; ice (phase -1) of density != 917 is mixed
 // with air (eps_mix); the equal-volume radius follows the aspect ratio.
 // back_spec is the "NN" backscattering per bin, 4 pi ndens Sback(1,1).
-int orc_tmatrix_species(int nummu, double frequency, double ref_re, double ref_im, int phase, int nbins,
+int TMO_NAME(tmatrix_species)(int nummu, double frequency, double ref_re, double ref_im, int phase, int nbins,
                         const double* dmax, const double* del_d, const double* ndens, const double* density,
                         const double* as_ratio, const double* canting, double* scat, double* ext, double* emis,
                         double* back_spec, double* sback) {

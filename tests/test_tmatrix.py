@@ -287,3 +287,28 @@ def test_tmatrix_species_in_run_pamtra_points_to_calc_tmatrix():
     data["scat_name"][0] = "tmatrix"
     with pytest.raises(NotImplementedError, match="calc_tmatrix"):
         packing.species_from_df(data, False)
+
+
+@pytest.mark.parametrize("case", [
+    # (size parameter, aspect ratio, index, bound on the T difference, inside the FP64 envelope)
+    (10.0, 0.5, (1.78, 0.003), 1e-6, True),     # ice / snow: FP64 holds to x = 14 (2e-7)
+    (10.0, 2.0, (1.78, 0.003), 1e-6, True),
+    (3.0, 0.7, (5.5, 2.9), 1e-6, True),         # liquid water: small drops
+    (6.0, 0.5, (5.5, 2.9), 1e-4, False),        # large, strongly oblate drops: FP64 loses digits
+])
+def test_fp64_solve_envelope(oracle_mod, case):
+    """The CUDA path solves the EBCM system in FP64, the reference in REAL*16.
+    The double-precision twin of the oracle's solve (the same steps) against
+    the REAL*16 one marks where FP64 suffices: everywhere for ice and snow
+    indices, for liquid water only up to moderate size and asphericity."""
+    x, asr, (mr, mi), bound, inside = case
+    lam = C / 89e9
+    axi = x * lam / (2 * np.pi)
+    tq = oracle_mod.tmatrix_tmat(lam, mr, mi, axi, asr)
+    td = oracle_mod.tmatrix_tmat64(lam, mr, mi, axi, asr)
+    assert tq is not None and td is not None and tq.shape == td.shape
+    d = np.max(np.abs(tq - td)) / np.max(np.abs(tq))
+    if inside:
+        assert d <= bound, d
+    else:
+        assert d > bound, d
