@@ -342,28 +342,34 @@ def miecalc(x, mr, mi):
     return (ar[:n] + 1j * ai[:n]), (br[:n] + 1j * bi[:n])
 
 
-_lib64 = None
+_twins = {}
 
 
-def tmatrix_tmat64(lam, mrr, mri, axi, as_ratio):
-    """As tmatrix_tmat, from the double-precision twin of the solve
-    (liboracle_tm64.so, entry orc64_tmatrix_tmat): the FP64 counterpart of the
-    REAL*16 computation, for measuring the FP64 envelope."""
-    global _lib64
-    if _lib64 is None:
+def _twin_tmat(kind):
+    """orc64_tmatrix_tmat (FP64 twin) or orcdd_tmatrix_tmat (double-double twin)."""
+    if kind not in _twins:
         lib()
-        path = os.path.join(HERE, "_build", "liboracle_tm64.so")
+        name, prefix = {"f64": ("liboracle_tm64.so", "orc64"), "dd": ("liboracle_tmdd.so", "orcdd")}[kind]
+        path = os.path.join(HERE, "_build", name)
         if not os.path.exists(path):
             build()
-        _lib64 = ctypes.CDLL(path)
+        fn = getattr(ctypes.CDLL(path), prefix + "_tmatrix_tmat")
         fp = ctypes.POINTER(ctypes.c_float)
-        _lib64.orc64_tmatrix_tmat.restype = ctypes.c_int
-        _lib64.orc64_tmatrix_tmat.argtypes = [ctypes.c_double] * 5 + [ctypes.c_int, fp, fp]
+        fn.restype = ctypes.c_int
+        fn.argtypes = [ctypes.c_double] * 5 + [ctypes.c_int, fp, fp]
+        _twins[kind] = fn
+    return _twins[kind]
+
+
+def tmatrix_tmat64(lam, mrr, mri, axi, as_ratio, kind="f64"):
+    """As tmatrix_tmat, from a twin of the solve: ``kind`` "f64" runs the same
+    steps in double precision (the precision of the CUDA path), "dd" in
+    double-double; for measuring how far each departs from REAL*16."""
     cap = 101 * 4 * 100 * 100
     re = np.zeros(cap, np.float32)
     im = np.zeros(cap, np.float32)
     fp = ctypes.POINTER(ctypes.c_float)
-    nmax = _lib64.orc64_tmatrix_tmat(lam, mrr, mri, axi, as_ratio, cap, re.ctypes.data_as(fp), im.ctypes.data_as(fp))
+    nmax = _twin_tmat(kind)(lam, mrr, mri, axi, as_ratio, cap, re.ctypes.data_as(fp), im.ctypes.data_as(fp))
     if nmax <= 0:
         return None
     n = (nmax + 1) * 4 * nmax * nmax

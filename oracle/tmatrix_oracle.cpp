@@ -23,7 +23,9 @@
 // test-suite; the oracle is pinned by the sphere limit (aspect ratio 1
 // reproduces the Mie restatement's extinction and backscatter, which is pinned
 // to the reference's golden fixture).
-#ifndef TMO_DOUBLE
+#if defined(TMO_DD)
+#include "dd.h"
+#elif !defined(TMO_DOUBLE)
 #include <quadmath.h>
 #endif
 
@@ -38,7 +40,9 @@
 // -DTMO_DOUBLE, as a double-precision twin of the same steps whose entry
 // points carry the prefix orc64_.  The twin measures how far an FP64 solve
 // (the precision of the CUDA path) departs from the REAL*16 one.
-#ifdef TMO_DOUBLE
+#if defined(TMO_DD)
+#define TMO_NAME(x) orcdd_##x
+#elif defined(TMO_DOUBLE)
 #define TMO_NAME(x) orc64_##x
 #else
 #define TMO_NAME(x) orc_##x
@@ -46,7 +50,18 @@
 
 namespace tmo {
 
-#ifdef TMO_DOUBLE
+#if defined(TMO_DD)
+typedef ddm::dd Q;
+static inline Q qsqrt(Q x) { return ddm::dd_sqrt(x); }
+static inline Q qcos(Q x) { return ddm::dd_cos(x); }
+static inline Q qsin(Q x) { return ddm::dd_sin(x); }
+static inline Q qcosh(Q x) { return ddm::dd_cosh(x); }
+static inline Q qsinh(Q x) { return ddm::dd_sinh(x); }
+static inline Q qpow(Q x, Q y) { return ddm::dd_pow(x, y); }
+static inline Q qacos(Q x) { return (double)x == -1.0 ? ddm::DD_PI : Q(std::acos((double)x)); }
+static inline Q qfabs(Q x) { return ddm::dd_abs(x); }
+static const Q Q_NEWTON_TOL = Q(1e-31), Q_TINY = Q(1e-300);
+#elif defined(TMO_DOUBLE)
 typedef double Q;
 static inline Q qsqrt(Q x) { return std::sqrt(x); }
 static inline Q qcos(Q x) { return std::cos(x); }

@@ -312,3 +312,18 @@ def test_fp64_solve_envelope(oracle_mod, case):
         assert d <= bound, d
     else:
         assert d > bound, d
+
+
+@pytest.mark.parametrize("x, asr", [(6.0, 0.5), (10.0, 0.7)])
+def test_double_double_solve_reproduces_real16(oracle_mod, x, asr):
+    """Where FP64 fails (large aspherical water drops), the same steps in
+    double-double arithmetic give the REAL*16 single-precision T-matrix."""
+    lam = C / 89e9
+    axi = x * lam / (2 * np.pi)
+    tq = oracle_mod.tmatrix_tmat(lam, 5.5, 2.9, axi, asr)
+    tdd = oracle_mod.tmatrix_tmat64(lam, 5.5, 2.9, axi, asr, kind="dd")
+    td = oracle_mod.tmatrix_tmat64(lam, 5.5, 2.9, axi, asr, kind="f64")
+    assert tq is not None and tdd is not None and tq.shape == tdd.shape
+    scale = np.max(np.abs(tq))
+    assert np.max(np.abs(tdd - tq)) <= 1e-6 * scale
+    assert td is None or td.shape != tq.shape or np.max(np.abs(td - tq)) > 1e-4 * scale
