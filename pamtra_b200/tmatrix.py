@@ -97,3 +97,41 @@ def calc_tmatrix(frequency, ref_index, phase, dmax, del_d, ndens, density, as_ra
             o["extinct_matrix"][0].reshape((2, 2, nummu), order="F"),
             o["emis_vector"][0].reshape((2, nummu), order="F"), o["back_spec"][0],
             o["sback"][0].reshape((2, 2), order="F"))
+
+
+def _main(argv=None):
+    """``python -m pamtra_b200.tmatrix --items 4 --nbins 32 --reps 2``: soft
+    ice spheroids (300 kg/m3, aspect ratio 0.6, 0.2-4 mm, 89 GHz, NUMMU 16)
+    from device arrays, ``reps`` calls; prints the status, NMAX range and the
+    device time of the last call (a fixed case for profiling)."""
+    import argparse
+    import torch
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--items", type=int, default=4)
+    ap.add_argument("--nbins", type=int, default=32)
+    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--canting", type=float, default=0.0)
+    a = ap.parse_args(argv)
+    dev = torch.device("cuda", 0)
+    eng = _native.Engine(0)
+    d = np.linspace(0.2e-3, 4e-3, a.nbins)[None, :].repeat(a.items, 0)
+    t = {k: torch.tensor(v, dtype=torch.float64, device=dev) for k, v in dict(
+        dmax=d, del_d=np.full_like(d, 1.2e-4), ndens=np.full_like(d, 1e6), density=np.full_like(d, 300.0),
+        as_ratio=np.full_like(d, 0.6), canting=np.full_like(d, a.canting)).items()}
+    fr = torch.full((a.items,), 89e9, dtype=torch.float64, device=dev)
+    ri = torch.full((a.items,), 1.78 - 0.002j, dtype=torch.complex128, device=dev)
+    ph = torch.full((a.items,), -1, dtype=torch.int32, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(a.reps):
+        e0.record()
+        o = calc_tmatrix_batch(fr, ri, ph, t["dmax"], t["del_d"], t["ndens"], t["density"], t["as_ratio"],
+                               t["canting"], eng=eng)
+        e1.record()
+    torch.cuda.synchronize()
+    nm = o["nmax"].cpu().numpy()
+    print("status %d nmax %d-%d ms %.3f" % (int(o["status"].max()), int(nm.min()), int(nm.max()),
+                                           e0.elapsed_time(e1)))
+
+
+if __name__ == "__main__":
+    _main()
