@@ -327,3 +327,12 @@ def test_double_double_solve_reproduces_real16(oracle_mod, x, asr):
     scale = np.max(np.abs(tq))
     assert np.max(np.abs(tdd - tq)) <= 1e-6 * scale
     assert td is None or td.shape != tq.shape or np.max(np.abs(td - tq)) > 1e-4 * scale
+
+
+def test_tmatrix_entry_rejects_missing_context(native):
+    """The C-ABI entry validates its arguments before touching a device."""
+    import ctypes
+    lib = native.load()
+    ti, to = native.TmatrixIn(), native.TmatrixOut()
+    ti.n_items, ti.nbins, ti.nummu = 1, 1, 16
+    assert lib.pamtra_b200_tmatrix(None, ctypes.byref(ti), ctypes.byref(to), None) == 2
