@@ -99,6 +99,36 @@ def calc_tmatrix(frequency, ref_index, phase, dmax, del_d, ndens, density, as_ra
             o["sback"][0].reshape((2, 2), order="F"))
 
 
+RADAR_POLS = ("NN", "HH", "VV", "HV", "VH")
+
+
+def back_hydro(sback, radar_pol="NN"):
+    """Backscattering of a species per volume (m^-1, before the radar's
+    wavelength factors) for one radar polarisation, from its summed Sback
+    (2, 2) as the T-matrix branch forms ``back_hydro``
+    (src/scatProperties.f90:322-358): "NN" is 4 pi Sback(1,1); "HH", "VV",
+    "HV", "VH" take the half sums of Vivekanandan et al. (1991).  ``sback``
+    is a (2, 2) array indexed like the Fortran Sback(i, j), or the flat
+    four values of the C-ABI in Fortran order."""
+    S = np.asarray(sback, dtype=np.float64)
+    if S.shape != (2, 2):
+        S = S.reshape((2, 2), order="F")
+    s11, s12, s21, s22 = S[0, 0], S[0, 1], S[1, 0], S[1, 1]
+    if radar_pol == "NN":
+        b = s11
+    elif radar_pol == "HH":
+        b = (s11 - s12 - s21 + s22) * 0.5
+    elif radar_pol == "VV":
+        b = (s11 + s12 + s21 + s22) * 0.5
+    elif radar_pol == "HV":
+        b = (s11 - s12 + s21 - s22) * 0.5
+    elif radar_pol == "VH":
+        b = (s11 + s12 - s21 - s22) * 0.5
+    else:
+        raise ValueError("do not understand radar_pol: %r" % (radar_pol,))
+    return 4 * np.pi * b
+
+
 def _main(argv=None):
     """``python -m pamtra_b200.tmatrix --items 4 --nbins 32 --reps 2``: soft
     ice spheroids (300 kg/m3, aspect ratio 0.6, 0.2-4 mm, 89 GHz, NUMMU 16)

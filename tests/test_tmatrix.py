@@ -336,3 +336,27 @@ def test_tmatrix_entry_rejects_missing_context(native):
     ti, to = native.TmatrixIn(), native.TmatrixOut()
     ti.n_items, ti.nbins, ti.nummu = 1, 1, 16
     assert lib.pamtra_b200_tmatrix(None, ctypes.byref(ti), ctypes.byref(to), None) == 2
+
+
+def test_back_hydro_polarisations(oracle_mod):
+    """back_hydro per radar polarisation from a species' Sback (recorded for
+    vertical incidence from below, as the reference records it): a sphere
+    and an upright spheroid (seen along its axis) backscatter HH = VV = NN;
+    a spheroid tilted by 60 deg gives positive differential reflectivity;
+    with the tilt in the plane of the polarisation basis no cross-polar
+    power appears."""
+    from pamtra_b200.tmatrix import back_hydro
+    sph = oracle_mod.tmatrix_single(16, 9.6e9, 8.9, 1.5, 1.5e-3, 1.0)["sback"]
+    nn = back_hydro(sph, "NN")
+    assert abs(back_hydro(sph, "HH") / nn - 1) < 1e-12 and abs(back_hydro(sph, "VV") / nn - 1) < 1e-12
+    assert abs(back_hydro(sph, "HV")) < 1e-12 * nn and abs(back_hydro(sph, "VH")) < 1e-12 * nn
+    up = oracle_mod.tmatrix_single(16, 9.6e9, 8.9, 1.5, 1.5e-3, 0.6)["sback"]
+    assert abs(back_hydro(up, "HH") / back_hydro(up, "VV") - 1) < 1e-12
+    obl = oracle_mod.tmatrix_single(16, 9.6e9, 8.9, 1.5, 1.5e-3, 0.6, beta=60.0)["sback"]
+    zdr = 10 * np.log10(back_hydro(obl, "HH") / back_hydro(obl, "VV"))
+    assert 2.0 < zdr < 10.0, zdr
+    assert abs(back_hydro(obl, "HV")) < 1e-10 * back_hydro(obl, "HH")
+    # the flat C-ABI order is the Fortran order of Sback(2, 2)
+    assert back_hydro(np.asarray(obl).ravel(order="F"), "HH") == back_hydro(obl, "HH")
+    with pytest.raises(ValueError):
+        back_hydro(obl, "XX")
