@@ -44,7 +44,8 @@ class OrcSettings(ctypes.Structure):
 
 class OrcFullspec(ctypes.Structure):
     _fields_ = [("nbin", ctypes.c_int32), ("d", ctypes.c_void_p), ("d_bound", ctypes.c_void_p),
-                ("n", ctypes.c_void_p), ("rho", ctypes.c_void_p), ("mass", ctypes.c_void_p)]
+                ("n", ctypes.c_void_p), ("rho", ctypes.c_void_p), ("mass", ctypes.c_void_p),
+                ("as_ratio", ctypes.c_void_p), ("canting", ctypes.c_void_p)]
 
 
 PSD_KEYS = ("psd_d", "psd_deltad", "psd_n", "psd_mass", "psd_area", "psd_bscat")
@@ -116,14 +117,17 @@ def settings(pk_settings):
     return s
 
 
-def run_column(st, species, cols, c, freqs, debug=False, psd_nbin=0, scat_code=None, canting=None):
+def run_column(st, species, cols, c, freqs, debug=False, psd_nbin=0, scat_code=None, canting=None,
+               fs_as_ratio=None, fs_canting=None):
     """Run column ``c`` of packed ``cols`` (pamtra_b200.packing.profile_columns).
     ``debug`` True returns all intermediates, "radar" only the simple-radar
     outputs (back, ze, att_hydro, att_atmo; filled when ``st.active``).
     ``psd_nbin`` > 0 adds the save_psd bins, [L][nhydro][psd_nbin].
     ``scat_code`` (per species, 1 = T-matrix spheroid of the species' aspect
     ratio, 0 = Mie sphere) and ``canting`` (deg, per species) select the
-    scattering model of scatProperties.f90:289-367 (moment-based bins only)."""
+    scattering model of scatProperties.f90:289-367; with full spectra the
+    T-matrix species take ``fs_as_ratio`` / ``fs_canting`` of this column,
+    [L][nhydro][nbin] (hydrofs_as_ratio / hydrofs_canting, :257-265)."""
     l = lib()
     L = int(cols["nlyrs"][c])
     Lmax = int(cols["max_nlyrs"])
@@ -176,7 +180,16 @@ def run_column(st, species, cols, c, freqs, debug=False, psd_nbin=0, scat_code=N
         fsa = {k: f64(cols[k][c, :L]) for k in ("fs_d", "fs_d_bound", "fs_n", "fs_rho", "fs_mass")}
         fs = OrcFullspec(int(cols["fs_nbin"]), *[fsa[k].ctypes.data for k in
                                                   ("fs_d", "fs_d_bound", "fs_n", "fs_rho", "fs_mass")])
-        err = l.orc_run_column_fs(*(args + [ctypes.byref(fs)]))
+        if scat_code is not None:
+            keep = [f64(fs_as_ratio) if fs_as_ratio is not None else None,
+                    f64(fs_canting) if fs_canting is not None else None]
+            fs.as_ratio = keep[0].ctypes.data if keep[0] is not None else None
+            fs.canting = keep[1].ctypes.data if keep[1] is not None else None
+            sc = np.ascontiguousarray(np.asarray(scat_code, dtype=np.int32))
+            ct = f64(canting if canting is not None else np.zeros(H))
+            err = l.orc_run_column_tm(*(args + [ctypes.byref(fs), sc.ctypes.data, _p(ct)]))
+        else:
+            err = l.orc_run_column_fs(*(args + [ctypes.byref(fs)]))
     elif scat_code is not None:
         sc = np.ascontiguousarray(np.asarray(scat_code, dtype=np.int32))
         ct = f64(canting if canting is not None else np.zeros(H))

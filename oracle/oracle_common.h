@@ -115,6 +115,7 @@ typedef struct {
 typedef struct {
   int32_t nbin;
   const double *d, *d_bound, *n, *rho, *mass;
+  const double *as_ratio, *canting;  // per bin, T-matrix species only (may be NULL)
 } orc_fullspec;
 
 // Optional per-(layer,freq) intermediates for parity tests.

@@ -1801,9 +1801,9 @@ int orc_run_column_tm(const orc_settings* st, const orc_species* sp, int nhydro,
                       double* emissivity_out, double* angles_deg, orc_debug* dbg, const orc_fullspec* fs,
                       const int* scat_code, const double* canting) {
   const int N = st->nummu, n = 2 * N;
-  if (scat_code && fs)
+  if (scat_code && fs && !fs->as_ratio)
     for (int h = 0; h < nhydro; h++)
-      if (scat_code[h] == 1) return 2;  // per-bin aspect ratios of full spectra: not restated
+      if (scat_code[h] == 1) return 2;  // full spectra carry the aspect ratio per bin
   if (scat_code && N < 16)
     for (int h = 0; h < nhydro; h++)
       if (scat_code[h] == 1) return 2;  // kext_hydro reads extinct_matrix(1,1,16,1)
@@ -1880,6 +1880,47 @@ int orc_run_column_tm(const orc_settings* st, const orc_species* sp, int nhydro,
       bool pres = false;
       double qsum = 0.0;
       for (int h = 0; h < nhydro; h++) qsum += hydro_q[z * nhydro + h];
+      // calc_tmatrix of one species (src/scatProperties.f90:289-367): per-bin
+      // aspect ratio and canting, negative or NaN read as 0 (:284-287)
+      auto add_tmatrix = [&](const orc_species& s, const Bins& bn, const std::vector<double>& ndens, double refre,
+                             double refim, std::vector<double> asl, std::vector<double> cl) -> int {
+        const int nb = bn.nbin;
+        for (int i = 0; i < nb; i++) {
+          if (asl[i] < 0 || std::isnan(asl[i])) asl[i] = 0.0;
+          if (cl[i] < 0 || std::isnan(cl[i])) cl[i] = 0.0;
+        }
+        std::vector<double> bk(nb), ts((size_t)8 * N * N), te(4 * N), tv(2 * N), sb(4);
+        if (orc_tmatrix_species(N, freq * 1e9, refre, -refim, s.liq_ice, nb, bn.diam.data(), bn.delta_d.data(),
+                                ndens.data(), bn.dens.data(), asl.data(), cl.data(), ts.data(), te.data(), tv.data(),
+                                bk.data(), sb.data()))
+          return 2;
+        if (tm_scat[z].empty()) {
+          tm_scat[z].assign((size_t)4 * n * n, 0.0);
+          tm_ext[z].assign(4 * N, 0.0);
+          tm_emis[z].assign(2 * N, 0.0);
+        }
+        // scatter_matrix(i2, ll, i1, jj, kk) -> quadrant L = kk and L = 5 - kk
+        // (src/scatProperties.f90:316-317), rows (i2, ll), columns (i1, jj)
+        for (int kk = 0; kk < 2; kk++)
+          for (int jj = 0; jj < N; jj++)
+            for (int i1 = 0; i1 < 2; i1++)
+              for (int ll = 0; ll < N; ll++)
+                for (int i2 = 0; i2 < 2; i2++) {
+                  const double v = ts[i2 + 2 * (ll + N * (i1 + 2 * (jj + N * kk)))];
+                  const size_t qi = (size_t)(i2 + 2 * ll) * n + (i1 + 2 * jj);
+                  tm_scat[z][(size_t)kk * n * n + qi] += v;
+                  tm_scat[z][(size_t)(3 - kk) * n * n + qi] += v;
+                }
+        for (int e = 0; e < 4 * N; e++) tm_ext[z][e] += te[e];
+        for (int e = 0; e < 2 * N; e++) tm_emis[z][e] += tv[e];
+        const double kext_hydro = te[0 + 2 * (0 + 2 * 15)];  // extinct_matrix(1,1,16,1) (:367)
+        kexttot = kexttot + kext_hydro;
+        backtot = backtot + 4.0 * PI * sb[0];  // "NN": 4 pi Sback(1,1) (:322-358)
+        if (kexttot == 0.0) salbedo = 0.0;
+        else salbedo = salbedo + (0.0 * kext_hydro);
+        if (kexttot < 0.0 || std::isnan(kexttot)) return 2;
+        return 0;
+      };
       for (int h = 0; h < nhydro; h++) {
         const orc_species& s = sp[h];
         if (fs) {
@@ -1907,6 +1948,14 @@ int orc_run_column_tm(const orc_settings* st, const orc_species* sp, int nhydro,
             if (ref_water_mod(st->liq_mod, a.temp[z] - F(273.15f), freq, refre, refim)) return 2;
           } else {
             ref_ice(a.temp[z], freq, refre, refim);
+          }
+          if (scat_code && scat_code[h] == 1) {
+            // hydrofs_as_ratio / hydrofs_canting per bin (src/scatProperties.f90:257-265)
+            std::vector<double> asl(fs->as_ratio + o, fs->as_ratio + o + nb);
+            std::vector<double> cl = fs->canting ? std::vector<double>(fs->canting + o, fs->canting + o + nb)
+                                                 : std::vector<double>(nb, 0.0);
+            if (add_tmatrix(s, bn, ndens, refre, refim, asl, cl)) return 2;
+            continue;
           }
           MieOut mo;
           if (calc_mie_spheres(*st, freq * 1e9, s.liq_ice, bn, ndens, refre, refim, mo)) return 2;
@@ -1965,42 +2014,10 @@ int orc_run_column_tm(const orc_settings* st, const orc_species* sp, int nhydro,
           ref_ice(a.temp[z], freq, refre, refim);
         }
         if (scat_code && scat_code[h] == 1) {
-          // calc_tmatrix (src/scatProperties.f90:289-306): every bin with the
-          // species' aspect ratio and canting (negative or NaN read as 0, :284-287)
-          const int nb = bn.nbin;
-          double asr = s.as_ratio, cant = canting ? canting[h] : 0.0;
-          if (asr < 0 || std::isnan(asr)) asr = 0.0;
-          if (cant < 0 || std::isnan(cant)) cant = 0.0;
-          std::vector<double> asl(nb, asr), cl(nb, cant), bk(nb), ts((size_t)8 * N * N), te(4 * N), tv(2 * N), sb(4);
-          if (orc_tmatrix_species(N, freq * 1e9, refre, -refim, s.liq_ice, nb, bn.diam.data(), bn.delta_d.data(),
-                                  ndens.data(), bn.dens.data(), asl.data(), cl.data(), ts.data(), te.data(),
-                                  tv.data(), bk.data(), sb.data()))
+          // every bin with the species' aspect ratio and canting
+          if (add_tmatrix(s, bn, ndens, refre, refim, std::vector<double>(bn.nbin, s.as_ratio),
+                          std::vector<double>(bn.nbin, canting ? canting[h] : 0.0)))
             return 2;
-          if (tm_scat[z].empty()) {
-            tm_scat[z].assign((size_t)4 * n * n, 0.0);
-            tm_ext[z].assign(4 * N, 0.0);
-            tm_emis[z].assign(2 * N, 0.0);
-          }
-          // scatter_matrix(i2, ll, i1, jj, kk) -> quadrant L = kk and L = 5 - kk
-          // (src/scatProperties.f90:316-317), rows (i2, ll), columns (i1, jj)
-          for (int kk = 0; kk < 2; kk++)
-            for (int jj = 0; jj < N; jj++)
-              for (int i1 = 0; i1 < 2; i1++)
-                for (int ll = 0; ll < N; ll++)
-                  for (int i2 = 0; i2 < 2; i2++) {
-                    const double v = ts[i2 + 2 * (ll + N * (i1 + 2 * (jj + N * kk)))];
-                    const size_t qi = (size_t)(i2 + 2 * ll) * n + (i1 + 2 * jj);
-                    tm_scat[z][(size_t)kk * n * n + qi] += v;
-                    tm_scat[z][(size_t)(3 - kk) * n * n + qi] += v;
-                  }
-          for (int e = 0; e < 4 * N; e++) tm_ext[z][e] += te[e];
-          for (int e = 0; e < 2 * N; e++) tm_emis[z][e] += tv[e];
-          const double kext_hydro = te[0 + 2 * (0 + 2 * 15)];  // extinct_matrix(1,1,16,1) (:367)
-          kexttot = kexttot + kext_hydro;
-          backtot = backtot + 4.0 * PI * sb[0];  // "NN": 4 pi Sback(1,1) (:322-358)
-          if (kexttot == 0.0) salbedo = 0.0;
-          else salbedo = salbedo + (0.0 * kext_hydro);
-          if (kexttot < 0.0 || std::isnan(kexttot)) return 2;
           continue;
         }
         MieOut mo;

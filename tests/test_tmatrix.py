@@ -360,3 +360,41 @@ def test_back_hydro_polarisations(oracle_mod):
     assert back_hydro(np.asarray(obl).ravel(order="F"), "HH") == back_hydro(obl, "HH")
     with pytest.raises(ValueError):
         back_hydro(obl, "XX")
+
+
+def test_oracle_fullspec_tmatrix_matches_moment_path(oracle_mod):
+    """A T-matrix ice species through the moment-based bins, and the same
+    bins handed over as a full spectrum whose per-bin aspect ratio is the
+    species' (hydrofs_as_ratio, src/scatProperties.f90:257-265): the same
+    brightness temperatures."""
+    import test_fullspec as tf
+    from pamtra_b200 import packing
+    freqs = [89.0]
+    pam0 = tf._one_species_pam(False)
+    st = oracle_mod.settings(packing.settings_from_nml(pam0.nmlSet, 16))
+    sp0 = packing.species_from_df(pam0.df.data, False)
+    sp0["as_ratio"] = 0.6
+    cols0 = packing.profile_columns(pam0.p, pam0.df.nhydro)
+    e0, tb0, _, _, _ = oracle_mod.run_column(st, sp0, cols0, 0, freqs, scat_code=[1])
+    pam = tf._one_species_pam(True)
+    nb = pam.df.fs_nbin
+    edges = tf._merged_grid(tf.wl.ICE_FS[15] + 1e-8, tf.wl.ICE_FS[16], nb)
+    f = 3e8 * np.exp(-3000.0 * edges)
+    fs = pam.df.dataFullSpec
+    fs["d_bound_ds"][:] = edges
+    d = 0.5 * (edges[1:] + edges[:-1])
+    fs["d_ds"][:] = d
+    fs["n_ds"][:] = (f[:-1] + f[1:]) / 2.0 * np.diff(edges)
+    fs["rho_ds"][:] = 200.0
+    fs["mass_ds"][:] = np.pi / 6.0 * 200.0 * d ** 3
+    sp = packing.species_from_df(pam.df.data, True)
+    cols = packing.profile_columns(pam.p, pam.df.nhydro)
+    packing.fullspec_columns(cols, fs)
+    L = int(cols["nlyrs"][0])
+    e1, tb1, _, _, _ = oracle_mod.run_column(st, sp, cols, 0, freqs, scat_code=[1],
+                                             fs_as_ratio=np.full((L, 1, nb), 0.6))
+    assert e0 == 0 and e1 == 0
+    assert np.max(np.abs(tb1 - tb0)) < 1e-6
+    # without per-bin aspect ratios a full-spectrum T-matrix species is refused
+    e2, _, _, _, _ = oracle_mod.run_column(st, sp, cols, 0, freqs, scat_code=[1])
+    assert e2 == 2
