@@ -18,6 +18,27 @@ from . import _native
 OUT_KEYS = ("scatter_matrix", "extinct_matrix", "emis_vector", "sback", "back_spec", "nmax", "status")
 
 
+C_LIGHT = 299792458.0
+
+
+def fp64_envelope(freq, ref_index, phase, dmax, as_ratio):
+    """Bins whose T-matrix the FP64 solve reproduces (True), judged by the
+    envelope measured against the REAL*16 solve of the reference: every ice
+    bin (|m| <= 1.8, all sizes to size parameter 14), and liquid bins of
+    equal-volume size parameter x <= 3, or x <= 6 with aspect ratio within
+    0.7-1.5.  Arrays [n_items, nbins] for dmax / as_ratio, [n_items] for the
+    rest."""
+    freq = np.asarray(freq, dtype=np.float64)[:, None]
+    m = np.abs(np.asarray(ref_index, dtype=np.complex128))[:, None]
+    liquid = (np.asarray(phase)[:, None] == 1)
+    dmax = np.asarray(dmax, dtype=np.float64)
+    asr = np.asarray(as_ratio, dtype=np.float64)
+    axi = np.where(asr <= 1.0, 0.5 * dmax * np.cbrt(asr), 0.5 * dmax / np.maximum(asr, 1e-300) ** (2.0 / 3.0))
+    x = 2.0 * np.pi * axi * freq / C_LIGHT
+    ok_liquid = (x <= 3.0) | ((x <= 6.0) & (asr >= 0.7) & (asr <= 1.5))
+    return ~liquid | (m <= 1.8) | ok_liquid
+
+
 def _shapes(n_items, nbins, nummu):
     return {"scatter_matrix": (n_items, 2 * nummu * 2 * nummu * 2), "extinct_matrix": (n_items, 4 * nummu),
             "emis_vector": (n_items, 2 * nummu), "sback": (n_items, 4), "back_spec": (n_items, nbins),
@@ -54,6 +75,15 @@ def calc_tmatrix_batch(freq, ref_index, phase, dmax, del_d, ndens, density, as_r
     else:
         dmax = np.asarray(dmax, dtype=np.float64)
         n_items, nbins = dmax.shape
+        inside = fp64_envelope(np.asarray(freq).reshape(n_items), np.asarray(ref_index).reshape(n_items),
+                               np.asarray(phase).reshape(n_items), dmax,
+                               np.asarray(as_ratio, dtype=np.float64).reshape(n_items, nbins))
+        occupied = np.asarray(ndens, dtype=np.float64).reshape(n_items, nbins) > 0
+        if np.any(~inside & occupied):
+            import warnings
+            warnings.warn("%d bins lie outside the FP64 envelope of the T-matrix solve (large, aspherical "
+                          "liquid drops): their T-matrix departs from the reference's REAL*16 solve"
+                          % int(np.count_nonzero(~inside & occupied)), RuntimeWarning)
         ri = np.asarray(ref_index, dtype=np.complex128).reshape(n_items)
         args = {"freq": np.ascontiguousarray(np.asarray(freq, dtype=np.float64).reshape(n_items)),
                 "ref_re": np.ascontiguousarray(ri.real), "ref_im": np.ascontiguousarray(ri.imag),

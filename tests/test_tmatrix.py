@@ -398,3 +398,17 @@ def test_oracle_fullspec_tmatrix_matches_moment_path(oracle_mod):
     # without per-bin aspect ratios a full-spectrum T-matrix species is refused
     e2, _, _, _, _ = oracle_mod.run_column(st, sp, cols, 0, freqs, scat_code=[1])
     assert e2 == 2
+
+
+def test_fp64_envelope_marks_large_aspherical_drops():
+    from pamtra_b200.tmatrix import fp64_envelope
+    # 89 GHz: x = 2 pi axi / lambda with lambda = 3.37 mm
+    freq = np.array([89e9, 89e9, 89e9])
+    ref = np.array([5.5 - 2.9j, 5.5 - 2.9j, 1.78 - 0.003j])
+    phase = np.array([1, 1, -1])
+    dmax = np.array([[1e-3, 6e-3], [1e-3, 6e-3], [1e-3, 2e-2]])
+    asr = np.array([[0.6, 0.6], [1.0, 1.0], [0.6, 0.6]])
+    ok = fp64_envelope(freq, ref, phase, dmax, asr)
+    assert ok[0, 0] and not ok[0, 1]      # a 6 mm oblate drop: x ~ 4.7, aspect ratio 0.6
+    assert ok[1, 0] and ok[1, 1]          # spheres of the same size stay inside to x = 6
+    assert ok[2].all()                    # ice: inside at all sizes
