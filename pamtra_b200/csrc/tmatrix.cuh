@@ -28,6 +28,7 @@
 // single-precision float() arithmetic (CONST, VIG) are formed the same way.
 #pragma once
 #include "common.cuh"
+#include "mie.cuh"  // eps_mix_m
 
 namespace pb {
 
