@@ -29,17 +29,9 @@
 #pragma once
 #include "common.cuh"
 #include "mie.cuh"  // eps_mix_m
+#include "tmatrix_limits.cuh"
 
 namespace pb {
-
-constexpr int TM_THREADS = 256;
-constexpr int TM_NMAX = 48;                     // orders (the reference allows 100)
-constexpr int TM_NGAUSS = 128;                  // Gauss points per half (the reference allows 500)
-constexpr int TM_NG = 2 * TM_NGAUSS;            // one node per thread
-constexpr int TM_N2 = 2 * TM_NMAX;              // unknowns of one solve
-constexpr int TM_NA = 64;                       // scattered polar angles (2 nummu, nummu <= 32)
-constexpr int TM_NAZ = 30;                      // scattering azimuths (tmatrix.f90:142)
-constexpr int TM_LBES = 1200;                   // NMAX + NNMAX2 limit of the reference (VARY)
 static_assert(TM_NG <= TM_THREADS, "one Gauss node per thread");
 
 // Scratch slot of one CTA, in doubles.

@@ -147,3 +147,143 @@ def test_double_double_solve_compiles_for_sm100a(tmp_path):
     subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "--fmad=false", "-std=c++17",
                     "-I", os.path.join(ROOT, "pamtra_b200", "csrc"), "-c", str(src), "-o", str(tmp_path / "kdd.o")],
                    check=True)
+
+
+HOST_SOLVE = r'''
+#include <cmath>
+#include <vector>
+#include "tmatrix_dd_core.cuh"
+using namespace pb;
+
+// Serial driver over the steps of the double-double solve: the flow of
+// k_tmatrix's convergence in NMAX and Gauss points, then the m >= 1 blocks.
+static bool setup(double* sd, int nmax, int ngauss, double lam, double mrr, double mri, double rev, double eps) {
+  const int ng = 2 * ngauss;
+  for (int k = 0; k < (ng + 1) / 2; k++) tdd_gauss_pair(sd, ng, k);
+  for (int t = 0; t < ngauss; t++) tdd_surface_node(sd, t, ngauss, rev, eps);
+  double ta = 0.0;
+  for (int t = 0; t < ng; t++) ta = fmax(ta, tdd_size_node(sd, t, lam, mrr, mri));
+  int n1 = 0, n2 = 0;
+  if (!tdd_lengths(ta, nmax, mrr, mri, &n1, &n2)) return false;
+  for (int t = 0; t < ng; t++) tdd_bessel_node(sd, t, nmax, n1, n2, mrr, mri);
+  return true;
+}
+static int solve(double* sd, double* tout, int m, int nmax, int ngauss, double lam, double mrr, double mri) {
+  const int mm1 = m == 0 ? 1 : m, nm = nmax - mm1 + 1, n2m = 2 * nm, ldw = 2 * n2m;
+  for (int t = 0; t < ngauss; t++) tdd_vig_node(sd, t, ngauss, nmax, m);
+  for (int pr = 0; pr < nm * nm; pr++) tdd_pair(sd, pr, m, nmax, ngauss, lam, mrr, mri);
+  for (int e = 0; e < n2m * n2m; e++) tdd_identity(sd, e, n2m);
+  for (int c = 0; c < n2m; c++) {
+    double best = -1.0;
+    int br = c;
+    for (int r = c; r < n2m; r++) {
+      const double a = tdd_pivot_key(sd, r, c, n2m);
+      if (a > best) { best = a; br = r; }
+    }
+    if (!(best > 0.0)) return 0;
+    const ddc ip = tdd_pivot_inverse(sd, br, c, n2m);
+    for (int j = c; j < ldw; j++) tdd_swap_scale(sd, c, br, j, n2m, ip);
+    for (int e = 0; e < n2m * (ldw - c - 1); e++) tdd_elim(sd, c, e, n2m);
+  }
+  for (int e = 0; e < n2m * n2m; e++) tdd_product(sd, tout, e, n2m);
+  return n2m;
+}
+extern "C" int dd_tmat(double lam, double mrr, double mri, double axi, double as_ratio, int cap, float* re,
+                       float* im) {
+  std::vector<double> sd(TDO_END), tout((size_t)2 * TM_N2 * 2 * TM_N2);
+  const double eps = 1.0 / as_ratio, rev = 1.0 * axi;
+  const double xev = 2.0 * 3.141592653589793 * rev / lam;
+  const int inm1 = (int)(xev + 4.05 * pow(xev, 0.333333)) > 4 ? (int)(xev + 4.05 * pow(xev, 0.333333)) : 4;
+  int nmax = 0, ngauss = 0, n2m = 0;
+  double qext1 = 0.0, qsca1 = 0.0;
+  auto tget = [&](int r, int c, double& a, double& b) {
+    const size_t o = 2 * ((size_t)c * (2 * n2m) + n2m + r);
+    a = tout[o];
+    b = tout[o + 1];
+  };
+  auto converged = [&]() {
+    double qe = 0.0, qs = 0.0;
+    for (int k = 1; k <= nmax; k++) {
+      double ar, ai, br, bi;
+      tget(k - 1, k - 1, ar, ai);
+      tget(k - 1 + nmax, k - 1 + nmax, br, bi);
+      const double dn1 = (double)(2 * k + 1);
+      qs = qs + dn1 * (ar * ar + ai * ai + br * br + bi * bi);
+      qe = qe + (ar + br) * dn1;
+    }
+    const double dsca = fabs((qsca1 - qs) / qs), dext = fabs((qext1 - qe) / qe);
+    qext1 = qe;
+    qsca1 = qs;
+    return dsca <= 0.001 && dext <= 0.001;
+  };
+  bool conv = false;
+  for (nmax = inm1; nmax <= TM_NMAX; nmax++) {
+    ngauss = 2 * nmax;
+    if (ngauss > TM_NGAUSS || !setup(sd.data(), nmax, ngauss, lam, mrr, mri, rev, eps)) return 0;
+    n2m = solve(sd.data(), tout.data(), 0, nmax, ngauss, lam, mrr, mri);
+    if (!n2m) return 0;
+    if (converged()) { conv = true; break; }
+  }
+  if (!conv) return 0;
+  for (int ng2 = ngauss + 1;; ng2++) {
+    if (ng2 > TM_NGAUSS) return 0;
+    ngauss = ng2;
+    if (!setup(sd.data(), nmax, ngauss, lam, mrr, mri, rev, eps)) return 0;
+    n2m = solve(sd.data(), tout.data(), 0, nmax, ngauss, lam, mrr, mri);
+    if (!n2m) return 0;
+    if (converged()) break;
+  }
+  if ((size_t)cap < (size_t)(nmax + 1) * 4 * nmax * nmax) return 0;
+  for (int m = 0; m <= nmax; m++) {
+    if (m > 0 && !(n2m = solve(sd.data(), tout.data(), m, nmax, ngauss, lam, mrr, mri))) return 0;
+    const int nm = n2m / 2, off = m == 0 ? 0 : m - 1;
+    for (int n1 = 0; n1 < nm; n1++)
+      for (int n2 = 0; n2 < nm; n2++) {
+        const int r[4] = {n1, n1, n1 + nm, n1 + nm}, c[4] = {n2, n2 + nm, n2, n2 + nm};
+        for (int b = 0; b < 4; b++) {
+          double a, bi;
+          tget(r[b], c[b], a, bi);
+          const size_t o = (((size_t)m * 4 + b) * nmax + (n1 + off)) * nmax + (n2 + off);
+          re[o] = (float)a;
+          im[o] = (float)bi;
+        }
+      }
+  }
+  return nmax;
+}
+'''
+
+
+@pytest.fixture(scope="module")
+def ddsolve():
+    d = tempfile.mkdtemp(prefix="ddsolve_")
+    src = os.path.join(d, "solve.cpp")
+    so = os.path.join(d, "libsolve.so")
+    with open(src, "w") as f:
+        f.write(HOST_SOLVE)
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-fPIC", "-shared", "-I",
+                    os.path.join(ROOT, "pamtra_b200", "csrc"), "-o", so, src], check=True)
+    lib = ctypes.CDLL(so)
+    fp = ctypes.POINTER(ctypes.c_float)
+    lib.dd_tmat.restype = ctypes.c_int
+    lib.dd_tmat.argtypes = [ctypes.c_double] * 5 + [ctypes.c_int, fp, fp]
+    return lib
+
+
+@pytest.mark.parametrize("x, asr, m", [(6.0, 0.5, (5.5, 2.9)), (10.0, 0.7, (5.5, 2.9)), (6.0, 2.0, (1.78, 0.003))])
+def test_double_double_solve_steps_reproduce_real16(ddsolve, oracle_mod, x, asr, m):
+    """The steps of the device's double-double solve (tmatrix_dd_core.cuh),
+    driven serially on the host in k_tmatrix's order, give the REAL*16
+    oracle's single-precision T-matrix where the FP64 solve does not."""
+    lam = 299792458.0 / 89e9
+    axi = x * lam / (2 * np.pi)
+    tq = oracle_mod.tmatrix_tmat(lam, m[0], m[1], axi, asr)
+    cap = 101 * 4 * 100 * 100
+    re = np.zeros(cap, np.float32)
+    im = np.zeros(cap, np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    nmax = ddsolve.dd_tmat(lam, m[0], m[1], axi, asr, cap, re.ctypes.data_as(fp), im.ctypes.data_as(fp))
+    assert tq is not None and nmax == tq.shape[2]
+    n = (nmax + 1) * 4 * nmax * nmax
+    td = (re[:n] + 1j * im[:n].astype(np.complex64)).reshape(tq.shape)
+    assert np.max(np.abs(td - tq)) <= 1e-6 * np.max(np.abs(tq))
