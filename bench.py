@@ -144,6 +144,34 @@ def oracle_tb_errors(b, idxs, tbs, pool):
     return errs, bad
 
 
+def _tm_oracle_bin(task):
+    """One bin of the T-matrix branch on the oracle (quad-precision solve,
+    one core): the worker side of tmatrix_cpu_baseline."""
+    nummu, freq, ref_re, ref_im, phase, arrs = task
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    t0 = time.perf_counter()
+    r = oracle.tmatrix_species(nummu, freq, ref_re, ref_im, phase, *arrs)
+    return time.perf_counter() - t0, r is not None
+
+
+def tmatrix_cpu_baseline(pool, cores, bins, nummu=16, freq=89e9, ref=(1.78, -0.002), phase=-1, min_tasks=0):
+    """All-core CPU figure of the T-matrix line: the given bins (dict of
+    per-bin arrays dmax, del_d, ndens, density, as_ratio, canting), cycled to
+    at least max(8 cores, min_tasks) single-bin tasks, one worker process per
+    core (the process model of runParallelPamtra); returns (bins/s, tasks,
+    wall seconds, all solved)."""
+    keys = ("dmax", "del_d", "ndens", "density", "as_ratio", "canting")
+    nb = len(bins["dmax"])
+    ntask = max(nb, 8 * cores, min_tasks)
+    tasks = [(nummu, freq, ref[0], ref[1], phase, [np.asarray(bins[k][i % nb:i % nb + 1], dtype=np.float64)
+                                                   for k in keys]) for i in range(ntask)]
+    t0 = time.perf_counter()
+    res = pool.map(_tm_oracle_bin, tasks)
+    wall = time.perf_counter() - t0
+    return ntask / wall, ntask, wall, all(ok for _, ok in res)
+
+
 def make_pool(cores):
     """Worker processes (spawned, so no CUDA state is inherited), warmed up
     outside any timed region."""
@@ -515,7 +543,7 @@ def _serving(args, local):
 
 
 # ---------------------------------------------------------------- reference arm
-def _tmatrix_line(args, eng, dev, cpu_leg):
+def _tmatrix_line(args, eng, dev, cpu_leg, pool=None, cores=1):
     """The T-matrix branch (scat_name 'tmatrix', src/tmatrix.f90:14) on a
     snow-like batch: soft ice spheroids (300 kg/m3, aspect ratio 0.6) in 32
     bins of 0.2-4 mm at 89 GHz, NUMMU 16, upright, per (layer, frequency)
@@ -596,6 +624,12 @@ def _tmatrix_line(args, eng, dev, cpu_leg):
         line["cpu_baseline"] = {"value": nb / cpu_s, "unit": "bins/s", "cores": 1, "kind": "port",
                                 "sample": "the first item's %d bins, quad-precision T-matrix solve like the "
                                           "reference's REAL*16 tmatrix_amplq" % nb}
+        if pool is not None:
+            v, ntask, wall, ok = tmatrix_cpu_baseline(pool, cores, {k: a[k][0] for k in a})
+            line["cpu_baseline"]["all_cores"] = {"value": v, "unit": "bins/s", "cores": cores, "tasks": ntask,
+                                                 "wall_s": wall, "all_solved": ok,
+                                                 "sample": "the first item's bins cycled to %d one-bin tasks, "
+                                                           "one worker process per core" % ntask}
         line["max_rel_err_vs_oracle"] = err
     return line
 
@@ -802,7 +836,7 @@ def main():
                             wl.mie_heavy_batch(args.mieheavy_cols, seed=6), local, eng, stream, pool) \
         if args.mieheavy_cols > 0 else None
     serving = _serving(args, local) if args.serve_requests > 0 else None
-    tmat = _tmatrix_line(args, eng, dev, not args.no_cpu) if args.tmatrix_items > 0 else None
+    tmat = _tmatrix_line(args, eng, dev, not args.no_cpu, pool, cores) if args.tmatrix_items > 0 else None
     # ---- roofline of the dominant kernel (doubling stage)
     peak = fp64_peak_tflops(dev)
     t_layer = stage_tot.get("layer", 0.0) / args.steps * 1e-3
@@ -916,6 +950,7 @@ def main():
                                               g(serving, "batched_3xtf32", "rate_half_capacity", "p99_ms")],
         "tmatrix_bins_per_s": {"gpu": g(tmat, "value"), "e2e": g(tmat, "e2e", "value"),
                                "cpu_1core": g(tmat, "cpu_baseline", "value"),
+                               "cpu_all_cores": g(tmat, "cpu_baseline", "all_cores", "value"),
                                "max_rel_err_vs_oracle": g(tmat, "max_rel_err_vs_oracle")},
         "serving_solves_per_s": {"3xtf32": g(serving, "batched_3xtf32", "rate_200", "solves_per_s"),
                                  "fp64": g(serving, "batched_fp64", "rate_200", "solves_per_s"),

@@ -412,3 +412,19 @@ def test_fp64_envelope_marks_large_aspherical_drops():
     assert ok[0, 0] and not ok[0, 1]      # a 6 mm oblate drop: x ~ 4.7, aspect ratio 0.6
     assert ok[1, 0] and ok[1, 1]          # spheres of the same size stay inside to x = 6
     assert ok[2].all()                    # ice: inside at all sizes
+
+
+def test_bench_tmatrix_cpu_baseline_all_cores():
+    """The all-core CPU figure of the bench's T-matrix line: single-bin oracle
+    tasks over a spawned pool (no GPU involved)."""
+    import multiprocessing as mp
+    import bench
+    bins = {"dmax": np.array([0.5e-3, 1.0e-3]), "del_d": np.full(2, 1e-4), "ndens": np.full(2, 1e6),
+            "density": np.full(2, 300.0), "as_ratio": np.full(2, 0.6), "canting": np.zeros(2)}
+    pool = mp.get_context("spawn").Pool(2)
+    try:
+        v, ntask, wall, ok = bench.tmatrix_cpu_baseline(pool, 2, bins, min_tasks=4)
+    finally:
+        pool.close()
+        pool.join()
+    assert ok and ntask == 16 and v > 0 and wall > 0
