@@ -96,6 +96,10 @@ def lib():
         l.orc_tmatrix_species.restype = ctypes.c_int
         l.orc_tmatrix_species.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                                           ctypes.c_int, ctypes.c_int] + [dp] * 11
+        l.orc_layer_start.restype = ctypes.c_int
+        l.orc_layer_start.argtypes = [ctypes.c_int] + [ctypes.c_double] * 4 + [dp, ctypes.c_double, ctypes.c_double,
+                                                                                ctypes.c_void_p, ctypes.c_void_p] + \
+            [dp] * 4
         l.orc_miecalc.restype = ctypes.c_int
         l.orc_miecalc.argtypes = [ctypes.c_double] * 3 + [ctypes.c_int] + [dp] * 4
         l.orc_minvert.restype = ctypes.c_int
@@ -387,3 +391,21 @@ def tmatrix_tmat64(lam, mrr, mri, axi, as_ratio, kind="f64"):
         return None
     n = (nmax + 1) * 4 * nmax * nmax
     return (re[:n] + 1j * im[:n].astype(np.complex64)).reshape(nmax + 1, 4, nmax, nmax)
+
+
+def layer_start(N, zdiff, gas, planck0, planck1, scat, ext_k, emis_k, tm_ext=None, tm_emis=None):
+    """The oracle's start of a scattering layer (doubling count, INITIAL_SOURCE4,
+    INITIALIZE4): scat [4][2N][2N] row-major; returns (num_doubles, R, T
+    [2][2N][2N] column-major, lin [2][2N], linfactor)."""
+    n = 2 * N
+    sc = np.ascontiguousarray(scat, dtype=np.float64)
+    R = np.zeros(2 * n * n)
+    T = np.zeros(2 * n * n)
+    lin = np.zeros(2 * n)
+    lf = ctypes.c_double(0.0)
+    te = None if tm_ext is None else np.ascontiguousarray(tm_ext, dtype=np.float64)
+    tv = None if tm_emis is None else np.ascontiguousarray(tm_emis, dtype=np.float64)
+    nd = lib().orc_layer_start(N, zdiff, gas, planck0, planck1, _p(sc), ext_k, emis_k,
+                               te.ctypes.data if te is not None else None,
+                               tv.ctypes.data if tv is not None else None, _p(R), _p(T), _p(lin), ctypes.byref(lf))
+    return nd, R, T, lin, lf.value

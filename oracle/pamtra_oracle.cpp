@@ -1399,10 +1399,14 @@ struct Layer {  // R,T (n x n, two parts each), S (n, two parts)
   std::vector<double> S;
 };
 
-// src/radintg4.f90:1-45 INITIALIZE4 + 51-73 INITIAL_SOURCE4 + 174-309 DOUBLING_INTEGRATION4
-void scattering_layer(int N, const std::vector<double>& mu, const std::vector<double>& w, double zdiff, double gas,
-                      double planck0, double planck1, const std::vector<double>& scat, double ext_k, double emis_k,
-                      Layer& out, int& num_doubles, const double* tm_ext = nullptr, const double* tm_emis = nullptr) {
+// The start of a scattering layer: the number of doublings from
+// extinct_matrix(1) + gas (src/radtran4.f90:319-329), INITIAL_SOURCE4
+// (src/radintg4.f90:51-73) and INITIALIZE4 (:1-45).  With T-matrix species
+// the extinction matrix and emission vector are theirs plus scatcnv's.
+void layer_start(int N, const std::vector<double>& mu, const std::vector<double>& w, double zdiff, double gas,
+                 double planck0, double planck1, const std::vector<double>& scat, double ext_k, double emis_k,
+                 const double* tm_ext, const double* tm_emis, Mat& R, Mat& T, std::vector<double>& lin,
+                 int& num_doubles, double& linfactor) {
   const int n = 2 * N;
   // extinct_matrix(1) + gas (src/radtran4.f90:323); with T-matrix species the
   // layer's matrices are theirs plus scatcnv's
@@ -1413,7 +1417,7 @@ void scattering_layer(int N, const std::vector<double>& mu, const std::vector<do
   double num_sub = (double)std::ldexp(1.0f, num_doubles);
   double delta_z = zdiff / num_sub;
   // INITIAL_SOURCE4
-  std::vector<double> lin(2 * n);
+  lin.assign(2 * n, 0.0);
   for (int i = 0; i < 2; i++)
     for (int j = 0; j < N; j++) {
       double e = (i == 0) ? gas : 0.0;
@@ -1423,10 +1427,11 @@ void scattering_layer(int N, const std::vector<double>& mu, const std::vector<do
       lin[i + 2 * j] = tmp * (ev + e);
       lin[n + i + 2 * j] = tmp * (ev + e);
     }
-  double linfactor = (planck0 == 0.0) ? 0.0 : (planck1 / planck0 - 1.0) / num_sub;
+  linfactor = (planck0 == 0.0) ? 0.0 : (planck1 / planck0 - 1.0) / num_sub;
   // INITIALIZE4
   const double C = 2.0 * 3.1415926535897932384;
-  Mat R((size_t)2 * n * n), T((size_t)2 * n * n);
+  R.assign((size_t)2 * n * n, 0.0);
+  T.assign((size_t)2 * n * n, 0.0);
   const double* Q1 = &scat[0];
   const double* Q2 = &scat[(size_t)1 * n * n];
   const double* Q3 = &scat[(size_t)2 * n * n];
@@ -1454,6 +1459,18 @@ void scattering_layer(int N, const std::vector<double>& mu, const std::vector<do
         }
       }
     }
+}
+
+// src/radintg4.f90:1-45 INITIALIZE4 + 51-73 INITIAL_SOURCE4 + 174-309 DOUBLING_INTEGRATION4
+void scattering_layer(int N, const std::vector<double>& mu, const std::vector<double>& w, double zdiff, double gas,
+                      double planck0, double planck1, const std::vector<double>& scat, double ext_k, double emis_k,
+                      Layer& out, int& num_doubles, const double* tm_ext = nullptr, const double* tm_emis = nullptr) {
+  const int n = 2 * N;
+  Mat R, T;
+  std::vector<double> lin;
+  double linfactor = 0.0;
+  layer_start(N, mu, w, zdiff, gas, planck0, planck1, scat, ext_k, emis_k, tm_ext, tm_emis, R, T, lin, num_doubles,
+              linfactor);
   // DOUBLING_INTEGRATION4 with SYMMETRIC = .true.
   std::vector<double> cst(lin), tlin(2 * n), tcst(2 * n);
   double linfac = linfactor;
@@ -1729,6 +1746,26 @@ int orc_miecalc(double x, double mr, double mi, int cap, double* a_re, double* a
     b_im[n] = b[n + 1].im;
   }
   return nterms;
+}
+
+// The start of a scattering layer (layer_start) for tests of the device's
+// layer start: scat [4][n][n] (rows i2 + 2 j2, columns i1 + 2 j1), the
+// optional T-matrix extinction matrix [2][2][N] and emission [2][N]; R and T
+// [2][n][n] column-major, lin [2][n]; returns the number of doublings.
+int orc_layer_start(int N, double zdiff, double gas, double planck0, double planck1, const double* scat, double ext_k,
+                    double emis_k, const double* tm_ext, const double* tm_emis, double* R_out, double* T_out,
+                    double* lin_out, double* linfactor) {
+  const int n = 2 * N;
+  std::vector<double> mu, w;
+  lobatto(N, mu, w);
+  std::vector<double> sc(scat, scat + (size_t)4 * n * n), lin;
+  Mat R, T;
+  int nd = 0;
+  layer_start(N, mu, w, zdiff, gas, planck0, planck1, sc, ext_k, emis_k, tm_ext, tm_emis, R, T, lin, nd, *linfactor);
+  std::copy(R.begin(), R.end(), R_out);
+  std::copy(T.begin(), T.end(), T_out);
+  std::copy(lin.begin(), lin.end(), lin_out);
+  return nd;
 }
 
 // eps_mix((1,0), m, density) of src/eps_mix.f90 (the soft-spheroid mixing

@@ -131,15 +131,21 @@ def test_ddreal_pow(ddlib):
 
 
 def test_double_double_solve_compiles_for_sm100a(tmp_path):
-    """The double-double T-matrix solve (tmatrix_dd.cuh) is not yet linked
-    into the library; it must keep compiling for sm_100a until its GPU parity
-    run enables it."""
+    """The double-double T-matrix solve (tmatrix_dd.cuh) and the layer start
+    with T-matrix species (tm_layer_core.cuh) are not yet linked into the
+    library; they must keep compiling for sm_100a until their GPU parity
+    runs enable them."""
     import shutil
     nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     if not os.path.exists(nvcc):
         pytest.skip("nvcc not available")
     src = tmp_path / "kdd.cu"
-    src.write_text('#include "tmatrix_dd.cuh"\nusing namespace pb;\n'
+    src.write_text('#include "tmatrix_dd.cuh"\n#include "tm_layer_core.cuh"\nusing namespace pb;\n'
+                   '__global__ void kly(const double* mu, const double* w, const double* te, const double* tv,\n'
+                   '                    double* R, double* T, double* lin) {\n'
+                   '  double dz; tml_doublings(1e-3, te, 1e-4, 250.0, &dz);\n'
+                   '  tml_init4(threadIdx.x, 32, 32, mu, w, dz, 1e-4, 1e-3, te, R, T);\n'
+                   '  lin[threadIdx.x] = tml_source(threadIdx.x, mu, 1e-7, dz, 1e-4, 1e-4, tv);\n}\n'
                    '__global__ void __launch_bounds__(256, 1) kdd(double* s, double* sd, int* o) {\n'
                    '  __shared__ TmShared sh;\n'
                    '  if (!tdd_setup(sd, sh, 8, 16, 3.37e-3, 5.5, 2.9, 1e-3, 1.6)) { o[0] = -1; return; }\n'
